@@ -1,0 +1,410 @@
+"""Benchmark of the LIJ (line-implicit Jacobi) solver on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--config c2|c3a|c3b] [--algo fp64|ref|mixed]
+
+A step is one LIJ solve of the configured system from U = 0 to the relative
+residual tolerance (default: 360 lines x 384 cells = 138,240 cells, 9x9
+FP64 blocks, seeded synthetic values with shift 9, tolerance 1e-12).  The
+metric is LIJ sweeps per second: total sweeps of all steps on all GPUs
+divided by the device time (CUDA events, max over ranks).  The blocks stay
+resident in HBM for `value`; `e2e` repeats the step through the C ABI from
+pinned host buffers (Jacobian upload, factorization, solve, solution
+read-back every step).
+
+With N > 1 (torchrun) every rank solves its own independent system of the
+same size: independent systems shard with no data-path collective (weak
+scaling); NCCL carries only the barrier and the max/sum reductions of the
+timings.  --impl reference times the CPU restatement of the reference path
+(oracle/, OpenMP over lines on all host cores) on the same system: one
+sweep per step, rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+CONFIGS = {
+    # name: (lines L, cells per line K, diagonal shift, tolerance)
+    "c1": (60, 64, 9.0, 1e-12),
+    "c2": (360, 384, 9.0, 1e-12),
+    "c3a": (600, 640, 4.0, 1e-10),
+    "c3b": (1200, 1280, 4.0, 1e-10),
+}
+SEED = 1
+# paper Table 5 (V100, FP64): 5 LIJ iterations on ex06 (138,240 cells) in 8.470 ms
+PUBLISHED_SWEEPS_PER_S = {"c2": 5 / 0.008470, "c3a": 5 / 0.018741, "c3b": 5 / 0.076733}
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def aggregate(values, op):
+    """max / sum of per-rank values (plain Python; the NCCL path mirrors it)."""
+    return max(values) if op == "max" else sum(values)
+
+
+class Dist:
+    def __init__(self, ws, rank, local, backend):
+        self.ws, self.rank, self.local = ws, rank, local
+        self.pg = None
+        if ws > 1:
+            import datetime
+
+            import torch.distributed as dist
+            dist.init_process_group(backend, timeout=datetime.timedelta(seconds=300))
+            self.pg = dist
+
+    def barrier(self):
+        if self.pg:
+            self.pg.barrier()
+
+    def reduce(self, value, op):
+        if not self.pg:
+            return value
+        import torch
+        dev = "cuda" if torch.cuda.is_available() and self.pg.get_backend() == "nccl" else "cpu"
+        t = torch.tensor([float(value)], dtype=torch.float64, device=dev)
+        self.pg.all_reduce(t, op=self.pg.ReduceOp.MAX if op == "max" else self.pg.ReduceOp.SUM)
+        return float(t.item())
+
+    def close(self):
+        if self.pg:
+            self.pg.destroy_process_group()
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons while the measurement runs."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+
+    def __enter__(self):
+        try:
+            os.makedirs(os.path.dirname(self.path), exist_ok=True)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100", "-i", str(self.gpu)], stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+            self.f.close()
+
+    def summary(self):
+        if not self.proc:
+            return None
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                rows.append((float(parts[1]), float(parts[2]), float(parts[3]), parts[5:9]))
+            except ValueError:
+                continue
+        if not rows:
+            return None
+        loaded = [r for r in rows if r[2] > 200.0] or rows
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in loaded for i, v in enumerate(r[3]) if v == "Active"})
+        return {"sm_mhz": statistics.median(r[0] for r in loaded), "sm_max_mhz": loaded[0][1],
+                "reasons": reasons, "samples": len(rows), "samples_under_load": len(loaded)}
+
+
+def measured_peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        return float(json.load(open(p))["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def build_problem(L, K, shift, pinned):
+    from triblocksolve_b200 import Mesh
+    from triblocksolve_b200 import _native as N
+    mesh = Mesh.structured(L, K)
+    nb = 81
+    sizes = {"jacD": nb * mesh.nelem, "jacO1": nb * mesh.nintface, "jacO2": nb * mesh.nintface,
+             "rhs": 9 * mesh.nelem}
+    if pinned:
+        import torch
+        host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+                for k, n in sizes.items()}
+    else:
+        host = {k: np.empty(n) for k, n in sizes.items()}
+    N.check(N.lib.tbs_gen_jacobian(9, mesh.nelem, mesh.nintface, float(shift), SEED,
+                                   N.dptr(host["jacD"]), N.dptr(host["jacO1"]),
+                                   N.dptr(host["jacO2"]), N.dptr(host["rhs"]), None))
+    return mesh, host
+
+
+def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
+    """The oracle (restated reference path) on all host cores; sweeps/s."""
+    import oracle
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    t_factor = time.perf_counter() - t0
+    if sweeps is None:
+        t0 = time.perf_counter()
+        b.sweeps(1)
+        t1 = time.perf_counter() - t0
+        sweeps = int(max(1, min(200, budget_s / max(t1, 1e-6))))
+        b.reset()
+    t0 = time.perf_counter()
+    b.sweeps(sweeps)
+    dt = time.perf_counter() - t0
+    return {"value": sweeps / dt, "unit": "sweeps/s", "cores": threads, "kind": "port",
+            "sample": f"{sweeps} FP64 sweeps of the same {mesh.nline}x{mesh.max_line_nelem} system "
+                      f"after one factorization ({t_factor:.2f} s), oracle/lij_oracle.c, OpenMP "
+                      f"over lines, {threads} threads",
+            "factor_s": t_factor, "seconds": dt}
+
+
+def run_reference(args, L, K, shift, tol):
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    mesh, host = build_problem(L, K, shift, pinned=False)
+    import oracle
+    threads = os.cpu_count() or 1
+    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    for _ in range(args.warmup):
+        b.sweeps(1)
+    b.reset()
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(args.steps):
+        b.sweeps(1)
+        done += 1
+    dt = time.perf_counter() - t0
+    v = done / dt
+    line = {"impl": "reference", "metric": "LIJ sweeps/s", "value": v, "unit": "sweeps/s",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"LIJ FP64 sweeps, {L}x{K} structured mesh ({mesh.nelem} cells), "
+                                   f"shift {shift}, seed {SEED}; one sweep per step",
+                       "cells": mesh.nelem},
+            "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": threads, "kind": "port",
+                             "sample": f"{done} sweeps (one per step) after one factorization; "
+                                       "oracle/lij_oracle.c with OpenMP over lines (the "
+                                       "reference's OCCA kernels need OCCA/MPI/gfortran, absent)"},
+            "e2e": {"value": v, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed"])
+    ap.add_argument("--e2e-steps", type=int, default=None)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    L, K, shift, tol = CONFIGS[args.config]
+    if args.impl == "reference":
+        return run_reference(args, L, K, shift, tol)
+
+    import torch
+
+    import triblocksolve_b200 as tbs
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    algo = {"fp64": tbs.ALGO_FP64, "ref": tbs.ALGO_REFERENCE, "mixed": tbs.ALGO_MIXED}[args.algo]
+
+    mesh, host = build_problem(L, K, shift, pinned=True)
+    # a dedicated stream: CUDA graphs cannot be captured on the legacy default stream
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    solver = tbs.Solver(local)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_mesh(mesh)
+    solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+    torch.cuda.synchronize()
+    f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    f0.record()
+    solver.factor(algo)
+    f1.record()
+    torch.cuda.synchronize()
+    factor_ms = f0.elapsed_time(f1)
+    max_sweeps = 400
+
+    with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 0)):
+            solver.solve(tol, max_sweeps)
+        # ---------------- timed region: K solves, blocks resident in HBM
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        sweeps_total = 0
+        last_hist = None
+        for _ in range(args.steps):
+            s, last_hist = solver.solve(tol, max_sweeps)
+            sweeps_total += s
+        t1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        elapsed_ms = t0.elapsed_time(t1)
+        # ---------------- per-kernel CUDA-event timing (same solves, eager launch)
+        solver.profile(True)
+        solver.profile_reset()
+        nprof = max(1, min(args.steps, 20))
+        prof_sweeps = 0
+        for _ in range(nprof):
+            s, _h = solver.solve(tol, max_sweeps)
+            prof_sweeps += s
+        prof = solver.profile_read()
+        solver.profile(False)
+        # ---------------- e2e: upload + factor + solve + read back, from pinned host memory
+        ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 20))
+        Uh = torch.empty(9 * mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
+        for _ in range(1):
+            solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+            solver.factor(algo)
+            solver.solve(tol, max_sweeps)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_sweeps = 0
+        for _ in range(ne2e):
+            solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+            solver.factor(algo)
+            s, hh = solver.solve(tol, max_sweeps)
+            Uh[:] = solver.solution()
+            e2e_sweeps += s
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.summary()
+
+    max_ms = dist.reduce(elapsed_ms, "max")
+    all_sweeps = dist.reduce(sweeps_total, "sum")
+    max_e2e_ms = dist.reduce(e2e_ms, "max")
+    all_e2e_sweeps = dist.reduce(e2e_sweeps, "sum")
+    true_rel = solver.true_residual_norm() / float(last_hist[0])
+
+    if rank == 0:
+        value = all_sweeps / (max_ms * 1e-3)
+        peak, peak_kind = measured_peak_hbm()
+        kern = {}
+        for name, (launches, ms) in prof.items():
+            try:
+                b = solver.kernel_bytes(name)
+            except Exception:
+                b = None
+            avg_us = 1e3 * ms / launches if launches else 0.0
+            kern[name] = {"launches": launches, "total_ms": round(ms, 4),
+                          "avg_us": round(avg_us, 3),
+                          "bytes_per_launch": b,
+                          "gbs": round(b / (avg_us * 1e-6) / 1e9, 1) if b and avg_us > 0 else None}
+        hot = [k for k in kern if kern[k]["bytes_per_launch"] and k not in ("fast_resid_rhs",
+                                                                             "fast_resid32_rhs")]
+        dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
+        traffic = None
+        tpath = os.path.join(ROOT, "profiles", "traffic.json")
+        if dom and os.path.exists(tpath):
+            t = json.load(open(tpath)).get(args.config, {}).get(dom)
+            if t:
+                traffic = t
+        roof = None
+        if dom:
+            ach = kern[dom]["gbs"]
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "traffic": traffic,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": kern[dom]["bytes_per_launch"],
+                    "avg_launch_us": kern[dom]["avg_us"]}
+        launches_per_solve = sum(v["launches"] for v in kern.values()) / nprof
+        sweeps_per_solve = sweeps_total / args.steps
+        h2d = sum(host[k].nbytes for k in ("jacD", "jacO1", "jacO2", "rhs"))
+        d2h = Uh.nbytes + 8 * (max_sweeps + 1)
+        ref_bytes = (8.0 * (387 * mesh.nelem + 162 * mesh.nintface)) * sweeps_per_solve
+        line = {
+            "metric": "LIJ sweeps/s", "value": round(value, 2), "unit": "sweeps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak",
+            "vs_baseline": (round(value / ws / PUBLISHED_SWEEPS_PER_S[args.config], 3)
+                            if args.config in PUBLISHED_SWEEPS_PER_S and args.algo != "mixed"
+                            else None),
+            "dtype": "f64" if args.algo != "mixed" else "f32+f64",
+            "data": "synthetic: seeded structured mesh and values (shift %g, seed %d); the "
+                    "reference's real Jacobians are not available" % (shift, SEED),
+            "config": {
+                "workload": f"LIJ solve to {tol:g} relative residual from U=0, {L} lines x {K} "
+                            f"cells ({mesh.nelem} cells, {mesh.nintface} faces), 9x9 blocks, "
+                            f"algo {args.algo}",
+                "cells": mesh.nelem, "lines": L, "cells_per_line": K, "tol": tol,
+                "algo": args.algo, "sweeps_per_solve": sweeps_per_solve,
+                "time_to_tol_ms": round(max_ms / args.steps, 4),
+                "factor_ms": round(factor_ms, 3),
+                "true_rel_residual": true_rel,
+                "l2": "no flush: every sweep streams %.0f MB of blocks, > 126 MB L2" %
+                      (8 * 81 * 5 * mesh.nelem / 1e6),
+                "reference_model_gbs": round(ref_bytes * value / ws / 1e9, 1),
+                "published_baseline": "V100 FP64 LIJ, paper Table 5 (5 sweeps); vs_baseline "
+                                      "is per GPU",
+                "parallelism": f"{ws} independent systems, one per GPU" if ws > 1 else "1 GPU",
+            },
+            "roofline": roof,
+            "kernels": kern,
+            "e2e": {"value": round(all_e2e_sweeps / (max_e2e_ms * 1e-3), 2), "unit": "sweeps/s",
+                    "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h),
+                    "steps": ne2e,
+                    "what": "per step: tbs_set_jacobian from pinned host memory, tbs_factor, "
+                            "tbs_solve, tbs_get_solution"},
+            "gpu_launches": int(round(launches_per_solve * args.steps)),
+            "clocks": clk,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            line["cpu_baseline"] = cpu_baseline(mesh, host)
+        print(json.dumps(line), flush=True)
+    solver.close()
+    dist.close()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,254 @@
+/*
+ * triblock.h -- C ABI of libtriblock.so, the B200 line-implicit Jacobi (LIJ) solver.
+ *
+ * The reference (ackirby88/triblocksolve) exposes no plugin API.  Its de-facto
+ * boundary is (1) the two Fortran bind(C) readers, (2) the Mesh/Jacobian
+ * classes, (3) the OKL kernel argument lists launched from src/main.cxx and
+ * (4) the CLI `triblock.exe <compute_mode> <device_id> <block_size>`.  Every
+ * entry point below names the reference interface it replaces.
+ *
+ * Conventions
+ *   - Every tbs_* function returns an int status (TBS_OK == 0).  Nothing
+ *     exits the process and no C++ exception crosses this boundary.
+ *   - Index arrays passed to tbs_* are 0-based, i.e. exactly what the
+ *     reference holds in memory after read_mesh_data_ shifted them
+ *     (src/F90/read_mesh_data.F90:41-64).
+ *   - Block storage is column-major FP64: entry (row i, col j) of block b is
+ *     at i + nvar*j + nvar*nvar*b, the OKL @dim(NVAR,NVAR,n) convention
+ *     (src/okl/linesmoothLU_TriBlock_v3.okl:7).
+ *   - A context owns one CUDA stream and all of its device memory; one
+ *     context must be used from one host thread at a time.
+ *   - There is no CPU fallback: a context can only be created on a CUDA
+ *     device, and compute_mode values other than 2 (CUDA) are rejected.
+ */
+#ifndef TRIBLOCK_H
+#define TRIBLOCK_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- status */
+#define TBS_OK               0
+#define TBS_ERR_ARG          1  /* bad argument (null pointer, negative size, ...) */
+#define TBS_ERR_IO           2  /* file missing, short read, write failure */
+#define TBS_ERR_FORMAT       3  /* header/array inconsistency in mesh or Jacobian */
+#define TBS_ERR_CUDA         4  /* CUDA runtime error or no device */
+#define TBS_ERR_STATE        5  /* call out of order (e.g. sweep before factor) */
+#define TBS_ERR_NUMERIC      6  /* zero / non-finite pivot in the no-pivot block LU */
+#define TBS_ERR_UNSUPPORTED  7  /* nvar or mode this build does not support */
+#define TBS_ERR_NOMEM        8  /* device or host allocation refused */
+
+/* ---------------------------------------------------- algorithm / precision
+ * TBS_ALGO_REFERENCE  reference operation order (LU-form blocks, solveLU,
+ *                     full residual R = rhs + J U each sweep).  Compiled
+ *                     without FMA contraction so that U, dU and R are
+ *                     bit-identical to the CPU oracle.
+ * TBS_ALGO_FP64       FP64, line-ordered storage, explicit block inverses,
+ *                     residual updated from the cross-line couplings only
+ *                     (R_{s+1} = O dU_{s+1}, exact for an exact line solve).
+ * TBS_ALGO_MIXED      FP32 line factors and FP32 inner sweeps on the
+ *                     correction equation; residual, solution accumulation
+ *                     and convergence test in FP64 (outer refinement).
+ */
+#define TBS_ALGO_REFERENCE 0
+#define TBS_ALGO_FP64      1
+#define TBS_ALGO_MIXED     2
+
+/* compute modes of the reference CLI (include/Platform.hxx:17-23) */
+#define TBS_SERIAL_MODE 0
+#define TBS_HIP_MODE    1
+#define TBS_CUDA_MODE   2
+#define TBS_OPENCL_MODE 3
+#define TBS_OPENMP_MODE 4
+#define TBS_DPCPP_MODE  5
+#define TBS_METAL_MODE  6
+
+typedef struct tbs_ctx tbs_ctx;
+
+/* ============================================================ file formats */
+
+/* Replaces the Fortran reader src/F90/read_mesh_data.F90:8-65 (declared at
+ * include/Mesh.hxx:22-25).  Same signature and semantics: reads
+ * ./gpuline.mesh.data.bin (stream binary, little-endian int32), fills the
+ * caller-sized arrays and converts 1-based indices to 0-based.  The Fortran
+ * routine reports nothing; failures here leave the arrays untouched and are
+ * reported by tbs_last_error(NULL). */
+void read_mesh_data_(int *nvar, int *nelem, int *nintface,
+                     int *eftot, int *nline, int *nlineelem,
+                     int *epoint, int *ef, int *fc, int *lines,
+                     int *linesize, int *linepoint, int *lineface);
+
+/* Replaces src/F90/read_jacobian_data.F90:8-33 (declared at
+ * include/Jacobian.hxx:23-25): reads ./gpuline.jacobian.data.bin. */
+void read_jacobian_data_(int *nvar, int *nelem, int *nintface,
+                         double *jacD, double *jacO1, double *jacO2,
+                         double *rhs, double *U0);
+
+/* Header of a mesh file: hdr = {nvar, nelem, nintface, eftot, nline, nlineelem}
+ * (src/Mesh.cxx:21-32).  Also checks that the file size matches the header. */
+int tbs_read_mesh_header(const char *path, int hdr[6]);
+
+/* Path form of read_mesh_data_ with a status; outputs are 0-based. */
+int tbs_read_mesh(const char *path, const int hdr[6],
+                  int *epoint, int *ef, int *fc, int *linesize,
+                  int *linepoint, int *lines, int *lineface);
+
+/* Writes a mesh file in the reference layout (inputs 0-based, written 1-based). */
+int tbs_write_mesh(const char *path, const int hdr[6],
+                   const int *epoint, const int *ef, const int *fc,
+                   const int *linesize, const int *linepoint,
+                   const int *lines, const int *lineface);
+
+/* Header of a Jacobian file: hdr = {nvar, nelem, nintface}
+ * (src/Jacobian.cxx:22-27); checks the file size. */
+int tbs_read_jacobian_header(const char *path, int hdr[3]);
+
+int tbs_read_jacobian(const char *path, const int hdr[3],
+                      double *jacD, double *jacO1, double *jacO2,
+                      double *rhs, double *U0);
+
+int tbs_write_jacobian(const char *path, const int hdr[3],
+                       const double *jacD, const double *jacO1,
+                       const double *jacO2, const double *rhs,
+                       const double *U0);
+
+/* Checks the index invariants every solver path relies on: index ranges,
+ * linepoint prefix sums, lines a permutation of the elements, lineface[m]
+ * (k >= 1) joining lines[m-1] and lines[m].  The reference checks nothing. */
+int tbs_validate_mesh(const int hdr[6],
+                      const int *epoint, const int *ef, const int *fc,
+                      const int *linesize, const int *linepoint,
+                      const int *lines, const int *lineface);
+
+/* ======================================================= synthetic inputs
+ * Structured L x K quad mesh in the reference's numbering; it reproduces
+ * data/ex05/gpuline.mesh.data.bin (L=60, K=64) bit for bit. */
+int tbs_gen_structured_header(int L, int K, int nvar, int hdr[6]);
+int tbs_gen_structured_mesh(int L, int K,
+                            int *epoint, int *ef, int *fc, int *linesize,
+                            int *linepoint, int *lines, int *lineface);
+
+/* Seeded values in file order: jacD = U(-1,1) + shift*I, jacO1/jacO2 =
+ * 0.1*U(-1,1), rhs = U(-1,1), U0 = 0.  U(-1,1) of stream position n is
+ * splitmix64(seed + (n+1)*0x9E3779B97F4A7C15) mapped to [-1,1) with 53
+ * bits, so host and device generation agree bit for bit.  Runs on all host
+ * threads. */
+int tbs_gen_jacobian(int nvar, int nelem, int nintface, double shift,
+                     uint64_t seed, double *jacD, double *jacO1,
+                     double *jacO2, double *rhs, double *U0);
+
+/* Block-size change of src/Jacobian.cxx:153-238 with the same resulting
+ * arrays: new diagonals of D, O1, O2 set to 10.0, the old min(nv)-square
+ * sub-blocks copied in, and -- as the reference's vector::resize leaves
+ * them -- the leading entries of every array keeping the old flat data
+ * wherever neither rule writes.  rhs and U0 copy their first
+ * nelem*min(nv) entries flat.  Output arrays are sized for nv_new. */
+int tbs_resize_block_size(int nv_old, int nv_new, int nelem, int nintface,
+                          const double *D_old, const double *O1_old,
+                          const double *O2_old, const double *rhs_old,
+                          const double *U0_old, double *D, double *O1,
+                          double *O2, double *rhs, double *U0);
+
+/* ================================================================ solver */
+
+/* Device selection, replacing Platform(comm, mode, device_id)
+ * (src/Platform.cxx:11-78).  Fails with TBS_ERR_CUDA when no device exists. */
+int tbs_create(int device_id, tbs_ctx **out);
+int tbs_destroy(tbs_ctx *ctx);
+
+/* Last error text of ctx, or of the calling thread when ctx is NULL. */
+const char *tbs_last_error(const tbs_ctx *ctx);
+
+/* Launch on a caller-owned cudaStream_t instead of the context's own
+ * stream (pass NULL to return to the context's stream). */
+int tbs_set_stream(tbs_ctx *ctx, void *cuda_stream);
+
+/* Replaces Mesh::setupDevice/toDevice (src/Mesh.cxx:75-94).  Copies the
+ * 0-based mesh in; the caller keeps ownership of its arrays. */
+int tbs_set_mesh(tbs_ctx *ctx, int nvar, int nelem, int nintface, int eftot,
+                 int nline, int nlineelem,
+                 const int *epoint, const int *ef, const int *fc,
+                 const int *linesize, const int *linepoint,
+                 const int *lines, const int *lineface);
+
+/* Replaces Jacobian::setupDevice/toDevice (src/Jacobian.cxx:240-277).
+ * Host pointers; U0 may be NULL.  As in the reference, the solution
+ * starts at zero (U0 is kept only for tbs_set_initial). */
+int tbs_set_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1,
+                     const double *jacO2, const double *rhs, const double *U0);
+
+/* Same, from device pointers already resident on the context's device
+ * (copied device-to-device on the context's stream). */
+int tbs_set_jacobian_device(tbs_ctx *ctx, const double *d_jacD,
+                            const double *d_jacO1, const double *d_jacO2,
+                            const double *d_rhs);
+
+/* New right-hand side for the already factored Jacobian (host pointer);
+ * resets U to zero and R to rhs. */
+int tbs_set_rhs(tbs_ctx *ctx, const double *rhs);
+
+/* Starting solution (host pointer, 9*nelem): R becomes rhs + J U.
+ * Checkpoint/resume of a solve; the reference always starts from 0. */
+int tbs_set_initial(tbs_ctx *ctx, const double *U);
+
+/* Replaces copyAtoBjac + lineLU (src/main.cxx:180-190,
+ * src/okl/lineLU_v2.okl:58-182, src/okl/linesmoothLU_v5.okl:85-93) and the
+ * host packing Jacobian::assembleTriBlocks (src/Jacobian.cxx:76-117).
+ * algo is one of TBS_ALGO_*.  Resets U to zero and R to rhs. */
+int tbs_factor(tbs_ctx *ctx, int algo);
+
+/* n LIJ sweeps (src/main.cxx:207-229: solveDU -> U += dU -> R = rhs ->
+ * R += J U).  rnorm_out (may be NULL) receives n+1 values: ||R|| before
+ * the first sweep and after each sweep (2-norm over all 9*nelem entries).
+ * TBS_ALGO_MIXED counts one outer refinement step as one sweep. */
+int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out);
+
+/* Sweeps until ||R|| <= rel_tol * ||R_0|| or max_sweeps, with the
+ * convergence test on the device (one CUDA graph launch, no host round
+ * trip per sweep).  *sweeps_out = sweeps done; hist_out (may be NULL)
+ * receives sweeps+1 norms, hist[0] = ||R_0||. */
+int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps,
+              int *sweeps_out, double *hist_out);
+
+/* Jacobian::fromDevice (src/Jacobian.cxx:279-290) for the vectors, in the
+ * element order of the input (9*nelem doubles each). */
+int tbs_get_solution(tbs_ctx *ctx, double *U);
+int tbs_get_residual(tbs_ctx *ctx, double *R);
+int tbs_get_update(tbs_ctx *ctx, double *dU);
+
+/* ||rhs + J U|| recomputed from the original FP64 blocks, whatever the
+ * algorithm (the check behind every reported convergence). */
+int tbs_true_residual_norm(tbs_ctx *ctx, double *out);
+
+/* Device bytes held by the context (replaces
+ * gpu.device.memoryAllocated(), src/main.cxx:97-99). */
+int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes);
+
+/* TBS_ALGO_MIXED: FP32 inner sweeps per FP64 outer refinement step
+ * (default 4, range 1..64). */
+int tbs_set_inner_sweeps(tbs_ctx *ctx, int m);
+
+/* Per-kernel CUDA-event timing.  While enabled, every launch is bracketed
+ * by events on the launching stream; tbs_profile_read returns, for kernel
+ * slot k < *n, its name, launch count and total milliseconds. */
+#define TBS_PROFILE_MAX 16
+int tbs_profile_enable(tbs_ctx *ctx, int on);
+int tbs_profile_reset(tbs_ctx *ctx);
+int tbs_profile_read(tbs_ctx *ctx, int *n, const char **names,
+                     long long *launches, double *ms);
+
+/* Algorithmic bytes one launch of each kernel moves (reads + writes of
+ * every array it must touch once), for the roofline numerator. */
+int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
+
+/* Library version string. */
+const char *tbs_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TRIBLOCK_H */

@@ -1,0 +1,160 @@
+"""CPU oracle of the reference LIJ path -- TEST INFRASTRUCTURE ONLY.
+
+ctypes wrapper of ``oracle/_build/liboracle.so`` (built from lij_oracle.c by
+oracle/Makefile).  Only the tests, ``__graft_entry__.smoke()`` and the CPU
+baseline / reference arm of ``bench.py`` use it, and only as the checker or
+as the timed CPU baseline; the product (libtriblock.so) never does.
+
+Parity status: the arithmetic restatement is unpinned by reference outputs
+(the reference needs OCCA, MPI and gfortran to build and ships no golden
+vectors); the mesh format is pinned by the ex05 fixture in tests/golden.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "_build", "liboracle.so")
+
+
+def _load():
+    if not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-C", HERE], check=True, capture_output=True)
+    return C.CDLL(LIB_PATH)
+
+
+lib = _load()
+_i, _ip, _dp = C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_double)
+lib.oracle_set_threads.argtypes = [_i]
+lib.oracle_max_threads.restype = _i
+lib.oracle_lij.restype = _i
+lib.oracle_lij.argtypes = [_i, _i, _i, _i] + [_ip] * 7 + [_dp] * 4 + [_i] + [_dp] * 6
+lib.oracle_norm.restype = C.c_double
+lib.oracle_norm.argtypes = [_dp, C.c_size_t]
+lib.oracle_resize_block_size.argtypes = [_i, _i, _i, _i] + [_dp] * 10
+lib.oracle_line_res.argtypes = [_i, _i] + [_ip] * 6 + [_dp] * 5
+lib.oracle_solve_du.argtypes = [_i, _i] + [_ip] * 3 + [_dp] * 5
+lib.oracle_line_lu.argtypes = [_i, _i] + [_ip] * 5 + [_dp] * 4
+lib.oracle_assemble_A.argtypes = [_i, _i] + [_ip] * 5 + [_dp] * 3
+lib.oracle_factor.restype = _i
+lib.oracle_factor.argtypes = [_i, _i, _i] + [_ip] * 5 + [_dp] * 6
+lib.oracle_sweeps.restype = _i
+lib.oracle_sweeps.argtypes = [_i, _i, _i] + [_ip] * 6 + [_dp] * 10 + [_i, _dp]
+
+
+def _ip_(a):
+    a = np.ascontiguousarray(a, np.int32)
+    return a, a.ctypes.data_as(_ip)
+
+
+def _dp_(a):
+    assert a.dtype == np.float64 and a.flags.c_contiguous
+    return a.ctypes.data_as(_dp)
+
+
+def set_threads(n: int) -> None:
+    lib.oracle_set_threads(int(n))
+
+
+def max_threads() -> int:
+    return int(lib.oracle_max_threads())
+
+
+def lij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1, want_factors=False):
+    """The reference flow (src/main.cxx:180-229) for `iters` sweeps from U = 0.
+
+    `mesh` has the reference's 0-based arrays (epoint, ef, fc, linesize,
+    linepoint, lines, lineface) and nvar / nelem / nintface / nline.
+    Returns dict(U, R, dU, hist[, DLU, DinvC]).
+    """
+    set_threads(threads)
+    nv, ne = int(mesh.nvar), int(mesh.nelem)
+    keep = []
+    ptrs = []
+    for f in ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface"):
+        a, p = _ip_(getattr(mesh, f))
+        keep.append(a)
+        ptrs.append(p)
+    U = np.zeros(nv * ne)
+    R = np.zeros(nv * ne)
+    dU = np.zeros(nv * ne)
+    hist = np.zeros(iters + 1)
+    DLU = np.zeros(nv * nv * ne) if want_factors else None
+    DinvC = np.zeros(nv * nv * ne) if want_factors else None
+    rc = lib.oracle_lij(nv, ne, int(mesh.nintface), int(mesh.nline), *ptrs,
+                        _dp_(jacD), _dp_(jacO1), _dp_(jacO2), _dp_(rhs), int(iters),
+                        _dp_(U), _dp_(R), _dp_(dU), _dp_(hist),
+                        _dp_(DLU) if want_factors else None,
+                        _dp_(DinvC) if want_factors else None)
+    if rc != 0:
+        raise RuntimeError(f"oracle_lij failed ({rc})")
+    out = dict(U=U, R=R, dU=dU, hist=hist)
+    if want_factors:
+        out.update(DLU=DLU, DinvC=DinvC)
+    return out
+
+
+def resize_block_size(nv_old, nv_new, nelem, nintface, D, O1, O2, rhs, U0):
+    """Jacobian.cxx:153-238 restated; returns the new (D, O1, O2, rhs, U0)."""
+    bn = nv_new * nv_new
+    out = [np.zeros(bn * nelem), np.zeros(bn * nintface), np.zeros(bn * nintface),
+           np.zeros(nv_new * nelem), np.zeros(nv_new * nelem)]
+    lib.oracle_resize_block_size(nv_old, nv_new, nelem, nintface, _dp_(D), _dp_(O1), _dp_(O2),
+                                 _dp_(rhs), _dp_(U0), *[_dp_(a) for a in out])
+    return out
+
+
+def true_residual(mesh, jacD, jacO1, jacO2, rhs, U):
+    """rhs + J U with the reference's residual rule (linesmoothLU_TriBlock_v3.okl:228-336)."""
+    nv, ne = int(mesh.nvar), int(mesh.nelem)
+    R = np.ascontiguousarray(rhs, np.float64).copy()
+    keep, ptrs = [], []
+    for f in ("epoint", "ef", "fc", "linesize", "linepoint", "lines"):
+        a, p = _ip_(getattr(mesh, f))
+        keep.append(a)
+        ptrs.append(p)
+    U = np.ascontiguousarray(U, np.float64)
+    lib.oracle_line_res(nv, int(mesh.nline), *ptrs, _dp_(jacD), _dp_(jacO1), _dp_(jacO2),
+                        _dp_(U), _dp_(R))
+    return R
+
+
+class Baseline:
+    """Factor once, then time sweeps: the CPU baseline of bench.py.
+
+    Runs the restated reference path (oracle_factor + oracle_sweeps) with
+    `threads` OpenMP threads over lines, the work split of the reference's
+    OpenMP mode (compute_mode 4)."""
+
+    def __init__(self, mesh, jacD, jacO1, jacO2, rhs, threads: int):
+        set_threads(threads)
+        self.nv, self.ne, self.nline = int(mesh.nvar), int(mesh.nelem), int(mesh.nline)
+        self._ints = {f: np.ascontiguousarray(getattr(mesh, f), np.int32) for f in
+                      ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface")}
+        self.jacD, self.jacO1, self.jacO2, self.rhs = jacD, jacO1, jacO2, rhs
+        nb = self.nv * self.nv * self.ne
+        self.DLU, self.DinvC, self.A = np.zeros(nb), np.zeros(nb), np.zeros(nb)
+        ip = lambda f: self._ints[f].ctypes.data_as(_ip)
+        lib.oracle_factor(self.nv, self.ne, self.nline, ip("fc"), ip("linesize"), ip("linepoint"),
+                          ip("lines"), ip("lineface"), _dp_(jacD), _dp_(jacO1), _dp_(jacO2),
+                          _dp_(self.DLU), _dp_(self.DinvC), _dp_(self.A))
+        self.reset()
+
+    def reset(self):
+        self.U = np.zeros(self.nv * self.ne)
+        self.dU = np.zeros(self.nv * self.ne)
+        self.R = np.array(self.rhs, np.float64, copy=True)
+
+    def sweeps(self, n: int) -> np.ndarray:
+        ip = lambda f: self._ints[f].ctypes.data_as(_ip)
+        hist = np.zeros(max(n, 1))
+        lib.oracle_sweeps(self.nv, self.ne, self.nline, ip("epoint"), ip("ef"), ip("fc"),
+                          ip("linesize"), ip("linepoint"), ip("lines"), _dp_(self.jacD),
+                          _dp_(self.jacO1), _dp_(self.jacO2), _dp_(self.rhs), _dp_(self.DLU),
+                          _dp_(self.DinvC), _dp_(self.A), _dp_(self.U), _dp_(self.R),
+                          _dp_(self.dU), int(n), _dp_(hist))
+        return hist[:n]

@@ -1,0 +1,69 @@
+"""Error paths on the device: statuses, never traps; the context stays usable."""
+import numpy as np
+import pytest
+
+from triblocksolve_b200 import (ALGO_FP64, ALGO_MIXED, ALGO_REFERENCE, Jacobian, Mesh, Platform,
+                                Solver, TbsError)
+from triblocksolve_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+
+def test_calls_out_of_order():
+    s = Solver(0)
+    with pytest.raises(TbsError) as e:
+        s.factor(ALGO_FP64)
+    assert e.value.code == N.TBS_ERR_STATE
+    mesh = Mesh.structured(4, 4)
+    s.set_mesh(mesh)
+    with pytest.raises(TbsError) as e:
+        s.sweep(1)
+    assert e.value.code == N.TBS_ERR_STATE
+    s.close()
+
+
+@pytest.mark.parametrize("algo", [ALGO_REFERENCE, ALGO_FP64, ALGO_MIXED])
+def test_zero_pivot_reports_numeric_error(algo):
+    s = Solver(0)
+    mesh = Mesh.structured(4, 6)
+    jac = Jacobian.generate(mesh, 9.0, 1)
+    bad = jac.jacD.copy()
+    bad[81 * 5: 81 * 6] = 0.0  # a zero diagonal block
+    s.set_mesh(mesh)
+    s.set_jacobian_arrays(bad, jac.jacO1, jac.jacO2, jac.rhs)
+    with pytest.raises(TbsError) as e:
+        s.factor(algo)
+    assert e.value.code == N.TBS_ERR_NUMERIC
+    # the context is still usable
+    s.set_jacobian(jac)
+    s.factor(algo)
+    h = s.sweep(3)
+    assert np.all(np.isfinite(h)) and h[-1] < h[0]
+    s.close()
+
+
+def test_other_compute_modes_rejected():
+    for mode in (0, 1, 3, 4, 5, 6):
+        with pytest.raises(TbsError) as e:
+            Platform(mode, 0)
+        assert e.value.code == N.TBS_ERR_UNSUPPORTED
+
+
+def test_bad_device_id():
+    with pytest.raises(TbsError) as e:
+        Platform(2, 4096)
+    assert e.value.code == N.TBS_ERR_ARG
+
+
+def test_fast_algos_need_nvar9():
+    s = Solver(0)
+    from meshes import ragged_mesh
+    mesh = ragged_mesh([3, 4], seed=1, nvar=5)
+    jac = Jacobian.generate(mesh, 5.0, 1)
+    s.set_mesh(mesh)
+    s.set_jacobian(jac)
+    with pytest.raises(TbsError) as e:
+        s.factor(ALGO_FP64)
+    assert e.value.code == N.TBS_ERR_UNSUPPORTED
+    s.factor(ALGO_REFERENCE)
+    s.close()

@@ -1,0 +1,1177 @@
+/*
+ * api.cu -- the tbs_* solver entry points: device context, memory, the
+ * line-ordered layout, and the launch sequences of the three algorithms.
+ *
+ * Reference flow replaced (src/main.cxx):
+ *   Platform gpu(...)              :80    -> tbs_create
+ *   mesh.setupDevice/toDevice      :84-85 -> tbs_set_mesh
+ *   Jac.setupDevice/toDevice       :92-93 -> tbs_set_jacobian
+ *   copyAtoBjac + lineLU_v2        :180-190 -> tbs_factor
+ *   copyAtoB; loop{solveDU; addAtoB; copyAtoB; lineRes} :201-229
+ *                                  -> tbs_sweep / tbs_solve
+ * tbs_solve runs the sweep loop as one CUDA graph whose while-node is
+ * driven by a device-side convergence test, so a solve costs one launch.
+ */
+#include "tbs_internal.hxx"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace tbs;
+
+namespace {
+
+struct ProfSlot {
+    const char *name;
+    long long launches;
+    double ms;
+};
+
+struct PendingEvent {
+    int slot;
+    cudaEvent_t a, b;
+};
+
+}  // namespace
+
+struct tbs_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    /* ---- mesh ---- */
+    bool have_mesh = false, have_jac = false, factored = false;
+    int nvar = 0, nelem = 0, nintface = 0, eftot = 0, nline = 0, nlineelem = 0, max_line = 0;
+    std::vector<int> h_epoint, h_ef, h_fc, h_linesize, h_linepoint, h_lines, h_lineface;
+    int *d_epoint = nullptr, *d_ef = nullptr, *d_fc = nullptr, *d_linesize = nullptr;
+    int *d_linepoint = nullptr, *d_lines = nullptr, *d_lineface = nullptr, *d_identity = nullptr;
+
+    /* ---- Jacobian (element / face order, as read) ---- */
+    double *d_jacD = nullptr, *d_O1 = nullptr, *d_O2 = nullptr, *d_rhs = nullptr;
+    double *d_U = nullptr, *d_dU = nullptr, *d_R = nullptr, *d_Uinit = nullptr;
+    double *d_scratch = nullptr; /* 9*nelem element-order scratch */
+
+    /* ---- TBS_ALGO_REFERENCE ---- */
+    double *d_DLU = nullptr, *d_DinvC = nullptr, *d_A = nullptr;
+
+    /* ---- line-ordered layout (FP64 / MIXED) ---- */
+    FastLayout L{};
+    bool layout_ok = false;
+    long long n_xslots_real = 0;
+    double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
+    double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
+    double *d_rhsp = nullptr, *d_Rp = nullptr;
+    float *d_Dinv32 = nullptr, *d_G32 = nullptr, *d_Gam32 = nullptr, *d_X32 = nullptr;
+    float *d_b32 = nullptr, *d_y32 = nullptr, *d_d32 = nullptr, *d_c32 = nullptr,
+          *d_R32 = nullptr;
+    int inner_sweeps = 4;
+
+    /* ---- norms / solve state ---- */
+    double *d_partials = nullptr, *d_partials2 = nullptr;
+    int npart_cap = 0;
+    int npart_cur = 0; /* partials produced by the residual of the current state */
+    SolveState *d_state = nullptr;
+    SolveState *h_state = nullptr; /* pinned */
+    double *d_hist = nullptr;
+    int hist_cap = 0;
+    unsigned *d_status = nullptr;
+    unsigned *h_status = nullptr; /* pinned */
+    int algo = -1;
+
+    /* ---- graph cache ---- */
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_algo = -1;
+
+    /* ---- memory accounting ---- */
+    std::vector<std::pair<void *, size_t>> allocs;
+    size_t bytes = 0;
+
+    /* ---- profiling ---- */
+    bool prof = false;
+    std::vector<ProfSlot> slots;
+    std::vector<PendingEvent> pending;
+    std::vector<cudaEvent_t> pool;
+};
+
+/* ================================================================ errors */
+
+static int ctx_fail(tbs_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->err = msg;
+    set_thread_error(msg);
+    return code;
+}
+
+#define CK(call)                                                                          \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return ctx_fail(ctx, TBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define CKL(call)                                                                         \
+    do {                                                                                  \
+        int e_ = (call);                                                                  \
+        if (e_ != 0)                                                                      \
+            return ctx_fail(ctx, TBS_ERR_CUDA,                                            \
+                            std::string(#call) + ": " + cudaGetErrorString((cudaError_t)e_)); \
+    } while (0)
+
+#define GUARD_BEGIN try {
+#define GUARD_END                                                                        \
+    }                                                                                     \
+    catch (const std::bad_alloc &) {                                                      \
+        return ctx_fail(ctx, TBS_ERR_NOMEM, "host allocation failed");                    \
+    }                                                                                     \
+    catch (const std::exception &ex) {                                                    \
+        return ctx_fail(ctx, TBS_ERR_STATE, std::string("internal error: ") + ex.what()); \
+    }                                                                                     \
+    catch (...) {                                                                         \
+        return ctx_fail(ctx, TBS_ERR_STATE, "internal error");                            \
+    }
+
+/* ================================================================ memory */
+
+template <typename T>
+static int dalloc(tbs_ctx *ctx, T **p, size_t count) {
+    if (*p) return TBS_OK;
+    size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
+    void *q = nullptr;
+    cudaError_t e = cudaMalloc(&q, nbytes);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return ctx_fail(ctx, TBS_ERR_NOMEM,
+                        "cudaMalloc of " + std::to_string(nbytes) + " bytes failed: " +
+                            cudaGetErrorString(e));
+    }
+    e = cudaMemsetAsync(q, 0, nbytes, ctx->stream);
+    if (e != cudaSuccess) {
+        cudaFree(q);
+        return ctx_fail(ctx, TBS_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    }
+    ctx->allocs.push_back({q, nbytes});
+    ctx->bytes += nbytes;
+    *p = static_cast<T *>(q);
+    return TBS_OK;
+}
+
+template <typename T>
+static void dfree(tbs_ctx *ctx, T **p) {
+    if (!*p) return;
+    for (size_t i = 0; i < ctx->allocs.size(); ++i) {
+        if (ctx->allocs[i].first == (void *)*p) {
+            ctx->bytes -= ctx->allocs[i].second;
+            ctx->allocs.erase(ctx->allocs.begin() + i);
+            break;
+        }
+    }
+    cudaFree(*p);
+    *p = nullptr;
+}
+
+#define DA(ptr, n)                          \
+    do {                                    \
+        int s_ = dalloc(ctx, &(ptr), (n));  \
+        if (s_) return s_;                  \
+    } while (0)
+
+static void drop_graph(tbs_ctx *ctx) {
+    if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
+    if (ctx->graph) cudaGraphDestroy(ctx->graph);
+    ctx->gexec = nullptr;
+    ctx->graph = nullptr;
+    ctx->graph_algo = -1;
+}
+
+/* free everything that depends on the mesh */
+static void drop_mesh(tbs_ctx *ctx) {
+    drop_graph(ctx);
+    for (auto &a : ctx->allocs) cudaFree(a.first);
+    ctx->allocs.clear();
+    ctx->bytes = 0;
+    double **dps[] = {&ctx->d_jacD, &ctx->d_O1, &ctx->d_O2, &ctx->d_rhs, &ctx->d_U, &ctx->d_dU,
+                      &ctx->d_R, &ctx->d_Uinit, &ctx->d_scratch, &ctx->d_DLU, &ctx->d_DinvC,
+                      &ctx->d_A, &ctx->d_Dinv, &ctx->d_G, &ctx->d_Gam, &ctx->d_X, &ctx->d_Up,
+                      &ctx->d_dUp, &ctx->d_b, &ctx->d_y, &ctx->d_rhsp, &ctx->d_Rp,
+                      &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist};
+    for (auto p : dps) *p = nullptr;
+    float **fps[] = {&ctx->d_Dinv32, &ctx->d_G32, &ctx->d_Gam32, &ctx->d_X32, &ctx->d_b32,
+                     &ctx->d_y32, &ctx->d_d32, &ctx->d_c32, &ctx->d_R32};
+    for (auto p : fps) *p = nullptr;
+    int **ips[] = {&ctx->d_epoint, &ctx->d_ef, &ctx->d_fc, &ctx->d_linesize, &ctx->d_linepoint,
+                   &ctx->d_lines, &ctx->d_lineface, &ctx->d_identity, &ctx->L.line_start,
+                   &ctx->L.line_len, &ctx->L.pos_of_elem, &ctx->L.elem_of_pos, &ctx->L.xnbr,
+                   &ctx->L.xsrc, &ctx->L.fsrc};
+    for (auto p : ips) *p = nullptr;
+    ctx->d_state = nullptr;
+    ctx->d_status = nullptr;
+    ctx->npart_cap = 0;
+    ctx->hist_cap = 0;
+    ctx->have_mesh = ctx->have_jac = ctx->factored = false;
+    ctx->layout_ok = false;
+    ctx->algo = -1;
+}
+
+/* ============================================================= profiling */
+
+static int prof_slot(tbs_ctx *ctx, const char *name) {
+    for (size_t i = 0; i < ctx->slots.size(); ++i)
+        if (std::strcmp(ctx->slots[i].name, name) == 0) return (int)i;
+    if (ctx->slots.size() >= TBS_PROFILE_MAX) return -1;
+    ctx->slots.push_back({name, 0, 0.0});
+    return (int)ctx->slots.size() - 1;
+}
+
+static cudaEvent_t prof_event(tbs_ctx *ctx) {
+    if (!ctx->pool.empty()) {
+        cudaEvent_t e = ctx->pool.back();
+        ctx->pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+static void prof_resolve(tbs_ctx *ctx) {
+    if (ctx->pending.empty()) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &p : ctx->pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && p.slot >= 0) {
+            ctx->slots[p.slot].ms += ms;
+            ctx->slots[p.slot].launches += 1;
+        }
+        ctx->pool.push_back(p.a);
+        ctx->pool.push_back(p.b);
+    }
+    ctx->pending.clear();
+}
+
+static bool capturing(tbs_ctx *ctx) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(ctx->stream, &cs);
+    return cs != cudaStreamCaptureStatusNone;
+}
+
+/* run one launch, bracketed by events when profiling */
+template <typename F>
+static int timed(tbs_ctx *ctx, const char *name, F &&launch) {
+    if (!ctx->prof || capturing(ctx)) return launch();
+    if (ctx->pending.size() > 4000) prof_resolve(ctx);
+    PendingEvent pe{prof_slot(ctx, name), prof_event(ctx), prof_event(ctx)};
+    cudaEventRecord(pe.a, ctx->stream);
+    int rc = launch();
+    cudaEventRecord(pe.b, ctx->stream);
+    ctx->pending.push_back(pe);
+    return rc;
+}
+
+#define RUN(name, call) CKL(timed(ctx, name, [&]() { return (int)(call); }))
+
+/* ============================================================ layout (host) */
+
+static int build_layout(tbs_ctx *ctx) {
+    const int nline = ctx->nline, nelem = ctx->nelem;
+    const int *ls = ctx->h_linesize.data(), *lp = ctx->h_linepoint.data();
+    const int *lines = ctx->h_lines.data(), *lf = ctx->h_lineface.data();
+    const int *fc = ctx->h_fc.data(), *ep = ctx->h_epoint.data(), *ef = ctx->h_ef.data();
+    std::vector<int> start(nline), len(nline);
+    long long np = 0;
+    for (int l = 0; l < nline; ++l) {
+        start[l] = (int)np;
+        len[l] = ls[l];
+        np += (ls[l] + 3) & ~3;
+    }
+    if (np > 0x7fffffffLL / 81)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "mesh too large for int32 block offsets");
+    const int np16 = (int)((np + RES_TILE - 1) / RES_TILE * RES_TILE);
+    std::vector<int> pos_of_elem(nelem), elem_of_pos(np16, -1), fsrc((size_t)np16 * 3, 0);
+    for (int l = 0; l < nline; ++l) {
+        for (int k = 0; k < ls[l]; ++k) {
+            const int m = lp[l] + k, e = lines[m], p = start[l] + k;
+            pos_of_elem[e] = p;
+            elem_of_pos[p] = e;
+            fsrc[3 * (size_t)p] = e;
+            if (k >= 1) {
+                const int f = lf[m];
+                fsrc[3 * (size_t)p + 1] = f;
+                fsrc[3 * (size_t)p + 2] = (e == fc[2 * f]) ? 1 : 0;
+            } else {
+                fsrc[3 * (size_t)p + 1] = -1;
+            }
+        }
+    }
+    /* cross-line slots: every interior face of the cell that is not one of
+     * the (at most two) in-line faces used by the Thomas factorization */
+    std::vector<std::vector<std::pair<int, int>>> xs(np16);
+    int nx = 0;
+    long long nreal = 0;
+    for (int l = 0; l < nline; ++l) {
+        for (int k = 0; k < ls[l]; ++k) {
+            const int m = lp[l] + k, e = lines[m], p = start[l] + k;
+            int fprev = (k >= 1) ? lf[m] : -1;
+            int fnext = (k + 1 < ls[l]) ? lf[m + 1] : -1;
+            auto &v = xs[p];
+            for (int k2 = ep[e]; k2 < ep[e + 1]; ++k2) {
+                const int f = ef[k2];
+                if (f < 0) continue;
+                if (f == fprev) {
+                    fprev = -2;
+                    continue;
+                }
+                if (f == fnext) {
+                    fnext = -2;
+                    continue;
+                }
+                const bool is1 = (e == fc[2 * f]);
+                const int nb = is1 ? fc[2 * f + 1] : fc[2 * f];
+                v.push_back({2 * f + (is1 ? 1 : 0), pos_of_elem[nb]});
+            }
+            nx = std::max<int>(nx, (int)v.size());
+            nreal += (long long)v.size();
+        }
+    }
+    std::vector<int> xsrc((size_t)np16 * std::max(nx, 1), -1), xnbr((size_t)np16 * std::max(nx, 1), -1);
+    for (int p = 0; p < np16; ++p)
+        for (size_t q = 0; q < xs[p].size(); ++q) {
+            xsrc[(size_t)p * nx + q] = xs[p][q].first;
+            xnbr[(size_t)p * nx + q] = xs[p][q].second;
+        }
+    FastLayout &L = ctx->L;
+    L.nv = ctx->nvar;
+    L.np = (int)np;
+    L.np16 = np16;
+    L.nx = nx;
+    L.nline = nline;
+    L.max_len = ctx->max_line;
+    ctx->n_xslots_real = nreal;
+    DA(L.line_start, nline);
+    DA(L.line_len, nline);
+    DA(L.pos_of_elem, nelem);
+    DA(L.elem_of_pos, np16);
+    DA(L.fsrc, (size_t)np16 * 3);
+    DA(L.xsrc, (size_t)np16 * std::max(nx, 1));
+    DA(L.xnbr, (size_t)np16 * std::max(nx, 1));
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(L.line_start, start.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.line_len, len.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.pos_of_elem, pos_of_elem.data(), nelem * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.elem_of_pos, elem_of_pos.data(), np16 * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.fsrc, fsrc.data(), fsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.xsrc, xsrc.data(), xsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.xnbr, xnbr.data(), xnbr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    /* the residual kernel stages RES_TILE cells x nx blocks per pipeline
+     * stage; beyond 4 cross-line couplings per cell it would not fit in
+     * shared memory, and such meshes use TBS_ALGO_REFERENCE */
+    ctx->layout_ok = (ctx->nvar == 9) && nx <= 4;
+    return TBS_OK;
+}
+
+/* ============================================================ sequences */
+
+static int status_check(tbs_ctx *ctx) {
+    CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    const unsigned s = *ctx->h_status;
+    if (s) {
+        CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+        if (s & ST_PIVOT)
+            return ctx_fail(ctx, TBS_ERR_NUMERIC,
+                            "zero or non-finite pivot in the no-pivot block factorization");
+        if (s & ST_TIMEOUT)
+            return ctx_fail(ctx, TBS_ERR_CUDA, "a device-side wait ran out of its time budget");
+        return ctx_fail(ctx, TBS_ERR_CUDA, "device status " + std::to_string(s));
+    }
+    return TBS_OK;
+}
+
+static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; }
+
+/* Bring the state to "U = U_init, residual of U known": the partials of
+ * ||R_0|| are in d_partials and the first sweep's inputs are ready. */
+static int prime(tbs_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int nv = ctx->nvar, ne = ctx->nelem;
+    const size_t vb = (size_t)nvec(ctx) * sizeof(double);
+    if (ctx->algo == TBS_ALGO_REFERENCE) {
+        if (ctx->d_Uinit) {
+            CK(cudaMemcpyAsync(ctx->d_U, ctx->d_Uinit, vb, cudaMemcpyDeviceToDevice, st));
+            CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
+            int np = 0;
+            RUN("ref_line_res", launch_ref_line_res(st, nv, ctx->nline, ne, ctx->d_epoint, ctx->d_ef,
+                                                    ctx->d_fc, ctx->d_linesize, ctx->d_linepoint,
+                                                    ctx->d_lines, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                    ctx->d_U, ctx->d_R, ctx->d_partials, &np));
+            ctx->npart_cur = np;
+        } else {
+            CK(cudaMemsetAsync(ctx->d_U, 0, vb, st));
+            CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
+            const int np = ref_line_res_partials(ne);
+            RUN("norm_partials", launch_norm_partials(st, ctx->d_R, nvec(ctx), ctx->d_partials, np));
+            ctx->npart_cur = np;
+        }
+        CK(cudaMemsetAsync(ctx->d_dU, 0, vb, st));
+        return TBS_OK;
+    }
+    const FastLayout &L = ctx->L;
+    const size_t pb = (size_t)L.np16 * 9 * sizeof(double);
+    const int np = fast_resid_grid(L.np16);
+    if (ctx->algo == TBS_ALGO_FP64) {
+        if (ctx->d_Uinit) {
+            RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
+            RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                        L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
+                                                        ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
+                                                        ctx->d_partials2));
+            RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
+                                                        ctx->d_Rp, ctx->d_b, ctx->d_partials, np,
+                                                        ctx->d_status));
+        } else {
+            CK(cudaMemsetAsync(ctx->d_Up, 0, pb, st));
+            RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
+                                                        ctx->d_rhsp, ctx->d_b, ctx->d_partials, np,
+                                                        ctx->d_status));
+        }
+        ctx->npart_cur = np;
+        return TBS_OK;
+    }
+    /* TBS_ALGO_MIXED */
+    const int nfb = full_resid_blocks(ne);
+    if (ctx->d_Uinit) {
+        RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
+        RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                   L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                   ctx->d_rhs, ctx->d_Up, ctx->d_R32,
+                                                   ctx->d_partials));
+        ctx->npart_cur = nfb;
+    } else {
+        CK(cudaMemsetAsync(ctx->d_Up, 0, pb, st));
+        RUN("cast", launch_cast_f64_f32(st, ctx->d_rhsp, ctx->d_R32, (long long)L.np16 * 9));
+        const int npn = ref_line_res_partials(ne);
+        RUN("norm_partials", launch_norm_partials(st, ctx->d_rhsp, (long long)L.np16 * 9,
+                                                  ctx->d_partials, npn));
+        ctx->npart_cur = npn;
+    }
+    return TBS_OK;
+}
+
+/* one sweep from the primed state; leaves the new residual's partials in
+ * d_partials (npart_cur entries) */
+static int body(tbs_ctx *ctx) {
+    cudaStream_t st = ctx->stream;
+    const int nv = ctx->nvar, ne = ctx->nelem;
+    if (ctx->algo == TBS_ALGO_REFERENCE) {
+        RUN("ref_solve_du", launch_ref_solve_du(st, nv, ctx->nline, ctx->d_linesize, ctx->d_linepoint,
+                                                ctx->d_lines, ctx->d_DLU, ctx->d_DinvC, ctx->d_A,
+                                                ctx->d_dU, ctx->d_R));
+        RUN("ref_add_copy", launch_ref_add_copy(st, nvec(ctx), ctx->d_dU, ctx->d_U, ctx->d_rhs, ctx->d_R));
+        int np = 0;
+        RUN("ref_line_res", launch_ref_line_res(st, nv, ctx->nline, ne, ctx->d_epoint, ctx->d_ef,
+                                                ctx->d_fc, ctx->d_linesize, ctx->d_linepoint,
+                                                ctx->d_lines, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                ctx->d_U, ctx->d_R, ctx->d_partials, &np));
+        ctx->npart_cur = np;
+        return TBS_OK;
+    }
+    const FastLayout &L = ctx->L;
+    const int np = fast_resid_grid(L.np16);
+    if (ctx->algo == TBS_ALGO_FP64) {
+        RUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
+                                                      ctx->d_dUp, ctx->d_Up, ctx->d_status, 1));
+        RUN("fast_resid", launch_fast_resid<double>(st, L, 1, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
+                                                    ctx->d_Rp, ctx->d_b, ctx->d_partials, np,
+                                                    ctx->d_status));
+        ctx->npart_cur = np;
+        return TBS_OK;
+    }
+    /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
+     * FP64 residual R = rhs + J U from the original blocks */
+    RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
+                                                 ctx->d_R32, ctx->d_b32, ctx->d_partials2, np,
+                                                 ctx->d_status));
+    for (int m = 0; m < ctx->inner_sweeps; ++m) {
+        RUN("fast_thomas32", launch_fast_thomas<float>(st, L, ctx->d_G32, ctx->d_Gam32, ctx->d_b32,
+                                                       ctx->d_y32, ctx->d_d32, ctx->d_c32,
+                                                       ctx->d_status, m > 0 ? 1 : 0));
+        if (m + 1 < ctx->inner_sweeps)
+            RUN("fast_resid32", launch_fast_resid<float>(st, L, 1, ctx->d_Dinv32, ctx->d_X32,
+                                                         ctx->d_d32, ctx->d_R32, ctx->d_b32,
+                                                         ctx->d_partials2, np, ctx->d_status));
+    }
+    RUN("axpy", launch_axpy_f32_f64(st, ctx->d_c32, ctx->d_Up, (long long)L.np16 * 9));
+    RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                               L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                               ctx->d_rhs, ctx->d_Up, ctx->d_R32, ctx->d_partials));
+    ctx->npart_cur = full_resid_blocks(ne);
+    return TBS_OK;
+}
+
+static int ensure_hist(tbs_ctx *ctx, int need) {
+    if (need <= ctx->hist_cap) return TBS_OK;
+    drop_graph(ctx);
+    dfree(ctx, &ctx->d_hist);
+    int cap = std::max(need, 1024);
+    DA(ctx->d_hist, (size_t)cap);
+    ctx->hist_cap = cap;
+    return TBS_OK;
+}
+
+static int set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
+    std::memset(ctx->h_state, 0, sizeof(SolveState));
+    ctx->h_state->tol = tol;
+    ctx->h_state->max_sweeps = max_sweeps;
+    ctx->h_state->hist_cap = ctx->hist_cap;
+    CK(cudaMemcpyAsync(ctx->d_state, ctx->h_state, sizeof(SolveState), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    return TBS_OK;
+}
+
+static int read_state(tbs_ctx *ctx) {
+    CK(cudaMemcpyAsync(ctx->h_state, ctx->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost,
+                       ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return TBS_OK;
+}
+
+/* Graph: prime -> reduce(start) -> while (cond) { sweep -> reduce }. */
+static int build_graph(tbs_ctx *ctx) {
+    drop_graph(ctx);
+    cudaStream_t st = ctx->stream;
+    cudaGraph_t g = nullptr;
+    CK(cudaGraphCreate(&g, 0));
+    ctx->graph = g;
+    cudaGraphConditionalHandle h;
+    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = prime(ctx);
+    if (rc == TBS_OK)
+        rc = launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state, ctx->d_hist, 1,
+                                (unsigned long long)h, 1)
+                 ? ctx_fail(ctx, TBS_ERR_CUDA, "reduce launch failed")
+                 : TBS_OK;
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if (rc == TBS_OK) {
+        cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(e));
+    }
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraph_t bodyg = nullptr;
+    if (rc == TBS_OK) {
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaError_t e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(e));
+        else bodyg = cp.conditional.phGraph_out[0];
+    }
+    if (rc == TBS_OK) {
+        cudaError_t e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(e));
+    }
+    cudaGraph_t outg = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(st, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
+    if (rc != TBS_OK) {
+        drop_graph(ctx);
+        return rc;
+    }
+    CK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    rc = body(ctx);
+    if (rc == TBS_OK)
+        rc = launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state, ctx->d_hist, 0,
+                                (unsigned long long)h, 1)
+                 ? ctx_fail(ctx, TBS_ERR_CUDA, "reduce launch failed")
+                 : TBS_OK;
+    ee = cudaStreamEndCapture(st, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    if (rc != TBS_OK) {
+        drop_graph(ctx);
+        return rc;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&ctx->gexec, g, 0);
+    if (ie != cudaSuccess) {
+        drop_graph(ctx);
+        return ctx_fail(ctx, TBS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    ctx->graph_algo = ctx->algo;
+    return TBS_OK;
+}
+
+/* =========================================================== algorithms */
+
+static int alloc_algo(tbs_ctx *ctx, int algo) {
+    const size_t bs = 81, ne = ctx->nelem;
+    DA(ctx->d_U, (size_t)nvec(ctx));
+    DA(ctx->d_dU, (size_t)nvec(ctx));
+    DA(ctx->d_R, (size_t)nvec(ctx));
+    DA(ctx->d_scratch, (size_t)nvec(ctx));
+    const int npmax = std::max({ref_line_res_partials(ctx->nelem) * 8, fast_resid_grid(ctx->L.np16),
+                                full_resid_blocks(ctx->nelem), 1024});
+    if (ctx->npart_cap < npmax) {
+        dfree(ctx, &ctx->d_partials);
+        dfree(ctx, &ctx->d_partials2);
+        DA(ctx->d_partials, (size_t)npmax);
+        DA(ctx->d_partials2, (size_t)npmax);
+        ctx->npart_cap = npmax;
+    }
+    if (algo == TBS_ALGO_REFERENCE) {
+        const size_t nb = (size_t)ctx->nvar * ctx->nvar * ne;
+        DA(ctx->d_DLU, nb);
+        DA(ctx->d_DinvC, nb);
+        DA(ctx->d_A, nb);
+        return TBS_OK;
+    }
+    const FastLayout &L = ctx->L;
+    const size_t npb = (size_t)L.np16 * bs, npv = (size_t)L.np16 * 9;
+    const size_t nxb = (size_t)L.np16 * std::max(L.nx, 1) * bs;
+    DA(ctx->d_Up, npv);
+    DA(ctx->d_rhsp, npv);
+    DA(ctx->d_Rp, npv);
+    if (algo == TBS_ALGO_FP64) {
+        DA(ctx->d_Dinv, npb);
+        DA(ctx->d_G, npb);
+        DA(ctx->d_Gam, npb);
+        DA(ctx->d_X, nxb);
+        DA(ctx->d_dUp, npv);
+        DA(ctx->d_b, npv);
+        DA(ctx->d_y, npv);
+    } else {
+        DA(ctx->d_Dinv32, npb);
+        DA(ctx->d_G32, npb);
+        DA(ctx->d_Gam32, npb);
+        DA(ctx->d_X32, nxb);
+        DA(ctx->d_b32, npv);
+        DA(ctx->d_y32, npv);
+        DA(ctx->d_d32, npv);
+        DA(ctx->d_c32, npv);
+        DA(ctx->d_R32, npv);
+    }
+    return TBS_OK;
+}
+
+static int run_factor(tbs_ctx *ctx, int algo) {
+    cudaStream_t st = ctx->stream;
+    const int nv = ctx->nvar;
+    if (algo == TBS_ALGO_REFERENCE) {
+        const size_t nb = (size_t)nv * nv * ctx->nelem;
+        CK(cudaMemcpyAsync(ctx->d_DLU, ctx->d_jacD, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CK(cudaMemsetAsync(ctx->d_DinvC, 0, nb * sizeof(double), st));
+        CK(cudaMemsetAsync(ctx->d_A, 0, nb * sizeof(double), st));
+        RUN("ref_assemble_A", launch_ref_assemble_A(st, nv, ctx->nline, ctx->d_fc, ctx->d_linesize,
+                                                    ctx->d_linepoint, ctx->d_lines, ctx->d_lineface,
+                                                    ctx->d_O1, ctx->d_O2, ctx->d_A));
+        RUN("ref_line_lu", launch_ref_line_lu(st, nv, ctx->nline, ctx->d_fc, ctx->d_linesize,
+                                              ctx->d_linepoint, ctx->d_lines, ctx->d_lineface,
+                                              ctx->d_DLU, ctx->d_O1, ctx->d_O2, ctx->d_DinvC,
+                                              ctx->d_status));
+        return TBS_OK;
+    }
+    const FastLayout &L = ctx->L;
+    RUN("permute", launch_permute_to_pos(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_rhs, ctx->d_rhsp));
+    if (algo == TBS_ALGO_FP64) {
+        RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,
+                                              ctx->d_G, ctx->d_Gam, nullptr, nullptr, nullptr,
+                                              ctx->d_status));
+        RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, ctx->d_X, nullptr));
+    } else {
+        RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, nullptr,
+                                              nullptr, nullptr, ctx->d_Dinv32, ctx->d_G32,
+                                              ctx->d_Gam32, ctx->d_status));
+        RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, nullptr, ctx->d_X32));
+    }
+    return TBS_OK;
+}
+
+/* ============================================================ C entry points */
+
+extern "C" {
+
+const char *tbs_last_error(const tbs_ctx *ctx) {
+    if (ctx) return ctx->err.c_str();
+    return thread_error();
+}
+
+int tbs_create(int device_id, tbs_ctx **out) {
+    tbs_ctx *ctx = nullptr;
+    if (!out) return ctx_fail(nullptr, TBS_ERR_ARG, "tbs_create: null output pointer");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return ctx_fail(nullptr, TBS_ERR_CUDA,
+                        std::string("no CUDA device available (") + cudaGetErrorString(e) +
+                            "); this library has no CPU path");
+    }
+    if (device_id < 0 || device_id >= ndev)
+        return ctx_fail(nullptr, TBS_ERR_ARG, "device_id " + std::to_string(device_id) +
+                                                  " out of range (" + std::to_string(ndev) + " devices)");
+    ctx = new (std::nothrow) tbs_ctx();
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
+    ctx->device = device_id;
+    e = cudaSetDevice(device_id);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_state, sizeof(SolveState));
+    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_status, sizeof(unsigned));
+    if (e == cudaSuccess) e = (cudaError_t)fast_kernels_init();
+    if (e != cudaSuccess) {
+        std::string msg = std::string("device setup failed: ") + cudaGetErrorString(e);
+        if (ctx->own) cudaStreamDestroy(ctx->own);
+        delete ctx;
+        return ctx_fail(nullptr, TBS_ERR_CUDA, msg);
+    }
+    ctx->stream = ctx->own;
+    *out = ctx;
+    return TBS_OK;
+}
+
+int tbs_destroy(tbs_ctx *ctx) {
+    if (!ctx) return TBS_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    drop_mesh(ctx);
+    for (auto &p : ctx->pending) {
+        cudaEventDestroy(p.a);
+        cudaEventDestroy(p.b);
+    }
+    for (auto ev : ctx->pool) cudaEventDestroy(ev);
+    if (ctx->h_state) cudaFreeHost(ctx->h_state);
+    if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->own) cudaStreamDestroy(ctx->own);
+    delete ctx;
+    return TBS_OK;
+}
+
+int tbs_set_stream(tbs_ctx *ctx, void *cuda_stream) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    cudaStream_t ns = cuda_stream ? (cudaStream_t)cuda_stream : ctx->own;
+    if (ns != ctx->stream) {
+        cudaStreamSynchronize(ctx->stream);
+        drop_graph(ctx); /* graphs are launched on, and captured from, the stream */
+        ctx->stream = ns;
+    }
+    return TBS_OK;
+}
+
+int tbs_set_mesh(tbs_ctx *ctx, int nvar, int nelem, int nintface, int eftot, int nline,
+                 int nlineelem, const int *epoint, const int *ef, const int *fc,
+                 const int *linesize, const int *linepoint, const int *lines,
+                 const int *lineface) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int hdr[6] = {nvar, nelem, nintface, eftot, nline, nlineelem};
+    int st = validate_mesh(hdr, epoint, ef, fc, linesize, linepoint, lines, lineface);
+    if (st) return ctx_fail(ctx, st, thread_error());
+    if (nvar > 32) return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "nvar > 32 is not supported");
+    CK(cudaStreamSynchronize(ctx->stream));
+    drop_mesh(ctx);
+    CK(cudaMalloc((void **)&ctx->d_status, sizeof(unsigned)));
+    ctx->allocs.push_back({ctx->d_status, sizeof(unsigned)});
+    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+    DA(ctx->d_state, 1);
+    ctx->nvar = nvar;
+    ctx->nelem = nelem;
+    ctx->nintface = nintface;
+    ctx->eftot = eftot;
+    ctx->nline = nline;
+    ctx->nlineelem = nlineelem;
+    ctx->h_epoint.assign(epoint, epoint + nelem + 1);
+    ctx->h_ef.assign(ef, ef + eftot);
+    ctx->h_fc.assign(fc, fc + 2 * (size_t)nintface);
+    ctx->h_linesize.assign(linesize, linesize + nline);
+    ctx->h_linepoint.assign(linepoint, linepoint + nline + 1);
+    ctx->h_lines.assign(lines, lines + nlineelem);
+    ctx->h_lineface.assign(lineface, lineface + nlineelem);
+    ctx->max_line = 0;
+    for (int l = 0; l < nline; ++l) ctx->max_line = std::max(ctx->max_line, linesize[l]);
+    DA(ctx->d_epoint, (size_t)nelem + 1);
+    DA(ctx->d_ef, (size_t)eftot);
+    DA(ctx->d_fc, 2 * (size_t)nintface);
+    DA(ctx->d_linesize, (size_t)nline);
+    DA(ctx->d_linepoint, (size_t)nline + 1);
+    DA(ctx->d_lines, (size_t)nlineelem);
+    DA(ctx->d_lineface, (size_t)nlineelem);
+    DA(ctx->d_identity, (size_t)nelem);
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_epoint, epoint, (nelem + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (eftot) CK(cudaMemcpyAsync(ctx->d_ef, ef, eftot * sizeof(int), cudaMemcpyHostToDevice, s));
+    if (nintface) CK(cudaMemcpyAsync(ctx->d_fc, fc, 2 * (size_t)nintface * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_linesize, linesize, nline * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_linepoint, linepoint, (nline + 1) * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_lines, lines, nlineelem * sizeof(int), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(ctx->d_lineface, lineface, nlineelem * sizeof(int), cudaMemcpyHostToDevice, s));
+    {
+        std::vector<int> id(nelem);
+        for (int e = 0; e < nelem; ++e) id[e] = e;
+        CK(cudaMemcpyAsync(ctx->d_identity, id.data(), nelem * sizeof(int), cudaMemcpyHostToDevice, s));
+        CK(cudaStreamSynchronize(s));
+    }
+    int rc = build_layout(ctx);
+    if (rc) return rc;
+    ctx->have_mesh = true;
+    return TBS_OK;
+    GUARD_END
+}
+
+static int upload_jacobian(tbs_ctx *ctx, const double *jacD, const double *O1, const double *O2,
+                           const double *rhs, cudaMemcpyKind kind) {
+    if (!ctx->have_mesh) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
+    if (!jacD || (ctx->nintface > 0 && (!O1 || !O2)) || !rhs)
+        return ctx_fail(ctx, TBS_ERR_ARG, "null Jacobian array");
+    const size_t nb = (size_t)ctx->nvar * ctx->nvar;
+    DA(ctx->d_jacD, nb * ctx->nelem);
+    DA(ctx->d_O1, nb * ctx->nintface);
+    DA(ctx->d_O2, nb * ctx->nintface);
+    DA(ctx->d_rhs, (size_t)nvec(ctx));
+    cudaStream_t s = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_jacD, jacD, nb * ctx->nelem * sizeof(double), kind, s));
+    if (ctx->nintface) {
+        CK(cudaMemcpyAsync(ctx->d_O1, O1, nb * ctx->nintface * sizeof(double), kind, s));
+        CK(cudaMemcpyAsync(ctx->d_O2, O2, nb * ctx->nintface * sizeof(double), kind, s));
+    }
+    CK(cudaMemcpyAsync(ctx->d_rhs, rhs, (size_t)nvec(ctx) * sizeof(double), kind, s));
+    /* same mesh -> same allocations, so an instantiated solve graph stays valid */
+    ctx->have_jac = true;
+    ctx->factored = false;
+    return TBS_OK;
+}
+
+int tbs_set_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1, const double *jacO2,
+                     const double *rhs, const double *U0) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    (void)U0; /* read but unused, as in the reference (U starts at zero) */
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return upload_jacobian(ctx, jacD, jacO1, jacO2, rhs, cudaMemcpyHostToDevice);
+    GUARD_END
+}
+
+int tbs_set_jacobian_device(tbs_ctx *ctx, const double *d_jacD, const double *d_jacO1,
+                            const double *d_jacO2, const double *d_rhs) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return upload_jacobian(ctx, d_jacD, d_jacO1, d_jacO2, d_rhs, cudaMemcpyDeviceToDevice);
+    GUARD_END
+}
+
+int tbs_factor(tbs_ctx *ctx, int algo) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->have_jac) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_jacobian must come first");
+    if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_FP64 && algo != TBS_ALGO_MIXED)
+        return ctx_fail(ctx, TBS_ERR_ARG, "unknown algorithm " + std::to_string(algo));
+    if (algo != TBS_ALGO_REFERENCE && !ctx->layout_ok)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
+                        "TBS_ALGO_FP64 / TBS_ALGO_MIXED need nvar == 9 and at most 4 cross-line "
+                        "faces per cell; use TBS_ALGO_REFERENCE");
+    int rc = alloc_algo(ctx, algo);
+    if (rc) return rc;
+    if (ctx->algo != algo) drop_graph(ctx);
+    ctx->algo = algo;
+    ctx->factored = false;
+    rc = run_factor(ctx, algo);
+    if (rc) return rc;
+    rc = prime(ctx);
+    if (rc) return rc;
+    rc = status_check(ctx);
+    if (rc) return rc;
+    ctx->factored = true;
+    return TBS_OK;
+    GUARD_END
+}
+
+int tbs_set_rhs(tbs_ctx *ctx, const double *rhs) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (!rhs) return ctx_fail(ctx, TBS_ERR_ARG, "null rhs");
+    CK(cudaMemcpyAsync(ctx->d_rhs, rhs, (size_t)nvec(ctx) * sizeof(double), cudaMemcpyHostToDevice,
+                       ctx->stream));
+    if (ctx->algo != TBS_ALGO_REFERENCE) {
+        RUN("permute", launch_permute_to_pos(ctx->stream, 9, ctx->nelem, ctx->L.pos_of_elem, ctx->d_rhs,
+                                             ctx->d_rhsp));
+    }
+    return prime(ctx);
+    GUARD_END
+}
+
+int tbs_set_initial(tbs_ctx *ctx, const double *U) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (U) {
+        DA(ctx->d_Uinit, (size_t)nvec(ctx));
+        CK(cudaMemcpyAsync(ctx->d_Uinit, U, (size_t)nvec(ctx) * sizeof(double),
+                           cudaMemcpyHostToDevice, ctx->stream));
+    } else {
+        dfree(ctx, &ctx->d_Uinit);
+    }
+    drop_graph(ctx);
+    return prime(ctx);
+    GUARD_END
+}
+
+int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (n < 0) return ctx_fail(ctx, TBS_ERR_ARG, "negative sweep count");
+    int rc = ensure_hist(ctx, n + 1);
+    if (rc) return rc;
+    rc = set_state(ctx, 0.0, n);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
+                                          ctx->d_hist, 1, 0ull, 0));
+    for (int s = 0; s < n; ++s) {
+        rc = body(ctx);
+        if (rc) return rc;
+        RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
+                                              ctx->d_hist, 0, 0ull, 0));
+    }
+    if (rnorm_out)
+        CK(cudaMemcpyAsync(rnorm_out, ctx->d_hist, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    if (ctx->prof) prof_resolve(ctx);
+    return status_check(ctx);
+    GUARD_END
+}
+
+int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, double *hist_out) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (max_sweeps < 0 || !(rel_tol >= 0.0)) return ctx_fail(ctx, TBS_ERR_ARG, "bad tolerance or sweep limit");
+    int rc = ensure_hist(ctx, max_sweeps + 1);
+    if (rc) return rc;
+    rc = set_state(ctx, rel_tol, max_sweeps);
+    if (rc) return rc;
+    cudaStream_t st = ctx->stream;
+    if (ctx->prof) {
+        /* eager form with a host-side test, so that every kernel is timed */
+        rc = prime(ctx);
+        if (rc) return rc;
+        RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
+                                              ctx->d_hist, 1, 0ull, 0));
+        for (;;) {
+            rc = read_state(ctx);
+            if (rc) return rc;
+            const SolveState &S = *ctx->h_state;
+            const bool go = std::isfinite(S.last) && S.last > S.tol * S.norm0 && S.sweep < S.max_sweeps;
+            if (!go) break;
+            rc = body(ctx);
+            if (rc) return rc;
+            RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
+                                                  ctx->d_hist, 0, 0ull, 0));
+        }
+        prof_resolve(ctx);
+    } else {
+        if (!ctx->gexec || ctx->graph_algo != ctx->algo) {
+            rc = build_graph(ctx);
+            if (rc) return rc;
+        }
+        CK(cudaGraphLaunch(ctx->gexec, st));
+        rc = read_state(ctx);
+        if (rc) return rc;
+    }
+    const int sw = ctx->h_state->sweep;
+    if (sweeps_out) *sweeps_out = sw;
+    if (hist_out)
+        CK(cudaMemcpyAsync(hist_out, ctx->d_hist, (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double),
+                           cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return status_check(ctx);
+    GUARD_END
+}
+
+static int get_vec(tbs_ctx *ctx, int which, double *out) {
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (!out) return ctx_fail(ctx, TBS_ERR_ARG, "null output");
+    cudaStream_t st = ctx->stream;
+    const size_t vb = (size_t)nvec(ctx) * sizeof(double);
+    const double *src = nullptr;
+    if (ctx->algo == TBS_ALGO_REFERENCE) {
+        src = which == 0 ? ctx->d_U : which == 1 ? ctx->d_R : ctx->d_dU;
+    } else {
+        const FastLayout &L = ctx->L;
+        if (which == 0) {
+            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_Up, ctx->d_scratch));
+        } else if (which == 1) {
+            RUN("full_resid", launch_full_resid<double>(st, ctx->nelem, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                        L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                        ctx->d_rhs, ctx->d_Up, ctx->d_Rp, ctx->d_partials2));
+            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_Rp, ctx->d_scratch));
+        } else if (ctx->algo == TBS_ALGO_FP64) {
+            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_dUp, ctx->d_scratch));
+        } else {
+            RUN("permute", launch_permute_f32_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_c32, ctx->d_scratch));
+        }
+        src = ctx->d_scratch;
+    }
+    CK(cudaMemcpyAsync(out, src, vb, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return TBS_OK;
+}
+
+int tbs_get_solution(tbs_ctx *ctx, double *U) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return get_vec(ctx, 0, U);
+    GUARD_END
+}
+
+int tbs_get_residual(tbs_ctx *ctx, double *R) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return get_vec(ctx, 1, R);
+    GUARD_END
+}
+
+int tbs_get_update(tbs_ctx *ctx, double *dU) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return get_vec(ctx, 2, dU);
+    GUARD_END
+}
+
+int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (!out) return ctx_fail(ctx, TBS_ERR_ARG, "null output");
+    if (ctx->nvar != 9) {
+        /* generic block size: the reference path's R is the true residual */
+        std::vector<double> R((size_t)nvec(ctx));
+        int rc = get_vec(ctx, 1, R.data());
+        if (rc) return rc;
+        double s = 0.0;
+        for (double v : R) s += v * v;
+        *out = std::sqrt(s);
+        return TBS_OK;
+    }
+    cudaStream_t st = ctx->stream;
+    const int nb = full_resid_blocks(ctx->nelem);
+    const bool ref = ctx->algo == TBS_ALGO_REFERENCE;
+    RUN("full_resid", launch_full_resid<double>(st, ctx->nelem, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                ref ? ctx->d_identity : ctx->L.pos_of_elem,
+                                                ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_rhs,
+                                                ref ? ctx->d_U : ctx->d_Up,
+                                                ref ? ctx->d_scratch : ctx->d_Rp, ctx->d_partials2));
+    std::vector<double> part(nb);
+    CK(cudaMemcpyAsync(part.data(), ctx->d_partials2, nb * sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    double s = 0.0;
+    for (double v : part) s += v;
+    *out = std::sqrt(s);
+    return TBS_OK;
+    GUARD_END
+}
+
+int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes) {
+    if (!ctx || !bytes) return ctx_fail(nullptr, TBS_ERR_ARG, "null argument");
+    *bytes = ctx->bytes;
+    return TBS_OK;
+}
+
+int tbs_set_inner_sweeps(tbs_ctx *ctx, int m) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    if (m < 1 || m > 64) return ctx_fail(ctx, TBS_ERR_ARG, "inner sweeps must be in 1..64");
+    if (m != ctx->inner_sweeps) drop_graph(ctx);
+    ctx->inner_sweeps = m;
+    return TBS_OK;
+}
+
+int tbs_profile_enable(tbs_ctx *ctx, int on) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    if (!on) prof_resolve(ctx);
+    ctx->prof = on != 0;
+    return TBS_OK;
+}
+
+int tbs_profile_reset(tbs_ctx *ctx) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    prof_resolve(ctx);
+    ctx->slots.clear();
+    return TBS_OK;
+}
+
+int tbs_profile_read(tbs_ctx *ctx, int *n, const char **names, long long *launches, double *ms) {
+    if (!ctx || !n) return ctx_fail(ctx, TBS_ERR_ARG, "null argument");
+    prof_resolve(ctx);
+    const int cap = *n;
+    const int cnt = (int)ctx->slots.size();
+    for (int i = 0; i < cnt && i < cap; ++i) {
+        if (names) names[i] = ctx->slots[i].name;
+        if (launches) launches[i] = ctx->slots[i].launches;
+        if (ms) ms[i] = ctx->slots[i].ms;
+    }
+    *n = cnt;
+    return TBS_OK;
+}
+
+/* Algorithmic bytes of one launch: every array the kernel must read or
+ * write, counted once per read and once per write (block = 648 B, vector
+ * entry = 72 B per cell in FP64; halves in FP32). */
+int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
+    if (!ctx || !kernel || !bytes) return ctx_fail(ctx, TBS_ERR_ARG, "null argument");
+    if (!ctx->have_mesh) return ctx_fail(ctx, TBS_ERR_STATE, "no mesh");
+    const double N = ctx->nelem, F = ctx->nintface, nv = ctx->nvar;
+    const double blk = nv * nv * 8.0, vec = nv * 8.0;
+    const double X = (double)ctx->n_xslots_real;
+    const std::string k(kernel);
+    double b = -1.0;
+    if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out */
+        b = N * (blk + vec) + X * (blk + 4.0 + vec);
+    else if (k == "fast_resid_rhs") /* Dinv, R in, b out */
+        b = N * (blk + 2 * vec);
+    else if (k == "fast_resid32_rhs")
+        b = N * (blk + 2 * vec) / 2;
+    else if (k == "fast_resid32")
+        b = N * (blk + vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
+    else if (k == "fast_thomas") /* G, b, y out | Gam, y in, U in/out, dU out */
+        b = N * (2 * blk + 6 * vec);
+    else if (k == "fast_thomas32")
+        b = N * (2 * blk + 6 * vec) / 2;
+    else if (k == "full_resid") /* D, 2 blocks per face, U (own + nbrs), rhs, R out, ints */
+        b = N * blk + 2 * F * blk + N * vec + 2 * F * vec + N * vec + N * vec / 2 +
+            4.0 * (N + 1 + ctx->eftot + 2 * F + N);
+    else if (k == "ref_solve_du") /* DLU, A, DinvC, R, dU out, dU in+out (back) */
+        b = N * (3 * blk + 4 * vec) + 4.0 * N;
+    else if (k == "ref_add_copy")
+        b = N * 5 * vec;
+    else if (k == "ref_line_res")
+        b = N * blk + 2 * F * blk + N * vec + 2 * F * vec + 2 * N * vec +
+            4.0 * (N + 1 + ctx->eftot + 2 * F);
+    else if (k == "fast_factor") /* D, A, C in; Dinv, G, Gam out */
+        b = N * blk + 2 * (N - ctx->nline) * blk + 3 * N * blk;
+    if (b < 0) return ctx_fail(ctx, TBS_ERR_ARG, "unknown kernel name " + k);
+    *bytes = b;
+    return TBS_OK;
+}
+
+}  // extern "C"

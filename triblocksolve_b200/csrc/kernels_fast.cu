@@ -1,0 +1,874 @@
+/*
+ * kernels_fast.cu -- TBS_ALGO_FP64 / TBS_ALGO_MIXED kernels for sm_100a,
+ * plus the norm / permutation helpers every algorithm uses.
+ *
+ * The LIJ sweep of the reference (src/main.cxx:207-229) is
+ *     dU = -M^-1 R ;  U += dU ;  R = rhs + J U
+ * with M the block-tridiagonal part of J along each line.  Writing
+ * J = M + O (O = couplings between different lines) and using M dU = -R,
+ *     R_new = R + J dU = O dU,
+ * so after the first sweep only the cross-line blocks are read to update
+ * the residual.  The line solve is rewritten with explicit inverses:
+ *     b_k  = -Dinv_k R_k                         (fast_resid, all cells)
+ *     y_k  = b_k - G_k y_{k-1},   G_k = Dinv_k A_k (fast_thomas forward)
+ *     dU_k = y_k - Gam_k dU_{k+1}, Gam_k = Dinv_k C_k (backward)
+ * where Dinv_k = (D_k - A_k Gam_{k-1})^-1 is the inverse of the block-Thomas
+ * pivot of src/okl/lineLU_v2.okl:58-182.  The recurrence on each line is
+ * then one 9x9 matvec per cell; everything else is data parallel.
+ *
+ * Data are "position" ordered: cells in line order, each line starting at a
+ * multiple of 4 positions, so that runs of cells are 16-byte aligned for
+ * cp.async.bulk in FP64 and FP32 alike.
+ */
+#include "tbs_internal.hxx"
+#include "tma.cuh"
+
+#include <cuda_runtime.h>
+
+namespace tbs {
+
+constexpr int NV = 9;
+constexpr int NB = 81;
+constexpr unsigned FULL = 0xffffffffu;
+
+/* ================================================================ helpers */
+
+__global__ void zero_kernel(double *p, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        p[t] = 0.0;
+}
+
+static int grid_for(long long n, int threads, int cap = 148 * 8) {
+    long long b = (n + threads - 1) / threads;
+    if (b > cap) b = cap;
+    if (b < 1) b = 1;
+    return (int)b;
+}
+
+int launch_zero(cudaStream_t st, double *p, long long n) {
+    zero_kernel<<<grid_for(n, 256), 256, 0, st>>>(p, n);
+    return (int)cudaGetLastError();
+}
+
+/* block b sums v[b*chunk : (b+1)*chunk)^2 in a fixed order */
+__global__ void norm_partials_kernel(const double *__restrict__ v, long long n, long long chunk,
+                                     double *__restrict__ partials) {
+    const long long lo = blockIdx.x * chunk;
+    long long hi = lo + chunk;
+    if (hi > n) hi = n;
+    double s = 0.0;
+    for (long long t = lo + threadIdx.x; t < hi; t += blockDim.x) s += v[t] * v[t];
+    __shared__ double red[8];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(FULL, s, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = s;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w) tot += red[w];
+        partials[blockIdx.x] = tot;
+    }
+}
+
+int launch_norm_partials(cudaStream_t st, const double *v, long long n, double *partials,
+                         int npart) {
+    long long chunk = (n + npart - 1) / npart;
+    if (chunk < 1) chunk = 1;
+    norm_partials_kernel<<<npart, 256, 0, st>>>(v, n, chunk, partials);
+    return (int)cudaGetLastError();
+}
+
+/* Sum the partials in a fixed order, record the norm and decide whether the
+ * solve goes on.  The decision feeds the CUDA graph's while-node, so the
+ * sweep loop never returns to the host. */
+__global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, SolveState *state,
+                                   double *hist, int is_start,
+                                   cudaGraphConditionalHandle handle, int use_cond) {
+    __shared__ double s[256];
+    double acc = 0.0;
+    for (int t = threadIdx.x; t < n; t += 256) acc += partials[t];
+    s[threadIdx.x] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int t = 0; t < 256; ++t) tot += s[t];
+        const double nrm = sqrt(tot);
+        if (is_start) {
+            state->sweep = 0;
+            state->norm0 = nrm;
+        } else {
+            state->sweep += 1;
+        }
+        const int sw = state->sweep;
+        if (sw < state->hist_cap) hist[sw] = nrm;
+        state->last = nrm;
+        const bool go = isfinite(nrm) && nrm > state->tol * state->norm0 && sw < state->max_sweeps;
+        if (use_cond) cudaGraphSetConditional(handle, go ? 1u : 0u);
+    }
+}
+
+int launch_reduce_norm(cudaStream_t st, const double *partials, int n, SolveState *state,
+                       double *hist, int is_start, unsigned long long cond_handle, int use_cond) {
+    reduce_norm_kernel<<<1, 256, 0, st>>>(partials, n, state, hist, is_start,
+                                         (cudaGraphConditionalHandle)cond_handle, use_cond);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+__global__ void permute_to_pos_kernel(int nv, int nelem, const int *__restrict__ pos_of_elem,
+                                      const double *__restrict__ src, T *__restrict__ dst) {
+    long long n = (long long)nv * nelem;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int e = (int)(t / nv), i = (int)(t - (long long)e * nv);
+        dst[(long long)pos_of_elem[e] * nv + i] = (T)src[t];
+    }
+}
+
+__global__ void permute_to_elem_kernel(int nv, int nelem, const int *__restrict__ pos_of_elem,
+                                       const double *__restrict__ src, double *__restrict__ dst) {
+    long long n = (long long)nv * nelem;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int e = (int)(t / nv), i = (int)(t - (long long)e * nv);
+        dst[t] = src[(long long)pos_of_elem[e] * nv + i];
+    }
+}
+
+int launch_permute_to_pos(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                          const double *src_elem, double *dst_pos) {
+    permute_to_pos_kernel<double>
+        <<<grid_for((long long)nv * nelem, 256), 256, 0, st>>>(nv, nelem, pos_of_elem, src_elem, dst_pos);
+    return (int)cudaGetLastError();
+}
+
+int launch_permute_to_elem(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                           const double *src_pos, double *dst_elem) {
+    permute_to_elem_kernel<<<grid_for((long long)nv * nelem, 256), 256, 0, st>>>(
+        nv, nelem, pos_of_elem, src_pos, dst_elem);
+    return (int)cudaGetLastError();
+}
+
+__global__ void permute_f32_to_elem_kernel(int nv, int nelem, const int *__restrict__ pos_of_elem,
+                                           const float *__restrict__ src,
+                                           double *__restrict__ dst) {
+    long long n = (long long)nv * nelem;
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x) {
+        int e = (int)(t / nv), i = (int)(t - (long long)e * nv);
+        dst[t] = (double)src[(long long)pos_of_elem[e] * nv + i];
+    }
+}
+
+int launch_permute_f32_to_elem(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                               const float *src_pos, double *dst_elem) {
+    permute_f32_to_elem_kernel<<<grid_for((long long)nv * nelem, 256), 256, 0, st>>>(
+        nv, nelem, pos_of_elem, src_pos, dst_elem);
+    return (int)cudaGetLastError();
+}
+
+__global__ void cast_kernel(const double *__restrict__ s, float *__restrict__ d, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        d[t] = (float)s[t];
+}
+
+int launch_cast_f64_f32(cudaStream_t st, const double *src, float *dst, long long n) {
+    cast_kernel<<<grid_for(n, 256), 256, 0, st>>>(src, dst, n);
+    return (int)cudaGetLastError();
+}
+
+__global__ void axpy_kernel(const float *__restrict__ d, double *__restrict__ U, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        U[t] += (double)d[t];
+}
+
+int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n) {
+    axpy_kernel<<<grid_for(n, 256), 256, 0, st>>>(d, U, n);
+    return (int)cudaGetLastError();
+}
+
+/* ====================================================== line factorization
+ * One CTA of 128 threads per line, thread t < 81 owns entry t of each 9x9
+ * block (row t%9, column t/9).  Per cell k >= 1:
+ *   Gam_{k-1} = Dinv_{k-1} C_{k-1}
+ *   W         = D_k - A_k Gam_{k-1}          (block-Thomas pivot D'_k)
+ *   Dinv_k    = W^-1   (in-place Gauss-Jordan, no pivoting, as the
+ *                        reference's LU has none: lineLU_v2.okl:17-27)
+ *   G_k       = Dinv_k A_k
+ * A/C are the two blocks of the in-line face joining cells k-1 and k,
+ * picked as in lineLU_v2.okl:116-117.  The FP32 arrays, when given, are
+ * the FP64 results rounded once. */
+__device__ __forceinline__ void gj_invert(double *W, int t, unsigned *status) {
+    const int i = t % NV, j = t / NV;
+#pragma unroll 1
+    for (int p = 0; p < NV; ++p) {
+        double wpp = 0.0, wip = 0.0, wpj = 0.0, wij = 0.0;
+        if (t < NB) {
+            wpp = W[p * (NV + 1)];
+            wip = W[i + NV * p];
+            wpj = W[p + NV * j];
+            wij = W[t];
+        }
+        __syncthreads();
+        if (t < NB) {
+            const double r = 1.0 / wpp;
+            double v;
+            if (i == p && j == p)
+                v = r;
+            else if (i == p)
+                v = wpj * r;
+            else if (j == p)
+                v = -wip * r;
+            else
+                v = wij - wip * (wpj * r);
+            W[t] = v;
+        }
+        if (t == 0 && !(fabs(wpp) > 0.0 && isfinite(wpp))) atomicOr(status, ST_PIVOT);
+        __syncthreads();
+    }
+}
+
+__global__ void __launch_bounds__(128) fast_factor_kernel(
+    int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
+    const int *__restrict__ fsrc, const double *__restrict__ jacD, const double *__restrict__ O1,
+    const double *__restrict__ O2, double *__restrict__ Dinv, double *__restrict__ G,
+    double *__restrict__ Gam, float *__restrict__ Dinv32, float *__restrict__ G32,
+    float *__restrict__ Gam32, unsigned *status) {
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    const int t = threadIdx.x;
+    const bool act = t < NB;
+    const int i = t % NV, j = t / NV;
+    __shared__ double sW[NB], sPrev[NB], sA[NB], sC[NB], sGam[NB];
+    const int ps = line_start[l];
+    const int n = line_len[l];
+
+    double d = 0.0, a = 0.0, c = 0.0;
+    if (act) d = jacD[(size_t)fsrc[3 * ps] * NB + t];
+    if (act) sW[t] = d;
+    __syncthreads();
+    gj_invert(sW, t, status);
+    if (act) {
+        const double w = sW[t];
+        if (Dinv) {
+            Dinv[(size_t)ps * NB + t] = w;
+            G[(size_t)ps * NB + t] = 0.0;
+        }
+        if (Dinv32) {
+            Dinv32[(size_t)ps * NB + t] = (float)w;
+            G32[(size_t)ps * NB + t] = 0.0f;
+        }
+        sPrev[t] = w;
+    }
+    /* prefetch cell 1 */
+    auto fetch = [&](int p) {
+        if (act) {
+            const int e = fsrc[3 * p], f = fsrc[3 * p + 1], side = fsrc[3 * p + 2];
+            const double *Ap = side ? O2 : O1;
+            const double *Cp = side ? O1 : O2;
+            a = Ap[(size_t)f * NB + t];
+            c = Cp[(size_t)f * NB + t];
+            d = jacD[(size_t)e * NB + t];
+        }
+    };
+    if (n > 1) fetch(ps + 1);
+    for (int k = 1; k < n; ++k) {
+        const int p = ps + k;
+        __syncthreads();
+        if (act) {
+            sA[t] = a;
+            sC[t] = c;
+            sW[t] = d;
+        }
+        __syncthreads();
+        if (k + 1 < n) fetch(p + 1);
+        double g = 0.0;
+        if (act) {
+#pragma unroll
+            for (int q = 0; q < NV; ++q) g += sPrev[i + NV * q] * sC[q + NV * j];
+            sGam[t] = g;
+            if (Gam) Gam[(size_t)(p - 1) * NB + t] = g;
+            if (Gam32) Gam32[(size_t)(p - 1) * NB + t] = (float)g;
+        }
+        __syncthreads();
+        if (act) {
+            double w = sW[t];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) w -= sA[i + NV * q] * sGam[q + NV * j];
+            sW[t] = w;
+        }
+        __syncthreads();
+        gj_invert(sW, t, status);
+        if (act) {
+            double gk = 0.0;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) gk += sW[i + NV * q] * sA[q + NV * j];
+            const double w = sW[t];
+            if (Dinv) {
+                G[(size_t)p * NB + t] = gk;
+                Dinv[(size_t)p * NB + t] = w;
+            }
+            if (Dinv32) {
+                G32[(size_t)p * NB + t] = (float)gk;
+                Dinv32[(size_t)p * NB + t] = (float)w;
+            }
+            sPrev[t] = w;
+        }
+    }
+    if (act) {
+        if (Gam) Gam[(size_t)(ps + n - 1) * NB + t] = 0.0;
+        if (Gam32) Gam32[(size_t)(ps + n - 1) * NB + t] = 0.0f;
+    }
+}
+
+int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD, const double *O1,
+                       const double *O2, double *Dinv, double *G, double *Gam, float *Dinv32,
+                       float *G32, float *Gam32, unsigned *status) {
+    if (L.nv != NV) return (int)cudaErrorInvalidValue;
+    fast_factor_kernel<<<L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.fsrc, jacD, O1,
+                                                O2, Dinv, G, Gam, Dinv32, G32, Gam32, status);
+    return (int)cudaGetLastError();
+}
+
+/* X[slot] = cross-line block of that slot, or zeros; one warp per slot */
+__global__ void fast_xlayout_kernel(long long nslots, const int *__restrict__ xsrc,
+                                    const double *__restrict__ O1, const double *__restrict__ O2,
+                                    double *__restrict__ X, float *__restrict__ X32) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long q = w0; q < nslots; q += nw) {
+        const int src = xsrc[q];
+        for (int tt = lane; tt < NB; tt += 32) {
+            double v = 0.0;
+            if (src >= 0) v = ((src & 1) ? O2 : O1)[(size_t)(src >> 1) * NB + tt];
+            if (X) X[q * NB + tt] = v;
+            if (X32) X32[q * NB + tt] = (float)v;
+        }
+    }
+}
+
+int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, const double *O2,
+                        double *X, float *X32) {
+    const long long nslots = (long long)L.np16 * L.nx;
+    if (nslots == 0) return 0;
+    fast_xlayout_kernel<<<grid_for(nslots * 32, 256), 256, 0, st>>>(nslots, L.xsrc, O1, O2, X, X32);
+    return (int)cudaGetLastError();
+}
+
+/* ================================================ residual -> Thomas RHS
+ * Persistent CTAs stream tiles of RES_TILE positions through a 3-stage
+ * cp.async.bulk ring.  Per tile:
+ *   mode 0:  R = Rsrc (a residual already in position order)
+ *   mode 1:  R = sum over slots X_slot dU[xnbr_slot]   (R_new = O dU)
+ * then b = -Dinv R, and every CTA adds sum R^2 of its tiles into its own
+ * partial (fixed order).  Thread (c,i), c < 16, i < 9, owns row i of cell c.
+ */
+constexpr int RES_THREADS_FAST = 160;
+constexpr int RES_STAGES = 3;
+
+int fast_resid_grid(int np16) {
+    int ntiles = np16 / RES_TILE;
+    int g = 2 * 148;
+    if (ntiles < g) g = ntiles;
+    return g < 1 ? 1 : g;
+}
+
+template <typename T>
+__host__ __device__ inline uint32_t resid_stage_bytes(int nx) {
+    return (uint32_t)(RES_TILE * NB * sizeof(T) + RES_TILE * nx * NB * sizeof(T) +
+                      RES_TILE * nx * sizeof(int) + RES_TILE * NV * sizeof(T));
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
+    int ntiles, int nx, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
+    const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
+    T *__restrict__ b, double *__restrict__ partials, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    unsigned char *st0 = smem + 128;
+    const uint32_t szD = RES_TILE * NB * sizeof(T);
+    const uint32_t szX = RES_TILE * nx * NB * sizeof(T);
+    const uint32_t szN = RES_TILE * nx * sizeof(int);
+    const uint32_t szR = RES_TILE * NV * sizeof(T);
+    const uint32_t stage = szD + szX + szN + szR;
+    T *sg = reinterpret_cast<T *>(st0 + RES_STAGES * stage);
+    T *sr = sg + RES_TILE * (nx > 0 ? nx : 1) * NV;
+
+    const int tid = threadIdx.x;
+    const int c = tid / NV, i = tid - NV * (tid / NV);
+    const bool act = tid < RES_TILE * NV;
+
+    if (tid == 0) {
+        for (int s = 0; s < RES_STAGES; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    uint64_t pol = 0;
+    if (tid == 0) pol = policy_evict_first();
+    auto issue = [&](int s, int tile) {
+        unsigned char *base = st0 + (size_t)s * stage;
+        if (mode == 0) {
+            mbar_arrive_expect_tx(&bars[s], szD + szR);
+            bulk_g2s_hint(base, Dinv + (size_t)tile * RES_TILE * NB, szD, &bars[s], pol);
+            bulk_g2s(base + szD + szX + szN, Rsrc + (size_t)tile * RES_TILE * NV, szR, &bars[s]);
+        } else {
+            mbar_arrive_expect_tx(&bars[s], szD + szX + szN);
+            bulk_g2s_hint(base, Dinv + (size_t)tile * RES_TILE * NB, szD, &bars[s], pol);
+            bulk_g2s_hint(base + szD, X + (size_t)tile * RES_TILE * nx * NB, szX, &bars[s], pol);
+            bulk_g2s(base + szD + szX, xnbr + (size_t)tile * RES_TILE * nx, szN, &bars[s]);
+        }
+    };
+    int issued[RES_STAGES] = {0}, used[RES_STAGES] = {0};
+    if (tid == 0) {
+        for (int s = 0; s < RES_STAGES; ++s) {
+            const int tile = blockIdx.x + s * gridDim.x;
+            if (tile < ntiles) {
+                issue(s, tile);
+                issued[s]++;
+            }
+        }
+    }
+
+    double sq = 0.0;
+    int it = 0;
+    bool timed_out = false;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
+        const int s = it % RES_STAGES;
+        const uint32_t par = (uint32_t)((it / RES_STAGES) & 1);
+        const bool ok = mbar_wait(&bars[s], par);
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        if (tid == 0) used[s]++;
+        const unsigned char *base = st0 + (size_t)s * stage;
+        const T *sD = reinterpret_cast<const T *>(base);
+        T r = T(0);
+        if (mode == 0) {
+            const T *sR = reinterpret_cast<const T *>(base + szD + szX + szN);
+            if (act) r = sR[c * NV + i];
+        } else {
+            const T *sX = reinterpret_cast<const T *>(base + szD);
+            const int *sN = reinterpret_cast<const int *>(base + szD + szX);
+            if (act) {
+                for (int q = 0; q < nx; ++q) {
+                    const int nb = sN[c * nx + q];
+                    sg[(c * nx + q) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
+                }
+            }
+            __syncthreads();
+            if (act) {
+                T a0 = T(0), a1 = T(0), a2 = T(0);
+                for (int q = 0; q < nx; ++q) {
+                    const T *xr = sX + (c * nx + q) * NB + i;
+                    const T *g = sg + (c * nx + q) * NV;
+                    a0 += xr[0] * g[0];
+                    a1 += xr[9] * g[1];
+                    a2 += xr[18] * g[2];
+                    a0 += xr[27] * g[3];
+                    a1 += xr[36] * g[4];
+                    a2 += xr[45] * g[5];
+                    a0 += xr[54] * g[6];
+                    a1 += xr[63] * g[7];
+                    a2 += xr[72] * g[8];
+                }
+                r = a0 + (a1 + a2);
+            }
+        }
+        if (act) {
+            sr[c * NV + i] = r;
+            sq += (double)r * (double)r;
+        }
+        __syncthreads();
+        if (act) {
+            const T *dr = sD + c * NB + i;
+            const T *rv = sr + c * NV;
+            T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
+            a0 += dr[27] * rv[3];
+            a1 += dr[36] * rv[4];
+            a2 += dr[45] * rv[5];
+            a0 += dr[54] * rv[6];
+            a1 += dr[63] * rv[7];
+            a2 += dr[72] * rv[8];
+            b[((size_t)tile * RES_TILE + c) * NV + i] = -(a0 + (a1 + a2));
+        }
+        __syncthreads();
+        if (tid == 0) {
+            const int next = tile + RES_STAGES * gridDim.x;
+            if (next < ntiles) {
+                issue(s, next);
+                issued[s]++;
+            }
+        }
+    }
+    if (timed_out) {
+        if (tid == 0) {
+            atomicOr(status, ST_TIMEOUT);
+            /* let copies still in flight land before the CTA retires */
+            for (int s = 0; s < RES_STAGES; ++s)
+                for (int u = used[s]; u < issued[s]; ++u)
+                    mbar_wait(&bars[s], (uint32_t)(u & 1), 1LL << 28);
+        }
+        return;
+    }
+    __shared__ double red[RES_THREADS_FAST / 32];
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+    if ((tid & 31) == 0) red[tid >> 5] = sq;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
+        partials[blockIdx.x] = tot;
+    }
+}
+
+template <typename T>
+int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv, const T *X,
+                      const T *dU, const T *Rsrc, T *b, double *partials, int npart,
+                      unsigned *status) {
+    if (L.nv != NV) return (int)cudaErrorInvalidValue;
+    const int ntiles = L.np16 / RES_TILE;
+    const int grid = fast_resid_grid(L.np16);
+    if (npart != grid) return (int)cudaErrorInvalidValue;
+    const int nxa = L.nx > 0 ? L.nx : 1;
+    const size_t smem = 128 + RES_STAGES * (size_t)resid_stage_bytes<T>(L.nx) +
+                        (size_t)RES_TILE * nxa * NV * sizeof(T) + RES_TILE * NV * sizeof(T);
+    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
+    if (mode == 1 && L.nx == 0) mode = 2; /* no cross-line couplings: R = 0 */
+    if (mode == 2) {
+        /* a mesh that is a single line: the line solve is exact, R_new = 0 */
+        cudaMemsetAsync(b, 0, (size_t)L.np16 * NV * sizeof(T), st);
+        cudaMemsetAsync(partials, 0, (size_t)npart * sizeof(double), st);
+        return (int)cudaGetLastError();
+    }
+    fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(ntiles, L.nx, mode, Dinv, X, L.xnbr,
+                                                               dU, Rsrc, b, partials, status);
+    return (int)cudaGetLastError();
+}
+
+template int launch_fast_resid<double>(cudaStream_t, const FastLayout &, int, const double *,
+                                       const double *, const double *, const double *, double *,
+                                       double *, int, unsigned *);
+template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, const float *,
+                                      const float *, const float *, const float *, float *,
+                                      double *, int, unsigned *);
+
+/* =========================================================== line Thomas
+ * One warp per line.  Lane 0 streams "jobs" through an NS-stage bulk-copy
+ * ring: jobs 0..nch-1 are forward chunks (G and b of P cells), jobs
+ * nch..2nch-1 backward chunks in reverse (Gam of P cells).  Lanes 0..8 own
+ * rows; the 9-vector of the previous cell is replicated in every lane with
+ * shuffles.  y (forward result) is written to global memory and read back
+ * by the same lane in the backward pass; U and y loads of the next
+ * backward chunk are issued one chunk ahead.
+ *   accumulate = 0:  U = dU  (first sweep of a solve, U starts at 0)
+ *   accumulate = 1:  U += dU
+ */
+constexpr int THOMAS_P = 8;
+
+template <typename T>
+__host__ __device__ inline uint32_t thomas_stage_bytes() {
+    return (uint32_t)(THOMAS_P * (NB + NV) * sizeof(T));
+}
+
+template <typename T, int P>
+__global__ void __launch_bounds__(32) fast_thomas_kernel(
+    int nline, int NS, int accumulate, const int *__restrict__ line_start,
+    const int *__restrict__ line_len, const T *__restrict__ G, const T *__restrict__ Gam,
+    const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU, T *__restrict__ U,
+    unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    unsigned char *st0 = smem + 128;
+    const uint32_t stage = P * (NB + NV) * sizeof(T);
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    const int lane = threadIdx.x;
+    const int i = lane < NV ? lane : NV - 1;
+    const int ps = line_start[l];
+    const int n = line_len[l];
+    const int npad = (n + 3) & ~3;
+    const int nch = (npad + P - 1) / P;
+    const int njobs = 2 * nch;
+
+    if (lane == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+
+    uint64_t pol = 0;
+    if (lane == 0) pol = policy_evict_first();
+    auto issue = [&](int job, int s) {
+        unsigned char *base = st0 + (size_t)s * stage;
+        if (job < nch) {
+            const int c = job;
+            const int cnt = min(P, npad - c * P);
+            const uint32_t bg = cnt * NB * sizeof(T), bb = cnt * NV * sizeof(T);
+            mbar_arrive_expect_tx(&bars[s], bg + bb);
+            bulk_g2s_hint(base, G + (size_t)(ps + c * P) * NB, bg, &bars[s], pol);
+            bulk_g2s(base + P * NB * sizeof(T), b + (size_t)(ps + c * P) * NV, bb, &bars[s]);
+        } else {
+            const int c = njobs - 1 - job;
+            const int cnt = min(P, npad - c * P);
+            const uint32_t bg = cnt * NB * sizeof(T);
+            mbar_arrive_expect_tx(&bars[s], bg);
+            bulk_g2s_hint(base, Gam + (size_t)(ps + c * P) * NB, bg, &bars[s], pol);
+        }
+    };
+    int issued = 0;
+    if (lane == 0) {
+        for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
+    }
+    int consumed = 0;
+    bool timed_out = false;
+
+    /* ---------------- forward: y_k = b_k - G_k y_{k-1} */
+    T yp[NV];
+#pragma unroll
+    for (int j = 0; j < NV; ++j) yp[j] = T(0);
+    for (int c = 0; c < nch; ++c) {
+        const int s = c % NS;
+        const uint32_t par = (uint32_t)((c / NS) & 1);
+        const bool ok = mbar_wait(&bars[s], par);
+        if (__any_sync(FULL, !ok)) {
+            timed_out = true;
+            break;
+        }
+        ++consumed;
+        const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
+        const T *sB = sG + P * NB;
+#pragma unroll
+        for (int q = 0; q < P; ++q) {
+            const int k = c * P + q;
+            if (k < n) {
+                const T *g = sG + q * NB + i;
+                T a0 = sB[q * NV + i], a1 = T(0), a2 = T(0);
+                a0 -= g[0] * yp[0];
+                a1 -= g[9] * yp[1];
+                a2 -= g[18] * yp[2];
+                a0 -= g[27] * yp[3];
+                a1 -= g[36] * yp[4];
+                a2 -= g[45] * yp[5];
+                a0 -= g[54] * yp[6];
+                a1 -= g[63] * yp[7];
+                a2 -= g[72] * yp[8];
+                const T yi = a0 + (a1 + a2);
+                if (lane < NV) y[(size_t)(ps + k) * NV + lane] = yi;
+#pragma unroll
+                for (int j = 0; j < NV; ++j) yp[j] = __shfl_sync(FULL, yi, j);
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && issued < njobs) {
+            issue(issued, s);
+            ++issued;
+        }
+    }
+
+    /* ---------------- backward: dU_k = y_k - Gam_k dU_{k+1} */
+    if (!timed_out) {
+        T dn[NV];
+#pragma unroll
+        for (int j = 0; j < NV; ++j) dn[j] = T(0);
+        T yv[P], uv[P], nyv[P], nuv[P];
+        auto load_chunk = [&](int c, T *yy, T *uu) {
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                const int k = c * P + q;
+                yy[q] = T(0);
+                uu[q] = T(0);
+                if (k < n && lane < NV) {
+                    yy[q] = y[(size_t)(ps + k) * NV + lane];
+                    if (accumulate) uu[q] = U[(size_t)(ps + k) * NV + lane];
+                }
+            }
+        };
+        load_chunk(nch - 1, yv, uv);
+        for (int jb = 0; jb < nch; ++jb) {
+            const int job = nch + jb;
+            const int c = nch - 1 - jb;
+            if (c > 0) load_chunk(c - 1, nyv, nuv);
+            const int s = job % NS;
+            const uint32_t par = (uint32_t)((job / NS) & 1);
+            const bool ok = mbar_wait(&bars[s], par);
+            if (__any_sync(FULL, !ok)) {
+                timed_out = true;
+                break;
+            }
+            ++consumed;
+            const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
+#pragma unroll
+            for (int q = P - 1; q >= 0; --q) {
+                const int k = c * P + q;
+                if (k < n) {
+                    const T *g = sG + q * NB + i;
+                    T a0 = yv[q], a1 = T(0), a2 = T(0);
+                    a0 -= g[0] * dn[0];
+                    a1 -= g[9] * dn[1];
+                    a2 -= g[18] * dn[2];
+                    a0 -= g[27] * dn[3];
+                    a1 -= g[36] * dn[4];
+                    a2 -= g[45] * dn[5];
+                    a0 -= g[54] * dn[6];
+                    a1 -= g[63] * dn[7];
+                    a2 -= g[72] * dn[8];
+                    const T d = a0 + (a1 + a2);
+                    if (lane < NV) {
+                        dU[(size_t)(ps + k) * NV + lane] = d;
+                        U[(size_t)(ps + k) * NV + lane] = uv[q] + d;
+                    }
+#pragma unroll
+                    for (int j = 0; j < NV; ++j) dn[j] = __shfl_sync(FULL, d, j);
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && issued < njobs) {
+                issue(issued, s);
+                ++issued;
+            }
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                yv[q] = nyv[q];
+                uv[q] = nuv[q];
+            }
+        }
+    }
+    if (timed_out && lane == 0) {
+        atomicOr(status, ST_TIMEOUT);
+        for (int job = consumed; job < issued; ++job)
+            mbar_wait(&bars[job % NS], (uint32_t)((job / NS) & 1), 1LL << 28);
+    }
+}
+
+static int thomas_stages(int nline, size_t stage_bytes) {
+    const int per_sm = (nline + 147) / 148;
+    long long budget = 200LL * 1024 / (per_sm > 0 ? per_sm : 1);
+    long long ns = (budget - 128) / (long long)stage_bytes;
+    if (ns > 8) ns = 8;
+    if (ns < 2) ns = 2;
+    return (int)ns;
+}
+
+template <typename T>
+int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
+                       T *y, T *dU, T *U, unsigned *status, int accumulate) {
+    if (L.nv != NV) return (int)cudaErrorInvalidValue;
+    const size_t sb = thomas_stage_bytes<T>();
+    const int NS = thomas_stages(L.nline, sb);
+    const size_t smem = 128 + NS * sb;
+    fast_thomas_kernel<T, THOMAS_P><<<L.nline, 32, smem, st>>>(
+        L.nline, NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
+    return (int)cudaGetLastError();
+}
+
+template int launch_fast_thomas<double>(cudaStream_t, const FastLayout &, const double *,
+                                        const double *, const double *, double *, double *,
+                                        double *, unsigned *, int);
+template int launch_fast_thomas<float>(cudaStream_t, const FastLayout &, const float *,
+                                       const float *, const float *, float *, float *, float *,
+                                       unsigned *, int);
+
+/* Opt the streaming kernels into the large shared-memory carve-out on the
+ * current device (called once per context after cudaSetDevice). */
+int fast_kernels_init() {
+    cudaFuncSetAttribute(fast_resid_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    cudaFuncSetAttribute(fast_resid_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                         227 * 1024);
+    cudaFuncSetAttribute(fast_thomas_kernel<double, THOMAS_P>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    cudaFuncSetAttribute(fast_thomas_kernel<float, THOMAS_P>,
+                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
+    return (int)cudaGetLastError();
+}
+
+/* ============================================ true residual, any ordering
+ * R(pos(e)) = rhs(e) + D_e U(pos(e)) + sum_{faces} offJ U(pos(nbr)) with the
+ * original FP64 blocks (face rule of linesmoothLU_TriBlock_v3.okl:299-328),
+ * output in position order as T, plus fixed-order per-block sum R^2.
+ * Used for the FP64 outer residual of TBS_ALGO_MIXED, for a non-zero
+ * starting solution, and for tbs_true_residual_norm / tbs_get_residual. */
+constexpr int FULLRES_THREADS = 288;
+
+template <typename T>
+__global__ void __launch_bounds__(FULLRES_THREADS) full_resid_kernel(
+    int nelem, const int *__restrict__ epoint, const int *__restrict__ ef,
+    const int *__restrict__ fc, const int *__restrict__ pos_of_elem,
+    const double *__restrict__ D, const double *__restrict__ O1, const double *__restrict__ O2,
+    const double *__restrict__ rhs, const double *__restrict__ Up, T *__restrict__ Rp,
+    double *__restrict__ partials) {
+    const int epb = FULLRES_THREADS / NV;
+    const int le = threadIdx.x / NV;
+    const int i = threadIdx.x - le * NV;
+    const int e = blockIdx.x * epb + le;
+    double sq = 0.0;
+    if (e < nelem) {
+        const int pe = pos_of_elem[e];
+        const double *u = Up + (size_t)pe * NV;
+        const double *dr = D + (size_t)e * NB + i;
+        double a0 = dr[0] * u[0], a1 = dr[9] * u[1], a2 = dr[18] * u[2];
+        a0 += dr[27] * u[3];
+        a1 += dr[36] * u[4];
+        a2 += dr[45] * u[5];
+        a0 += dr[54] * u[6];
+        a1 += dr[63] * u[7];
+        a2 += dr[72] * u[8];
+        for (int k2 = epoint[e]; k2 < epoint[e + 1]; ++k2) {
+            const int f = ef[k2];
+            if (f >= 0) {
+                const int e1 = fc[2 * f], e2 = fc[2 * f + 1];
+                const double *o = ((e == e1) ? O2 : O1) + (size_t)f * NB + i;
+                const double *un = Up + (size_t)pos_of_elem[(e == e1) ? e2 : e1] * NV;
+                a0 += o[0] * un[0];
+                a1 += o[9] * un[1];
+                a2 += o[18] * un[2];
+                a0 += o[27] * un[3];
+                a1 += o[36] * un[4];
+                a2 += o[45] * un[5];
+                a0 += o[54] * un[6];
+                a1 += o[63] * un[7];
+                a2 += o[72] * un[8];
+            }
+        }
+        const double r = rhs[(size_t)e * NV + i] + (a0 + (a1 + a2));
+        Rp[(size_t)pe * NV + i] = (T)r;
+        sq = r * r;
+    }
+    __shared__ double red[FULLRES_THREADS / 32];
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = sq;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < FULLRES_THREADS / 32; ++w) tot += red[w];
+        partials[blockIdx.x] = tot;
+    }
+}
+
+int full_resid_blocks(int nelem) { return (nelem + (FULLRES_THREADS / NV) - 1) / (FULLRES_THREADS / NV); }
+
+template <typename T>
+int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *ef, const int *fc,
+                      const int *pos_of_elem, const double *D, const double *O1, const double *O2,
+                      const double *rhs, const double *Up, T *Rp, double *partials) {
+    full_resid_kernel<T><<<full_resid_blocks(nelem), FULLRES_THREADS, 0, st>>>(
+        nelem, epoint, ef, fc, pos_of_elem, D, O1, O2, rhs, Up, Rp, partials);
+    return (int)cudaGetLastError();
+}
+
+template int launch_full_resid<double>(cudaStream_t, int, const int *, const int *, const int *,
+                                       const int *, const double *, const double *,
+                                       const double *, const double *, const double *, double *,
+                                       double *);
+template int launch_full_resid<float>(cudaStream_t, int, const int *, const int *, const int *,
+                                      const int *, const double *, const double *,
+                                      const double *, const double *, const double *, float *,
+                                      double *);
+
+}  // namespace tbs

@@ -1,0 +1,155 @@
+/*
+ * tbs_internal.hxx -- declarations shared by the host code (formats.cpp,
+ * api.cu) and the kernel translation units (kernels_ref.cu,
+ * kernels_fast.cu).  Not installed; the public surface is include/triblock.h.
+ */
+#ifndef TBS_INTERNAL_HXX
+#define TBS_INTERNAL_HXX
+
+#include "../../include/triblock.h"
+
+#include <cstddef>
+#include <cstdint>
+#include <string>
+
+#ifdef __CUDACC__
+#include <cuda_runtime.h>
+#else
+typedef struct CUstream_st *cudaStream_t;
+#endif
+
+namespace tbs {
+
+/* -------------------------------------------------------------- formats */
+void set_thread_error(const std::string &msg);
+const char *thread_error();
+long long mesh_file_bytes(const int hdr[6]);
+long long jacobian_file_bytes(const int hdr[3]);
+int read_mesh_header(const char *path, int hdr[6]);
+int read_mesh(const char *path, const int hdr[6], int *epoint, int *ef, int *fc, int *linesize,
+              int *linepoint, int *lines, int *lineface);
+int write_mesh(const char *path, const int hdr[6], const int *epoint, const int *ef, const int *fc,
+               const int *linesize, const int *linepoint, const int *lines, const int *lineface);
+int read_jacobian_header(const char *path, int hdr[3]);
+int read_jacobian(const char *path, const int hdr[3], double *jacD, double *jacO1, double *jacO2,
+                  double *rhs, double *U0);
+int write_jacobian(const char *path, const int hdr[3], const double *jacD, const double *jacO1,
+                   const double *jacO2, const double *rhs, const double *U0);
+int validate_mesh(const int hdr[6], const int *epoint, const int *ef, const int *fc,
+                  const int *linesize, const int *linepoint, const int *lines,
+                  const int *lineface);
+int gen_structured_header(int L, int K, int nvar, int hdr[6]);
+int gen_structured_mesh(int L, int K, int *epoint, int *ef, int *fc, int *linesize,
+                        int *linepoint, int *lines, int *lineface);
+int gen_jacobian(int nvar, int nelem, int nintface, double shift, uint64_t seed, double *jacD,
+                 double *jacO1, double *jacO2, double *rhs, double *U0);
+
+/* ------------------------------------------------------ device status bits
+ * Kernels never trap: they OR one of these into a device status word that
+ * the host reads after the launch sequence. */
+enum : unsigned {
+    ST_PIVOT = 1u,       /* zero or non-finite pivot in a block factorization */
+    ST_TIMEOUT = 2u,     /* an mbarrier wait ran out of its clock budget */
+    ST_BOUNDS = 4u,      /* an index failed a device-side range check */
+};
+
+/* Per-solve state that lives in device memory so that one instantiated
+ * CUDA graph serves every tolerance and sweep limit. */
+struct SolveState {
+    double norm0;      /* ||R_0|| of the current solve */
+    double tol;        /* relative tolerance */
+    double last;       /* latest ||R|| */
+    int max_sweeps;
+    int sweep;         /* sweeps done in the current solve */
+    int hist_cap;      /* entries available in hist */
+    int pad;
+};
+
+/* ------------------------------------------------- fast (line-ordered) layout
+ * Positions p index cells in line order; every line starts at a multiple of
+ * 4 positions (zero pad cells follow lines whose length is not a multiple
+ * of 4) so that a run of 4 cells of 9x9 blocks (2592 B in FP64, 1296 B in
+ * FP32) starts and ends on a 16-byte boundary, the rule for cp.async.bulk.
+ * np16 = positions rounded up to a multiple of RES_TILE, the residual
+ * kernel's tile. */
+constexpr int RES_TILE = 16;
+
+struct FastLayout {
+    int nv;        /* block size (9) */
+    int np;        /* positions incl. line pads */
+    int np16;      /* np rounded up to RES_TILE */
+    int nx;        /* cross-line coupling slots per position */
+    int nline;
+    int max_len;   /* longest line */
+    /* device arrays */
+    int *line_start;   /* [nline] even */
+    int *line_len;     /* [nline] */
+    int *pos_of_elem;  /* [nelem] */
+    int *elem_of_pos;  /* [np16], -1 for pads */
+    int *xnbr;         /* [np16*nx] neighbour position or -1 */
+    int *xsrc;         /* [np16*nx] 2*face + (1 if the block is O2), or -1 */
+    int *fsrc;         /* [np16*3] factor sources: elem, face of A/C, side */
+};
+
+/* ------------------------------------------------------ kernel launchers
+ * All launches go on `st`; they return cudaGetLastError() as an int. */
+
+/* reference-order kernels (kernels_ref.cu, built with -fmad=false) */
+int launch_ref_line_lu(cudaStream_t st, int nv, int nline, const int *fc, const int *linesize,
+                       const int *linepoint, const int *lines, const int *lineface, double *DLU,
+                       const double *O1, const double *O2, double *DinvC, unsigned *status);
+int launch_ref_assemble_A(cudaStream_t st, int nv, int nline, const int *fc, const int *linesize,
+                          const int *linepoint, const int *lines, const int *lineface,
+                          const double *O1, const double *O2, double *A);
+int launch_ref_solve_du(cudaStream_t st, int nv, int nline, const int *linesize,
+                        const int *linepoint, const int *lines, const double *DLU,
+                        const double *DinvC, const double *A, double *dU, const double *R);
+int launch_ref_add_copy(cudaStream_t st, long long n, const double *dU, double *U,
+                        const double *rhs, double *R);
+int launch_ref_line_res(cudaStream_t st, int nv, int nline, int nelem, const int *epoint,
+                        const int *ef, const int *fc, const int *linesize, const int *linepoint,
+                        const int *lines, const double *D, const double *O1, const double *O2,
+                        const double *U, double *R, double *partials, int *npartials_out);
+int ref_line_res_partials(int nelem);
+
+/* generic helpers (kernels_fast.cu) */
+int launch_norm_partials(cudaStream_t st, const double *v, long long n, double *partials,
+                         int npart);
+int launch_reduce_norm(cudaStream_t st, const double *partials, int n, SolveState *state,
+                       double *hist, int is_start, unsigned long long cond_handle, int use_cond);
+int launch_zero(cudaStream_t st, double *p, long long n);
+int launch_permute_to_pos(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                          const double *src_elem, double *dst_pos);
+int launch_permute_to_elem(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                           const double *src_pos, double *dst_elem);
+int launch_permute_f32_to_elem(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
+                               const float *src_pos, double *dst_elem);
+
+/* fast FP64 / FP32 kernels (kernels_fast.cu) */
+int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
+                       const double *O1, const double *O2, double *Dinv, double *G, double *Gam,
+                       float *Dinv32, float *G32, float *Gam32, unsigned *status);
+int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, const double *O2,
+                        double *X, float *X32);
+int fast_resid_grid(int np16);
+template <typename T>
+int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
+                      const T *X, const T *dU, const T *Rsrc, T *b, double *partials,
+                      int npart, unsigned *status);
+template <typename T>
+int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
+                       const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
+int fast_kernels_init();
+int full_resid_blocks(int nelem);
+template <typename T>
+int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *ef, const int *fc,
+                      const int *pos_of_elem, const double *D, const double *O1, const double *O2,
+                      const double *rhs, const double *Up, T *Rp, double *partials);
+
+/* mixed-precision glue (kernels_fast.cu) */
+int launch_cast_f64_f32(cudaStream_t st, const double *src, float *dst, long long n);
+int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n);
+
+}  // namespace tbs
+
+#endif /* TBS_INTERNAL_HXX */

@@ -1,0 +1,90 @@
+/*
+ * tma.cuh -- thin inline-PTX wrappers for the Blackwell (sm_100a) bulk-copy
+ * engine and shared-memory mbarriers used by the streaming kernels.
+ *
+ * Only the untiled bulk form is used (cp.async.bulk global -> shared, no
+ * multicast): every copy starts on a 16-byte boundary and moves a multiple
+ * of 16 bytes, which the callers guarantee through the even-cell layout.
+ * Every wait is bounded by a clock64 budget; on expiry the caller gets
+ * `false`, records ST_TIMEOUT and leaves instead of spinning forever.
+ */
+#ifndef TBS_TMA_CUH
+#define TBS_TMA_CUH
+
+#include <cstdint>
+
+namespace tbs {
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count)
+                 : "memory");
+}
+
+/* make initialised barriers visible to the async (bulk-copy) proxy */
+__device__ __forceinline__ void mbar_fence_init() {
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)),
+                 "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+/* Wait for phase `parity` of `bar` to complete; false after ~budget cycles. */
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
+                                          long long budget = (1LL << 31)) {
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long t0 = clock64();
+    while (!mbar_try_wait(bar, parity)) {
+        if (clock64() - t0 > budget) return false;
+    }
+    return true;
+}
+
+/* bulk copy global -> this CTA's shared memory, completing on `bar` */
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes,
+                                         uint64_t *bar) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
+        : "memory");
+}
+
+/* same, with an L2 eviction-priority policy (evict_first for streams that
+ * are read once per sweep, so that reused vectors stay resident) */
+__device__ __forceinline__ uint64_t policy_evict_first() {
+    uint64_t pol;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(pol));
+    return pol;
+}
+
+__device__ __forceinline__ void bulk_g2s_hint(void *dst, const void *src, uint32_t bytes,
+                                              uint64_t *bar, uint64_t pol) {
+    asm volatile(
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1], %2, [%3], %4;" ::"r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar)), "l"(pol)
+        : "memory");
+}
+
+}  // namespace tbs
+
+#endif /* TBS_TMA_CUH */

@@ -1,0 +1,344 @@
+"""Python mirror of the reference's host interface for the LIJ path.
+
+``Platform``, ``Mesh`` and ``Jacobian`` keep the member and method names of
+the reference's C++ classes (include/Platform.hxx:25-93,
+include/Mesh.hxx:27-67, include/Jacobian.hxx:43-98); ``Solver`` is the
+device phase of src/main.cxx:180-229 (factor, sweeps, report) over the
+C ABI.  Arrays are numpy, 0-based, column-major 9x9 blocks as in the files.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _native as N
+
+
+class Platform:
+    """Device selection (src/Platform.cxx:11-78).  Only compute_mode 2 (CUDA)."""
+
+    def __init__(self, compute_mode: int = N.CUDA_MODE, device_id: int = 0):
+        if compute_mode != N.CUDA_MODE:
+            raise N.TbsError(N.TBS_ERR_UNSUPPORTED,
+                             f"compute_mode {compute_mode} is not available: this build runs "
+                             "only on CUDA (mode 2)")
+        self.compute_mode = compute_mode
+        self.device_id = device_id
+        h = C.c_void_p()
+        N.check(N.lib.tbs_create(device_id, C.byref(h)))
+        self.ctx = h
+
+    def memoryAllocated(self) -> int:
+        b = C.c_size_t()
+        N.check(N.lib.tbs_memory_allocated(self.ctx, C.byref(b)), self.ctx)
+        return b.value
+
+    def close(self):
+        if self.ctx:
+            N.lib.tbs_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Mesh:
+    """Line mesh (include/Mesh.hxx:27-67)."""
+
+    FIELDS = ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface")
+
+    def __init__(self):
+        self.nvar = self.nelem = self.nintface = self.eftot = 0
+        self.nline = self.nlineelem = self.max_line_nelem = 0
+        for f in self.FIELDS:
+            setattr(self, f, np.zeros(0, np.int32))
+        self._gpu = None
+
+    # ------------------------------------------------------------ construction
+    def _alloc(self, hdr):
+        (self.nvar, self.nelem, self.nintface, self.eftot,
+         self.nline, self.nlineelem) = (int(v) for v in hdr)
+        self.epoint = np.zeros(self.nelem + 1, np.int32)
+        self.ef = np.zeros(self.eftot, np.int32)
+        self.fc = np.zeros(2 * self.nintface, np.int32)
+        self.linesize = np.zeros(self.nline, np.int32)
+        self.linepoint = np.zeros(self.nline + 1, np.int32)
+        self.lines = np.zeros(self.nlineelem, np.int32)
+        self.lineface = np.zeros(self.nlineelem, np.int32)
+
+    def _finish(self):
+        self.max_line_nelem = int(self.linesize.max()) if self.nline else 0
+        self.nbytes = sum(getattr(self, f).size for f in self.FIELDS)
+
+    @property
+    def header(self) -> np.ndarray:
+        return np.array([self.nvar, self.nelem, self.nintface, self.eftot, self.nline,
+                         self.nlineelem], np.int32)
+
+    def _arrays(self):
+        return [N.iptr(getattr(self, f)) for f in self.FIELDS]
+
+    def fromFile(self, path: str = "gpuline.mesh.data.bin") -> bool:
+        """src/Mesh.cxx:11-73 (raises instead of exit(1))."""
+        hdr = np.zeros(6, np.int32)
+        N.check(N.lib.tbs_read_mesh_header(path.encode(), N.iptr(hdr)))
+        self._alloc(hdr)
+        N.check(N.lib.tbs_read_mesh(path.encode(), N.iptr(hdr), *self._arrays()))
+        self._finish()
+        return True
+
+    @classmethod
+    def from_file(cls, path: str = "gpuline.mesh.data.bin") -> "Mesh":
+        m = cls()
+        m.fromFile(path)
+        return m
+
+    @classmethod
+    def structured(cls, L: int, K: int, nvar: int = 9) -> "Mesh":
+        """L lines of K cells in the numbering of the reference's data sets."""
+        m = cls()
+        hdr = np.zeros(6, np.int32)
+        N.check(N.lib.tbs_gen_structured_header(L, K, nvar, N.iptr(hdr)))
+        m._alloc(hdr)
+        N.check(N.lib.tbs_gen_structured_mesh(L, K, *m._arrays()))
+        m._finish()
+        return m
+
+    @classmethod
+    def from_arrays(cls, nvar, **arrays) -> "Mesh":
+        m = cls()
+        for f in cls.FIELDS:
+            setattr(m, f, np.ascontiguousarray(arrays[f], np.int32))
+        m.nvar = int(nvar)
+        m.nelem = m.epoint.size - 1
+        m.nintface = m.fc.size // 2
+        m.eftot = m.ef.size
+        m.nline = m.linesize.size
+        m.nlineelem = m.lines.size
+        m._finish()
+        return m
+
+    def toFile(self, path: str) -> None:
+        hdr = self.header
+        N.check(N.lib.tbs_write_mesh(path.encode(), N.iptr(hdr), *self._arrays()))
+
+    def validate(self) -> None:
+        hdr = self.header
+        N.check(N.lib.tbs_validate_mesh(N.iptr(hdr), *self._arrays()))
+
+    # ------------------------------------------------------------------ device
+    def setupDevice(self, gpu: Platform) -> None:
+        self._gpu = gpu
+
+    def toDevice(self) -> None:
+        g = self._gpu
+        N.check(N.lib.tbs_set_mesh(g.ctx, self.nvar, self.nelem, self.nintface, self.eftot,
+                                   self.nline, self.nlineelem, *self._arrays()), g.ctx)
+
+    def fromDevice(self) -> None:
+        """The mesh is never modified on the device."""
+
+
+class Jacobian:
+    """Block Jacobian and vectors (include/Jacobian.hxx:43-98)."""
+
+    def __init__(self):
+        self.nvar = self.nelem = self.nintface = 0
+        self._gpu = None
+
+    def _alloc(self, nvar, nelem, nintface, nlineelem):
+        self.nvar, self.nelem, self.nintface = int(nvar), int(nelem), int(nintface)
+        nb = self.nvar * self.nvar
+        self.jacD = np.zeros(nb * nelem)
+        self.jacDLU = np.zeros(nb * nelem)
+        self.jacO1 = np.zeros(nb * nintface)
+        self.jacO2 = np.zeros(nb * nintface)
+        self.rhs = np.zeros(self.nvar * nelem)
+        self.U0 = np.zeros(self.nvar * nelem)
+        self.U = np.zeros(self.nvar * nelem)
+        self.dU = np.zeros(self.nvar * nelem)
+        self.res = np.zeros(self.nvar * nelem)
+        self.DinvC = np.zeros(nb * nelem)
+        self.A = np.zeros(nb * nlineelem)
+
+    def fromFile(self, nlineelem: int, path: str = "gpuline.jacobian.data.bin") -> bool:
+        """src/Jacobian.cxx:11-74."""
+        hdr = np.zeros(3, np.int32)
+        N.check(N.lib.tbs_read_jacobian_header(path.encode(), N.iptr(hdr)))
+        self._alloc(hdr[0], hdr[1], hdr[2], nlineelem)
+        N.check(N.lib.tbs_read_jacobian(path.encode(), N.iptr(hdr), N.dptr(self.jacD),
+                                        N.dptr(self.jacO1), N.dptr(self.jacO2), N.dptr(self.rhs),
+                                        N.dptr(self.U0)))
+        return True
+
+    @classmethod
+    def generate(cls, mesh: Mesh, shift: float = 9.0, seed: int = 1) -> "Jacobian":
+        """Seeded synthetic values: jacD = U(-1,1) + shift I, O = 0.1 U(-1,1), rhs = U(-1,1)."""
+        j = cls()
+        j._alloc(mesh.nvar, mesh.nelem, mesh.nintface, mesh.nlineelem)
+        N.check(N.lib.tbs_gen_jacobian(mesh.nvar, mesh.nelem, mesh.nintface, float(shift),
+                                       int(seed), N.dptr(j.jacD), N.dptr(j.jacO1),
+                                       N.dptr(j.jacO2), N.dptr(j.rhs), N.dptr(j.U0)))
+        return j
+
+    def toFile(self, path: str) -> None:
+        hdr = np.array([self.nvar, self.nelem, self.nintface], np.int32)
+        N.check(N.lib.tbs_write_jacobian(path.encode(), N.iptr(hdr), N.dptr(self.jacD),
+                                         N.dptr(self.jacO1), N.dptr(self.jacO2),
+                                         N.dptr(self.rhs), N.dptr(self.U0)))
+
+    def assembleTriBlocks(self, mesh: Mesh) -> None:
+        """src/Jacobian.cxx:76-117: A[e] = in-line lower block of row e."""
+        nb = self.nvar * self.nvar
+        if self.A.size < nb * mesh.nelem:
+            self.A = np.zeros(nb * mesh.nelem)
+        O1 = self.jacO1.reshape(-1, nb)
+        O2 = self.jacO2.reshape(-1, nb)
+        A = self.A.reshape(-1, nb)
+        for l in range(mesh.nline):
+            for k in range(1, int(mesh.linesize[l])):
+                m = int(mesh.linepoint[l]) + k
+                f = int(mesh.lineface[m])
+                e = int(mesh.lines[m])
+                A[e] = O2[f] if e == mesh.fc[2 * f] else O1[f]
+
+    def resizeBlockSize(self, nvar_new: int) -> None:
+        """src/Jacobian.cxx:153-238 (same resulting arrays)."""
+        if nvar_new == self.nvar:
+            return
+        nb = nvar_new * nvar_new
+        D = np.zeros(nb * self.nelem)
+        O1 = np.zeros(nb * self.nintface)
+        O2 = np.zeros(nb * self.nintface)
+        r = np.zeros(nvar_new * self.nelem)
+        u0 = np.zeros(nvar_new * self.nelem)
+        N.check(N.lib.tbs_resize_block_size(self.nvar, nvar_new, self.nelem, self.nintface,
+                                            N.dptr(self.jacD), N.dptr(self.jacO1),
+                                            N.dptr(self.jacO2), N.dptr(self.rhs),
+                                            N.dptr(self.U0), N.dptr(D), N.dptr(O1), N.dptr(O2),
+                                            N.dptr(r), N.dptr(u0)))
+        self.nvar = nvar_new
+        self.jacD, self.jacO1, self.jacO2, self.rhs, self.U0 = D, O1, O2, r, u0
+        self.U = np.zeros(nvar_new * self.nelem)
+        self.dU = np.zeros(nvar_new * self.nelem)
+        self.res = np.zeros(nvar_new * self.nelem)
+        self.jacDLU = np.zeros(nb * self.nelem)
+        self.A = np.zeros(nb * self.nelem)
+
+    def setupDevice(self, gpu: Platform) -> None:
+        self._gpu = gpu
+
+    def toDevice(self) -> None:
+        g = self._gpu
+        N.check(N.lib.tbs_set_jacobian(g.ctx, N.dptr(self.jacD), N.dptr(self.jacO1),
+                                       N.dptr(self.jacO2), N.dptr(self.rhs), N.dptr(self.U0)),
+                g.ctx)
+
+    def fromDevice(self) -> None:
+        g = self._gpu
+        N.check(N.lib.tbs_get_solution(g.ctx, N.dptr(self.U)), g.ctx)
+        N.check(N.lib.tbs_get_residual(g.ctx, N.dptr(self.res)), g.ctx)
+        N.check(N.lib.tbs_get_update(g.ctx, N.dptr(self.dU)), g.ctx)
+
+
+class Solver:
+    """One device context: upload, factor, sweep, solve, read back."""
+
+    def __init__(self, device_id: int = 0, platform: Platform | None = None):
+        self.platform = platform or Platform(N.CUDA_MODE, device_id)
+        self.ctx = self.platform.ctx
+        self.nvar = self.nelem = 0
+
+    def _chk(self, rc):
+        N.check(rc, self.ctx)
+
+    def set_stream(self, stream_handle: int | None):
+        self._chk(N.lib.tbs_set_stream(self.ctx, stream_handle))
+
+    def set_mesh(self, mesh: Mesh):
+        mesh.setupDevice(self.platform)
+        mesh.toDevice()
+        self.nvar, self.nelem = mesh.nvar, mesh.nelem
+
+    def set_jacobian(self, jac: Jacobian):
+        jac.setupDevice(self.platform)
+        jac.toDevice()
+
+    def set_jacobian_arrays(self, jacD, jacO1, jacO2, rhs):
+        self._chk(N.lib.tbs_set_jacobian(self.ctx, N.dptr(jacD), N.dptr(jacO1), N.dptr(jacO2),
+                                         N.dptr(rhs), None))
+
+    def set_jacobian_device(self, d_jacD: int, d_jacO1: int, d_jacO2: int, d_rhs: int):
+        self._chk(N.lib.tbs_set_jacobian_device(self.ctx, d_jacD, d_jacO1, d_jacO2, d_rhs))
+
+    def set_rhs(self, rhs: np.ndarray):
+        self._chk(N.lib.tbs_set_rhs(self.ctx, N.dptr(np.ascontiguousarray(rhs, np.float64))))
+
+    def set_initial(self, U: np.ndarray | None):
+        self._chk(N.lib.tbs_set_initial(
+            self.ctx, None if U is None else N.dptr(np.ascontiguousarray(U, np.float64))))
+
+    def set_inner_sweeps(self, m: int):
+        self._chk(N.lib.tbs_set_inner_sweeps(self.ctx, m))
+
+    def factor(self, algo: int = N.ALGO_FP64):
+        self._chk(N.lib.tbs_factor(self.ctx, algo))
+
+    def sweep(self, n: int) -> np.ndarray:
+        h = np.zeros(n + 1)
+        self._chk(N.lib.tbs_sweep(self.ctx, n, N.dptr(h)))
+        return h
+
+    def solve(self, rel_tol: float, max_sweeps: int = 1000):
+        h = np.zeros(max_sweeps + 1)
+        s = C.c_int()
+        self._chk(N.lib.tbs_solve(self.ctx, rel_tol, max_sweeps, C.byref(s), N.dptr(h)))
+        return s.value, h[: s.value + 1]
+
+    def _vec(self, fn):
+        out = np.zeros(self.nvar * self.nelem)
+        self._chk(fn(self.ctx, N.dptr(out)))
+        return out
+
+    def solution(self) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_solution)
+
+    def residual(self) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_residual)
+
+    def update(self) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_update)
+
+    def true_residual_norm(self) -> float:
+        v = C.c_double()
+        self._chk(N.lib.tbs_true_residual_norm(self.ctx, C.byref(v)))
+        return v.value
+
+    def profile(self, on: bool = True):
+        self._chk(N.lib.tbs_profile_enable(self.ctx, 1 if on else 0))
+
+    def profile_reset(self):
+        self._chk(N.lib.tbs_profile_reset(self.ctx))
+
+    def profile_read(self) -> dict:
+        n = C.c_int(16)
+        names = (C.c_char_p * 16)()
+        launches = (C.c_longlong * 16)()
+        ms = (C.c_double * 16)()
+        self._chk(N.lib.tbs_profile_read(self.ctx, C.byref(n), names, launches, ms))
+        return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(n.value)}
+
+    def kernel_bytes(self, name: str) -> float:
+        v = C.c_double()
+        self._chk(N.lib.tbs_kernel_bytes(self.ctx, name.encode(), C.byref(v)))
+        return v.value
+
+    def memory_allocated(self) -> int:
+        return self.platform.memoryAllocated()
+
+    def close(self):
+        self.platform.close()
