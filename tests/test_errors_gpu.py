@@ -28,7 +28,7 @@ def test_zero_pivot_reports_numeric_error(algo):
     mesh = Mesh.structured(4, 6)
     jac = Jacobian.generate(mesh, 9.0, 1)
     bad = jac.jacD.copy()
-    bad[81 * 5: 81 * 6] = 0.0  # a zero diagonal block
+    bad[81 * 6: 81 * 7] = 0.0  # zero diagonal block of the first cell of line 1 (D' = D)
     s.set_mesh(mesh)
     s.set_jacobian_arrays(bad, jac.jacO1, jac.jacO2, jac.rhs)
     with pytest.raises(TbsError) as e:

@@ -681,6 +681,7 @@ static int run_factor(tbs_ctx *ctx, int algo) {
         return TBS_OK;
     }
     const FastLayout &L = ctx->L;
+    CKL(fast_prepare(L));
     RUN("permute", launch_permute_to_pos(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_rhs, ctx->d_rhsp));
     if (algo == TBS_ALGO_FP64) {
         RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,

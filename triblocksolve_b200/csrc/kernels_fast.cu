@@ -538,7 +538,6 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
     const int nxa = L.nx > 0 ? L.nx : 1;
     const size_t smem = 128 + RES_STAGES * (size_t)resid_stage_bytes<T>(L.nx) +
                         (size_t)RES_TILE * nxa * NV * sizeof(T) + RES_TILE * NV * sizeof(T);
-    if (smem > 227 * 1024) return (int)cudaErrorInvalidConfiguration;
     if (mode == 1 && L.nx == 0) mode = 2; /* no cross-line couplings: R = 0 */
     if (mode == 2) {
         /* a mesh that is a single line: the line solve is exact, R_new = 0 */
@@ -774,19 +773,43 @@ template int launch_fast_thomas<float>(cudaStream_t, const FastLayout &, const f
                                        const float *, const float *, float *, float *, float *,
                                        unsigned *, int);
 
-/* Opt the streaming kernels into the large shared-memory carve-out on the
- * current device (called once per context after cudaSetDevice). */
-int fast_kernels_init() {
-    cudaFuncSetAttribute(fast_resid_kernel<double>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         227 * 1024);
-    cudaFuncSetAttribute(fast_resid_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                         227 * 1024);
-    cudaFuncSetAttribute(fast_thomas_kernel<double, THOMAS_P>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    cudaFuncSetAttribute(fast_thomas_kernel<float, THOMAS_P>,
-                         cudaFuncAttributeMaxDynamicSharedMemorySize, 227 * 1024);
-    return (int)cudaGetLastError();
+/* Shared memory the streaming kernels need for a layout. */
+template <typename T>
+static size_t resid_smem(const FastLayout &L) {
+    const int nxa = L.nx > 0 ? L.nx : 1;
+    return 128 + RES_STAGES * (size_t)resid_stage_bytes<T>(L.nx) +
+           (size_t)RES_TILE * nxa * NV * sizeof(T) + RES_TILE * NV * sizeof(T);
 }
+
+static int smem_limit(const void *fn) {
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    cudaFuncAttributes fa{};
+    cudaFuncGetAttributes(&fa, fn);
+    return optin - (int)fa.sharedSizeBytes;
+}
+
+template <typename T>
+static int set_smem(const void *fn, size_t need) {
+    if ((long long)need > smem_limit(fn)) return (int)cudaErrorInvalidConfiguration;
+    if (need <= 48 * 1024) return 0;
+    return (int)cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
+
+/* Called before any launch (and outside stream capture) once the layout is
+ * known: opts the streaming kernels into the shared memory they need. */
+int fast_prepare(const FastLayout &L) {
+    int rc = set_smem<double>((const void *)fast_resid_kernel<double>, resid_smem<double>(L));
+    if (!rc) rc = set_smem<float>((const void *)fast_resid_kernel<float>, resid_smem<float>(L));
+    const size_t t64 = 128 + thomas_stages(L.nline, thomas_stage_bytes<double>()) * (size_t)thomas_stage_bytes<double>();
+    const size_t t32 = 128 + thomas_stages(L.nline, thomas_stage_bytes<float>()) * (size_t)thomas_stage_bytes<float>();
+    if (!rc) rc = set_smem<double>((const void *)fast_thomas_kernel<double, THOMAS_P>, t64);
+    if (!rc) rc = set_smem<float>((const void *)fast_thomas_kernel<float, THOMAS_P>, t32);
+    return rc;
+}
+
+int fast_kernels_init() { return 0; }
 
 /* ============================================ true residual, any ordering
  * R(pos(e)) = rhs(e) + D_e U(pos(e)) + sum_{faces} offJ U(pos(nbr)) with the

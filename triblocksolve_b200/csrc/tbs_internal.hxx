@@ -140,6 +140,7 @@ template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
                        const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
 int fast_kernels_init();
+int fast_prepare(const FastLayout &L);
 int full_resid_blocks(int nelem);
 template <typename T>
 int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *ef, const int *fc,
