@@ -18,6 +18,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstddef>
 #include <cstring>
 #include <new>
 #include <string>
@@ -76,13 +77,13 @@ struct tbs_ctx {
     /* ---- norms / solve state ---- */
     double *d_partials = nullptr, *d_partials2 = nullptr;
     int npart_cap = 0;
-    int npart_cur = 0; /* partials produced by the residual of the current state */
     SolveState *d_state = nullptr;
     SolveState *h_state = nullptr; /* pinned */
     double *d_hist = nullptr;
     int hist_cap = 0;
     unsigned *d_status = nullptr;
     unsigned *h_status = nullptr; /* pinned */
+    unsigned *d_counter = nullptr; /* last-CTA ticket of the fused norm */
     int algo = -1;
 
     /* ---- graph cache ---- */
@@ -212,6 +213,7 @@ static void drop_mesh(tbs_ctx *ctx) {
     for (auto p : ips) *p = nullptr;
     ctx->d_state = nullptr;
     ctx->d_status = nullptr;
+    ctx->d_counter = nullptr;
     ctx->npart_cap = 0;
     ctx->hist_cap = 0;
     ctx->have_mesh = ctx->have_jac = ctx->factored = false;
@@ -342,8 +344,8 @@ static int build_layout(tbs_ctx *ctx) {
     std::vector<int> xsrc((size_t)np16 * std::max(nx, 1), -1), xnbr((size_t)np16 * std::max(nx, 1), -1);
     for (int p = 0; p < np16; ++p)
         for (size_t q = 0; q < xs[p].size(); ++q) {
-            xsrc[(size_t)p * nx + q] = xs[p][q].first;
-            xnbr[(size_t)p * nx + q] = xs[p][q].second;
+            xsrc[q * (size_t)np16 + p] = xs[p][q].first;
+            xnbr[q * (size_t)np16 + p] = xs[p][q].second;
         }
     FastLayout &L = ctx->L;
     L.nv = ctx->nvar;
@@ -385,6 +387,7 @@ static int status_check(tbs_ctx *ctx) {
     const unsigned s = *ctx->h_status;
     if (s) {
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+        if (ctx->d_counter) CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream));
         if (s & ST_PIVOT)
             return ctx_fail(ctx, TBS_ERR_NUMERIC,
                             "zero or non-finite pivot in the no-pivot block factorization");
@@ -397,77 +400,96 @@ static int status_check(tbs_ctx *ctx) {
 
 static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; }
 
-/* Bring the state to "U = U_init, residual of U known": the partials of
- * ||R_0|| are in d_partials and the first sweep's inputs are ready. */
-static int prime(tbs_ctx *ctx) {
+/* How a sequence ends: the norm of its residual is recorded as the start
+ * of a solve (is_start) or as one more sweep, and, inside the solve graph,
+ * sets the while-node's condition. */
+struct CondCtl {
+    unsigned long long handle;
+    int use_cond;
+};
+
+static NormSink sink(tbs_ctx *ctx, int is_start, CondCtl cc) {
+    NormSink ns{};
+    ns.partials = ctx->d_partials;
+    ns.counter = ctx->d_counter;
+    ns.state = ctx->d_state;
+    ns.hist = ctx->d_hist;
+    ns.is_start = is_start;
+    ns.use_cond = cc.use_cond;
+    ns.handle = cc.handle;
+    return ns;
+}
+
+static NormSink no_sink() { return NormSink{}; }
+
+static int reduce(tbs_ctx *ctx, int npart, int is_start, CondCtl cc) {
+    RUN("reduce_norm", launch_reduce_norm(ctx->stream, ctx->d_partials, npart, ctx->d_state,
+                                          ctx->d_hist, is_start, cc.handle, cc.use_cond));
+    return TBS_OK;
+}
+
+/* Bring the state to "U = U_init, residual of U known and recorded as
+ * ||R_0||", with the first sweep's inputs ready. */
+static int prime(tbs_ctx *ctx, CondCtl cc) {
     cudaStream_t st = ctx->stream;
     const int nv = ctx->nvar, ne = ctx->nelem;
     const size_t vb = (size_t)nvec(ctx) * sizeof(double);
     if (ctx->algo == TBS_ALGO_REFERENCE) {
+        int np = 0;
+        CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
         if (ctx->d_Uinit) {
             CK(cudaMemcpyAsync(ctx->d_U, ctx->d_Uinit, vb, cudaMemcpyDeviceToDevice, st));
-            CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
-            int np = 0;
             RUN("ref_line_res", launch_ref_line_res(st, nv, ctx->nline, ne, ctx->d_epoint, ctx->d_ef,
                                                     ctx->d_fc, ctx->d_linesize, ctx->d_linepoint,
                                                     ctx->d_lines, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                     ctx->d_U, ctx->d_R, ctx->d_partials, &np));
-            ctx->npart_cur = np;
         } else {
             CK(cudaMemsetAsync(ctx->d_U, 0, vb, st));
-            CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
-            const int np = ref_line_res_partials(ne);
+            np = ref_line_res_partials(ne);
             RUN("norm_partials", launch_norm_partials(st, ctx->d_R, nvec(ctx), ctx->d_partials, np));
-            ctx->npart_cur = np;
         }
         CK(cudaMemsetAsync(ctx->d_dU, 0, vb, st));
-        return TBS_OK;
+        return reduce(ctx, np, 1, cc);
     }
     const FastLayout &L = ctx->L;
     const size_t pb = (size_t)L.np16 * 9 * sizeof(double);
-    const int np = fast_resid_grid(L.np16);
     if (ctx->algo == TBS_ALGO_FP64) {
+        const double *Rsrc = ctx->d_rhsp;
         if (ctx->d_Uinit) {
             RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
             RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                         L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
                                                         ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
                                                         ctx->d_partials2));
-            RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
-                                                        ctx->d_Rp, ctx->d_b, ctx->d_partials, np,
-                                                        ctx->d_status));
+            Rsrc = ctx->d_Rp;
         } else {
             CK(cudaMemsetAsync(ctx->d_Up, 0, pb, st));
-            RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
-                                                        ctx->d_rhsp, ctx->d_b, ctx->d_partials, np,
-                                                        ctx->d_status));
         }
-        ctx->npart_cur = np;
+        RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
+                                                        Rsrc, ctx->d_b, sink(ctx, 1, cc),
+                                                        ctx->d_status));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED */
-    const int nfb = full_resid_blocks(ne);
     if (ctx->d_Uinit) {
         RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
         RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                    L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                    ctx->d_rhs, ctx->d_Up, ctx->d_R32,
                                                    ctx->d_partials));
-        ctx->npart_cur = nfb;
-    } else {
-        CK(cudaMemsetAsync(ctx->d_Up, 0, pb, st));
-        RUN("cast", launch_cast_f64_f32(st, ctx->d_rhsp, ctx->d_R32, (long long)L.np16 * 9));
-        const int npn = ref_line_res_partials(ne);
-        RUN("norm_partials", launch_norm_partials(st, ctx->d_rhsp, (long long)L.np16 * 9,
-                                                  ctx->d_partials, npn));
-        ctx->npart_cur = npn;
+        return reduce(ctx, full_resid_blocks(ne), 1, cc);
     }
-    return TBS_OK;
+    CK(cudaMemsetAsync(ctx->d_Up, 0, pb, st));
+    RUN("cast", launch_cast_f64_f32(st, ctx->d_rhsp, ctx->d_R32, (long long)L.np16 * 9));
+    const int npn = ref_line_res_partials(ne);
+    RUN("norm_partials", launch_norm_partials(st, ctx->d_rhsp, (long long)L.np16 * 9,
+                                              ctx->d_partials, npn));
+    return reduce(ctx, npn, 1, cc);
 }
 
-/* one sweep from the primed state; leaves the new residual's partials in
- * d_partials (npart_cur entries) */
-static int body(tbs_ctx *ctx) {
+/* One sweep from the primed state, ending with the new residual's norm
+ * recorded as one more sweep. */
+static int body(tbs_ctx *ctx, CondCtl cc) {
     cudaStream_t st = ctx->stream;
     const int nv = ctx->nvar, ne = ctx->nelem;
     if (ctx->algo == TBS_ALGO_REFERENCE) {
@@ -480,40 +502,35 @@ static int body(tbs_ctx *ctx) {
                                                 ctx->d_fc, ctx->d_linesize, ctx->d_linepoint,
                                                 ctx->d_lines, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                 ctx->d_U, ctx->d_R, ctx->d_partials, &np));
-        ctx->npart_cur = np;
-        return TBS_OK;
+        return reduce(ctx, np, 0, cc);
     }
     const FastLayout &L = ctx->L;
-    const int np = fast_resid_grid(L.np16);
     if (ctx->algo == TBS_ALGO_FP64) {
         RUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
                                                       ctx->d_dUp, ctx->d_Up, ctx->d_status, 1));
         RUN("fast_resid", launch_fast_resid<double>(st, L, 1, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
-                                                    ctx->d_Rp, ctx->d_b, ctx->d_partials, np,
+                                                    nullptr, ctx->d_b, sink(ctx, 0, cc),
                                                     ctx->d_status));
-        ctx->npart_cur = np;
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
      * FP64 residual R = rhs + J U from the original blocks */
     RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
-                                                 ctx->d_R32, ctx->d_b32, ctx->d_partials2, np,
-                                                 ctx->d_status));
+                                                     ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status));
     for (int m = 0; m < ctx->inner_sweeps; ++m) {
         RUN("fast_thomas32", launch_fast_thomas<float>(st, L, ctx->d_G32, ctx->d_Gam32, ctx->d_b32,
                                                        ctx->d_y32, ctx->d_d32, ctx->d_c32,
                                                        ctx->d_status, m > 0 ? 1 : 0));
         if (m + 1 < ctx->inner_sweeps)
             RUN("fast_resid32", launch_fast_resid<float>(st, L, 1, ctx->d_Dinv32, ctx->d_X32,
-                                                         ctx->d_d32, ctx->d_R32, ctx->d_b32,
-                                                         ctx->d_partials2, np, ctx->d_status));
+                                                         ctx->d_d32, nullptr, ctx->d_b32, no_sink(),
+                                                         ctx->d_status));
     }
     RUN("axpy", launch_axpy_f32_f64(st, ctx->d_c32, ctx->d_Up, (long long)L.np16 * 9));
     RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                ctx->d_rhs, ctx->d_Up, ctx->d_R32, ctx->d_partials));
-    ctx->npart_cur = full_resid_blocks(ne);
-    return TBS_OK;
+    return reduce(ctx, full_resid_blocks(ne), 0, cc);
 }
 
 static int ensure_hist(tbs_ctx *ctx, int need) {
@@ -526,13 +543,17 @@ static int ensure_hist(tbs_ctx *ctx, int need) {
     return TBS_OK;
 }
 
+/* write the control block of the device SolveState (tol, max_sweeps,
+ * hist_cap), leaving the recorded norms alone */
 static int set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
-    std::memset(ctx->h_state, 0, sizeof(SolveState));
-    ctx->h_state->tol = tol;
-    ctx->h_state->max_sweeps = max_sweeps;
-    ctx->h_state->hist_cap = ctx->hist_cap;
-    CK(cudaMemcpyAsync(ctx->d_state, ctx->h_state, sizeof(SolveState), cudaMemcpyHostToDevice,
-                       ctx->stream));
+    SolveState *h = ctx->h_state;
+    h->tol = tol;
+    h->max_sweeps = max_sweeps;
+    h->hist_cap = ctx->hist_cap;
+    const size_t off = offsetof(SolveState, tol);
+    CK(cudaMemcpyAsync(reinterpret_cast<char *>(ctx->d_state) + off,
+                       reinterpret_cast<char *>(h) + off, sizeof(SolveState) - off,
+                       cudaMemcpyHostToDevice, ctx->stream));
     return TBS_OK;
 }
 
@@ -543,7 +564,7 @@ static int read_state(tbs_ctx *ctx) {
     return TBS_OK;
 }
 
-/* Graph: prime -> reduce(start) -> while (cond) { sweep -> reduce }. */
+/* Graph: prime (records ||R_0||, sets the condition) -> while (cond) { sweep } */
 static int build_graph(tbs_ctx *ctx) {
     drop_graph(ctx);
     cudaStream_t st = ctx->stream;
@@ -552,13 +573,9 @@ static int build_graph(tbs_ctx *ctx) {
     ctx->graph = g;
     cudaGraphConditionalHandle h;
     CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    const CondCtl cc{(unsigned long long)h, 1};
     CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = prime(ctx);
-    if (rc == TBS_OK)
-        rc = launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state, ctx->d_hist, 1,
-                                (unsigned long long)h, 1)
-                 ? ctx_fail(ctx, TBS_ERR_CUDA, "reduce launch failed")
-                 : TBS_OK;
+    int rc = prime(ctx, cc);
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
@@ -590,12 +607,7 @@ static int build_graph(tbs_ctx *ctx) {
         return rc;
     }
     CK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = body(ctx);
-    if (rc == TBS_OK)
-        rc = launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state, ctx->d_hist, 0,
-                                (unsigned long long)h, 1)
-                 ? ctx_fail(ctx, TBS_ERR_CUDA, "reduce launch failed")
-                 : TBS_OK;
+    rc = body(ctx, cc);
     ee = cudaStreamEndCapture(st, &outg);
     if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
     if (rc != TBS_OK) {
@@ -621,6 +633,7 @@ static int alloc_algo(tbs_ctx *ctx, int algo) {
     DA(ctx->d_scratch, (size_t)nvec(ctx));
     const int npmax = std::max({ref_line_res_partials(ctx->nelem) * 8, fast_resid_grid(ctx->L.np16),
                                 full_resid_blocks(ctx->nelem), 1024});
+    DA(ctx->d_counter, 1);
     if (ctx->npart_cap < npmax) {
         dfree(ctx, &ctx->d_partials);
         dfree(ctx, &ctx->d_partials2);
@@ -889,7 +902,7 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
     ctx->factored = false;
     rc = run_factor(ctx, algo);
     if (rc) return rc;
-    rc = prime(ctx);
+    rc = prime(ctx, CondCtl{0, 0});
     if (rc) return rc;
     rc = status_check(ctx);
     if (rc) return rc;
@@ -910,7 +923,7 @@ int tbs_set_rhs(tbs_ctx *ctx, const double *rhs) {
         RUN("permute", launch_permute_to_pos(ctx->stream, 9, ctx->nelem, ctx->L.pos_of_elem, ctx->d_rhs,
                                              ctx->d_rhsp));
     }
-    return prime(ctx);
+    return prime(ctx, CondCtl{0, 0});
     GUARD_END
 }
 
@@ -927,7 +940,7 @@ int tbs_set_initial(tbs_ctx *ctx, const double *U) {
         dfree(ctx, &ctx->d_Uinit);
     }
     drop_graph(ctx);
-    return prime(ctx);
+    return prime(ctx, CondCtl{0, 0});
     GUARD_END
 }
 
@@ -942,13 +955,12 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
     rc = set_state(ctx, 0.0, n);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
-    RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
-                                          ctx->d_hist, 1, 0ull, 0));
+    /* the current residual norm (recorded by the last sequence) opens the history */
+    rc = reduce(ctx, 0, 1, CondCtl{0, 0});
+    if (rc) return rc;
     for (int s = 0; s < n; ++s) {
-        rc = body(ctx);
+        rc = body(ctx, CondCtl{0, 0});
         if (rc) return rc;
-        RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
-                                              ctx->d_hist, 0, 0ull, 0));
     }
     if (rnorm_out)
         CK(cudaMemcpyAsync(rnorm_out, ctx->d_hist, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
@@ -971,20 +983,16 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
     cudaStream_t st = ctx->stream;
     if (ctx->prof) {
         /* eager form with a host-side test, so that every kernel is timed */
-        rc = prime(ctx);
+        rc = prime(ctx, CondCtl{0, 0});
         if (rc) return rc;
-        RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
-                                              ctx->d_hist, 1, 0ull, 0));
         for (;;) {
             rc = read_state(ctx);
             if (rc) return rc;
             const SolveState &S = *ctx->h_state;
             const bool go = std::isfinite(S.last) && S.last > S.tol * S.norm0 && S.sweep < S.max_sweeps;
             if (!go) break;
-            rc = body(ctx);
+            rc = body(ctx, CondCtl{0, 0});
             if (rc) return rc;
-            RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials, ctx->npart_cur, ctx->d_state,
-                                                  ctx->d_hist, 0, 0ull, 0));
         }
         prof_resolve(ctx);
     } else {

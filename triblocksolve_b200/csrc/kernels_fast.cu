@@ -80,19 +80,21 @@ int launch_norm_partials(cudaStream_t st, const double *v, long long n, double *
 
 /* Sum the partials in a fixed order, record the norm and decide whether the
  * solve goes on.  The decision feeds the CUDA graph's while-node, so the
- * sweep loop never returns to the host. */
+ * sweep loop never returns to the host.  n == 0 re-records the latest norm
+ * (state->last) as the start of a new sweep sequence. */
 __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, SolveState *state,
                                    double *hist, int is_start,
                                    cudaGraphConditionalHandle handle, int use_cond) {
-    __shared__ double s[256];
+    __shared__ double red[8];
     double acc = 0.0;
     for (int t = threadIdx.x; t < n; t += 256) acc += partials[t];
-    s[threadIdx.x] = acc;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot = 0.0;
-        for (int t = 0; t < 256; ++t) tot += s[t];
-        const double nrm = sqrt(tot);
+        for (int w = 0; w < 8; ++w) tot += red[w];
+        const double nrm = n > 0 ? sqrt(tot) : state->last;
         if (is_start) {
             state->sweep = 0;
             state->norm0 = nrm;
@@ -198,8 +200,10 @@ int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n)
  *                        reference's LU has none: lineLU_v2.okl:17-27)
  *   G_k       = Dinv_k A_k
  * A/C are the two blocks of the in-line face joining cells k-1 and k,
- * picked as in lineLU_v2.okl:116-117.  The FP32 arrays, when given, are
- * the FP64 results rounded once. */
+ * picked as in lineLU_v2.okl:116-117.  Dinv is stored column-major like the
+ * input blocks; G and Gam row-major (entry (i,j) at 9i+j), the order the
+ * Thomas kernel reads them in.  The FP32 arrays, when given, are the FP64
+ * results rounded once. */
 __device__ __forceinline__ void gj_invert(double *W, int t, unsigned *status) {
     const int i = t % NV, j = t / NV;
 #pragma unroll 1
@@ -289,8 +293,8 @@ __global__ void __launch_bounds__(128) fast_factor_kernel(
 #pragma unroll
             for (int q = 0; q < NV; ++q) g += sPrev[i + NV * q] * sC[q + NV * j];
             sGam[t] = g;
-            if (Gam) Gam[(size_t)(p - 1) * NB + t] = g;
-            if (Gam32) Gam32[(size_t)(p - 1) * NB + t] = (float)g;
+            if (Gam) Gam[(size_t)(p - 1) * NB + NV * i + j] = g;
+            if (Gam32) Gam32[(size_t)(p - 1) * NB + NV * i + j] = (float)g;
         }
         __syncthreads();
         if (act) {
@@ -307,11 +311,11 @@ __global__ void __launch_bounds__(128) fast_factor_kernel(
             for (int q = 0; q < NV; ++q) gk += sW[i + NV * q] * sA[q + NV * j];
             const double w = sW[t];
             if (Dinv) {
-                G[(size_t)p * NB + t] = gk;
+                G[(size_t)p * NB + NV * i + j] = gk;
                 Dinv[(size_t)p * NB + t] = w;
             }
             if (Dinv32) {
-                G32[(size_t)p * NB + t] = (float)gk;
+                G32[(size_t)p * NB + NV * i + j] = (float)gk;
                 Dinv32[(size_t)p * NB + t] = (float)w;
             }
             sPrev[t] = w;
@@ -332,7 +336,8 @@ int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
     return (int)cudaGetLastError();
 }
 
-/* X[slot] = cross-line block of that slot, or zeros; one warp per slot */
+/* X[q] = cross-line block of slot q = s*np16 + p (slot-major), or zeros;
+ * one warp per slot */
 __global__ void fast_xlayout_kernel(long long nslots, const int *__restrict__ xsrc,
                                     const double *__restrict__ O1, const double *__restrict__ O2,
                                     double *__restrict__ X, float *__restrict__ X32) {
@@ -359,212 +364,219 @@ int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, 
 }
 
 /* ================================================ residual -> Thomas RHS
- * Persistent CTAs stream tiles of RES_TILE positions through a 3-stage
- * cp.async.bulk ring.  Per tile:
+ * One CTA per tile of RES_TILE positions (no persistent loop: ~6 CTAs per
+ * SM keep ~200 KB of bulk copies in flight).  Per tile:
  *   mode 0:  R = Rsrc (a residual already in position order)
  *   mode 1:  R = sum over slots X_slot dU[xnbr_slot]   (R_new = O dU)
- * then b = -Dinv R, and every CTA adds sum R^2 of its tiles into its own
- * partial (fixed order).  Thread (c,i), c < 16, i < 9, owns row i of cell c.
+ * then b = -Dinv R.  Thread t < 144 owns (cell c = t % 16, row i = t / 16):
+ * with blocks 81 doubles apart, the 16 cells of a half-warp hit 16
+ * distinct bank pairs, so the shared-memory reads are conflict-free.
+ * X and xnbr are slot-major ([slot][position]) for the same reason.
+ * Every CTA writes sum R^2 of its tile; the last CTA to finish (atomic
+ * ticket) adds the partials in a fixed order and, when asked, records the
+ * norm, the sweep count and the graph's loop condition.
  */
 constexpr int RES_THREADS_FAST = 160;
-constexpr int RES_STAGES = 3;
 
-int fast_resid_grid(int np16) {
-    int ntiles = np16 / RES_TILE;
-    int g = 2 * 148;
-    if (ntiles < g) g = ntiles;
-    return g < 1 ? 1 : g;
+int fast_resid_grid(int np16) { return np16 / RES_TILE > 0 ? np16 / RES_TILE : 1; }
+
+/* Fixed-order sum of the per-CTA partials by the last CTA; updates the
+ * solve state like reduce_norm_kernel.  Called by every thread of the
+ * block; `block_sum` is valid in thread 0. */
+__device__ void finalize_norm(const NormSink &ns, double block_sum) {
+    __shared__ unsigned ticket;
+    __shared__ double red[32];
+    if (!ns.partials) return;
+    if (threadIdx.x == 0) {
+        ns.partials[blockIdx.x] = block_sum;
+        __threadfence();
+        ticket = atomicAdd(ns.counter, 1u);
+    }
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return;
+    if (!ns.state) {
+        if (threadIdx.x == 0) *ns.counter = 0u;
+        return;
+    }
+    __threadfence();
+    double acc = 0.0;
+    for (unsigned t = threadIdx.x; t < gridDim.x; t += blockDim.x) acc += __ldcg(ns.partials + t);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
+        const double nrm = sqrt(tot);
+        SolveState *S = ns.state;
+        if (ns.is_start) {
+            S->sweep = 0;
+            S->norm0 = nrm;
+        } else {
+            S->sweep += 1;
+        }
+        const int sw = S->sweep;
+        if (sw < S->hist_cap) ns.hist[sw] = nrm;
+        S->last = nrm;
+        const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
+        if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
+        *ns.counter = 0u;
+    }
 }
 
 template <typename T>
-__host__ __device__ inline uint32_t resid_stage_bytes(int nx) {
-    return (uint32_t)(RES_TILE * NB * sizeof(T) + RES_TILE * nx * NB * sizeof(T) +
-                      RES_TILE * nx * sizeof(int) + RES_TILE * NV * sizeof(T));
+__host__ __device__ inline size_t resid_smem_bytes(int nx) {
+    const int nxa = nx > 0 ? nx : 1;
+    return 128 + (size_t)RES_TILE * NB * sizeof(T) * (1 + nx) +
+           (size_t)nxa * RES_TILE * NV * sizeof(T) + (size_t)RES_TILE * NV * sizeof(T) * 2;
 }
 
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
-    int ntiles, int nx, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
+    int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
-    T *__restrict__ b, double *__restrict__ partials, unsigned *status) {
+    T *__restrict__ b, NormSink ns, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    unsigned char *st0 = smem + 128;
-    const uint32_t szD = RES_TILE * NB * sizeof(T);
-    const uint32_t szX = RES_TILE * nx * NB * sizeof(T);
-    const uint32_t szN = RES_TILE * nx * sizeof(int);
-    const uint32_t szR = RES_TILE * NV * sizeof(T);
-    const uint32_t stage = szD + szX + szN + szR;
-    T *sg = reinterpret_cast<T *>(st0 + RES_STAGES * stage);
-    T *sr = sg + RES_TILE * (nx > 0 ? nx : 1) * NV;
-
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    T *sD = reinterpret_cast<T *>(smem + 128);
+    T *sX = sD + RES_TILE * NB;
+    const int nxa = nx > 0 ? nx : 1;
+    T *sg = sX + nx * RES_TILE * NB;
+    T *sr = sg + nxa * RES_TILE * NV;
+    T *sb = sr + RES_TILE * NV;
+    const int p0 = blockIdx.x * RES_TILE;
     const int tid = threadIdx.x;
-    const int c = tid / NV, i = tid - NV * (tid / NV);
+    const int c = tid % RES_TILE, i = tid / RES_TILE;
     const bool act = tid < RES_TILE * NV;
+    const uint32_t szD = RES_TILE * NB * sizeof(T), szR = RES_TILE * NV * sizeof(T);
 
     if (tid == 0) {
-        for (int s = 0; s < RES_STAGES; ++s) mbar_init(&bars[s], 1);
+        mbar_init(bar, 1);
         mbar_fence_init();
     }
     __syncthreads();
-
-    uint64_t pol = 0;
-    if (tid == 0) pol = policy_evict_first();
-    auto issue = [&](int s, int tile) {
-        unsigned char *base = st0 + (size_t)s * stage;
-        if (mode == 0) {
-            mbar_arrive_expect_tx(&bars[s], szD + szR);
-            bulk_g2s_hint(base, Dinv + (size_t)tile * RES_TILE * NB, szD, &bars[s], pol);
-            bulk_g2s(base + szD + szX + szN, Rsrc + (size_t)tile * RES_TILE * NV, szR, &bars[s]);
-        } else {
-            mbar_arrive_expect_tx(&bars[s], szD + szX + szN);
-            bulk_g2s_hint(base, Dinv + (size_t)tile * RES_TILE * NB, szD, &bars[s], pol);
-            bulk_g2s_hint(base + szD, X + (size_t)tile * RES_TILE * nx * NB, szX, &bars[s], pol);
-            bulk_g2s(base + szD + szX, xnbr + (size_t)tile * RES_TILE * nx, szN, &bars[s]);
-        }
-    };
-    int issued[RES_STAGES] = {0}, used[RES_STAGES] = {0};
     if (tid == 0) {
-        for (int s = 0; s < RES_STAGES; ++s) {
-            const int tile = blockIdx.x + s * gridDim.x;
-            if (tile < ntiles) {
-                issue(s, tile);
-                issued[s]++;
-            }
-        }
-    }
-
-    double sq = 0.0;
-    int it = 0;
-    bool timed_out = false;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++it) {
-        const int s = it % RES_STAGES;
-        const uint32_t par = (uint32_t)((it / RES_STAGES) & 1);
-        const bool ok = mbar_wait(&bars[s], par);
-        if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
-        }
-        if (tid == 0) used[s]++;
-        const unsigned char *base = st0 + (size_t)s * stage;
-        const T *sD = reinterpret_cast<const T *>(base);
-        T r = T(0);
-        if (mode == 0) {
-            const T *sR = reinterpret_cast<const T *>(base + szD + szX + szN);
-            if (act) r = sR[c * NV + i];
+        const uint64_t pol = policy_evict_first();
+        const uint32_t bytes = szD + (mode == 1 ? nx * szD : szR);
+        mbar_arrive_expect_tx(bar, bytes);
+        bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+        if (mode == 1) {
+            for (int s = 0; s < nx; ++s)
+                bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
         } else {
-            const T *sX = reinterpret_cast<const T *>(base + szD);
-            const int *sN = reinterpret_cast<const int *>(base + szD + szX);
-            if (act) {
-                for (int q = 0; q < nx; ++q) {
-                    const int nb = sN[c * nx + q];
-                    sg[(c * nx + q) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
-                }
-            }
-            __syncthreads();
-            if (act) {
-                T a0 = T(0), a1 = T(0), a2 = T(0);
-                for (int q = 0; q < nx; ++q) {
-                    const T *xr = sX + (c * nx + q) * NB + i;
-                    const T *g = sg + (c * nx + q) * NV;
-                    a0 += xr[0] * g[0];
-                    a1 += xr[9] * g[1];
-                    a2 += xr[18] * g[2];
-                    a0 += xr[27] * g[3];
-                    a1 += xr[36] * g[4];
-                    a2 += xr[45] * g[5];
-                    a0 += xr[54] * g[6];
-                    a1 += xr[63] * g[7];
-                    a2 += xr[72] * g[8];
-                }
-                r = a0 + (a1 + a2);
-            }
-        }
-        if (act) {
-            sr[c * NV + i] = r;
-            sq += (double)r * (double)r;
-        }
-        __syncthreads();
-        if (act) {
-            const T *dr = sD + c * NB + i;
-            const T *rv = sr + c * NV;
-            T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
-            a0 += dr[27] * rv[3];
-            a1 += dr[36] * rv[4];
-            a2 += dr[45] * rv[5];
-            a0 += dr[54] * rv[6];
-            a1 += dr[63] * rv[7];
-            a2 += dr[72] * rv[8];
-            b[((size_t)tile * RES_TILE + c) * NV + i] = -(a0 + (a1 + a2));
-        }
-        __syncthreads();
-        if (tid == 0) {
-            const int next = tile + RES_STAGES * gridDim.x;
-            if (next < ntiles) {
-                issue(s, next);
-                issued[s]++;
-            }
+            bulk_g2s(sr, Rsrc + (size_t)p0 * NV, szR, bar);
         }
     }
-    if (timed_out) {
+    if (mode == 1 && act) {
+        /* neighbour dU gathers overlap the bulk copies */
+        for (int s = 0; s < nx; ++s) {
+            const int nb = xnbr[(size_t)s * np16 + p0 + c];
+            sg[(s * RES_TILE + c) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
+        }
+    }
+    const bool ok = mbar_wait(bar, 0);
+    if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             atomicOr(status, ST_TIMEOUT);
-            /* let copies still in flight land before the CTA retires */
-            for (int s = 0; s < RES_STAGES; ++s)
-                for (int u = used[s]; u < issued[s]; ++u)
-                    mbar_wait(&bars[s], (uint32_t)(u & 1), 1LL << 28);
+            mbar_wait(bar, 0, 1LL << 28); /* let the copies land before the CTA retires */
         }
         return;
     }
-    __shared__ double red[RES_THREADS_FAST / 32];
-    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
-    if ((tid & 31) == 0) red[tid >> 5] = sq;
+    T r = T(0);
+    if (mode == 1) {
+        if (act) {
+            T a0 = T(0), a1 = T(0), a2 = T(0);
+            for (int s = 0; s < nx; ++s) {
+                const T *xr = sX + (s * RES_TILE + c) * NB + i;
+                const T *g = sg + (s * RES_TILE + c) * NV;
+                a0 += xr[0] * g[0];
+                a1 += xr[9] * g[1];
+                a2 += xr[18] * g[2];
+                a0 += xr[27] * g[3];
+                a1 += xr[36] * g[4];
+                a2 += xr[45] * g[5];
+                a0 += xr[54] * g[6];
+                a1 += xr[63] * g[7];
+                a2 += xr[72] * g[8];
+            }
+            r = a0 + (a1 + a2);
+            sr[c * NV + i] = r;
+        }
+        __syncthreads();
+    } else if (act) {
+        r = sr[c * NV + i];
+    }
+    double sq = act ? (double)r * (double)r : 0.0;
+    if (act) {
+        const T *dr = sD + c * NB + i;
+        const T *rv = sr + c * NV;
+        T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
+        a0 += dr[27] * rv[3];
+        a1 += dr[36] * rv[4];
+        a2 += dr[45] * rv[5];
+        a0 += dr[54] * rv[6];
+        a1 += dr[63] * rv[7];
+        a2 += dr[72] * rv[8];
+        sb[c * NV + i] = -(a0 + (a1 + a2));
+    }
     __syncthreads();
-    if (tid == 0) {
+    if (act) b[(size_t)p0 * NV + tid] = sb[tid]; /* contiguous tile store */
+    if (ns.partials) {
+        __shared__ double red[RES_THREADS_FAST / 32];
+        for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+        if ((tid & 31) == 0) red[tid >> 5] = sq;
+        __syncthreads();
         double tot = 0.0;
-        for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
-        partials[blockIdx.x] = tot;
+        if (tid == 0)
+            for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
+        finalize_norm(ns, tot);
     }
 }
 
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv, const T *X,
-                      const T *dU, const T *Rsrc, T *b, double *partials, int npart,
-                      unsigned *status) {
+                      const T *dU, const T *Rsrc, T *b, const NormSink &ns, unsigned *status) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    const int ntiles = L.np16 / RES_TILE;
     const int grid = fast_resid_grid(L.np16);
-    if (npart != grid) return (int)cudaErrorInvalidValue;
-    const int nxa = L.nx > 0 ? L.nx : 1;
-    const size_t smem = 128 + RES_STAGES * (size_t)resid_stage_bytes<T>(L.nx) +
-                        (size_t)RES_TILE * nxa * NV * sizeof(T) + RES_TILE * NV * sizeof(T);
-    if (mode == 1 && L.nx == 0) mode = 2; /* no cross-line couplings: R = 0 */
-    if (mode == 2) {
-        /* a mesh that is a single line: the line solve is exact, R_new = 0 */
-        cudaMemsetAsync(b, 0, (size_t)L.np16 * NV * sizeof(T), st);
-        cudaMemsetAsync(partials, 0, (size_t)npart * sizeof(double), st);
-        return (int)cudaGetLastError();
+    if (mode == 1 && L.nx == 0) {
+        /* a mesh that is one line: the line solve is exact, R_new = 0 */
+        mode = 0;
+        Rsrc = nullptr;
     }
-    fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(ntiles, L.nx, mode, Dinv, X, L.xnbr,
-                                                               dU, Rsrc, b, partials, status);
+    if (mode == 0 && !Rsrc) {
+        cudaMemsetAsync(b, 0, (size_t)L.np16 * NV * sizeof(T), st);
+        /* still run the kernel so that the norm bookkeeping happens: a zero
+         * residual read from b itself */
+        Rsrc = b;
+    }
+    const size_t smem = resid_smem_bytes<T>(mode == 1 ? L.nx : 0);
+    fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(mode == 1 ? L.nx : 0, L.np16, mode,
+                                                               Dinv, X, L.xnbr, dU, Rsrc, b, ns,
+                                                               status);
     return (int)cudaGetLastError();
 }
 
 template int launch_fast_resid<double>(cudaStream_t, const FastLayout &, int, const double *,
                                        const double *, const double *, const double *, double *,
-                                       double *, int, unsigned *);
+                                       const NormSink &, unsigned *);
 template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, const float *,
                                       const float *, const float *, const float *, float *,
-                                      double *, int, unsigned *);
+                                      const NormSink &, unsigned *);
 
 /* =========================================================== line Thomas
  * One warp per line.  Lane 0 streams "jobs" through an NS-stage bulk-copy
  * ring: jobs 0..nch-1 are forward chunks (G and b of P cells), jobs
- * nch..2nch-1 backward chunks in reverse (Gam of P cells).  Lanes 0..8 own
- * rows; the 9-vector of the previous cell is replicated in every lane with
- * shuffles.  y (forward result) is written to global memory and read back
- * by the same lane in the backward pass; U and y loads of the next
- * backward chunk are issued one chunk ahead.
+ * nch..2nch-1 backward chunks in reverse (Gam of P cells).  G and Gam are
+ * stored row-major; lane i < 9 owns row i and holds the row of the NEXT
+ * cell in registers while the current cell's dot product runs, so that the
+ * critical path of a step is one shuffle broadcast plus five dependent
+ * FP64 operations (a shared-memory broadcast would need __syncwarp, whose
+ * memory ordering waits for the step's global stores).  A row starting at
+ * an odd double is read as single + four 16-byte pairs, one starting at an
+ * even double as four pairs + single; each lane gathers the vector from
+ * lanes 0..8 in the matching order.  The forward results y stay in shared
+ * memory when the line fits (YS), otherwise they go to global memory and
+ * come back one chunk ahead.
  *   accumulate = 0:  U = dU  (first sweep of a solve, U starts at 0)
  *   accumulate = 1:  U += dU
  */
@@ -575,7 +587,149 @@ __host__ __device__ inline uint32_t thomas_stage_bytes() {
     return (uint32_t)(THOMAS_P * (NB + NV) * sizeof(T));
 }
 
-template <typename T, int P>
+/* Lane constants for rows of parity odd (0/1 = parity of q): pair offset,
+ * single offset and the source lane of the first vector element. */
+struct LaneOff {
+    int row;     /* NV * i */
+    int rp[2];   /* first pair element */
+    int rs[2];   /* single element */
+    int par[2];  /* vector element order: y_{par+j} for j < 8, then the single */
+};
+
+__device__ __forceinline__ LaneOff lane_offsets(int i) {
+    LaneOff o;
+    o.row = NV * i;
+    for (int odd = 0; odd < 2; ++odd) {
+        const int par = (i + odd) & 1; /* row q*81 + 9i starts at parity (q + i) & 1 */
+        o.rp[odd] = NV * i + par;
+        o.rs[odd] = NV * i + (par ? 0 : 8);
+        o.par[odd] = par;
+    }
+    return o;
+}
+
+struct RowD {
+    double2 r0, r1, r2, r3;
+    double s;
+};
+struct RowF {
+    float r[9];
+};
+template <typename T> struct RowOf;
+template <> struct RowOf<double> { using type = RowD; };
+template <> struct RowOf<float> { using type = RowF; };
+
+__device__ __forceinline__ void load_row(RowD &R, const double *rowbase, const LaneOff &o, int odd) {
+    const double2 *r = reinterpret_cast<const double2 *>(rowbase + o.rp[odd]);
+    R.r0 = r[0];
+    R.r1 = r[1];
+    R.r2 = r[2];
+    R.r3 = r[3];
+    R.s = rowbase[o.rs[odd]];
+}
+
+__device__ __forceinline__ void load_row(RowF &R, const float *rowbase, const LaneOff &o, int) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) R.r[j] = rowbase[o.row + j];
+}
+
+/* the vector of lanes 0..8 in this lane's order for a row of parity `odd` */
+template <typename T>
+__device__ __forceinline__ void gather_vec(T (&v)[9], T x, const LaneOff &o, int odd) {
+    const int par = o.par[odd];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) v[j] = __shfl_sync(FULL, x, par + j);
+    v[8] = __shfl_sync(FULL, x, par ? 0 : 8);
+}
+
+__device__ __forceinline__ void gather_vec(float (&v)[9], float x, const LaneOff &, int) {
+#pragma unroll
+    for (int j = 0; j < 9; ++j) v[j] = __shfl_sync(FULL, x, j);
+}
+
+__device__ __forceinline__ double row_dot(const RowD &R, const double (&v)[9], double init) {
+    double a0 = init - R.s * v[8];
+    double a1 = R.r0.x * v[0];
+    double a2 = R.r0.y * v[1];
+    a0 -= R.r1.x * v[2];
+    a1 += R.r1.y * v[3];
+    a2 += R.r2.x * v[4];
+    a0 -= R.r2.y * v[5];
+    a1 += R.r3.x * v[6];
+    a2 += R.r3.y * v[7];
+    return a0 - (a1 + a2);
+}
+
+__device__ __forceinline__ float row_dot(const RowF &R, const float (&v)[9], float init) {
+    float a0 = init, a1 = 0.f, a2 = 0.f;
+    a0 -= R.r[0] * v[0];
+    a1 -= R.r[1] * v[1];
+    a2 -= R.r[2] * v[2];
+    a0 -= R.r[3] * v[3];
+    a1 -= R.r[4] * v[4];
+    a2 -= R.r[5] * v[5];
+    a0 -= R.r[6] * v[6];
+    a1 -= R.r[7] * v[7];
+    a2 -= R.r[8] * v[8];
+    return a0 + (a1 + a2);
+}
+
+/* v holds the previous cell's vector in the order of row parity (kbase&1 ^ 0)
+ * on entry and the last cell's in the order of the following row on exit. */
+template <typename T, int P, bool CHECK, bool YS>
+__device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T (&v)[9], T *ys, T *yg,
+                                          int kbase, int n, int i, bool writer,
+                                          const LaneOff &o) {
+    typename RowOf<T>::type cur_row, next_row;
+    load_row(cur_row, sG, o, 0);
+    T cur_b = sB[i];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        if (CHECK && kbase + q >= n) break;
+        const int odd = q & 1;
+        T next_b = T(0);
+        if (q + 1 < P) {
+            load_row(next_row, sG + (q + 1) * NB, o, odd ^ 1);
+            next_b = sB[(q + 1) * NV + i];
+        }
+        const T yi = row_dot(cur_row, v, cur_b);
+        if (writer) {
+            if (YS)
+                ys[(kbase + q) * NV + i] = yi;
+            else
+                yg[(size_t)(kbase + q) * NV + i] = yi;
+        }
+        gather_vec(v, yi, o, odd ^ 1);
+        cur_row = next_row;
+        cur_b = next_b;
+    }
+}
+
+template <typename T, int P, bool CHECK, bool YS>
+__device__ __forceinline__ void bwd_chunk(const T *sG, T (&v)[9], const T *ys, const T *yv,
+                                          const T *uv, T *dUl, T *Ul, int kbase, int n, int i,
+                                          bool writer, const LaneOff &o) {
+    typename RowOf<T>::type cur_row, next_row;
+    load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q) {
+        const int k = kbase + q;
+        const int odd = q & 1;
+        if (q > 0) load_row(next_row, sG + (q - 1) * NB, o, odd ^ 1);
+        if (!(CHECK && k >= n)) {
+            const T yk = YS ? ys[k * NV + i] : yv[q];
+            const T d = row_dot(cur_row, v, yk);
+            if (writer) {
+                dUl[(size_t)k * NV + i] = d;
+                Ul[(size_t)k * NV + i] = uv[q] + d;
+            }
+            gather_vec(v, d, o, odd ^ 1);
+        }
+        cur_row = next_row;
+    }
+}
+
+template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(32) fast_thomas_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const T *__restrict__ G, const T *__restrict__ Gam,
@@ -583,17 +737,23 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    unsigned char *st0 = smem + 128;
     const uint32_t stage = P * (NB + NV) * sizeof(T);
+    unsigned char *st0 = smem + 128;
+    T *ys = reinterpret_cast<T *>(st0 + (size_t)NS * stage);
     const int l = blockIdx.x;
     if (l >= nline) return;
     const int lane = threadIdx.x;
     const int i = lane < NV ? lane : NV - 1;
+    const bool writer = lane < NV;
+    const LaneOff off = lane_offsets(i);
     const int ps = line_start[l];
     const int n = line_len[l];
     const int npad = (n + 3) & ~3;
     const int nch = (npad + P - 1) / P;
     const int njobs = 2 * nch;
+    T *yl = y + (size_t)ps * NV;
+    T *dUl = dU + (size_t)ps * NV;
+    T *Ul = U + (size_t)ps * NV;
 
     if (lane == 0) {
         for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
@@ -626,15 +786,15 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     }
     int consumed = 0;
     bool timed_out = false;
+    const int nfull = n / P; /* chunks with P valid cells */
 
     /* ---------------- forward: y_k = b_k - G_k y_{k-1} */
-    T yp[NV];
+    T v[9];
 #pragma unroll
-    for (int j = 0; j < NV; ++j) yp[j] = T(0);
+    for (int j = 0; j < 9; ++j) v[j] = T(0);
     for (int c = 0; c < nch; ++c) {
         const int s = c % NS;
-        const uint32_t par = (uint32_t)((c / NS) & 1);
-        const bool ok = mbar_wait(&bars[s], par);
+        const bool ok = mbar_wait(&bars[s], (uint32_t)((c / NS) & 1));
         if (__any_sync(FULL, !ok)) {
             timed_out = true;
             break;
@@ -642,27 +802,10 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
         ++consumed;
         const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
         const T *sB = sG + P * NB;
-#pragma unroll
-        for (int q = 0; q < P; ++q) {
-            const int k = c * P + q;
-            if (k < n) {
-                const T *g = sG + q * NB + i;
-                T a0 = sB[q * NV + i], a1 = T(0), a2 = T(0);
-                a0 -= g[0] * yp[0];
-                a1 -= g[9] * yp[1];
-                a2 -= g[18] * yp[2];
-                a0 -= g[27] * yp[3];
-                a1 -= g[36] * yp[4];
-                a2 -= g[45] * yp[5];
-                a0 -= g[54] * yp[6];
-                a1 -= g[63] * yp[7];
-                a2 -= g[72] * yp[8];
-                const T yi = a0 + (a1 + a2);
-                if (lane < NV) y[(size_t)(ps + k) * NV + lane] = yi;
-#pragma unroll
-                for (int j = 0; j < NV; ++j) yp[j] = __shfl_sync(FULL, yi, j);
-            }
-        }
+        if (c < nfull)
+            fwd_chunk<T, P, false, YS>(sG, sB, v, ys, yl, c * P, n, i, writer, off);
+        else
+            fwd_chunk<T, P, true, YS>(sG, sB, v, ys, yl, c * P, n, i, writer, off);
         __syncwarp();
         if (lane == 0 && issued < njobs) {
             issue(issued, s);
@@ -672,9 +815,8 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
 
     /* ---------------- backward: dU_k = y_k - Gam_k dU_{k+1} */
     if (!timed_out) {
-        T dn[NV];
 #pragma unroll
-        for (int j = 0; j < NV; ++j) dn[j] = T(0);
+        for (int j = 0; j < 9; ++j) v[j] = T(0);
         T yv[P], uv[P], nyv[P], nuv[P];
         auto load_chunk = [&](int c, T *yy, T *uu) {
 #pragma unroll
@@ -682,9 +824,9 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
                 const int k = c * P + q;
                 yy[q] = T(0);
                 uu[q] = T(0);
-                if (k < n && lane < NV) {
-                    yy[q] = y[(size_t)(ps + k) * NV + lane];
-                    if (accumulate) uu[q] = U[(size_t)(ps + k) * NV + lane];
+                if (k < n && writer) {
+                    if (!YS) yy[q] = yl[(size_t)k * NV + i];
+                    if (accumulate) uu[q] = Ul[(size_t)k * NV + i];
                 }
             }
         };
@@ -694,38 +836,17 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             const int c = nch - 1 - jb;
             if (c > 0) load_chunk(c - 1, nyv, nuv);
             const int s = job % NS;
-            const uint32_t par = (uint32_t)((job / NS) & 1);
-            const bool ok = mbar_wait(&bars[s], par);
+            const bool ok = mbar_wait(&bars[s], (uint32_t)((job / NS) & 1));
             if (__any_sync(FULL, !ok)) {
                 timed_out = true;
                 break;
             }
             ++consumed;
             const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
-#pragma unroll
-            for (int q = P - 1; q >= 0; --q) {
-                const int k = c * P + q;
-                if (k < n) {
-                    const T *g = sG + q * NB + i;
-                    T a0 = yv[q], a1 = T(0), a2 = T(0);
-                    a0 -= g[0] * dn[0];
-                    a1 -= g[9] * dn[1];
-                    a2 -= g[18] * dn[2];
-                    a0 -= g[27] * dn[3];
-                    a1 -= g[36] * dn[4];
-                    a2 -= g[45] * dn[5];
-                    a0 -= g[54] * dn[6];
-                    a1 -= g[63] * dn[7];
-                    a2 -= g[72] * dn[8];
-                    const T d = a0 + (a1 + a2);
-                    if (lane < NV) {
-                        dU[(size_t)(ps + k) * NV + lane] = d;
-                        U[(size_t)(ps + k) * NV + lane] = uv[q] + d;
-                    }
-#pragma unroll
-                    for (int j = 0; j < NV; ++j) dn[j] = __shfl_sync(FULL, d, j);
-                }
-            }
+            if (c < nfull)
+                bwd_chunk<T, P, false, YS>(sG, v, ys, yv, uv, dUl, Ul, c * P, n, i, writer, off);
+            else
+                bwd_chunk<T, P, true, YS>(sG, v, ys, yv, uv, dUl, Ul, c * P, n, i, writer, off);
             __syncwarp();
             if (lane == 0 && issued < njobs) {
                 issue(issued, s);
@@ -745,24 +866,41 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     }
 }
 
-static int thomas_stages(int nline, size_t stage_bytes) {
-    const int per_sm = (nline + 147) / 148;
-    long long budget = 200LL * 1024 / (per_sm > 0 ? per_sm : 1);
-    long long ns = (budget - 128) / (long long)stage_bytes;
+struct ThomasCfg {
+    int NS;
+    bool ys;
+    size_t smem;
+};
+
+template <typename T>
+static ThomasCfg thomas_cfg(const FastLayout &L) {
+    const size_t sb = thomas_stage_bytes<T>();
+    const int per_sm = (L.nline + 147) / 148;
+    const long long budget = 210LL * 1024 / (per_sm > 0 ? per_sm : 1);
+    const size_t ys_bytes = (size_t)((L.max_len + 3) & ~3) * NV * sizeof(T);
+    const size_t fixed = 128;
+    ThomasCfg c;
+    c.ys = (long long)(fixed + ys_bytes + 4 * sb) <= budget;
+    long long left = budget - (long long)fixed - (c.ys ? (long long)ys_bytes : 0);
+    long long ns = left / (long long)sb;
     if (ns > 8) ns = 8;
     if (ns < 2) ns = 2;
-    return (int)ns;
+    c.NS = (int)ns;
+    c.smem = fixed + (size_t)c.NS * sb + (c.ys ? ys_bytes : 0);
+    return c;
 }
 
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
                        T *y, T *dU, T *U, unsigned *status, int accumulate) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    const size_t sb = thomas_stage_bytes<T>();
-    const int NS = thomas_stages(L.nline, sb);
-    const size_t smem = 128 + NS * sb;
-    fast_thomas_kernel<T, THOMAS_P><<<L.nline, 32, smem, st>>>(
-        L.nline, NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
+    const ThomasCfg cfg = thomas_cfg<T>(L);
+    if (cfg.ys)
+        fast_thomas_kernel<T, THOMAS_P, true><<<L.nline, 32, cfg.smem, st>>>(
+            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
+    else
+        fast_thomas_kernel<T, THOMAS_P, false><<<L.nline, 32, cfg.smem, st>>>(
+            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
     return (int)cudaGetLastError();
 }
 
@@ -773,14 +911,6 @@ template int launch_fast_thomas<float>(cudaStream_t, const FastLayout &, const f
                                        const float *, const float *, float *, float *, float *,
                                        unsigned *, int);
 
-/* Shared memory the streaming kernels need for a layout. */
-template <typename T>
-static size_t resid_smem(const FastLayout &L) {
-    const int nxa = L.nx > 0 ? L.nx : 1;
-    return 128 + RES_STAGES * (size_t)resid_stage_bytes<T>(L.nx) +
-           (size_t)RES_TILE * nxa * NV * sizeof(T) + RES_TILE * NV * sizeof(T);
-}
-
 static int smem_limit(const void *fn) {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
@@ -790,7 +920,6 @@ static int smem_limit(const void *fn) {
     return optin - (int)fa.sharedSizeBytes;
 }
 
-template <typename T>
 static int set_smem(const void *fn, size_t need) {
     if ((long long)need > smem_limit(fn)) return (int)cudaErrorInvalidConfiguration;
     if (need <= 48 * 1024) return 0;
@@ -800,12 +929,17 @@ static int set_smem(const void *fn, size_t need) {
 /* Called before any launch (and outside stream capture) once the layout is
  * known: opts the streaming kernels into the shared memory they need. */
 int fast_prepare(const FastLayout &L) {
-    int rc = set_smem<double>((const void *)fast_resid_kernel<double>, resid_smem<double>(L));
-    if (!rc) rc = set_smem<float>((const void *)fast_resid_kernel<float>, resid_smem<float>(L));
-    const size_t t64 = 128 + thomas_stages(L.nline, thomas_stage_bytes<double>()) * (size_t)thomas_stage_bytes<double>();
-    const size_t t32 = 128 + thomas_stages(L.nline, thomas_stage_bytes<float>()) * (size_t)thomas_stage_bytes<float>();
-    if (!rc) rc = set_smem<double>((const void *)fast_thomas_kernel<double, THOMAS_P>, t64);
-    if (!rc) rc = set_smem<float>((const void *)fast_thomas_kernel<float, THOMAS_P>, t32);
+    int rc = set_smem((const void *)fast_resid_kernel<double>, resid_smem_bytes<double>(L.nx));
+    if (!rc) rc = set_smem((const void *)fast_resid_kernel<float>, resid_smem_bytes<float>(L.nx));
+    const ThomasCfg c64 = thomas_cfg<double>(L), c32 = thomas_cfg<float>(L);
+    if (!rc)
+        rc = set_smem(c64.ys ? (const void *)fast_thomas_kernel<double, THOMAS_P, true>
+                             : (const void *)fast_thomas_kernel<double, THOMAS_P, false>,
+                      c64.smem);
+    if (!rc)
+        rc = set_smem(c32.ys ? (const void *)fast_thomas_kernel<float, THOMAS_P, true>
+                             : (const void *)fast_thomas_kernel<float, THOMAS_P, false>,
+                      c32.smem);
     return rc;
 }
 

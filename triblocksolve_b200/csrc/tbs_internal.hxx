@@ -57,12 +57,13 @@ enum : unsigned {
  * CUDA graph serves every tolerance and sweep limit. */
 struct SolveState {
     double norm0;      /* ||R_0|| of the current solve */
-    double tol;        /* relative tolerance */
     double last;       /* latest ||R|| */
-    int max_sweeps;
     int sweep;         /* sweeps done in the current solve */
-    int hist_cap;      /* entries available in hist */
     int pad;
+    /* control block, written by the host before a solve (offset 24) */
+    double tol;        /* relative tolerance */
+    int max_sweeps;
+    int hist_cap;      /* entries available in hist */
 };
 
 /* ------------------------------------------------- fast (line-ordered) layout
@@ -86,8 +87,8 @@ struct FastLayout {
     int *line_len;     /* [nline] */
     int *pos_of_elem;  /* [nelem] */
     int *elem_of_pos;  /* [np16], -1 for pads */
-    int *xnbr;         /* [np16*nx] neighbour position or -1 */
-    int *xsrc;         /* [np16*nx] 2*face + (1 if the block is O2), or -1 */
+    int *xnbr;         /* [nx*np16] slot-major: neighbour position or -1 */
+    int *xsrc;         /* [nx*np16] 2*face + (1 if the block is O2), or -1 */
     int *fsrc;         /* [np16*3] factor sources: elem, face of A/C, side */
 };
 
@@ -132,10 +133,23 @@ int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
 int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, const double *O2,
                         double *X, float *X32);
 int fast_resid_grid(int np16);
+/* Where a streaming kernel's sum of R^2 goes: per-CTA partials, and, when
+ * `state` is set, the last CTA's fixed-order total recorded like
+ * reduce_norm (norm history, sweep count, graph loop condition). */
+struct NormSink {
+    double *partials;            /* [grid] or null: no norm */
+    unsigned *counter;           /* zero between launches */
+    SolveState *state;           /* null: partials only */
+    double *hist;
+    int is_start;
+    int use_cond;
+    unsigned long long handle;   /* cudaGraphConditionalHandle */
+};
+
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
-                      const T *X, const T *dU, const T *Rsrc, T *b, double *partials,
-                      int npart, unsigned *status);
+                      const T *X, const T *dU, const T *Rsrc, T *b, const NormSink &ns,
+                      unsigned *status);
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
                        const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
