@@ -65,6 +65,7 @@ struct tbs_ctx {
     /* ---- line-ordered layout (FP64 / MIXED) ---- */
     FastLayout L{};
     bool layout_ok = false;
+    double *d_gamlast = nullptr; /* per line and chain: last Gam toward the twist, FP64 */
     long long n_xslots_real = 0;
     double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
     double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
@@ -201,14 +202,14 @@ static void drop_mesh(tbs_ctx *ctx) {
                       &ctx->d_R, &ctx->d_Uinit, &ctx->d_scratch, &ctx->d_DLU, &ctx->d_DinvC,
                       &ctx->d_A, &ctx->d_Dinv, &ctx->d_G, &ctx->d_Gam, &ctx->d_X, &ctx->d_Up,
                       &ctx->d_dUp, &ctx->d_b, &ctx->d_y, &ctx->d_rhsp, &ctx->d_Rp,
-                      &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist};
+                      &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist, &ctx->d_gamlast};
     for (auto p : dps) *p = nullptr;
     float **fps[] = {&ctx->d_Dinv32, &ctx->d_G32, &ctx->d_Gam32, &ctx->d_X32, &ctx->d_b32,
                      &ctx->d_y32, &ctx->d_d32, &ctx->d_c32, &ctx->d_R32};
     for (auto p : fps) *p = nullptr;
     int **ips[] = {&ctx->d_epoint, &ctx->d_ef, &ctx->d_fc, &ctx->d_linesize, &ctx->d_linepoint,
                    &ctx->d_lines, &ctx->d_lineface, &ctx->d_identity, &ctx->L.line_start,
-                   &ctx->L.line_len, &ctx->L.pos_of_elem, &ctx->L.elem_of_pos, &ctx->L.xnbr,
+                   &ctx->L.line_len, &ctx->L.line_twist, &ctx->L.pos_of_elem, &ctx->L.elem_of_pos, &ctx->L.xnbr,
                    &ctx->L.xsrc, &ctx->L.fsrc};
     for (auto p : ips) *p = nullptr;
     ctx->d_state = nullptr;
@@ -285,40 +286,58 @@ static int build_layout(tbs_ctx *ctx) {
     const int *ls = ctx->h_linesize.data(), *lp = ctx->h_linepoint.data();
     const int *lines = ctx->h_lines.data(), *lf = ctx->h_lineface.data();
     const int *fc = ctx->h_fc.data(), *ep = ctx->h_epoint.data(), *ef = ctx->h_ef.data();
-    std::vector<int> start(nline), len(nline);
+    std::vector<int> start(nline), len(nline), twist(nline);
     long long np = 0;
     for (int l = 0; l < nline; ++l) {
         start[l] = (int)np;
         len[l] = ls[l];
+        twist[l] = line_twist_of(ls[l]);
         np += (ls[l] + 3) & ~3;
     }
     if (np > 0x7fffffffLL / 81)
         return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "mesh too large for int32 block offsets");
     const int np16 = (int)((np + RES_TILE - 1) / RES_TILE * RES_TILE);
-    std::vector<int> pos_of_elem(nelem), elem_of_pos(np16, -1), fsrc((size_t)np16 * 3, 0);
+    std::vector<int> pos_of_elem(nelem), elem_of_pos(np16, -1), fsrc((size_t)np16 * 5, -1);
+    auto side_of = [&](int e, int f) { return (e == fc[2 * f]) ? 1 : 0; };
     for (int l = 0; l < nline; ++l) {
-        for (int k = 0; k < ls[l]; ++k) {
-            const int m = lp[l] + k, e = lines[m], p = start[l] + k;
+        const int n = ls[l], m = twist[l], ps = start[l];
+        for (int k = 0; k < n; ++k) {
+            const int e = lines[lp[l] + k];
+            const int p = (k < m) ? ps + k : (k > m) ? ps + m + (n - 1 - k) : ps + n - 1;
             pos_of_elem[e] = p;
             elem_of_pos[p] = e;
-            fsrc[3 * (size_t)p] = e;
-            if (k >= 1) {
-                const int f = lf[m];
-                fsrc[3 * (size_t)p + 1] = f;
-                fsrc[3 * (size_t)p + 2] = (e == fc[2 * f]) ? 1 : 0;
-            } else {
-                fsrc[3 * (size_t)p + 1] = -1;
+            int *fs = &fsrc[5 * (size_t)p];
+            fs[0] = e;
+            if (k < m) { /* top chain: predecessor k-1 */
+                if (k >= 1) {
+                    fs[1] = lf[lp[l] + k];
+                    fs[2] = side_of(e, fs[1]);
+                }
+            } else if (k > m) { /* bottom chain: predecessor k+1 */
+                if (k + 1 < n) {
+                    fs[1] = lf[lp[l] + k + 1];
+                    fs[2] = side_of(e, fs[1]);
+                }
+            } else { /* twist: faces to m-1 and m+1 */
+                if (m >= 1) {
+                    fs[1] = lf[lp[l] + m];
+                    fs[2] = side_of(e, fs[1]);
+                }
+                if (m + 1 < n) {
+                    fs[3] = lf[lp[l] + m + 1];
+                    fs[4] = side_of(e, fs[3]);
+                }
             }
         }
     }
     /* cross-line slots: every interior face of the cell that is not one of
-     * the (at most two) in-line faces used by the Thomas factorization */
+     * the (at most two) in-line faces used by the line factorization */
     std::vector<std::vector<std::pair<int, int>>> xs(np16);
     int nx = 0;
     long long nreal = 0;
     for (int l = 0; l < nline; ++l) {
         for (int k = 0; k < ls[l]; ++k) {
-            const int m = lp[l] + k, e = lines[m], p = start[l] + k;
+            const int m = lp[l] + k, e = lines[m], p = pos_of_elem[e];
             int fprev = (k >= 1) ? lf[m] : -1;
             int fnext = (k + 1 < ls[l]) ? lf[m + 1] : -1;
             auto &v = xs[p];
@@ -357,23 +376,26 @@ static int build_layout(tbs_ctx *ctx) {
     ctx->n_xslots_real = nreal;
     DA(L.line_start, nline);
     DA(L.line_len, nline);
+    DA(L.line_twist, nline);
     DA(L.pos_of_elem, nelem);
     DA(L.elem_of_pos, np16);
-    DA(L.fsrc, (size_t)np16 * 3);
+    DA(L.fsrc, (size_t)np16 * 5);
     DA(L.xsrc, (size_t)np16 * std::max(nx, 1));
     DA(L.xnbr, (size_t)np16 * std::max(nx, 1));
+    DA(ctx->d_gamlast, (size_t)nline * 2 * 81);
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(L.line_start, start.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.line_len, len.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.line_twist, twist.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.pos_of_elem, pos_of_elem.data(), nelem * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.elem_of_pos, elem_of_pos.data(), np16 * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.fsrc, fsrc.data(), fsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.xsrc, xsrc.data(), xsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.xnbr, xnbr.data(), xnbr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
-    /* the residual kernel stages RES_TILE cells x nx blocks per pipeline
-     * stage; beyond 4 cross-line couplings per cell it would not fit in
-     * shared memory, and such meshes use TBS_ALGO_REFERENCE */
+    /* the residual kernel stages RES_TILE cells x nx blocks per tile; beyond
+     * 4 cross-line couplings per cell it would not fit in shared memory,
+     * and such meshes use TBS_ALGO_REFERENCE */
     ctx->layout_ok = (ctx->nvar == 9) && nx <= 4;
     return TBS_OK;
 }
@@ -699,12 +721,12 @@ static int run_factor(tbs_ctx *ctx, int algo) {
     if (algo == TBS_ALGO_FP64) {
         RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,
                                               ctx->d_G, ctx->d_Gam, nullptr, nullptr, nullptr,
-                                              ctx->d_status));
+                                              ctx->d_gamlast, ctx->d_status));
         RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, ctx->d_X, nullptr));
     } else {
         RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, nullptr,
                                               nullptr, nullptr, ctx->d_Dinv32, ctx->d_G32,
-                                              ctx->d_Gam32, ctx->d_status));
+                                              ctx->d_Gam32, ctx->d_gamlast, ctx->d_status));
         RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, nullptr, ctx->d_X32));
     }
     return TBS_OK;

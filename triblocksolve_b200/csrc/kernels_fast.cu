@@ -192,18 +192,25 @@ int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n)
 }
 
 /* ====================================================== line factorization
- * One CTA of 128 threads per line, thread t < 81 owns entry t of each 9x9
- * block (row t%9, column t/9).  Per cell k >= 1:
- *   Gam_{k-1} = Dinv_{k-1} C_{k-1}
- *   W         = D_k - A_k Gam_{k-1}          (block-Thomas pivot D'_k)
- *   Dinv_k    = W^-1   (in-place Gauss-Jordan, no pivoting, as the
+ * Twisted block Thomas.  Each line is split into a top chain (cells
+ * 0..m-1, eliminated downward as in src/okl/lineLU_v2.okl:58-182), a
+ * bottom chain (cells n-1 down to m+1, the same elimination run upward) and
+ * the twist cell m.  One CTA of 128 threads per chain (grid = 2 x lines);
+ * thread t < 81 owns entry t of each 9x9 block (row t%9, column t/9).  For
+ * chain step s >= 1 with A = block(row c_s, col c_{s-1}) and C =
+ * block(row c_{s-1}, col c_s), both from the in-line face between them
+ * (picked as in lineLU_v2.okl:116-117):
+ *   Gam_{s-1} = Dinv_{s-1} C
+ *   W         = D_s - A Gam_{s-1}          (block-Thomas pivot)
+ *   Dinv_s    = W^-1   (in-place Gauss-Jordan, no pivoting, as the
  *                        reference's LU has none: lineLU_v2.okl:17-27)
- *   G_k       = Dinv_k A_k
- * A/C are the two blocks of the in-line face joining cells k-1 and k,
- * picked as in lineLU_v2.okl:116-117.  Dinv is stored column-major like the
- * input blocks; G and Gam row-major (entry (i,j) at 9i+j), the order the
- * Thomas kernel reads them in.  The FP32 arrays, when given, are the FP64
- * results rounded once. */
+ *   G_s       = Dinv_s A
+ * and the chain's last Gam couples it to the twist cell.  The twist kernel
+ * then forms Dinv_tw = (D_m - A_tw Gam_top - C_tw Gam_bot)^-1 and stores
+ * Dinv_tw A_tw / Dinv_tw C_tw in the G / Gam slots of the twist position.
+ * Dinv is stored column-major like the input blocks; G and Gam row-major
+ * (entry (i,j) at 9i+j), the order the Thomas kernel reads them in.  The
+ * FP32 arrays, when given, are the FP64 results rounded once. */
 __device__ __forceinline__ void gj_invert(double *W, int t, unsigned *status) {
     const int i = t % NV, j = t / NV;
 #pragma unroll 1
@@ -234,52 +241,64 @@ __device__ __forceinline__ void gj_invert(double *W, int t, unsigned *status) {
     }
 }
 
+struct FactorOut {
+    double *Dinv, *G, *Gam;
+    float *Dinv32, *G32, *Gam32;
+    __device__ void put_dinv(size_t p, int t, double w) const {
+        if (Dinv) Dinv[p * NB + t] = w;
+        if (Dinv32) Dinv32[p * NB + t] = (float)w;
+    }
+    /* row-major store of entry (i, j) */
+    __device__ void put_g(size_t p, int i, int j, double v) const {
+        if (G) G[p * NB + NV * i + j] = v;
+        if (G32) G32[p * NB + NV * i + j] = (float)v;
+    }
+    __device__ void put_gam(size_t p, int i, int j, double v) const {
+        if (Gam) Gam[p * NB + NV * i + j] = v;
+        if (Gam32) Gam32[p * NB + NV * i + j] = (float)v;
+    }
+};
+
 __global__ void __launch_bounds__(128) fast_factor_kernel(
     int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
-    const int *__restrict__ fsrc, const double *__restrict__ jacD, const double *__restrict__ O1,
-    const double *__restrict__ O2, double *__restrict__ Dinv, double *__restrict__ G,
-    double *__restrict__ Gam, float *__restrict__ Dinv32, float *__restrict__ G32,
-    float *__restrict__ Gam32, unsigned *status) {
-    const int l = blockIdx.x;
+    const int *__restrict__ line_twist, const int *__restrict__ fsrc,
+    const double *__restrict__ jacD, const double *__restrict__ O1, const double *__restrict__ O2,
+    FactorOut out, double *__restrict__ gamlast, unsigned *status) {
+    const int l = blockIdx.x >> 1, g = blockIdx.x & 1;
     if (l >= nline) return;
     const int t = threadIdx.x;
     const bool act = t < NB;
     const int i = t % NV, j = t / NV;
     __shared__ double sW[NB], sPrev[NB], sA[NB], sC[NB], sGam[NB];
-    const int ps = line_start[l];
-    const int n = line_len[l];
-
+    const int ps = line_start[l], n = line_len[l], m = line_twist[l];
+    const int len = g ? n - 1 - m : m;
+    const int cs = ps + (g ? m : 0);
+    const int ptw = ps + n - 1;
+    if (len == 0) {
+        if (act) gamlast[((size_t)l * 2 + g) * NB + t] = 0.0;
+        return;
+    }
     double d = 0.0, a = 0.0, c = 0.0;
-    if (act) d = jacD[(size_t)fsrc[3 * ps] * NB + t];
-    if (act) sW[t] = d;
+    if (act) sW[t] = jacD[(size_t)fsrc[5 * cs] * NB + t];
     __syncthreads();
     gj_invert(sW, t, status);
     if (act) {
         const double w = sW[t];
-        if (Dinv) {
-            Dinv[(size_t)ps * NB + t] = w;
-            G[(size_t)ps * NB + t] = 0.0;
-        }
-        if (Dinv32) {
-            Dinv32[(size_t)ps * NB + t] = (float)w;
-            G32[(size_t)ps * NB + t] = 0.0f;
-        }
+        out.put_dinv(cs, t, w);
+        out.put_g(cs, i, j, 0.0);
         sPrev[t] = w;
     }
-    /* prefetch cell 1 */
     auto fetch = [&](int p) {
         if (act) {
-            const int e = fsrc[3 * p], f = fsrc[3 * p + 1], side = fsrc[3 * p + 2];
-            const double *Ap = side ? O2 : O1;
-            const double *Cp = side ? O1 : O2;
-            a = Ap[(size_t)f * NB + t];
-            c = Cp[(size_t)f * NB + t];
+            const int e = fsrc[5 * p], f = fsrc[5 * p + 1], side = fsrc[5 * p + 2];
+            a = (side ? O2 : O1)[(size_t)f * NB + t];
+            c = (side ? O1 : O2)[(size_t)f * NB + t];
             d = jacD[(size_t)e * NB + t];
         }
     };
-    if (n > 1) fetch(ps + 1);
-    for (int k = 1; k < n; ++k) {
-        const int p = ps + k;
+    if (len > 1) fetch(cs + 1);
+    for (int s = 1; s < len; ++s) {
+        const int p = cs + s;
         __syncthreads();
         if (act) {
             sA[t] = a;
@@ -287,14 +306,13 @@ __global__ void __launch_bounds__(128) fast_factor_kernel(
             sW[t] = d;
         }
         __syncthreads();
-        if (k + 1 < n) fetch(p + 1);
-        double g = 0.0;
+        if (s + 1 < len) fetch(p + 1);
         if (act) {
+            double gm = 0.0;
 #pragma unroll
-            for (int q = 0; q < NV; ++q) g += sPrev[i + NV * q] * sC[q + NV * j];
-            sGam[t] = g;
-            if (Gam) Gam[(size_t)(p - 1) * NB + NV * i + j] = g;
-            if (Gam32) Gam32[(size_t)(p - 1) * NB + NV * i + j] = (float)g;
+            for (int q = 0; q < NV; ++q) gm += sPrev[i + NV * q] * sC[q + NV * j];
+            out.put_gam(p - 1, i, j, gm);
+            sGam[t] = gm; /* Gam_{s-1}, column-major */
         }
         __syncthreads();
         if (act) {
@@ -309,30 +327,84 @@ __global__ void __launch_bounds__(128) fast_factor_kernel(
             double gk = 0.0;
 #pragma unroll
             for (int q = 0; q < NV; ++q) gk += sW[i + NV * q] * sA[q + NV * j];
+            out.put_g(p, i, j, gk);
             const double w = sW[t];
-            if (Dinv) {
-                G[(size_t)p * NB + NV * i + j] = gk;
-                Dinv[(size_t)p * NB + t] = w;
-            }
-            if (Dinv32) {
-                G32[(size_t)p * NB + NV * i + j] = (float)gk;
-                Dinv32[(size_t)p * NB + t] = (float)w;
-            }
+            out.put_dinv(p, t, w);
             sPrev[t] = w;
         }
     }
+    /* coupling of the chain's last cell to the twist: block(row last, col m) */
+    __syncthreads();
     if (act) {
-        if (Gam) Gam[(size_t)(ps + n - 1) * NB + t] = 0.0;
-        if (Gam32) Gam32[(size_t)(ps + n - 1) * NB + t] = 0.0f;
+        const int f = fsrc[5 * ptw + (g ? 3 : 1)], side = fsrc[5 * ptw + (g ? 4 : 2)];
+        sC[t] = (side ? O1 : O2)[(size_t)f * NB + t];
+    }
+    __syncthreads();
+    if (act) {
+        double gm = 0.0;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) gm += sPrev[i + NV * q] * sC[q + NV * j];
+        out.put_gam(cs + len - 1, i, j, gm);
+        gamlast[((size_t)l * 2 + g) * NB + t] = gm; /* column-major, FP64 */
+    }
+}
+
+__global__ void __launch_bounds__(128) fast_twist_kernel(
+    int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
+    const int *__restrict__ line_twist, const int *__restrict__ fsrc,
+    const double *__restrict__ jacD, const double *__restrict__ O1, const double *__restrict__ O2,
+    FactorOut out, const double *__restrict__ gamlast, unsigned *status) {
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    const int t = threadIdx.x;
+    const bool act = t < NB;
+    const int i = t % NV, j = t / NV;
+    __shared__ double sW[NB], sA[NB], sC[NB], sGt[NB], sGb[NB];
+    const int ps = line_start[l], n = line_len[l];
+    const int ptw = ps + n - 1;
+    if (act) {
+        const int e = fsrc[5 * ptw];
+        const int fa = fsrc[5 * ptw + 1], sa = fsrc[5 * ptw + 2];
+        const int fb = fsrc[5 * ptw + 3], sb = fsrc[5 * ptw + 4];
+        sW[t] = jacD[(size_t)e * NB + t];
+        sA[t] = fa >= 0 ? (sa ? O2 : O1)[(size_t)fa * NB + t] : 0.0;
+        sC[t] = fb >= 0 ? (sb ? O2 : O1)[(size_t)fb * NB + t] : 0.0;
+        sGt[t] = gamlast[((size_t)l * 2 + 0) * NB + t];
+        sGb[t] = gamlast[((size_t)l * 2 + 1) * NB + t];
+    }
+    __syncthreads();
+    if (act) {
+        double w = sW[t];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) w -= sA[i + NV * q] * sGt[q + NV * j];
+#pragma unroll
+        for (int q = 0; q < NV; ++q) w -= sC[i + NV * q] * sGb[q + NV * j];
+        sW[t] = w; /* only this thread reads or writes sW[t] in this phase */
+    }
+    __syncthreads();
+    gj_invert(sW, t, status);
+    if (act) {
+        double ga = 0.0, gc = 0.0;
+#pragma unroll
+        for (int q = 0; q < NV; ++q) {
+            ga += sW[i + NV * q] * sA[q + NV * j];
+            gc += sW[i + NV * q] * sC[q + NV * j];
+        }
+        out.put_dinv(ptw, t, sW[t]);
+        out.put_g(ptw, i, j, ga);
+        out.put_gam(ptw, i, j, gc);
     }
 }
 
 int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD, const double *O1,
                        const double *O2, double *Dinv, double *G, double *Gam, float *Dinv32,
-                       float *G32, float *Gam32, unsigned *status) {
+                       float *G32, float *Gam32, double *gamlast, unsigned *status) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    fast_factor_kernel<<<L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.fsrc, jacD, O1,
-                                                O2, Dinv, G, Gam, Dinv32, G32, Gam32, status);
+    FactorOut out{Dinv, G, Gam, Dinv32, G32, Gam32};
+    fast_factor_kernel<<<2 * L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.line_twist,
+                                                    L.fsrc, jacD, O1, O2, out, gamlast, status);
+    fast_twist_kernel<<<L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.line_twist,
+                                               L.fsrc, jacD, O1, O2, out, gamlast, status);
     return (int)cudaGetLastError();
 }
 
@@ -564,46 +636,54 @@ template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, con
                                       const NormSink &, unsigned *);
 
 /* =========================================================== line Thomas
- * One warp per line.  Lane 0 streams "jobs" through an NS-stage bulk-copy
- * ring: jobs 0..nch-1 are forward chunks (G and b of P cells), jobs
- * nch..2nch-1 backward chunks in reverse (Gam of P cells).  G and Gam are
- * stored row-major; lane i < 9 owns row i and holds the row of the NEXT
- * cell in registers while the current cell's dot product runs, so that the
- * critical path of a step is one shuffle broadcast plus five dependent
- * FP64 operations (a shared-memory broadcast would need __syncwarp, whose
- * memory ordering waits for the step's global stores).  A row starting at
- * an odd double is read as single + four 16-byte pairs, one starting at an
- * even double as four pairs + single; each lane gathers the vector from
- * lanes 0..8 in the matching order.  The forward results y stay in shared
- * memory when the line fits (YS), otherwise they go to global memory and
- * come back one chunk ahead.
+ * One warp per line, twisted: lanes 0..8 run the top chain and lanes
+ * 16..24 the bottom chain of the line with the same instruction stream, so
+ * a line of n cells takes n+1 dependent steps instead of 2n.  Lane 0
+ * streams "jobs" through an NS-stage bulk-copy ring, each stage holding one
+ * chunk of P cells per chain: jobs 0..nf-1 forward chunks (G rows and b),
+ * jobs nf..2nf-1 backward chunks in reverse (Gam rows).  G and Gam are
+ * row-major; lane i owns row i and holds the row of the NEXT cell in
+ * registers while the current cell's dot product runs.  The previous
+ * cell's 9-vector is published through shared memory in two copies (at
+ * offsets 0 and 11), so that every lane reads it with the 16-byte
+ * alignment of its row.  Chain forward:  y_s = b_s - G_s y_{s-1};  twist:
+ * x_m = b_m - G_tw y_top - Gam_tw y_bot;  chain backward:  x_s = y_s -
+ * Gam_s x_{s+1} (s+1 toward the twist).
+ * YS: the line's y and x live in shared memory, and dU / U are written with
+ * coalesced 16-byte accesses after the line is solved; otherwise y goes to
+ * global memory (read back one chunk ahead) and dU / U per step.
  *   accumulate = 0:  U = dU  (first sweep of a solve, U starts at 0)
  *   accumulate = 1:  U += dU
  */
 constexpr int THOMAS_P = 8;
 
 template <typename T>
-__host__ __device__ inline uint32_t thomas_stage_bytes() {
+__host__ __device__ inline uint32_t thomas_half_bytes() {
     return (uint32_t)(THOMAS_P * (NB + NV) * sizeof(T));
 }
+template <typename T>
+__host__ __device__ inline uint32_t thomas_stage_bytes() {
+    return 2 * thomas_half_bytes<T>();
+}
 
-/* Lane constants for rows of parity odd (0/1 = parity of q): pair offset,
- * single offset and the source lane of the first vector element. */
+/* Lane constants for rows whose start parity is (q + i) & 1: pairs start at
+ * row+par, the single element is row[8] (par 0) or row[0] (par 1); the
+ * broadcast vector is read from copy A (offset 0) or copy B (offset 10,
+ * holding y_j at 11+j) so that the pairs line up. */
 struct LaneOff {
-    int row;     /* NV * i */
-    int rp[2];   /* first pair element */
-    int rs[2];   /* single element */
-    int par[2];  /* vector element order: y_{par+j} for j < 8, then the single */
+    int row;
+    int rp[2], rs[2], vp[2], vs[2];
 };
 
 __device__ __forceinline__ LaneOff lane_offsets(int i) {
     LaneOff o;
     o.row = NV * i;
     for (int odd = 0; odd < 2; ++odd) {
-        const int par = (i + odd) & 1; /* row q*81 + 9i starts at parity (q + i) & 1 */
+        const int par = (i + odd) & 1;
         o.rp[odd] = NV * i + par;
         o.rs[odd] = NV * i + (par ? 0 : 8);
-        o.par[odd] = par;
+        o.vp[odd] = par ? 12 : 0;
+        o.vs[odd] = par ? 0 : 8;
     }
     return o;
 }
@@ -633,98 +713,104 @@ __device__ __forceinline__ void load_row(RowF &R, const float *rowbase, const La
     for (int j = 0; j < 9; ++j) R.r[j] = rowbase[o.row + j];
 }
 
-/* the vector of lanes 0..8 in this lane's order for a row of parity `odd` */
-template <typename T>
-__device__ __forceinline__ void gather_vec(T (&v)[9], T x, const LaneOff &o, int odd) {
-    const int par = o.par[odd];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) v[j] = __shfl_sync(FULL, x, par + j);
-    v[8] = __shfl_sync(FULL, x, par ? 0 : 8);
-}
-
-__device__ __forceinline__ void gather_vec(float (&v)[9], float x, const LaneOff &, int) {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) v[j] = __shfl_sync(FULL, x, j);
-}
-
-__device__ __forceinline__ double row_dot(const RowD &R, const double (&v)[9], double init) {
-    double a0 = init - R.s * v[8];
-    double a1 = R.r0.x * v[0];
-    double a2 = R.r0.y * v[1];
-    a0 -= R.r1.x * v[2];
-    a1 += R.r1.y * v[3];
-    a2 += R.r2.x * v[4];
-    a0 -= R.r2.y * v[5];
-    a1 += R.r3.x * v[6];
-    a2 += R.r3.y * v[7];
+/* init - row . vec, vec from the broadcast buffer `cur` */
+__device__ __forceinline__ double row_dot(const RowD &R, const double *cur, const LaneOff &o,
+                                          int odd, double init) {
+    const double2 *v = reinterpret_cast<const double2 *>(cur + o.vp[odd]);
+    const double2 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    const double w = cur[o.vs[odd]];
+    double a0 = init - R.s * w;
+    double a1 = R.r0.x * v0.x;
+    double a2 = R.r0.y * v0.y;
+    a0 -= R.r1.x * v1.x;
+    a1 += R.r1.y * v1.y;
+    a2 += R.r2.x * v2.x;
+    a0 -= R.r2.y * v2.y;
+    a1 += R.r3.x * v3.x;
+    a2 += R.r3.y * v3.y;
     return a0 - (a1 + a2);
 }
 
-__device__ __forceinline__ float row_dot(const RowF &R, const float (&v)[9], float init) {
+__device__ __forceinline__ float row_dot(const RowF &R, const float *cur, const LaneOff &, int,
+                                         float init) {
     float a0 = init, a1 = 0.f, a2 = 0.f;
-    a0 -= R.r[0] * v[0];
-    a1 -= R.r[1] * v[1];
-    a2 -= R.r[2] * v[2];
-    a0 -= R.r[3] * v[3];
-    a1 -= R.r[4] * v[4];
-    a2 -= R.r[5] * v[5];
-    a0 -= R.r[6] * v[6];
-    a1 -= R.r[7] * v[7];
-    a2 -= R.r[8] * v[8];
+    a0 -= R.r[0] * cur[0];
+    a1 -= R.r[1] * cur[1];
+    a2 -= R.r[2] * cur[2];
+    a0 -= R.r[3] * cur[3];
+    a1 -= R.r[4] * cur[4];
+    a2 -= R.r[5] * cur[5];
+    a0 -= R.r[6] * cur[6];
+    a1 -= R.r[7] * cur[7];
+    a2 -= R.r[8] * cur[8];
     return a0 + (a1 + a2);
 }
 
-/* v holds the previous cell's vector in the order of row parity (kbase&1 ^ 0)
- * on entry and the last cell's in the order of the following row on exit. */
+/* Forward steps kbase..kbase+P-1 of this half's chain (length len, first
+ * position cpos relative to the line start).  CHECK: some steps of the
+ * warp may lie beyond one chain's end; those compute but write nothing. */
 template <typename T, int P, bool CHECK, bool YS>
-__device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T (&v)[9], T *ys, T *yg,
-                                          int kbase, int n, int i, bool writer,
+__device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys, T *yg, int kbase,
+                                          int len, int cpos, int i, bool writer,
                                           const LaneOff &o) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG, o, 0);
     T cur_b = sB[i];
 #pragma unroll
     for (int q = 0; q < P; ++q) {
-        if (CHECK && kbase + q >= n) break;
         const int odd = q & 1;
         T next_b = T(0);
         if (q + 1 < P) {
             load_row(next_row, sG + (q + 1) * NB, o, odd ^ 1);
             next_b = sB[(q + 1) * NV + i];
         }
-        const T yi = row_dot(cur_row, v, cur_b);
-        if (writer) {
+        const T *cur = bc + odd * 20;
+        T *nxt = bc + (odd ^ 1) * 20;
+        const T yi = row_dot(cur_row, cur, o, odd, cur_b);
+        if (writer && (!CHECK || kbase + q < len)) {
+            nxt[i] = yi;
+            nxt[11 + i] = yi;
+            const int pos = cpos + kbase + q;
             if (YS)
-                ys[(kbase + q) * NV + i] = yi;
+                ys[pos * NV + i] = yi;
             else
-                yg[(size_t)(kbase + q) * NV + i] = yi;
+                yg[(size_t)pos * NV + i] = yi;
         }
-        gather_vec(v, yi, o, odd ^ 1);
+        __syncwarp();
         cur_row = next_row;
         cur_b = next_b;
     }
 }
 
 template <typename T, int P, bool CHECK, bool YS>
-__device__ __forceinline__ void bwd_chunk(const T *sG, T (&v)[9], const T *ys, const T *yv,
-                                          const T *uv, T *dUl, T *Ul, int kbase, int n, int i,
+__device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv, const T *uv,
+                                          T *dUl, T *Ul, int kbase, int len, int cpos, int i,
                                           bool writer, const LaneOff &o) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
 #pragma unroll
     for (int q = P - 1; q >= 0; --q) {
-        const int k = kbase + q;
         const int odd = q & 1;
         if (q > 0) load_row(next_row, sG + (q - 1) * NB, o, odd ^ 1);
-        if (!(CHECK && k >= n)) {
-            const T yk = YS ? ys[k * NV + i] : yv[q];
-            const T d = row_dot(cur_row, v, yk);
-            if (writer) {
-                dUl[(size_t)k * NV + i] = d;
-                Ul[(size_t)k * NV + i] = uv[q] + d;
+        const int f = (P - 1 - q) & 1; /* buffer alternates per step */
+        const T *cur = bc + f * 20;
+        T *nxt = bc + (f ^ 1) * 20;
+        const bool valid = !CHECK || (kbase + q >= 0 && kbase + q < len);
+        const int pos = cpos + kbase + q;
+        T yk = T(0);
+        if (valid) yk = YS ? ys[pos * NV + i] : yv[q];
+        const T d = row_dot(cur_row, cur, o, odd, yk);
+        if (writer && valid) {
+            nxt[i] = d;
+            nxt[11 + i] = d;
+            if (YS) {
+                ys[pos * NV + i] = d;
+            } else {
+                dUl[(size_t)pos * NV + i] = d;
+                Ul[(size_t)pos * NV + i] = uv[q] + d;
             }
-            gather_vec(v, d, o, odd ^ 1);
         }
+        __syncwarp();
         cur_row = next_row;
     }
 }
@@ -732,25 +818,35 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T (&v)[9], const T *ys, c
 template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(32) fast_thomas_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
-    const int *__restrict__ line_len, const T *__restrict__ G, const T *__restrict__ Gam,
-    const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU, T *__restrict__ U,
-    unsigned *status) {
+    const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
+    const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
+    T *__restrict__ U, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    const uint32_t stage = P * (NB + NV) * sizeof(T);
+    const uint32_t stage = 2 * P * (NB + NV) * sizeof(T);
+    const uint32_t half = P * (NB + NV) * sizeof(T);
     unsigned char *st0 = smem + 128;
-    T *ys = reinterpret_cast<T *>(st0 + (size_t)NS * stage);
+    /* broadcast: 2 halves x 2 alternating buffers x [copy A: 10][copy B: 10] */
+    T *bcall = reinterpret_cast<T *>(st0 + (size_t)NS * stage);
+    T *ys = bcall + 80;
     const int l = blockIdx.x;
     if (l >= nline) return;
     const int lane = threadIdx.x;
-    const int i = lane < NV ? lane : NV - 1;
-    const bool writer = lane < NV;
+    const int h = lane >> 4, li = lane & 15;
+    const int i = li < NV ? li : NV - 1;
+    const bool writer = li < NV;
     const LaneOff off = lane_offsets(i);
     const int ps = line_start[l];
     const int n = line_len[l];
-    const int npad = (n + 3) & ~3;
-    const int nch = (npad + P - 1) / P;
-    const int njobs = 2 * nch;
+    const int m = line_twist[l];
+    const int nb = n - 1 - m;
+    const int len = h ? nb : m;      /* this half's chain length */
+    const int cpos = h ? m : 0;      /* its first position, relative to ps */
+    const int nchT = (m + P - 1) / P, nchB = (nb + P - 1) / P;
+    const int nch = h ? nchB : nchT;
+    const int nf = nchT > nchB ? nchT : nchB;
+    const int njobs = 2 * nf;
+    T *bc = bcall + h * 40;
     T *yl = y + (size_t)ps * NV;
     T *dUl = dU + (size_t)ps * NV;
     T *Ul = U + (size_t)ps * NV;
@@ -759,25 +855,43 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
         for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
     }
+    for (int t = lane; t < 80; t += 32) bcall[t] = T(0);
     __syncwarp();
 
     uint64_t pol = 0;
     if (lane == 0) pol = policy_evict_first();
+    /* copy size of chunk c of a chain of length ln, rounded up to 4 cells
+     * (16-byte multiple); the extra cells stay inside the line's range */
+    auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
     auto issue = [&](int job, int s) {
         unsigned char *base = st0 + (size_t)s * stage;
-        if (job < nch) {
+        uint32_t bytes = 0;
+        if (job < nf) {
             const int c = job;
-            const int cnt = min(P, npad - c * P);
-            const uint32_t bg = cnt * NB * sizeof(T), bb = cnt * NV * sizeof(T);
-            mbar_arrive_expect_tx(&bars[s], bg + bb);
-            bulk_g2s_hint(base, G + (size_t)(ps + c * P) * NB, bg, &bars[s], pol);
-            bulk_g2s(base + P * NB * sizeof(T), b + (size_t)(ps + c * P) * NV, bb, &bars[s]);
+            if (c < nchT) bytes += cells(m, c) * (NB + NV) * sizeof(T);
+            if (c < nchB) bytes += cells(nb, c) * (NB + NV) * sizeof(T);
         } else {
-            const int c = njobs - 1 - job;
-            const int cnt = min(P, npad - c * P);
-            const uint32_t bg = cnt * NB * sizeof(T);
-            mbar_arrive_expect_tx(&bars[s], bg);
-            bulk_g2s_hint(base, Gam + (size_t)(ps + c * P) * NB, bg, &bars[s], pol);
+            const int jb = job - nf;
+            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * NB * sizeof(T);
+            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * NB * sizeof(T);
+        }
+        mbar_arrive_expect_tx(&bars[s], bytes);
+        for (int hh = 0; hh < 2; ++hh) {
+            const int ln = hh ? nb : m, nc = hh ? nchB : nchT, cp = hh ? m : 0;
+            unsigned char *hb = base + hh * half;
+            if (job < nf) {
+                const int c = job;
+                if (c >= nc) continue;
+                const int cnt = cells(ln, c);
+                bulk_g2s_hint(hb, G + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(T), &bars[s], pol);
+                bulk_g2s(hb + P * NB * sizeof(T), b + (size_t)(ps + cp + c * P) * NV, cnt * NV * sizeof(T),
+                         &bars[s]);
+            } else {
+                const int c = nc - 1 - (job - nf);
+                if (c < 0) continue;
+                const int cnt = cells(ln, c);
+                bulk_g2s_hint(hb, Gam + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(T), &bars[s], pol);
+            }
         }
     };
     int issued = 0;
@@ -786,13 +900,10 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     }
     int consumed = 0;
     bool timed_out = false;
-    const int nfull = n / P; /* chunks with P valid cells */
+    const int both_full = (m < nb ? m : nb) / P; /* jobs where both chains run P steps */
 
-    /* ---------------- forward: y_k = b_k - G_k y_{k-1} */
-    T v[9];
-#pragma unroll
-    for (int j = 0; j < 9; ++j) v[j] = T(0);
-    for (int c = 0; c < nch; ++c) {
+    /* ---------------- forward */
+    for (int c = 0; c < nf; ++c) {
         const int s = c % NS;
         const bool ok = mbar_wait(&bars[s], (uint32_t)((c / NS) & 1));
         if (__any_sync(FULL, !ok)) {
@@ -800,12 +911,12 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             break;
         }
         ++consumed;
-        const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
+        const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
         const T *sB = sG + P * NB;
-        if (c < nfull)
-            fwd_chunk<T, P, false, YS>(sG, sB, v, ys, yl, c * P, n, i, writer, off);
+        if (c < both_full)
+            fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, writer, off);
         else
-            fwd_chunk<T, P, true, YS>(sG, sB, v, ys, yl, c * P, n, i, writer, off);
+            fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, writer, off);
         __syncwarp();
         if (lane == 0 && issued < njobs) {
             issue(issued, s);
@@ -813,10 +924,36 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
         }
     }
 
-    /* ---------------- backward: dU_k = y_k - Gam_k dU_{k+1} */
     if (!timed_out) {
+        /* ---------------- twist: x_m = b_m - G_tw y_top - Gam_tw y_bot */
+        const int ptw = n - 1; /* relative to ps */
+        const T *ytop = bcall + 0 * 40 + (m & 1) * 20;
+        const T *ybot = bcall + 1 * 40 + (nb & 1) * 20;
+        T xm = T(0);
+        if (lane < NV) {
+            const T *gr = G + (size_t)(ps + ptw) * NB + NV * lane;
+            const T *cr = Gam + (size_t)(ps + ptw) * NB + NV * lane;
+            T acc = b[(size_t)(ps + ptw) * NV + lane];
 #pragma unroll
-        for (int j = 0; j < 9; ++j) v[j] = T(0);
+            for (int j = 0; j < NV; ++j) acc -= gr[j] * ytop[j] + cr[j] * ybot[j];
+            xm = acc;
+        }
+        __syncwarp();
+        if (lane < NV) {
+            for (int t = 0; t < 4; ++t) {
+                bcall[t * 20 + lane] = xm;
+                bcall[t * 20 + 11 + lane] = xm;
+            }
+            if (YS)
+                ys[ptw * NV + lane] = xm;
+            else {
+                dUl[(size_t)ptw * NV + lane] = xm;
+                Ul[(size_t)ptw * NV + lane] = (accumulate ? Ul[(size_t)ptw * NV + lane] : T(0)) + xm;
+            }
+        }
+        __syncwarp();
+
+        /* ---------------- backward */
         T yv[P], uv[P], nyv[P], nuv[P];
         auto load_chunk = [&](int c, T *yy, T *uu) {
 #pragma unroll
@@ -824,17 +961,17 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
                 const int k = c * P + q;
                 yy[q] = T(0);
                 uu[q] = T(0);
-                if (k < n && writer) {
-                    if (!YS) yy[q] = yl[(size_t)k * NV + i];
-                    if (accumulate) uu[q] = Ul[(size_t)k * NV + i];
+                if (!YS && c >= 0 && k < len && writer) {
+                    yy[q] = yl[(size_t)(cpos + k) * NV + i];
+                    if (accumulate) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
                 }
             }
         };
-        load_chunk(nch - 1, yv, uv);
-        for (int jb = 0; jb < nch; ++jb) {
-            const int job = nch + jb;
-            const int c = nch - 1 - jb;
-            if (c > 0) load_chunk(c - 1, nyv, nuv);
+        if (!YS) load_chunk(nch - 1, yv, uv);
+        for (int jb = 0; jb < nf; ++jb) {
+            const int job = nf + jb;
+            const int c = nch - 1 - jb; /* this half's chunk (may be < 0) */
+            if (!YS) load_chunk(c - 1, nyv, nuv);
             const int s = job % NS;
             const bool ok = mbar_wait(&bars[s], (uint32_t)((job / NS) & 1));
             if (__any_sync(FULL, !ok)) {
@@ -842,20 +979,33 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
                 break;
             }
             ++consumed;
-            const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
-            if (c < nfull)
-                bwd_chunk<T, P, false, YS>(sG, v, ys, yv, uv, dUl, Ul, c * P, n, i, writer, off);
+            const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
+            const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
+                              nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
+            if (full)
+                bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, Ul, c * P, len, cpos, i, writer, off);
             else
-                bwd_chunk<T, P, true, YS>(sG, v, ys, yv, uv, dUl, Ul, c * P, n, i, writer, off);
+                bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, Ul, c * P, len, cpos, i, writer, off);
             __syncwarp();
             if (lane == 0 && issued < njobs) {
                 issue(issued, s);
                 ++issued;
             }
+            if (!YS) {
 #pragma unroll
-            for (int q = 0; q < P; ++q) {
-                yv[q] = nyv[q];
-                uv[q] = nuv[q];
+                for (int q = 0; q < P; ++q) {
+                    yv[q] = nyv[q];
+                    uv[q] = nuv[q];
+                }
+            }
+        }
+        if (YS && !timed_out) {
+            /* dU = x, U (+)= x for the line's n cells, 16-byte accesses */
+            const int nv = n * NV;
+            for (int t = lane; t < nv; t += 32) {
+                const T x = ys[t];
+                dUl[t] = x;
+                Ul[t] = (accumulate ? Ul[t] : T(0)) + x;
             }
         }
     }
@@ -878,9 +1028,9 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
     const int per_sm = (L.nline + 147) / 148;
     const long long budget = 210LL * 1024 / (per_sm > 0 ? per_sm : 1);
     const size_t ys_bytes = (size_t)((L.max_len + 3) & ~3) * NV * sizeof(T);
-    const size_t fixed = 128;
+    const size_t fixed = 128 + 80 * sizeof(T);
     ThomasCfg c;
-    c.ys = (long long)(fixed + ys_bytes + 4 * sb) <= budget;
+    c.ys = (long long)(fixed + ys_bytes + 3 * sb) <= budget;
     long long left = budget - (long long)fixed - (c.ys ? (long long)ys_bytes : 0);
     long long ns = left / (long long)sb;
     if (ns > 8) ns = 8;
@@ -897,10 +1047,12 @@ int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T
     const ThomasCfg cfg = thomas_cfg<T>(L);
     if (cfg.ys)
         fast_thomas_kernel<T, THOMAS_P, true><<<L.nline, 32, cfg.smem, st>>>(
-            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
+            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
+            U, status);
     else
         fast_thomas_kernel<T, THOMAS_P, false><<<L.nline, 32, cfg.smem, st>>>(
-            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, G, Gam, b, y, dU, U, status);
+            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
+            U, status);
     return (int)cudaGetLastError();
 }
 

@@ -67,13 +67,25 @@ struct SolveState {
 };
 
 /* ------------------------------------------------- fast (line-ordered) layout
- * Positions p index cells in line order; every line starts at a multiple of
- * 4 positions (zero pad cells follow lines whose length is not a multiple
- * of 4) so that a run of 4 cells of 9x9 blocks (2592 B in FP64, 1296 B in
- * FP32) starts and ends on a 16-byte boundary, the rule for cp.async.bulk.
- * np16 = positions rounded up to a multiple of RES_TILE, the residual
- * kernel's tile. */
+ * Each line of n cells is solved as a twisted block-Thomas system: a top
+ * chain (cells 0..m-1, eliminated downward), a bottom chain (cells n-1
+ * down to m+1, eliminated upward) and the twist cell m where they meet.
+ * Positions p give every line a contiguous range starting at a multiple of
+ * 4: [top chain in order][bottom chain in elimination order][twist], then
+ * zero pad cells up to the next multiple of 4.  m is a multiple of 4, so
+ * both chains start 16-byte aligned for cp.async.bulk in FP64 and FP32
+ * (4 cells of 9x9 blocks = 2592 / 1296 B).  np16 = positions rounded up to
+ * a multiple of RES_TILE, the residual kernel's tile. */
 constexpr int RES_TILE = 16;
+
+/* twist cell of a line of n cells: the top chain gets m = 4*round((n-1)/8)
+ * cells, the bottom chain n-1-m */
+inline int line_twist_of(int n) {
+    if (n < 2) return 0;
+    int m = 4 * (int)((n - 1 + 4) / 8);
+    if (m > n - 1) m = n - 1 - ((n - 1) % 4);
+    return m;
+}
 
 struct FastLayout {
     int nv;        /* block size (9) */
@@ -83,13 +95,17 @@ struct FastLayout {
     int nline;
     int max_len;   /* longest line */
     /* device arrays */
-    int *line_start;   /* [nline] even */
+    int *line_start;   /* [nline] multiple of 4 */
     int *line_len;     /* [nline] */
+    int *line_twist;   /* [nline] m: top chain length (multiple of 4) */
     int *pos_of_elem;  /* [nelem] */
     int *elem_of_pos;  /* [np16], -1 for pads */
     int *xnbr;         /* [nx*np16] slot-major: neighbour position or -1 */
     int *xsrc;         /* [nx*np16] 2*face + (1 if the block is O2), or -1 */
-    int *fsrc;         /* [np16*3] factor sources: elem, face of A/C, side */
+    int *fsrc;         /* [np16*5] factor sources: elem, face to the chain
+                        * predecessor (-1 at a chain start), side (1 if elem is
+                        * fc[2f]); the twist position adds the face to its
+                        * bottom neighbour and its side (its top face in 1-2) */
 };
 
 /* ------------------------------------------------------ kernel launchers
@@ -129,7 +145,8 @@ int launch_permute_f32_to_elem(cudaStream_t st, int nv, int nelem, const int *po
 /* fast FP64 / FP32 kernels (kernels_fast.cu) */
 int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
                        const double *O1, const double *O2, double *Dinv, double *G, double *Gam,
-                       float *Dinv32, float *G32, float *Gam32, unsigned *status);
+                       float *Dinv32, float *G32, float *Gam32, double *gamlast,
+                       unsigned *status);
 int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, const double *O2,
                         double *X, float *X32);
 int fast_resid_grid(int np16);
