@@ -245,6 +245,25 @@ int tbs_profile_read(tbs_ctx *ctx, int *n, const char **names,
  * every array it must touch once), for the roofline numerator. */
 int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
 
+/* Linear residual R = rhs + J U (the rule of the reference's lineRes) and
+ * its 2-norm for nvar = 9, on device buffers owned by the caller, without
+ * allocating device memory -- for callers that cannot call cudaMalloc
+ * (a solver whose memory pool owns the GPU, a time loop that must not
+ * allocate).  No counterpart in the reference.  Arrays are device pointers
+ * in element order (epoint, ef, fc 0-based; jacD, jacO1, jacO2, rhs, U as
+ * in the Jacobian file); d_R may be NULL; *norm_out is written on the host
+ * (the call synchronises `cuda_stream`, NULL = legacy default stream).
+ * Its only work array is a fixed file-scope device array: at most 2,097,152
+ * cells (TBS_ERR_ARG beyond), kept by every GPU that loads the library
+ * until exit, shared by all calls (calls that overlap on the GPU race).
+ * The first call on a device looks up that array's address and should come
+ * before any stream capture. */
+int tbs_residual_noalloc(int device_id, void *cuda_stream, int nelem,
+                         const int *d_epoint, const int *d_ef, const int *d_fc,
+                         const double *d_jacD, const double *d_jacO1,
+                         const double *d_jacO2, const double *d_rhs,
+                         const double *d_U, double *d_R, double *norm_out);
+
 /* Library version string. */
 const char *tbs_version(void);
 

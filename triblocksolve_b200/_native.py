@@ -89,6 +89,7 @@ _sig("tbs_profile_enable", _i, _vp, _i)
 _sig("tbs_profile_reset", _i, _vp)
 _sig("tbs_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)
 _sig("tbs_kernel_bytes", _i, _vp, _cp, _dp)
+_sig("tbs_residual_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dp)
 
 
 class TbsError(RuntimeError):
