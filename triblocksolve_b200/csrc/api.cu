@@ -528,27 +528,31 @@ static int body(tbs_ctx *ctx, CondCtl cc) {
     }
     const FastLayout &L = ctx->L;
     if (ctx->algo == TBS_ALGO_FP64) {
+        /* the Thomas kernel writes dU; the residual kernel adds it to U */
         RUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
-                                                      ctx->d_dUp, ctx->d_Up, ctx->d_status, 1));
+                                                      ctx->d_dUp, ctx->d_Up, ctx->d_status, 2));
         RUN("fast_resid", launch_fast_resid<double>(st, L, 1, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
                                                     nullptr, ctx->d_b, sink(ctx, 0, cc),
-                                                    ctx->d_status));
+                                                    ctx->d_status, ctx->d_Up));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
      * FP64 residual R = rhs + J U from the original blocks */
     RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
                                                      ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status));
+    /* c = sum of the inner updates but the last: each inner residual kernel
+     * adds its sweep's d to c; the last d is added with c to U below */
+    CK(cudaMemsetAsync(ctx->d_c32, 0, (size_t)L.np16 * 9 * sizeof(float), st));
     for (int m = 0; m < ctx->inner_sweeps; ++m) {
         RUN("fast_thomas32", launch_fast_thomas<float>(st, L, ctx->d_G32, ctx->d_Gam32, ctx->d_b32,
                                                        ctx->d_y32, ctx->d_d32, ctx->d_c32,
-                                                       ctx->d_status, m > 0 ? 1 : 0));
+                                                       ctx->d_status, 2));
         if (m + 1 < ctx->inner_sweeps)
             RUN("fast_resid32", launch_fast_resid<float>(st, L, 1, ctx->d_Dinv32, ctx->d_X32,
                                                          ctx->d_d32, nullptr, ctx->d_b32, no_sink(),
-                                                         ctx->d_status));
+                                                         ctx->d_status, ctx->d_c32));
     }
-    RUN("axpy", launch_axpy_f32_f64(st, ctx->d_c32, ctx->d_Up, (long long)L.np16 * 9));
+    RUN("axpy", launch_axpy2_f32_f64(st, ctx->d_c32, ctx->d_d32, ctx->d_Up, (long long)L.np16 * 9));
     RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                ctx->d_rhs, ctx->d_Up, ctx->d_R32, ctx->d_partials));
@@ -1057,6 +1061,9 @@ static int get_vec(tbs_ctx *ctx, int which, double *out) {
             RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_dUp, ctx->d_scratch));
         } else {
             RUN("permute", launch_permute_f32_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_c32, ctx->d_scratch));
+            /* the outer correction is c + d (see body()); add d */
+            RUN("permute", launch_permute_f32_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_d32, ctx->d_R));
+            RUN("axpy", launch_axpy_f64(st, ctx->d_R, ctx->d_scratch, (long long)nvec(ctx)));
         }
         src = ctx->d_scratch;
     }
@@ -1176,18 +1183,18 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     const double X = (double)ctx->n_xslots_real;
     const std::string k(kernel);
     double b = -1.0;
-    if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out */
-        b = N * (blk + vec) + X * (blk + 4.0 + vec);
+    if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out, own dU + U in/out */
+        b = N * (blk + vec + 3 * vec) + X * (blk + 4.0 + vec);
     else if (k == "fast_resid_rhs") /* Dinv, R in, b out */
         b = N * (blk + 2 * vec);
     else if (k == "fast_resid32_rhs")
         b = N * (blk + 2 * vec) / 2;
     else if (k == "fast_resid32")
-        b = N * (blk + vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
-    else if (k == "fast_thomas") /* G, b, y out | Gam, y in, U in/out, dU out */
-        b = N * (2 * blk + 6 * vec);
+        b = N * (blk + 4 * vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
+    else if (k == "fast_thomas") /* G, b | Gam, dU out (y stays on chip when the line fits) */
+        b = N * (2 * blk + 2 * vec);
     else if (k == "fast_thomas32")
-        b = N * (2 * blk + 6 * vec) / 2;
+        b = N * (2 * blk + 2 * vec) / 2;
     else if (k == "full_resid") /* D, 2 blocks per face, U (own + nbrs), rhs, R out, ints */
         b = N * blk + 2 * F * blk + N * vec + 2 * F * vec + N * vec + N * vec / 2 +
             4.0 * (N + 1 + ctx->eftot + 2 * F + N);

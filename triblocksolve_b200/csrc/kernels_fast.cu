@@ -169,6 +169,13 @@ int launch_permute_f32_to_elem(cudaStream_t st, int nv, int nelem, const int *po
     return (int)cudaGetLastError();
 }
 
+template <typename T>
+__global__ void axpy_same_kernel(const T *__restrict__ d, T *__restrict__ U, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        U[t] += d[t];
+}
+
 __global__ void cast_kernel(const double *__restrict__ s, float *__restrict__ d, long long n) {
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
          t += (long long)gridDim.x * blockDim.x)
@@ -188,6 +195,23 @@ __global__ void axpy_kernel(const float *__restrict__ d, double *__restrict__ U,
 
 int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n) {
     axpy_kernel<<<grid_for(n, 256), 256, 0, st>>>(d, U, n);
+    return (int)cudaGetLastError();
+}
+
+__global__ void axpy2_kernel(const float *__restrict__ c, const float *__restrict__ d,
+                             double *__restrict__ U, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        U[t] += (double)c[t] + (double)d[t];
+}
+
+int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n) {
+    axpy_same_kernel<double><<<grid_for(n, 256), 256, 0, st>>>(d, U, n);
+    return (int)cudaGetLastError();
+}
+
+int launch_axpy2_f32_f64(cudaStream_t st, const float *c, const float *d, double *U, long long n) {
+    axpy2_kernel<<<grid_for(n, 256), 256, 0, st>>>(c, d, U, n);
     return (int)cudaGetLastError();
 }
 
@@ -504,10 +528,10 @@ __host__ __device__ inline size_t resid_smem_bytes(int nx) {
 }
 
 template <typename T>
-__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
+__device__ __forceinline__ void fast_resid_body(
     int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
-    T *__restrict__ b, NormSink ns, unsigned *status) {
+    T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     T *sD = reinterpret_cast<T *>(smem + 128);
@@ -538,6 +562,11 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
         } else {
             bulk_g2s(sr, Rsrc + (size_t)p0 * NV, szR, bar);
         }
+    }
+    if (mode == 1 && act && Uacc) {
+        /* U += dU of this tile (the Thomas kernel leaves U to this kernel) */
+        const size_t q = (size_t)p0 * NV + tid;
+        Uacc[q] += dU[q];
     }
     if (mode == 1 && act) {
         /* neighbour dU gathers overlap the bulk copies */
@@ -605,13 +634,35 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     }
 }
 
+/* mode 1 (R = sum X dU over the cross-line slots) */
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
+    int nx, int np16, const T *__restrict__ Dinv, const T *__restrict__ X,
+    const int *__restrict__ xnbr, const T *__restrict__ dU, T *__restrict__ b,
+    T *__restrict__ Uacc, NormSink ns, unsigned *status) {
+    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status);
+}
+
+/* mode 0 (R given in position order) */
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
+    int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
+    NormSink ns, unsigned *status) {
+    fast_resid_body<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, nullptr, ns, status);
+}
+
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv, const T *X,
-                      const T *dU, const T *Rsrc, T *b, const NormSink &ns, unsigned *status) {
+                      const T *dU, const T *Rsrc, T *b, const NormSink &ns, unsigned *status,
+                      T *Uacc) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     const int grid = fast_resid_grid(L.np16);
     if (mode == 1 && L.nx == 0) {
         /* a mesh that is one line: the line solve is exact, R_new = 0 */
+        if (Uacc) {
+            const long long n = (long long)L.np16 * NV;
+            axpy_same_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(dU, Uacc, n);
+        }
         mode = 0;
         Rsrc = nullptr;
     }
@@ -622,18 +673,21 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
         Rsrc = b;
     }
     const size_t smem = resid_smem_bytes<T>(mode == 1 ? L.nx : 0);
-    fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(mode == 1 ? L.nx : 0, L.np16, mode,
-                                                               Dinv, X, L.xnbr, dU, Rsrc, b, ns,
-                                                               status);
+    if (mode == 1)
+        fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr,
+                                                                   dU, b, Uacc, ns, status);
+    else
+        fast_resid_rhs_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b, ns,
+                                                                       status);
     return (int)cudaGetLastError();
 }
 
 template int launch_fast_resid<double>(cudaStream_t, const FastLayout &, int, const double *,
                                        const double *, const double *, const double *, double *,
-                                       const NormSink &, unsigned *);
+                                       const NormSink &, unsigned *, double *);
 template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, const float *,
                                       const float *, const float *, const float *, float *,
-                                      const NormSink &, unsigned *);
+                                      const NormSink &, unsigned *, float *);
 
 /* =========================================================== line Thomas
  * One warp per line, twisted: lanes 0..8 run the top chain and lanes
@@ -652,8 +706,10 @@ template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, con
  * YS: the line's y and x live in shared memory, and dU / U are written with
  * coalesced 16-byte accesses after the line is solved; otherwise y goes to
  * global memory (read back one chunk ahead) and dU / U per step.
- *   accumulate = 0:  U = dU  (first sweep of a solve, U starts at 0)
+ *   accumulate = 0:  U = dU
  *   accumulate = 1:  U += dU
+ *   accumulate = 2:  U untouched (the residual kernel that follows adds
+ *                    dU to U for its tile, with coalesced tile accesses)
  */
 constexpr int THOMAS_P = 8;
 
@@ -807,7 +863,7 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
                 ys[pos * NV + i] = d;
             } else {
                 dUl[(size_t)pos * NV + i] = d;
-                Ul[(size_t)pos * NV + i] = uv[q] + d;
+                if (Ul) Ul[(size_t)pos * NV + i] = uv[q] + d;
             }
         }
         __syncwarp();
@@ -948,7 +1004,8 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
                 ys[ptw * NV + lane] = xm;
             else {
                 dUl[(size_t)ptw * NV + lane] = xm;
-                Ul[(size_t)ptw * NV + lane] = (accumulate ? Ul[(size_t)ptw * NV + lane] : T(0)) + xm;
+                if (accumulate < 2)
+                    Ul[(size_t)ptw * NV + lane] = (accumulate ? Ul[(size_t)ptw * NV + lane] : T(0)) + xm;
             }
         }
         __syncwarp();
@@ -963,7 +1020,7 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
                 uu[q] = T(0);
                 if (!YS && c >= 0 && k < len && writer) {
                     yy[q] = yl[(size_t)(cpos + k) * NV + i];
-                    if (accumulate) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
+                    if (accumulate == 1) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
                 }
             }
         };
@@ -983,9 +1040,11 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
                               nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
             if (full)
-                bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, Ul, c * P, len, cpos, i, writer, off);
+                bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
+                                           c * P, len, cpos, i, writer, off);
             else
-                bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, Ul, c * P, len, cpos, i, writer, off);
+                bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
+                                          c * P, len, cpos, i, writer, off);
             __syncwarp();
             if (lane == 0 && issued < njobs) {
                 issue(issued, s);
@@ -1000,12 +1059,26 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             }
         }
         if (YS && !timed_out) {
-            /* dU = x, U (+)= x for the line's n cells, 16-byte accesses */
+            /* dU = x (and U = x or U += x) for the line's n cells; the U loads
+             * of a batch are issued together so that their latencies overlap */
             const int nv = n * NV;
-            for (int t = lane; t < nv; t += 32) {
-                const T x = ys[t];
-                dUl[t] = x;
-                Ul[t] = (accumulate ? Ul[t] : T(0)) + x;
+            constexpr int B = 8;
+            for (int t0 = lane; t0 < nv; t0 += 32 * B) {
+                T u[B];
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = t0 + 32 * k;
+                    u[k] = (accumulate == 1 && t < nv) ? Ul[t] : T(0);
+                }
+#pragma unroll
+                for (int k = 0; k < B; ++k) {
+                    const int t = t0 + 32 * k;
+                    if (t < nv) {
+                        const T x = ys[t];
+                        dUl[t] = x;
+                        if (accumulate < 2) Ul[t] = u[k] + x;
+                    }
+                }
             }
         }
     }

@@ -163,10 +163,11 @@ struct NormSink {
     unsigned long long handle;   /* cudaGraphConditionalHandle */
 };
 
+/* Uacc (mode 1, may be null): U += dU for the tile's positions */
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
                       const T *X, const T *dU, const T *Rsrc, T *b, const NormSink &ns,
-                      unsigned *status);
+                      unsigned *status, T *Uacc = nullptr);
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
                        const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
@@ -181,6 +182,8 @@ int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *
 /* mixed-precision glue (kernels_fast.cu) */
 int launch_cast_f64_f32(cudaStream_t st, const double *src, float *dst, long long n);
 int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n);
+int launch_axpy2_f32_f64(cudaStream_t st, const float *c, const float *d, double *U, long long n);
+int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
 
 }  // namespace tbs
 
