@@ -219,8 +219,8 @@ int launch_axpy2_f32_f64(cudaStream_t st, const float *c, const float *d, double
  * Twisted block Thomas.  Each line is split into a top chain (cells
  * 0..m-1, eliminated downward as in src/okl/lineLU_v2.okl:58-182), a
  * bottom chain (cells n-1 down to m+1, the same elimination run upward) and
- * the twist cell m.  One CTA of 128 threads per chain (grid = 2 x lines);
- * thread t < 81 owns entry t of each 9x9 block (row t%9, column t/9).  For
+ * the twist cell m.  One warp per chain (grid = 2 x lines); lane j < 9 owns
+ * column j of each 9x9 block.  For
  * chain step s >= 1 with A = block(row c_s, col c_{s-1}) and C =
  * block(row c_{s-1}, col c_s), both from the in-line face between them
  * (picked as in lineLU_v2.okl:116-117):
@@ -283,93 +283,152 @@ struct FactorOut {
     }
 };
 
-__global__ void __launch_bounds__(128) fast_factor_kernel(
+/* In-place Gauss-Jordan inverse of a 9x9 block distributed by columns:
+ * lane j < 9 holds column j in w[0..8].  Pivot column p is broadcast with
+ * shuffles; no pivoting, as the reference's LU has none. */
+__device__ __forceinline__ void gj_invert_cols(double (&w)[NV], int j, unsigned *status) {
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        double colp[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) colp[i] = __shfl_sync(FULL, w[i], p);
+        const double piv = colp[p];
+        if (threadIdx.x == 0 && !(fabs(piv) > 0.0 && isfinite(piv))) atomicOr(status, ST_PIVOT);
+        const double r = __drcp_rn(piv);
+        const bool isp = (j == p);
+        const double t = w[p] * r;
+#pragma unroll
+        for (int i = 0; i < NV; ++i)
+            if (i != p) w[i] = isp ? -colp[i] * r : w[i] - colp[i] * t;
+        w[p] = isp ? r : t;
+    }
+}
+
+/* One warp per chain (grid = 2 x lines), lane j < 9 owning column j of
+ * every block; the matrix that all lanes need in a product (Dinv_{s-1},
+ * A_s, Dinv_s) is published in shared memory and read by broadcast. */
+__global__ void __launch_bounds__(32) fast_factor_kernel(
     int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
     const int *__restrict__ line_twist, const int *__restrict__ fsrc,
     const double *__restrict__ jacD, const double *__restrict__ O1, const double *__restrict__ O2,
     FactorOut out, double *__restrict__ gamlast, unsigned *status) {
     const int l = blockIdx.x >> 1, g = blockIdx.x & 1;
     if (l >= nline) return;
-    const int t = threadIdx.x;
-    const bool act = t < NB;
-    const int i = t % NV, j = t / NV;
-    __shared__ double sW[NB], sPrev[NB], sA[NB], sC[NB], sGam[NB];
+    const int lane = threadIdx.x;
+    const int j = lane < NV ? lane : NV - 1;
+    const bool act = lane < NV;
+    __shared__ double sM[NB], sA[NB];
     const int ps = line_start[l], n = line_len[l], m = line_twist[l];
     const int len = g ? n - 1 - m : m;
     const int cs = ps + (g ? m : 0);
     const int ptw = ps + n - 1;
     if (len == 0) {
-        if (act) gamlast[((size_t)l * 2 + g) * NB + t] = 0.0;
+        for (int t = lane; t < NB; t += 32) gamlast[((size_t)l * 2 + g) * NB + t] = 0.0;
         return;
     }
-    double d = 0.0, a = 0.0, c = 0.0;
-    if (act) sW[t] = jacD[(size_t)fsrc[5 * cs] * NB + t];
-    __syncthreads();
-    gj_invert(sW, t, status);
-    if (act) {
-        const double w = sW[t];
-        out.put_dinv(cs, t, w);
-        out.put_g(cs, i, j, 0.0);
-        sPrev[t] = w;
+    double w[NV], an[NV], cn[NV], dn[NV];
+    {
+        const double *D0 = jacD + (size_t)fsrc[5 * cs] * NB + NV * j;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) w[i] = D0[i];
     }
     auto fetch = [&](int p) {
-        if (act) {
-            const int e = fsrc[5 * p], f = fsrc[5 * p + 1], side = fsrc[5 * p + 2];
-            a = (side ? O2 : O1)[(size_t)f * NB + t];
-            c = (side ? O1 : O2)[(size_t)f * NB + t];
-            d = jacD[(size_t)e * NB + t];
+        const int e = fsrc[5 * p], f = fsrc[5 * p + 1], side = fsrc[5 * p + 2];
+        const double *Ap = (side ? O2 : O1) + (size_t)f * NB + NV * j;
+        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * j;
+        const double *Dp = jacD + (size_t)e * NB + NV * j;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            an[i] = Ap[i];
+            cn[i] = Cp[i];
+            dn[i] = Dp[i];
         }
     };
     if (len > 1) fetch(cs + 1);
+    gj_invert_cols(w, j, status);
+    if (act) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            out.put_dinv(cs, i + NV * j, w[i]);
+            out.put_g(cs, i, j, 0.0);
+            sM[i + NV * j] = w[i];
+        }
+    }
     for (int s = 1; s < len; ++s) {
         const int p = cs + s;
-        __syncthreads();
-        if (act) {
-            sA[t] = a;
-            sC[t] = c;
-            sW[t] = d;
+        double a[NV], c[NV], d[NV];
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            a[i] = an[i];
+            c[i] = cn[i];
+            d[i] = dn[i];
         }
-        __syncthreads();
         if (s + 1 < len) fetch(p + 1);
-        if (act) {
-            double gm = 0.0;
+        __syncwarp();
+        /* Gam_{s-1}(:, j) = Dinv_{s-1} C(:, j) */
+        double gm[NV];
 #pragma unroll
-            for (int q = 0; q < NV; ++q) gm += sPrev[i + NV * q] * sC[q + NV * j];
-            out.put_gam(p - 1, i, j, gm);
-            sGam[t] = gm; /* Gam_{s-1}, column-major */
+        for (int i = 0; i < NV; ++i) {
+            double acc = 0.0;
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * c[q];
+            gm[i] = acc;
         }
-        __syncthreads();
         if (act) {
-            double w = sW[t];
 #pragma unroll
-            for (int q = 0; q < NV; ++q) w -= sA[i + NV * q] * sGam[q + NV * j];
-            sW[t] = w;
+            for (int i = 0; i < NV; ++i) {
+                out.put_gam(p - 1, i, j, gm[i]);
+                sA[i + NV * j] = a[i];
+            }
         }
-        __syncthreads();
-        gj_invert(sW, t, status);
-        if (act) {
-            double gk = 0.0;
+        __syncwarp();
+        /* W(:, j) = D(:, j) - A Gam_{s-1}(:, j) */
 #pragma unroll
-            for (int q = 0; q < NV; ++q) gk += sW[i + NV * q] * sA[q + NV * j];
-            out.put_g(p, i, j, gk);
-            const double w = sW[t];
-            out.put_dinv(p, t, w);
-            sPrev[t] = w;
+        for (int i = 0; i < NV; ++i) {
+            double acc = d[i];
+#pragma unroll
+            for (int q = 0; q < NV; ++q) acc -= sA[i + NV * q] * gm[q];
+            w[i] = acc;
+        }
+        gj_invert_cols(w, j, status);
+        __syncwarp();
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                out.put_dinv(p, i + NV * j, w[i]);
+                sM[i + NV * j] = w[i];
+            }
+        }
+        __syncwarp();
+        /* G_s(:, j) = Dinv_s A(:, j) */
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * a[q];
+                out.put_g(p, i, j, acc);
+            }
         }
     }
-    /* coupling of the chain's last cell to the twist: block(row last, col m) */
-    __syncthreads();
-    if (act) {
+    /* coupling of the chain's last cell to the twist: Gam = Dinv_last block(row last, col m) */
+    {
         const int f = fsrc[5 * ptw + (g ? 3 : 1)], side = fsrc[5 * ptw + (g ? 4 : 2)];
-        sC[t] = (side ? O1 : O2)[(size_t)f * NB + t];
-    }
-    __syncthreads();
-    if (act) {
-        double gm = 0.0;
+        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * j;
+        double c[NV];
 #pragma unroll
-        for (int q = 0; q < NV; ++q) gm += sPrev[i + NV * q] * sC[q + NV * j];
-        out.put_gam(cs + len - 1, i, j, gm);
-        gamlast[((size_t)l * 2 + g) * NB + t] = gm; /* column-major, FP64 */
+        for (int i = 0; i < NV; ++i) c[i] = Cp[i];
+        __syncwarp();
+        if (act) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) {
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * c[q];
+                out.put_gam(cs + len - 1, i, j, acc);
+                gamlast[((size_t)l * 2 + g) * NB + i + NV * j] = acc; /* column-major, FP64 */
+            }
+        }
     }
 }
 
@@ -425,8 +484,8 @@ int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
                        float *G32, float *Gam32, double *gamlast, unsigned *status) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     FactorOut out{Dinv, G, Gam, Dinv32, G32, Gam32};
-    fast_factor_kernel<<<2 * L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.line_twist,
-                                                    L.fsrc, jacD, O1, O2, out, gamlast, status);
+    fast_factor_kernel<<<2 * L.nline, 32, 0, st>>>(L.nline, L.line_start, L.line_len, L.line_twist,
+                                                   L.fsrc, jacD, O1, O2, out, gamlast, status);
     fast_twist_kernel<<<L.nline, 128, 0, st>>>(L.nline, L.line_start, L.line_len, L.line_twist,
                                                L.fsrc, jacD, O1, O2, out, gamlast, status);
     return (int)cudaGetLastError();
