@@ -263,6 +263,9 @@ def main():
     torch.cuda.synchronize()
     factor_ms = f0.elapsed_time(f1)
     max_sweeps = 400
+    inner = None
+    if args.algo == "mixed":
+        inner, _ = solver.tune_inner(tol, max_sweeps)
 
     with ClockSampler(local) as clocks:
         for _ in range(max(args.warmup, 0)):
@@ -378,6 +381,7 @@ def main():
                             f"algo {args.algo}",
                 "cells": mesh.nelem, "lines": L, "cells_per_line": K, "tol": tol,
                 "algo": args.algo, "sweeps_per_solve": sweeps_per_solve,
+                "inner_sweeps": inner,
                 "time_to_tol_ms": round(max_ms / args.steps, 4),
                 "factor_ms": round(factor_ms, 3),
                 "true_rel_residual": true_rel,

@@ -232,6 +232,12 @@ int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes);
  * (default 4, range 1..64). */
 int tbs_set_inner_sweeps(tbs_ctx *ctx, int m);
 
+/* Autotuner for TBS_ALGO_MIXED: times a solve to rel_tol on the device for
+ * each inner sweep count in {2,3,4,5,6,8,10}, keeps the fastest that
+ * converges (set in the context) and reports it and its time in ms. */
+int tbs_tune_inner(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *best_m,
+                   double *best_ms);
+
 /* Per-kernel CUDA-event timing.  While enabled, every launch is bracketed
  * by events on the launching stream; tbs_profile_read returns, for kernel
  * slot k < *n, its name, launch count and total milliseconds. */

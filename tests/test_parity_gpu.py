@@ -155,3 +155,25 @@ def test_checkpoint_resume(solver):
         assert np.linalg.norm(solver.solution() - r["U"]) <= 1e-12 * np.linalg.norm(r["U"])
         assert abs(h[-1] - r["hist"][-1]) <= 1e-12 * r["hist"][0]
         solver.set_initial(None)
+
+
+@pytest.mark.parametrize("case", ["ragged", "single_line", "odd_lines", "single_cells"])
+def test_mixed_other_meshes(solver, case):
+    mesh = CASES[case]()
+    jac = Jacobian.generate(mesh, 6.0, 8)
+    setup(solver, mesh, jac, ALGO_MIXED)
+    sweeps, h = solver.solve(1e-10, 60)
+    assert h[-1] <= 1e-10 * h[0]
+    assert solver.true_residual_norm() <= 1.0000001e-10 * h[0]
+    r = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, 40)
+    assert np.linalg.norm(solver.solution() - r["U"]) <= 1e-9 * np.linalg.norm(r["U"])
+
+
+def test_tune_inner_picks_a_converging_count(solver):
+    mesh = Mesh.structured(40, 48)
+    jac = Jacobian.generate(mesh, 4.0, 2)
+    setup(solver, mesh, jac, ALGO_MIXED)
+    m, ms = solver.tune_inner(1e-10, 60)
+    assert m in (2, 3, 4, 5, 6, 8, 10) and ms > 0
+    sweeps, h = solver.solve(1e-10, 60)
+    assert h[-1] <= 1e-10 * h[0]

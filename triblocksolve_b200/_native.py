@@ -85,6 +85,7 @@ _sig("tbs_get_update", _i, _vp, _dp)
 _sig("tbs_true_residual_norm", _i, _vp, _dp)
 _sig("tbs_memory_allocated", _i, _vp, C.POINTER(C.c_size_t))
 _sig("tbs_set_inner_sweeps", _i, _vp, _i)
+_sig("tbs_tune_inner", _i, _vp, C.c_double, _i, _ip, _dp)
 _sig("tbs_profile_enable", _i, _vp, _i)
 _sig("tbs_profile_reset", _i, _vp)
 _sig("tbs_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)

@@ -548,8 +548,8 @@ static int body(tbs_ctx *ctx, CondCtl cc) {
                                                        ctx->d_y32, ctx->d_d32, ctx->d_c32,
                                                        ctx->d_status, 2));
         if (m + 1 < ctx->inner_sweeps)
-            RUN("fast_resid32", launch_fast_resid<float>(st, L, 1, ctx->d_Dinv32, ctx->d_X32,
-                                                         ctx->d_d32, nullptr, ctx->d_b32, no_sink(),
+            RUN("fast_resid32", launch_fast_resid<float>(st, L, 3, nullptr, ctx->d_X32, ctx->d_d32,
+                                                         nullptr, ctx->d_b32, no_sink(),
                                                          ctx->d_status, ctx->d_c32));
     }
     RUN("axpy", launch_axpy2_f32_f64(st, ctx->d_c32, ctx->d_d32, ctx->d_Up, (long long)L.np16 * 9));
@@ -689,10 +689,11 @@ static int alloc_algo(tbs_ctx *ctx, int algo) {
         DA(ctx->d_b, npv);
         DA(ctx->d_y, npv);
     } else {
+        DA(ctx->d_Dinv, npb); /* FP64 inverse, input of the premultiplied DX blocks */
         DA(ctx->d_Dinv32, npb);
         DA(ctx->d_G32, npb);
         DA(ctx->d_Gam32, npb);
-        DA(ctx->d_X32, nxb);
+        DA(ctx->d_X32, nxb); /* holds DX = Dinv X in FP32 */
         DA(ctx->d_b32, npv);
         DA(ctx->d_y32, npv);
         DA(ctx->d_d32, npv);
@@ -728,10 +729,10 @@ static int run_factor(tbs_ctx *ctx, int algo) {
                                               ctx->d_gamlast, ctx->d_status));
         RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, ctx->d_X, nullptr));
     } else {
-        RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, nullptr,
+        RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,
                                               nullptr, nullptr, ctx->d_Dinv32, ctx->d_G32,
                                               ctx->d_Gam32, ctx->d_gamlast, ctx->d_status));
-        RUN("fast_xlayout", launch_fast_xlayout(st, L, ctx->d_O1, ctx->d_O2, nullptr, ctx->d_X32));
+        RUN("fast_dx", launch_fast_dx(st, L, ctx->d_Dinv, ctx->d_O1, ctx->d_O2, ctx->d_X32));
     }
     return TBS_OK;
 }
@@ -1144,6 +1145,57 @@ int tbs_set_inner_sweeps(tbs_ctx *ctx, int m) {
     return TBS_OK;
 }
 
+int tbs_tune_inner(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *best_m, double *best_ms) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored || ctx->algo != TBS_ALGO_MIXED)
+        return ctx_fail(ctx, TBS_ERR_STATE, "tbs_tune_inner needs a TBS_ALGO_MIXED factorization");
+    const int cand[] = {2, 3, 4, 5, 6, 8, 10};
+    const bool prof = ctx->prof;
+    ctx->prof = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    int best = -1;
+    double best_t = 0.0;
+    int rc = TBS_OK;
+    for (int m : cand) {
+        if (rc) break;
+        rc = tbs_set_inner_sweeps(ctx, m);
+        int sw = 0;
+        if (!rc) rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr); /* builds the graph */
+        double t = 1e300;
+        for (int rep = 0; rep < 2 && !rc; ++rep) {
+            cudaEventRecord(e0, ctx->stream);
+            rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr);
+            cudaEventRecord(e1, ctx->stream);
+            cudaEventSynchronize(e1);
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, e0, e1);
+            t = std::min(t, (double)ms);
+        }
+        if (rc) break;
+        const SolveState &S = *ctx->h_state;
+        const bool conv = std::isfinite(S.last) && S.last <= S.tol * S.norm0;
+        if (conv && (best < 0 || t < best_t)) {
+            best = m;
+            best_t = t;
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    ctx->prof = prof;
+    if (rc) return rc;
+    if (best < 0) return ctx_fail(ctx, TBS_ERR_NUMERIC, "no inner sweep count reached the tolerance");
+    rc = tbs_set_inner_sweeps(ctx, best);
+    if (rc) return rc;
+    if (best_m) *best_m = best;
+    if (best_ms) *best_ms = best_t;
+    return TBS_OK;
+    GUARD_END
+}
+
 int tbs_profile_enable(tbs_ctx *ctx, int on) {
     if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
     if (!on) prof_resolve(ctx);
@@ -1189,8 +1241,8 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
         b = N * (blk + 2 * vec);
     else if (k == "fast_resid32_rhs")
         b = N * (blk + 2 * vec) / 2;
-    else if (k == "fast_resid32")
-        b = N * (blk + 4 * vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
+    else if (k == "fast_resid32") /* DX blocks, xnbr, neighbour d, b out, own d + c in/out */
+        b = N * (4 * vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
     else if (k == "fast_thomas") /* G, b | Gam, dU out (y stays on chip when the line fits) */
         b = N * (2 * blk + 2 * vec);
     else if (k == "fast_thomas32")

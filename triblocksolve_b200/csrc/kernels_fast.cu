@@ -491,6 +491,46 @@ int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
     return (int)cudaGetLastError();
 }
 
+/* DX[q] = Dinv(p) X(q) for slot q = s*np16 + p, rounded once to FP32, from
+ * the FP64 inverse and the original FP64 face block; one warp per slot */
+__global__ void __launch_bounds__(256) fast_dx_kernel(long long nslots, int np16,
+                                                      const int *__restrict__ xsrc,
+                                                      const double *__restrict__ Dinv,
+                                                      const double *__restrict__ O1,
+                                                      const double *__restrict__ O2,
+                                                      float *__restrict__ DX) {
+    __shared__ double sm[8][2 * NB];
+    const int lane = threadIdx.x & 31, wb = threadIdx.x >> 5;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    double *sD = sm[wb], *sX = sm[wb] + NB;
+    for (long long q = w0; q < nslots; q += nw) {
+        const int src = xsrc[q];
+        const long long p = q % np16;
+        __syncwarp();
+        for (int t = lane; t < NB; t += 32) {
+            sD[t] = Dinv[p * NB + t];
+            sX[t] = src >= 0 ? ((src & 1) ? O2 : O1)[(size_t)(src >> 1) * NB + t] : 0.0;
+        }
+        __syncwarp();
+        for (int t = lane; t < NB; t += 32) {
+            const int i = t % NV, j = t / NV;
+            double acc = 0.0;
+#pragma unroll
+            for (int k = 0; k < NV; ++k) acc += sD[i + NV * k] * sX[k + NV * j];
+            DX[q * NB + t] = (float)acc;
+        }
+    }
+}
+
+int launch_fast_dx(cudaStream_t st, const FastLayout &L, const double *Dinv, const double *O1,
+                   const double *O2, float *DX) {
+    const long long nslots = (long long)L.np16 * L.nx;
+    if (nslots == 0) return 0;
+    fast_dx_kernel<<<grid_for(nslots * 32, 256), 256, 0, st>>>(nslots, L.np16, L.xsrc, Dinv, O1, O2, DX);
+    return (int)cudaGetLastError();
+}
+
 /* X[q] = cross-line block of slot q = s*np16 + p (slot-major), or zeros;
  * one warp per slot */
 __global__ void fast_xlayout_kernel(long long nslots, const int *__restrict__ xsrc,
@@ -612,22 +652,22 @@ __device__ __forceinline__ void fast_resid_body(
     __syncthreads();
     if (tid == 0) {
         const uint64_t pol = policy_evict_first();
-        const uint32_t bytes = szD + (mode == 1 ? nx * szD : szR);
+        const uint32_t bytes = (mode == 3 ? 0u : szD) + (mode >= 1 ? nx * szD : szR);
         mbar_arrive_expect_tx(bar, bytes);
-        bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
-        if (mode == 1) {
+        if (mode != 3) bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+        if (mode >= 1) {
             for (int s = 0; s < nx; ++s)
                 bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
         } else {
             bulk_g2s(sr, Rsrc + (size_t)p0 * NV, szR, bar);
         }
     }
-    if (mode == 1 && act && Uacc) {
+    if (mode >= 1 && act && Uacc) {
         /* U += dU of this tile (the Thomas kernel leaves U to this kernel) */
         const size_t q = (size_t)p0 * NV + tid;
         Uacc[q] += dU[q];
     }
-    if (mode == 1 && act) {
+    if (mode >= 1 && act) {
         /* neighbour dU gathers overlap the bulk copies */
         for (int s = 0; s < nx; ++s) {
             const int nb = xnbr[(size_t)s * np16 + p0 + c];
@@ -643,7 +683,7 @@ __device__ __forceinline__ void fast_resid_body(
         return;
     }
     T r = T(0);
-    if (mode == 1) {
+    if (mode >= 1) {
         if (act) {
             T a0 = T(0), a1 = T(0), a2 = T(0);
             for (int s = 0; s < nx; ++s) {
@@ -667,7 +707,10 @@ __device__ __forceinline__ void fast_resid_body(
         r = sr[c * NV + i];
     }
     double sq = act ? (double)r * (double)r : 0.0;
-    if (act) {
+    if (mode == 3) {
+        /* X held Dinv X: r is already Dinv R */
+        if (act) sb[c * NV + i] = -r;
+    } else if (act) {
         const T *dr = sD + c * NB + i;
         const T *rv = sr + c * NV;
         T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
@@ -702,6 +745,14 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status);
 }
 
+/* mode 3 (b = -sum (Dinv X) dU: premultiplied cross-line blocks, no norm) */
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_dx_kernel(
+    int nx, int np16, const T *__restrict__ DX, const int *__restrict__ xnbr,
+    const T *__restrict__ dU, T *__restrict__ b, T *__restrict__ Uacc, unsigned *status) {
+    fast_resid_body<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status);
+}
+
 /* mode 0 (R given in position order) */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
@@ -716,23 +767,25 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
                       T *Uacc) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     const int grid = fast_resid_grid(L.np16);
-    if (mode == 1 && L.nx == 0) {
+    if (mode >= 1 && L.nx == 0) {
         /* a mesh that is one line: the line solve is exact, R_new = 0 */
         if (Uacc) {
             const long long n = (long long)L.np16 * NV;
             axpy_same_kernel<T><<<grid_for(n, 256), 256, 0, st>>>(dU, Uacc, n);
         }
-        mode = 0;
-        Rsrc = nullptr;
-    }
-    if (mode == 0 && !Rsrc) {
         cudaMemsetAsync(b, 0, (size_t)L.np16 * NV * sizeof(T), st);
-        /* still run the kernel so that the norm bookkeeping happens: a zero
-         * residual read from b itself */
+        if (mode == 3) return (int)cudaGetLastError(); /* no norm wanted */
+        /* run the kernel on a zero residual (read from b itself) so that the
+         * norm bookkeeping happens */
+        mode = 0;
         Rsrc = b;
     }
-    const size_t smem = resid_smem_bytes<T>(mode == 1 ? L.nx : 0);
-    if (mode == 1)
+    if (mode == 0 && !Rsrc) return (int)cudaErrorInvalidValue;
+    const size_t smem = resid_smem_bytes<T>(mode >= 1 ? L.nx : 0);
+    if (mode == 3)
+        fast_resid_dx_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, X, L.xnbr, dU,
+                                                                      b, Uacc, status);
+    else if (mode == 1)
         fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr,
                                                                    dU, b, Uacc, ns, status);
     else
@@ -784,7 +837,8 @@ __host__ __device__ inline uint32_t thomas_stage_bytes() {
 /* Lane constants for rows whose start parity is (q + i) & 1: pairs start at
  * row+par, the single element is row[8] (par 0) or row[0] (par 1); the
  * broadcast vector is read from copy A (offset 0) or copy B (offset 10,
- * holding y_j at 11+j) so that the pairs line up. */
+ * holding y_j at 11+j) so that the pairs line up.  The same scheme serves
+ * FP64 (16-byte pairs) and FP32 (8-byte pairs). */
 struct LaneOff {
     int row;
     int rp[2], rs[2], vp[2], vs[2];
@@ -808,7 +862,8 @@ struct RowD {
     double s;
 };
 struct RowF {
-    float r[9];
+    float2 r0, r1, r2, r3;
+    float s;
 };
 template <typename T> struct RowOf;
 template <> struct RowOf<double> { using type = RowD; };
@@ -823,9 +878,13 @@ __device__ __forceinline__ void load_row(RowD &R, const double *rowbase, const L
     R.s = rowbase[o.rs[odd]];
 }
 
-__device__ __forceinline__ void load_row(RowF &R, const float *rowbase, const LaneOff &o, int) {
-#pragma unroll
-    for (int j = 0; j < 9; ++j) R.r[j] = rowbase[o.row + j];
+__device__ __forceinline__ void load_row(RowF &R, const float *rowbase, const LaneOff &o, int odd) {
+    const float2 *r = reinterpret_cast<const float2 *>(rowbase + o.rp[odd]);
+    R.r0 = r[0];
+    R.r1 = r[1];
+    R.r2 = r[2];
+    R.r3 = r[3];
+    R.s = rowbase[o.rs[odd]];
 }
 
 /* init - row . vec, vec from the broadcast buffer `cur` */
@@ -846,19 +905,21 @@ __device__ __forceinline__ double row_dot(const RowD &R, const double *cur, cons
     return a0 - (a1 + a2);
 }
 
-__device__ __forceinline__ float row_dot(const RowF &R, const float *cur, const LaneOff &, int,
-                                         float init) {
-    float a0 = init, a1 = 0.f, a2 = 0.f;
-    a0 -= R.r[0] * cur[0];
-    a1 -= R.r[1] * cur[1];
-    a2 -= R.r[2] * cur[2];
-    a0 -= R.r[3] * cur[3];
-    a1 -= R.r[4] * cur[4];
-    a2 -= R.r[5] * cur[5];
-    a0 -= R.r[6] * cur[6];
-    a1 -= R.r[7] * cur[7];
-    a2 -= R.r[8] * cur[8];
-    return a0 + (a1 + a2);
+__device__ __forceinline__ float row_dot(const RowF &R, const float *cur, const LaneOff &o,
+                                         int odd, float init) {
+    const float2 *v = reinterpret_cast<const float2 *>(cur + o.vp[odd]);
+    const float2 v0 = v[0], v1 = v[1], v2 = v[2], v3 = v[3];
+    const float w = cur[o.vs[odd]];
+    float a0 = init - R.s * w;
+    float a1 = R.r0.x * v0.x;
+    float a2 = R.r0.y * v0.y;
+    a0 -= R.r1.x * v1.x;
+    a1 += R.r1.y * v1.y;
+    a2 += R.r2.x * v2.x;
+    a0 -= R.r2.y * v2.y;
+    a1 += R.r3.x * v3.x;
+    a2 += R.r3.y * v3.y;
+    return a0 - (a1 + a2);
 }
 
 /* Forward steps kbase..kbase+P-1 of this half's chain (length len, first

@@ -149,6 +149,9 @@ int launch_fast_factor(cudaStream_t st, const FastLayout &L, const double *jacD,
                        unsigned *status);
 int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, const double *O2,
                         double *X, float *X32);
+/* DX = Dinv X per cross-line slot, FP32 (TBS_ALGO_MIXED inner sweeps) */
+int launch_fast_dx(cudaStream_t st, const FastLayout &L, const double *Dinv, const double *O1,
+                   const double *O2, float *DX);
 int fast_resid_grid(int np16);
 /* Where a streaming kernel's sum of R^2 goes: per-CTA partials, and, when
  * `state` is set, the last CTA's fixed-order total recorded like
@@ -163,7 +166,9 @@ struct NormSink {
     unsigned long long handle;   /* cudaGraphConditionalHandle */
 };
 
-/* Uacc (mode 1, may be null): U += dU for the tile's positions */
+/* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
+ * b = -sum X dU, no norm.  Uacc (modes 1, 3; may be null): U += dU for the
+ * tile's positions */
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
                       const T *X, const T *dU, const T *Rsrc, T *b, const NormSink &ns,

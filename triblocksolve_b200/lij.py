@@ -285,6 +285,13 @@ class Solver:
     def set_inner_sweeps(self, m: int):
         self._chk(N.lib.tbs_set_inner_sweeps(self.ctx, m))
 
+    def tune_inner(self, rel_tol: float, max_sweeps: int = 100):
+        """Pick the fastest FP32 inner sweep count for TBS_ALGO_MIXED (device timing)."""
+        m = C.c_int()
+        ms = C.c_double()
+        self._chk(N.lib.tbs_tune_inner(self.ctx, rel_tol, max_sweeps, C.byref(m), C.byref(ms)))
+        return m.value, ms.value
+
     def factor(self, algo: int = N.ALGO_FP64):
         self._chk(N.lib.tbs_factor(self.ctx, algo))
 
