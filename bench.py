@@ -42,6 +42,10 @@ CONFIGS = {
     "c3b": (1200, 1280, 4.0, 1e-10),
 }
 SEED = 1
+# batched uneven systems: 64 meshes, lines log-uniform in [60, 1200], cells per line
+# log-uniform in [32, 1280], shift 9, tolerance 1e-10
+BATCH_CONFIGS = {"c4": {"nsys": 64, "L": (60, 1200), "K": (32, 1280), "shift": 9.0,
+                        "tol": 1e-10, "seed": 4}}
 # paper Table 5 (V100, FP64): 5 LIJ iterations on ex06 (138,240 cells) in 8.470 ms
 PUBLISHED_SWEEPS_PER_S = {"c2": 5 / 0.008470, "c3a": 5 / 0.018741, "c3b": 5 / 0.076733}
 
@@ -190,6 +194,237 @@ def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
             "factor_s": t_factor, "seconds": dt}
 
 
+def batch_shapes(cfg):
+    """Seeded (lines, cells per line) of every system of a batched workload."""
+    rng = np.random.default_rng(cfg["seed"])
+    lo, hi = cfg["L"]
+    Ls = np.exp(rng.uniform(np.log(lo), np.log(hi), cfg["nsys"])).round().astype(int)
+    lo, hi = cfg["K"]
+    Ks = np.exp(rng.uniform(np.log(lo), np.log(hi), cfg["nsys"])).round().astype(int)
+    return [(int(a), int(b)) for a, b in zip(Ls, Ks)]
+
+
+def run_batch(args):
+    """A step is one batched solve of all systems from U = 0 to the tolerance."""
+    import torch
+
+    import triblocksolve_b200 as tbs
+    from triblocksolve_b200 import _native as N
+    cfg = BATCH_CONFIGS[args.config]
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    algo = {"fp64": tbs.ALGO_FP64, "mixed": tbs.ALGO_MIXED}[args.algo]
+    tol, shift = cfg["tol"], cfg["shift"]
+    shapes = batch_shapes(cfg)
+    solvers, meshes, rhs_h = [], [], []
+    t_setup = time.perf_counter()
+    for k, (L, K) in enumerate(shapes):
+        mesh = tbs.Mesh.structured(L, K)
+        nb = 81
+        jacD = np.empty(nb * mesh.nelem)
+        O1 = np.empty(nb * mesh.nintface)
+        O2 = np.empty(nb * mesh.nintface)
+        rhs = torch.empty(9 * mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
+        N.check(N.lib.tbs_gen_jacobian(9, mesh.nelem, mesh.nintface, shift, 1000 * SEED + k,
+                                       N.dptr(jacD), N.dptr(O1), N.dptr(O2), N.dptr(rhs), None))
+        s = tbs.Solver(local)
+        s.set_mesh(mesh)
+        s.set_jacobian_arrays(jacD, O1, O2, rhs)
+        s.factor(algo)
+        del jacD, O1, O2
+        solvers.append(s)
+        meshes.append(mesh)
+        rhs_h.append(rhs)
+    setup_s = time.perf_counter() - t_setup
+    batch = tbs.Batch(solvers)
+    # a dedicated stream for the batch's graph launches, visible to the CUDA events
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    batch.set_stream(stream.cuda_stream)
+    footprint = sum(s.memory_allocated() for s in solvers)
+    cells = np.array([m.nelem for m in meshes], dtype=np.int64)
+    max_sweeps = 400
+    inner = None
+    if args.algo == "mixed":
+        inner = 3
+        batch.set_inner_sweeps(inner)
+    ctas, stages, order, tune_ms = batch.tune()
+    with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 0)):
+            batch.solve(tol, max_sweeps)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record(stream)
+        cell_sweeps = 0
+        sw = None
+        for _ in range(args.steps):
+            sw, hist = batch.solve(tol, max_sweeps)
+            cell_sweeps += int((cells * sw).sum())
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        elapsed_ms = ev0.elapsed_time(ev1)
+        batch.profile(True)
+        batch.profile_reset()
+        nprof = max(1, min(args.steps, 3))
+        for _ in range(nprof):
+            swp, _h = batch.solve(tol, max_sweeps)
+        prof = batch.profile_read()
+        batch.profile(False)
+        # e2e: new right-hand sides from pinned host memory, batched solve, solutions back
+        ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 5))
+        sol_h = [torch.empty(9 * m.nelem, dtype=torch.float64, pin_memory=True).numpy()
+                 for m in meshes]
+        for s in solvers:
+            s.set_stream(stream.cuda_stream)
+        torch.cuda.synchronize()
+        ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev2.record(stream)
+        e2e_cs = 0
+        for _ in range(ne2e):
+            for s, r in zip(solvers, rhs_h):
+                s.set_rhs(r)
+            swe, _h = batch.solve(tol, max_sweeps)
+            for s, u in zip(solvers, sol_h):
+                N.check(N.lib.tbs_get_solution(s.ctx, N.dptr(u)), s.ctx)
+            e2e_cs += int((cells * swe).sum())
+        ev3.record(stream)
+        torch.cuda.synchronize()
+        e2e_ms = ev2.elapsed_time(ev3)
+    clk = clocks.summary()
+    max_ms = dist.reduce(elapsed_ms, "max")
+    all_cs = dist.reduce(cell_sweeps, "sum")
+    max_e2e = dist.reduce(e2e_ms, "max")
+    all_e2e = dist.reduce(e2e_cs, "sum")
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        kern = {}
+        names = {"fast_thomas": "fast_thomas", "fast_resid": "fast_resid",
+                 "fast_thomas32": "fast_thomas32", "fast_resid32": "fast_resid32",
+                 "full_resid": "full_resid", "fast_resid32_rhs": "fast_resid32_rhs"}
+        for name, (launches, ms) in prof.items():
+            b = None
+            if name in names:
+                # every system contributes its bytes once per launch in each sweep it runs
+                per_sweep = {"fast_thomas32": inner, "fast_resid32": (inner or 1) - 1}.get(name, 1)
+                b = nprof * per_sweep * sum(s.kernel_bytes(name) * int(n_sw)
+                                            for s, n_sw in zip(solvers, swp))
+            kern[name] = {"launches": launches, "total_ms": round(ms, 3),
+                          "avg_us": round(1e3 * ms / launches, 2) if launches else None,
+                          "bytes_total": b,
+                          "gbs": round(b / (ms * 1e-3) / 1e9, 1) if b and ms > 0 else None}
+        hot = [k for k in kern if kern[k]["bytes_total"]]
+        dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
+        roof = None
+        if dom:
+            ach = kern[dom]["gbs"]
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "traffic": None,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes": "sum over systems of the kernel's bytes x sweeps run",
+                    "avg_launch_us": kern[dom]["avg_us"]}
+        launches_per_solve = sum(v["launches"] for v in kern.values()) / nprof
+        value = all_cs / (max_ms * 1e-3)
+        line = {
+            "metric": "batched LIJ cell-sweeps/s", "value": round(value, 1), "unit": "cell-sweeps/s",
+            "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.algo == "fp64" else "f32+f64",
+            "data": "synthetic: seeded structured meshes and values (shift %g)" % shift,
+            "config": {
+                "workload": f"{len(shapes)} independent LIJ systems solved together to {tol:g} "
+                            f"relative residual each, lines log-U[{cfg['L'][0]},{cfg['L'][1]}], "
+                            f"cells per line log-U[{cfg['K'][0]},{cfg['K'][1]}], 9x9 blocks, "
+                            f"algo {args.algo}",
+                "systems": len(shapes), "cells_total": int(cells.sum()),
+                "cells_min": int(cells.min()), "cells_max": int(cells.max()),
+                "lines_total": int(sum(m.nline for m in meshes)),
+                "device_footprint_gb": round(footprint / 1e9, 2),
+                "sweeps_min": int(sw.min()), "sweeps_max": int(sw.max()),
+                "inner_sweeps": inner,
+                "schedule": {"ctas_per_sm": ctas, "stages": stages,
+                             "order": "longest lines first" if order == 0 else "mesh order",
+                             "tuned_thomas_ms": round(tune_ms, 4)},
+                "setup_s": round(setup_s, 1),
+                "time_per_batch_ms": round(max_ms / args.steps, 3),
+                "l2": "no flush: every sweep streams %.1f GB of blocks, > 126 MB L2" %
+                      (8 * 81 * 5 * cells.sum() / 1e9),
+                "timing": "CUDA events on the batch's stream around the synchronous batched "
+                          "solves (one graph launch each)",
+                "parallelism": f"{ws} ranks, each its own batch" if ws > 1 else "1 GPU",
+            },
+            "roofline": roof,
+            "kernels": kern,
+            "e2e": {"value": round(all_e2e / (max_e2e * 1e-3), 1), "unit": "cell-sweeps/s",
+                    "h2d_bytes_per_step": int(sum(r.nbytes for r in rhs_h)),
+                    "d2h_bytes_per_step": int(sum(u.nbytes for u in sol_h)), "steps": ne2e,
+                    "what": "per step: tbs_set_rhs of every system from pinned host memory, "
+                            "tbs_batch_solve, tbs_get_solution of every system"},
+            "gpu_launches": int(round(launches_per_solve * args.steps)),
+            "clocks": clk,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            # bounded sample: the oracle on the median-size system of the batch
+            k = int(np.argsort(cells)[len(cells) // 2])
+            L, K = shapes[k]
+            m2, host = build_problem(L, K, shift, pinned=False)
+            cb = cpu_baseline(m2, host, budget_s=10.0)
+            cb["value"] = cb["value"] * m2.nelem
+            cb["unit"] = "cell-sweeps/s"
+            cb["sample"] = f"median system of the batch ({L}x{K}): " + cb["sample"]
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for s in solvers:
+        s.close()
+    dist.close()
+    return 0
+
+
+def run_batch_reference(args):
+    """The oracle on the host cores for a batched workload: one FP64 sweep of
+    the batch's median-size system per step (a bounded sample), in cell-sweeps/s."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    cfg = BATCH_CONFIGS[args.config]
+    shapes = batch_shapes(cfg)
+    cells = np.array([L * K for L, K in shapes])
+    L, K = shapes[int(np.argsort(cells)[len(cells) // 2])]
+    mesh, host = build_problem(L, K, cfg["shift"], pinned=False)
+    import oracle
+    threads = os.cpu_count() or 1
+    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    for _ in range(args.warmup):
+        b.sweeps(1)
+    b.reset()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.sweeps(1)
+    dt = time.perf_counter() - t0
+    v = mesh.nelem * args.steps / dt
+    line = {"impl": "reference", "metric": "batched LIJ cell-sweeps/s", "value": round(v, 1),
+            "unit": "cell-sweeps/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * dt / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured meshes and values",
+            "config": {"workload": f"one FP64 sweep per step of the median system ({L}x{K}) of "
+                                   f"the {len(shapes)}-system batch", "cells": mesh.nelem},
+            "cpu_baseline": {"value": round(v, 1), "unit": "cell-sweeps/s", "cores": threads,
+                             "kind": "port",
+                             "sample": f"{args.steps} sweeps of the {L}x{K} system; "
+                                       "oracle/lij_oracle.c, OpenMP over lines"},
+            "e2e": {"value": round(v, 1), "unit": "cell-sweeps/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_reference(args, L, K, shift, tol):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -230,11 +465,15 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS))
+    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS))
     ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.config in BATCH_CONFIGS:
+        if args.impl == "reference":
+            return run_batch_reference(args)
+        return run_batch(args)
     L, K, shift, tol = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, L, K, shift, tol)

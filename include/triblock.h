@@ -270,6 +270,61 @@ int tbs_residual_noalloc(int device_id, void *cuda_stream, int nelem,
                          const double *d_jacO2, const double *d_rhs,
                          const double *d_U, double *d_R, double *norm_out);
 
+/* ======================================================== batched solves
+ * Many independent systems solved together on one GPU (no counterpart in
+ * the reference, whose driver solves one system per process).  A batch is
+ * built over contexts factored with the same algorithm (TBS_ALGO_FP64 or
+ * TBS_ALGO_MIXED) on the same device; each keeps its own blocks, rhs,
+ * starting solution (tbs_set_initial) and result, read with
+ * tbs_get_solution as after tbs_solve.  tbs_batch_solve runs one CUDA
+ * graph launch: every sweep is one persistent Thomas launch over the lines
+ * of all systems still above their tolerance, taken from a device work
+ * queue (longest lines first by default), one residual launch over their
+ * tiles and one launch for the per-system norms; each system stops at its
+ * own tolerance or sweep limit.  Each system's iterates, norm history and
+ * sweep count are bit-identical to tbs_solve on that context alone.
+ * The batch reads the members' device arrays at each solve; re-factoring
+ * a member with the same algorithm or giving it a new rhs is allowed,
+ * tbs_set_mesh or tbs_destroy on a member is not while the batch lives.
+ * Calls on one batch and on its members must not overlap. */
+typedef struct tbs_batch tbs_batch;
+int tbs_batch_create(tbs_ctx *const *systems, int nsys, tbs_batch **out);
+int tbs_batch_destroy(tbs_batch *batch);
+const char *tbs_batch_last_error(const tbs_batch *batch);
+int tbs_batch_size(const tbs_batch *batch, int *nsys);
+/* Launch on `cuda_stream` (not the legacy default stream; NULL: the
+ * batch's own stream). */
+int tbs_batch_set_stream(tbs_batch *batch, void *cuda_stream);
+
+/* sweeps_out[nsys]; hist_out: nsys rows of (max_sweeps + 1) norms, row s
+ * valid up to entry sweeps_out[s]; either may be NULL */
+int tbs_batch_solve(tbs_batch *batch, double rel_tol, int max_sweeps,
+                    int *sweeps_out, double *hist_out);
+
+/* Shape of the persistent Thomas launch: CTAs (one warp each, one line at
+ * a time) per SM, bulk-copy ring stages (2..8), line order (0: longest
+ * first, 1: mesh order).  TBS_ERR_ARG when the shape does not fit. */
+int tbs_batch_set_schedule(tbs_batch *batch, int ctas_per_sm, int stages, int order);
+int tbs_batch_get_schedule(const tbs_batch *batch, int *ctas_per_sm, int *stages,
+                           int *order);
+
+/* Autotuner: times the persistent Thomas launch over every CTAs-per-SM /
+ * stage count / line order that fits, keeps the fastest and reports it and
+ * its time per launch in ms (any output may be NULL). */
+int tbs_batch_tune(tbs_batch *batch, int *ctas_per_sm, int *stages, int *order,
+                   double *best_ms);
+
+/* TBS_ALGO_MIXED: FP32 inner sweeps per outer step for every member
+ * (default: the first member's setting). */
+int tbs_batch_set_inner_sweeps(tbs_batch *batch, int m);
+
+/* Per-kernel CUDA-event timing of batched solves (eager launches while
+ * enabled), as tbs_profile_*. */
+int tbs_batch_profile_enable(tbs_batch *batch, int on);
+int tbs_batch_profile_reset(tbs_batch *batch);
+int tbs_batch_profile_read(tbs_batch *batch, int *n, const char **names,
+                           long long *launches, double *ms);
+
 /* Library version string. */
 const char *tbs_version(void);
 

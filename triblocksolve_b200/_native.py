@@ -91,6 +91,19 @@ _sig("tbs_profile_reset", _i, _vp)
 _sig("tbs_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)
 _sig("tbs_kernel_bytes", _i, _vp, _cp, _dp)
 _sig("tbs_residual_noalloc", _i, _i, _vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _dp)
+_sig("tbs_batch_create", _i, C.POINTER(_vp), _i, C.POINTER(_vp))
+_sig("tbs_batch_destroy", _i, _vp)
+_sig("tbs_batch_last_error", _cp, _vp)
+_sig("tbs_batch_size", _i, _vp, _ip)
+_sig("tbs_batch_set_stream", _i, _vp, _vp)
+_sig("tbs_batch_solve", _i, _vp, C.c_double, _i, _ip, _dp)
+_sig("tbs_batch_set_schedule", _i, _vp, _i, _i, _i)
+_sig("tbs_batch_get_schedule", _i, _vp, _ip, _ip, _ip)
+_sig("tbs_batch_tune", _i, _vp, _ip, _ip, _ip, _dp)
+_sig("tbs_batch_set_inner_sweeps", _i, _vp, _i)
+_sig("tbs_batch_profile_enable", _i, _vp, _i)
+_sig("tbs_batch_profile_reset", _i, _vp)
+_sig("tbs_batch_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)
 
 
 class TbsError(RuntimeError):
@@ -109,6 +122,12 @@ def last_error(ctx=None) -> str:
 def check(code: int, ctx=None) -> None:
     if code != TBS_OK:
         raise TbsError(code, last_error(ctx))
+
+
+def check_batch(code: int, batch=None) -> None:
+    if code != TBS_OK:
+        s = lib.tbs_batch_last_error(batch)
+        raise TbsError(code, s.decode() if s else "")
 
 
 def iptr(a: np.ndarray):

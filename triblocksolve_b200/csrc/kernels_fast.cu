@@ -578,10 +578,14 @@ int fast_resid_grid(int np16) { return np16 / RES_TILE > 0 ? np16 / RES_TILE : 1
 /* Fixed-order sum of the per-CTA partials by the last CTA; updates the
  * solve state like reduce_norm_kernel.  Called by every thread of the
  * block; `block_sum` is valid in thread 0. */
-__device__ void finalize_norm(const NormSink &ns, double block_sum) {
+__device__ void finalize_norm(const NormSink &ns, double block_sum, int blk) {
     __shared__ unsigned ticket;
     __shared__ double red[32];
     if (!ns.partials) return;
+    if (!ns.counter) { /* batched launch: the partial only, reduced per system later */
+        if (threadIdx.x == 0) ns.partials[blk] = block_sum;
+        return;
+    }
     if (threadIdx.x == 0) {
         ns.partials[blockIdx.x] = block_sum;
         __threadfence();
@@ -630,7 +634,7 @@ template <typename T>
 __device__ __forceinline__ void fast_resid_body(
     int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
-    T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status) {
+    T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status, int blk) {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     T *sD = reinterpret_cast<T *>(smem + 128);
@@ -639,7 +643,7 @@ __device__ __forceinline__ void fast_resid_body(
     T *sg = sX + nx * RES_TILE * NB;
     T *sr = sg + nxa * RES_TILE * NV;
     T *sb = sr + RES_TILE * NV;
-    const int p0 = blockIdx.x * RES_TILE;
+    const int p0 = blk * RES_TILE;
     const int tid = threadIdx.x;
     const int c = tid % RES_TILE, i = tid / RES_TILE;
     const bool act = tid < RES_TILE * NV;
@@ -662,10 +666,11 @@ __device__ __forceinline__ void fast_resid_body(
             bulk_g2s(sr, Rsrc + (size_t)p0 * NV, szR, bar);
         }
     }
-    if (mode >= 1 && act && Uacc) {
-        /* U += dU of this tile (the Thomas kernel leaves U to this kernel) */
+    if (act && Uacc) {
+        /* modes 1, 3: U += dU of this tile (the Thomas kernel leaves U to
+         * this kernel); mode 0: U = 0, the start of a sweep sequence */
         const size_t q = (size_t)p0 * NV + tid;
-        Uacc[q] += dU[q];
+        Uacc[q] = (mode >= 1) ? Uacc[q] + dU[q] : T(0);
     }
     if (mode >= 1 && act) {
         /* neighbour dU gathers overlap the bulk copies */
@@ -732,7 +737,7 @@ __device__ __forceinline__ void fast_resid_body(
         double tot = 0.0;
         if (tid == 0)
             for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
-        finalize_norm(ns, tot);
+        finalize_norm(ns, tot, blk);
     }
 }
 
@@ -742,7 +747,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     int nx, int np16, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, T *__restrict__ b,
     T *__restrict__ Uacc, NormSink ns, unsigned *status) {
-    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status);
+    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status, blockIdx.x);
 }
 
 /* mode 3 (b = -sum (Dinv X) dU: premultiplied cross-line blocks, no norm) */
@@ -750,15 +755,17 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_dx_kernel(
     int nx, int np16, const T *__restrict__ DX, const int *__restrict__ xnbr,
     const T *__restrict__ dU, T *__restrict__ b, T *__restrict__ Uacc, unsigned *status) {
-    fast_resid_body<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status);
+    fast_resid_body<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status,
+                       blockIdx.x);
 }
 
 /* mode 0 (R given in position order) */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
     int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
-    NormSink ns, unsigned *status) {
-    fast_resid_body<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, nullptr, ns, status);
+    T *__restrict__ Uzero, NormSink ns, unsigned *status) {
+    fast_resid_body<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status,
+                       blockIdx.x);
 }
 
 template <typename T>
@@ -779,6 +786,7 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
          * norm bookkeeping happens */
         mode = 0;
         Rsrc = b;
+        Uacc = nullptr;
     }
     if (mode == 0 && !Rsrc) return (int)cudaErrorInvalidValue;
     const size_t smem = resid_smem_bytes<T>(mode >= 1 ? L.nx : 0);
@@ -789,8 +797,8 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
         fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr,
                                                                    dU, b, Uacc, ns, status);
     else
-        fast_resid_rhs_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b, ns,
-                                                                       status);
+        fast_resid_rhs_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b,
+                                                                       Uacc, ns, status);
     return (int)cudaGetLastError();
 }
 
@@ -991,13 +999,17 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
     }
 }
 
+/* Solve one line (start ps, n cells, twist m) with the warp of the calling
+ * CTA.  The staging barriers live at the start of `smem` and stay
+ * initialised across the lines that a persistent CTA solves: bit s of
+ * `pbase` is the parity with which barrier s completes its next phase.
+ * Returns false when a staging wait ran out of time; the status bit is
+ * then set and the copies in flight have landed. */
 template <typename T, int P, bool YS>
-__global__ void __launch_bounds__(32) fast_thomas_kernel(
-    int nline, int NS, int accumulate, const int *__restrict__ line_start,
-    const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
+__device__ __forceinline__ bool thomas_line(
+    int NS, int accumulate, int ps, int n, int m, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
-    T *__restrict__ U, unsigned *status) {
-    extern __shared__ __align__(128) unsigned char smem[];
+    T *__restrict__ U, unsigned *status, unsigned char *smem, uint32_t &pbase, uint64_t pol) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     const uint32_t stage = 2 * P * (NB + NV) * sizeof(T);
     const uint32_t half = P * (NB + NV) * sizeof(T);
@@ -1005,16 +1017,11 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     /* broadcast: 2 halves x 2 alternating buffers x [copy A: 10][copy B: 10] */
     T *bcall = reinterpret_cast<T *>(st0 + (size_t)NS * stage);
     T *ys = bcall + 80;
-    const int l = blockIdx.x;
-    if (l >= nline) return;
-    const int lane = threadIdx.x;
+    const int lane = threadIdx.x & 31;
     const int h = lane >> 4, li = lane & 15;
     const int i = li < NV ? li : NV - 1;
     const bool writer = li < NV;
     const LaneOff off = lane_offsets(i);
-    const int ps = line_start[l];
-    const int n = line_len[l];
-    const int m = line_twist[l];
     const int nb = n - 1 - m;
     const int len = h ? nb : m;      /* this half's chain length */
     const int cpos = h ? m : 0;      /* its first position, relative to ps */
@@ -1025,17 +1032,13 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     T *bc = bcall + h * 40;
     T *yl = y + (size_t)ps * NV;
     T *dUl = dU + (size_t)ps * NV;
-    T *Ul = U + (size_t)ps * NV;
+    T *Ul = U ? U + (size_t)ps * NV : nullptr;
+    auto parity = [&](int job) { return ((pbase >> (job % NS)) ^ (uint32_t)(job / NS)) & 1u; };
 
-    if (lane == 0) {
-        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
-        mbar_fence_init();
-    }
+    __syncwarp(); /* the previous line's readers of the stages are done */
     for (int t = lane; t < 80; t += 32) bcall[t] = T(0);
     __syncwarp();
 
-    uint64_t pol = 0;
-    if (lane == 0) pol = policy_evict_first();
     /* copy size of chunk c of a chain of length ln, rounded up to 4 cells
      * (16-byte multiple); the extra cells stay inside the line's range */
     auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
@@ -1081,7 +1084,7 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     /* ---------------- forward */
     for (int c = 0; c < nf; ++c) {
         const int s = c % NS;
-        const bool ok = mbar_wait(&bars[s], (uint32_t)((c / NS) & 1));
+        const bool ok = mbar_wait(&bars[s], parity(c));
         if (__any_sync(FULL, !ok)) {
             timed_out = true;
             break;
@@ -1150,7 +1153,7 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             const int c = nch - 1 - jb; /* this half's chunk (may be < 0) */
             if (!YS) load_chunk(c - 1, nyv, nuv);
             const int s = job % NS;
-            const bool ok = mbar_wait(&bars[s], (uint32_t)((job / NS) & 1));
+            const bool ok = mbar_wait(&bars[s], parity(job));
             if (__any_sync(FULL, !ok)) {
                 timed_out = true;
                 break;
@@ -1202,10 +1205,85 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
             }
         }
     }
-    if (timed_out && lane == 0) {
-        atomicOr(status, ST_TIMEOUT);
-        for (int job = consumed; job < issued; ++job)
-            mbar_wait(&bars[job % NS], (uint32_t)((job / NS) & 1), 1LL << 28);
+    if (timed_out) {
+        if (lane == 0) {
+            atomicOr(status, ST_TIMEOUT);
+            for (int job = consumed; job < issued; ++job)
+                mbar_wait(&bars[job % NS], parity(job), 1LL << 28);
+        }
+        __syncwarp();
+        return false;
+    }
+    /* every job was waited for: barrier s completed one phase per job
+     * j = s, s+NS, ... below njobs */
+    for (int s = 0; s < NS && s < njobs; ++s) {
+        const int cnt = (njobs - 1 - s) / NS + 1;
+        pbase ^= (uint32_t)(cnt & 1) << s;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void thomas_init_bars(unsigned char *smem, int NS) {
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    if ((threadIdx.x & 31) == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
+}
+
+/* one CTA (one warp) per line */
+template <typename T, int P, bool YS>
+__global__ void __launch_bounds__(32) fast_thomas_kernel(
+    int nline, int NS, int accumulate, const int *__restrict__ line_start,
+    const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
+    const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
+    T *__restrict__ U, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    thomas_init_bars(smem, NS);
+    const uint64_t pol = threadIdx.x == 0 ? policy_evict_first() : 0;
+    uint32_t pbase = 0;
+    thomas_line<T, P, YS>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam, b, y,
+                          dU, U, status, smem, pbase, pol);
+}
+
+/* Persistent form over many systems: each CTA (one warp) takes (system,
+ * line) items from a device work queue, in the order of `work` (longest
+ * lines first, so that the long lines do not start last), and skips the
+ * lines of systems that have converged.  queue[0] is the next item,
+ * queue[1] counts retired CTAs; the last CTA to retire resets both for the
+ * next launch.  U is left to the residual kernel (accumulate = 2). */
+template <typename T, int P>
+__global__ void __launch_bounds__(32) fast_thomas_batch_kernel(
+    const ThomasSys<T> *__restrict__ sys, const WorkItem *__restrict__ work, int nwork,
+    const int *__restrict__ active, unsigned *queue, int NS, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int lane = threadIdx.x & 31;
+    thomas_init_bars(smem, NS);
+    const uint64_t pol = lane == 0 ? policy_evict_first() : 0;
+    uint32_t pbase = 0;
+    for (;;) {
+        int w = 0;
+        if (lane == 0) w = (int)atomicAdd(queue, 1u);
+        w = __shfl_sync(FULL, w, 0);
+        if (w >= nwork) break;
+        const WorkItem it = work[w];
+        if (active && !active[it.sys]) continue;
+        const ThomasSys<T> S = sys[it.sys];
+        const int l = it.unit;
+        if (!thomas_line<T, P, false>(NS, 2, S.line_start[l], S.line_len[l], S.line_twist[l], S.G,
+                                      S.Gam, S.b, S.y, S.dU, nullptr, status, smem, pbase, pol))
+            break;
+    }
+    if (lane == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+            queue[0] = 0u;
+            queue[1] = 0u;
+            __threadfence();
+        }
     }
 }
 
@@ -1299,16 +1377,16 @@ int fast_kernels_init() { return 0; }
 constexpr int FULLRES_THREADS = 288;
 
 template <typename T>
-__global__ void __launch_bounds__(FULLRES_THREADS) full_resid_kernel(
+__device__ __forceinline__ void full_resid_body(
     int nelem, const int *__restrict__ epoint, const int *__restrict__ ef,
     const int *__restrict__ fc, const int *__restrict__ pos_of_elem,
     const double *__restrict__ D, const double *__restrict__ O1, const double *__restrict__ O2,
     const double *__restrict__ rhs, const double *__restrict__ Up, T *__restrict__ Rp,
-    double *__restrict__ partials) {
+    double *__restrict__ partials, int blk) {
     const int epb = FULLRES_THREADS / NV;
     const int le = threadIdx.x / NV;
     const int i = threadIdx.x - le * NV;
-    const int e = blockIdx.x * epb + le;
+    const int e = blk * epb + le;
     double sq = 0.0;
     if (e < nelem) {
         const int pe = pos_of_elem[e];
@@ -1349,8 +1427,19 @@ __global__ void __launch_bounds__(FULLRES_THREADS) full_resid_kernel(
     if (threadIdx.x == 0) {
         double tot = 0.0;
         for (int w = 0; w < FULLRES_THREADS / 32; ++w) tot += red[w];
-        partials[blockIdx.x] = tot;
+        partials[blk] = tot;
     }
+}
+
+template <typename T>
+__global__ void __launch_bounds__(FULLRES_THREADS) full_resid_kernel(
+    int nelem, const int *__restrict__ epoint, const int *__restrict__ ef,
+    const int *__restrict__ fc, const int *__restrict__ pos_of_elem,
+    const double *__restrict__ D, const double *__restrict__ O1, const double *__restrict__ O2,
+    const double *__restrict__ rhs, const double *__restrict__ Up, T *__restrict__ Rp,
+    double *__restrict__ partials) {
+    full_resid_body<T>(nelem, epoint, ef, fc, pos_of_elem, D, O1, O2, rhs, Up, Rp, partials,
+                       blockIdx.x);
 }
 
 int full_resid_blocks(int nelem) { return (nelem + (FULLRES_THREADS / NV) - 1) / (FULLRES_THREADS / NV); }
@@ -1372,5 +1461,238 @@ template int launch_full_resid<float>(cudaStream_t, int, const int *, const int 
                                       const int *, const double *, const double *,
                                       const double *, const double *, const double *, float *,
                                       double *);
+
+
+/* ================================================ mixed-precision prime
+ * Per tile of RES_TILE positions (160 threads, 144 active): U = 0, the
+ * FP32 copy of the residual R = rhs, and the tile's sum rhs^2 in a fixed
+ * order (lane order within a warp, then warps in order). */
+__device__ __forceinline__ void mixed_prime_body(const double *__restrict__ rhsp,
+                                                 float *__restrict__ R32, double *__restrict__ Up,
+                                                 double *__restrict__ partials, int blk) {
+    const int tid = threadIdx.x;
+    const bool act = tid < RES_TILE * NV;
+    double sq = 0.0;
+    if (act) {
+        const size_t q = (size_t)blk * RES_TILE * NV + tid;
+        const double v = rhsp[q];
+        R32[q] = (float)v;
+        Up[q] = 0.0;
+        sq = v * v;
+    }
+    __shared__ double red[RES_THREADS_FAST / 32];
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+    if ((tid & 31) == 0) red[tid >> 5] = sq;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
+        partials[blk] = tot;
+    }
+}
+
+__global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_kernel(
+    const double *__restrict__ rhsp, float *__restrict__ R32, double *__restrict__ Up,
+    double *__restrict__ partials) {
+    mixed_prime_body(rhsp, R32, Up, partials, blockIdx.x);
+}
+
+int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
+                       double *Up, double *partials) {
+    mixed_prime_kernel<<<fast_resid_grid(L.np16), RES_THREADS_FAST, 0, st>>>(rhsp, R32, Up,
+                                                                             partials);
+    return (int)cudaGetLastError();
+}
+
+/* ================================================================ batches */
+
+template <typename T>
+size_t thomas_batch_smem(int stages) {
+    return 128 + (size_t)stages * 2 * THOMAS_P * (NB + NV) * sizeof(T) + 80 * sizeof(T);
+}
+
+template <typename T>
+int thomas_batch_fit(int stages) {
+    int n = 0;
+    const size_t smem = thomas_batch_smem<T>(stages);
+    if (cudaFuncSetAttribute((const void *)fast_thomas_batch_kernel<T, THOMAS_P>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fast_thomas_batch_kernel<T, THOMAS_P>, 32,
+                                                      smem) != cudaSuccess)
+        return 0;
+    return n;
+}
+
+static int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
+
+template <typename T>
+int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
+                        const WorkItem *work, int nwork, const int *active, unsigned *queue,
+                        unsigned *status) {
+    if (nwork <= 0) return 0;
+    if (bs.stages < 2 || bs.stages > 8 || bs.ctas_per_sm < 1) return (int)cudaErrorInvalidValue;
+    const size_t smem = thomas_batch_smem<T>(bs.stages);
+    long long grid = (long long)bs.ctas_per_sm * sm_count();
+    if (grid > nwork) grid = nwork;
+    fast_thomas_batch_kernel<T, THOMAS_P><<<(int)grid, 32, smem, st>>>(sys, work, nwork, active,
+                                                                        queue, bs.stages, status);
+    return (int)cudaGetLastError();
+}
+
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_batch_kernel(
+    const ResidSys<T> *__restrict__ sys, const WorkItem *__restrict__ work, int mode,
+    const int *__restrict__ active, unsigned *status) {
+    const WorkItem it = work[blockIdx.x];
+    if (active && !active[it.sys]) return;
+    const ResidSys<T> S = sys[it.sys];
+    NormSink ns{};
+    ns.partials = (mode == 3) ? nullptr : S.partials; /* no counter: partials only */
+    fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr, S.dU, S.Rsrc, S.b,
+                       S.Uacc, ns, status, it.unit);
+}
+
+template <typename T>
+int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
+                       const WorkItem *work, int nwork, const int *active, unsigned *status) {
+    if (nwork <= 0) return 0;
+    if (mode != 0 && mode != 1 && mode != 3) return (int)cudaErrorInvalidValue;
+    const size_t smem = resid_smem_bytes<T>(mode == 0 ? 0 : max_nx);
+    fast_resid_batch_kernel<T><<<nwork, RES_THREADS_FAST, smem, st>>>(sys, work, mode, active,
+                                                                      status);
+    return (int)cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(FULLRES_THREADS) full_resid_batch_kernel(
+    const FullResSys *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ active) {
+    const WorkItem it = work[blockIdx.x];
+    if (active && !active[it.sys]) return;
+    const FullResSys S = sys[it.sys];
+    full_resid_body<float>(S.nelem, S.epoint, S.ef, S.fc, S.pos_of_elem, S.D, S.O1, S.O2, S.rhs,
+                           S.Up, S.R32, S.partials, it.unit);
+}
+
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work, int nwork,
+                            const int *active) {
+    if (nwork <= 0) return 0;
+    full_resid_batch_kernel<<<nwork, FULLRES_THREADS, 0, st>>>(sys, work, active);
+    return (int)cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_batch_kernel(
+    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work) {
+    const WorkItem it = work[blockIdx.x];
+    const VecSys S = sys[it.sys];
+    mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, it.unit);
+}
+
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork) {
+    if (nwork <= 0) return 0;
+    mixed_prime_batch_kernel<<<nwork, RES_THREADS_FAST, 0, st>>>(sys, work);
+    return (int)cudaGetLastError();
+}
+
+/* U += c + d over one tile (elementwise: the same values as axpy2_kernel) */
+__global__ void __launch_bounds__(RES_THREADS_FAST) axpy2_batch_kernel(
+    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ active) {
+    const WorkItem it = work[blockIdx.x];
+    if (active && !active[it.sys]) return;
+    if (threadIdx.x >= RES_TILE * NV) return;
+    const VecSys S = sys[it.sys];
+    const size_t q = (size_t)it.unit * RES_TILE * NV + threadIdx.x;
+    S.Up[q] += (double)S.c32[q] + (double)S.d32[q];
+}
+
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork,
+                       const int *active) {
+    if (nwork <= 0) return 0;
+    axpy2_batch_kernel<<<nwork, RES_THREADS_FAST, 0, st>>>(sys, work, active);
+    return (int)cudaGetLastError();
+}
+
+__global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, int nsys, int is_start,
+                                    int *active, unsigned *counter,
+                                    cudaGraphConditionalHandle handle, int use_cond) {
+    __shared__ double red[32];
+    __shared__ unsigned ticket;
+    const int s = blockIdx.x;
+    const ReduceSys R = sys[s];
+    if (is_start || active[s]) {
+        double acc = 0.0;
+        for (int t = threadIdx.x; t < R.n; t += blockDim.x) acc += R.partials[t];
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
+            const double nrm = sqrt(tot);
+            SolveState *S = R.state;
+            if (is_start) {
+                S->sweep = 0;
+                S->norm0 = nrm;
+            } else {
+                S->sweep += 1;
+            }
+            const int sw = S->sweep;
+            if (sw < S->hist_cap) R.hist[sw] = nrm;
+            S->last = nrm;
+            active[s] = (isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps) ? 1 : 0;
+        }
+    }
+    if (threadIdx.x == 0) {
+        __threadfence();
+        ticket = atomicAdd(counter, 1u);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0 && ticket == gridDim.x - 1) {
+        __threadfence();
+        int any = 0;
+        for (int k = 0; k < nsys; ++k) any |= __ldcg(active + k);
+        if (use_cond) cudaGraphSetConditional(handle, any ? 1u : 0u);
+        *counter = 0u;
+    }
+}
+
+int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, int nsys,
+                        int is_start, int *active, unsigned *counter,
+                        unsigned long long cond_handle, int use_cond) {
+    if (nsys <= 0) return 0;
+    if (threads != RES_THREADS_FAST && threads != 256) return (int)cudaErrorInvalidValue;
+    batch_reduce_kernel<<<nsys, threads, 0, st>>>(sys, nsys, is_start, active, counter,
+                                                  (cudaGraphConditionalHandle)cond_handle,
+                                                  use_cond);
+    return (int)cudaGetLastError();
+}
+
+/* opt the batched residual kernels into the shared memory of the widest
+ * system (outside stream capture) */
+int batch_prepare(int max_nx) {
+    int rc = set_smem((const void *)fast_resid_batch_kernel<double>, resid_smem_bytes<double>(max_nx));
+    if (!rc)
+        rc = set_smem((const void *)fast_resid_batch_kernel<float>, resid_smem_bytes<float>(max_nx));
+    return rc;
+}
+
+template size_t thomas_batch_smem<double>(int);
+template size_t thomas_batch_smem<float>(int);
+template int thomas_batch_fit<double>(int);
+template int thomas_batch_fit<float>(int);
+template int launch_thomas_batch<double>(cudaStream_t, const BatchSched &, const ThomasSys<double> *,
+                                         const WorkItem *, int, const int *, unsigned *, unsigned *);
+template int launch_thomas_batch<float>(cudaStream_t, const BatchSched &, const ThomasSys<float> *,
+                                        const WorkItem *, int, const int *, unsigned *, unsigned *);
+template int launch_resid_batch<double>(cudaStream_t, int, int, const ResidSys<double> *,
+                                        const WorkItem *, int, const int *, unsigned *);
+template int launch_resid_batch<float>(cudaStream_t, int, int, const ResidSys<float> *,
+                                       const WorkItem *, int, const int *, unsigned *);
 
 }  // namespace tbs

@@ -167,8 +167,8 @@ struct NormSink {
 };
 
 /* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
- * b = -sum X dU, no norm.  Uacc (modes 1, 3; may be null): U += dU for the
- * tile's positions */
+ * b = -sum X dU, no norm.  Uacc (may be null): modes 1, 3 add dU to it for
+ * the tile's positions, mode 0 sets it to zero there */
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
                       const T *X, const T *dU, const T *Rsrc, T *b, const NormSink &ns,
@@ -189,6 +189,85 @@ int launch_cast_f64_f32(cudaStream_t st, const double *src, float *dst, long lon
 int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n);
 int launch_axpy2_f32_f64(cudaStream_t st, const float *c, const float *d, double *U, long long n);
 int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
+/* per tile of RES_TILE positions: Up = 0, R32 = (float)rhsp, partials[tile]
+ * = sum rhsp^2 in a fixed order (the start of a TBS_ALGO_MIXED solve) */
+int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
+                       double *Up, double *partials);
+
+/* ------------------------------------------------------------ batches
+ * Many independent systems swept together.  Each kernel takes one
+ * descriptor per system and a list of work items (system, unit), so that
+ * a launch covers the units of every system that has not converged
+ * (active[system] != 0).  The per-unit arithmetic is the one of the
+ * single-system kernels, unit for unit, so a system's iterates do not
+ * depend on the batch it is solved in. */
+struct alignas(8) WorkItem {
+    int sys;                    /* index into the launch's descriptors */
+    int unit;                   /* line, residual tile or element block */
+};
+template <typename T>
+struct ThomasSys {
+    const int *line_start, *line_len, *line_twist;
+    const T *G, *Gam, *b;
+    T *y, *dU;
+};
+template <typename T>
+struct ResidSys {
+    int np16, nx;
+    const int *xnbr;
+    const T *Dinv, *X, *dU, *Rsrc;
+    T *b, *Uacc;
+    double *partials;
+};
+struct FullResSys {
+    int nelem, pad;
+    const int *epoint, *ef, *fc, *pos_of_elem;
+    const double *D, *O1, *O2, *rhs, *Up;
+    float *R32;
+    double *partials;
+};
+struct VecSys {                 /* mixed-precision glue of one system */
+    const double *rhsp;
+    float *R32, *c32, *d32;
+    double *Up;
+    double *partials;
+};
+struct ReduceSys {
+    const double *partials;
+    int n, pad;
+    SolveState *state;
+    double *hist;
+};
+struct BatchSched {             /* persistent Thomas launch shape */
+    int ctas_per_sm;            /* one warp per CTA, one line at a time */
+    int stages;                 /* bulk-copy ring depth */
+};
+
+template <typename T>
+size_t thomas_batch_smem(int stages);
+/* CTAs of the persistent Thomas kernel that fit on one SM with `stages` */
+template <typename T>
+int thomas_batch_fit(int stages);
+template <typename T>
+int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
+                        const WorkItem *work, int nwork, const int *active, unsigned *queue,
+                        unsigned *status);
+template <typename T>
+int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
+                       const WorkItem *work, int nwork, const int *active, unsigned *status);
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work, int nwork,
+                            const int *active);
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork);
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork,
+                       const int *active);
+/* one CTA of `threads` threads per system: the fixed-order sum of its
+ * partials (the order of finalize_norm for threads = 160 and of
+ * reduce_norm for threads = 256), its norm history and active flag; the
+ * last CTA sets the graph condition to "some system is still active" */
+int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, int nsys,
+                        int is_start, int *active, unsigned *counter,
+                        unsigned long long cond_handle, int use_cond);
+int batch_prepare(int max_nx);
 
 }  // namespace tbs
 

@@ -349,3 +349,83 @@ class Solver:
 
     def close(self):
         self.platform.close()
+
+
+class Batch:
+    """Independent systems (factored Solvers on one GPU) solved together.
+
+    ``solve`` runs one CUDA graph launch in which every sweep is a persistent
+    Thomas launch over the lines of all unconverged systems (device work
+    queue, longest lines first), a residual launch over their tiles and a
+    per-system norm launch.  Each system stops at its own tolerance, and its
+    iterates are bit-identical to ``Solver.solve`` on it alone.
+    """
+
+    def __init__(self, solvers: list[Solver]):
+        if not solvers:
+            raise ValueError("a batch needs at least one system")
+        self.solvers = list(solvers)
+        arr = (C.c_void_p * len(solvers))(*[s.ctx for s in solvers])
+        h = C.c_void_p()
+        N.check_batch(N.lib.tbs_batch_create(arr, len(solvers), C.byref(h)))
+        self.handle = h
+
+    def _chk(self, rc):
+        N.check_batch(rc, self.handle)
+
+    def __len__(self):
+        return len(self.solvers)
+
+    def solve(self, rel_tol: float, max_sweeps: int = 1000):
+        """Returns (sweeps per system, list of per-system norm histories)."""
+        n = len(self.solvers)
+        sw = np.zeros(n, np.int32)
+        h = np.zeros((n, max_sweeps + 1))
+        self._chk(N.lib.tbs_batch_solve(self.handle, rel_tol, max_sweeps, N.iptr(sw), N.dptr(h)))
+        return sw, [h[s, : sw[s] + 1].copy() for s in range(n)]
+
+    def set_stream(self, stream_handle: int | None):
+        self._chk(N.lib.tbs_batch_set_stream(self.handle, stream_handle))
+
+    def set_schedule(self, ctas_per_sm: int, stages: int, order: int = 0):
+        self._chk(N.lib.tbs_batch_set_schedule(self.handle, ctas_per_sm, stages, order))
+
+    def schedule(self):
+        a, b, c = C.c_int(), C.c_int(), C.c_int()
+        self._chk(N.lib.tbs_batch_get_schedule(self.handle, C.byref(a), C.byref(b), C.byref(c)))
+        return a.value, b.value, c.value
+
+    def tune(self):
+        """Autotune the persistent Thomas launch; returns (ctas_per_sm, stages, order, ms)."""
+        a, b, c, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self._chk(N.lib.tbs_batch_tune(self.handle, C.byref(a), C.byref(b), C.byref(c),
+                                       C.byref(ms)))
+        return a.value, b.value, c.value, ms.value
+
+    def set_inner_sweeps(self, m: int):
+        self._chk(N.lib.tbs_batch_set_inner_sweeps(self.handle, m))
+
+    def profile(self, on: bool = True):
+        self._chk(N.lib.tbs_batch_profile_enable(self.handle, 1 if on else 0))
+
+    def profile_reset(self):
+        self._chk(N.lib.tbs_batch_profile_reset(self.handle))
+
+    def profile_read(self) -> dict:
+        n = C.c_int(16)
+        names = (C.c_char_p * 16)()
+        launches = (C.c_longlong * 16)()
+        ms = (C.c_double * 16)()
+        self._chk(N.lib.tbs_batch_profile_read(self.handle, C.byref(n), names, launches, ms))
+        return {names[i].decode(): (int(launches[i]), float(ms[i])) for i in range(n.value)}
+
+    def close(self):
+        if self.handle:
+            N.lib.tbs_batch_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
