@@ -28,6 +28,7 @@ import statistics
 import subprocess
 import sys
 import time
+import types
 
 import numpy as np
 
@@ -386,6 +387,234 @@ def run_batch(args):
     return 0
 
 
+# serving: Poisson arrivals over the 60x64, 360x384, 600x640 and 1200x1280 systems, 1-8
+# right-hand sides per request, 20% of requests bring new Jacobian values (re-factor),
+# tolerance 1e-10 for every right-hand side
+SERVE_CONFIGS = {"c5": {"systems": [(60, 64, 9.0), (360, 384, 9.0), (600, 640, 4.0),
+                                    (1200, 1280, 4.0)],
+                        "rhs": (1, 8), "refactor": 0.2, "tol": 1e-10, "seed": 5,
+                        "load": 0.6}}
+
+
+def run_serving(args):
+    """Steps are requests.  Phase 1 submits all requests at once (saturation:
+    the server's capacity in right-hand-side solves/s); phase 2 replays them
+    as a Poisson process at `load` x that capacity and reports p50/p99
+    latency.  Latency is host wall clock from submit to the solution in host
+    memory, as a client sees it."""
+    import threading
+
+    import torch
+
+    import triblocksolve_b200 as tbs
+    from triblocksolve_b200 import _native as N
+    cfg = SERVE_CONFIGS[args.config]
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    algo = {"fp64": tbs.ALGO_FP64, "mixed": tbs.ALGO_MIXED}[args.algo]
+    tol = cfg["tol"]
+    rng = np.random.default_rng(cfg["seed"] + 7 * rank)
+
+    def pinned(n):
+        return torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+
+    srv = tbs.Server(local, algo, budget_bytes=64 << 30, max_rhs=64, chunk=4)
+    sys_ids, meshes, rhs_pool, alt = [], [], [], []
+    t_setup = time.perf_counter()
+    for k, (L, K, shift) in enumerate(cfg["systems"]):
+        mesh = tbs.Mesh.structured(L, K)
+        jac = types.SimpleNamespace(jacD=np.empty(81 * mesh.nelem), jacO1=np.empty(81 * mesh.nintface),
+                                    jacO2=np.empty(81 * mesh.nintface), rhs=np.empty(9 * mesh.nelem))
+        N.check(N.lib.tbs_gen_jacobian(9, mesh.nelem, mesh.nintface, shift, 2000 + k,
+                                       N.dptr(jac.jacD), N.dptr(jac.jacO1), N.dptr(jac.jacO2),
+                                       N.dptr(jac.rhs), None))
+        sys_ids.append(srv.add_system(mesh, jac))
+        # the values a re-factoring request brings (pinned, as a serving client would stage them)
+        a = types.SimpleNamespace(jacD=pinned(81 * mesh.nelem), jacO1=pinned(81 * mesh.nintface),
+                                  jacO2=pinned(81 * mesh.nintface))
+        junk = np.empty(9 * mesh.nelem)
+        N.check(N.lib.tbs_gen_jacobian(9, mesh.nelem, mesh.nintface, shift, 3000 + k,
+                                       N.dptr(a.jacD), N.dptr(a.jacO1), N.dptr(a.jacO2),
+                                       N.dptr(junk), None))
+        alt.append(a)
+        pool = pinned(8 * 9 * mesh.nelem).reshape(8, 9 * mesh.nelem)
+        pool[:] = rng.uniform(-1.0, 1.0, pool.shape)
+        rhs_pool.append(pool)
+        meshes.append(mesh)
+        del jac
+    setup_s = time.perf_counter() - t_setup
+    nreq = max(1, args.steps)
+    lo, hi = cfg["rhs"]
+    plan = [(int(rng.integers(len(sys_ids))), int(rng.integers(lo, hi + 1)),
+             bool(rng.random() < cfg["refactor"])) for _ in range(nreq)]
+    outs = [pinned(8 * 9 * m.nelem).reshape(8, 9 * m.nelem) for m in meshes]
+
+    def submit(s, nrhs, refac):
+        return srv.submit(sys_ids[s], rhs_pool[s][:nrhs], tol, 400,
+                          new_jacobian=alt[s] if refac else None, out=outs[s][:nrhs])
+
+    # warm-up: every system once, and a re-factor of the smallest
+    for _ in range(max(args.warmup, 1)):
+        for s in range(len(sys_ids)):
+            submit(s, 2, False).wait()
+    submit(0, 1, True).wait()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        # phase 1: saturation
+        st0 = srv.stats()
+        t0 = time.perf_counter()
+        reqs = [submit(*p) for p in plan]
+        res = [r.wait() for r in reqs]
+        sat_s = time.perf_counter() - t0
+        st1 = srv.stats()
+        rhs_done = sum(p[1] for p in plan)
+        capacity = rhs_done / sat_s
+        sat_lat = np.array([r[3] for r in res])
+        worst_rel = max(float(r[2].max()) for r in res)
+        # phase 2: Poisson arrivals at load x capacity (requests per second)
+        rate = cfg["load"] * capacity / ((lo + hi) / 2.0)
+        gaps = rng.exponential(1.0 / rate, nreq)
+        lat, qms = [None] * nreq, [None] * nreq
+        handles = [None] * nreq
+        ready = threading.Semaphore(0)
+
+        def waiter():
+            for i in range(nreq):
+                ready.acquire()
+                _U, _sw, _rel, lat[i], qms[i] = handles[i].wait()
+
+        th = threading.Thread(target=waiter)
+        th.start()
+        t1 = time.perf_counter()
+        due = t1
+        for i, p in enumerate(plan):
+            due += gaps[i]
+            d = due - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            handles[i] = submit(*p)
+            ready.release()
+        th.join()
+        open_s = time.perf_counter() - t1
+        st2 = srv.stats()
+    clk = clocks.summary()
+    lat = np.array(lat)
+    qms = np.array(qms)
+    if rank == 0:
+        per_shape = {}
+        for (s, nrhs, refac), l in zip(plan, lat):
+            key = f"{cfg['systems'][s][0]}x{cfg['systems'][s][1]}"
+            per_shape.setdefault(key, []).append(l)
+        line = {
+            "metric": "serving right-hand-side solves/s", "value": round(capacity, 2),
+            "unit": "rhs-solves/s", "n_gpus": ws, "steps": nreq, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * sat_s / nreq, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64" if args.algo == "fp64" else "f32+f64",
+            "data": "synthetic: seeded structured meshes, values and right-hand sides",
+            "config": {
+                "workload": f"{nreq} requests over {len(sys_ids)} resident systems "
+                            f"({', '.join(f'{a}x{b}' for a, b, _ in cfg['systems'])}), "
+                            f"{lo}-{hi} right-hand sides each, {int(100 * cfg['refactor'])}% "
+                            f"re-factor with new Jacobian values, {tol:g} relative residual "
+                            f"per right-hand side, algo {args.algo}",
+                "requests": nreq, "rhs_total": rhs_done,
+                "refactor_requests": int(sum(p[2] for p in plan)),
+                "saturation": {"seconds": round(sat_s, 3),
+                               "requests_per_s": round(nreq / sat_s, 2),
+                               "rhs_solves_per_s": round(capacity, 2),
+                               "p50_ms": round(float(np.percentile(sat_lat, 50)), 3),
+                               "p99_ms": round(float(np.percentile(sat_lat, 99)), 3),
+                               "graph_launches": st1["graph_launches"] - st0["graph_launches"]},
+                "poisson": {"offered_requests_per_s": round(rate, 2),
+                            "load": cfg["load"], "seconds": round(open_s, 3),
+                            "rhs_solves_per_s": round(rhs_done / open_s, 2),
+                            "p50_ms": round(float(np.percentile(lat, 50)), 3),
+                            "p90_ms": round(float(np.percentile(lat, 90)), 3),
+                            "p99_ms": round(float(np.percentile(lat, 99)), 3),
+                            "queue_p50_ms": round(float(np.percentile(qms, 50)), 3),
+                            "queue_p99_ms": round(float(np.percentile(qms, 99)), 3),
+                            "p50_ms_by_shape": {k: round(float(np.percentile(v, 50)), 3)
+                                                for k, v in per_shape.items()},
+                            "p99_ms_by_shape": {k: round(float(np.percentile(v, 99)), 3)
+                                                for k, v in per_shape.items()}},
+                "peak_rhs_in_flight": st2["peak_rhs_in_flight"],
+                "peak_rhs_gb": round(st2["peak_rhs_bytes"] / 1e9, 2),
+                "resident_systems_gb": round(st2["resident_system_bytes"] / 1e9, 2),
+                "worst_rel_residual": worst_rel,
+                "setup_s": round(setup_s, 1),
+                "timing": "host wall clock: saturation = first submit to last solution in host "
+                          "memory; latency per request = submit to its solution in host memory",
+                "parallelism": f"{ws} ranks, each its own server" if ws > 1 else "1 GPU",
+            },
+            "e2e": {"value": round(capacity, 2), "unit": "rhs-solves/s",
+                    "h2d_bytes_per_step": int(sum(8 * 9 * meshes[p[0]].nelem * p[1] for p in plan)
+                                              / nreq),
+                    "d2h_bytes_per_step": int(sum(8 * 9 * meshes[p[0]].nelem * p[1] for p in plan)
+                                              / nreq),
+                    "what": "the value itself: right-hand sides from pinned host memory, "
+                            "solutions back to pinned host memory, re-factor uploads included"},
+            "gpu_launches": int(st1["graph_launches"] - st0["graph_launches"]),
+            "clocks": clk,
+        }
+        if ws == 1 and not args.no_cpu_baseline:
+            L, K, shift = cfg["systems"][1]
+            m2, host = build_problem(L, K, shift, pinned=False)
+            cb = cpu_baseline(m2, host, budget_s=8.0)
+            # sweeps per solve of that shape from the saturation run
+            sw = [int(r[1].mean()) for p, r in zip(plan, res) if p[0] == 1] or [10]
+            cb["value"] = cb["value"] / max(1.0, float(np.mean(sw)))
+            cb["unit"] = "rhs-solves/s"
+            cb["sample"] = (f"{L}x{K} system only, solves/s = oracle sweeps/s / "
+                            f"{np.mean(sw):.1f} sweeps per solve: " + cb["sample"])
+            line["cpu_baseline"] = cb
+        print(json.dumps(line), flush=True)
+    srv.close()
+    dist.close()
+    return 0
+
+
+def run_serving_reference(args):
+    """The oracle on the host cores for the serving workload: per step one FP64
+    sweep of the 360x384 system (a bounded sample), reported as right-hand-side
+    solves/s with the sweeps per solve of that shape at the tolerance."""
+    ws, rank, local = dist_env()
+    if rank != 0:
+        return 0
+    cfg = SERVE_CONFIGS[args.config]
+    L, K, shift = cfg["systems"][1]
+    mesh, host = build_problem(L, K, shift, pinned=False)
+    import oracle
+    threads = os.cpu_count() or 1
+    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    for _ in range(args.warmup):
+        b.sweeps(1)
+    b.reset()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        b.sweeps(1)
+    dt = time.perf_counter() - t0
+    sweeps_per_solve = 7.0  # 360x384, shift 9, 1e-10 (the GPU solve's count)
+    v = args.steps / dt / sweeps_per_solve
+    line = {"impl": "reference", "metric": "serving right-hand-side solves/s", "value": round(v, 3),
+            "unit": "rhs-solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(1e3 * dt / args.steps, 4), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured mesh and values",
+            "config": {"workload": f"one FP64 sweep per step of the {L}x{K} system; solves/s = "
+                                   f"sweeps/s / {sweeps_per_solve:g} sweeps per solve",
+                       "cells": mesh.nelem},
+            "cpu_baseline": {"value": round(v, 3), "unit": "rhs-solves/s", "cores": threads,
+                             "kind": "port",
+                             "sample": f"{args.steps} sweeps of the {L}x{K} system; "
+                                       "oracle/lij_oracle.c, OpenMP over lines"},
+            "e2e": {"value": round(v, 3), "unit": "rhs-solves/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
 def run_batch_reference(args):
     """The oracle on the host cores for a batched workload: one FP64 sweep of
     the batch's median-size system per step (a bounded sample), in cell-sweeps/s."""
@@ -465,11 +694,16 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2", choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS))
+    ap.add_argument("--config", default="c2",
+                    choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS))
     ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
+    if args.config in SERVE_CONFIGS:
+        if args.impl == "reference":
+            return run_serving_reference(args)
+        return run_serving(args)
     if args.config in BATCH_CONFIGS:
         if args.impl == "reference":
             return run_batch_reference(args)

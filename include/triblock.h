@@ -325,6 +325,62 @@ int tbs_batch_profile_reset(tbs_batch *batch);
 int tbs_batch_profile_read(tbs_batch *batch, int *n, const char **names,
                            long long *launches, double *ms);
 
+/* ================================================================= serving
+ * A request loop on one GPU (no counterpart in the reference).  Systems are
+ * registered once and stay factored in HBM.  Requests bring 1.. right-hand
+ * sides for a system and, optionally, new Jacobian values (same mesh) that
+ * re-factor it before the request's solves; the loop runs on a thread of
+ * the server.  It admits queued requests in arrival order while their
+ * right-hand sides fit the device budget (resident systems plus the
+ * vectors of every right-hand side in flight) and the limit on right-hand
+ * sides in flight; a request that does not fit holds back the later ones.
+ * All admitted right-hand sides are swept together (continuous batching):
+ * a request that arrives while others are on the GPU joins them at the
+ * next sweep boundary, and each right-hand side leaves when it reaches its
+ * tolerance or sweep limit.  Re-factorizations run on a second thread while
+ * the other systems keep sweeping; a system is re-factored only when none
+ * of its right-hand sides is in flight.  Every solution is bit-identical to
+ * tbs_solve of the same system and right-hand side on its own.
+ * The rhs, U_out and new Jacobian arrays stay owned by the caller and must
+ * stay valid until tbs_server_wait returns for the request. */
+typedef struct tbs_server tbs_server;
+/* algo: TBS_ALGO_FP64 or TBS_ALGO_MIXED; device_budget_bytes: systems plus
+ * right-hand sides in flight; max_rhs_in_flight >= 1 */
+int tbs_server_create(int device_id, int algo, size_t device_budget_bytes,
+                      int max_rhs_in_flight, tbs_server **out);
+/* finishes the right-hand sides in flight; queued requests fail */
+int tbs_server_destroy(tbs_server *srv);
+const char *tbs_server_last_error(const tbs_server *srv);
+/* sweeps per graph launch at most (default 4): how long a new arrival can
+ * wait for the next sweep boundary */
+int tbs_server_set_chunk(tbs_server *srv, int sweeps);
+/* uploads and factors a system (blocking); arrays as tbs_set_mesh and
+ * tbs_set_jacobian */
+int tbs_server_add_system(tbs_server *srv, int nvar, int nelem, int nintface, int eftot,
+                          int nline, int nlineelem, const int *epoint, const int *ef,
+                          const int *fc, const int *linesize, const int *linepoint,
+                          const int *lines, const int *lineface, const double *jacD,
+                          const double *jacO1, const double *jacO2, int *system_id);
+/* device bytes the system holds and one right-hand side of it needs in
+ * flight with a sweep limit of max_sweeps (the admission footprint) */
+int tbs_server_system_bytes(tbs_server *srv, int system_id, int max_sweeps,
+                            size_t *resident, size_t *per_rhs);
+/* rhs and U_out: nrhs x 9*nelem doubles, element order; jacD/jacO1/jacO2
+ * NULL keeps the factors.  Returns at once with the request's id. */
+int tbs_server_submit(tbs_server *srv, int system_id, int nrhs, const double *rhs,
+                      double *U_out, double rel_tol, int max_sweeps, const double *jacD,
+                      const double *jacO1, const double *jacO2, long long *request_id);
+int tbs_server_poll(tbs_server *srv, long long request_id, int *done);
+/* blocks until the request is done, then forgets it: sweeps[nrhs],
+ * rel_residual[nrhs] (final / initial norm), latency (submit to done) and
+ * queueing time (submit to admission) in ms; any output may be NULL */
+int tbs_server_wait(tbs_server *srv, long long request_id, int *sweeps,
+                    double *rel_residual, double *latency_ms, double *queue_ms);
+/* stats[0..n): requests done, right-hand sides done, graph launches,
+ * re-factorizations, peak right-hand sides in flight, peak bytes of
+ * right-hand sides in flight, bytes of resident systems, requests queued */
+int tbs_server_stats(tbs_server *srv, long long *stats, int n);
+
 /* Library version string. */
 const char *tbs_version(void);
 

@@ -104,6 +104,18 @@ _sig("tbs_batch_set_inner_sweeps", _i, _vp, _i)
 _sig("tbs_batch_profile_enable", _i, _vp, _i)
 _sig("tbs_batch_profile_reset", _i, _vp)
 _sig("tbs_batch_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)
+_sig("tbs_server_create", _i, _i, _i, C.c_size_t, _i, C.POINTER(_vp))
+_sig("tbs_server_destroy", _i, _vp)
+_sig("tbs_server_last_error", _cp, _vp)
+_sig("tbs_server_set_chunk", _i, _vp, _i)
+_sig("tbs_server_add_system", _i, _vp, _i, _i, _i, _i, _i, _i, _ip, _ip, _ip, _ip, _ip, _ip, _ip,
+     _dp, _dp, _dp, _ip)
+_sig("tbs_server_system_bytes", _i, _vp, _i, _i, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t))
+_sig("tbs_server_submit", _i, _vp, _i, _i, _dp, _dp, C.c_double, _i, _dp, _dp, _dp,
+     C.POINTER(C.c_longlong))
+_sig("tbs_server_poll", _i, _vp, C.c_longlong, _ip)
+_sig("tbs_server_wait", _i, _vp, C.c_longlong, _ip, _dp, _dp, _dp)
+_sig("tbs_server_stats", _i, _vp, C.POINTER(C.c_longlong), _i)
 
 
 class TbsError(RuntimeError):
@@ -122,6 +134,12 @@ def last_error(ctx=None) -> str:
 def check(code: int, ctx=None) -> None:
     if code != TBS_OK:
         raise TbsError(code, last_error(ctx))
+
+
+def check_server(code: int, srv=None) -> None:
+    if code != TBS_OK:
+        s = lib.tbs_server_last_error(srv)
+        raise TbsError(code, s.decode() if s else "")
 
 
 def check_batch(code: int, batch=None) -> None:

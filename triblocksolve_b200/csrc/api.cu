@@ -12,7 +12,7 @@
  * tbs_solve runs the sweep loop as one CUDA graph whose while-node is
  * driven by a device-side convergence test, so a solve costs one launch.
  */
-#include "tbs_internal.hxx"
+#include "ctx.hxx"
 
 #include <cuda_runtime.h>
 
@@ -25,83 +25,6 @@
 #include <vector>
 
 using namespace tbs;
-
-namespace {
-
-struct ProfSlot {
-    const char *name;
-    long long launches;
-    double ms;
-};
-
-struct PendingEvent {
-    int slot;
-    cudaEvent_t a, b;
-};
-
-}  // namespace
-
-struct tbs_ctx {
-    int device = 0;
-    cudaStream_t own = nullptr;
-    cudaStream_t stream = nullptr;
-    std::string err;
-
-    /* ---- mesh ---- */
-    bool have_mesh = false, have_jac = false, factored = false;
-    int nvar = 0, nelem = 0, nintface = 0, eftot = 0, nline = 0, nlineelem = 0, max_line = 0;
-    std::vector<int> h_epoint, h_ef, h_fc, h_linesize, h_linepoint, h_lines, h_lineface;
-    int *d_epoint = nullptr, *d_ef = nullptr, *d_fc = nullptr, *d_linesize = nullptr;
-    int *d_linepoint = nullptr, *d_lines = nullptr, *d_lineface = nullptr, *d_identity = nullptr;
-
-    /* ---- Jacobian (element / face order, as read) ---- */
-    double *d_jacD = nullptr, *d_O1 = nullptr, *d_O2 = nullptr, *d_rhs = nullptr;
-    double *d_U = nullptr, *d_dU = nullptr, *d_R = nullptr, *d_Uinit = nullptr;
-    double *d_scratch = nullptr; /* 9*nelem element-order scratch */
-
-    /* ---- TBS_ALGO_REFERENCE ---- */
-    double *d_DLU = nullptr, *d_DinvC = nullptr, *d_A = nullptr;
-
-    /* ---- line-ordered layout (FP64 / MIXED) ---- */
-    FastLayout L{};
-    bool layout_ok = false;
-    double *d_gamlast = nullptr; /* per line and chain: last Gam toward the twist, FP64 */
-    long long n_xslots_real = 0;
-    double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
-    double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
-    double *d_rhsp = nullptr, *d_Rp = nullptr;
-    float *d_Dinv32 = nullptr, *d_G32 = nullptr, *d_Gam32 = nullptr, *d_X32 = nullptr;
-    float *d_b32 = nullptr, *d_y32 = nullptr, *d_d32 = nullptr, *d_c32 = nullptr,
-          *d_R32 = nullptr;
-    int inner_sweeps = 4;
-
-    /* ---- norms / solve state ---- */
-    double *d_partials = nullptr, *d_partials2 = nullptr;
-    int npart_cap = 0;
-    SolveState *d_state = nullptr;
-    SolveState *h_state = nullptr; /* pinned */
-    double *d_hist = nullptr;
-    int hist_cap = 0;
-    unsigned *d_status = nullptr;
-    unsigned *h_status = nullptr; /* pinned */
-    unsigned *d_counter = nullptr; /* last-CTA ticket of the fused norm */
-    int algo = -1;
-
-    /* ---- graph cache ---- */
-    cudaGraphExec_t gexec = nullptr;
-    cudaGraph_t graph = nullptr;
-    int graph_algo = -1;
-
-    /* ---- memory accounting ---- */
-    std::vector<std::pair<void *, size_t>> allocs;
-    size_t bytes = 0;
-
-    /* ---- profiling ---- */
-    bool prof = false;
-    std::vector<ProfSlot> slots;
-    std::vector<PendingEvent> pending;
-    std::vector<cudaEvent_t> pool;
-};
 
 /* ================================================================ errors */
 
@@ -555,7 +478,7 @@ static int body(tbs_ctx *ctx, CondCtl cc) {
     return reduce(ctx, full_resid_blocks(ne), 0, cc);
 }
 
-static int ensure_hist(tbs_ctx *ctx, int need) {
+int ctx_ensure_hist(tbs_ctx *ctx, int need) {
     if (need <= ctx->hist_cap) return TBS_OK;
     drop_graph(ctx);
     dfree(ctx, &ctx->d_hist);
@@ -567,7 +490,7 @@ static int ensure_hist(tbs_ctx *ctx, int need) {
 
 /* write the control block of the device SolveState (tol, max_sweeps,
  * hist_cap), leaving the recorded norms alone */
-static int set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
+int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
     SolveState *h = ctx->h_state;
     h->tol = tol;
     h->max_sweeps = max_sweeps;
@@ -973,9 +896,9 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
     CK(cudaSetDevice(ctx->device));
     if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
     if (n < 0) return ctx_fail(ctx, TBS_ERR_ARG, "negative sweep count");
-    int rc = ensure_hist(ctx, n + 1);
+    int rc = ctx_ensure_hist(ctx, n + 1);
     if (rc) return rc;
-    rc = set_state(ctx, 0.0, n);
+    rc = ctx_set_state(ctx, 0.0, n);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
     /* the current residual norm (recorded by the last sequence) opens the history */
@@ -999,9 +922,9 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
     CK(cudaSetDevice(ctx->device));
     if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
     if (max_sweeps < 0 || !(rel_tol >= 0.0)) return ctx_fail(ctx, TBS_ERR_ARG, "bad tolerance or sweep limit");
-    int rc = ensure_hist(ctx, max_sweeps + 1);
+    int rc = ctx_ensure_hist(ctx, max_sweeps + 1);
     if (rc) return rc;
-    rc = set_state(ctx, rel_tol, max_sweeps);
+    rc = ctx_set_state(ctx, rel_tol, max_sweeps);
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
     if (ctx->prof) {
@@ -1262,740 +1185,3 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
 
 }  // extern "C"
 
-/* ================================================================ batches
- * Many independent systems (contexts factored with the same algorithm on
- * one GPU) solved together.  Every launch covers the work units of all
- * systems still above their tolerance: one persistent Thomas launch over
- * their lines from a device work queue, one residual launch over their
- * tiles, one launch for the per-system norms.  The per-unit arithmetic and
- * the order of every norm sum are those of the single-system sequences
- * (prime / body above), so each system's iterates are bit-identical to a
- * tbs_solve of its context alone. */
-
-struct tbs_batch {
-    int device = 0;
-    cudaStream_t own = nullptr;    /* created with the batch */
-    cudaStream_t stream = nullptr; /* where the launches go: own or the caller's */
-    std::string err;
-    std::vector<tbs_ctx *> sys;
-    int algo = -1;
-    int inner = 4;
-    BatchSched sched{8, 2};
-    int order = 0; /* 0: longest lines first, 1: mesh order */
-    int max_nx = 0;
-    /* device: descriptors and work lists (one allocation each) */
-    std::vector<void *> allocs;
-    ThomasSys<double> *d_th64 = nullptr;
-    ThomasSys<float> *d_th32 = nullptr;
-    ResidSys<double> *d_rs_prime = nullptr, *d_rs_body = nullptr;
-    ResidSys<float> *d_rs32_rhs = nullptr, *d_rs32_dx = nullptr;
-    FullResSys *d_fr = nullptr;
-    VecSys *d_vec = nullptr;
-    ReduceSys *d_red_prime = nullptr, *d_red_body = nullptr;
-    WorkItem *d_lines_lpt = nullptr, *d_lines_mesh = nullptr, *d_tiles = nullptr,
-             *d_prime_tiles = nullptr, *d_blocks = nullptr;
-    int nlines = 0, ntiles = 0, nprime_tiles = 0, nblocks = 0;
-    int *d_active = nullptr;
-    unsigned *d_queue = nullptr, *d_counter = nullptr, *d_status = nullptr;
-    unsigned *h_status = nullptr; /* pinned */
-    /* what the descriptors and the graph were built from */
-    std::vector<const void *> fingerprint;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t gexec = nullptr;
-    bool graph_ok = false;
-    /* profiling (eager launches bracketed by events) */
-    bool prof = false;
-    std::vector<ProfSlot> slots;
-    std::vector<PendingEvent> pending;
-    std::vector<cudaEvent_t> pool;
-};
-
-static int bfail(tbs_batch *b, int code, const std::string &msg) {
-    if (b) b->err = msg;
-    set_thread_error(msg);
-    return code;
-}
-
-#define BCK(call)                                                                         \
-    do {                                                                                  \
-        cudaError_t e_ = (call);                                                          \
-        if (e_ != cudaSuccess)                                                            \
-            return bfail(b, TBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
-    } while (0)
-
-#define BCKL(call)                                                                        \
-    do {                                                                                  \
-        int e_ = (call);                                                                  \
-        if (e_ != 0)                                                                      \
-            return bfail(b, TBS_ERR_CUDA,                                                 \
-                         std::string(#call) + ": " + cudaGetErrorString((cudaError_t)e_)); \
-    } while (0)
-
-template <typename T>
-static int balloc(tbs_batch *b, T **p, size_t count) {
-    void *q = nullptr;
-    const size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
-    cudaError_t e = cudaMalloc(&q, nbytes);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return bfail(b, TBS_ERR_NOMEM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed");
-    }
-    b->allocs.push_back(q);
-    *p = static_cast<T *>(q);
-    return TBS_OK;
-}
-
-template <typename T>
-static int bupload(tbs_batch *b, T **p, const std::vector<T> &h) {
-    if (!*p) {
-        int rc = balloc(b, p, h.size());
-        if (rc) return rc;
-    }
-    if (!h.empty())
-        BCK(cudaMemcpyAsync(*p, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, b->stream));
-    return TBS_OK;
-}
-
-static void bdrop_graph(tbs_batch *b) {
-    if (b->gexec) cudaGraphExecDestroy(b->gexec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->gexec = nullptr;
-    b->graph = nullptr;
-    b->graph_ok = false;
-}
-
-/* every device pointer and setting the descriptors and graph depend on */
-static std::vector<const void *> batch_fingerprint(tbs_batch *b) {
-    std::vector<const void *> f;
-    for (tbs_ctx *c : b->sys) {
-        const void *p[] = {c->d_G, c->d_Gam, c->d_Dinv, c->d_X, c->d_b, c->d_y, c->d_dUp, c->d_Up,
-                           c->d_rhsp, c->d_Rp, c->d_partials, c->d_state, c->d_hist, c->d_Uinit,
-                           c->d_G32, c->d_Gam32, c->d_Dinv32, c->d_X32, c->d_b32, c->d_y32,
-                           c->d_d32, c->d_c32, c->d_R32, c->L.line_start, c->L.xnbr, c->d_jacD,
-                           c->d_O1, c->d_O2, c->d_rhs, c->d_epoint};
-        f.insert(f.end(), std::begin(p), std::end(p));
-        f.push_back(reinterpret_cast<const void *>((uintptr_t)c->algo));
-    }
-    f.push_back(reinterpret_cast<const void *>((uintptr_t)b->inner));
-    return f;
-}
-
-static int batch_check_members(tbs_batch *b) {
-    for (size_t s = 0; s < b->sys.size(); ++s) {
-        tbs_ctx *c = b->sys[s];
-        if (!c->factored || !c->layout_ok)
-            return bfail(b, TBS_ERR_STATE, "batch member " + std::to_string(s) + " is not factored");
-        if (c->algo != b->algo)
-            return bfail(b, TBS_ERR_STATE,
-                         "batch member " + std::to_string(s) + " was re-factored with another algorithm");
-    }
-    return TBS_OK;
-}
-
-/* descriptors of every launch, from the members' current arrays */
-static int batch_descriptors(tbs_batch *b) {
-    const int n = (int)b->sys.size();
-    std::vector<ThomasSys<double>> th64;
-    std::vector<ThomasSys<float>> th32;
-    std::vector<ResidSys<double>> rsp, rsb;
-    std::vector<ResidSys<float>> rs32r, rs32d;
-    std::vector<FullResSys> fr;
-    std::vector<VecSys> vec;
-    std::vector<ReduceSys> redp, redb;
-    std::vector<WorkItem> prime_tiles;
-    const bool mixed = b->algo == TBS_ALGO_MIXED;
-    for (int s = 0; s < n; ++s) {
-        tbs_ctx *c = b->sys[s];
-        const FastLayout &L = c->L;
-        const int nt = fast_resid_grid(L.np16);
-        if (!mixed) {
-            th64.push_back({L.line_start, L.line_len, L.line_twist, c->d_G, c->d_Gam, c->d_b, c->d_y,
-                            c->d_dUp});
-            /* prime: R = rhs (U = 0, cleared here) or the residual of U_init */
-            rsp.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv, c->d_X, c->d_dUp,
-                           c->d_Uinit ? c->d_Rp : c->d_rhsp, c->d_b, c->d_Uinit ? nullptr : c->d_Up,
-                           c->d_partials});
-            rsb.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv, c->d_X, c->d_dUp, nullptr, c->d_b,
-                           c->d_Up, c->d_partials});
-            redp.push_back({c->d_partials, nt, 0, c->d_state, c->d_hist});
-            redb.push_back({c->d_partials, nt, 0, c->d_state, c->d_hist});
-        } else {
-            th32.push_back({L.line_start, L.line_len, L.line_twist, c->d_G32, c->d_Gam32, c->d_b32,
-                            c->d_y32, c->d_d32});
-            rs32r.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv32, c->d_X32, c->d_d32, c->d_R32,
-                             c->d_b32, c->d_c32, nullptr});
-            rs32d.push_back({L.np16, L.nx, L.xnbr, nullptr, c->d_X32, c->d_d32, nullptr, c->d_b32,
-                             c->d_c32, nullptr});
-            fr.push_back({c->nelem, 0, c->d_epoint, c->d_ef, c->d_fc, L.pos_of_elem, c->d_jacD,
-                          c->d_O1, c->d_O2, c->d_rhs, c->d_Up, c->d_R32, c->d_partials});
-            vec.push_back({c->d_rhsp, c->d_R32, c->d_c32, c->d_d32, c->d_Up, c->d_partials});
-            redp.push_back({c->d_partials, c->d_Uinit ? full_resid_blocks(c->nelem) : nt, 0,
-                            c->d_state, c->d_hist});
-            redb.push_back({c->d_partials, full_resid_blocks(c->nelem), 0, c->d_state, c->d_hist});
-            if (!c->d_Uinit)
-                for (int t = 0; t < nt; ++t) prime_tiles.push_back({s, t});
-        }
-    }
-    int rc = TBS_OK;
-    if (!mixed) {
-        if (!rc) rc = bupload(b, &b->d_th64, th64);
-        if (!rc) rc = bupload(b, &b->d_rs_prime, rsp);
-        if (!rc) rc = bupload(b, &b->d_rs_body, rsb);
-    } else {
-        if (!rc) rc = bupload(b, &b->d_th32, th32);
-        if (!rc) rc = bupload(b, &b->d_rs32_rhs, rs32r);
-        if (!rc) rc = bupload(b, &b->d_rs32_dx, rs32d);
-        if (!rc) rc = bupload(b, &b->d_fr, fr);
-        if (!rc) rc = bupload(b, &b->d_vec, vec);
-        /* the prime tile list depends on which members start from U_init */
-        if (!rc && b->d_prime_tiles && (int)prime_tiles.size() > b->nprime_tiles) {
-            cudaFree(b->d_prime_tiles);
-            b->allocs.erase(std::find(b->allocs.begin(), b->allocs.end(), (void *)b->d_prime_tiles));
-            b->d_prime_tiles = nullptr;
-        }
-        if (!rc) rc = bupload(b, &b->d_prime_tiles, prime_tiles);
-        b->nprime_tiles = (int)prime_tiles.size();
-    }
-    if (!rc) rc = bupload(b, &b->d_red_prime, redp);
-    if (!rc) rc = bupload(b, &b->d_red_body, redb);
-    if (!rc) BCK(cudaStreamSynchronize(b->stream));
-    return rc;
-}
-
-static cudaEvent_t bprof_event(tbs_batch *b) {
-    if (!b->pool.empty()) {
-        cudaEvent_t e = b->pool.back();
-        b->pool.pop_back();
-        return e;
-    }
-    cudaEvent_t e = nullptr;
-    cudaEventCreate(&e);
-    return e;
-}
-
-static void bprof_resolve(tbs_batch *b) {
-    if (b->pending.empty()) return;
-    cudaStreamSynchronize(b->stream);
-    for (auto &p : b->pending) {
-        float ms = 0.f;
-        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && p.slot >= 0) {
-            b->slots[p.slot].ms += ms;
-            b->slots[p.slot].launches += 1;
-        }
-        b->pool.push_back(p.a);
-        b->pool.push_back(p.b);
-    }
-    b->pending.clear();
-}
-
-template <typename F>
-static int btimed(tbs_batch *b, const char *name, F &&launch) {
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    cudaStreamIsCapturing(b->stream, &cs);
-    if (!b->prof || cs != cudaStreamCaptureStatusNone) return launch();
-    int slot = -1;
-    for (size_t i = 0; i < b->slots.size(); ++i)
-        if (std::strcmp(b->slots[i].name, name) == 0) slot = (int)i;
-    if (slot < 0 && b->slots.size() < TBS_PROFILE_MAX) {
-        b->slots.push_back({name, 0, 0.0});
-        slot = (int)b->slots.size() - 1;
-    }
-    if (b->pending.size() > 4000) bprof_resolve(b);
-    PendingEvent pe{slot, bprof_event(b), bprof_event(b)};
-    cudaEventRecord(pe.a, b->stream);
-    int rc = launch();
-    cudaEventRecord(pe.b, b->stream);
-    b->pending.push_back(pe);
-    return rc;
-}
-
-#define BRUN(name, call) BCKL(btimed(b, name, [&]() { return (int)(call); }))
-
-static const WorkItem *batch_lines(tbs_batch *b) {
-    return b->order == 0 ? b->d_lines_lpt : b->d_lines_mesh;
-}
-
-/* start of a batched solve: every member's residual of U_init (or rhs),
- * its norm recorded as ||R_0|| and its active flag */
-static int batch_prime(tbs_batch *b, CondCtl cc) {
-    cudaStream_t st = b->stream;
-    const int n = (int)b->sys.size();
-    for (tbs_ctx *c : b->sys) {
-        if (!c->d_Uinit) continue;
-        const FastLayout &L = c->L;
-        BRUN("permute", launch_permute_to_pos(st, 9, c->nelem, L.pos_of_elem, c->d_Uinit, c->d_Up));
-        if (b->algo == TBS_ALGO_FP64)
-            BRUN("full_resid", launch_full_resid<double>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
-                                                         L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
-                                                         c->d_rhs, c->d_Up, c->d_Rp, c->d_partials2));
-        else
-            BRUN("full_resid", launch_full_resid<float>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
-                                                        L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
-                                                        c->d_rhs, c->d_Up, c->d_R32, c->d_partials));
-    }
-    if (b->algo == TBS_ALGO_FP64) {
-        BRUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, b->max_nx, b->d_rs_prime, b->d_tiles,
-                                                          b->ntiles, nullptr, b->d_status));
-        BRUN("reduce_norm", launch_reduce_batch(st, 160, b->d_red_prime, n, 1, b->d_active,
-                                                b->d_counter, cc.handle, cc.use_cond));
-    } else {
-        BRUN("mixed_prime", launch_mixed_prime_batch(st, b->d_vec, b->d_prime_tiles, b->nprime_tiles));
-        BRUN("reduce_norm", launch_reduce_batch(st, 256, b->d_red_prime, n, 1, b->d_active,
-                                                b->d_counter, cc.handle, cc.use_cond));
-    }
-    return TBS_OK;
-}
-
-/* one sweep of every active member */
-static int batch_body(tbs_batch *b, CondCtl cc) {
-    cudaStream_t st = b->stream;
-    const int n = (int)b->sys.size();
-    if (b->algo == TBS_ALGO_FP64) {
-        BRUN("fast_thomas", launch_thomas_batch<double>(st, b->sched, b->d_th64, batch_lines(b),
-                                                        b->nlines, b->d_active, b->d_queue,
-                                                        b->d_status));
-        BRUN("fast_resid", launch_resid_batch<double>(st, 1, b->max_nx, b->d_rs_body, b->d_tiles,
-                                                      b->ntiles, b->d_active, b->d_status));
-        BRUN("reduce_norm", launch_reduce_batch(st, 160, b->d_red_body, n, 0, b->d_active,
-                                                b->d_counter, cc.handle, cc.use_cond));
-        return TBS_OK;
-    }
-    BRUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, b->max_nx, b->d_rs32_rhs, b->d_tiles,
-                                                       b->ntiles, b->d_active, b->d_status));
-    for (int m = 0; m < b->inner; ++m) {
-        BRUN("fast_thomas32", launch_thomas_batch<float>(st, b->sched, b->d_th32, batch_lines(b),
-                                                         b->nlines, b->d_active, b->d_queue,
-                                                         b->d_status));
-        if (m + 1 < b->inner)
-            BRUN("fast_resid32", launch_resid_batch<float>(st, 3, b->max_nx, b->d_rs32_dx, b->d_tiles,
-                                                           b->ntiles, b->d_active, b->d_status));
-    }
-    BRUN("axpy", launch_axpy2_batch(st, b->d_vec, b->d_tiles, b->ntiles, b->d_active));
-    BRUN("full_resid", launch_full_resid_batch(st, b->d_fr, b->d_blocks, b->nblocks, b->d_active));
-    BRUN("reduce_norm", launch_reduce_batch(st, 256, b->d_red_body, n, 0, b->d_active, b->d_counter,
-                                            cc.handle, cc.use_cond));
-    return TBS_OK;
-}
-
-static int batch_build_graph(tbs_batch *b) {
-    bdrop_graph(b);
-    cudaStream_t st = b->stream;
-    cudaGraph_t g = nullptr;
-    BCK(cudaGraphCreate(&g, 0));
-    b->graph = g;
-    cudaGraphConditionalHandle h;
-    BCK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    const CondCtl cc{(unsigned long long)h, 1};
-    BCK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = batch_prime(b, cc);
-    cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    if (rc == TBS_OK) {
-        cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
-        if (e != cudaSuccess) rc = bfail(b, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(e));
-    }
-    cudaGraphNode_t cnode = nullptr;
-    cudaGraph_t bodyg = nullptr;
-    if (rc == TBS_OK) {
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaError_t e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
-        if (e != cudaSuccess) rc = bfail(b, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(e));
-        else bodyg = cp.conditional.phGraph_out[0];
-    }
-    if (rc == TBS_OK) {
-        cudaError_t e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
-        if (e != cudaSuccess) rc = bfail(b, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(e));
-    }
-    cudaGraph_t outg = nullptr;
-    cudaError_t ee = cudaStreamEndCapture(st, &outg);
-    if (rc == TBS_OK && ee != cudaSuccess) rc = bfail(b, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
-    if (rc != TBS_OK) {
-        bdrop_graph(b);
-        return rc;
-    }
-    BCK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = batch_body(b, cc);
-    ee = cudaStreamEndCapture(st, &outg);
-    if (rc == TBS_OK && ee != cudaSuccess) rc = bfail(b, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
-    if (rc != TBS_OK) {
-        bdrop_graph(b);
-        return rc;
-    }
-    cudaError_t ie = cudaGraphInstantiate(&b->gexec, g, 0);
-    if (ie != cudaSuccess) {
-        bdrop_graph(b);
-        return bfail(b, TBS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
-    }
-    b->graph_ok = true;
-    return TBS_OK;
-}
-
-static int batch_status(tbs_batch *b) {
-    BCK(cudaMemcpyAsync(b->h_status, b->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, b->stream));
-    BCK(cudaStreamSynchronize(b->stream));
-    const unsigned s = *b->h_status;
-    if (s) {
-        BCK(cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), b->stream));
-        BCK(cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(unsigned), b->stream));
-        BCK(cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream));
-        BCK(cudaStreamSynchronize(b->stream));
-        if (s & ST_TIMEOUT) return bfail(b, TBS_ERR_CUDA, "a device-side wait ran out of its time budget");
-        return bfail(b, TBS_ERR_CUDA, "device status " + std::to_string(s));
-    }
-    return TBS_OK;
-}
-
-/* members' device state (tolerance, sweep limit, history capacity) and
- * the descriptors / graph, refreshed when a member's arrays changed */
-static int batch_ready(tbs_batch *b, double tol, int max_sweeps) {
-    int rc = batch_check_members(b);
-    if (rc) return rc;
-    for (tbs_ctx *c : b->sys) {
-        BCK(cudaStreamSynchronize(c->stream));
-        rc = ensure_hist(c, max_sweeps + 1);
-        if (!rc) rc = set_state(c, tol, max_sweeps);
-        if (rc) return bfail(b, rc, "batch member: " + c->err);
-        BCK(cudaStreamSynchronize(c->stream));
-    }
-    std::vector<const void *> fp = batch_fingerprint(b);
-    if (fp != b->fingerprint) {
-        bdrop_graph(b);
-        rc = batch_descriptors(b);
-        if (rc) return rc;
-        b->fingerprint = fp;
-    }
-    return TBS_OK;
-}
-
-static int batch_destroy_all(tbs_batch *b) {
-    if (!b) return TBS_OK;
-    cudaSetDevice(b->device);
-    if (b->stream) cudaStreamSynchronize(b->stream);
-    bprof_resolve(b);
-    bdrop_graph(b);
-    for (void *p : b->allocs) cudaFree(p);
-    for (cudaEvent_t e : b->pool) cudaEventDestroy(e);
-    if (b->h_status) cudaFreeHost(b->h_status);
-    if (b->own) cudaStreamDestroy(b->own);
-    delete b;
-    return TBS_OK;
-}
-
-extern "C" {
-
-const char *tbs_batch_last_error(const tbs_batch *b) {
-    if (!b) return thread_error();
-    return b->err.c_str();
-}
-
-int tbs_batch_create(tbs_ctx *const *systems, int nsys, tbs_batch **out) {
-    tbs_batch *b = nullptr;
-    if (!out || !systems || nsys < 1) return bfail(nullptr, TBS_ERR_ARG, "tbs_batch_create: bad arguments");
-    *out = nullptr;
-    try {
-        b = new tbs_batch();
-    } catch (...) {
-        return bfail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
-    }
-    auto fail = [&](int rc) {
-        std::string msg = b->err;
-        batch_destroy_all(b);
-        set_thread_error(msg);
-        return rc;
-    };
-    try {
-        for (int s = 0; s < nsys; ++s) {
-            tbs_ctx *c = systems[s];
-            if (!c) return fail(bfail(b, TBS_ERR_ARG, "null system " + std::to_string(s)));
-            for (int t = 0; t < s; ++t)
-                if (systems[t] == c)
-                    return fail(bfail(b, TBS_ERR_ARG, "system " + std::to_string(s) + " appears twice"));
-            if (!c->factored)
-                return fail(bfail(b, TBS_ERR_STATE, "system " + std::to_string(s) + " is not factored"));
-            if (c->algo != TBS_ALGO_FP64 && c->algo != TBS_ALGO_MIXED)
-                return fail(bfail(b, TBS_ERR_UNSUPPORTED,
-                                  "batches take TBS_ALGO_FP64 or TBS_ALGO_MIXED systems"));
-            if (s > 0 && (c->algo != systems[0]->algo || c->device != systems[0]->device))
-                return fail(bfail(b, TBS_ERR_ARG,
-                                  "all systems of a batch need the same algorithm and GPU"));
-            b->sys.push_back(c);
-        }
-        b->algo = systems[0]->algo;
-        b->device = systems[0]->device;
-        b->inner = systems[0]->inner_sweeps;
-        if (cudaSetDevice(b->device) != cudaSuccess)
-            return fail(bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed"));
-        if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess)
-            return fail(bfail(b, TBS_ERR_CUDA, "cudaStreamCreate failed"));
-        b->stream = b->own;
-        if (cudaMallocHost(&b->h_status, sizeof(unsigned)) != cudaSuccess)
-            return fail(bfail(b, TBS_ERR_NOMEM, "pinned allocation failed"));
-        /* work lists */
-        std::vector<WorkItem> lines, tiles, blocks;
-        std::vector<int> len;
-        for (int s = 0; s < nsys; ++s) {
-            tbs_ctx *c = b->sys[s];
-            b->max_nx = std::max(b->max_nx, c->L.nx);
-            for (int l = 0; l < c->nline; ++l) {
-                lines.push_back({s, l});
-                len.push_back(c->h_linesize[l]);
-            }
-            for (int t = 0; t < fast_resid_grid(c->L.np16); ++t) tiles.push_back({s, t});
-            for (int k = 0; k < full_resid_blocks(c->nelem); ++k) blocks.push_back({s, k});
-        }
-        std::vector<int> idx(lines.size());
-        for (size_t k = 0; k < idx.size(); ++k) idx[k] = (int)k;
-        std::stable_sort(idx.begin(), idx.end(), [&](int x, int y) { return len[x] > len[y]; });
-        std::vector<WorkItem> lpt(lines.size());
-        for (size_t k = 0; k < idx.size(); ++k) lpt[k] = lines[idx[k]];
-        b->nlines = (int)lines.size();
-        b->ntiles = (int)tiles.size();
-        b->nblocks = (int)blocks.size();
-        int rc = bupload(b, &b->d_lines_lpt, lpt);
-        if (!rc) rc = bupload(b, &b->d_lines_mesh, lines);
-        if (!rc) rc = bupload(b, &b->d_tiles, tiles);
-        if (!rc && b->algo == TBS_ALGO_MIXED) rc = bupload(b, &b->d_blocks, blocks);
-        if (!rc) rc = balloc(b, &b->d_active, (size_t)nsys);
-        if (!rc) rc = balloc(b, &b->d_queue, 2);
-        if (!rc) rc = balloc(b, &b->d_counter, 1);
-        if (!rc) rc = balloc(b, &b->d_status, 1);
-        if (rc) return fail(rc);
-        if (cudaMemsetAsync(b->d_active, 0, nsys * sizeof(int), b->stream) != cudaSuccess ||
-            cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(unsigned), b->stream) != cudaSuccess ||
-            cudaMemsetAsync(b->d_counter, 0, sizeof(unsigned), b->stream) != cudaSuccess ||
-            cudaMemsetAsync(b->d_status, 0, sizeof(unsigned), b->stream) != cudaSuccess)
-            return fail(bfail(b, TBS_ERR_CUDA, "cudaMemsetAsync failed"));
-        if (batch_prepare(b->max_nx)) return fail(bfail(b, TBS_ERR_CUDA, "shared-memory opt-in failed"));
-        /* default schedule: 2 stages, as many CTAs per SM as fit, at most 8 */
-        const int fit = b->algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(2) : thomas_batch_fit<float>(2);
-        if (fit < 1) return fail(bfail(b, TBS_ERR_CUDA, "the batched Thomas kernel does not fit on an SM"));
-        b->sched = BatchSched{std::min(fit, 8), 2};
-        if (cudaStreamSynchronize(b->stream) != cudaSuccess)
-            return fail(bfail(b, TBS_ERR_CUDA, "cudaStreamSynchronize failed"));
-    } catch (...) {
-        return fail(bfail(b, TBS_ERR_NOMEM, "host allocation failed"));
-    }
-    *out = b;
-    return TBS_OK;
-}
-
-int tbs_batch_destroy(tbs_batch *b) { return batch_destroy_all(b); }
-
-int tbs_batch_set_stream(tbs_batch *b, void *cuda_stream) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    cudaStream_t ns = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : b->own;
-    if (ns != b->stream) {
-        cudaStreamSynchronize(b->stream);
-        bdrop_graph(b);
-        b->stream = ns;
-    }
-    return TBS_OK;
-}
-
-int tbs_batch_size(const tbs_batch *b, int *nsys) {
-    if (!b || !nsys) return bfail(nullptr, TBS_ERR_ARG, "null argument");
-    *nsys = (int)b->sys.size();
-    return TBS_OK;
-}
-
-int tbs_batch_set_inner_sweeps(tbs_batch *b, int m) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (m < 1 || m > 64) return bfail(b, TBS_ERR_ARG, "inner sweeps must be in 1..64");
-    if (m != b->inner) bdrop_graph(b);
-    b->inner = m;
-    b->fingerprint.clear();
-    return TBS_OK;
-}
-
-int tbs_batch_set_schedule(tbs_batch *b, int ctas_per_sm, int stages, int order) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (stages < 2 || stages > 8 || ctas_per_sm < 1 || (order != 0 && order != 1))
-        return bfail(b, TBS_ERR_ARG, "bad schedule");
-    try {
-        BCK(cudaSetDevice(b->device));
-        const int fit = b->algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(stages)
-                                                 : thomas_batch_fit<float>(stages);
-        if (ctas_per_sm > fit)
-            return bfail(b, TBS_ERR_ARG, "schedule does not fit: at most " + std::to_string(fit) +
-                                             " CTAs per SM with " + std::to_string(stages) + " stages");
-        b->sched = BatchSched{ctas_per_sm, stages};
-        b->order = order;
-        bdrop_graph(b);
-    } catch (...) {
-        return bfail(b, TBS_ERR_STATE, "internal error");
-    }
-    return TBS_OK;
-}
-
-int tbs_batch_get_schedule(const tbs_batch *b, int *ctas_per_sm, int *stages, int *order) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (ctas_per_sm) *ctas_per_sm = b->sched.ctas_per_sm;
-    if (stages) *stages = b->sched.stages;
-    if (order) *order = b->order;
-    return TBS_OK;
-}
-
-int tbs_batch_solve(tbs_batch *b, double rel_tol, int max_sweeps, int *sweeps_out,
-                    double *hist_out) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (max_sweeps < 0 || !(rel_tol >= 0.0)) return bfail(b, TBS_ERR_ARG, "bad tolerance or sweep limit");
-    try {
-        BCK(cudaSetDevice(b->device));
-        int rc = batch_ready(b, rel_tol, max_sweeps);
-        if (rc) return rc;
-        cudaStream_t st = b->stream;
-        const int n = (int)b->sys.size();
-        if (b->prof) {
-            /* eager form with a host-side test, so that every kernel is timed */
-            rc = batch_prime(b, CondCtl{0, 0});
-            if (rc) return rc;
-            std::vector<int> act(n);
-            for (;;) {
-                BCK(cudaMemcpyAsync(act.data(), b->d_active, n * sizeof(int), cudaMemcpyDeviceToHost, st));
-                BCK(cudaStreamSynchronize(st));
-                bool any = false;
-                for (int v : act) any = any || v;
-                if (!any) break;
-                rc = batch_body(b, CondCtl{0, 0});
-                if (rc) return rc;
-            }
-            bprof_resolve(b);
-        } else {
-            if (!b->graph_ok) {
-                rc = batch_build_graph(b);
-                if (rc) return rc;
-            }
-            BCK(cudaGraphLaunch(b->gexec, st));
-        }
-        rc = batch_status(b);
-        if (rc) return rc;
-        for (int s = 0; s < n; ++s) {
-            tbs_ctx *c = b->sys[s];
-            BCK(cudaMemcpyAsync(c->h_state, c->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, st));
-        }
-        BCK(cudaStreamSynchronize(st));
-        for (int s = 0; s < n; ++s) {
-            tbs_ctx *c = b->sys[s];
-            const int sw = c->h_state->sweep;
-            if (sweeps_out) sweeps_out[s] = sw;
-            if (hist_out)
-                BCK(cudaMemcpyAsync(hist_out + (size_t)s * (max_sweeps + 1), c->d_hist,
-                                    (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double),
-                                    cudaMemcpyDeviceToHost, st));
-        }
-        BCK(cudaStreamSynchronize(st));
-    } catch (...) {
-        return bfail(b, TBS_ERR_STATE, "internal error");
-    }
-    return TBS_OK;
-}
-
-int tbs_batch_tune(tbs_batch *b, int *ctas_per_sm, int *stages, int *order, double *best_ms) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    try {
-        BCK(cudaSetDevice(b->device));
-        int rc = batch_ready(b, 0.0, 1);
-        if (rc) return rc;
-        cudaStream_t st = b->stream;
-        const int n = (int)b->sys.size();
-        std::vector<int> ones(n, 1);
-        BCK(cudaMemcpyAsync(b->d_active, ones.data(), n * sizeof(int), cudaMemcpyHostToDevice, st));
-        cudaEvent_t e0, e1;
-        BCK(cudaEventCreate(&e0));
-        BCK(cudaEventCreate(&e1));
-        const BatchSched keep = b->sched;
-        const int keep_order = b->order;
-        double best = 1e30;
-        BatchSched best_s = keep;
-        int best_o = keep_order;
-        const int cand_ctas[] = {2, 3, 4, 6, 8, 12, 16};
-        for (int ns = 2; ns <= 4 && !rc; ++ns) {
-            const int fit = b->algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(ns)
-                                                     : thomas_batch_fit<float>(ns);
-            for (int cps : cand_ctas) {
-                if (cps > fit || rc) continue;
-                for (int o = 0; o < 2 && !rc; ++o) {
-                    b->sched = BatchSched{cps, ns};
-                    b->order = o;
-                    auto launch = [&]() {
-                        return b->algo == TBS_ALGO_FP64
-                                   ? launch_thomas_batch<double>(st, b->sched, b->d_th64, batch_lines(b),
-                                                                 b->nlines, b->d_active, b->d_queue,
-                                                                 b->d_status)
-                                   : launch_thomas_batch<float>(st, b->sched, b->d_th32, batch_lines(b),
-                                                                b->nlines, b->d_active, b->d_queue,
-                                                                b->d_status);
-                    };
-                    int e = launch();
-                    const int reps = 3;
-                    if (!e) cudaEventRecord(e0, st);
-                    for (int r = 0; r < reps && !e; ++r) e = launch();
-                    if (!e) cudaEventRecord(e1, st);
-                    if (e) {
-                        rc = bfail(b, TBS_ERR_CUDA, std::string("tuning launch: ") +
-                                                        cudaGetErrorString((cudaError_t)e));
-                        break;
-                    }
-                    cudaEventSynchronize(e1);
-                    float ms = 0.f;
-                    cudaEventElapsedTime(&ms, e0, e1);
-                    rc = batch_status(b);
-                    if (rc) break;
-                    if (ms / reps < best) {
-                        best = ms / reps;
-                        best_s = b->sched;
-                        best_o = o;
-                    }
-                }
-            }
-        }
-        cudaEventDestroy(e0);
-        cudaEventDestroy(e1);
-        b->sched = rc ? keep : best_s;
-        b->order = rc ? keep_order : best_o;
-        bdrop_graph(b);
-        if (rc) return rc;
-        if (ctas_per_sm) *ctas_per_sm = best_s.ctas_per_sm;
-        if (stages) *stages = best_s.stages;
-        if (order) *order = best_o;
-        if (best_ms) *best_ms = best;
-    } catch (...) {
-        return bfail(b, TBS_ERR_STATE, "internal error");
-    }
-    return TBS_OK;
-}
-
-int tbs_batch_profile_enable(tbs_batch *b, int on) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (!on) bprof_resolve(b);
-    b->prof = on != 0;
-    return TBS_OK;
-}
-
-int tbs_batch_profile_reset(tbs_batch *b) {
-    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    bprof_resolve(b);
-    b->slots.clear();
-    return TBS_OK;
-}
-
-int tbs_batch_profile_read(tbs_batch *b, int *n, const char **names, long long *launches,
-                           double *ms) {
-    if (!b || !n) return bfail(b, TBS_ERR_ARG, "null argument");
-    bprof_resolve(b);
-    const int cap = *n, cnt = (int)b->slots.size();
-    for (int i = 0; i < cnt && i < cap; ++i) {
-        if (names) names[i] = b->slots[i].name;
-        if (launches) launches[i] = b->slots[i].launches;
-        if (ms) ms[i] = b->slots[i].ms;
-    }
-    *n = cnt;
-    return TBS_OK;
-}
-
-}  // extern "C"

@@ -1,0 +1,982 @@
+/*
+ * batch.cu -- the batched launch engine (engine.hxx) and the tbs_batch_*
+ * entry points: many independent factored systems solved together.
+ *
+ * Every launch covers the work units of all members still above their
+ * tolerance: one persistent Thomas launch over their lines from a device
+ * work queue, one persistent residual launch over their tiles and one
+ * launch for the per-member norms.  The per-unit arithmetic and the order
+ * of every norm sum are those of the single-system sequences in api.cu, so
+ * each member's iterates are bit-identical to a tbs_solve of it alone.
+ * No counterpart in the reference, whose driver (src/main.cxx) solves one
+ * system per process.
+ */
+#include "engine.hxx"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+using namespace tbs;
+
+namespace tbs {
+
+/* ================================================================ helpers */
+
+static int efail(Engine &e, int code, const std::string &msg) {
+    e.err = msg;
+    set_thread_error(msg);
+    return code;
+}
+
+#define ECK(call)                                                                         \
+    do {                                                                                  \
+        cudaError_t e_ = (call);                                                          \
+        if (e_ != cudaSuccess)                                                            \
+            return efail(e, TBS_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+    } while (0)
+
+#define ECKL(call)                                                                        \
+    do {                                                                                  \
+        int e_ = (call);                                                                  \
+        if (e_ != 0)                                                                      \
+            return efail(e, TBS_ERR_CUDA,                                                 \
+                         std::string(#call) + ": " + cudaGetErrorString((cudaError_t)e_)); \
+    } while (0)
+
+template <typename T>
+static int ealloc(Engine &e, T **p, size_t count) {
+    void *q = nullptr;
+    const size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (cudaMalloc(&q, nbytes) != cudaSuccess) {
+        cudaGetLastError();
+        return efail(e, TBS_ERR_NOMEM, "cudaMalloc of " + std::to_string(nbytes) + " bytes failed");
+    }
+    e.allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return TBS_OK;
+}
+
+template <typename T>
+static void efree(Engine &e, T **p) {
+    if (!*p) return;
+    auto it = std::find(e.allocs.begin(), e.allocs.end(), (void *)*p);
+    if (it != e.allocs.end()) e.allocs.erase(it);
+    cudaFree(*p);
+    *p = nullptr;
+}
+
+template <typename T>
+static int eupload(Engine &e, T *dst, const std::vector<T> &h) {
+    if (!h.empty())
+        ECK(cudaMemcpyAsync(dst, h.data(), h.size() * sizeof(T), cudaMemcpyHostToDevice, e.stream));
+    return TBS_OK;
+}
+
+static cudaEvent_t eprof_event(Engine &e) {
+    if (!e.pool.empty()) {
+        cudaEvent_t ev = e.pool.back();
+        e.pool.pop_back();
+        return ev;
+    }
+    cudaEvent_t ev = nullptr;
+    cudaEventCreate(&ev);
+    return ev;
+}
+
+static void eprof_resolve(Engine &e) {
+    if (e.pending.empty()) return;
+    cudaStreamSynchronize(e.stream);
+    for (auto &p : e.pending) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, p.a, p.b) == cudaSuccess && p.slot >= 0) {
+            e.slots[p.slot].ms += ms;
+            e.slots[p.slot].launches += 1;
+        }
+        e.pool.push_back(p.a);
+        e.pool.push_back(p.b);
+    }
+    e.pending.clear();
+}
+
+template <typename F>
+static int etimed(Engine &e, const char *name, F &&launch) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaStreamIsCapturing(e.stream, &cs);
+    if (!e.prof || cs != cudaStreamCaptureStatusNone) return launch();
+    int slot = -1;
+    for (size_t i = 0; i < e.slots.size(); ++i)
+        if (std::strcmp(e.slots[i].name, name) == 0) slot = (int)i;
+    if (slot < 0 && e.slots.size() < TBS_PROFILE_MAX) {
+        e.slots.push_back({name, 0, 0.0});
+        slot = (int)e.slots.size() - 1;
+    }
+    if (e.pending.size() > 4000) eprof_resolve(e);
+    PendingEvent pe{slot, eprof_event(e), eprof_event(e)};
+    cudaEventRecord(pe.a, e.stream);
+    int rc = launch();
+    cudaEventRecord(pe.b, e.stream);
+    e.pending.push_back(pe);
+    return rc;
+}
+
+#define ERUN(name, call) ECKL(etimed(e, name, [&]() { return (int)(call); }))
+
+VecSet ctx_vectors(tbs_ctx *c) {
+    VecSet v;
+    v.Up = c->d_Up;
+    v.dUp = c->d_dUp;
+    v.b = c->d_b;
+    v.y = c->d_y;
+    v.rhsp = c->d_rhsp;
+    v.rhs = c->d_rhs;
+    v.Rp = c->d_Rp;
+    v.partials = c->d_partials;
+    v.partials2 = c->d_partials2;
+    v.Uinit = c->d_Uinit;
+    v.state = c->d_state;
+    v.hist = c->d_hist;
+    v.b32 = c->d_b32;
+    v.y32 = c->d_y32;
+    v.d32 = c->d_d32;
+    v.c32 = c->d_c32;
+    v.R32 = c->d_R32;
+    return v;
+}
+
+/* ================================================================ engine */
+
+int engine_init(Engine &e, int device, cudaStream_t stream, int algo) {
+    e.device = device;
+    e.stream = stream;
+    e.algo = algo;
+    int rc = ealloc(e, &e.d_queue, 2);
+    if (!rc) rc = ealloc(e, &e.d_counter, 1);
+    if (!rc) rc = ealloc(e, &e.d_status, 1);
+    if (!rc) rc = ealloc(e, &e.d_ctl, 1);
+    if (rc) return rc;
+    if (cudaMallocHost(&e.h_ctl, sizeof(BatchCtl)) != cudaSuccess ||
+        cudaMallocHost(&e.h_status, sizeof(unsigned)) != cudaSuccess)
+        return efail(e, TBS_ERR_NOMEM, "pinned allocation failed");
+    std::memset(e.h_ctl, 0, sizeof(BatchCtl));
+    ECK(cudaMemsetAsync(e.d_queue, 0, 2 * sizeof(unsigned), e.stream));
+    ECK(cudaMemsetAsync(e.d_counter, 0, sizeof(unsigned), e.stream));
+    ECK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
+    ECK(cudaMemsetAsync(e.d_ctl, 0, sizeof(BatchCtl), e.stream));
+    /* default schedule: 2 stages, as many CTAs per SM as fit, at most 8 */
+    const int fit = algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(2) : thomas_batch_fit<float>(2);
+    if (fit < 1) return efail(e, TBS_ERR_CUDA, "the batched Thomas kernel does not fit on an SM");
+    e.sched = BatchSched{std::min(fit, 8), 2};
+    ECK(cudaStreamSynchronize(e.stream));
+    return TBS_OK;
+}
+
+void engine_drop_graph(Engine &e) {
+    if (e.gexec) cudaGraphExecDestroy(e.gexec);
+    if (e.graph) cudaGraphDestroy(e.graph);
+    e.gexec = nullptr;
+    e.graph = nullptr;
+    e.graph_ok = false;
+}
+
+void engine_free(Engine &e) {
+    if (e.stream) cudaStreamSynchronize(e.stream);
+    eprof_resolve(e);
+    engine_drop_graph(e);
+    for (void *p : e.allocs) cudaFree(p);
+    e.allocs.clear();
+    for (cudaEvent_t ev : e.pool) cudaEventDestroy(ev);
+    e.pool.clear();
+    if (e.h_ctl) cudaFreeHost(e.h_ctl);
+    if (e.h_status) cudaFreeHost(e.h_status);
+    e.h_ctl = nullptr;
+    e.h_status = nullptr;
+}
+
+/* grow the capacity-sized arrays (never shrinks); growth invalidates the graph */
+static int ensure_capacity(Engine &e, int nmem, int nlines, int ntiles, int nblocks) {
+    auto grow = [](int need, int have) { return need <= have ? have : std::max(need, have + have / 2); };
+    int rc = TBS_OK;
+    if (nmem > e.cap_mem) {
+        const int c = grow(nmem, e.cap_mem);
+        efree(e, &e.d_th64);
+        efree(e, &e.d_th32);
+        efree(e, &e.d_rs_prime);
+        efree(e, &e.d_rs_body);
+        efree(e, &e.d_rs32_rhs);
+        efree(e, &e.d_rs32_dx);
+        efree(e, &e.d_fr);
+        efree(e, &e.d_vec);
+        efree(e, &e.d_red_prime);
+        efree(e, &e.d_red_body);
+        efree(e, &e.d_active);
+        if (e.algo == TBS_ALGO_FP64) {
+            if (!rc) rc = ealloc(e, &e.d_th64, c);
+            if (!rc) rc = ealloc(e, &e.d_rs_prime, c);
+            if (!rc) rc = ealloc(e, &e.d_rs_body, c);
+        } else {
+            if (!rc) rc = ealloc(e, &e.d_th32, c);
+            if (!rc) rc = ealloc(e, &e.d_rs32_rhs, c);
+            if (!rc) rc = ealloc(e, &e.d_rs32_dx, c);
+            if (!rc) rc = ealloc(e, &e.d_fr, c);
+            if (!rc) rc = ealloc(e, &e.d_vec, c);
+        }
+        if (!rc) rc = ealloc(e, &e.d_red_prime, c);
+        if (!rc) rc = ealloc(e, &e.d_red_body, c);
+        if (!rc) rc = ealloc(e, &e.d_active, c);
+        e.cap_mem = rc ? 0 : c;
+        engine_drop_graph(e);
+    }
+    if (!rc && nlines > e.cap_lines) {
+        const int c = grow(nlines, e.cap_lines);
+        efree(e, &e.d_lines);
+        rc = ealloc(e, &e.d_lines, c);
+        e.cap_lines = rc ? 0 : c;
+        engine_drop_graph(e);
+    }
+    if (!rc && ntiles > e.cap_tiles) {
+        const int c = grow(ntiles, e.cap_tiles);
+        efree(e, &e.d_tiles);
+        efree(e, &e.d_prime_tiles);
+        rc = ealloc(e, &e.d_tiles, c);
+        if (!rc) rc = ealloc(e, &e.d_prime_tiles, c);
+        e.cap_tiles = rc ? 0 : c;
+        engine_drop_graph(e);
+    }
+    if (!rc && nblocks > e.cap_blocks) {
+        const int c = grow(nblocks, e.cap_blocks);
+        efree(e, &e.d_blocks);
+        rc = ealloc(e, &e.d_blocks, c);
+        e.cap_blocks = rc ? 0 : c;
+        engine_drop_graph(e);
+    }
+    return rc;
+}
+
+/* Thomas items in the engine's order.  Longest lines first; items of the
+ * same line of the same system (several right-hand sides) are adjacent, so
+ * that warps running them together share the line's blocks in L2. */
+static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Member> &m) {
+    std::vector<WorkItem> items;
+    std::vector<int> sys_rank(m.size());
+    for (size_t k = 0; k < m.size(); ++k) {
+        sys_rank[k] = (int)k;
+        for (size_t j = 0; j < k; ++j)
+            if (m[j].sys == m[k].sys) {
+                sys_rank[k] = sys_rank[j];
+                break;
+            }
+    }
+    for (size_t k = 0; k < m.size(); ++k)
+        for (int l = 0; l < m[k].sys->nline; ++l) items.push_back({(int)k, l});
+    if (e.order == 0) {
+        std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
+            const int la = m[a.sys].sys->h_linesize[a.unit], lb = m[b.sys].sys->h_linesize[b.unit];
+            if (la != lb) return la > lb;
+            if (sys_rank[a.sys] != sys_rank[b.sys]) return sys_rank[a.sys] < sys_rank[b.sys];
+            if (a.unit != b.unit) return a.unit < b.unit;
+            return a.sys < b.sys;
+        });
+    }
+    return items;
+}
+
+int engine_set_members(Engine &e, const std::vector<Member> &members) {
+    const int n = (int)members.size();
+    const bool mixed = e.algo == TBS_ALGO_MIXED;
+    int nx = e.max_nx;
+    long long nlines = 0, ntiles = 0, nblocks = 0;
+    for (const Member &m : members) {
+        nx = std::max(nx, m.sys->L.nx);
+        nlines += m.sys->nline;
+        ntiles += fast_resid_grid(m.sys->L.np16);
+        if (mixed) nblocks += full_resid_blocks(m.sys->nelem);
+    }
+    if (nlines > 0x7fffffff || ntiles > 0x7fffffff || nblocks > 0x7fffffff)
+        return efail(e, TBS_ERR_UNSUPPORTED, "batch too large for int32 work lists");
+    if (nx > e.max_nx) {
+        if (batch_prepare(nx)) return efail(e, TBS_ERR_CUDA, "shared-memory opt-in failed");
+        e.max_nx = nx;
+        engine_drop_graph(e);
+    }
+    int rc = ensure_capacity(e, std::max(n, 1), (int)std::max(nlines, 1LL), (int)std::max(ntiles, 1LL),
+                             (int)std::max(nblocks, 1LL));
+    if (rc) return rc;
+
+    std::vector<ThomasSys<double>> th64;
+    std::vector<ThomasSys<float>> th32;
+    std::vector<ResidSys<double>> rsp, rsb;
+    std::vector<ResidSys<float>> rs32r, rs32d;
+    std::vector<FullResSys> fr;
+    std::vector<VecSys> vec;
+    std::vector<ReduceSys> redp, redb;
+    std::vector<WorkItem> tiles, prime_tiles, blocks;
+    std::vector<int> uinit;
+    e.h_active.assign(n, 0);
+    for (int k = 0; k < n; ++k) {
+        const Member &m = members[k];
+        tbs_ctx *c = m.sys;
+        const VecSet &v = m.v;
+        const FastLayout &L = c->L;
+        const int nt = fast_resid_grid(L.np16);
+        const bool ui = m.fresh && v.Uinit;
+        if (!mixed) {
+            th64.push_back({L.line_start, L.line_len, L.line_twist, c->d_G, c->d_Gam, v.b, v.y, v.dUp});
+            /* prime: R = rhs (U = 0, cleared by the same launch) or the residual of U_init */
+            rsp.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv, c->d_X, v.dUp, ui ? v.Rp : v.rhsp, v.b,
+                           ui ? nullptr : v.Up, v.partials});
+            rsb.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv, c->d_X, v.dUp, nullptr, v.b, v.Up,
+                           v.partials});
+            if (m.fresh) redp.push_back({v.partials, nt, k, v.state, v.hist});
+            redb.push_back({v.partials, nt, k, v.state, v.hist});
+        } else {
+            th32.push_back({L.line_start, L.line_len, L.line_twist, c->d_G32, c->d_Gam32, v.b32, v.y32,
+                            v.d32});
+            rs32r.push_back({L.np16, L.nx, L.xnbr, c->d_Dinv32, c->d_X32, v.d32, v.R32, v.b32, v.c32,
+                             nullptr});
+            rs32d.push_back({L.np16, L.nx, L.xnbr, nullptr, c->d_X32, v.d32, nullptr, v.b32, v.c32,
+                             nullptr});
+            fr.push_back({c->nelem, 0, c->d_epoint, c->d_ef, c->d_fc, L.pos_of_elem, c->d_jacD, c->d_O1,
+                          c->d_O2, v.rhs, v.Up, v.R32, v.partials});
+            vec.push_back({v.rhsp, v.R32, v.c32, v.d32, v.Up, v.partials});
+            if (m.fresh) redp.push_back({v.partials, ui ? full_resid_blocks(c->nelem) : nt, k, v.state, v.hist});
+            redb.push_back({v.partials, full_resid_blocks(c->nelem), k, v.state, v.hist});
+            for (int b = 0; b < full_resid_blocks(c->nelem); ++b) blocks.push_back({k, b});
+        }
+        for (int t = 0; t < nt; ++t) tiles.push_back({k, t});
+        if (m.fresh && !(mixed && ui))
+            for (int t = 0; t < nt; ++t) prime_tiles.push_back({k, t});
+        if (ui) uinit.push_back(k);
+        e.h_active[k] = m.fresh ? 0 : 1;
+    }
+    if (uinit != e.uinit) {
+        e.uinit = uinit;
+        engine_drop_graph(e);
+    }
+    /* residual tiles and element blocks of right-hand sides of the same
+     * system next to each other (system, unit, member), so that CTAs that
+     * run them together share the blocks in L2 */
+    std::vector<int> sys_rank(n);
+    for (int k = 0; k < n; ++k) {
+        sys_rank[k] = k;
+        for (int j = 0; j < k; ++j)
+            if (members[j].sys == members[k].sys) {
+                sys_rank[k] = sys_rank[j];
+                break;
+            }
+    }
+    auto by_unit = [&](const WorkItem &a, const WorkItem &b) {
+        if (sys_rank[a.sys] != sys_rank[b.sys]) return sys_rank[a.sys] < sys_rank[b.sys];
+        if (a.unit != b.unit) return a.unit < b.unit;
+        return a.sys < b.sys;
+    };
+    std::stable_sort(tiles.begin(), tiles.end(), by_unit);
+    std::stable_sort(prime_tiles.begin(), prime_tiles.end(), by_unit);
+    std::stable_sort(blocks.begin(), blocks.end(), by_unit);
+    e.members = members;
+    std::vector<WorkItem> lines = line_items(e, members);
+    if (!mixed) {
+        if (!rc) rc = eupload(e, e.d_th64, th64);
+        if (!rc) rc = eupload(e, e.d_rs_prime, rsp);
+        if (!rc) rc = eupload(e, e.d_rs_body, rsb);
+    } else {
+        if (!rc) rc = eupload(e, e.d_th32, th32);
+        if (!rc) rc = eupload(e, e.d_rs32_rhs, rs32r);
+        if (!rc) rc = eupload(e, e.d_rs32_dx, rs32d);
+        if (!rc) rc = eupload(e, e.d_fr, fr);
+        if (!rc) rc = eupload(e, e.d_vec, vec);
+        if (!rc) rc = eupload(e, e.d_blocks, blocks);
+    }
+    if (!rc) rc = eupload(e, e.d_red_prime, redp);
+    if (!rc) rc = eupload(e, e.d_red_body, redb);
+    if (!rc) rc = eupload(e, e.d_lines, lines);
+    if (!rc) rc = eupload(e, e.d_tiles, tiles);
+    if (!rc) rc = eupload(e, e.d_prime_tiles, prime_tiles);
+    if (!rc) rc = eupload(e, e.d_active, e.h_active);
+    if (rc) return rc;
+    BatchCtl &C = *e.h_ctl;
+    C.nsys = n;
+    C.nlines = (int)lines.size();
+    C.ntiles = (int)tiles.size();
+    C.nblocks = (int)blocks.size();
+    C.nprime_sys = (int)redp.size();
+    C.nprime_tiles = (int)prime_tiles.size();
+    ECK(cudaStreamSynchronize(e.stream));
+    return TBS_OK;
+}
+
+int engine_restart(Engine &e) {
+    bool all_fresh = true;
+    for (const Member &m : e.members) all_fresh = all_fresh && m.fresh;
+    if (!all_fresh) {
+        std::vector<Member> m = e.members;
+        for (Member &x : m) x.fresh = true;
+        return engine_set_members(e, m);
+    }
+    std::fill(e.h_active.begin(), e.h_active.end(), 0);
+    int rc = eupload(e, e.d_active, e.h_active);
+    if (rc) return rc;
+    ECK(cudaStreamSynchronize(e.stream));
+    return TBS_OK;
+}
+
+void engine_mark_started(Engine &e) {
+    for (Member &m : e.members) m.fresh = false;
+    e.h_ctl->nprime_sys = 0;
+    e.h_ctl->nprime_tiles = 0;
+}
+
+struct Cond {
+    unsigned long long handle;
+    int use;
+};
+
+static int engine_prime(Engine &e, Cond cc) {
+    cudaStream_t st = e.stream;
+    for (int k : e.uinit) {
+        const Member &m = e.members[k];
+        tbs_ctx *c = m.sys;
+        const VecSet &v = m.v;
+        const FastLayout &L = c->L;
+        ERUN("permute", launch_permute_to_pos(st, 9, c->nelem, L.pos_of_elem, v.Uinit, v.Up));
+        if (e.algo == TBS_ALGO_FP64)
+            ERUN("full_resid", launch_full_resid<double>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
+                                                         L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
+                                                         v.rhs, v.Up, v.Rp, v.partials2));
+        else
+            ERUN("full_resid", launch_full_resid<float>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
+                                                        L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
+                                                        v.rhs, v.Up, v.R32, v.partials));
+    }
+    BatchCtl *C = e.d_ctl;
+    if (e.algo == TBS_ALGO_FP64) {
+        ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_prime_tiles,
+                                                          &C->nprime_tiles, nullptr, e.d_status));
+        ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
+                                                e.d_active, C, e.d_counter, cc.handle, cc.use));
+    } else {
+        ERUN("mixed_prime", launch_mixed_prime_batch(st, e.d_vec, e.d_prime_tiles, &C->nprime_tiles));
+        ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
+                                                e.d_active, C, e.d_counter, cc.handle, cc.use));
+    }
+    return TBS_OK;
+}
+
+static int engine_body(Engine &e, Cond cc) {
+    cudaStream_t st = e.stream;
+    BatchCtl *C = e.d_ctl;
+    if (e.algo == TBS_ALGO_FP64) {
+        ERUN("fast_thomas", launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines, &C->nlines,
+                                                        e.d_active, e.d_queue, e.d_status));
+        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_tiles,
+                                                      &C->ntiles, e.d_active, e.d_status));
+        ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_body, &C->nsys, e.cap_mem, 0,
+                                                e.d_active, C, e.d_counter, cc.handle, cc.use));
+        return TBS_OK;
+    }
+    /* c (the sum of the inner updates but the last) is cleared by the first
+     * launch, each inner residual adds its sweep's d to it, and the last d
+     * goes to U with c (the order of the single-system sequence) */
+    ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_tiles,
+                                                       &C->ntiles, e.d_active, e.d_status));
+    for (int m = 0; m < e.inner; ++m) {
+        ERUN("fast_thomas32", launch_thomas_batch<float>(st, e.sched, e.d_th32, e.d_lines, &C->nlines,
+                                                         e.d_active, e.d_queue, e.d_status));
+        if (m + 1 < e.inner)
+            ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_tiles,
+                                                           &C->ntiles, e.d_active, e.d_status));
+    }
+    ERUN("axpy", launch_axpy2_batch(st, e.d_vec, e.d_tiles, &C->ntiles, e.d_active));
+    ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_blocks, &C->nblocks, e.d_active));
+    ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_body, &C->nsys, e.cap_mem, 0, e.d_active,
+                                            C, e.d_counter, cc.handle, cc.use));
+    return TBS_OK;
+}
+
+static int engine_build_graph(Engine &e) {
+    engine_drop_graph(e);
+    cudaStream_t st = e.stream;
+    cudaGraph_t g = nullptr;
+    ECK(cudaGraphCreate(&g, 0));
+    e.graph = g;
+    cudaGraphConditionalHandle h;
+    ECK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
+    const Cond cc{(unsigned long long)h, 1};
+    ECK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = engine_prime(e, cc);
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    if (rc == TBS_OK) {
+        cudaError_t x = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(x));
+    }
+    cudaGraphNode_t cnode = nullptr;
+    cudaGraph_t bodyg = nullptr;
+    if (rc == TBS_OK) {
+        cudaGraphNodeParams cp{};
+        cp.type = cudaGraphNodeTypeConditional;
+        cp.conditional.handle = h;
+        cp.conditional.type = cudaGraphCondTypeWhile;
+        cp.conditional.size = 1;
+        cudaError_t x = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
+        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(x));
+        else bodyg = cp.conditional.phGraph_out[0];
+    }
+    if (rc == TBS_OK) {
+        cudaError_t x = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
+        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(x));
+    }
+    cudaGraph_t outg = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(st, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
+    if (rc != TBS_OK) {
+        engine_drop_graph(e);
+        return rc;
+    }
+    ECK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    rc = engine_body(e, cc);
+    ee = cudaStreamEndCapture(st, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    if (rc != TBS_OK) {
+        engine_drop_graph(e);
+        return rc;
+    }
+    cudaError_t ie = cudaGraphInstantiate(&e.gexec, g, 0);
+    if (ie != cudaSuccess) {
+        engine_drop_graph(e);
+        return efail(e, TBS_ERR_CUDA, std::string("graph instantiate: ") + cudaGetErrorString(ie));
+    }
+    e.graph_ok = true;
+    return TBS_OK;
+}
+
+static int engine_status(Engine &e) {
+    ECK(cudaMemcpyAsync(e.h_status, e.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, e.stream));
+    ECK(cudaStreamSynchronize(e.stream));
+    const unsigned s = *e.h_status;
+    if (s) {
+        ECK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
+        ECK(cudaMemsetAsync(e.d_queue, 0, 2 * sizeof(unsigned), e.stream));
+        ECK(cudaMemsetAsync(e.d_counter, 0, sizeof(unsigned), e.stream));
+        ECK(cudaStreamSynchronize(e.stream));
+        if (s & ST_TIMEOUT) return efail(e, TBS_ERR_CUDA, "a device-side wait ran out of its time budget");
+        return efail(e, TBS_ERR_CUDA, "device status " + std::to_string(s));
+    }
+    return TBS_OK;
+}
+
+int engine_read_active(Engine &e) {
+    const int n = e.h_ctl->nsys;
+    e.h_active.resize(n);
+    if (n > 0)
+        ECK(cudaMemcpyAsync(e.h_active.data(), e.d_active, n * sizeof(int), cudaMemcpyDeviceToHost,
+                            e.stream));
+    ECK(cudaStreamSynchronize(e.stream));
+    return TBS_OK;
+}
+
+int engine_run(Engine &e, int chunk_limit, int stop_on_finish) {
+    BatchCtl &C = *e.h_ctl;
+    C.chunk = 0;
+    C.finished = 0;
+    C.chunk_limit = chunk_limit;
+    C.stop_on_finish = stop_on_finish;
+    ECK(cudaMemcpyAsync(e.d_ctl, e.h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, e.stream));
+    if (e.prof) {
+        /* eager form with the graph's loop rule tested on the host, so
+         * that every kernel is timed */
+        int rc = engine_prime(e, Cond{0, 0});
+        if (rc) return rc;
+        BatchCtl now{};
+        for (;;) {
+            ECK(cudaMemcpyAsync(&now, e.d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, e.stream));
+            rc = engine_read_active(e);
+            if (rc) return rc;
+            bool any = false;
+            for (int v : e.h_active) any = any || v;
+            bool go = any;
+            if (chunk_limit > 0 && now.chunk >= chunk_limit) go = false;
+            if (stop_on_finish && now.finished) go = false;
+            if (!go) break;
+            rc = engine_body(e, Cond{0, 0});
+            if (rc) return rc;
+        }
+        eprof_resolve(e);
+    } else {
+        if (!e.graph_ok) {
+            int rc = engine_build_graph(e);
+            if (rc) return rc;
+        }
+        ECK(cudaGraphLaunch(e.gexec, e.stream));
+    }
+    return engine_status(e);
+}
+
+static int engine_upload_lines(Engine &e) {
+    std::vector<WorkItem> lines = line_items(e, e.members);
+    int rc = eupload(e, e.d_lines, lines);
+    if (rc) return rc;
+    ECK(cudaStreamSynchronize(e.stream));
+    return TBS_OK;
+}
+
+int engine_set_schedule(Engine &e, BatchSched s, int order) {
+    const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(s.stages)
+                                            : thomas_batch_fit<float>(s.stages);
+    if (s.stages < 2 || s.stages > 8 || s.ctas_per_sm < 1 || s.ctas_per_sm > fit)
+        return efail(e, TBS_ERR_ARG, "schedule does not fit: at most " + std::to_string(fit) +
+                                         " CTAs per SM with " + std::to_string(s.stages) + " stages");
+    const bool new_order = order != e.order;
+    e.sched = s;
+    e.order = order;
+    engine_drop_graph(e);
+    if (new_order && !e.members.empty()) return engine_upload_lines(e);
+    return TBS_OK;
+}
+
+int engine_tune(Engine &e, BatchSched *best_s, int *best_o, double *best_ms) {
+    cudaStream_t st = e.stream;
+    const int n = e.h_ctl->nsys;
+    if (n < 1) return efail(e, TBS_ERR_STATE, "no members to tune on");
+    std::vector<int> ones(n, 1);
+    int rc = eupload(e, e.d_active, ones);
+    if (rc) return rc;
+    ECK(cudaMemcpyAsync(e.d_ctl, e.h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, st));
+    cudaEvent_t e0, e1;
+    ECK(cudaEventCreate(&e0));
+    ECK(cudaEventCreate(&e1));
+    const BatchSched keep = e.sched;
+    const int keep_order = e.order;
+    double best = 1e30;
+    BatchSched bs = keep;
+    int bo = keep_order;
+    const int cand_ctas[] = {2, 3, 4, 6, 8, 12, 16};
+    for (int o = 0; o < 2 && !rc; ++o) {
+        e.order = o;
+        rc = engine_upload_lines(e);
+        for (int ns = 2; ns <= 4 && !rc; ++ns) {
+            const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(ns)
+                                                    : thomas_batch_fit<float>(ns);
+            for (int cps : cand_ctas) {
+                if (cps > fit || rc) continue;
+                e.sched = BatchSched{cps, ns};
+                auto launch = [&]() {
+                    return e.algo == TBS_ALGO_FP64
+                               ? launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines,
+                                                             &e.d_ctl->nlines, e.d_active, e.d_queue,
+                                                             e.d_status)
+                               : launch_thomas_batch<float>(st, e.sched, e.d_th32, e.d_lines,
+                                                            &e.d_ctl->nlines, e.d_active, e.d_queue,
+                                                            e.d_status);
+                };
+                int x = launch();
+                const int reps = 3;
+                if (!x) cudaEventRecord(e0, st);
+                for (int r = 0; r < reps && !x; ++r) x = launch();
+                if (!x) cudaEventRecord(e1, st);
+                if (x) {
+                    rc = efail(e, TBS_ERR_CUDA,
+                               std::string("tuning launch: ") + cudaGetErrorString((cudaError_t)x));
+                    break;
+                }
+                cudaEventSynchronize(e1);
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                rc = engine_status(e);
+                if (rc) break;
+                if (ms / reps < best) {
+                    best = ms / reps;
+                    bs = e.sched;
+                    bo = o;
+                }
+            }
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    e.sched = rc ? keep : bs;
+    e.order = rc ? keep_order : bo;
+    engine_drop_graph(e);
+    int rc2 = engine_upload_lines(e);
+    if (rc) return rc;
+    if (rc2) return rc2;
+    if (best_s) *best_s = bs;
+    if (best_o) *best_o = bo;
+    if (best_ms) *best_ms = best;
+    return TBS_OK;
+}
+
+}  // namespace tbs
+
+/* ============================================================= tbs_batch */
+
+struct tbs_batch {
+    Engine eng;
+    cudaStream_t own = nullptr;
+    std::vector<tbs_ctx *> sys;
+    std::vector<const void *> fingerprint;
+};
+
+static int bfail(tbs_batch *b, int code, const std::string &msg) {
+    if (b) b->eng.err = msg;
+    set_thread_error(msg);
+    return code;
+}
+
+/* every device pointer and setting the members' descriptors depend on */
+static std::vector<const void *> batch_fingerprint(tbs_batch *b) {
+    std::vector<const void *> f;
+    for (tbs_ctx *c : b->sys) {
+        const void *p[] = {c->d_G, c->d_Gam, c->d_Dinv, c->d_X, c->d_b, c->d_y, c->d_dUp, c->d_Up,
+                           c->d_rhsp, c->d_Rp, c->d_partials, c->d_partials2, c->d_state, c->d_hist,
+                           c->d_Uinit, c->d_G32, c->d_Gam32, c->d_Dinv32, c->d_X32, c->d_b32,
+                           c->d_y32, c->d_d32, c->d_c32, c->d_R32, c->L.line_start, c->L.xnbr,
+                           c->d_jacD, c->d_O1, c->d_O2, c->d_rhs, c->d_epoint};
+        f.insert(f.end(), std::begin(p), std::end(p));
+        f.push_back(reinterpret_cast<const void *>((uintptr_t)c->algo));
+    }
+    return f;
+}
+
+static int batch_check_members(tbs_batch *b) {
+    for (size_t s = 0; s < b->sys.size(); ++s) {
+        tbs_ctx *c = b->sys[s];
+        if (!c->factored || !c->layout_ok)
+            return bfail(b, TBS_ERR_STATE, "batch member " + std::to_string(s) + " is not factored");
+        if (c->algo != b->eng.algo)
+            return bfail(b, TBS_ERR_STATE,
+                         "batch member " + std::to_string(s) + " was re-factored with another algorithm");
+    }
+    return TBS_OK;
+}
+
+/* members' device state (tolerance, sweep limit, history capacity) and the
+ * engine's descriptors, rebuilt when a member's arrays changed */
+static int batch_ready(tbs_batch *b, double tol, int max_sweeps) {
+    int rc = batch_check_members(b);
+    if (rc) return rc;
+    for (tbs_ctx *c : b->sys) {
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return bfail(b, TBS_ERR_CUDA, "member stream synchronisation failed");
+        rc = ctx_ensure_hist(c, max_sweeps + 1);
+        if (!rc) rc = ctx_set_state(c, tol, max_sweeps);
+        if (rc) return bfail(b, rc, "batch member: " + c->err);
+        if (cudaStreamSynchronize(c->stream) != cudaSuccess)
+            return bfail(b, TBS_ERR_CUDA, "member stream synchronisation failed");
+    }
+    std::vector<const void *> fp = batch_fingerprint(b);
+    if (fp != b->fingerprint) {
+        std::vector<Member> m;
+        for (tbs_ctx *c : b->sys) m.push_back({c, ctx_vectors(c), true});
+        rc = engine_set_members(b->eng, m);
+        if (rc) return rc;
+        b->fingerprint = fp;
+        return TBS_OK;
+    }
+    return engine_restart(b->eng);
+}
+
+static int batch_destroy_all(tbs_batch *b) {
+    if (!b) return TBS_OK;
+    cudaSetDevice(b->eng.device);
+    engine_free(b->eng);
+    if (b->own) cudaStreamDestroy(b->own);
+    delete b;
+    return TBS_OK;
+}
+
+#define BGUARD_BEGIN try {
+#define BGUARD_END                                                                        \
+    }                                                                                     \
+    catch (const std::bad_alloc &) {                                                      \
+        return bfail(b, TBS_ERR_NOMEM, "host allocation failed");                         \
+    }                                                                                     \
+    catch (...) {                                                                         \
+        return bfail(b, TBS_ERR_STATE, "internal error");                                 \
+    }
+
+extern "C" {
+
+const char *tbs_batch_last_error(const tbs_batch *b) {
+    if (!b) return thread_error();
+    return b->eng.err.c_str();
+}
+
+int tbs_batch_create(tbs_ctx *const *systems, int nsys, tbs_batch **out) {
+    if (!out || !systems || nsys < 1) return bfail(nullptr, TBS_ERR_ARG, "tbs_batch_create: bad arguments");
+    *out = nullptr;
+    tbs_batch *b = nullptr;
+    try {
+        b = new tbs_batch();
+    } catch (...) {
+        return bfail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
+    }
+    auto fail = [&](int rc) {
+        std::string msg = b->eng.err;
+        batch_destroy_all(b);
+        set_thread_error(msg);
+        return rc;
+    };
+    try {
+        for (int s = 0; s < nsys; ++s) {
+            tbs_ctx *c = systems[s];
+            if (!c) return fail(bfail(b, TBS_ERR_ARG, "null system " + std::to_string(s)));
+            for (int t = 0; t < s; ++t)
+                if (systems[t] == c)
+                    return fail(bfail(b, TBS_ERR_ARG, "system " + std::to_string(s) + " appears twice"));
+            if (!c->factored)
+                return fail(bfail(b, TBS_ERR_STATE, "system " + std::to_string(s) + " is not factored"));
+            if (c->algo != TBS_ALGO_FP64 && c->algo != TBS_ALGO_MIXED)
+                return fail(bfail(b, TBS_ERR_UNSUPPORTED,
+                                  "batches take TBS_ALGO_FP64 or TBS_ALGO_MIXED systems"));
+            if (s > 0 && (c->algo != systems[0]->algo || c->device != systems[0]->device))
+                return fail(bfail(b, TBS_ERR_ARG,
+                                  "all systems of a batch need the same algorithm and GPU"));
+            b->sys.push_back(c);
+        }
+        const int dev = systems[0]->device;
+        if (cudaSetDevice(dev) != cudaSuccess) return fail(bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed"));
+        if (cudaStreamCreateWithFlags(&b->own, cudaStreamNonBlocking) != cudaSuccess)
+            return fail(bfail(b, TBS_ERR_CUDA, "cudaStreamCreate failed"));
+        int rc = engine_init(b->eng, dev, b->own, systems[0]->algo);
+        if (rc) return fail(rc);
+        b->eng.inner = systems[0]->inner_sweeps;
+    } catch (...) {
+        return fail(bfail(b, TBS_ERR_NOMEM, "host allocation failed"));
+    }
+    *out = b;
+    return TBS_OK;
+}
+
+int tbs_batch_destroy(tbs_batch *b) { return batch_destroy_all(b); }
+
+int tbs_batch_set_stream(tbs_batch *b, void *cuda_stream) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    cudaStream_t ns = cuda_stream ? static_cast<cudaStream_t>(cuda_stream) : b->own;
+    if (ns != b->eng.stream) {
+        cudaStreamSynchronize(b->eng.stream);
+        engine_drop_graph(b->eng);
+        b->eng.stream = ns;
+    }
+    return TBS_OK;
+}
+
+int tbs_batch_size(const tbs_batch *b, int *nsys) {
+    if (!b || !nsys) return bfail(nullptr, TBS_ERR_ARG, "null argument");
+    *nsys = (int)b->sys.size();
+    return TBS_OK;
+}
+
+int tbs_batch_set_inner_sweeps(tbs_batch *b, int m) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (m < 1 || m > 64) return bfail(b, TBS_ERR_ARG, "inner sweeps must be in 1..64");
+    if (m != b->eng.inner) engine_drop_graph(b->eng);
+    b->eng.inner = m;
+    return TBS_OK;
+}
+
+int tbs_batch_set_schedule(tbs_batch *b, int ctas_per_sm, int stages, int order) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (order != 0 && order != 1) return bfail(b, TBS_ERR_ARG, "bad line order");
+    BGUARD_BEGIN
+    if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
+    return engine_set_schedule(b->eng, BatchSched{ctas_per_sm, stages}, order);
+    BGUARD_END
+}
+
+int tbs_batch_get_schedule(const tbs_batch *b, int *ctas_per_sm, int *stages, int *order) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (ctas_per_sm) *ctas_per_sm = b->eng.sched.ctas_per_sm;
+    if (stages) *stages = b->eng.sched.stages;
+    if (order) *order = b->eng.order;
+    return TBS_OK;
+}
+
+int tbs_batch_solve(tbs_batch *b, double rel_tol, int max_sweeps, int *sweeps_out,
+                    double *hist_out) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (max_sweeps < 0 || !(rel_tol >= 0.0)) return bfail(b, TBS_ERR_ARG, "bad tolerance or sweep limit");
+    BGUARD_BEGIN
+    if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
+    int rc = batch_ready(b, rel_tol, max_sweeps);
+    if (rc) return rc;
+    rc = engine_run(b->eng, 0, 0);
+    if (rc) return rc;
+    cudaStream_t st = b->eng.stream;
+    const int n = (int)b->sys.size();
+    for (int s = 0; s < n; ++s) {
+        tbs_ctx *c = b->sys[s];
+        if (cudaMemcpyAsync(c->h_state, c->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, st) !=
+            cudaSuccess)
+            return bfail(b, TBS_ERR_CUDA, "state read-back failed");
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "synchronisation failed");
+    for (int s = 0; s < n; ++s) {
+        tbs_ctx *c = b->sys[s];
+        const int sw = c->h_state->sweep;
+        if (sweeps_out) sweeps_out[s] = sw;
+        if (hist_out &&
+            cudaMemcpyAsync(hist_out + (size_t)s * (max_sweeps + 1), c->d_hist,
+                            (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double),
+                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            return bfail(b, TBS_ERR_CUDA, "history read-back failed");
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "synchronisation failed");
+    return TBS_OK;
+    BGUARD_END
+}
+
+int tbs_batch_tune(tbs_batch *b, int *ctas_per_sm, int *stages, int *order, double *best_ms) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    BGUARD_BEGIN
+    if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
+    int rc = batch_ready(b, 0.0, 1);
+    if (rc) return rc;
+    BatchSched s{};
+    int o = 0;
+    double ms = 0.0;
+    rc = engine_tune(b->eng, &s, &o, &ms);
+    if (rc) return rc;
+    if (ctas_per_sm) *ctas_per_sm = s.ctas_per_sm;
+    if (stages) *stages = s.stages;
+    if (order) *order = o;
+    if (best_ms) *best_ms = ms;
+    return TBS_OK;
+    BGUARD_END
+}
+
+int tbs_batch_profile_enable(tbs_batch *b, int on) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (!on) eprof_resolve(b->eng);
+    b->eng.prof = on != 0;
+    return TBS_OK;
+}
+
+int tbs_batch_profile_reset(tbs_batch *b) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    eprof_resolve(b->eng);
+    b->eng.slots.clear();
+    return TBS_OK;
+}
+
+int tbs_batch_profile_read(tbs_batch *b, int *n, const char **names, long long *launches,
+                           double *ms) {
+    if (!b || !n) return bfail(b, TBS_ERR_ARG, "null argument");
+    eprof_resolve(b->eng);
+    const int cap = *n, cnt = (int)b->eng.slots.size();
+    for (int i = 0; i < cnt && i < cap; ++i) {
+        if (names) names[i] = b->eng.slots[i].name;
+        if (launches) launches[i] = b->eng.slots[i].launches;
+        if (ms) ms[i] = b->eng.slots[i].ms;
+    }
+    *n = cnt;
+    return TBS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,96 @@
+/*
+ * ctx.hxx -- the solver context (struct tbs_ctx) shared by the host
+ * translation units: api.cu (single systems), batch.cu (batched launch
+ * sequences over many systems) and server.cu (the request loop).
+ * Not installed; the public surface is include/triblock.h.
+ */
+#ifndef TBS_CTX_HXX
+#define TBS_CTX_HXX
+
+#include "tbs_internal.hxx"
+
+#include <cuda_runtime.h>
+
+#include <string>
+#include <utility>
+#include <vector>
+
+struct ProfSlot {
+    const char *name;
+    long long launches;
+    double ms;
+};
+
+struct PendingEvent {
+    int slot;
+    cudaEvent_t a, b;
+};
+
+struct tbs_ctx {
+    int device = 0;
+    cudaStream_t own = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string err;
+
+    /* ---- mesh ---- */
+    bool have_mesh = false, have_jac = false, factored = false;
+    int nvar = 0, nelem = 0, nintface = 0, eftot = 0, nline = 0, nlineelem = 0, max_line = 0;
+    std::vector<int> h_epoint, h_ef, h_fc, h_linesize, h_linepoint, h_lines, h_lineface;
+    int *d_epoint = nullptr, *d_ef = nullptr, *d_fc = nullptr, *d_linesize = nullptr;
+    int *d_linepoint = nullptr, *d_lines = nullptr, *d_lineface = nullptr, *d_identity = nullptr;
+
+    /* ---- Jacobian (element / face order, as read) ---- */
+    double *d_jacD = nullptr, *d_O1 = nullptr, *d_O2 = nullptr, *d_rhs = nullptr;
+    double *d_U = nullptr, *d_dU = nullptr, *d_R = nullptr, *d_Uinit = nullptr;
+    double *d_scratch = nullptr; /* 9*nelem element-order scratch */
+
+    /* ---- TBS_ALGO_REFERENCE ---- */
+    double *d_DLU = nullptr, *d_DinvC = nullptr, *d_A = nullptr;
+
+    /* ---- line-ordered layout (FP64 / MIXED) ---- */
+    tbs::FastLayout L{};
+    bool layout_ok = false;
+    double *d_gamlast = nullptr; /* per line and chain: last Gam toward the twist, FP64 */
+    long long n_xslots_real = 0;
+    double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
+    double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
+    double *d_rhsp = nullptr, *d_Rp = nullptr;
+    float *d_Dinv32 = nullptr, *d_G32 = nullptr, *d_Gam32 = nullptr, *d_X32 = nullptr;
+    float *d_b32 = nullptr, *d_y32 = nullptr, *d_d32 = nullptr, *d_c32 = nullptr,
+          *d_R32 = nullptr;
+    int inner_sweeps = 4;
+
+    /* ---- norms / solve state ---- */
+    double *d_partials = nullptr, *d_partials2 = nullptr;
+    int npart_cap = 0;
+    tbs::SolveState *d_state = nullptr;
+    tbs::SolveState *h_state = nullptr; /* pinned */
+    double *d_hist = nullptr;
+    int hist_cap = 0;
+    unsigned *d_status = nullptr;
+    unsigned *h_status = nullptr; /* pinned */
+    unsigned *d_counter = nullptr; /* last-CTA ticket of the fused norm */
+    int algo = -1;
+
+    /* ---- graph cache ---- */
+    cudaGraphExec_t gexec = nullptr;
+    cudaGraph_t graph = nullptr;
+    int graph_algo = -1;
+
+    /* ---- memory accounting ---- */
+    std::vector<std::pair<void *, size_t>> allocs;
+    size_t bytes = 0;
+
+    /* ---- profiling ---- */
+    bool prof = false;
+    std::vector<ProfSlot> slots;
+    std::vector<PendingEvent> pending;
+    std::vector<cudaEvent_t> pool;
+};
+
+/* device history of at least `need` norms (drops the cached graph when it grows) */
+int ctx_ensure_hist(tbs_ctx *ctx, int need);
+/* tolerance, sweep limit and history capacity of the device SolveState */
+int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps);
+
+#endif /* TBS_CTX_HXX */

@@ -51,6 +51,23 @@ int launch_zero(cudaStream_t st, double *p, long long n) {
     return (int)cudaGetLastError();
 }
 
+/* sum of p[t], p[t + stride], p[t + 2 stride], ... (t = threadIdx.x), added
+ * in that order; eight loads are issued ahead of their adds so that their
+ * latencies overlap without changing the sum */
+__device__ __forceinline__ double strided_sum(const double *p, int n, int stride) {
+    double acc = 0.0;
+    int t = threadIdx.x;
+    for (; t + 7 * stride < n; t += 8 * stride) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldcg(p + t + k * stride);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc += v[k];
+    }
+    for (; t < n; t += stride) acc += __ldcg(p + t);
+    return acc;
+}
+
 /* block b sums v[b*chunk : (b+1)*chunk)^2 in a fixed order */
 __global__ void norm_partials_kernel(const double *__restrict__ v, long long n, long long chunk,
                                      double *__restrict__ partials) {
@@ -86,8 +103,7 @@ __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, S
                                    double *hist, int is_start,
                                    cudaGraphConditionalHandle handle, int use_cond) {
     __shared__ double red[8];
-    double acc = 0.0;
-    for (int t = threadIdx.x; t < n; t += 256) acc += partials[t];
+    double acc = strided_sum(partials, n, 256);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
@@ -598,8 +614,7 @@ __device__ void finalize_norm(const NormSink &ns, double block_sum, int blk) {
         return;
     }
     __threadfence();
-    double acc = 0.0;
-    for (unsigned t = threadIdx.x; t < gridDim.x; t += blockDim.x) acc += __ldcg(ns.partials + t);
+    double acc = strided_sum(ns.partials, (int)gridDim.x, (int)blockDim.x);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
@@ -630,13 +645,30 @@ __host__ __device__ inline size_t resid_smem_bytes(int nx) {
            (size_t)nxa * RES_TILE * NV * sizeof(T) + (size_t)RES_TILE * NV * sizeof(T) * 2;
 }
 
-template <typename T>
-__device__ __forceinline__ void fast_resid_body(
-    int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
-    const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
-    T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status, int blk) {
+/* The residual kernels' staging barrier sits at the start of the dynamic
+ * shared memory; it is initialised once per CTA, and each tile the CTA
+ * processes completes one phase of it. */
+__device__ __forceinline__ uint64_t *resid_bar_init() {
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    if (threadIdx.x == 0) {
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    return bar;
+}
+
+/* One tile (positions blk*RES_TILE ..) with the staging barrier's phase of
+ * the given parity.  Returns false (status set, copies landed) when the
+ * wait for the tile's bulk copies ran out of time. */
+template <typename T>
+__device__ __forceinline__ bool fast_resid_body(
+    int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
+    const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
+    T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status, int blk,
+    uint64_t *bar, uint32_t parity) {
+    extern __shared__ __align__(128) unsigned char smem[];
     T *sD = reinterpret_cast<T *>(smem + 128);
     T *sX = sD + RES_TILE * NB;
     const int nxa = nx > 0 ? nx : 1;
@@ -649,11 +681,6 @@ __device__ __forceinline__ void fast_resid_body(
     const bool act = tid < RES_TILE * NV;
     const uint32_t szD = RES_TILE * NB * sizeof(T), szR = RES_TILE * NV * sizeof(T);
 
-    if (tid == 0) {
-        mbar_init(bar, 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
     if (tid == 0) {
         const uint64_t pol = policy_evict_first();
         const uint32_t bytes = (mode == 3 ? 0u : szD) + (mode >= 1 ? nx * szD : szR);
@@ -679,13 +706,13 @@ __device__ __forceinline__ void fast_resid_body(
             sg[(s * RES_TILE + c) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
         }
     }
-    const bool ok = mbar_wait(bar, 0);
+    const bool ok = mbar_wait(bar, parity);
     if (__syncthreads_or(!ok)) {
         if (tid == 0) {
             atomicOr(status, ST_TIMEOUT);
-            mbar_wait(bar, 0, 1LL << 28); /* let the copies land before the CTA retires */
+            mbar_wait(bar, parity, 1LL << 28); /* let the copies land before the CTA retires */
         }
-        return;
+        return false;
     }
     T r = T(0);
     if (mode >= 1) {
@@ -739,6 +766,7 @@ __device__ __forceinline__ void fast_resid_body(
             for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
         finalize_norm(ns, tot, blk);
     }
+    return true;
 }
 
 /* mode 1 (R = sum X dU over the cross-line slots) */
@@ -747,7 +775,9 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     int nx, int np16, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, T *__restrict__ b,
     T *__restrict__ Uacc, NormSink ns, unsigned *status) {
-    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status, blockIdx.x);
+    uint64_t *bar = resid_bar_init();
+    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status, blockIdx.x,
+                       bar, 0);
 }
 
 /* mode 3 (b = -sum (Dinv X) dU: premultiplied cross-line blocks, no norm) */
@@ -755,8 +785,9 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_dx_kernel(
     int nx, int np16, const T *__restrict__ DX, const int *__restrict__ xnbr,
     const T *__restrict__ dU, T *__restrict__ b, T *__restrict__ Uacc, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
     fast_resid_body<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status,
-                       blockIdx.x);
+                       blockIdx.x, bar, 0);
 }
 
 /* mode 0 (R given in position order) */
@@ -764,8 +795,9 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
     int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
     T *__restrict__ Uzero, NormSink ns, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
     fast_resid_body<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status,
-                       blockIdx.x);
+                       blockIdx.x, bar, 0);
 }
 
 template <typename T>
@@ -1257,10 +1289,12 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
  * next launch.  U is left to the residual kernel (accumulate = 2). */
 template <typename T, int P>
 __global__ void __launch_bounds__(32) fast_thomas_batch_kernel(
-    const ThomasSys<T> *__restrict__ sys, const WorkItem *__restrict__ work, int nwork,
-    const int *__restrict__ active, unsigned *queue, int NS, unsigned *status) {
+    const ThomasSys<T> *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ nwork_p, const int *__restrict__ active, unsigned *queue, int NS,
+    unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int lane = threadIdx.x & 31;
+    const int nwork = *nwork_p;
     thomas_init_bars(smem, NS);
     const uint64_t pol = lane == 0 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
@@ -1504,7 +1538,18 @@ int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp,
     return (int)cudaGetLastError();
 }
 
-/* ================================================================ batches */
+/* ================================================================ batches
+ * Every batched kernel reads its work count from device memory (a field of
+ * the launch sequence's BatchCtl), so one instantiated graph serves any set
+ * of members; all but the per-member norm kernel are persistent, with grids
+ * sized to the SMs. */
+
+static int sm_count() {
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    return n > 0 ? n : 1;
+}
 
 template <typename T>
 size_t thomas_batch_smem(int stages) {
@@ -1524,128 +1569,166 @@ int thomas_batch_fit(int stages) {
     return n;
 }
 
-static int sm_count() {
-    int dev = 0, n = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
-    return n > 0 ? n : 1;
-}
-
 template <typename T>
 int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
-                        const WorkItem *work, int nwork, const int *active, unsigned *queue,
+                        const WorkItem *work, const int *nwork, const int *active, unsigned *queue,
                         unsigned *status) {
-    if (nwork <= 0) return 0;
     if (bs.stages < 2 || bs.stages > 8 || bs.ctas_per_sm < 1) return (int)cudaErrorInvalidValue;
     const size_t smem = thomas_batch_smem<T>(bs.stages);
-    long long grid = (long long)bs.ctas_per_sm * sm_count();
-    if (grid > nwork) grid = nwork;
-    fast_thomas_batch_kernel<T, THOMAS_P><<<(int)grid, 32, smem, st>>>(sys, work, nwork, active,
-                                                                        queue, bs.stages, status);
+    const int grid = bs.ctas_per_sm * sm_count();
+    fast_thomas_batch_kernel<T, THOMAS_P><<<grid, 32, smem, st>>>(sys, work, nwork, active, queue,
+                                                                   bs.stages, status);
     return (int)cudaGetLastError();
 }
 
+/* persistent residual over (member, tile) items: CTA k takes items k,
+ * k + grid, ...; each tile completes one phase of the CTA's barrier */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_batch_kernel(
-    const ResidSys<T> *__restrict__ sys, const WorkItem *__restrict__ work, int mode,
-    const int *__restrict__ active, unsigned *status) {
-    const WorkItem it = work[blockIdx.x];
-    if (active && !active[it.sys]) return;
-    const ResidSys<T> S = sys[it.sys];
-    NormSink ns{};
-    ns.partials = (mode == 3) ? nullptr : S.partials; /* no counter: partials only */
-    fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr, S.dU, S.Rsrc, S.b,
-                       S.Uacc, ns, status, it.unit);
+    const ResidSys<T> *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ nwork_p, int mode, const int *__restrict__ active, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
+    const int nwork = *nwork_p;
+    uint32_t parity = 0;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const WorkItem it = work[w];
+        if (active && !active[it.sys]) continue;
+        const ResidSys<T> S = sys[it.sys];
+        NormSink ns{};
+        ns.partials = (mode == 3) ? nullptr : S.partials; /* no counter: partials only */
+        const bool ok = fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr,
+                                           S.dU, S.Rsrc, S.b, S.Uacc, ns, status, it.unit, bar,
+                                           parity);
+        parity ^= 1u;
+        if (!ok) break;
+        __syncthreads(); /* the next tile's copies overwrite the stages */
+    }
+}
+
+static int resid_batch_grid(size_t smem, const void *fn) {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, RES_THREADS_FAST, smem) != cudaSuccess ||
+        per < 1)
+        per = 1;
+    return per * sm_count();
 }
 
 template <typename T>
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const WorkItem *work, int nwork, const int *active, unsigned *status) {
-    if (nwork <= 0) return 0;
+                       const WorkItem *work, const int *nwork, const int *active, unsigned *status) {
     if (mode != 0 && mode != 1 && mode != 3) return (int)cudaErrorInvalidValue;
     const size_t smem = resid_smem_bytes<T>(mode == 0 ? 0 : max_nx);
-    fast_resid_batch_kernel<T><<<nwork, RES_THREADS_FAST, smem, st>>>(sys, work, mode, active,
-                                                                      status);
+    const int grid = resid_batch_grid(smem, (const void *)fast_resid_batch_kernel<T>);
+    fast_resid_batch_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(sys, work, nwork, mode, active,
+                                                                     status);
     return (int)cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(FULLRES_THREADS) full_resid_batch_kernel(
     const FullResSys *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ active) {
-    const WorkItem it = work[blockIdx.x];
-    if (active && !active[it.sys]) return;
-    const FullResSys S = sys[it.sys];
-    full_resid_body<float>(S.nelem, S.epoint, S.ef, S.fc, S.pos_of_elem, S.D, S.O1, S.O2, S.rhs,
-                           S.Up, S.R32, S.partials, it.unit);
+    const int *__restrict__ nwork_p, const int *__restrict__ active) {
+    const int nwork = *nwork_p;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const WorkItem it = work[w];
+        if (active && !active[it.sys]) continue;
+        const FullResSys S = sys[it.sys];
+        full_resid_body<float>(S.nelem, S.epoint, S.ef, S.fc, S.pos_of_elem, S.D, S.O1, S.O2,
+                               S.rhs, S.Up, S.R32, S.partials, it.unit);
+        __syncthreads(); /* the block sum's shared array is reused */
+    }
 }
 
-int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work, int nwork,
-                            const int *active) {
-    if (nwork <= 0) return 0;
-    full_resid_batch_kernel<<<nwork, FULLRES_THREADS, 0, st>>>(sys, work, active);
+static int plain_batch_grid(const void *fn, int threads) {
+    int per = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, threads, 0) != cudaSuccess || per < 1)
+        per = 1;
+    return per * sm_count();
+}
+
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work,
+                            const int *nwork, const int *active) {
+    const int grid = plain_batch_grid((const void *)full_resid_batch_kernel, FULLRES_THREADS);
+    full_resid_batch_kernel<<<grid, FULLRES_THREADS, 0, st>>>(sys, work, nwork, active);
     return (int)cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_batch_kernel(
-    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work) {
-    const WorkItem it = work[blockIdx.x];
-    const VecSys S = sys[it.sys];
-    mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, it.unit);
+    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ nwork_p) {
+    const int nwork = *nwork_p;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const WorkItem it = work[w];
+        const VecSys S = sys[it.sys];
+        mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, it.unit);
+        __syncthreads();
+    }
 }
 
-int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork) {
-    if (nwork <= 0) return 0;
-    mixed_prime_batch_kernel<<<nwork, RES_THREADS_FAST, 0, st>>>(sys, work);
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work,
+                             const int *nwork) {
+    const int grid = plain_batch_grid((const void *)mixed_prime_batch_kernel, RES_THREADS_FAST);
+    mixed_prime_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, work, nwork);
     return (int)cudaGetLastError();
 }
 
 /* U += c + d over one tile (elementwise: the same values as axpy2_kernel) */
 __global__ void __launch_bounds__(RES_THREADS_FAST) axpy2_batch_kernel(
     const VecSys *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ active) {
-    const WorkItem it = work[blockIdx.x];
-    if (active && !active[it.sys]) return;
-    if (threadIdx.x >= RES_TILE * NV) return;
-    const VecSys S = sys[it.sys];
-    const size_t q = (size_t)it.unit * RES_TILE * NV + threadIdx.x;
-    S.Up[q] += (double)S.c32[q] + (double)S.d32[q];
+    const int *__restrict__ nwork_p, const int *__restrict__ active) {
+    const int nwork = *nwork_p;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const WorkItem it = work[w];
+        if (active && !active[it.sys]) continue;
+        if (threadIdx.x >= RES_TILE * NV) continue;
+        const VecSys S = sys[it.sys];
+        const size_t q = (size_t)it.unit * RES_TILE * NV + threadIdx.x;
+        S.Up[q] += (double)S.c32[q] + (double)S.d32[q];
+    }
 }
 
-int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork,
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, const int *nwork,
                        const int *active) {
-    if (nwork <= 0) return 0;
-    axpy2_batch_kernel<<<nwork, RES_THREADS_FAST, 0, st>>>(sys, work, active);
+    const int grid = plain_batch_grid((const void *)axpy2_batch_kernel, RES_THREADS_FAST);
+    axpy2_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, work, nwork, active);
     return (int)cudaGetLastError();
 }
 
-__global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, int nsys, int is_start,
-                                    int *active, unsigned *counter,
+/* One CTA per descriptor (grid = capacity; CTAs beyond *nred only take
+ * their ticket).  The last CTA to finish decides whether the graph's loop
+ * goes on: some member is active, the sweep limit of the launch is not
+ * reached and, when asked, no member stopped during the launch. */
+__global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, const int *__restrict__ nred_p,
+                                    int is_start, int *active, BatchCtl *ctl, unsigned *counter,
                                     cudaGraphConditionalHandle handle, int use_cond) {
     __shared__ double red[32];
     __shared__ unsigned ticket;
     const int s = blockIdx.x;
-    const ReduceSys R = sys[s];
-    if (is_start || active[s]) {
-        double acc = 0.0;
-        for (int t = threadIdx.x; t < R.n; t += blockDim.x) acc += R.partials[t];
-        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            double tot = 0.0;
-            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
-            const double nrm = sqrt(tot);
-            SolveState *S = R.state;
-            if (is_start) {
-                S->sweep = 0;
-                S->norm0 = nrm;
-            } else {
-                S->sweep += 1;
+    if (s < *nred_p) {
+        const ReduceSys R = sys[s];
+        const int m = R.member;
+        if (is_start || active[m]) {
+            double acc = strided_sum(R.partials, R.n, (int)blockDim.x);
+            for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+            if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+            __syncthreads();
+            if (threadIdx.x == 0) {
+                double tot = 0.0;
+                for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
+                const double nrm = sqrt(tot);
+                SolveState *S = R.state;
+                if (is_start) {
+                    S->sweep = 0;
+                    S->norm0 = nrm;
+                } else {
+                    S->sweep += 1;
+                }
+                const int sw = S->sweep;
+                if (sw < S->hist_cap) R.hist[sw] = nrm;
+                S->last = nrm;
+                const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
+                active[m] = go ? 1 : 0;
+                if (!go) ctl->finished = 1;
             }
-            const int sw = S->sweep;
-            if (sw < S->hist_cap) R.hist[sw] = nrm;
-            S->last = nrm;
-            active[s] = (isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps) ? 1 : 0;
         }
     }
     if (threadIdx.x == 0) {
@@ -1656,25 +1739,31 @@ __global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, int nsys,
     if (threadIdx.x == 0 && ticket == gridDim.x - 1) {
         __threadfence();
         int any = 0;
-        for (int k = 0; k < nsys; ++k) any |= __ldcg(active + k);
-        if (use_cond) cudaGraphSetConditional(handle, any ? 1u : 0u);
+        const int n = ctl->nsys;
+        for (int k = 0; k < n; ++k) any |= __ldcg(active + k);
+        bool go = any != 0;
+        if (!is_start && ctl->chunk_limit > 0) {
+            ctl->chunk += 1;
+            if (ctl->chunk >= ctl->chunk_limit) go = false;
+        }
+        if (ctl->stop_on_finish && __ldcg(&ctl->finished)) go = false;
+        if (use_cond) cudaGraphSetConditional(handle, go ? 1u : 0u);
         *counter = 0u;
     }
 }
 
-int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, int nsys,
-                        int is_start, int *active, unsigned *counter,
+int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, const int *nred,
+                        int cap, int is_start, int *active, BatchCtl *ctl, unsigned *counter,
                         unsigned long long cond_handle, int use_cond) {
-    if (nsys <= 0) return 0;
+    if (cap <= 0) return 0;
     if (threads != RES_THREADS_FAST && threads != 256) return (int)cudaErrorInvalidValue;
-    batch_reduce_kernel<<<nsys, threads, 0, st>>>(sys, nsys, is_start, active, counter,
-                                                  (cudaGraphConditionalHandle)cond_handle,
-                                                  use_cond);
+    batch_reduce_kernel<<<cap, threads, 0, st>>>(sys, nred, is_start, active, ctl, counter,
+                                                 (cudaGraphConditionalHandle)cond_handle, use_cond);
     return (int)cudaGetLastError();
 }
 
-/* opt the batched residual kernels into the shared memory of the widest
- * system (outside stream capture) */
+/* opt the batched kernels into the shared memory of the widest member
+ * (outside stream capture) */
 int batch_prepare(int max_nx) {
     int rc = set_smem((const void *)fast_resid_batch_kernel<double>, resid_smem_bytes<double>(max_nx));
     if (!rc)
@@ -1687,12 +1776,14 @@ template size_t thomas_batch_smem<float>(int);
 template int thomas_batch_fit<double>(int);
 template int thomas_batch_fit<float>(int);
 template int launch_thomas_batch<double>(cudaStream_t, const BatchSched &, const ThomasSys<double> *,
-                                         const WorkItem *, int, const int *, unsigned *, unsigned *);
+                                         const WorkItem *, const int *, const int *, unsigned *,
+                                         unsigned *);
 template int launch_thomas_batch<float>(cudaStream_t, const BatchSched &, const ThomasSys<float> *,
-                                        const WorkItem *, int, const int *, unsigned *, unsigned *);
+                                        const WorkItem *, const int *, const int *, unsigned *,
+                                        unsigned *);
 template int launch_resid_batch<double>(cudaStream_t, int, int, const ResidSys<double> *,
-                                        const WorkItem *, int, const int *, unsigned *);
+                                        const WorkItem *, const int *, const int *, unsigned *);
 template int launch_resid_batch<float>(cudaStream_t, int, int, const ResidSys<float> *,
-                                       const WorkItem *, int, const int *, unsigned *);
+                                       const WorkItem *, const int *, const int *, unsigned *);
 
 }  // namespace tbs

@@ -1,0 +1,683 @@
+/*
+ * server.cu -- tbs_server_*: a request loop over systems whose factors stay
+ * resident in HBM (continuous batching).  No counterpart in the reference,
+ * whose driver (src/main.cxx) factors and sweeps one system per run.
+ *
+ * Requests carry right-hand sides for a registered system and, optionally,
+ * new Jacobian values that re-factor the system first.  A loop thread
+ *   - admits queued requests in arrival order while their right-hand sides
+ *     fit the device budget and the slot limit (admission by footprint;
+ *     a request that does not fit holds back the ones behind it, so that
+ *     large requests are not starved),
+ *   - runs every admitted right-hand side together through the batched
+ *     engine (engine.hxx): one graph launch primes the newly admitted ones
+ *     and sweeps all of them until one reaches its tolerance or a chunk of
+ *     sweeps is done, so new arrivals join at the next sweep boundary,
+ *   - retires each right-hand side as soon as it stops and completes a
+ *     request when all of its right-hand sides have.
+ * A second thread re-factors systems (upload of the new values and the
+ * factorization on the system's own stream) while the loop keeps sweeping
+ * the other systems' right-hand sides; a system is re-factored only when
+ * none of its right-hand sides is in flight, and its later requests wait
+ * for the new factors.
+ *
+ * The per-right-hand-side arithmetic is that of tbs_solve: a result does
+ * not depend on what else was in flight.
+ */
+#include "engine.hxx"
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <vector>
+
+using namespace tbs;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+double ms_between(Clock::time_point a, Clock::time_point b) {
+    return std::chrono::duration<double, std::milli>(b - a).count();
+}
+
+struct SrvSystem {
+    tbs_ctx *ctx = nullptr;
+    int inflight = 0;       /* right-hand sides in flight */
+    bool refactoring = false;
+    bool broken = false;    /* a re-factorization failed: its requests fail */
+};
+
+struct SrvRequest {
+    long long id = 0;
+    int sys = 0;
+    tbs_ctx *ctx = nullptr;      /* the system's context (stable while the server lives) */
+    int nrhs = 0;
+    const double *rhs = nullptr; /* caller's: nrhs x 9 nelem, valid until completion */
+    double *U = nullptr;         /* caller's output */
+    double tol = 0.0;
+    int max_sweeps = 0;
+    const double *jacD = nullptr, *jacO1 = nullptr, *jacO2 = nullptr; /* re-factor first */
+    bool refactored = false;
+    std::vector<int> sweeps;
+    std::vector<double> rel;
+    int remaining = 0;
+    enum { QUEUED, FACTORING, RUNNING, DONE, FAILED } state = QUEUED;
+    int err = 0;
+    std::string msg;
+    size_t bytes = 0;            /* device bytes of its right-hand sides */
+    Clock::time_point t_submit, t_admit, t_done;
+};
+
+struct SrvSlot {               /* one right-hand side in flight (an engine member) */
+    SrvRequest *req = nullptr;
+    int k = 0;                 /* which right-hand side of the request */
+    void *mem = nullptr;       /* one stream-ordered allocation for all its vectors */
+    size_t bytes = 0;
+    VecSet v;
+    double *rhs_elem = nullptr; /* element-order rhs, reused for the solution read-back */
+    bool fresh = true;
+};
+
+}  // namespace
+
+struct tbs_server {
+    int device = 0;
+    int algo = TBS_ALGO_FP64;
+    size_t budget = 0;         /* device bytes for systems + right-hand sides in flight */
+    int max_slots = 64;
+    int chunk = 4;             /* sweeps per graph launch at most */
+    std::string err;
+
+    std::mutex mu;
+    std::condition_variable cv_loop, cv_done, cv_factor;
+    bool stopping = false;
+    std::vector<SrvSystem> systems;
+    size_t sys_bytes = 0;
+    size_t slot_bytes_in_flight = 0;
+    std::deque<SrvRequest *> queue;
+    std::map<long long, std::unique_ptr<SrvRequest>> requests;
+    std::deque<SrvRequest *> factor_jobs;
+    long long next_id = 1;
+
+    /* loop-thread state */
+    Engine eng;
+    cudaStream_t stream = nullptr;
+    cudaMemPool_t pool = nullptr;
+    std::vector<SrvSlot> slots;
+    std::thread loop, factor;
+
+    /* statistics */
+    long long n_done = 0, n_rhs_done = 0, n_launches = 0, n_refactor = 0;
+    long long peak_rhs = 0, peak_bytes = 0;
+};
+
+static int sfail(tbs_server *s, int code, const std::string &msg) {
+    if (s) s->err = msg;
+    set_thread_error(msg);
+    return code;
+}
+
+static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+/* device bytes of one right-hand side of system c with a history of hist_n */
+static size_t slot_bytes(const tbs_ctx *c, int algo, int hist_n) {
+    const size_t npv = (size_t)c->L.np16 * 9, ne = (size_t)c->nelem * 9;
+    const size_t nt = (size_t)fast_resid_grid(c->L.np16);
+    size_t b = 0;
+    if (algo == TBS_ALGO_FP64) {
+        b += 5 * align256(npv * sizeof(double)); /* Up, dUp, b, y, rhsp */
+        b += align256(nt * sizeof(double));
+    } else {
+        b += 2 * align256(npv * sizeof(double)); /* Up, rhsp */
+        b += 5 * align256(npv * sizeof(float));  /* b32, y32, d32, c32, R32 */
+        b += align256(std::max(nt, (size_t)full_resid_blocks(c->nelem)) * sizeof(double));
+    }
+    b += align256(ne * sizeof(double));          /* rhs, element order */
+    b += align256(sizeof(SolveState));
+    b += align256((size_t)hist_n * sizeof(double));
+    return b;
+}
+
+/* carve a slot's vectors out of its allocation */
+static void slot_layout(SrvSlot &sl, const tbs_ctx *c, int algo, int hist_n) {
+    const size_t npv = (size_t)c->L.np16 * 9, ne = (size_t)c->nelem * 9;
+    const size_t nt = (size_t)fast_resid_grid(c->L.np16);
+    char *p = static_cast<char *>(sl.mem);
+    auto take = [&](size_t n) {
+        char *q = p;
+        p += align256(n);
+        return q;
+    };
+    VecSet v;
+    if (algo == TBS_ALGO_FP64) {
+        v.Up = (double *)take(npv * sizeof(double));
+        v.dUp = (double *)take(npv * sizeof(double));
+        v.b = (double *)take(npv * sizeof(double));
+        v.y = (double *)take(npv * sizeof(double));
+        v.rhsp = (double *)take(npv * sizeof(double));
+        v.partials = (double *)take(nt * sizeof(double));
+    } else {
+        v.Up = (double *)take(npv * sizeof(double));
+        v.rhsp = (double *)take(npv * sizeof(double));
+        v.b32 = (float *)take(npv * sizeof(float));
+        v.y32 = (float *)take(npv * sizeof(float));
+        v.d32 = (float *)take(npv * sizeof(float));
+        v.c32 = (float *)take(npv * sizeof(float));
+        v.R32 = (float *)take(npv * sizeof(float));
+        v.partials = (double *)take(std::max(nt, (size_t)full_resid_blocks(c->nelem)) * sizeof(double));
+    }
+    sl.rhs_elem = (double *)take(ne * sizeof(double));
+    v.rhs = sl.rhs_elem;
+    v.state = (SolveState *)take(sizeof(SolveState));
+    v.hist = (double *)take((size_t)hist_n * sizeof(double));
+    sl.v = v;
+}
+
+static void complete(tbs_server *s, SrvRequest *r, int err, const std::string &msg) {
+    r->t_done = Clock::now();
+    r->state = err ? SrvRequest::FAILED : SrvRequest::DONE;
+    r->err = err;
+    r->msg = msg;
+    if (!err) {
+        s->n_done += 1;
+        s->n_rhs_done += r->nrhs;
+    }
+}
+
+/* ---------------------------------------------------------------- factor thread */
+
+static void factor_main(tbs_server *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        s->cv_factor.wait(lk, [&] { return s->stopping || !s->factor_jobs.empty(); });
+        if (s->factor_jobs.empty()) {
+            if (s->stopping) break;
+            continue;
+        }
+        SrvRequest *r = s->factor_jobs.front();
+        s->factor_jobs.pop_front();
+        tbs_ctx *c = r->ctx;
+        lk.unlock();
+        int rc = tbs_set_jacobian(c, r->jacD, r->jacO1, r->jacO2, r->rhs, nullptr);
+        if (!rc) rc = tbs_factor(c, s->algo);
+        std::string msg = rc ? std::string(tbs_last_error(c)) : std::string();
+        lk.lock();
+        s->systems[r->sys].refactoring = false;
+        s->n_refactor += 1;
+        if (rc) {
+            /* the request fails, and so do the system's later requests: its
+             * factors may be half replaced */
+            s->systems[r->sys].broken = true;
+            complete(s, r, rc, "re-factorization failed: " + msg);
+            s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
+            s->cv_done.notify_all();
+        } else {
+            r->refactored = true;
+            r->state = SrvRequest::QUEUED;
+        }
+        s->cv_loop.notify_all();
+    }
+}
+
+/* ---------------------------------------------------------------- loop thread */
+
+/* Admission scan under the lock: requests in arrival order; a request that
+ * needs a re-factorization goes to the factor thread once its system is
+ * idle; later requests of a system that is being re-factored wait; the
+ * first request whose right-hand sides do not fit ends the scan. */
+static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
+    std::vector<char> blocked(s->systems.size(), 0);
+    const size_t avail = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
+    for (auto it = s->queue.begin(); it != s->queue.end();) {
+        SrvRequest *r = *it;
+        SrvSystem &sys = s->systems[r->sys];
+        if (sys.broken && r->state == SrvRequest::QUEUED) {
+            complete(s, r, TBS_ERR_STATE, "the system's re-factorization failed");
+            s->cv_done.notify_all();
+            it = s->queue.erase(it);
+            continue;
+        }
+        if (r->state == SrvRequest::FACTORING || blocked[r->sys] || sys.refactoring) {
+            blocked[r->sys] = 1;
+            ++it;
+            continue;
+        }
+        if (r->jacD && !r->refactored) {
+            if (sys.inflight == 0) {
+                sys.refactoring = true;
+                r->state = SrvRequest::FACTORING;
+                s->factor_jobs.push_back(r);
+                s->cv_factor.notify_all();
+            }
+            blocked[r->sys] = 1;
+            ++it;
+            continue;
+        }
+        const int in_flight = (int)s->slots.size() + [&] {
+            int n = 0;
+            for (SrvRequest *a : admitted) n += a->nrhs;
+            return n;
+        }();
+        if (in_flight + r->nrhs > s->max_slots || s->slot_bytes_in_flight + r->bytes > avail) break;
+        s->slot_bytes_in_flight += r->bytes;
+        sys.inflight += r->nrhs;
+        r->state = SrvRequest::RUNNING;
+        r->t_admit = Clock::now();
+        admitted.push_back(r);
+        it = s->queue.erase(it);
+    }
+}
+
+/* allocate and fill the right-hand sides of newly admitted requests */
+static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitted,
+                          std::vector<SrvRequest *> &failed) {
+    for (SrvRequest *r : admitted) {
+        tbs_ctx *c = r->ctx;
+        const size_t nv = (size_t)c->nelem * 9;
+        const size_t per = r->bytes / r->nrhs;
+        bool ok = true;
+        std::vector<SrvSlot> mine;
+        for (int k = 0; k < r->nrhs && ok; ++k) {
+            SrvSlot sl;
+            sl.req = r;
+            sl.k = k;
+            sl.bytes = per;
+            if (cudaMallocFromPoolAsync(&sl.mem, per, s->pool, s->stream) != cudaSuccess) {
+                cudaGetLastError();
+                ok = false;
+                break;
+            }
+            slot_layout(sl, c, s->algo, r->max_sweeps + 1);
+            /* pad positions of the layout are never written by the kernels
+             * but enter the first norm (rhs) and the U accumulation: start
+             * from zeros, as a context's arrays do */
+            if (cudaMemsetAsync(sl.mem, 0, per, s->stream) != cudaSuccess) {
+                mine.push_back(sl);
+                ok = false;
+                break;
+            }
+            SolveState st{};
+            st.tol = r->tol;
+            st.max_sweeps = r->max_sweeps;
+            st.hist_cap = r->max_sweeps + 1;
+            ok = cudaMemcpyAsync(sl.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream) == cudaSuccess &&
+                 cudaMemcpyAsync(sl.rhs_elem, r->rhs + k * nv, nv * sizeof(double),
+                                 cudaMemcpyHostToDevice, s->stream) == cudaSuccess &&
+                 launch_permute_to_pos(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.rhs_elem,
+                                       sl.v.rhsp) == 0;
+            mine.push_back(sl);
+        }
+        if (!ok) {
+            for (SrvSlot &sl : mine)
+                if (sl.mem) cudaFreeAsync(sl.mem, s->stream);
+            failed.push_back(r);
+            continue;
+        }
+        for (SrvSlot &sl : mine) s->slots.push_back(sl);
+    }
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "upload failed");
+    return TBS_OK;
+}
+
+static int engine_members(tbs_server *s) {
+    std::vector<Member> m;
+    m.reserve(s->slots.size());
+    for (SrvSlot &sl : s->slots) m.push_back({sl.req->ctx, sl.v, sl.fresh});
+    return engine_set_members(s->eng, m);
+}
+
+/* read back the right-hand sides that stopped; returns them in `out` */
+static int retire(tbs_server *s, std::vector<SrvSlot> &out) {
+    std::vector<SrvSlot> keep;
+    std::vector<SolveState> st;
+    for (size_t k = 0; k < s->slots.size(); ++k) {
+        if (s->eng.h_active[k]) {
+            keep.push_back(s->slots[k]);
+            continue;
+        }
+        out.push_back(s->slots[k]);
+    }
+    if (out.empty()) return TBS_OK;
+    st.resize(out.size());
+    for (size_t k = 0; k < out.size(); ++k) {
+        SrvSlot &sl = out[k];
+        tbs_ctx *c = sl.req->ctx;
+        const size_t nv = (size_t)c->nelem * 9;
+        if (cudaMemcpyAsync(&st[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
+            launch_permute_to_elem(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0 ||
+            cudaMemcpyAsync(sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double),
+                            cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+            return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
+        cudaFreeAsync(sl.mem, s->stream);
+    }
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
+        return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
+    for (size_t k = 0; k < out.size(); ++k) {
+        SrvRequest *r = out[k].req;
+        r->sweeps[out[k].k] = st[k].sweep;
+        r->rel[out[k].k] = st[k].norm0 > 0.0 ? st[k].last / st[k].norm0 : 0.0;
+    }
+    s->slots.swap(keep);
+    return TBS_OK;
+}
+
+static void loop_main(tbs_server *s) {
+    cudaSetDevice(s->device);
+    std::unique_lock<std::mutex> lk(s->mu);
+    for (;;) {
+        std::vector<SrvRequest *> admitted;
+        admit_scan(s, admitted);
+        if (admitted.empty() && s->slots.empty()) {
+            if (s->stopping && s->queue.empty() && s->factor_jobs.empty()) break;
+            s->cv_loop.wait(lk);
+            continue;
+        }
+        const int chunk = s->chunk;
+        lk.unlock();
+        std::vector<SrvRequest *> failed;
+        int rc = start_requests(s, admitted, failed);
+        const bool changed = !admitted.empty();
+        if (!rc && changed) rc = engine_members(s);
+        if (!rc) rc = engine_run(s->eng, chunk, 1);
+        if (!rc) rc = engine_read_active(s->eng);
+        std::vector<SrvSlot> done;
+        if (!rc) {
+            for (SrvSlot &sl : s->slots) sl.fresh = false;
+            engine_mark_started(s->eng);
+            rc = retire(s, done);
+        }
+        if (!rc && !done.empty() && !s->slots.empty()) rc = engine_members(s);
+        std::string msg = rc ? s->eng.err + s->err : std::string();
+        lk.lock();
+        s->n_launches += 1;
+        s->peak_rhs = std::max<long long>(s->peak_rhs, (long long)s->slots.size() + (long long)done.size());
+        s->peak_bytes = std::max<long long>(s->peak_bytes, (long long)s->slot_bytes_in_flight);
+        for (SrvRequest *r : failed) {
+            s->systems[r->sys].inflight -= r->nrhs;
+            s->slot_bytes_in_flight -= r->bytes;
+            complete(s, r, TBS_ERR_NOMEM, "device allocation for the right-hand sides failed");
+        }
+        for (SrvSlot &sl : done) {
+            SrvRequest *r = sl.req;
+            s->systems[r->sys].inflight -= 1;
+            s->slot_bytes_in_flight -= sl.bytes;
+            if (--r->remaining == 0) complete(s, r, 0, "");
+        }
+        if (rc) {
+            /* a device error ends every request in flight */
+            for (SrvSlot &sl : s->slots) {
+                SrvRequest *r = sl.req;
+                s->systems[r->sys].inflight -= 1;
+                s->slot_bytes_in_flight -= sl.bytes;
+                if (r->state == SrvRequest::RUNNING) complete(s, r, rc, msg);
+            }
+            s->slots.clear();
+            s->err = msg;
+        }
+        if (!failed.empty() || !done.empty() || rc) s->cv_done.notify_all();
+    }
+}
+
+/* ---------------------------------------------------------------- entry points */
+
+static void server_stop(tbs_server *s) {
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stopping = true;
+        /* queued requests that never started fail */
+        for (SrvRequest *r : s->queue)
+            if (r->state == SrvRequest::QUEUED) complete(s, r, TBS_ERR_STATE, "server stopped");
+        std::deque<SrvRequest *> keep;
+        for (SrvRequest *r : s->queue)
+            if (r->state == SrvRequest::FACTORING) keep.push_back(r);
+        s->queue.swap(keep);
+        s->cv_loop.notify_all();
+        s->cv_factor.notify_all();
+        s->cv_done.notify_all();
+    }
+    if (s->factor.joinable()) s->factor.join();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        for (SrvRequest *r : s->queue) complete(s, r, TBS_ERR_STATE, "server stopped");
+        s->queue.clear();
+        s->cv_loop.notify_all();
+    }
+    if (s->loop.joinable()) s->loop.join();
+}
+
+extern "C" {
+
+const char *tbs_server_last_error(const tbs_server *s) {
+    if (!s) return thread_error();
+    return s->err.c_str();
+}
+
+int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int max_rhs_in_flight,
+                      tbs_server **out) {
+    if (!out) return sfail(nullptr, TBS_ERR_ARG, "null output");
+    *out = nullptr;
+    if (algo != TBS_ALGO_FP64 && algo != TBS_ALGO_MIXED)
+        return sfail(nullptr, TBS_ERR_UNSUPPORTED, "the server runs TBS_ALGO_FP64 or TBS_ALGO_MIXED");
+    if (max_rhs_in_flight < 1 || device_budget_bytes == 0)
+        return sfail(nullptr, TBS_ERR_ARG, "bad budget or slot limit");
+    tbs_server *s = nullptr;
+    try {
+        s = new tbs_server();
+    } catch (...) {
+        return sfail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
+    }
+    s->device = device_id;
+    s->algo = algo;
+    s->budget = device_budget_bytes;
+    s->max_slots = max_rhs_in_flight;
+    auto fail = [&](int code, const std::string &msg) {
+        if (s->eng.h_ctl) engine_free(s->eng);
+        if (s->pool) cudaMemPoolDestroy(s->pool);
+        if (s->stream) cudaStreamDestroy(s->stream);
+        delete s;
+        return sfail(nullptr, code, msg);
+    };
+    if (cudaSetDevice(device_id) != cudaSuccess) return fail(TBS_ERR_CUDA, "cudaSetDevice failed");
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+        return fail(TBS_ERR_CUDA, "cudaStreamCreate failed");
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device_id;
+    if (cudaMemPoolCreate(&s->pool, &props) != cudaSuccess)
+        return fail(TBS_ERR_CUDA, "cudaMemPoolCreate failed");
+    uint64_t keep = ~0ull; /* freed right-hand-side memory stays in the pool */
+    cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    int rc = engine_init(s->eng, device_id, s->stream, algo);
+    if (rc) return fail(rc, s->eng.err);
+    try {
+        s->loop = std::thread(loop_main, s);
+        s->factor = std::thread(factor_main, s);
+    } catch (...) {
+        s->stopping = true;
+        if (s->loop.joinable()) {
+            s->cv_loop.notify_all();
+            s->loop.join();
+        }
+        return fail(TBS_ERR_STATE, "thread start failed");
+    }
+    *out = s;
+    return TBS_OK;
+}
+
+int tbs_server_destroy(tbs_server *s) {
+    if (!s) return TBS_OK;
+    server_stop(s);
+    cudaSetDevice(s->device);
+    cudaStreamSynchronize(s->stream);
+    engine_free(s->eng);
+    for (SrvSystem &sys : s->systems) tbs_destroy(sys.ctx);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
+    if (s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+    return TBS_OK;
+}
+
+int tbs_server_set_chunk(tbs_server *s, int sweeps) {
+    if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
+    if (sweeps < 1) return sfail(s, TBS_ERR_ARG, "chunk must be at least one sweep");
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->chunk = sweeps;
+    return TBS_OK;
+}
+
+int tbs_server_add_system(tbs_server *s, int nvar, int nelem, int nintface, int eftot, int nline,
+                          int nlineelem, const int *epoint, const int *ef, const int *fc,
+                          const int *linesize, const int *linepoint, const int *lines,
+                          const int *lineface, const double *jacD, const double *jacO1,
+                          const double *jacO2, int *system_id) {
+    if (!s || !system_id) return sfail(s, TBS_ERR_ARG, "null argument");
+    tbs_ctx *c = nullptr;
+    int rc = tbs_create(s->device, &c);
+    if (rc) return sfail(s, rc, thread_error());
+    auto fail = [&](int code) {
+        std::string msg = tbs_last_error(c);
+        tbs_destroy(c);
+        return sfail(s, code, msg);
+    };
+    rc = tbs_set_mesh(c, nvar, nelem, nintface, eftot, nline, nlineelem, epoint, ef, fc, linesize,
+                      linepoint, lines, lineface);
+    if (rc) return fail(rc);
+    try {
+        std::vector<double> zero((size_t)nvar * nelem, 0.0);
+        rc = tbs_set_jacobian(c, jacD, jacO1, jacO2, zero.data(), nullptr);
+    } catch (...) {
+        rc = TBS_ERR_NOMEM;
+    }
+    if (rc) return fail(rc);
+    rc = tbs_factor(c, s->algo);
+    if (rc) return fail(rc);
+    size_t bytes = 0;
+    tbs_memory_allocated(c, &bytes);
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (s->sys_bytes + bytes > s->budget) {
+        tbs_destroy(c);
+        return sfail(s, TBS_ERR_NOMEM, "the system does not fit the server's device budget");
+    }
+    s->sys_bytes += bytes;
+    SrvSystem sys;
+    sys.ctx = c;
+    s->systems.push_back(sys);
+    *system_id = (int)s->systems.size() - 1;
+    return TBS_OK;
+}
+
+int tbs_server_system_bytes(tbs_server *s, int system_id, int max_sweeps, size_t *resident,
+                            size_t *per_rhs) {
+    if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (system_id < 0 || system_id >= (int)s->systems.size())
+        return sfail(s, TBS_ERR_ARG, "unknown system");
+    tbs_ctx *c = s->systems[system_id].ctx;
+    if (resident) tbs_memory_allocated(c, resident);
+    if (per_rhs) *per_rhs = slot_bytes(c, s->algo, std::max(max_sweeps, 0) + 1);
+    return TBS_OK;
+}
+
+int tbs_server_submit(tbs_server *s, int system_id, int nrhs, const double *rhs, double *U_out,
+                      double rel_tol, int max_sweeps, const double *jacD, const double *jacO1,
+                      const double *jacO2, long long *request_id) {
+    if (!s || !request_id) return sfail(s, TBS_ERR_ARG, "null argument");
+    if (nrhs < 1 || !rhs || !U_out || max_sweeps < 0 || !(rel_tol >= 0.0))
+        return sfail(s, TBS_ERR_ARG, "bad request");
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->stopping) return sfail(s, TBS_ERR_STATE, "server stopping");
+    if (system_id < 0 || system_id >= (int)s->systems.size())
+        return sfail(s, TBS_ERR_ARG, "unknown system");
+    tbs_ctx *c = s->systems[system_id].ctx;
+    if (jacD && (!jacO1 || !jacO2) && c->nintface > 0)
+        return sfail(s, TBS_ERR_ARG, "new Jacobian values need jacD, jacO1 and jacO2");
+    const size_t per = slot_bytes(c, s->algo, max_sweeps + 1);
+    const size_t avail = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
+    if (nrhs > s->max_slots || per * nrhs > avail)
+        return sfail(s, TBS_ERR_NOMEM, "the request can never fit the server's budget or slot limit");
+    std::unique_ptr<SrvRequest> r;
+    try {
+        r.reset(new SrvRequest());
+        r->sweeps.assign(nrhs, 0);
+        r->rel.assign(nrhs, 0.0);
+    } catch (...) {
+        return sfail(s, TBS_ERR_NOMEM, "host allocation failed");
+    }
+    r->id = s->next_id++;
+    r->sys = system_id;
+    r->ctx = c;
+    r->nrhs = nrhs;
+    r->rhs = rhs;
+    r->U = U_out;
+    r->tol = rel_tol;
+    r->max_sweeps = max_sweeps;
+    r->jacD = jacD;
+    r->jacO1 = jacO1;
+    r->jacO2 = jacO2;
+    r->remaining = nrhs;
+    r->bytes = per * nrhs;
+    r->t_submit = Clock::now();
+    SrvRequest *raw = r.get();
+    s->requests[raw->id] = std::move(r);
+    s->queue.push_back(raw);
+    *request_id = raw->id;
+    s->cv_loop.notify_all();
+    return TBS_OK;
+}
+
+int tbs_server_poll(tbs_server *s, long long request_id, int *done) {
+    if (!s || !done) return sfail(s, TBS_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return sfail(s, TBS_ERR_ARG, "unknown request");
+    const auto st = it->second->state;
+    *done = (st == SrvRequest::DONE || st == SrvRequest::FAILED) ? 1 : 0;
+    return TBS_OK;
+}
+
+int tbs_server_wait(tbs_server *s, long long request_id, int *sweeps, double *rel_residual,
+                    double *latency_ms, double *queue_ms) {
+    if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->requests.find(request_id);
+    if (it == s->requests.end()) return sfail(s, TBS_ERR_ARG, "unknown request");
+    SrvRequest *r = it->second.get();
+    s->cv_done.wait(lk, [&] { return r->state == SrvRequest::DONE || r->state == SrvRequest::FAILED; });
+    const int err = r->err;
+    const std::string msg = r->msg;
+    if (!err) {
+        for (int k = 0; k < r->nrhs; ++k) {
+            if (sweeps) sweeps[k] = r->sweeps[k];
+            if (rel_residual) rel_residual[k] = r->rel[k];
+        }
+        if (latency_ms) *latency_ms = ms_between(r->t_submit, r->t_done);
+        if (queue_ms) *queue_ms = ms_between(r->t_submit, r->t_admit);
+    }
+    s->requests.erase(it);
+    if (err) return sfail(s, err, msg);
+    return TBS_OK;
+}
+
+int tbs_server_stats(tbs_server *s, long long *stats, int n) {
+    if (!s || !stats) return sfail(s, TBS_ERR_ARG, "null argument");
+    std::lock_guard<std::mutex> lk(s->mu);
+    const long long v[] = {s->n_done, s->n_rhs_done, s->n_launches, s->n_refactor, s->peak_rhs,
+                           s->peak_bytes, (long long)s->sys_bytes, (long long)s->queue.size()};
+    for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) stats[k] = v[k];
+    return TBS_OK;
+}
+
+}  // extern "C"

@@ -234,9 +234,25 @@ struct VecSys {                 /* mixed-precision glue of one system */
 };
 struct ReduceSys {
     const double *partials;
-    int n, pad;
+    int n;                      /* partials to sum */
+    int member;                 /* index into active[] */
     SolveState *state;
     double *hist;
+};
+/* Device-side control of a batched launch sequence: the work counts the
+ * kernels read (so that one graph serves any set of members) and the rule
+ * by which the per-member norm launch ends the graph's sweep loop. */
+struct BatchCtl {
+    int nsys;                   /* members: active[0..nsys) */
+    int nlines;                 /* Thomas work items */
+    int ntiles;                 /* residual tiles */
+    int nblocks;                /* full-residual element blocks */
+    int nprime_sys;             /* norm descriptors of the members started now */
+    int nprime_tiles;           /* their tiles */
+    int chunk;                  /* sweeps done by the current graph launch */
+    int chunk_limit;            /* > 0: the loop ends after this many sweeps */
+    int stop_on_finish;         /* 1: the loop ends when a member stops */
+    int finished;               /* set by the norm launch when a member stops */
 };
 struct BatchSched {             /* persistent Thomas launch shape */
     int ctas_per_sm;            /* one warp per CTA, one line at a time */
@@ -250,22 +266,24 @@ template <typename T>
 int thomas_batch_fit(int stages);
 template <typename T>
 int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
-                        const WorkItem *work, int nwork, const int *active, unsigned *queue,
+                        const WorkItem *work, const int *nwork, const int *active, unsigned *queue,
                         unsigned *status);
 template <typename T>
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const WorkItem *work, int nwork, const int *active, unsigned *status);
-int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work, int nwork,
-                            const int *active);
-int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork);
-int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, int nwork,
+                       const WorkItem *work, const int *nwork, const int *active, unsigned *status);
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work,
+                            const int *nwork, const int *active);
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work,
+                             const int *nwork);
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, const int *nwork,
                        const int *active);
-/* one CTA of `threads` threads per system: the fixed-order sum of its
- * partials (the order of finalize_norm for threads = 160 and of
- * reduce_norm for threads = 256), its norm history and active flag; the
- * last CTA sets the graph condition to "some system is still active" */
-int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, int nsys,
-                        int is_start, int *active, unsigned *counter,
+/* one CTA of `threads` threads per norm descriptor (grid = cap, *nred in
+ * use): the fixed-order sum of the member's partials (the order of
+ * finalize_norm for threads = 160 and of reduce_norm for threads = 256),
+ * its norm history and active flag; the last CTA sets the graph condition
+ * by the rule in `ctl` */
+int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, const int *nred,
+                        int cap, int is_start, int *active, BatchCtl *ctl, unsigned *counter,
                         unsigned long long cond_handle, int use_cond);
 int batch_prepare(int max_nx);
 
