@@ -539,6 +539,8 @@ def run_serving(args):
                                                 for k, v in per_shape.items()},
                             "p99_ms_by_shape": {k: round(float(np.percentile(v, 99)), 3)
                                                 for k, v in per_shape.items()}},
+                "loop_ms": {k: round((st1[k] - st0[k]) / 1e3, 1)
+                            for k in ("us_start", "us_members", "us_run", "us_retire")},
                 "peak_rhs_in_flight": st2["peak_rhs_in_flight"],
                 "peak_rhs_gb": round(st2["peak_rhs_bytes"] / 1e9, 2),
                 "resident_systems_gb": round(st2["resident_system_bytes"] / 1e9, 2),

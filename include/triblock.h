@@ -337,10 +337,13 @@ int tbs_batch_profile_read(tbs_batch *batch, int *n, const char **names,
  * All admitted right-hand sides are swept together (continuous batching):
  * a request that arrives while others are on the GPU joins them at the
  * next sweep boundary, and each right-hand side leaves when it reaches its
- * tolerance or sweep limit.  Re-factorizations run on a second thread while
- * the other systems keep sweeping; a system is re-factored only when none
- * of its right-hand sides is in flight.  Every solution is bit-identical to
- * tbs_solve of the same system and right-hand side on its own.
+ * tolerance or sweep limit.  Re-factorizations run on a second thread into
+ * a spare copy of the system's factors (counted against the budget; when
+ * it does not fit, in place once the system's right-hand sides are done),
+ * so the right-hand sides already admitted keep sweeping on the current
+ * factors; the system's later requests use the new ones.  Every solution
+ * is bit-identical to tbs_solve of the same system and right-hand side on
+ * its own.
  * The rhs, U_out and new Jacobian arrays stay owned by the caller and must
  * stay valid until tbs_server_wait returns for the request. */
 typedef struct tbs_server tbs_server;
@@ -378,7 +381,9 @@ int tbs_server_wait(tbs_server *srv, long long request_id, int *sweeps,
                     double *rel_residual, double *latency_ms, double *queue_ms);
 /* stats[0..n): requests done, right-hand sides done, graph launches,
  * re-factorizations, peak right-hand sides in flight, peak bytes of
- * right-hand sides in flight, bytes of resident systems, requests queued */
+ * right-hand sides in flight, bytes of resident systems, requests queued,
+ * then the loop thread's microseconds spent starting right-hand sides,
+ * rebuilding the member set, in graph launches, and reading results back */
 int tbs_server_stats(tbs_server *srv, long long *stats, int n);
 
 /* Library version string. */

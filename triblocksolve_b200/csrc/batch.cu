@@ -78,6 +78,47 @@ static int eupload(Engine &e, T *dst, const std::vector<T> &h) {
     return TBS_OK;
 }
 
+/* Uploads through the engine's pinned staging buffer: asynchronous on the
+ * engine's stream without a synchronisation; the buffer is reused after
+ * the previous batch of uploads has been consumed (stage_ev). */
+struct Stager {
+    Engine &e;
+    size_t used = 0;
+    std::vector<std::pair<void *, std::pair<size_t, size_t>>> jobs; /* dst, (offset, bytes) */
+    std::vector<char> host;
+    explicit Stager(Engine &en) : e(en) {}
+    template <typename T>
+    void put(T *dst, const std::vector<T> &v) {
+        if (v.empty()) return;
+        const size_t b = v.size() * sizeof(T);
+        const size_t off = host.size();
+        const char *src = reinterpret_cast<const char *>(v.data());
+        host.insert(host.end(), src, src + b);
+        host.resize(off + ((b + 255) & ~(size_t)255));
+        jobs.push_back({(void *)dst, {off, b}});
+    }
+    int flush() {
+        if (jobs.empty()) return TBS_OK;
+        if (e.stage_ev) ECK(cudaEventSynchronize(e.stage_ev));
+        if (host.size() > e.stage_cap) {
+            if (e.h_stage) cudaFreeHost(e.h_stage);
+            e.h_stage = nullptr;
+            e.stage_cap = 0;
+            const size_t cap = host.size() + host.size() / 2;
+            if (cudaMallocHost(&e.h_stage, cap) != cudaSuccess)
+                return efail(e, TBS_ERR_NOMEM, "pinned staging allocation failed");
+            e.stage_cap = cap;
+        }
+        std::memcpy(e.h_stage, host.data(), host.size());
+        for (auto &j : jobs)
+            ECK(cudaMemcpyAsync(j.first, e.h_stage + j.second.first, j.second.second,
+                                cudaMemcpyHostToDevice, e.stream));
+        if (!e.stage_ev) ECK(cudaEventCreateWithFlags(&e.stage_ev, cudaEventDisableTiming));
+        ECK(cudaEventRecord(e.stage_ev, e.stream));
+        return TBS_OK;
+    }
+};
+
 static cudaEvent_t eprof_event(Engine &e) {
     if (!e.pool.empty()) {
         cudaEvent_t ev = e.pool.back();
@@ -194,12 +235,17 @@ void engine_free(Engine &e) {
     e.pool.clear();
     if (e.h_ctl) cudaFreeHost(e.h_ctl);
     if (e.h_status) cudaFreeHost(e.h_status);
+    if (e.h_stage) cudaFreeHost(e.h_stage);
+    if (e.stage_ev) cudaEventDestroy(e.stage_ev);
     e.h_ctl = nullptr;
     e.h_status = nullptr;
+    e.h_stage = nullptr;
+    e.stage_cap = 0;
+    e.stage_ev = nullptr;
 }
 
 /* grow the capacity-sized arrays (never shrinks); growth invalidates the graph */
-static int ensure_capacity(Engine &e, int nmem, int nlines, int ntiles, int nblocks) {
+static int ensure_capacity(Engine &e, int nmem, int nlines) {
     auto grow = [](int need, int have) { return need <= have ? have : std::max(need, have + have / 2); };
     int rc = TBS_OK;
     if (nmem > e.cap_mem) {
@@ -215,6 +261,9 @@ static int ensure_capacity(Engine &e, int nmem, int nlines, int ntiles, int nblo
         efree(e, &e.d_red_prime);
         efree(e, &e.d_red_body);
         efree(e, &e.d_active);
+        efree(e, &e.d_g_tiles);
+        efree(e, &e.d_g_prime);
+        efree(e, &e.d_g_blocks);
         if (e.algo == TBS_ALGO_FP64) {
             if (!rc) rc = ealloc(e, &e.d_th64, c);
             if (!rc) rc = ealloc(e, &e.d_rs_prime, c);
@@ -229,6 +278,10 @@ static int ensure_capacity(Engine &e, int nmem, int nlines, int ntiles, int nblo
         if (!rc) rc = ealloc(e, &e.d_red_prime, c);
         if (!rc) rc = ealloc(e, &e.d_red_body, c);
         if (!rc) rc = ealloc(e, &e.d_active, c);
+        const size_t gi = group_index_ints(c, c);
+        if (!rc) rc = ealloc(e, &e.d_g_tiles, gi);
+        if (!rc) rc = ealloc(e, &e.d_g_prime, gi);
+        if (!rc) rc = ealloc(e, &e.d_g_blocks, gi);
         e.cap_mem = rc ? 0 : c;
         engine_drop_graph(e);
     }
@@ -239,49 +292,73 @@ static int ensure_capacity(Engine &e, int nmem, int nlines, int ntiles, int nblo
         e.cap_lines = rc ? 0 : c;
         engine_drop_graph(e);
     }
-    if (!rc && ntiles > e.cap_tiles) {
-        const int c = grow(ntiles, e.cap_tiles);
-        efree(e, &e.d_tiles);
-        efree(e, &e.d_prime_tiles);
-        rc = ealloc(e, &e.d_tiles, c);
-        if (!rc) rc = ealloc(e, &e.d_prime_tiles, c);
-        e.cap_tiles = rc ? 0 : c;
-        engine_drop_graph(e);
-    }
-    if (!rc && nblocks > e.cap_blocks) {
-        const int c = grow(nblocks, e.cap_blocks);
-        efree(e, &e.d_blocks);
-        rc = ealloc(e, &e.d_blocks, c);
-        e.cap_blocks = rc ? 0 : c;
-        engine_drop_graph(e);
-    }
     return rc;
 }
 
-/* Thomas items in the engine's order.  Longest lines first; items of the
- * same line of the same system (several right-hand sides) are adjacent, so
- * that warps running them together share the line's blocks in L2. */
-static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Member> &m) {
-    std::vector<WorkItem> items;
-    std::vector<int> sys_rank(m.size());
+/* members grouped by system, in order of first appearance */
+static std::vector<std::vector<int>> group_members(const std::vector<Member> &m,
+                                                   const std::vector<char> &take) {
+    std::vector<std::vector<int>> g;
+    std::vector<const tbs_ctx *> key;
     for (size_t k = 0; k < m.size(); ++k) {
-        sys_rank[k] = (int)k;
-        for (size_t j = 0; j < k; ++j)
-            if (m[j].sys == m[k].sys) {
-                sys_rank[k] = sys_rank[j];
-                break;
-            }
+        if (!take[k]) continue;
+        size_t j = 0;
+        while (j < key.size() && key[j] != m[k].sys) ++j;
+        if (j == key.size()) {
+            key.push_back(m[k].sys);
+            g.emplace_back();
+        }
+        g[j].push_back((int)k);
     }
-    for (size_t k = 0; k < m.size(); ++k)
-        for (int l = 0; l < m[k].sys->nline; ++l) items.push_back({(int)k, l});
+    return g;
+}
+
+/* host image of a group index (layout in tbs_internal.hxx) */
+static std::vector<int> group_index(const std::vector<std::vector<int>> &g,
+                                    const std::vector<int> &units_per_group) {
+    const int ng = (int)g.size();
+    std::vector<int> v;
+    v.push_back(ng);
+    long long base = 0;
+    for (int j = 0; j < ng; ++j) {
+        v.push_back((int)base);
+        base += (long long)units_per_group[j] * (long long)g[j].size();
+    }
+    v.push_back((int)base);
+    for (int j = 0; j < ng; ++j) v.push_back((int)g[j].size());
+    int off = 0;
+    for (int j = 0; j < ng; ++j) {
+        v.push_back(off);
+        off += (int)g[j].size();
+    }
+    for (int j = 0; j < ng; ++j)
+        for (int k : g[j]) v.push_back(k);
+    return v;
+}
+
+/* Thomas items in the engine's order.  Longest lines first; the items of
+ * one line of one system (several right-hand sides) are adjacent, so that
+ * the warps running them together share the line's blocks in L2. */
+static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Member> &m) {
+    std::vector<char> all(m.size(), 1);
+    const std::vector<std::vector<int>> g = group_members(m, all);
+    struct GL {
+        int len, group, line;
+    };
+    std::vector<GL> gl;
+    for (size_t j = 0; j < g.size(); ++j) {
+        const tbs_ctx *c = m[g[j][0]].sys;
+        for (int l = 0; l < c->nline; ++l) gl.push_back({c->h_linesize[l], (int)j, l});
+    }
+    if (e.order == 0)
+        std::stable_sort(gl.begin(), gl.end(), [](const GL &a, const GL &b) { return a.len > b.len; });
+    std::vector<WorkItem> items;
     if (e.order == 0) {
-        std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
-            const int la = m[a.sys].sys->h_linesize[a.unit], lb = m[b.sys].sys->h_linesize[b.unit];
-            if (la != lb) return la > lb;
-            if (sys_rank[a.sys] != sys_rank[b.sys]) return sys_rank[a.sys] < sys_rank[b.sys];
-            if (a.unit != b.unit) return a.unit < b.unit;
-            return a.sys < b.sys;
-        });
+        for (const GL &x : gl)
+            for (int k : g[x.group]) items.push_back({k, x.line});
+    } else {
+        for (size_t k = 0; k < m.size(); ++k)
+            for (int l = 0; l < m[k].sys->nline; ++l) items.push_back({(int)k, l});
     }
     return items;
 }
@@ -298,14 +375,13 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         if (mixed) nblocks += full_resid_blocks(m.sys->nelem);
     }
     if (nlines > 0x7fffffff || ntiles > 0x7fffffff || nblocks > 0x7fffffff)
-        return efail(e, TBS_ERR_UNSUPPORTED, "batch too large for int32 work lists");
+        return efail(e, TBS_ERR_UNSUPPORTED, "batch too large for int32 work indices");
     if (nx > e.max_nx) {
         if (batch_prepare(nx)) return efail(e, TBS_ERR_CUDA, "shared-memory opt-in failed");
         e.max_nx = nx;
         engine_drop_graph(e);
     }
-    int rc = ensure_capacity(e, std::max(n, 1), (int)std::max(nlines, 1LL), (int)std::max(ntiles, 1LL),
-                             (int)std::max(nblocks, 1LL));
+    int rc = ensure_capacity(e, std::max(n, 1), (int)std::max(nlines, 1LL));
     if (rc) return rc;
 
     std::vector<ThomasSys<double>> th64;
@@ -315,8 +391,8 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
     std::vector<FullResSys> fr;
     std::vector<VecSys> vec;
     std::vector<ReduceSys> redp, redb;
-    std::vector<WorkItem> tiles, prime_tiles, blocks;
     std::vector<int> uinit;
+    std::vector<char> all(n, 1), prime(n, 0);
     e.h_active.assign(n, 0);
     for (int k = 0; k < n; ++k) {
         const Member &m = members[k];
@@ -346,11 +422,8 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
             vec.push_back({v.rhsp, v.R32, v.c32, v.d32, v.Up, v.partials});
             if (m.fresh) redp.push_back({v.partials, ui ? full_resid_blocks(c->nelem) : nt, k, v.state, v.hist});
             redb.push_back({v.partials, full_resid_blocks(c->nelem), k, v.state, v.hist});
-            for (int b = 0; b < full_resid_blocks(c->nelem); ++b) blocks.push_back({k, b});
         }
-        for (int t = 0; t < nt; ++t) tiles.push_back({k, t});
-        if (m.fresh && !(mixed && ui))
-            for (int t = 0; t < nt; ++t) prime_tiles.push_back({k, t});
+        prime[k] = m.fresh && !(mixed && ui);
         if (ui) uinit.push_back(k);
         e.h_active[k] = m.fresh ? 0 : 1;
     }
@@ -358,55 +431,49 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         e.uinit = uinit;
         engine_drop_graph(e);
     }
-    /* residual tiles and element blocks of right-hand sides of the same
-     * system next to each other (system, unit, member), so that CTAs that
-     * run them together share the blocks in L2 */
-    std::vector<int> sys_rank(n);
-    for (int k = 0; k < n; ++k) {
-        sys_rank[k] = k;
-        for (int j = 0; j < k; ++j)
-            if (members[j].sys == members[k].sys) {
-                sys_rank[k] = sys_rank[j];
-                break;
-            }
-    }
-    auto by_unit = [&](const WorkItem &a, const WorkItem &b) {
-        if (sys_rank[a.sys] != sys_rank[b.sys]) return sys_rank[a.sys] < sys_rank[b.sys];
-        if (a.unit != b.unit) return a.unit < b.unit;
-        return a.sys < b.sys;
+    /* group indices of the residual-type launches */
+    auto units = [&](const std::vector<std::vector<int>> &g, bool blocks) {
+        std::vector<int> u;
+        for (const auto &grp : g) {
+            const tbs_ctx *c = members[grp[0]].sys;
+            u.push_back(blocks ? full_resid_blocks(c->nelem) : fast_resid_grid(c->L.np16));
+        }
+        return u;
     };
-    std::stable_sort(tiles.begin(), tiles.end(), by_unit);
-    std::stable_sort(prime_tiles.begin(), prime_tiles.end(), by_unit);
-    std::stable_sort(blocks.begin(), blocks.end(), by_unit);
+    const auto g_all = group_members(members, all);
+    const auto g_prime = group_members(members, prime);
+    const std::vector<int> gi_tiles = group_index(g_all, units(g_all, false));
+    const std::vector<int> gi_prime = group_index(g_prime, units(g_prime, false));
     e.members = members;
     std::vector<WorkItem> lines = line_items(e, members);
+    Stager up(e);
     if (!mixed) {
-        if (!rc) rc = eupload(e, e.d_th64, th64);
-        if (!rc) rc = eupload(e, e.d_rs_prime, rsp);
-        if (!rc) rc = eupload(e, e.d_rs_body, rsb);
+        up.put(e.d_th64, th64);
+        up.put(e.d_rs_prime, rsp);
+        up.put(e.d_rs_body, rsb);
     } else {
-        if (!rc) rc = eupload(e, e.d_th32, th32);
-        if (!rc) rc = eupload(e, e.d_rs32_rhs, rs32r);
-        if (!rc) rc = eupload(e, e.d_rs32_dx, rs32d);
-        if (!rc) rc = eupload(e, e.d_fr, fr);
-        if (!rc) rc = eupload(e, e.d_vec, vec);
-        if (!rc) rc = eupload(e, e.d_blocks, blocks);
+        up.put(e.d_th32, th32);
+        up.put(e.d_rs32_rhs, rs32r);
+        up.put(e.d_rs32_dx, rs32d);
+        up.put(e.d_fr, fr);
+        up.put(e.d_vec, vec);
+        up.put(e.d_g_blocks, group_index(g_all, units(g_all, true)));
     }
-    if (!rc) rc = eupload(e, e.d_red_prime, redp);
-    if (!rc) rc = eupload(e, e.d_red_body, redb);
-    if (!rc) rc = eupload(e, e.d_lines, lines);
-    if (!rc) rc = eupload(e, e.d_tiles, tiles);
-    if (!rc) rc = eupload(e, e.d_prime_tiles, prime_tiles);
-    if (!rc) rc = eupload(e, e.d_active, e.h_active);
+    up.put(e.d_red_prime, redp);
+    up.put(e.d_red_body, redb);
+    up.put(e.d_lines, lines);
+    up.put(e.d_g_tiles, gi_tiles);
+    up.put(e.d_g_prime, gi_prime);
+    up.put(e.d_active, e.h_active);
+    rc = up.flush();
     if (rc) return rc;
     BatchCtl &C = *e.h_ctl;
     C.nsys = n;
     C.nlines = (int)lines.size();
-    C.ntiles = (int)tiles.size();
-    C.nblocks = (int)blocks.size();
+    C.ntiles = gi_tiles[1 + gi_tiles[0]];
+    C.nblocks = (int)nblocks;
     C.nprime_sys = (int)redp.size();
-    C.nprime_tiles = (int)prime_tiles.size();
-    ECK(cudaStreamSynchronize(e.stream));
+    C.nprime_tiles = gi_prime[1 + gi_prime[0]];
     return TBS_OK;
 }
 
@@ -419,16 +486,19 @@ int engine_restart(Engine &e) {
         return engine_set_members(e, m);
     }
     std::fill(e.h_active.begin(), e.h_active.end(), 0);
-    int rc = eupload(e, e.d_active, e.h_active);
-    if (rc) return rc;
-    ECK(cudaStreamSynchronize(e.stream));
-    return TBS_OK;
+    Stager up(e);
+    up.put(e.d_active, e.h_active);
+    return up.flush();
 }
 
 void engine_mark_started(Engine &e) {
     for (Member &m : e.members) m.fresh = false;
     e.h_ctl->nprime_sys = 0;
     e.h_ctl->nprime_tiles = 0;
+    /* an empty prime group index (the count is read from it on the device) */
+    Stager up(e);
+    up.put(e.d_g_prime, std::vector<int>{0, 0});
+    up.flush();
 }
 
 struct Cond {
@@ -455,12 +525,12 @@ static int engine_prime(Engine &e, Cond cc) {
     }
     BatchCtl *C = e.d_ctl;
     if (e.algo == TBS_ALGO_FP64) {
-        ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_prime_tiles,
-                                                          &C->nprime_tiles, nullptr, e.d_status));
+        ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_g_prime,
+                                                          nullptr, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use));
     } else {
-        ERUN("mixed_prime", launch_mixed_prime_batch(st, e.d_vec, e.d_prime_tiles, &C->nprime_tiles));
+        ERUN("mixed_prime", launch_mixed_prime_batch(st, e.d_vec, e.d_g_prime));
         ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use));
     }
@@ -473,8 +543,8 @@ static int engine_body(Engine &e, Cond cc) {
     if (e.algo == TBS_ALGO_FP64) {
         ERUN("fast_thomas", launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines, &C->nlines,
                                                         e.d_active, e.d_queue, e.d_status));
-        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_tiles,
-                                                      &C->ntiles, e.d_active, e.d_status));
+        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_tiles,
+                                                      e.d_active, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_body, &C->nsys, e.cap_mem, 0,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use));
         return TBS_OK;
@@ -482,17 +552,17 @@ static int engine_body(Engine &e, Cond cc) {
     /* c (the sum of the inner updates but the last) is cleared by the first
      * launch, each inner residual adds its sweep's d to it, and the last d
      * goes to U with c (the order of the single-system sequence) */
-    ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_tiles,
-                                                       &C->ntiles, e.d_active, e.d_status));
+    ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_g_tiles,
+                                                       e.d_active, e.d_status));
     for (int m = 0; m < e.inner; ++m) {
         ERUN("fast_thomas32", launch_thomas_batch<float>(st, e.sched, e.d_th32, e.d_lines, &C->nlines,
                                                          e.d_active, e.d_queue, e.d_status));
         if (m + 1 < e.inner)
-            ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_tiles,
-                                                           &C->ntiles, e.d_active, e.d_status));
+            ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_g_tiles,
+                                                           e.d_active, e.d_status));
     }
-    ERUN("axpy", launch_axpy2_batch(st, e.d_vec, e.d_tiles, &C->ntiles, e.d_active));
-    ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_blocks, &C->nblocks, e.d_active));
+    ERUN("axpy", launch_axpy2_batch(st, e.d_vec, e.d_g_tiles, e.d_active));
+    ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_g_blocks, e.d_active));
     ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_body, &C->nsys, e.cap_mem, 0, e.d_active,
                                             C, e.d_counter, cc.handle, cc.use));
     return TBS_OK;
@@ -617,6 +687,24 @@ int engine_run(Engine &e, int chunk_limit, int stop_on_finish) {
     }
     return engine_status(e);
 }
+
+int engine_launch(Engine &e, int chunk_limit, int stop_on_finish) {
+    if (e.prof) return engine_run(e, chunk_limit, stop_on_finish);
+    BatchCtl &C = *e.h_ctl;
+    C.chunk = 0;
+    C.finished = 0;
+    C.chunk_limit = chunk_limit;
+    C.stop_on_finish = stop_on_finish;
+    ECK(cudaMemcpyAsync(e.d_ctl, e.h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, e.stream));
+    if (!e.graph_ok) {
+        int rc = engine_build_graph(e);
+        if (rc) return rc;
+    }
+    ECK(cudaGraphLaunch(e.gexec, e.stream));
+    return TBS_OK;
+}
+
+int engine_finish(Engine &e) { return engine_status(e); }
 
 static int engine_upload_lines(Engine &e) {
     std::vector<WorkItem> lines = line_items(e, e.members);

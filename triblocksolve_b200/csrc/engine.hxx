@@ -56,7 +56,7 @@ struct Engine {
     std::string err;
 
     /* capacity-sized device arrays (reallocated, and the graph rebuilt, on growth) */
-    int cap_mem = 0, cap_lines = 0, cap_tiles = 0, cap_blocks = 0;
+    int cap_mem = 0, cap_lines = 0;
     std::vector<void *> allocs;
     ThomasSys<double> *d_th64 = nullptr;
     ThomasSys<float> *d_th32 = nullptr;
@@ -65,14 +65,19 @@ struct Engine {
     FullResSys *d_fr = nullptr;
     VecSys *d_vec = nullptr;
     ReduceSys *d_red_prime = nullptr, *d_red_body = nullptr;
-    WorkItem *d_lines = nullptr, *d_tiles = nullptr, *d_prime_tiles = nullptr,
-             *d_blocks = nullptr;
+    WorkItem *d_lines = nullptr;                       /* Thomas items, explicit */
+    int *d_g_tiles = nullptr, *d_g_prime = nullptr, *d_g_blocks = nullptr; /* group indices */
     int *d_active = nullptr;
     unsigned *d_queue = nullptr, *d_counter = nullptr, *d_status = nullptr;
     BatchCtl *d_ctl = nullptr;
     BatchCtl *h_ctl = nullptr;     /* pinned */
     unsigned *h_status = nullptr;  /* pinned */
     std::vector<int> h_active;
+    /* pinned staging of the descriptor and work-list uploads, so that they
+     * never synchronise with the stream; reused once stage_ev has passed */
+    char *h_stage = nullptr;
+    size_t stage_cap = 0;
+    cudaEvent_t stage_ev = nullptr;
 
     /* the members of the last engine_set_members */
     std::vector<Member> members;
@@ -105,6 +110,10 @@ void engine_mark_started(Engine &e);
  * chunk_limit > 0 ends the sweep loop after that many sweeps, and
  * stop_on_finish ends it as soon as a member stops */
 int engine_run(Engine &e, int chunk_limit, int stop_on_finish);
+/* the same as an asynchronous graph launch (engine_finish waits for it and
+ * checks the device status); while profiling it runs engine_run */
+int engine_launch(Engine &e, int chunk_limit, int stop_on_finish);
+int engine_finish(Engine &e);
 /* times the persistent Thomas launch for each schedule that fits */
 int engine_tune(Engine &e, BatchSched *best, int *best_order, double *best_ms);
 int engine_set_schedule(Engine &e, BatchSched s, int order);

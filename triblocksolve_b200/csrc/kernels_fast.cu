@@ -1544,6 +1544,24 @@ int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp,
  * of members; all but the per-member norm kernel are persistent, with grids
  * sized to the SMs. */
 
+/* Item w of a group index (layout in tbs_internal.hxx): the group by
+ * binary search over the prefix sums, then unit-major within the group. */
+__device__ __forceinline__ WorkItem group_item(const int *__restrict__ gi, int w) {
+    const int ng = gi[0];
+    const int *base = gi + 1;
+    int lo = 0, hi = ng - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    const int *nmem = base + ng + 1, *moff = nmem + ng, *mlist = moff + ng;
+    const int off = w - base[lo], r = nmem[lo];
+    return WorkItem{mlist[moff[lo] + off % r], off / r};
+}
+
+__device__ __forceinline__ int group_items(const int *__restrict__ gi) { return gi[1 + gi[0]]; }
+
 static int sm_count() {
     int dev = 0, n = 0;
     cudaGetDevice(&dev);
@@ -1585,13 +1603,13 @@ int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T
  * k + grid, ...; each tile completes one phase of the CTA's barrier */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_batch_kernel(
-    const ResidSys<T> *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ nwork_p, int mode, const int *__restrict__ active, unsigned *status) {
+    const ResidSys<T> *__restrict__ sys, const int *__restrict__ groups, int mode,
+    const int *__restrict__ active, unsigned *status) {
     uint64_t *bar = resid_bar_init();
-    const int nwork = *nwork_p;
+    const int nwork = group_items(groups);
     uint32_t parity = 0;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = work[w];
+        const WorkItem it = group_item(groups, w);
         if (active && !active[it.sys]) continue;
         const ResidSys<T> S = sys[it.sys];
         NormSink ns{};
@@ -1615,21 +1633,21 @@ static int resid_batch_grid(size_t smem, const void *fn) {
 
 template <typename T>
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const WorkItem *work, const int *nwork, const int *active, unsigned *status) {
+                       const int *groups, const int *active, unsigned *status) {
     if (mode != 0 && mode != 1 && mode != 3) return (int)cudaErrorInvalidValue;
     const size_t smem = resid_smem_bytes<T>(mode == 0 ? 0 : max_nx);
     const int grid = resid_batch_grid(smem, (const void *)fast_resid_batch_kernel<T>);
-    fast_resid_batch_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(sys, work, nwork, mode, active,
+    fast_resid_batch_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, mode, active,
                                                                      status);
     return (int)cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(FULLRES_THREADS) full_resid_batch_kernel(
-    const FullResSys *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ nwork_p, const int *__restrict__ active) {
-    const int nwork = *nwork_p;
+    const FullResSys *__restrict__ sys, const int *__restrict__ groups,
+    const int *__restrict__ active) {
+    const int nwork = group_items(groups);
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = work[w];
+        const WorkItem it = group_item(groups, w);
         if (active && !active[it.sys]) continue;
         const FullResSys S = sys[it.sys];
         full_resid_body<float>(S.nelem, S.epoint, S.ef, S.fc, S.pos_of_elem, S.D, S.O1, S.O2,
@@ -1645,39 +1663,37 @@ static int plain_batch_grid(const void *fn, int threads) {
     return per * sm_count();
 }
 
-int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work,
-                            const int *nwork, const int *active) {
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *groups,
+                            const int *active) {
     const int grid = plain_batch_grid((const void *)full_resid_batch_kernel, FULLRES_THREADS);
-    full_resid_batch_kernel<<<grid, FULLRES_THREADS, 0, st>>>(sys, work, nwork, active);
+    full_resid_batch_kernel<<<grid, FULLRES_THREADS, 0, st>>>(sys, groups, active);
     return (int)cudaGetLastError();
 }
 
 __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_batch_kernel(
-    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ nwork_p) {
-    const int nwork = *nwork_p;
+    const VecSys *__restrict__ sys, const int *__restrict__ groups) {
+    const int nwork = group_items(groups);
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = work[w];
+        const WorkItem it = group_item(groups, w);
         const VecSys S = sys[it.sys];
         mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, it.unit);
         __syncthreads();
     }
 }
 
-int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work,
-                             const int *nwork) {
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const int *groups) {
     const int grid = plain_batch_grid((const void *)mixed_prime_batch_kernel, RES_THREADS_FAST);
-    mixed_prime_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, work, nwork);
+    mixed_prime_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, groups);
     return (int)cudaGetLastError();
 }
 
 /* U += c + d over one tile (elementwise: the same values as axpy2_kernel) */
 __global__ void __launch_bounds__(RES_THREADS_FAST) axpy2_batch_kernel(
-    const VecSys *__restrict__ sys, const WorkItem *__restrict__ work,
-    const int *__restrict__ nwork_p, const int *__restrict__ active) {
-    const int nwork = *nwork_p;
+    const VecSys *__restrict__ sys, const int *__restrict__ groups,
+    const int *__restrict__ active) {
+    const int nwork = group_items(groups);
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = work[w];
+        const WorkItem it = group_item(groups, w);
         if (active && !active[it.sys]) continue;
         if (threadIdx.x >= RES_TILE * NV) continue;
         const VecSys S = sys[it.sys];
@@ -1686,10 +1702,9 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) axpy2_batch_kernel(
     }
 }
 
-int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, const int *nwork,
-                       const int *active) {
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, const int *active) {
     const int grid = plain_batch_grid((const void *)axpy2_batch_kernel, RES_THREADS_FAST);
-    axpy2_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, work, nwork, active);
+    axpy2_batch_kernel<<<grid, RES_THREADS_FAST, 0, st>>>(sys, groups, active);
     return (int)cudaGetLastError();
 }
 
@@ -1782,8 +1797,8 @@ template int launch_thomas_batch<float>(cudaStream_t, const BatchSched &, const 
                                         const WorkItem *, const int *, const int *, unsigned *,
                                         unsigned *);
 template int launch_resid_batch<double>(cudaStream_t, int, int, const ResidSys<double> *,
-                                        const WorkItem *, const int *, const int *, unsigned *);
+                                        const int *, const int *, unsigned *);
 template int launch_resid_batch<float>(cudaStream_t, int, int, const ResidSys<float> *,
-                                       const WorkItem *, const int *, const int *, unsigned *);
+                                       const int *, const int *, unsigned *);
 
 }  // namespace tbs

@@ -16,10 +16,11 @@
  *   - retires each right-hand side as soon as it stops and completes a
  *     request when all of its right-hand sides have.
  * A second thread re-factors systems (upload of the new values and the
- * factorization on the system's own stream) while the loop keeps sweeping
- * the other systems' right-hand sides; a system is re-factored only when
- * none of its right-hand sides is in flight, and its later requests wait
- * for the new factors.
+ * factorization on the system's own stream) into a spare copy of the
+ * system's factors, so that the right-hand sides already admitted keep
+ * sweeping on the current copy; the system's later requests wait for the
+ * new factors.  When the spare copy does not fit the budget, the system is
+ * re-factored in place once none of its right-hand sides is in flight.
  *
  * The per-right-hand-side arithmetic is that of tbs_solve: a result does
  * not depend on what else was in flight.
@@ -52,16 +53,24 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 }
 
 struct SrvSystem {
-    tbs_ctx *ctx = nullptr;
-    int inflight = 0;       /* right-hand sides in flight */
+    /* two versions of the system's factors: new Jacobian values are
+     * uploaded and factored into the spare while the right-hand sides
+     * already admitted keep sweeping on the current one */
+    tbs_ctx *ctx[2] = {nullptr, nullptr};
+    int cur = 0;
+    int inflight[2] = {0, 0}; /* right-hand sides in flight per version */
     bool refactoring = false;
-    bool broken = false;    /* a re-factorization failed: its requests fail */
+    bool broken = false;      /* an in-place re-factorization failed */
+    size_t bytes = 0;         /* device bytes of one version */
 };
 
 struct SrvRequest {
     long long id = 0;
     int sys = 0;
-    tbs_ctx *ctx = nullptr;      /* the system's context (stable while the server lives) */
+    int ver = 0;                 /* the system version it runs on (set at admission) */
+    int target = 0;              /* the version a re-factorization writes */
+    bool new_version = false;    /* that version's context is created by the factor thread */
+    tbs_ctx *ctx = nullptr;      /* the version's context (stable while the server lives) */
     int nrhs = 0;
     const double *rhs = nullptr; /* caller's: nrhs x 9 nelem, valid until completion */
     double *U = nullptr;         /* caller's output */
@@ -112,14 +121,36 @@ struct tbs_server {
 
     /* loop-thread state */
     Engine eng;
-    cudaStream_t stream = nullptr;
+    cudaStream_t stream = nullptr;     /* graph launches */
+    cudaStream_t up = nullptr;         /* uploads of admitted right-hand sides */
+    cudaStream_t down = nullptr;       /* read-back of finished solutions */
     cudaMemPool_t pool = nullptr;
-    std::vector<SrvSlot> slots;
+    bool pool_reserved = false;
+    std::vector<SrvSlot> slots;        /* members of the engine */
+    struct Incoming {                  /* uploads issued, not yet members */
+        std::vector<SrvSlot> slots;
+        cudaEvent_t ev;                /* their uploads are done */
+    };
+    std::deque<Incoming> incoming;
+    cudaEvent_t ev_up = nullptr;       /* the last batch of uploads is done */
+    struct Pending {
+        std::vector<SrvSlot> slots;
+        std::vector<SolveState> st;
+        cudaEvent_t ev;
+    };
+    std::deque<Pending> pending;       /* read-backs in flight */
+    std::vector<cudaEvent_t> ev_pool;
+    SolveState *h_states = nullptr;    /* pinned, max_slots: read-back of states */
+    SolveState *h_up_states = nullptr; /* pinned, max_slots: states of admitted ones */
     std::thread loop, factor;
 
     /* statistics */
     long long n_done = 0, n_rhs_done = 0, n_launches = 0, n_refactor = 0;
     long long peak_rhs = 0, peak_bytes = 0;
+    /* loop-thread time (microseconds): starting admitted right-hand sides
+     * (clear, upload, permute), rebuilding the member set, graph launches
+     * until they return, retiring (read-back) */
+    double us_start = 0, us_members = 0, us_run = 0, us_retire = 0;
 };
 
 static int sfail(tbs_server *s, int code, const std::string &msg) {
@@ -208,22 +239,43 @@ static void factor_main(tbs_server *s) {
         }
         SrvRequest *r = s->factor_jobs.front();
         s->factor_jobs.pop_front();
-        tbs_ctx *c = r->ctx;
+        tbs_ctx *c = s->systems[r->sys].ctx[r->target];
+        const tbs_ctx *model = s->systems[r->sys].ctx[s->systems[r->sys].cur];
+        const bool fresh = r->new_version;
         lk.unlock();
-        int rc = tbs_set_jacobian(c, r->jacD, r->jacO1, r->jacO2, r->rhs, nullptr);
+        int rc = TBS_OK;
+        if (fresh) {
+            /* the spare version: same mesh as the current one */
+            rc = tbs_create(s->device, &c);
+            if (!rc)
+                rc = tbs_set_mesh(c, model->nvar, model->nelem, model->nintface, model->eftot,
+                                  model->nline, model->nlineelem, model->h_epoint.data(),
+                                  model->h_ef.data(), model->h_fc.data(), model->h_linesize.data(),
+                                  model->h_linepoint.data(), model->h_lines.data(),
+                                  model->h_lineface.data());
+        }
+        if (!rc) rc = tbs_set_jacobian(c, r->jacD, r->jacO1, r->jacO2, r->rhs, nullptr);
         if (!rc) rc = tbs_factor(c, s->algo);
-        std::string msg = rc ? std::string(tbs_last_error(c)) : std::string();
+        std::string msg = rc ? std::string(c ? tbs_last_error(c) : thread_error()) : std::string();
         lk.lock();
-        s->systems[r->sys].refactoring = false;
+        SrvSystem &sys = s->systems[r->sys]; /* re-read: systems may have been added */
+        sys.refactoring = false;
         s->n_refactor += 1;
         if (rc) {
-            /* the request fails, and so do the system's later requests: its
-             * factors may be half replaced */
-            s->systems[r->sys].broken = true;
+            if (fresh) {
+                /* the current version is untouched: only this request fails */
+                if (c) tbs_destroy(c);
+                s->sys_bytes -= sys.bytes;
+            } else if (r->target == sys.cur) {
+                /* in place: the factors may be half replaced */
+                sys.broken = true;
+            }
             complete(s, r, rc, "re-factorization failed: " + msg);
             s->queue.erase(std::find(s->queue.begin(), s->queue.end(), r));
             s->cv_done.notify_all();
         } else {
+            if (fresh) sys.ctx[r->target] = c;
+            sys.cur = r->target;
             r->refactored = true;
             r->state = SrvRequest::QUEUED;
         }
@@ -255,8 +307,17 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
             continue;
         }
         if (r->jacD && !r->refactored) {
-            if (sys.inflight == 0) {
+            /* into the spare version while the current one keeps sweeping;
+             * in place (after the system drains) when a spare does not fit */
+            const int spare = 1 - sys.cur;
+            const bool have = sys.ctx[spare] != nullptr;
+            const bool fits = have || s->sys_bytes + sys.bytes + s->slot_bytes_in_flight <= s->budget;
+            const int target = fits ? spare : sys.cur;
+            if (sys.inflight[target] == 0) {
                 sys.refactoring = true;
+                r->target = target;
+                r->new_version = fits && !have;
+                if (r->new_version) s->sys_bytes += sys.bytes;
                 r->state = SrvRequest::FACTORING;
                 s->factor_jobs.push_back(r);
                 s->cv_factor.notify_all();
@@ -268,11 +329,14 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
         const int in_flight = (int)s->slots.size() + [&] {
             int n = 0;
             for (SrvRequest *a : admitted) n += a->nrhs;
+            for (const tbs_server::Incoming &in : s->incoming) n += (int)in.slots.size();
             return n;
         }();
         if (in_flight + r->nrhs > s->max_slots || s->slot_bytes_in_flight + r->bytes > avail) break;
         s->slot_bytes_in_flight += r->bytes;
-        sys.inflight += r->nrhs;
+        r->ver = sys.cur;
+        r->ctx = sys.ctx[sys.cur];
+        sys.inflight[r->ver] += r->nrhs;
         r->state = SrvRequest::RUNNING;
         r->t_admit = Clock::now();
         admitted.push_back(r);
@@ -280,9 +344,42 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
     }
 }
 
-/* allocate and fill the right-hand sides of newly admitted requests */
+/* Keep freed right-hand-side memory in the pool and grow it once to the
+ * room the budget leaves after the resident systems, so that admissions do
+ * not pay for mapping new device memory. */
+static void reserve_pool(tbs_server *s, size_t avail) {
+    if (s->pool_reserved || avail == 0) return;
+    s->pool_reserved = true;
+    void *p = nullptr;
+    if (cudaMallocFromPoolAsync(&p, avail, s->pool, s->up) == cudaSuccess) {
+        cudaFreeAsync(p, s->up);
+        cudaStreamSynchronize(s->up);
+    } else {
+        cudaGetLastError(); /* not fatal: the pool then grows on demand */
+    }
+}
+
+static cudaEvent_t take_event(tbs_server *s) {
+    if (!s->ev_pool.empty()) {
+        cudaEvent_t e = s->ev_pool.back();
+        s->ev_pool.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+    return e;
+}
+
+/* allocate, clear and fill the right-hand sides of newly admitted requests
+ * on the upload stream (overlapping the running graph); they become engine
+ * members at the next member update, after ev_up */
 static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitted,
                           std::vector<SrvRequest *> &failed) {
+    if (admitted.empty()) return TBS_OK;
+    /* the staging of the previous uploads is free once they have run */
+    if (cudaEventSynchronize(s->ev_up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event failed");
+    int nst = 0;
+    tbs_server::Incoming batch;
     for (SrvRequest *r : admitted) {
         tbs_ctx *c = r->ctx;
         const size_t nv = (size_t)c->nelem * 9;
@@ -294,40 +391,42 @@ static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitt
             sl.req = r;
             sl.k = k;
             sl.bytes = per;
-            if (cudaMallocFromPoolAsync(&sl.mem, per, s->pool, s->stream) != cudaSuccess) {
+            if (cudaMallocFromPoolAsync(&sl.mem, per, s->pool, s->up) != cudaSuccess) {
                 cudaGetLastError();
                 ok = false;
                 break;
             }
-            slot_layout(sl, c, s->algo, r->max_sweeps + 1);
+            mine.push_back(sl);
+            SrvSlot &m = mine.back();
+            slot_layout(m, c, s->algo, r->max_sweeps + 1);
             /* pad positions of the layout are never written by the kernels
              * but enter the first norm (rhs) and the U accumulation: start
              * from zeros, as a context's arrays do */
-            if (cudaMemsetAsync(sl.mem, 0, per, s->stream) != cudaSuccess) {
-                mine.push_back(sl);
-                ok = false;
-                break;
-            }
-            SolveState st{};
+            SolveState &st = s->h_up_states[nst++];
+            st = SolveState{};
             st.tol = r->tol;
             st.max_sweeps = r->max_sweeps;
             st.hist_cap = r->max_sweeps + 1;
-            ok = cudaMemcpyAsync(sl.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, s->stream) == cudaSuccess &&
-                 cudaMemcpyAsync(sl.rhs_elem, r->rhs + k * nv, nv * sizeof(double),
-                                 cudaMemcpyHostToDevice, s->stream) == cudaSuccess &&
-                 launch_permute_to_pos(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.rhs_elem,
-                                       sl.v.rhsp) == 0;
-            mine.push_back(sl);
+            ok = cudaMemsetAsync(m.mem, 0, per, s->up) == cudaSuccess &&
+                 cudaMemcpyAsync(m.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, s->up) == cudaSuccess &&
+                 cudaMemcpyAsync(m.rhs_elem, r->rhs + k * nv, nv * sizeof(double),
+                                 cudaMemcpyHostToDevice, s->up) == cudaSuccess &&
+                 launch_permute_to_pos(s->up, 9, c->nelem, c->L.pos_of_elem, m.rhs_elem, m.v.rhsp) == 0;
         }
         if (!ok) {
             for (SrvSlot &sl : mine)
-                if (sl.mem) cudaFreeAsync(sl.mem, s->stream);
+                if (sl.mem) cudaFreeAsync(sl.mem, s->up);
             failed.push_back(r);
             continue;
         }
-        for (SrvSlot &sl : mine) s->slots.push_back(sl);
+        for (SrvSlot &sl : mine) batch.slots.push_back(sl);
     }
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "upload failed");
+    if (cudaEventRecord(s->ev_up, s->up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event record failed");
+    if (!batch.slots.empty()) {
+        batch.ev = take_event(s);
+        if (cudaEventRecord(batch.ev, s->up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event record failed");
+        s->incoming.push_back(std::move(batch));
+    }
     return TBS_OK;
 }
 
@@ -338,38 +437,57 @@ static int engine_members(tbs_server *s) {
     return engine_set_members(s->eng, m);
 }
 
-/* read back the right-hand sides that stopped; returns them in `out` */
-static int retire(tbs_server *s, std::vector<SrvSlot> &out) {
-    std::vector<SrvSlot> keep;
-    std::vector<SolveState> st;
-    for (size_t k = 0; k < s->slots.size(); ++k) {
-        if (s->eng.h_active[k]) {
-            keep.push_back(s->slots[k]);
-            continue;
-        }
-        out.push_back(s->slots[k]);
-    }
+/* the members that stopped: their states now (pinned, main stream), their
+ * solutions permuted to element order on the main stream and copied to the
+ * caller on the read-back stream (overlapping the next graph) */
+static int retire(tbs_server *s) {
+    std::vector<SrvSlot> keep, out;
+    for (size_t k = 0; k < s->slots.size(); ++k)
+        (s->eng.h_active[k] ? keep : out).push_back(s->slots[k]);
     if (out.empty()) return TBS_OK;
-    st.resize(out.size());
     for (size_t k = 0; k < out.size(); ++k) {
         SrvSlot &sl = out[k];
         tbs_ctx *c = sl.req->ctx;
-        const size_t nv = (size_t)c->nelem * 9;
-        if (cudaMemcpyAsync(&st[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost, s->stream) != cudaSuccess ||
-            launch_permute_to_elem(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0 ||
-            cudaMemcpyAsync(sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double),
-                            cudaMemcpyDeviceToHost, s->stream) != cudaSuccess)
+        if (cudaMemcpyAsync(&s->h_states[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost,
+                            s->stream) != cudaSuccess ||
+            launch_permute_to_elem(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0)
             return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
-        cudaFreeAsync(sl.mem, s->stream);
     }
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess)
-        return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
-    for (size_t k = 0; k < out.size(); ++k) {
-        SrvRequest *r = out[k].req;
-        r->sweeps[out[k].k] = st[k].sweep;
-        r->rel[out[k].k] = st[k].norm0 > 0.0 ? st[k].last / st[k].norm0 : 0.0;
+    cudaEvent_t ready = take_event(s);
+    if (cudaEventRecord(ready, s->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(s->down, ready, 0) != cudaSuccess)
+        return sfail(s, TBS_ERR_CUDA, "event failed");
+    s->ev_pool.push_back(ready); /* reusable once recorded work is ordered */
+    tbs_server::Pending p;
+    for (SrvSlot &sl : out) {
+        tbs_ctx *c = sl.req->ctx;
+        const size_t nv = (size_t)c->nelem * 9;
+        if (cudaMemcpyAsync(sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double),
+                            cudaMemcpyDeviceToHost, s->down) != cudaSuccess)
+            return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
+        cudaFreeAsync(sl.mem, s->down);
     }
+    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "state read-back failed");
+    p.st.assign(s->h_states, s->h_states + out.size());
+    p.slots.swap(out);
+    p.ev = take_event(s);
+    if (cudaEventRecord(p.ev, s->down) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event failed");
+    s->pending.push_back(std::move(p));
     s->slots.swap(keep);
+    return TBS_OK;
+}
+
+/* read-backs that finished (all of them when `all`): their requests'
+ * results; called without the lock, returns the finished batches */
+static int collect(tbs_server *s, bool all, std::vector<tbs_server::Pending> &done) {
+    while (!s->pending.empty()) {
+        tbs_server::Pending &p = s->pending.front();
+        if (!all && cudaEventQuery(p.ev) == cudaErrorNotReady) break;
+        if (cudaEventSynchronize(p.ev) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "read-back failed");
+        s->ev_pool.push_back(p.ev);
+        done.push_back(std::move(p));
+        s->pending.pop_front();
+    }
     return TBS_OK;
 }
 
@@ -377,56 +495,110 @@ static void loop_main(tbs_server *s) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        std::vector<SrvRequest *> admitted;
-        admit_scan(s, admitted);
-        if (admitted.empty() && s->slots.empty()) {
-            if (s->stopping && s->queue.empty() && s->factor_jobs.empty()) break;
-            s->cv_loop.wait(lk);
-            continue;
-        }
         const int chunk = s->chunk;
         lk.unlock();
-        std::vector<SrvRequest *> failed;
-        int rc = start_requests(s, admitted, failed);
-        const bool changed = !admitted.empty();
-        if (!rc && changed) rc = engine_members(s);
-        if (!rc) rc = engine_run(s->eng, chunk, 1);
-        if (!rc) rc = engine_read_active(s->eng);
-        std::vector<SrvSlot> done;
-        if (!rc) {
+        auto t0 = Clock::now();
+        /* 1. sweep the members while the host admits and copies */
+        int rc = TBS_OK;
+        const bool running = !s->slots.empty();
+        if (running) rc = engine_launch(s->eng, chunk, 1);
+        /* 2. admission and uploads */
+        std::vector<SrvRequest *> admitted, failed;
+        lk.lock();
+        admit_scan(s, admitted);
+        const size_t avail = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
+        lk.unlock();
+        if (!admitted.empty()) reserve_pool(s, avail);
+        auto t1 = Clock::now();
+        if (!rc) rc = start_requests(s, admitted, failed);
+        /* 3. solutions that reached the caller */
+        std::vector<tbs_server::Pending> copied;
+        if (!rc) rc = collect(s, true, copied);
+        auto t2 = Clock::now();
+        /* 4. the sweeps' end: retire the members that stopped */
+        if (running && !rc) rc = engine_finish(s->eng);
+        if (running && !rc) rc = engine_read_active(s->eng);
+        auto t3 = Clock::now();
+        if (running && !rc) {
             for (SrvSlot &sl : s->slots) sl.fresh = false;
             engine_mark_started(s->eng);
-            rc = retire(s, done);
+            rc = retire(s);
         }
-        if (!rc && !done.empty() && !s->slots.empty()) rc = engine_members(s);
+        auto t4 = Clock::now();
+        /* 5. the next member set: the remaining ones and the arrivals whose
+         * uploads are done (the sweeps never wait for a copy; with nothing
+         * to sweep the loop waits for the oldest upload) */
+        bool changed = running && s->eng.h_ctl->nsys != (int)s->slots.size();
+        while (!rc && !s->incoming.empty()) {
+            tbs_server::Incoming &in = s->incoming.front();
+            const cudaError_t q = s->slots.empty() ? cudaEventSynchronize(in.ev) : cudaEventQuery(in.ev);
+            if (q == cudaErrorNotReady) break;
+            if (q != cudaSuccess) {
+                rc = sfail(s, TBS_ERR_CUDA, "upload failed");
+                break;
+            }
+            for (SrvSlot &sl : in.slots) s->slots.push_back(sl);
+            s->ev_pool.push_back(in.ev);
+            s->incoming.pop_front();
+            changed = true;
+        }
+        if (!rc && changed && !s->slots.empty()) rc = engine_members(s);
+        auto t5 = Clock::now();
         std::string msg = rc ? s->eng.err + s->err : std::string();
         lk.lock();
-        s->n_launches += 1;
-        s->peak_rhs = std::max<long long>(s->peak_rhs, (long long)s->slots.size() + (long long)done.size());
+        s->us_start += 1e3 * ms_between(t1, t2);
+        s->us_members += 1e3 * ms_between(t4, t5);
+        s->us_run += 1e3 * (ms_between(t0, t1) + ms_between(t2, t3));
+        s->us_retire += 1e3 * ms_between(t3, t4);
+        if (running) s->n_launches += 1;
+        s->peak_rhs = std::max<long long>(s->peak_rhs, (long long)s->slots.size());
         s->peak_bytes = std::max<long long>(s->peak_bytes, (long long)s->slot_bytes_in_flight);
         for (SrvRequest *r : failed) {
-            s->systems[r->sys].inflight -= r->nrhs;
+            s->systems[r->sys].inflight[r->ver] -= r->nrhs;
             s->slot_bytes_in_flight -= r->bytes;
             complete(s, r, TBS_ERR_NOMEM, "device allocation for the right-hand sides failed");
         }
-        for (SrvSlot &sl : done) {
-            SrvRequest *r = sl.req;
-            s->systems[r->sys].inflight -= 1;
-            s->slot_bytes_in_flight -= sl.bytes;
-            if (--r->remaining == 0) complete(s, r, 0, "");
+        for (tbs_server::Pending &p : copied) {
+            for (size_t k = 0; k < p.slots.size(); ++k) {
+                SrvSlot &sl = p.slots[k];
+                SrvRequest *r = sl.req;
+                const SolveState &st = p.st[k];
+                r->sweeps[sl.k] = st.sweep;
+                r->rel[sl.k] = st.norm0 > 0.0 ? st.last / st.norm0 : 0.0;
+                s->systems[r->sys].inflight[r->ver] -= 1;
+                s->slot_bytes_in_flight -= sl.bytes;
+                if (--r->remaining == 0) complete(s, r, 0, "");
+            }
         }
         if (rc) {
             /* a device error ends every request in flight */
-            for (SrvSlot &sl : s->slots) {
+            std::vector<SrvSlot> all = s->slots;
+            for (tbs_server::Incoming &in : s->incoming) all.insert(all.end(), in.slots.begin(), in.slots.end());
+            for (tbs_server::Pending &p : s->pending) all.insert(all.end(), p.slots.begin(), p.slots.end());
+            for (SrvSlot &sl : all) {
                 SrvRequest *r = sl.req;
-                s->systems[r->sys].inflight -= 1;
+                s->systems[r->sys].inflight[r->ver] -= 1;
                 s->slot_bytes_in_flight -= sl.bytes;
                 if (r->state == SrvRequest::RUNNING) complete(s, r, rc, msg);
             }
             s->slots.clear();
+            s->incoming.clear();
+            s->pending.clear();
             s->err = msg;
         }
-        if (!failed.empty() || !done.empty() || rc) s->cv_done.notify_all();
+        if (!failed.empty() || !copied.empty() || rc) s->cv_done.notify_all();
+        /* 6. idle: nothing to sweep or copy; new requests or the end of a
+         * re-factorization wake the loop */
+        if (s->slots.empty() && s->incoming.empty() && s->pending.empty() && admitted.empty()) {
+            if (s->stopping && s->queue.empty() && s->factor_jobs.empty()) break;
+            bool ready = false;
+            for (SrvRequest *r : s->queue)
+                if (r->state == SrvRequest::QUEUED && !s->systems[r->sys].refactoring) ready = true;
+            if (s->queue.empty())
+                s->cv_loop.wait(lk);
+            else if (!ready) /* queued behind a re-factorization */
+                s->cv_loop.wait_for(lk, std::chrono::milliseconds(1));
+        }
     }
 }
 
@@ -485,13 +657,24 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
     auto fail = [&](int code, const std::string &msg) {
         if (s->eng.h_ctl) engine_free(s->eng);
         if (s->pool) cudaMemPoolDestroy(s->pool);
-        if (s->stream) cudaStreamDestroy(s->stream);
+        if (s->h_states) cudaFreeHost(s->h_states);
+        if (s->h_up_states) cudaFreeHost(s->h_up_states);
+        if (s->ev_up) cudaEventDestroy(s->ev_up);
+        for (cudaStream_t x : {s->stream, s->up, s->down})
+            if (x) cudaStreamDestroy(x);
         delete s;
         return sfail(nullptr, code, msg);
     };
     if (cudaSetDevice(device_id) != cudaSuccess) return fail(TBS_ERR_CUDA, "cudaSetDevice failed");
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess)
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) != cudaSuccess)
         return fail(TBS_ERR_CUDA, "cudaStreamCreate failed");
+    if (cudaEventCreateWithFlags(&s->ev_up, cudaEventDisableTiming) != cudaSuccess)
+        return fail(TBS_ERR_CUDA, "cudaEventCreate failed");
+    if (cudaMallocHost(&s->h_states, sizeof(SolveState) * (size_t)max_rhs_in_flight) != cudaSuccess ||
+        cudaMallocHost(&s->h_up_states, sizeof(SolveState) * (size_t)max_rhs_in_flight) != cudaSuccess)
+        return fail(TBS_ERR_NOMEM, "pinned allocation failed");
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -521,11 +704,19 @@ int tbs_server_destroy(tbs_server *s) {
     if (!s) return TBS_OK;
     server_stop(s);
     cudaSetDevice(s->device);
-    cudaStreamSynchronize(s->stream);
+    for (cudaStream_t x : {s->stream, s->up, s->down})
+        if (x) cudaStreamSynchronize(x);
     engine_free(s->eng);
-    for (SrvSystem &sys : s->systems) tbs_destroy(sys.ctx);
+    for (SrvSystem &sys : s->systems)
+        for (tbs_ctx *c : sys.ctx)
+            if (c) tbs_destroy(c);
+    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
+    if (s->ev_up) cudaEventDestroy(s->ev_up);
+    if (s->h_states) cudaFreeHost(s->h_states);
+    if (s->h_up_states) cudaFreeHost(s->h_up_states);
     if (s->pool) cudaMemPoolDestroy(s->pool);
-    if (s->stream) cudaStreamDestroy(s->stream);
+    for (cudaStream_t x : {s->stream, s->up, s->down})
+        if (x) cudaStreamDestroy(x);
     delete s;
     return TBS_OK;
 }
@@ -573,7 +764,8 @@ int tbs_server_add_system(tbs_server *s, int nvar, int nelem, int nintface, int 
     }
     s->sys_bytes += bytes;
     SrvSystem sys;
-    sys.ctx = c;
+    sys.ctx[0] = c;
+    sys.bytes = bytes;
     s->systems.push_back(sys);
     *system_id = (int)s->systems.size() - 1;
     return TBS_OK;
@@ -585,7 +777,8 @@ int tbs_server_system_bytes(tbs_server *s, int system_id, int max_sweeps, size_t
     std::lock_guard<std::mutex> lk(s->mu);
     if (system_id < 0 || system_id >= (int)s->systems.size())
         return sfail(s, TBS_ERR_ARG, "unknown system");
-    tbs_ctx *c = s->systems[system_id].ctx;
+    const SrvSystem &sys = s->systems[system_id];
+    tbs_ctx *c = sys.ctx[sys.cur];
     if (resident) tbs_memory_allocated(c, resident);
     if (per_rhs) *per_rhs = slot_bytes(c, s->algo, std::max(max_sweeps, 0) + 1);
     return TBS_OK;
@@ -601,7 +794,8 @@ int tbs_server_submit(tbs_server *s, int system_id, int nrhs, const double *rhs,
     if (s->stopping) return sfail(s, TBS_ERR_STATE, "server stopping");
     if (system_id < 0 || system_id >= (int)s->systems.size())
         return sfail(s, TBS_ERR_ARG, "unknown system");
-    tbs_ctx *c = s->systems[system_id].ctx;
+    const SrvSystem &sys = s->systems[system_id];
+    tbs_ctx *c = sys.ctx[sys.cur];
     if (jacD && (!jacO1 || !jacO2) && c->nintface > 0)
         return sfail(s, TBS_ERR_ARG, "new Jacobian values need jacD, jacO1 and jacO2");
     const size_t per = slot_bytes(c, s->algo, max_sweeps + 1);
@@ -675,7 +869,9 @@ int tbs_server_stats(tbs_server *s, long long *stats, int n) {
     if (!s || !stats) return sfail(s, TBS_ERR_ARG, "null argument");
     std::lock_guard<std::mutex> lk(s->mu);
     const long long v[] = {s->n_done, s->n_rhs_done, s->n_launches, s->n_refactor, s->peak_rhs,
-                           s->peak_bytes, (long long)s->sys_bytes, (long long)s->queue.size()};
+                           s->peak_bytes, (long long)s->sys_bytes, (long long)s->queue.size(),
+                           (long long)s->us_start, (long long)s->us_members, (long long)s->us_run,
+                           (long long)s->us_retire};
     for (int k = 0; k < n && k < (int)(sizeof(v) / sizeof(v[0])); ++k) stats[k] = v[k];
     return TBS_OK;
 }

@@ -268,15 +268,24 @@ template <typename T>
 int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
                         const WorkItem *work, const int *nwork, const int *active, unsigned *queue,
                         unsigned *status);
+/* Group index: the work items of the residual-type launches without a
+ * list of them.  Members that share a system form a group; group g covers
+ * items [base[g], base[g+1]) = (its units) x (its members), unit-major, so
+ * that the right-hand sides of one system run each unit side by side and
+ * share its blocks in L2.  Device layout (ints):
+ *   [ng][base[0..ng]][nmem[0..ng)][moff[0..ng)][mlist[...]]
+ * item w -> member mlist[moff[g] + (w - base[g]) % nmem[g]],
+ *           unit (w - base[g]) / nmem[g]. */
+inline size_t group_index_ints(int max_groups, int max_members) {
+    return 1 + (size_t)(max_groups + 1) + 2 * (size_t)max_groups + (size_t)max_members;
+}
 template <typename T>
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const WorkItem *work, const int *nwork, const int *active, unsigned *status);
-int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const WorkItem *work,
-                            const int *nwork, const int *active);
-int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work,
-                             const int *nwork);
-int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const WorkItem *work, const int *nwork,
-                       const int *active);
+                       const int *groups, const int *active, unsigned *status);
+int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *groups,
+                            const int *active);
+int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const int *groups);
+int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, const int *active);
 /* one CTA of `threads` threads per norm descriptor (grid = cap, *nred in
  * use): the fixed-order sum of the member's partials (the order of
  * finalize_norm for threads = 160 and of reduce_norm for threads = 256),

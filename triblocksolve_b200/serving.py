@@ -19,7 +19,8 @@ from . import _native as N
 from .lij import Jacobian, Mesh
 
 STAT_NAMES = ("requests_done", "rhs_done", "graph_launches", "refactors", "peak_rhs_in_flight",
-              "peak_rhs_bytes", "resident_system_bytes", "queued")
+              "peak_rhs_bytes", "resident_system_bytes", "queued", "us_start", "us_members",
+              "us_run", "us_retire")
 
 
 class Request:
