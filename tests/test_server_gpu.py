@@ -66,7 +66,9 @@ def check(req_result, expected):
 def test_same_alone_and_in_the_mix(algo):
     sy = systems()
     rng = np.random.default_rng(7)
-    srv = Server(0, algo, budget_bytes=8 << 30, max_rhs=32, chunk=2)
+    # FP64: two lanes (the 48x64 system sweeps apart from the small ones)
+    srv = Server(0, algo, budget_bytes=8 << 30, max_rhs=32, chunk=2,
+                 lane_split=1000 if algo == ALGO_FP64 else 0)
     try:
         ids = [srv.add_system(m, j) for m, j in sy]
         probe_sys = 2
@@ -145,7 +147,7 @@ def test_admission_by_footprint():
 
 def test_concurrent_clients():
     sy = systems()
-    srv = Server(0, ALGO_FP64, budget_bytes=8 << 30, max_rhs=32, chunk=1)
+    srv = Server(0, ALGO_FP64, budget_bytes=8 << 30, max_rhs=32, chunk=1, lane_split=500)
     try:
         ids = [srv.add_system(m, j) for m, j in sy]
         results, errors = {}, []

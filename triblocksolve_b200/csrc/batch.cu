@@ -71,6 +71,30 @@ static void efree(Engine &e, T **p) {
     *p = nullptr;
 }
 
+/* the capacity-sized arrays are stream-ordered: growing them does not
+ * synchronise the device (other engines' graphs keep running) */
+template <typename T>
+static int ealloc_async(Engine &e, T **p, size_t count) {
+    void *q = nullptr;
+    const size_t nbytes = std::max<size_t>(count, 1) * sizeof(T);
+    if (cudaMallocAsync(&q, nbytes, e.stream) != cudaSuccess) {
+        cudaGetLastError();
+        return efail(e, TBS_ERR_NOMEM, "cudaMallocAsync of " + std::to_string(nbytes) + " bytes failed");
+    }
+    e.allocs.push_back(q);
+    *p = static_cast<T *>(q);
+    return TBS_OK;
+}
+
+template <typename T>
+static void efree_async(Engine &e, T **p) {
+    if (!*p) return;
+    auto it = std::find(e.allocs.begin(), e.allocs.end(), (void *)*p);
+    if (it != e.allocs.end()) e.allocs.erase(it);
+    cudaFreeAsync(*p, e.stream);
+    *p = nullptr;
+}
+
 template <typename T>
 static int eupload(Engine &e, T *dst, const std::vector<T> &h) {
     if (!h.empty())
@@ -246,49 +270,51 @@ void engine_free(Engine &e) {
 
 /* grow the capacity-sized arrays (never shrinks); growth invalidates the graph */
 static int ensure_capacity(Engine &e, int nmem, int nlines) {
-    auto grow = [](int need, int have) { return need <= have ? have : std::max(need, have + have / 2); };
+    auto grow = [](int need, int have, int least) {
+        return need <= have ? have : std::max({need, 2 * have, least});
+    };
     int rc = TBS_OK;
     if (nmem > e.cap_mem) {
-        const int c = grow(nmem, e.cap_mem);
-        efree(e, &e.d_th64);
-        efree(e, &e.d_th32);
-        efree(e, &e.d_rs_prime);
-        efree(e, &e.d_rs_body);
-        efree(e, &e.d_rs32_rhs);
-        efree(e, &e.d_rs32_dx);
-        efree(e, &e.d_fr);
-        efree(e, &e.d_vec);
-        efree(e, &e.d_red_prime);
-        efree(e, &e.d_red_body);
-        efree(e, &e.d_active);
-        efree(e, &e.d_g_tiles);
-        efree(e, &e.d_g_prime);
-        efree(e, &e.d_g_blocks);
+        const int c = grow(nmem, e.cap_mem, 64);
+        efree_async(e, &e.d_th64);
+        efree_async(e, &e.d_th32);
+        efree_async(e, &e.d_rs_prime);
+        efree_async(e, &e.d_rs_body);
+        efree_async(e, &e.d_rs32_rhs);
+        efree_async(e, &e.d_rs32_dx);
+        efree_async(e, &e.d_fr);
+        efree_async(e, &e.d_vec);
+        efree_async(e, &e.d_red_prime);
+        efree_async(e, &e.d_red_body);
+        efree_async(e, &e.d_active);
+        efree_async(e, &e.d_g_tiles);
+        efree_async(e, &e.d_g_prime);
+        efree_async(e, &e.d_g_blocks);
         if (e.algo == TBS_ALGO_FP64) {
-            if (!rc) rc = ealloc(e, &e.d_th64, c);
-            if (!rc) rc = ealloc(e, &e.d_rs_prime, c);
-            if (!rc) rc = ealloc(e, &e.d_rs_body, c);
+            if (!rc) rc = ealloc_async(e, &e.d_th64, c);
+            if (!rc) rc = ealloc_async(e, &e.d_rs_prime, c);
+            if (!rc) rc = ealloc_async(e, &e.d_rs_body, c);
         } else {
-            if (!rc) rc = ealloc(e, &e.d_th32, c);
-            if (!rc) rc = ealloc(e, &e.d_rs32_rhs, c);
-            if (!rc) rc = ealloc(e, &e.d_rs32_dx, c);
-            if (!rc) rc = ealloc(e, &e.d_fr, c);
-            if (!rc) rc = ealloc(e, &e.d_vec, c);
+            if (!rc) rc = ealloc_async(e, &e.d_th32, c);
+            if (!rc) rc = ealloc_async(e, &e.d_rs32_rhs, c);
+            if (!rc) rc = ealloc_async(e, &e.d_rs32_dx, c);
+            if (!rc) rc = ealloc_async(e, &e.d_fr, c);
+            if (!rc) rc = ealloc_async(e, &e.d_vec, c);
         }
-        if (!rc) rc = ealloc(e, &e.d_red_prime, c);
-        if (!rc) rc = ealloc(e, &e.d_red_body, c);
-        if (!rc) rc = ealloc(e, &e.d_active, c);
+        if (!rc) rc = ealloc_async(e, &e.d_red_prime, c);
+        if (!rc) rc = ealloc_async(e, &e.d_red_body, c);
+        if (!rc) rc = ealloc_async(e, &e.d_active, c);
         const size_t gi = group_index_ints(c, c);
-        if (!rc) rc = ealloc(e, &e.d_g_tiles, gi);
-        if (!rc) rc = ealloc(e, &e.d_g_prime, gi);
-        if (!rc) rc = ealloc(e, &e.d_g_blocks, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_tiles, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_prime, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_blocks, gi);
         e.cap_mem = rc ? 0 : c;
         engine_drop_graph(e);
     }
     if (!rc && nlines > e.cap_lines) {
-        const int c = grow(nlines, e.cap_lines);
-        efree(e, &e.d_lines);
-        rc = ealloc(e, &e.d_lines, c);
+        const int c = grow(nlines, e.cap_lines, 1 << 16);
+        efree_async(e, &e.d_lines);
+        rc = ealloc_async(e, &e.d_lines, c);
         e.cap_lines = rc ? 0 : c;
         engine_drop_graph(e);
     }

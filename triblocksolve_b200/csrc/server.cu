@@ -62,6 +62,7 @@ struct SrvSystem {
     bool refactoring = false;
     bool broken = false;      /* an in-place re-factorization failed */
     size_t bytes = 0;         /* device bytes of one version */
+    int lane = 0;
 };
 
 struct SrvRequest {
@@ -100,6 +101,34 @@ struct SrvSlot {               /* one right-hand side in flight (an engine membe
 
 }  // namespace
 
+struct SrvIncoming {               /* uploads issued, not yet members */
+    std::vector<SrvSlot> slots;
+    cudaEvent_t ev;                /* their uploads are done */
+};
+
+struct SrvPending {                /* read-backs in flight */
+    std::vector<SrvSlot> slots;
+    std::vector<SolveState> st;
+    cudaEvent_t ev;
+};
+
+struct SrvLane {
+    int id = 0;
+    Engine eng;
+    cudaStream_t stream = nullptr;     /* graph launches */
+    cudaStream_t up = nullptr;         /* uploads of admitted right-hand sides */
+    cudaStream_t down = nullptr;       /* read-back of finished solutions */
+    std::vector<SrvSlot> slots;        /* members of the engine */
+    std::deque<SrvIncoming> incoming;
+    cudaEvent_t ev_up = nullptr;       /* the last batch of uploads is done */
+    std::deque<SrvPending> pending;
+    std::vector<cudaEvent_t> ev_pool;
+    SolveState *h_states = nullptr;    /* pinned, max_slots: read-back of states */
+    SolveState *h_up_states = nullptr; /* pinned, max_slots: states of admitted ones */
+    std::string err;
+    std::thread th;
+};
+
 struct tbs_server {
     int device = 0;
     int algo = TBS_ALGO_FP64;
@@ -119,30 +148,15 @@ struct tbs_server {
     std::deque<SrvRequest *> factor_jobs;
     long long next_id = 1;
 
-    /* loop-thread state */
-    Engine eng;
-    cudaStream_t stream = nullptr;     /* graph launches */
-    cudaStream_t up = nullptr;         /* uploads of admitted right-hand sides */
-    cudaStream_t down = nullptr;       /* read-back of finished solutions */
+    /* one loop thread per lane: systems below lane_split cells sweep in
+     * lane 0, the others in lane 1, so that small systems are not held to
+     * the pace of the large ones */
+    long long lane_split = 262144;
+    std::vector<std::unique_ptr<struct SrvLane>> lanes;
     cudaMemPool_t pool = nullptr;
     bool pool_reserved = false;
-    std::vector<SrvSlot> slots;        /* members of the engine */
-    struct Incoming {                  /* uploads issued, not yet members */
-        std::vector<SrvSlot> slots;
-        cudaEvent_t ev;                /* their uploads are done */
-    };
-    std::deque<Incoming> incoming;
-    cudaEvent_t ev_up = nullptr;       /* the last batch of uploads is done */
-    struct Pending {
-        std::vector<SrvSlot> slots;
-        std::vector<SolveState> st;
-        cudaEvent_t ev;
-    };
-    std::deque<Pending> pending;       /* read-backs in flight */
-    std::vector<cudaEvent_t> ev_pool;
-    SolveState *h_states = nullptr;    /* pinned, max_slots: read-back of states */
-    SolveState *h_up_states = nullptr; /* pinned, max_slots: states of admitted ones */
-    std::thread loop, factor;
+    int rhs_in_flight = 0;             /* admitted, not yet read back (all lanes) */
+    std::thread factor;
 
     /* statistics */
     long long n_done = 0, n_rhs_done = 0, n_launches = 0, n_refactor = 0;
@@ -283,18 +297,23 @@ static void factor_main(tbs_server *s) {
     }
 }
 
-/* ---------------------------------------------------------------- loop thread */
+/* ---------------------------------------------------------------- loop threads */
 
-/* Admission scan under the lock: requests in arrival order; a request that
- * needs a re-factorization goes to the factor thread once its system is
- * idle; later requests of a system that is being re-factored wait; the
- * first request whose right-hand sides do not fit ends the scan. */
-static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
+/* Admission scan of one lane under the lock: the lane's requests in
+ * arrival order; a request that needs a re-factorization goes to the
+ * factor thread once its target copy is idle; later requests of a system
+ * that is being re-factored wait; the first request whose right-hand sides
+ * do not fit (budget, or right-hand sides in flight) ends the scan. */
+static void admit_scan(tbs_server *s, SrvLane *L, std::vector<SrvRequest *> &admitted) {
     std::vector<char> blocked(s->systems.size(), 0);
     const size_t avail = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
     for (auto it = s->queue.begin(); it != s->queue.end();) {
         SrvRequest *r = *it;
         SrvSystem &sys = s->systems[r->sys];
+        if (sys.lane != L->id) {
+            ++it;
+            continue;
+        }
         if (sys.broken && r->state == SrvRequest::QUEUED) {
             complete(s, r, TBS_ERR_STATE, "the system's re-factorization failed");
             s->cv_done.notify_all();
@@ -307,7 +326,7 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
             continue;
         }
         if (r->jacD && !r->refactored) {
-            /* into the spare version while the current one keeps sweeping;
+            /* into the spare copy while the current one keeps sweeping;
              * in place (after the system drains) when a spare does not fit */
             const int spare = 1 - sys.cur;
             const bool have = sys.ctx[spare] != nullptr;
@@ -326,14 +345,9 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
             ++it;
             continue;
         }
-        const int in_flight = (int)s->slots.size() + [&] {
-            int n = 0;
-            for (SrvRequest *a : admitted) n += a->nrhs;
-            for (const tbs_server::Incoming &in : s->incoming) n += (int)in.slots.size();
-            return n;
-        }();
-        if (in_flight + r->nrhs > s->max_slots || s->slot_bytes_in_flight + r->bytes > avail) break;
+        if (s->rhs_in_flight + r->nrhs > s->max_slots || s->slot_bytes_in_flight + r->bytes > avail) break;
         s->slot_bytes_in_flight += r->bytes;
+        s->rhs_in_flight += r->nrhs;
         r->ver = sys.cur;
         r->ctx = sys.ctx[sys.cur];
         sys.inflight[r->ver] += r->nrhs;
@@ -347,22 +361,21 @@ static void admit_scan(tbs_server *s, std::vector<SrvRequest *> &admitted) {
 /* Keep freed right-hand-side memory in the pool and grow it once to the
  * room the budget leaves after the resident systems, so that admissions do
  * not pay for mapping new device memory. */
-static void reserve_pool(tbs_server *s, size_t avail) {
-    if (s->pool_reserved || avail == 0) return;
-    s->pool_reserved = true;
+static void reserve_pool(tbs_server *s, SrvLane *L, size_t avail) {
+    if (avail == 0) return;
     void *p = nullptr;
-    if (cudaMallocFromPoolAsync(&p, avail, s->pool, s->up) == cudaSuccess) {
-        cudaFreeAsync(p, s->up);
-        cudaStreamSynchronize(s->up);
+    if (cudaMallocFromPoolAsync(&p, avail, s->pool, L->up) == cudaSuccess) {
+        cudaFreeAsync(p, L->up);
+        cudaStreamSynchronize(L->up);
     } else {
         cudaGetLastError(); /* not fatal: the pool then grows on demand */
     }
 }
 
-static cudaEvent_t take_event(tbs_server *s) {
-    if (!s->ev_pool.empty()) {
-        cudaEvent_t e = s->ev_pool.back();
-        s->ev_pool.pop_back();
+static cudaEvent_t take_event(SrvLane *L) {
+    if (!L->ev_pool.empty()) {
+        cudaEvent_t e = L->ev_pool.back();
+        L->ev_pool.pop_back();
         return e;
     }
     cudaEvent_t e = nullptr;
@@ -370,16 +383,22 @@ static cudaEvent_t take_event(tbs_server *s) {
     return e;
 }
 
+static int lfail(SrvLane *L, int code, const std::string &msg) {
+    L->err = msg;
+    set_thread_error(msg);
+    return code;
+}
+
 /* allocate, clear and fill the right-hand sides of newly admitted requests
  * on the upload stream (overlapping the running graph); they become engine
- * members at the next member update, after ev_up */
-static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitted,
+ * members once their uploads are done */
+static int start_requests(tbs_server *s, SrvLane *L, const std::vector<SrvRequest *> &admitted,
                           std::vector<SrvRequest *> &failed) {
     if (admitted.empty()) return TBS_OK;
     /* the staging of the previous uploads is free once they have run */
-    if (cudaEventSynchronize(s->ev_up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event failed");
+    if (cudaEventSynchronize(L->ev_up) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "event failed");
     int nst = 0;
-    tbs_server::Incoming batch;
+    SrvIncoming batch;
     for (SrvRequest *r : admitted) {
         tbs_ctx *c = r->ctx;
         const size_t nv = (size_t)c->nelem * 9;
@@ -391,7 +410,7 @@ static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitt
             sl.req = r;
             sl.k = k;
             sl.bytes = per;
-            if (cudaMallocFromPoolAsync(&sl.mem, per, s->pool, s->up) != cudaSuccess) {
+            if (cudaMallocFromPoolAsync(&sl.mem, per, s->pool, L->up) != cudaSuccess) {
                 cudaGetLastError();
                 ok = false;
                 break;
@@ -402,96 +421,94 @@ static int start_requests(tbs_server *s, const std::vector<SrvRequest *> &admitt
             /* pad positions of the layout are never written by the kernels
              * but enter the first norm (rhs) and the U accumulation: start
              * from zeros, as a context's arrays do */
-            SolveState &st = s->h_up_states[nst++];
+            SolveState &st = L->h_up_states[nst++];
             st = SolveState{};
             st.tol = r->tol;
             st.max_sweeps = r->max_sweeps;
             st.hist_cap = r->max_sweeps + 1;
-            ok = cudaMemsetAsync(m.mem, 0, per, s->up) == cudaSuccess &&
-                 cudaMemcpyAsync(m.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, s->up) == cudaSuccess &&
+            ok = cudaMemsetAsync(m.mem, 0, per, L->up) == cudaSuccess &&
+                 cudaMemcpyAsync(m.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, L->up) == cudaSuccess &&
                  cudaMemcpyAsync(m.rhs_elem, r->rhs + k * nv, nv * sizeof(double),
-                                 cudaMemcpyHostToDevice, s->up) == cudaSuccess &&
-                 launch_permute_to_pos(s->up, 9, c->nelem, c->L.pos_of_elem, m.rhs_elem, m.v.rhsp) == 0;
+                                 cudaMemcpyHostToDevice, L->up) == cudaSuccess &&
+                 launch_permute_to_pos(L->up, 9, c->nelem, c->L.pos_of_elem, m.rhs_elem, m.v.rhsp) == 0;
         }
         if (!ok) {
             for (SrvSlot &sl : mine)
-                if (sl.mem) cudaFreeAsync(sl.mem, s->up);
+                if (sl.mem) cudaFreeAsync(sl.mem, L->up);
             failed.push_back(r);
             continue;
         }
         for (SrvSlot &sl : mine) batch.slots.push_back(sl);
     }
-    if (cudaEventRecord(s->ev_up, s->up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event record failed");
+    if (cudaEventRecord(L->ev_up, L->up) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "event record failed");
     if (!batch.slots.empty()) {
-        batch.ev = take_event(s);
-        if (cudaEventRecord(batch.ev, s->up) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event record failed");
-        s->incoming.push_back(std::move(batch));
+        batch.ev = take_event(L);
+        if (cudaEventRecord(batch.ev, L->up) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "event record failed");
+        L->incoming.push_back(std::move(batch));
     }
     return TBS_OK;
 }
 
-static int engine_members(tbs_server *s) {
+static int engine_members(SrvLane *L) {
     std::vector<Member> m;
-    m.reserve(s->slots.size());
-    for (SrvSlot &sl : s->slots) m.push_back({sl.req->ctx, sl.v, sl.fresh});
-    return engine_set_members(s->eng, m);
+    m.reserve(L->slots.size());
+    for (SrvSlot &sl : L->slots) m.push_back({sl.req->ctx, sl.v, sl.fresh});
+    return engine_set_members(L->eng, m);
 }
 
 /* the members that stopped: their states now (pinned, main stream), their
  * solutions permuted to element order on the main stream and copied to the
  * caller on the read-back stream (overlapping the next graph) */
-static int retire(tbs_server *s) {
+static int retire(SrvLane *L) {
     std::vector<SrvSlot> keep, out;
-    for (size_t k = 0; k < s->slots.size(); ++k)
-        (s->eng.h_active[k] ? keep : out).push_back(s->slots[k]);
+    for (size_t k = 0; k < L->slots.size(); ++k)
+        (L->eng.h_active[k] ? keep : out).push_back(L->slots[k]);
     if (out.empty()) return TBS_OK;
     for (size_t k = 0; k < out.size(); ++k) {
         SrvSlot &sl = out[k];
         tbs_ctx *c = sl.req->ctx;
-        if (cudaMemcpyAsync(&s->h_states[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost,
-                            s->stream) != cudaSuccess ||
-            launch_permute_to_elem(s->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0)
-            return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
+        if (cudaMemcpyAsync(&L->h_states[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost,
+                            L->stream) != cudaSuccess ||
+            launch_permute_to_elem(L->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0)
+            return lfail(L, TBS_ERR_CUDA, "solution read-back failed");
     }
-    cudaEvent_t ready = take_event(s);
-    if (cudaEventRecord(ready, s->stream) != cudaSuccess ||
-        cudaStreamWaitEvent(s->down, ready, 0) != cudaSuccess)
-        return sfail(s, TBS_ERR_CUDA, "event failed");
-    s->ev_pool.push_back(ready); /* reusable once recorded work is ordered */
-    tbs_server::Pending p;
+    cudaEvent_t ready = take_event(L);
+    if (cudaEventRecord(ready, L->stream) != cudaSuccess ||
+        cudaStreamWaitEvent(L->down, ready, 0) != cudaSuccess)
+        return lfail(L, TBS_ERR_CUDA, "event failed");
+    L->ev_pool.push_back(ready); /* reusable: the wait is already enqueued */
+    SrvPending p;
     for (SrvSlot &sl : out) {
         tbs_ctx *c = sl.req->ctx;
         const size_t nv = (size_t)c->nelem * 9;
         if (cudaMemcpyAsync(sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double),
-                            cudaMemcpyDeviceToHost, s->down) != cudaSuccess)
-            return sfail(s, TBS_ERR_CUDA, "solution read-back failed");
-        cudaFreeAsync(sl.mem, s->down);
+                            cudaMemcpyDeviceToHost, L->down) != cudaSuccess)
+            return lfail(L, TBS_ERR_CUDA, "solution read-back failed");
+        cudaFreeAsync(sl.mem, L->down);
     }
-    if (cudaStreamSynchronize(s->stream) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "state read-back failed");
-    p.st.assign(s->h_states, s->h_states + out.size());
+    if (cudaStreamSynchronize(L->stream) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "state read-back failed");
+    p.st.assign(L->h_states, L->h_states + out.size());
     p.slots.swap(out);
-    p.ev = take_event(s);
-    if (cudaEventRecord(p.ev, s->down) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "event failed");
-    s->pending.push_back(std::move(p));
-    s->slots.swap(keep);
+    p.ev = take_event(L);
+    if (cudaEventRecord(p.ev, L->down) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "event failed");
+    L->pending.push_back(std::move(p));
+    L->slots.swap(keep);
     return TBS_OK;
 }
 
-/* read-backs that finished (all of them when `all`): their requests'
- * results; called without the lock, returns the finished batches */
-static int collect(tbs_server *s, bool all, std::vector<tbs_server::Pending> &done) {
-    while (!s->pending.empty()) {
-        tbs_server::Pending &p = s->pending.front();
-        if (!all && cudaEventQuery(p.ev) == cudaErrorNotReady) break;
-        if (cudaEventSynchronize(p.ev) != cudaSuccess) return sfail(s, TBS_ERR_CUDA, "read-back failed");
-        s->ev_pool.push_back(p.ev);
+/* read-backs that finished; called without the lock */
+static int collect(SrvLane *L, std::vector<SrvPending> &done) {
+    while (!L->pending.empty()) {
+        SrvPending &p = L->pending.front();
+        if (cudaEventSynchronize(p.ev) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "read-back failed");
+        L->ev_pool.push_back(p.ev);
         done.push_back(std::move(p));
-        s->pending.pop_front();
+        L->pending.pop_front();
     }
     return TBS_OK;
 }
 
-static void loop_main(tbs_server *s) {
+static void loop_main(tbs_server *s, SrvLane *L) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
@@ -500,65 +517,70 @@ static void loop_main(tbs_server *s) {
         auto t0 = Clock::now();
         /* 1. sweep the members while the host admits and copies */
         int rc = TBS_OK;
-        const bool running = !s->slots.empty();
-        if (running) rc = engine_launch(s->eng, chunk, 1);
+        const bool running = !L->slots.empty();
+        if (running) rc = engine_launch(L->eng, chunk, 1);
         /* 2. admission and uploads */
         std::vector<SrvRequest *> admitted, failed;
         lk.lock();
-        admit_scan(s, admitted);
-        const size_t avail = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
+        admit_scan(s, L, admitted);
+        size_t reserve = 0;
+        if (!admitted.empty() && !s->pool_reserved) {
+            s->pool_reserved = true;
+            reserve = s->budget > s->sys_bytes ? s->budget - s->sys_bytes : 0;
+        }
         lk.unlock();
-        if (!admitted.empty()) reserve_pool(s, avail);
+        if (reserve) reserve_pool(s, L, reserve);
         auto t1 = Clock::now();
-        if (!rc) rc = start_requests(s, admitted, failed);
+        if (!rc) rc = start_requests(s, L, admitted, failed);
         /* 3. solutions that reached the caller */
-        std::vector<tbs_server::Pending> copied;
-        if (!rc) rc = collect(s, true, copied);
+        std::vector<SrvPending> copied;
+        if (!rc) rc = collect(L, copied);
         auto t2 = Clock::now();
         /* 4. the sweeps' end: retire the members that stopped */
-        if (running && !rc) rc = engine_finish(s->eng);
-        if (running && !rc) rc = engine_read_active(s->eng);
+        if (running && !rc) rc = engine_finish(L->eng);
+        if (running && !rc) rc = engine_read_active(L->eng);
         auto t3 = Clock::now();
         if (running && !rc) {
-            for (SrvSlot &sl : s->slots) sl.fresh = false;
-            engine_mark_started(s->eng);
-            rc = retire(s);
+            for (SrvSlot &sl : L->slots) sl.fresh = false;
+            engine_mark_started(L->eng);
+            rc = retire(L);
         }
         auto t4 = Clock::now();
         /* 5. the next member set: the remaining ones and the arrivals whose
          * uploads are done (the sweeps never wait for a copy; with nothing
          * to sweep the loop waits for the oldest upload) */
-        bool changed = running && s->eng.h_ctl->nsys != (int)s->slots.size();
-        while (!rc && !s->incoming.empty()) {
-            tbs_server::Incoming &in = s->incoming.front();
-            const cudaError_t q = s->slots.empty() ? cudaEventSynchronize(in.ev) : cudaEventQuery(in.ev);
+        bool changed = running && L->eng.h_ctl->nsys != (int)L->slots.size();
+        while (!rc && !L->incoming.empty()) {
+            SrvIncoming &in = L->incoming.front();
+            const cudaError_t q = L->slots.empty() ? cudaEventSynchronize(in.ev) : cudaEventQuery(in.ev);
             if (q == cudaErrorNotReady) break;
             if (q != cudaSuccess) {
-                rc = sfail(s, TBS_ERR_CUDA, "upload failed");
+                rc = lfail(L, TBS_ERR_CUDA, "upload failed");
                 break;
             }
-            for (SrvSlot &sl : in.slots) s->slots.push_back(sl);
-            s->ev_pool.push_back(in.ev);
-            s->incoming.pop_front();
+            for (SrvSlot &sl : in.slots) L->slots.push_back(sl);
+            L->ev_pool.push_back(in.ev);
+            L->incoming.pop_front();
             changed = true;
         }
-        if (!rc && changed && !s->slots.empty()) rc = engine_members(s);
+        if (!rc && changed && !L->slots.empty()) rc = engine_members(L);
         auto t5 = Clock::now();
-        std::string msg = rc ? s->eng.err + s->err : std::string();
+        std::string msg = rc ? L->eng.err + L->err : std::string();
         lk.lock();
         s->us_start += 1e3 * ms_between(t1, t2);
         s->us_members += 1e3 * ms_between(t4, t5);
         s->us_run += 1e3 * (ms_between(t0, t1) + ms_between(t2, t3));
         s->us_retire += 1e3 * ms_between(t3, t4);
         if (running) s->n_launches += 1;
-        s->peak_rhs = std::max<long long>(s->peak_rhs, (long long)s->slots.size());
+        s->peak_rhs = std::max<long long>(s->peak_rhs, (long long)s->rhs_in_flight);
         s->peak_bytes = std::max<long long>(s->peak_bytes, (long long)s->slot_bytes_in_flight);
         for (SrvRequest *r : failed) {
             s->systems[r->sys].inflight[r->ver] -= r->nrhs;
             s->slot_bytes_in_flight -= r->bytes;
+            s->rhs_in_flight -= r->nrhs;
             complete(s, r, TBS_ERR_NOMEM, "device allocation for the right-hand sides failed");
         }
-        for (tbs_server::Pending &p : copied) {
+        for (SrvPending &p : copied) {
             for (size_t k = 0; k < p.slots.size(); ++k) {
                 SrvSlot &sl = p.slots[k];
                 SrvRequest *r = sl.req;
@@ -567,42 +589,84 @@ static void loop_main(tbs_server *s) {
                 r->rel[sl.k] = st.norm0 > 0.0 ? st.last / st.norm0 : 0.0;
                 s->systems[r->sys].inflight[r->ver] -= 1;
                 s->slot_bytes_in_flight -= sl.bytes;
+                s->rhs_in_flight -= 1;
                 if (--r->remaining == 0) complete(s, r, 0, "");
             }
         }
         if (rc) {
-            /* a device error ends every request in flight */
-            std::vector<SrvSlot> all = s->slots;
-            for (tbs_server::Incoming &in : s->incoming) all.insert(all.end(), in.slots.begin(), in.slots.end());
-            for (tbs_server::Pending &p : s->pending) all.insert(all.end(), p.slots.begin(), p.slots.end());
+            /* a device error ends every request in flight in this lane */
+            std::vector<SrvSlot> all = L->slots;
+            for (SrvIncoming &in : L->incoming) all.insert(all.end(), in.slots.begin(), in.slots.end());
+            for (SrvPending &p : L->pending) all.insert(all.end(), p.slots.begin(), p.slots.end());
             for (SrvSlot &sl : all) {
                 SrvRequest *r = sl.req;
                 s->systems[r->sys].inflight[r->ver] -= 1;
                 s->slot_bytes_in_flight -= sl.bytes;
+                s->rhs_in_flight -= 1;
                 if (r->state == SrvRequest::RUNNING) complete(s, r, rc, msg);
             }
-            s->slots.clear();
-            s->incoming.clear();
-            s->pending.clear();
+            L->slots.clear();
+            L->incoming.clear();
+            L->pending.clear();
             s->err = msg;
         }
-        if (!failed.empty() || !copied.empty() || rc) s->cv_done.notify_all();
-        /* 6. idle: nothing to sweep or copy; new requests or the end of a
-         * re-factorization wake the loop */
-        if (s->slots.empty() && s->incoming.empty() && s->pending.empty() && admitted.empty()) {
-            if (s->stopping && s->queue.empty() && s->factor_jobs.empty()) break;
-            bool ready = false;
-            for (SrvRequest *r : s->queue)
+        if (!failed.empty() || !copied.empty() || rc) {
+            s->cv_done.notify_all();
+            s->cv_loop.notify_all(); /* room freed: the other lane may admit */
+        }
+        /* 6. idle: nothing to sweep or copy; new requests, freed room or
+         * the end of a re-factorization wake the loop */
+        if (L->slots.empty() && L->incoming.empty() && L->pending.empty() && admitted.empty()) {
+            bool mine = false, ready = false;
+            for (SrvRequest *r : s->queue) {
+                if (s->systems[r->sys].lane != L->id) continue;
+                mine = true;
                 if (r->state == SrvRequest::QUEUED && !s->systems[r->sys].refactoring) ready = true;
-            if (s->queue.empty())
+            }
+            if (s->stopping && !mine && s->factor_jobs.empty()) break;
+            if (!mine)
                 s->cv_loop.wait(lk);
             else if (!ready) /* queued behind a re-factorization */
+                s->cv_loop.wait_for(lk, std::chrono::milliseconds(1));
+            else /* queued but did not fit: wait for room */
                 s->cv_loop.wait_for(lk, std::chrono::milliseconds(1));
         }
     }
 }
 
 /* ---------------------------------------------------------------- entry points */
+
+static void lane_free(SrvLane *L) {
+    for (cudaStream_t x : {L->stream, L->up, L->down})
+        if (x) cudaStreamSynchronize(x);
+    if (L->eng.h_ctl) engine_free(L->eng);
+    for (cudaEvent_t e : L->ev_pool) cudaEventDestroy(e);
+    L->ev_pool.clear();
+    if (L->ev_up) cudaEventDestroy(L->ev_up);
+    if (L->h_states) cudaFreeHost(L->h_states);
+    if (L->h_up_states) cudaFreeHost(L->h_up_states);
+    for (cudaStream_t x : {L->stream, L->up, L->down})
+        if (x) cudaStreamDestroy(x);
+    L->ev_up = nullptr;
+    L->h_states = L->h_up_states = nullptr;
+    L->stream = L->up = L->down = nullptr;
+}
+
+static int lane_init(tbs_server *s, SrvLane *L, int id) {
+    L->id = id;
+    if (cudaStreamCreateWithFlags(&L->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&L->up, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&L->down, cudaStreamNonBlocking) != cudaSuccess)
+        return lfail(L, TBS_ERR_CUDA, "cudaStreamCreate failed");
+    if (cudaEventCreateWithFlags(&L->ev_up, cudaEventDisableTiming) != cudaSuccess)
+        return lfail(L, TBS_ERR_CUDA, "cudaEventCreate failed");
+    if (cudaMallocHost(&L->h_states, sizeof(SolveState) * (size_t)s->max_slots) != cudaSuccess ||
+        cudaMallocHost(&L->h_up_states, sizeof(SolveState) * (size_t)s->max_slots) != cudaSuccess)
+        return lfail(L, TBS_ERR_NOMEM, "pinned allocation failed");
+    int rc = engine_init(L->eng, s->device, L->stream, s->algo);
+    if (rc) return lfail(L, rc, L->eng.err);
+    return TBS_OK;
+}
 
 static void server_stop(tbs_server *s) {
     {
@@ -626,7 +690,8 @@ static void server_stop(tbs_server *s) {
         s->queue.clear();
         s->cv_loop.notify_all();
     }
-    if (s->loop.joinable()) s->loop.join();
+    for (auto &L : s->lanes)
+        if (L->th.joinable()) L->th.join();
 }
 
 extern "C" {
@@ -647,7 +712,9 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
     tbs_server *s = nullptr;
     try {
         s = new tbs_server();
+        for (int k = 0; k < 2; ++k) s->lanes.emplace_back(new SrvLane());
     } catch (...) {
+        delete s;
         return sfail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
     }
     s->device = device_id;
@@ -655,26 +722,16 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
     s->budget = device_budget_bytes;
     s->max_slots = max_rhs_in_flight;
     auto fail = [&](int code, const std::string &msg) {
-        if (s->eng.h_ctl) engine_free(s->eng);
+        for (auto &L : s->lanes) lane_free(L.get());
         if (s->pool) cudaMemPoolDestroy(s->pool);
-        if (s->h_states) cudaFreeHost(s->h_states);
-        if (s->h_up_states) cudaFreeHost(s->h_up_states);
-        if (s->ev_up) cudaEventDestroy(s->ev_up);
-        for (cudaStream_t x : {s->stream, s->up, s->down})
-            if (x) cudaStreamDestroy(x);
         delete s;
         return sfail(nullptr, code, msg);
     };
     if (cudaSetDevice(device_id) != cudaSuccess) return fail(TBS_ERR_CUDA, "cudaSetDevice failed");
-    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&s->up, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaStreamCreateWithFlags(&s->down, cudaStreamNonBlocking) != cudaSuccess)
-        return fail(TBS_ERR_CUDA, "cudaStreamCreate failed");
-    if (cudaEventCreateWithFlags(&s->ev_up, cudaEventDisableTiming) != cudaSuccess)
-        return fail(TBS_ERR_CUDA, "cudaEventCreate failed");
-    if (cudaMallocHost(&s->h_states, sizeof(SolveState) * (size_t)max_rhs_in_flight) != cudaSuccess ||
-        cudaMallocHost(&s->h_up_states, sizeof(SolveState) * (size_t)max_rhs_in_flight) != cudaSuccess)
-        return fail(TBS_ERR_NOMEM, "pinned allocation failed");
+    for (size_t k = 0; k < s->lanes.size(); ++k) {
+        int rc = lane_init(s, s->lanes[k].get(), (int)k);
+        if (rc) return fail(rc, s->lanes[k]->err);
+    }
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.location.type = cudaMemLocationTypeDevice;
@@ -683,17 +740,19 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
         return fail(TBS_ERR_CUDA, "cudaMemPoolCreate failed");
     uint64_t keep = ~0ull; /* freed right-hand-side memory stays in the pool */
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
-    int rc = engine_init(s->eng, device_id, s->stream, algo);
-    if (rc) return fail(rc, s->eng.err);
     try {
-        s->loop = std::thread(loop_main, s);
+        for (auto &L : s->lanes) L->th = std::thread(loop_main, s, L.get());
         s->factor = std::thread(factor_main, s);
     } catch (...) {
-        s->stopping = true;
-        if (s->loop.joinable()) {
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            s->stopping = true;
             s->cv_loop.notify_all();
-            s->loop.join();
+            s->cv_factor.notify_all();
         }
+        for (auto &L : s->lanes)
+            if (L->th.joinable()) L->th.join();
+        if (s->factor.joinable()) s->factor.join();
         return fail(TBS_ERR_STATE, "thread start failed");
     }
     *out = s;
@@ -704,20 +763,21 @@ int tbs_server_destroy(tbs_server *s) {
     if (!s) return TBS_OK;
     server_stop(s);
     cudaSetDevice(s->device);
-    for (cudaStream_t x : {s->stream, s->up, s->down})
-        if (x) cudaStreamSynchronize(x);
-    engine_free(s->eng);
+    for (auto &L : s->lanes) lane_free(L.get());
     for (SrvSystem &sys : s->systems)
         for (tbs_ctx *c : sys.ctx)
             if (c) tbs_destroy(c);
-    for (cudaEvent_t e : s->ev_pool) cudaEventDestroy(e);
-    if (s->ev_up) cudaEventDestroy(s->ev_up);
-    if (s->h_states) cudaFreeHost(s->h_states);
-    if (s->h_up_states) cudaFreeHost(s->h_up_states);
     if (s->pool) cudaMemPoolDestroy(s->pool);
-    for (cudaStream_t x : {s->stream, s->up, s->down})
-        if (x) cudaStreamDestroy(x);
     delete s;
+    return TBS_OK;
+}
+
+int tbs_server_set_lanes(tbs_server *s, long long split_cells) {
+    if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
+    if (split_cells < 0) return sfail(s, TBS_ERR_ARG, "negative split");
+    std::lock_guard<std::mutex> lk(s->mu);
+    if (!s->systems.empty()) return sfail(s, TBS_ERR_STATE, "lanes are set before systems are added");
+    s->lane_split = split_cells;
     return TBS_OK;
 }
 
@@ -766,6 +826,7 @@ int tbs_server_add_system(tbs_server *s, int nvar, int nelem, int nintface, int 
     SrvSystem sys;
     sys.ctx[0] = c;
     sys.bytes = bytes;
+    sys.lane = (s->lane_split > 0 && nelem >= s->lane_split) ? 1 : 0;
     s->systems.push_back(sys);
     *system_id = (int)s->systems.size() - 1;
     return TBS_OK;

@@ -58,13 +58,15 @@ class Request:
 
 class Server:
     def __init__(self, device_id: int = 0, algo: int = N.ALGO_FP64, budget_bytes: int = 32 << 30,
-                 max_rhs: int = 64, chunk: int | None = None):
+                 max_rhs: int = 64, chunk: int | None = None, lane_split: int | None = None):
         h = C.c_void_p()
         N.check_server(N.lib.tbs_server_create(device_id, algo, budget_bytes, max_rhs, C.byref(h)))
         self.handle = h
         self.nelem = {}
         if chunk is not None:
             self.set_chunk(chunk)
+        if lane_split is not None:
+            self._chk(N.lib.tbs_server_set_lanes(self.handle, lane_split))
 
     def _chk(self, rc):
         N.check_server(rc, self.handle)
