@@ -740,7 +740,8 @@ def main():
     max_sweeps = 400
     inner = None
     if args.algo == "mixed":
-        inner, _ = solver.tune_inner(tol, max_sweeps)
+        solver.tune_inner(tol, max_sweeps)
+        inner = list(solver.inner_schedule())  # [first outer step, the others]
 
     with ClockSampler(local) as clocks:
         for _ in range(max(args.warmup, 0)):

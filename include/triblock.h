@@ -229,12 +229,20 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out);
 int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes);
 
 /* TBS_ALGO_MIXED: FP32 inner sweeps per FP64 outer refinement step
- * (default 4, range 1..64). */
+ * (default 4, range 1..64), the same for every outer step. */
 int tbs_set_inner_sweeps(tbs_ctx *ctx, int m);
 
+/* TBS_ALGO_MIXED: `first` inner sweeps in the first outer step of a solve
+ * (or of a tbs_sweep sequence after a new rhs, initial solution or
+ * factorization), `rest` in the others. */
+int tbs_set_inner_schedule(tbs_ctx *ctx, int first, int rest);
+int tbs_get_inner_schedule(const tbs_ctx *ctx, int *first, int *rest);
+
 /* Autotuner for TBS_ALGO_MIXED: times a solve to rel_tol on the device for
- * each inner sweep count in {2,3,4,5,6,8,10}, keeps the fastest that
- * converges (set in the context) and reports it and its time in ms. */
+ * each uniform inner sweep count in {2,3,4,5,6,8,10}, then for first-step
+ * counts within 2 of the best and steady counts within 1 of it; keeps the
+ * fastest schedule that converges (set in the context) and reports its
+ * steady count and its time in ms (tbs_get_inner_schedule gives both). */
 int tbs_tune_inner(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *best_m,
                    double *best_ms);
 
@@ -314,9 +322,11 @@ int tbs_batch_get_schedule(const tbs_batch *batch, int *ctas_per_sm, int *stages
 int tbs_batch_tune(tbs_batch *batch, int *ctas_per_sm, int *stages, int *order,
                    double *best_ms);
 
-/* TBS_ALGO_MIXED: FP32 inner sweeps per outer step for every member
- * (default: the first member's setting). */
+/* TBS_ALGO_MIXED: FP32 inner sweeps per outer step for every member, or
+ * a first-step / steady schedule as tbs_set_inner_schedule (default: the
+ * first member's setting). */
 int tbs_batch_set_inner_sweeps(tbs_batch *batch, int m);
+int tbs_batch_set_inner_schedule(tbs_batch *batch, int first, int rest);
 
 /* Per-kernel CUDA-event timing of batched solves (eager launches while
  * enabled), as tbs_profile_*. */

@@ -145,6 +145,21 @@ def test_batch_initial_and_refactor(algo):
         close_all(members, b)
 
 
+def test_batch_inner_schedule_equals_alone():
+    members = make_members(ALGO_MIXED, pick={0, 1, 4, 6})
+    for s, _, _ in members:
+        s.set_inner_schedule(3, 5)
+    b = Batch([m[0] for m in members])   # takes the first member's schedule
+    try:
+        batch_vs_alone(members, b, 1e-10, 80)
+        b.set_inner_schedule(2, 4)
+        for s, _, _ in members:
+            s.set_inner_schedule(2, 4)
+        batch_vs_alone(members, b, 1e-10, 80)
+    finally:
+        close_all(members, b)
+
+
 def test_batch_sweep_limit_and_inner():
     members = make_members(ALGO_MIXED, pick={0, 4})
     b = Batch([m[0] for m in members])

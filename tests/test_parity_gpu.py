@@ -177,3 +177,31 @@ def test_tune_inner_picks_a_converging_count(solver):
     assert m in (2, 3, 4, 5, 6, 8, 10) and ms > 0
     sweeps, h = solver.solve(1e-10, 60)
     assert h[-1] <= 1e-10 * h[0]
+
+
+def test_mixed_inner_schedule(solver):
+    """A first outer step with its own inner sweep count: the graph solve,
+    the eager (profiled) solve and a tbs_sweep sequence give the same
+    iterates, and the solve still reaches the FP64 tolerance."""
+    mesh = Mesh.structured(40, 48)
+    jac = Jacobian.generate(mesh, 4.0, 3)
+    setup(solver, mesh, jac, ALGO_MIXED)
+    solver.set_inner_schedule(2, 4)
+    assert solver.inner_schedule() == (2, 4)
+    n, h = solver.solve(1e-10, 60)
+    assert h[-1] <= 1e-10 * h[0]
+    U = solver.solution()
+    solver.profile(True)
+    n2, h2 = solver.solve(1e-10, 60)
+    solver.profile(False)
+    assert n2 == n
+    np.testing.assert_array_equal(h2, h)
+    np.testing.assert_array_equal(solver.solution(), U)
+    solver.set_rhs(jac.rhs)  # a new start: the next sweep is a first step
+    h3 = solver.sweep(n)
+    np.testing.assert_array_equal(h3, h)
+    np.testing.assert_array_equal(solver.solution(), U)
+    # a different first step changes the iterates (the schedule is in effect)
+    solver.set_inner_schedule(4, 4)
+    _, h4 = solver.solve(1e-10, 60)
+    assert h4[1] != h[1]

@@ -86,6 +86,8 @@ _sig("tbs_true_residual_norm", _i, _vp, _dp)
 _sig("tbs_memory_allocated", _i, _vp, C.POINTER(C.c_size_t))
 _sig("tbs_set_inner_sweeps", _i, _vp, _i)
 _sig("tbs_tune_inner", _i, _vp, C.c_double, _i, _ip, _dp)
+_sig("tbs_set_inner_schedule", _i, _vp, _i, _i)
+_sig("tbs_get_inner_schedule", _i, _vp, _ip, _ip)
 _sig("tbs_profile_enable", _i, _vp, _i)
 _sig("tbs_profile_reset", _i, _vp)
 _sig("tbs_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)
@@ -101,6 +103,7 @@ _sig("tbs_batch_set_schedule", _i, _vp, _i, _i, _i)
 _sig("tbs_batch_get_schedule", _i, _vp, _ip, _ip, _ip)
 _sig("tbs_batch_tune", _i, _vp, _ip, _ip, _ip, _dp)
 _sig("tbs_batch_set_inner_sweeps", _i, _vp, _i)
+_sig("tbs_batch_set_inner_schedule", _i, _vp, _i, _i)
 _sig("tbs_batch_profile_enable", _i, _vp, _i)
 _sig("tbs_batch_profile_reset", _i, _vp)
 _sig("tbs_batch_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)

@@ -125,7 +125,8 @@ static void drop_mesh(tbs_ctx *ctx) {
                       &ctx->d_R, &ctx->d_Uinit, &ctx->d_scratch, &ctx->d_DLU, &ctx->d_DinvC,
                       &ctx->d_A, &ctx->d_Dinv, &ctx->d_G, &ctx->d_Gam, &ctx->d_X, &ctx->d_Up,
                       &ctx->d_dUp, &ctx->d_b, &ctx->d_y, &ctx->d_rhsp, &ctx->d_Rp,
-                      &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist, &ctx->d_gamlast};
+                      &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist, &ctx->d_gamlast,
+                      &ctx->d_Dp, &ctx->d_XF};
     for (auto p : dps) *p = nullptr;
     float **fps[] = {&ctx->d_Dinv32, &ctx->d_G32, &ctx->d_Gam32, &ctx->d_X32, &ctx->d_b32,
                      &ctx->d_y32, &ctx->d_d32, &ctx->d_c32, &ctx->d_R32};
@@ -133,7 +134,7 @@ static void drop_mesh(tbs_ctx *ctx) {
     int **ips[] = {&ctx->d_epoint, &ctx->d_ef, &ctx->d_fc, &ctx->d_linesize, &ctx->d_linepoint,
                    &ctx->d_lines, &ctx->d_lineface, &ctx->d_identity, &ctx->L.line_start,
                    &ctx->L.line_len, &ctx->L.line_twist, &ctx->L.pos_of_elem, &ctx->L.elem_of_pos, &ctx->L.xnbr,
-                   &ctx->L.xsrc, &ctx->L.fsrc};
+                   &ctx->L.xsrc, &ctx->L.fsrc, &ctx->L.xsrcf, &ctx->L.xnbrf};
     for (auto p : ips) *p = nullptr;
     ctx->d_state = nullptr;
     ctx->d_status = nullptr;
@@ -289,14 +290,40 @@ static int build_layout(tbs_ctx *ctx) {
             xsrc[q * (size_t)np16 + p] = xs[p][q].first;
             xnbr[q * (size_t)np16 + p] = xs[p][q].second;
         }
+    /* all-face slots (in-line and cross-line, ef order): the full residual
+     * in position order (TBS_ALGO_MIXED's outer residual) */
+    int nxf = 0;
+    long long nfreal = 0;
+    for (int e = 0; e < nelem; ++e) {
+        int cnt = 0;
+        for (int k2 = ep[e]; k2 < ep[e + 1]; ++k2) cnt += ef[k2] >= 0;
+        nxf = std::max(nxf, cnt);
+        nfreal += cnt;
+    }
+    const int nxfa = std::max(nxf, 1);
+    std::vector<int> xsrcf((size_t)np16 * nxfa, -1), xnbrf((size_t)np16 * nxfa, -1);
+    for (int e = 0; e < nelem; ++e) {
+        const int p = pos_of_elem[e];
+        int q = 0;
+        for (int k2 = ep[e]; k2 < ep[e + 1]; ++k2) {
+            const int f = ef[k2];
+            if (f < 0) continue;
+            const bool is1 = (e == fc[2 * f]);
+            xsrcf[q * (size_t)np16 + p] = 2 * f + (is1 ? 1 : 0);
+            xnbrf[q * (size_t)np16 + p] = pos_of_elem[is1 ? fc[2 * f + 1] : fc[2 * f]];
+            ++q;
+        }
+    }
     FastLayout &L = ctx->L;
     L.nv = ctx->nvar;
     L.np = (int)np;
     L.np16 = np16;
     L.nx = nx;
+    L.nxf = nxf;
     L.nline = nline;
     L.max_len = ctx->max_line;
     ctx->n_xslots_real = nreal;
+    ctx->n_fslots_real = nfreal;
     DA(L.line_start, nline);
     DA(L.line_len, nline);
     DA(L.line_twist, nline);
@@ -305,6 +332,8 @@ static int build_layout(tbs_ctx *ctx) {
     DA(L.fsrc, (size_t)np16 * 5);
     DA(L.xsrc, (size_t)np16 * std::max(nx, 1));
     DA(L.xnbr, (size_t)np16 * std::max(nx, 1));
+    DA(L.xsrcf, (size_t)np16 * nxfa);
+    DA(L.xnbrf, (size_t)np16 * nxfa);
     DA(ctx->d_gamlast, (size_t)nline * 2 * 81);
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(L.line_start, start.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -315,6 +344,8 @@ static int build_layout(tbs_ctx *ctx) {
     CK(cudaMemcpyAsync(L.fsrc, fsrc.data(), fsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.xsrc, xsrc.data(), xsrc.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.xnbr, xnbr.data(), xnbr.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.xsrcf, xsrcf.data(), xsrcf.size() * sizeof(int), cudaMemcpyHostToDevice, st));
+    CK(cudaMemcpyAsync(L.xnbrf, xnbrf.data(), xnbrf.size() * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaStreamSynchronize(st));
     /* the residual kernel stages RES_TILE cells x nx blocks per tile; beyond
      * 4 cross-line couplings per cell it would not fit in shared memory,
@@ -345,12 +376,18 @@ static int status_check(tbs_ctx *ctx) {
 
 static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; }
 
+/* TBS_ALGO_MIXED's outer residual streams position-ordered copies of the
+ * blocks when a cell has at most 4 interior faces (one shared-memory tile) */
+bool fullpos_ok(const tbs_ctx *ctx) { return ctx->L.nxf <= 4; }
+
 /* How a sequence ends: the norm of its residual is recorded as the start
  * of a solve (is_start) or as one more sweep, and, inside the solve graph,
  * sets the while-node's condition. */
 struct CondCtl {
     unsigned long long handle;
     int use_cond;
+    unsigned long long handle2; /* a second condition set to the same value (0: none) */
+    int use2;
 };
 
 static NormSink sink(tbs_ctx *ctx, int is_start, CondCtl cc) {
@@ -369,7 +406,8 @@ static NormSink no_sink() { return NormSink{}; }
 
 static int reduce(tbs_ctx *ctx, int npart, int is_start, CondCtl cc) {
     RUN("reduce_norm", launch_reduce_norm(ctx->stream, ctx->d_partials, npart, ctx->d_state,
-                                          ctx->d_hist, is_start, cc.handle, cc.use_cond));
+                                          ctx->d_hist, is_start, cc.handle, cc.use_cond, cc.handle2,
+                                          cc.use2));
     return TBS_OK;
 }
 
@@ -377,6 +415,7 @@ static int reduce(tbs_ctx *ctx, int npart, int is_start, CondCtl cc) {
  * ||R_0||", with the first sweep's inputs ready. */
 static int prime(tbs_ctx *ctx, CondCtl cc) {
     cudaStream_t st = ctx->stream;
+    ctx->outer_done = 0;
     const int nv = ctx->nvar, ne = ctx->nelem;
     const size_t vb = (size_t)nvec(ctx) * sizeof(double);
     if (ctx->algo == TBS_ALGO_REFERENCE) {
@@ -414,22 +453,33 @@ static int prime(tbs_ctx *ctx, CondCtl cc) {
                                                         ctx->d_Uinit ? nullptr : ctx->d_Up));
         return TBS_OK;
     }
-    /* TBS_ALGO_MIXED */
+    /* TBS_ALGO_MIXED: R32, its norm, and the first inner right-hand side
+     * b32 = -Dinv32 R32 with c32 = 0 */
     if (ctx->d_Uinit) {
         RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
         RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                    L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                    ctx->d_rhs, ctx->d_Up, ctx->d_R32,
                                                    ctx->d_partials));
+        RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
+                                                         ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status,
+                                                         ctx->d_c32));
         return reduce(ctx, full_resid_blocks(ne), 1, cc);
     }
-    RUN("mixed_prime", launch_mixed_prime(st, L, ctx->d_rhsp, ctx->d_R32, ctx->d_Up, ctx->d_partials));
+    RUN("mixed_prime", launch_mixed_prime(st, L, ctx->d_rhsp, ctx->d_R32, ctx->d_Up, ctx->d_partials,
+                                          ctx->d_Dinv32, ctx->d_b32, ctx->d_c32));
     return reduce(ctx, fast_resid_grid(L.np16), 1, cc);
 }
 
 /* One sweep from the primed state, ending with the new residual's norm
  * recorded as one more sweep. */
-static int body(tbs_ctx *ctx, CondCtl cc) {
+/* the inner FP32 sweeps of the next TBS_ALGO_MIXED outer step */
+static int inner_for_next(const tbs_ctx *ctx) {
+    return (ctx->outer_done == 0 && ctx->inner_first > 0) ? ctx->inner_first : ctx->inner_sweeps;
+}
+
+static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
+    ctx->outer_done += 1;
     cudaStream_t st = ctx->stream;
     const int nv = ctx->nvar, ne = ctx->nelem;
     if (ctx->algo == TBS_ALGO_REFERENCE) {
@@ -456,22 +506,31 @@ static int body(tbs_ctx *ctx, CondCtl cc) {
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
      * FP64 residual R = rhs + J U from the original blocks */
-    /* c = sum of the inner updates but the last: this launch clears c, each
-     * inner residual kernel adds its sweep's d to c; the last d is added
-     * with c to U below */
-    RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
-                                                     ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status,
-                                                     ctx->d_c32));
-    for (int m = 0; m < ctx->inner_sweeps; ++m) {
+    /* b32 = -Dinv32 R32 and c = 0 come from the previous step's residual
+     * (or the prime) when the position-ordered residual runs; c = sum of
+     * the inner updates but the last: each inner residual kernel adds its
+     * sweep's d to c; the last d is added with c to U below */
+    const bool pos = fullpos_ok(ctx);
+    if (!pos)
+        RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
+                                                         ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status,
+                                                         ctx->d_c32));
+    for (int m = 0; m < inner; ++m) {
         RUN("fast_thomas32", launch_fast_thomas<float>(st, L, ctx->d_G32, ctx->d_Gam32, ctx->d_b32,
                                                        ctx->d_y32, ctx->d_d32, ctx->d_c32,
                                                        ctx->d_status, 2));
-        if (m + 1 < ctx->inner_sweeps)
+        if (m + 1 < inner)
             RUN("fast_resid32", launch_fast_resid<float>(st, L, 3, nullptr, ctx->d_X32, ctx->d_d32,
                                                          nullptr, ctx->d_b32, no_sink(),
                                                          ctx->d_status, ctx->d_c32));
     }
     RUN("axpy", launch_axpy2_f32_f64(st, ctx->d_c32, ctx->d_d32, ctx->d_Up, (long long)L.np16 * 9));
+    if (pos) {
+        RUN("full_resid", launch_full_resid_pos(st, L, ctx->d_Dp, ctx->d_XF, ctx->d_rhsp, ctx->d_Up,
+                                                ctx->d_R32, ctx->d_partials, ctx->d_Dinv32, ctx->d_b32,
+                                                ctx->d_c32, ctx->d_status));
+        return reduce(ctx, fast_resid_grid(L.np16), 0, cc);
+    }
     RUN("full_resid", launch_full_resid<float>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                ctx->d_rhs, ctx->d_Up, ctx->d_R32, ctx->d_partials));
@@ -509,52 +568,72 @@ static int read_state(tbs_ctx *ctx) {
     return TBS_OK;
 }
 
-/* Graph: prime (records ||R_0||, sets the condition) -> while (cond) { sweep } */
+/* capture `fn` into the body graph of a conditional node */
+template <typename F>
+static int capture_into(tbs_ctx *ctx, cudaGraph_t g, F &&fn) {
+    cudaStream_t st = ctx->stream;
+    CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = fn();
+    cudaGraph_t outg = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(st, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess)
+        rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    return rc;
+}
+
+/* append a conditional node (type) after the capture's current nodes;
+ * returns its body graph */
+static int add_conditional(tbs_ctx *ctx, cudaGraph_t g, cudaGraphConditionalHandle h,
+                           cudaGraphConditionalNodeType type, cudaGraph_t *body_out) {
+    cudaStream_t st = ctx->stream;
+    cudaStreamCaptureStatus cs;
+    const cudaGraphNode_t *deps = nullptr;
+    size_t ndeps = 0;
+    cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
+    if (e != cudaSuccess) return ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(e));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    e = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+    if (e != cudaSuccess) return ctx_fail(ctx, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(e));
+    *body_out = cp.conditional.phGraph_out[0];
+    e = cudaStreamUpdateCaptureDependencies(st, &node, 1, cudaStreamSetCaptureDependencies);
+    if (e != cudaSuccess) return ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(e));
+    return TBS_OK;
+}
+
+/* Graph: prime (records ||R_0||, sets the condition) -> while (cond) { sweep }.
+ * TBS_ALGO_MIXED with its own inner sweep count for the first outer step:
+ * prime -> if (cond) { first step } -> while (cond) { step }, the prime
+ * setting both conditions and every step the loop's. */
 static int build_graph(tbs_ctx *ctx) {
     drop_graph(ctx);
     cudaStream_t st = ctx->stream;
     cudaGraph_t g = nullptr;
     CK(cudaGraphCreate(&g, 0));
     ctx->graph = g;
-    cudaGraphConditionalHandle h;
-    CK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    const CondCtl cc{(unsigned long long)h, 1};
+    const bool sched = ctx->algo == TBS_ALGO_MIXED && ctx->inner_first > 0 &&
+                       ctx->inner_first != ctx->inner_sweeps;
+    cudaGraphConditionalHandle hw, hf = 0;
+    CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+    if (sched) CK(cudaGraphConditionalHandleCreate(&hf, g, 0, cudaGraphCondAssignDefault));
+    const CondCtl loop{(unsigned long long)hw, 1, 0, 0};
+    const CondCtl both{(unsigned long long)hw, 1, (unsigned long long)hf, sched ? 1 : 0};
     CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = prime(ctx, cc);
-    cudaStreamCaptureStatus cs;
-    const cudaGraphNode_t *deps = nullptr;
-    size_t ndeps = 0;
-    if (rc == TBS_OK) {
-        cudaError_t e = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
-        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(e));
-    }
-    cudaGraphNode_t cnode = nullptr;
-    cudaGraph_t bodyg = nullptr;
-    if (rc == TBS_OK) {
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaError_t e = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
-        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(e));
-        else bodyg = cp.conditional.phGraph_out[0];
-    }
-    if (rc == TBS_OK) {
-        cudaError_t e = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
-        if (e != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(e));
-    }
+    int rc = prime(ctx, both);
+    cudaGraph_t firstg = nullptr, bodyg = nullptr;
+    if (rc == TBS_OK && sched) rc = add_conditional(ctx, g, hf, cudaGraphCondTypeIf, &firstg);
+    if (rc == TBS_OK) rc = add_conditional(ctx, g, hw, cudaGraphCondTypeWhile, &bodyg);
     cudaGraph_t outg = nullptr;
     cudaError_t ee = cudaStreamEndCapture(st, &outg);
     if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
-    if (rc != TBS_OK) {
-        drop_graph(ctx);
-        return rc;
-    }
-    CK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = body(ctx, cc);
-    ee = cudaStreamEndCapture(st, &outg);
-    if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    if (rc == TBS_OK && sched)
+        rc = capture_into(ctx, firstg, [&]() { return body(ctx, loop, ctx->inner_first); });
+    if (rc == TBS_OK)
+        rc = capture_into(ctx, bodyg, [&]() { return body(ctx, loop, ctx->inner_sweeps); });
     if (rc != TBS_OK) {
         drop_graph(ctx);
         return rc;
@@ -613,6 +692,10 @@ static int alloc_algo(tbs_ctx *ctx, int algo) {
         DA(ctx->d_G32, npb);
         DA(ctx->d_Gam32, npb);
         DA(ctx->d_X32, nxb); /* holds DX = Dinv X in FP32 */
+        if (fullpos_ok(ctx)) {
+            DA(ctx->d_Dp, npb);
+            DA(ctx->d_XF, (size_t)L.np16 * L.nxf * bs);
+        }
         DA(ctx->d_b32, npv);
         DA(ctx->d_y32, npv);
         DA(ctx->d_d32, npv);
@@ -652,6 +735,11 @@ static int run_factor(tbs_ctx *ctx, int algo) {
                                               nullptr, nullptr, ctx->d_Dinv32, ctx->d_G32,
                                               ctx->d_Gam32, ctx->d_gamlast, ctx->d_status));
         RUN("fast_dx", launch_fast_dx(st, L, ctx->d_Dinv, ctx->d_O1, ctx->d_O2, ctx->d_X32));
+        if (fullpos_ok(ctx)) {
+            CKL(fullpos_prepare(L));
+            RUN("fullpos_layout", launch_fullpos_layout(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                        ctx->d_Dp, ctx->d_XF));
+        }
     }
     return TBS_OK;
 }
@@ -848,7 +936,7 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
     ctx->factored = false;
     rc = run_factor(ctx, algo);
     if (rc) return rc;
-    rc = prime(ctx, CondCtl{0, 0});
+    rc = prime(ctx, CondCtl{});
     if (rc) return rc;
     rc = status_check(ctx);
     if (rc) return rc;
@@ -869,7 +957,7 @@ int tbs_set_rhs(tbs_ctx *ctx, const double *rhs) {
         RUN("permute", launch_permute_to_pos(ctx->stream, 9, ctx->nelem, ctx->L.pos_of_elem, ctx->d_rhs,
                                              ctx->d_rhsp));
     }
-    return prime(ctx, CondCtl{0, 0});
+    return prime(ctx, CondCtl{});
     GUARD_END
 }
 
@@ -886,7 +974,7 @@ int tbs_set_initial(tbs_ctx *ctx, const double *U) {
         dfree(ctx, &ctx->d_Uinit);
     }
     drop_graph(ctx);
-    return prime(ctx, CondCtl{0, 0});
+    return prime(ctx, CondCtl{});
     GUARD_END
 }
 
@@ -902,10 +990,10 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
     if (rc) return rc;
     cudaStream_t st = ctx->stream;
     /* the current residual norm (recorded by the last sequence) opens the history */
-    rc = reduce(ctx, 0, 1, CondCtl{0, 0});
+    rc = reduce(ctx, 0, 1, CondCtl{});
     if (rc) return rc;
     for (int s = 0; s < n; ++s) {
-        rc = body(ctx, CondCtl{0, 0});
+        rc = body(ctx, CondCtl{}, inner_for_next(ctx));
         if (rc) return rc;
     }
     if (rnorm_out)
@@ -929,7 +1017,7 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
     cudaStream_t st = ctx->stream;
     if (ctx->prof) {
         /* eager form with a host-side test, so that every kernel is timed */
-        rc = prime(ctx, CondCtl{0, 0});
+        rc = prime(ctx, CondCtl{});
         if (rc) return rc;
         for (;;) {
             rc = read_state(ctx);
@@ -937,7 +1025,7 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
             const SolveState &S = *ctx->h_state;
             const bool go = std::isfinite(S.last) && S.last > S.tol * S.norm0 && S.sweep < S.max_sweeps;
             if (!go) break;
-            rc = body(ctx, CondCtl{0, 0});
+            rc = body(ctx, CondCtl{}, inner_for_next(ctx));
             if (rc) return rc;
         }
         prof_resolve(ctx);
@@ -947,6 +1035,7 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
             if (rc) return rc;
         }
         CK(cudaGraphLaunch(ctx->gexec, st));
+        ctx->outer_done = 1; /* later tbs_sweep calls continue with the steady schedule */
         rc = read_state(ctx);
         if (rc) return rc;
     }
@@ -1056,11 +1145,47 @@ int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes) {
     return TBS_OK;
 }
 
-int tbs_set_inner_sweeps(tbs_ctx *ctx, int m) {
+int tbs_set_inner_sweeps(tbs_ctx *ctx, int m) { return tbs_set_inner_schedule(ctx, m, m); }
+
+int tbs_set_inner_schedule(tbs_ctx *ctx, int first, int rest) {
     if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
-    if (m < 1 || m > 64) return ctx_fail(ctx, TBS_ERR_ARG, "inner sweeps must be in 1..64");
-    if (m != ctx->inner_sweeps) drop_graph(ctx);
-    ctx->inner_sweeps = m;
+    if (first < 1 || first > 64 || rest < 1 || rest > 64)
+        return ctx_fail(ctx, TBS_ERR_ARG, "inner sweeps must be in 1..64");
+    const int f = first == rest ? 0 : first;
+    if (rest != ctx->inner_sweeps || f != ctx->inner_first) drop_graph(ctx);
+    ctx->inner_sweeps = rest;
+    ctx->inner_first = f;
+    return TBS_OK;
+}
+
+int tbs_get_inner_schedule(const tbs_ctx *ctx, int *first, int *rest) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    if (first) *first = ctx->inner_first > 0 ? ctx->inner_first : ctx->inner_sweeps;
+    if (rest) *rest = ctx->inner_sweeps;
+    return TBS_OK;
+}
+
+/* device time of a solve to rel_tol with the schedule (first, rest): best
+ * of two after a warm-up; +inf when it does not reach the tolerance */
+static int time_schedule(tbs_ctx *ctx, int first, int rest, double rel_tol, int max_sweeps,
+                         cudaEvent_t e0, cudaEvent_t e1, double *ms_out) {
+    int rc = tbs_set_inner_schedule(ctx, first, rest);
+    int sw = 0;
+    if (!rc) rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr); /* builds the graph */
+    double t = 1e300;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+        cudaEventRecord(e0, ctx->stream);
+        rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr);
+        cudaEventRecord(e1, ctx->stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t = std::min(t, (double)ms);
+    }
+    if (rc) return rc;
+    const SolveState &S = *ctx->h_state;
+    const bool conv = std::isfinite(S.last) && S.last <= S.tol * S.norm0;
+    *ms_out = conv ? t : 1e300;
     return TBS_OK;
 }
 
@@ -1070,46 +1195,43 @@ int tbs_tune_inner(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *best_m, do
     CK(cudaSetDevice(ctx->device));
     if (!ctx->factored || ctx->algo != TBS_ALGO_MIXED)
         return ctx_fail(ctx, TBS_ERR_STATE, "tbs_tune_inner needs a TBS_ALGO_MIXED factorization");
-    const int cand[] = {2, 3, 4, 5, 6, 8, 10};
     const bool prof = ctx->prof;
     ctx->prof = false;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    int best = -1;
-    double best_t = 0.0;
+    int bf = -1, br = -1;
+    double best_t = 1e300;
     int rc = TBS_OK;
-    for (int m : cand) {
-        if (rc) break;
-        rc = tbs_set_inner_sweeps(ctx, m);
-        int sw = 0;
-        if (!rc) rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr); /* builds the graph */
+    auto consider = [&](int f, int r) {
+        if (rc || f < 1 || r < 1) return;
         double t = 1e300;
-        for (int rep = 0; rep < 2 && !rc; ++rep) {
-            cudaEventRecord(e0, ctx->stream);
-            rc = tbs_solve(ctx, rel_tol, max_sweeps, &sw, nullptr);
-            cudaEventRecord(e1, ctx->stream);
-            cudaEventSynchronize(e1);
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, e0, e1);
-            t = std::min(t, (double)ms);
-        }
-        if (rc) break;
-        const SolveState &S = *ctx->h_state;
-        const bool conv = std::isfinite(S.last) && S.last <= S.tol * S.norm0;
-        if (conv && (best < 0 || t < best_t)) {
-            best = m;
+        rc = time_schedule(ctx, f, r, rel_tol, max_sweeps, e0, e1, &t);
+        if (!rc && t < best_t) {
             best_t = t;
+            bf = f;
+            br = r;
         }
+    };
+    /* one count for every outer step, then the first step's own count
+     * around the best one (the first step starts from the largest
+     * residual, and one inner sweep fewer or more there can save an outer
+     * step or an inner sweep overall) */
+    for (int m : {2, 3, 4, 5, 6, 8, 10}) consider(m, m);
+    if (!rc && br > 0) {
+        const int m = br;
+        for (int r : {m - 1, m, m + 1})
+            for (int f : {m - 2, m - 1, m, m + 1, m + 2})
+                if (!(f == r && (r == m - 1 || r == m || r == m + 1))) consider(f, r);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
     ctx->prof = prof;
     if (rc) return rc;
-    if (best < 0) return ctx_fail(ctx, TBS_ERR_NUMERIC, "no inner sweep count reached the tolerance");
-    rc = tbs_set_inner_sweeps(ctx, best);
+    if (bf < 0) return ctx_fail(ctx, TBS_ERR_NUMERIC, "no inner sweep schedule reached the tolerance");
+    rc = tbs_set_inner_schedule(ctx, bf, br);
     if (rc) return rc;
-    if (best_m) *best_m = best;
+    if (best_m) *best_m = br;
     if (best_ms) *best_ms = best_t;
     return TBS_OK;
     GUARD_END
@@ -1166,6 +1288,11 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
         b = N * (2 * blk + 2 * vec);
     else if (k == "fast_thomas32")
         b = N * (2 * blk + 2 * vec) / 2;
+    else if (k == "full_resid" && ctx->algo == TBS_ALGO_MIXED && fullpos_ok(ctx))
+        /* position order: D, one block + index + neighbour U per face slot, own U, rhs, R32
+         * out, and the next inner right-hand side: Dinv32 in, b32 and c32 out */
+        b = N * blk + (double)ctx->n_fslots_real * (blk + 4.0 + vec) + N * (2 * vec + vec / 2) +
+            N * (blk / 2 + vec);
     else if (k == "full_resid") /* D, 2 blocks per face, U (own + nbrs), rhs, R out, ints */
         b = N * blk + 2 * F * blk + N * vec + 2 * F * vec + N * vec + N * vec / 2 +
             4.0 * (N + 1 + ctx->eftot + 2 * F + N);

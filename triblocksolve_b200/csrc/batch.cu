@@ -283,6 +283,7 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         efree_async(e, &e.d_rs32_rhs);
         efree_async(e, &e.d_rs32_dx);
         efree_async(e, &e.d_fr);
+        efree_async(e, &e.d_fp);
         efree_async(e, &e.d_vec);
         efree_async(e, &e.d_red_prime);
         efree_async(e, &e.d_red_body);
@@ -299,6 +300,7 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
             if (!rc) rc = ealloc_async(e, &e.d_rs32_rhs, c);
             if (!rc) rc = ealloc_async(e, &e.d_rs32_dx, c);
             if (!rc) rc = ealloc_async(e, &e.d_fr, c);
+            if (!rc) rc = ealloc_async(e, &e.d_fp, c);
             if (!rc) rc = ealloc_async(e, &e.d_vec, c);
         }
         if (!rc) rc = ealloc_async(e, &e.d_red_prime, c);
@@ -415,7 +417,14 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
     std::vector<ResidSys<double>> rsp, rsb;
     std::vector<ResidSys<float>> rs32r, rs32d;
     std::vector<FullResSys> fr;
+    std::vector<FullPosSys> fp;
     std::vector<VecSys> vec;
+    bool fullpos = mixed;
+    int max_nxf = 0;
+    for (const Member &m : members) {
+        fullpos = fullpos && fullpos_ok(m.sys) && m.sys->d_Dp;
+        max_nxf = std::max(max_nxf, m.sys->L.nxf);
+    }
     std::vector<ReduceSys> redp, redb;
     std::vector<int> uinit;
     std::vector<char> all(n, 1), prime(n, 0);
@@ -445,16 +454,20 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
                              nullptr});
             fr.push_back({c->nelem, 0, c->d_epoint, c->d_ef, c->d_fc, L.pos_of_elem, c->d_jacD, c->d_O1,
                           c->d_O2, v.rhs, v.Up, v.R32, v.partials});
-            vec.push_back({v.rhsp, v.R32, v.c32, v.d32, v.Up, v.partials});
+            fp.push_back({L.np16, L.nxf, L.xnbrf, c->d_Dp, c->d_XF, v.rhsp, v.Up, v.R32, v.partials,
+                          c->d_Dinv32, v.b32, v.c32});
+            vec.push_back({v.rhsp, v.R32, v.c32, v.d32, v.Up, v.partials, c->d_Dinv32, v.b32});
             if (m.fresh) redp.push_back({v.partials, ui ? full_resid_blocks(c->nelem) : nt, k, v.state, v.hist});
-            redb.push_back({v.partials, full_resid_blocks(c->nelem), k, v.state, v.hist});
+            redb.push_back({v.partials, fullpos ? nt : full_resid_blocks(c->nelem), k, v.state, v.hist});
         }
         prime[k] = m.fresh && !(mixed && ui);
         if (ui) uinit.push_back(k);
         e.h_active[k] = m.fresh ? 0 : 1;
     }
-    if (uinit != e.uinit) {
+    if (uinit != e.uinit || fullpos != e.fullpos || max_nxf > e.max_nxf) {
         e.uinit = uinit;
+        e.fullpos = fullpos;
+        e.max_nxf = std::max(e.max_nxf, max_nxf);
         engine_drop_graph(e);
     }
     /* group indices of the residual-type launches */
@@ -482,6 +495,7 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         up.put(e.d_rs32_rhs, rs32r);
         up.put(e.d_rs32_dx, rs32d);
         up.put(e.d_fr, fr);
+        up.put(e.d_fp, fp);
         up.put(e.d_vec, vec);
         up.put(e.d_g_blocks, group_index(g_all, units(g_all, true)));
     }
@@ -530,6 +544,8 @@ void engine_mark_started(Engine &e) {
 struct Cond {
     unsigned long long handle;
     int use;
+    unsigned long long handle2; /* a second condition set to the same value (0: none) */
+    int use2;
 };
 
 static int engine_prime(Engine &e, Cond cc) {
@@ -544,26 +560,32 @@ static int engine_prime(Engine &e, Cond cc) {
             ERUN("full_resid", launch_full_resid<double>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
                                                          L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
                                                          v.rhs, v.Up, v.Rp, v.partials2));
-        else
+        else {
             ERUN("full_resid", launch_full_resid<float>(st, c->nelem, c->d_epoint, c->d_ef, c->d_fc,
                                                         L.pos_of_elem, c->d_jacD, c->d_O1, c->d_O2,
                                                         v.rhs, v.Up, v.R32, v.partials));
+            /* the first inner right-hand side, as the single-system prime */
+            ERUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, c->d_Dinv32, c->d_X32, v.d32,
+                                                              v.R32, v.b32, NormSink{}, e.d_status, v.c32));
+        }
     }
     BatchCtl *C = e.d_ctl;
     if (e.algo == TBS_ALGO_FP64) {
         ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_g_prime,
                                                           nullptr, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
-                                                e.d_active, C, e.d_counter, cc.handle, cc.use));
+                                                e.d_active, C, e.d_counter, cc.handle, cc.use,
+                                                cc.handle2, cc.use2));
     } else {
         ERUN("mixed_prime", launch_mixed_prime_batch(st, e.d_vec, e.d_g_prime));
-        ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
-                                                e.d_active, C, e.d_counter, cc.handle, cc.use));
+        ERUN("reduce_norm", launch_reduce_batch(st, 1024, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
+                                                e.d_active, C, e.d_counter, cc.handle, cc.use,
+                                                cc.handle2, cc.use2));
     }
     return TBS_OK;
 }
 
-static int engine_body(Engine &e, Cond cc) {
+static int engine_body(Engine &e, Cond cc, int inner) {
     cudaStream_t st = e.stream;
     BatchCtl *C = e.d_ctl;
     if (e.algo == TBS_ALGO_FP64) {
@@ -578,67 +600,89 @@ static int engine_body(Engine &e, Cond cc) {
     /* c (the sum of the inner updates but the last) is cleared by the first
      * launch, each inner residual adds its sweep's d to it, and the last d
      * goes to U with c (the order of the single-system sequence) */
-    ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_g_tiles,
-                                                       e.d_active, e.d_status));
-    for (int m = 0; m < e.inner; ++m) {
+    if (!e.fullpos)
+        ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_g_tiles,
+                                                           e.d_active, e.d_status));
+    for (int m = 0; m < inner; ++m) {
         ERUN("fast_thomas32", launch_thomas_batch<float>(st, e.sched, e.d_th32, e.d_lines, &C->nlines,
                                                          e.d_active, e.d_queue, e.d_status));
-        if (m + 1 < e.inner)
+        if (m + 1 < inner)
             ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_g_tiles,
                                                            e.d_active, e.d_status));
     }
     ERUN("axpy", launch_axpy2_batch(st, e.d_vec, e.d_g_tiles, e.d_active));
-    ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_g_blocks, e.d_active));
-    ERUN("reduce_norm", launch_reduce_batch(st, 256, e.d_red_body, &C->nsys, e.cap_mem, 0, e.d_active,
+    if (e.fullpos)
+        ERUN("full_resid", launch_full_resid_pos_batch(st, e.max_nxf, e.d_fp, e.d_g_tiles, e.d_active,
+                                                       e.d_status));
+    else
+        ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_g_blocks, e.d_active));
+    ERUN("reduce_norm", launch_reduce_batch(st, 1024, e.d_red_body, &C->nsys, e.cap_mem, 0, e.d_active,
                                             C, e.d_counter, cc.handle, cc.use));
     return TBS_OK;
 }
 
-static int engine_build_graph(Engine &e) {
-    engine_drop_graph(e);
-    cudaStream_t st = e.stream;
-    cudaGraph_t g = nullptr;
-    ECK(cudaGraphCreate(&g, 0));
-    e.graph = g;
-    cudaGraphConditionalHandle h;
-    ECK(cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault));
-    const Cond cc{(unsigned long long)h, 1};
-    ECK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    int rc = engine_prime(e, cc);
+/* capture `fn` into a conditional node's body graph */
+template <typename F>
+static int engine_capture_into(Engine &e, cudaGraph_t g, F &&fn) {
+    ECK(cudaStreamBeginCaptureToGraph(e.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = fn();
+    cudaGraph_t outg = nullptr;
+    cudaError_t ee = cudaStreamEndCapture(e.stream, &outg);
+    if (rc == TBS_OK && ee != cudaSuccess)
+        rc = efail(e, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    return rc;
+}
+
+static int engine_add_conditional(Engine &e, cudaGraph_t g, cudaGraphConditionalHandle h,
+                                  cudaGraphConditionalNodeType type, cudaGraph_t *body_out) {
     cudaStreamCaptureStatus cs;
     const cudaGraphNode_t *deps = nullptr;
     size_t ndeps = 0;
-    if (rc == TBS_OK) {
-        cudaError_t x = cudaStreamGetCaptureInfo(st, &cs, nullptr, nullptr, &deps, &ndeps);
-        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(x));
-    }
-    cudaGraphNode_t cnode = nullptr;
-    cudaGraph_t bodyg = nullptr;
-    if (rc == TBS_OK) {
-        cudaGraphNodeParams cp{};
-        cp.type = cudaGraphNodeTypeConditional;
-        cp.conditional.handle = h;
-        cp.conditional.type = cudaGraphCondTypeWhile;
-        cp.conditional.size = 1;
-        cudaError_t x = cudaGraphAddNode(&cnode, g, deps, ndeps, &cp);
-        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(x));
-        else bodyg = cp.conditional.phGraph_out[0];
-    }
-    if (rc == TBS_OK) {
-        cudaError_t x = cudaStreamUpdateCaptureDependencies(st, &cnode, 1, cudaStreamSetCaptureDependencies);
-        if (x != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(x));
-    }
+    cudaError_t x = cudaStreamGetCaptureInfo(e.stream, &cs, nullptr, nullptr, &deps, &ndeps);
+    if (x != cudaSuccess) return efail(e, TBS_ERR_CUDA, std::string("capture info: ") + cudaGetErrorString(x));
+    cudaGraphNodeParams cp{};
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = h;
+    cp.conditional.type = type;
+    cp.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    x = cudaGraphAddNode(&node, g, deps, ndeps, &cp);
+    if (x != cudaSuccess) return efail(e, TBS_ERR_CUDA, std::string("conditional node: ") + cudaGetErrorString(x));
+    *body_out = cp.conditional.phGraph_out[0];
+    x = cudaStreamUpdateCaptureDependencies(e.stream, &node, 1, cudaStreamSetCaptureDependencies);
+    if (x != cudaSuccess) return efail(e, TBS_ERR_CUDA, std::string("capture deps: ") + cudaGetErrorString(x));
+    return TBS_OK;
+}
+
+/* prime -> while (rule) { sweep }; MIXED with its own inner count for the
+ * first outer step (all members start together, as in tbs_batch):
+ * prime -> if (rule) { first step } -> while (rule) { step } */
+static bool engine_sched(const Engine &e) {
+    return e.algo == TBS_ALGO_MIXED && e.inner_first > 0 && e.inner_first != e.inner;
+}
+
+static int engine_build_graph(Engine &e) {
+    engine_drop_graph(e);
+    cudaGraph_t g = nullptr;
+    ECK(cudaGraphCreate(&g, 0));
+    e.graph = g;
+    const bool sched = engine_sched(e);
+    cudaGraphConditionalHandle hw, hf = 0;
+    ECK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
+    if (sched) ECK(cudaGraphConditionalHandleCreate(&hf, g, 0, cudaGraphCondAssignDefault));
+    const Cond loop{(unsigned long long)hw, 1, 0, 0};
+    const Cond both{(unsigned long long)hw, 1, (unsigned long long)hf, sched ? 1 : 0};
+    ECK(cudaStreamBeginCaptureToGraph(e.stream, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
+    int rc = engine_prime(e, both);
+    cudaGraph_t firstg = nullptr, bodyg = nullptr;
+    if (rc == TBS_OK && sched) rc = engine_add_conditional(e, g, hf, cudaGraphCondTypeIf, &firstg);
+    if (rc == TBS_OK) rc = engine_add_conditional(e, g, hw, cudaGraphCondTypeWhile, &bodyg);
     cudaGraph_t outg = nullptr;
-    cudaError_t ee = cudaStreamEndCapture(st, &outg);
+    cudaError_t ee = cudaStreamEndCapture(e.stream, &outg);
     if (rc == TBS_OK && ee != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
-    if (rc != TBS_OK) {
-        engine_drop_graph(e);
-        return rc;
-    }
-    ECK(cudaStreamBeginCaptureToGraph(st, bodyg, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
-    rc = engine_body(e, cc);
-    ee = cudaStreamEndCapture(st, &outg);
-    if (rc == TBS_OK && ee != cudaSuccess) rc = efail(e, TBS_ERR_CUDA, std::string("end body capture: ") + cudaGetErrorString(ee));
+    if (rc == TBS_OK && sched)
+        rc = engine_capture_into(e, firstg, [&]() { return engine_body(e, loop, e.inner_first); });
+    if (rc == TBS_OK) rc = engine_capture_into(e, bodyg, [&]() { return engine_body(e, loop, e.inner); });
     if (rc != TBS_OK) {
         engine_drop_graph(e);
         return rc;
@@ -687,10 +731,10 @@ int engine_run(Engine &e, int chunk_limit, int stop_on_finish) {
     if (e.prof) {
         /* eager form with the graph's loop rule tested on the host, so
          * that every kernel is timed */
-        int rc = engine_prime(e, Cond{0, 0});
+        int rc = engine_prime(e, Cond{});
         if (rc) return rc;
         BatchCtl now{};
-        for (;;) {
+        for (int step = 0;; ++step) {
             ECK(cudaMemcpyAsync(&now, e.d_ctl, sizeof(BatchCtl), cudaMemcpyDeviceToHost, e.stream));
             rc = engine_read_active(e);
             if (rc) return rc;
@@ -700,7 +744,7 @@ int engine_run(Engine &e, int chunk_limit, int stop_on_finish) {
             if (chunk_limit > 0 && now.chunk >= chunk_limit) go = false;
             if (stop_on_finish && now.finished) go = false;
             if (!go) break;
-            rc = engine_body(e, Cond{0, 0});
+            rc = engine_body(e, Cond{}, (step == 0 && engine_sched(e)) ? e.inner_first : e.inner);
             if (rc) return rc;
         }
         eprof_resolve(e);
@@ -961,6 +1005,7 @@ int tbs_batch_create(tbs_ctx *const *systems, int nsys, tbs_batch **out) {
         int rc = engine_init(b->eng, dev, b->own, systems[0]->algo);
         if (rc) return fail(rc);
         b->eng.inner = systems[0]->inner_sweeps;
+        b->eng.inner_first = systems[0]->inner_first;
     } catch (...) {
         return fail(bfail(b, TBS_ERR_NOMEM, "host allocation failed"));
     }
@@ -987,11 +1032,16 @@ int tbs_batch_size(const tbs_batch *b, int *nsys) {
     return TBS_OK;
 }
 
-int tbs_batch_set_inner_sweeps(tbs_batch *b, int m) {
+int tbs_batch_set_inner_sweeps(tbs_batch *b, int m) { return tbs_batch_set_inner_schedule(b, m, m); }
+
+int tbs_batch_set_inner_schedule(tbs_batch *b, int first, int rest) {
     if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
-    if (m < 1 || m > 64) return bfail(b, TBS_ERR_ARG, "inner sweeps must be in 1..64");
-    if (m != b->eng.inner) engine_drop_graph(b->eng);
-    b->eng.inner = m;
+    if (first < 1 || first > 64 || rest < 1 || rest > 64)
+        return bfail(b, TBS_ERR_ARG, "inner sweeps must be in 1..64");
+    const int f = first == rest ? 0 : first;
+    if (rest != b->eng.inner || f != b->eng.inner_first) engine_drop_graph(b->eng);
+    b->eng.inner = rest;
+    b->eng.inner_first = f;
     return TBS_OK;
 }
 

@@ -52,13 +52,17 @@ struct tbs_ctx {
     bool layout_ok = false;
     double *d_gamlast = nullptr; /* per line and chain: last Gam toward the twist, FP64 */
     long long n_xslots_real = 0;
+    long long n_fslots_real = 0; /* interior face slots of all cells */
     double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
+    double *d_Dp = nullptr, *d_XF = nullptr; /* MIXED: position-ordered original blocks */
     double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
     double *d_rhsp = nullptr, *d_Rp = nullptr;
     float *d_Dinv32 = nullptr, *d_G32 = nullptr, *d_Gam32 = nullptr, *d_X32 = nullptr;
     float *d_b32 = nullptr, *d_y32 = nullptr, *d_d32 = nullptr, *d_c32 = nullptr,
           *d_R32 = nullptr;
-    int inner_sweeps = 4;
+    int inner_sweeps = 4;  /* TBS_ALGO_MIXED inner sweeps per outer step */
+    int inner_first = 0;   /* > 0: the first outer step's inner sweeps */
+    int outer_done = 0;    /* outer steps since the last prime (eager sequences) */
 
     /* ---- norms / solve state ---- */
     double *d_partials = nullptr, *d_partials2 = nullptr;
@@ -88,6 +92,8 @@ struct tbs_ctx {
     std::vector<cudaEvent_t> pool;
 };
 
+/* whether TBS_ALGO_MIXED's outer residual uses the position-ordered blocks */
+bool fullpos_ok(const tbs_ctx *ctx);
 /* device history of at least `need` norms (drops the cached graph when it grows) */
 int ctx_ensure_hist(tbs_ctx *ctx, int need);
 /* tolerance, sweep limit and history capacity of the device SolveState */

@@ -48,7 +48,8 @@ struct Member {
 struct Engine {
     int device = 0;
     int algo = -1;
-    int inner = 4;            /* TBS_ALGO_MIXED inner sweeps */
+    int inner = 4;            /* TBS_ALGO_MIXED inner sweeps per outer step */
+    int inner_first = 0;      /* > 0: the first outer step's (all members fresh together) */
     cudaStream_t stream = nullptr;
     BatchSched sched{8, 2};
     int order = 0;            /* Thomas items: 0 longest lines first, 1 mesh order */
@@ -63,6 +64,9 @@ struct Engine {
     ResidSys<double> *d_rs_prime = nullptr, *d_rs_body = nullptr;
     ResidSys<float> *d_rs32_rhs = nullptr, *d_rs32_dx = nullptr;
     FullResSys *d_fr = nullptr;
+    FullPosSys *d_fp = nullptr;
+    bool fullpos = false;     /* MIXED outer residual from position-ordered blocks */
+    int max_nxf = 0;
     VecSys *d_vec = nullptr;
     ReduceSys *d_red_prime = nullptr, *d_red_body = nullptr;
     WorkItem *d_lines = nullptr;                       /* Thomas items, explicit */

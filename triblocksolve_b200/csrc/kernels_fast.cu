@@ -95,21 +95,26 @@ int launch_norm_partials(cudaStream_t st, const double *v, long long n, double *
     return (int)cudaGetLastError();
 }
 
+/* threads of the one-CTA norm sum (its order: thread t adds partials t,
+ * t + REDUCE_THREADS, ..., then the warps' sums in order) */
+constexpr int REDUCE_THREADS = 1024;
+
 /* Sum the partials in a fixed order, record the norm and decide whether the
  * solve goes on.  The decision feeds the CUDA graph's while-node, so the
  * sweep loop never returns to the host.  n == 0 re-records the latest norm
  * (state->last) as the start of a new sweep sequence. */
 __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, SolveState *state,
                                    double *hist, int is_start,
-                                   cudaGraphConditionalHandle handle, int use_cond) {
-    __shared__ double red[8];
-    double acc = strided_sum(partials, n, 256);
+                                   cudaGraphConditionalHandle handle, int use_cond,
+                                   cudaGraphConditionalHandle handle2, int use2) {
+    __shared__ double red[REDUCE_THREADS / 32];
+    double acc = strided_sum(partials, n, REDUCE_THREADS);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
     if (threadIdx.x == 0) {
         double tot = 0.0;
-        for (int w = 0; w < 8; ++w) tot += red[w];
+        for (int w = 0; w < REDUCE_THREADS / 32; ++w) tot += red[w];
         const double nrm = n > 0 ? sqrt(tot) : state->last;
         if (is_start) {
             state->sweep = 0;
@@ -122,13 +127,16 @@ __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, S
         state->last = nrm;
         const bool go = isfinite(nrm) && nrm > state->tol * state->norm0 && sw < state->max_sweeps;
         if (use_cond) cudaGraphSetConditional(handle, go ? 1u : 0u);
+        if (use2) cudaGraphSetConditional(handle2, go ? 1u : 0u);
     }
 }
 
 int launch_reduce_norm(cudaStream_t st, const double *partials, int n, SolveState *state,
-                       double *hist, int is_start, unsigned long long cond_handle, int use_cond) {
-    reduce_norm_kernel<<<1, 256, 0, st>>>(partials, n, state, hist, is_start,
-                                         (cudaGraphConditionalHandle)cond_handle, use_cond);
+                       double *hist, int is_start, unsigned long long cond_handle, int use_cond,
+                       unsigned long long cond_handle2, int use2) {
+    reduce_norm_kernel<<<1, REDUCE_THREADS, 0, st>>>(partials, n, state, hist, is_start,
+                                                     (cudaGraphConditionalHandle)cond_handle, use_cond,
+                                                     (cudaGraphConditionalHandle)cond_handle2, use2);
     return (int)cudaGetLastError();
 }
 
@@ -1330,8 +1338,18 @@ struct ThomasCfg {
 template <typename T>
 static ThomasCfg thomas_cfg(const FastLayout &L) {
     const size_t sb = thomas_stage_bytes<T>();
-    const int per_sm = (L.nline + 147) / 148;
-    const long long budget = 210LL * 1024 / (per_sm > 0 ? per_sm : 1);
+    /* lines resident per SM in one wave, and the shared memory each may use
+     * so that they all are: the SM's capacity over them, less the per-CTA
+     * reservation.  The deeper the copy ring, the more of the DRAM latency
+     * the chain steps hide. */
+    int dev = 0, nsm = 148, smem_sm = 228 * 1024, reserved = 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (nsm < 1) nsm = 148;
+    const int per_sm = (L.nline + nsm - 1) / nsm;
+    const long long budget = (long long)smem_sm / (per_sm > 0 ? per_sm : 1) - reserved;
     const size_t ys_bytes = (size_t)((L.max_len + 3) & ~3) * NV * sizeof(T);
     const size_t fixed = 128 + 80 * sizeof(T);
     ThomasCfg c;
@@ -1497,22 +1515,211 @@ template int launch_full_resid<float>(cudaStream_t, int, const int *, const int 
                                       double *);
 
 
+/* ============================================ full residual, position order
+ * Dp = D blocks by position, XF[s][p] = the block of interior face s of the
+ * cell (ef order) in the cell's row; both from the original FP64 arrays,
+ * zero where absent.  One warp per block. */
+__global__ void fullpos_layout_kernel(long long nblk, int np16, const int *__restrict__ elem_of_pos,
+                                      const int *__restrict__ xsrcf, const double *__restrict__ D,
+                                      const double *__restrict__ O1, const double *__restrict__ O2,
+                                      double *__restrict__ Dp, double *__restrict__ XF) {
+    const int lane = threadIdx.x & 31;
+    const long long w0 = (blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5;
+    const long long nw = ((long long)gridDim.x * blockDim.x) >> 5;
+    for (long long q = w0; q < nblk; q += nw) {
+        const double *src = nullptr;
+        double *dst;
+        if (q < np16) {
+            const int e = elem_of_pos[q];
+            if (e >= 0) src = D + (size_t)e * NB;
+            dst = Dp + q * NB;
+        } else {
+            const long long k = q - np16; /* slot-major index s*np16 + p */
+            const int f = xsrcf[k];
+            if (f >= 0) src = ((f & 1) ? O2 : O1) + (size_t)(f >> 1) * NB;
+            dst = XF + k * NB;
+        }
+        for (int tt = lane; tt < NB; tt += 32) dst[tt] = src ? src[tt] : 0.0;
+    }
+}
+
+int launch_fullpos_layout(cudaStream_t st, const FastLayout &L, const double *jacD,
+                          const double *O1, const double *O2, double *Dp, double *XF) {
+    const long long nblk = (long long)L.np16 * (1 + L.nxf);
+    fullpos_layout_kernel<<<grid_for(nblk * 32, 256), 256, 0, st>>>(nblk, L.np16, L.elem_of_pos,
+                                                                    L.xsrcf, jacD, O1, O2, Dp, XF);
+    return (int)cudaGetLastError();
+}
+
+__host__ __device__ inline size_t fullpos_smem_bytes(int nxf) {
+    return 128 + (size_t)RES_TILE * NB * sizeof(double) * (1 + nxf) +
+           (size_t)(nxf + 1) * RES_TILE * NV * sizeof(double) + (size_t)RES_TILE * NV * sizeof(double) +
+           (size_t)RES_TILE * NB * sizeof(float) + 2 * (size_t)RES_TILE * NV * sizeof(float);
+}
+
+/* b = -Dinv R of one cell row in FP32, the operation order of the FP32
+ * mode-0 residual (fast_resid_body): dr = column-major block row i, rv = R */
+__device__ __forceinline__ float neg_dinv_row(const float *dr, const float *rv) {
+    float a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
+    a0 += dr[27] * rv[3];
+    a1 += dr[36] * rv[4];
+    a2 += dr[45] * rv[5];
+    a0 += dr[54] * rv[6];
+    a1 += dr[63] * rv[7];
+    a2 += dr[72] * rv[8];
+    return -(a0 + (a1 + a2));
+}
+
+/* One tile of 16 positions (160 threads; thread t < 144 owns cell t % 16,
+ * row t / 16).  R = rhs + D u + sum over faces (ef order) offJ u_nbr with
+ * the accumulation pattern of full_resid_body; R32 out, partials[blk] =
+ * the tile's sum R^2 (fixed order).  With Dinv32: also the next inner
+ * solve's right-hand side b32 = -Dinv32 R32 and c32 = 0. */
+__device__ __forceinline__ bool full_resid_pos_body(
+    int nxf, int np16, const double *__restrict__ Dp, const double *__restrict__ XF,
+    const int *__restrict__ xnbrf, const double *__restrict__ rhsp, const double *__restrict__ Up,
+    float *__restrict__ R32, double *__restrict__ partials, const float *__restrict__ Dinv32,
+    float *__restrict__ b32, float *__restrict__ c32, unsigned *status, int blk, uint64_t *bar,
+    uint32_t parity) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    double *sD = reinterpret_cast<double *>(smem + 128);
+    double *sX = sD + RES_TILE * NB;
+    double *sg = sX + nxf * RES_TILE * NB;      /* [1 + nxf][16][9]: own u, then neighbours */
+    double *sr = sg + (nxf + 1) * RES_TILE * NV; /* rhs tile */
+    float *sDi = reinterpret_cast<float *>(sr + RES_TILE * NV); /* Dinv32 tile */
+    float *so = sDi + RES_TILE * NB;
+    float *sb = so + RES_TILE * NV;
+    const int p0 = blk * RES_TILE;
+    const int tid = threadIdx.x;
+    const int c = tid % RES_TILE, i = tid / RES_TILE;
+    const bool act = tid < RES_TILE * NV;
+    const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
+    const uint32_t szDi = RES_TILE * NB * sizeof(float);
+    if (tid == 0) {
+        const uint64_t pol = policy_evict_first();
+        mbar_arrive_expect_tx(bar, szD * (1 + nxf) + szR + (Dinv32 ? szDi : 0u));
+        bulk_g2s_hint(sD, Dp + (size_t)p0 * NB, szD, bar, pol);
+        for (int s = 0; s < nxf; ++s)
+            bulk_g2s_hint(sX + s * RES_TILE * NB, XF + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
+        bulk_g2s(sr, rhsp + (size_t)p0 * NV, szR, bar);
+        if (Dinv32) bulk_g2s_hint(sDi, Dinv32 + (size_t)p0 * NB, szDi, bar, pol);
+    }
+    if (act && c32) c32[(size_t)p0 * NV + tid] = 0.0f;
+    if (act) {
+        sg[c * NV + i] = Up[(size_t)(p0 + c) * NV + i];
+        for (int s = 0; s < nxf; ++s) {
+            const int nb = xnbrf[(size_t)s * np16 + p0 + c];
+            sg[((s + 1) * RES_TILE + c) * NV + i] = (nb >= 0) ? Up[(size_t)nb * NV + i] : 0.0;
+        }
+    }
+    const bool ok = mbar_wait(bar, parity);
+    if (__syncthreads_or(!ok)) {
+        if (tid == 0) {
+            atomicOr(status, ST_TIMEOUT);
+            mbar_wait(bar, parity, 1LL << 28); /* let the copies land before the CTA retires */
+        }
+        return false;
+    }
+    double sq = 0.0;
+    if (act) {
+        const double *dr = sD + c * NB + i;
+        const double *u = sg + c * NV;
+        double a0 = dr[0] * u[0], a1 = dr[9] * u[1], a2 = dr[18] * u[2];
+        a0 += dr[27] * u[3];
+        a1 += dr[36] * u[4];
+        a2 += dr[45] * u[5];
+        a0 += dr[54] * u[6];
+        a1 += dr[63] * u[7];
+        a2 += dr[72] * u[8];
+        for (int s = 0; s < nxf; ++s) {
+            const double *o = sX + (s * RES_TILE + c) * NB + i;
+            const double *un = sg + ((s + 1) * RES_TILE + c) * NV;
+            a0 += o[0] * un[0];
+            a1 += o[9] * un[1];
+            a2 += o[18] * un[2];
+            a0 += o[27] * un[3];
+            a1 += o[36] * un[4];
+            a2 += o[45] * un[5];
+            a0 += o[54] * un[6];
+            a1 += o[63] * un[7];
+            a2 += o[72] * un[8];
+        }
+        const double r = sr[c * NV + i] + (a0 + (a1 + a2));
+        so[c * NV + i] = (float)r;
+        sq = r * r;
+    }
+    __syncthreads();
+    if (act) R32[(size_t)p0 * NV + tid] = so[tid]; /* contiguous tile store */
+    if (Dinv32) {
+        if (act) sb[c * NV + i] = neg_dinv_row(sDi + c * NB + i, so + c * NV);
+        __syncthreads();
+        if (act) b32[(size_t)p0 * NV + tid] = sb[tid];
+    }
+    __shared__ double red[RES_THREADS_FAST / 32];
+    for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+    if ((tid & 31) == 0) red[tid >> 5] = sq;
+    __syncthreads();
+    if (tid == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
+        partials[blk] = tot;
+    }
+    return true;
+}
+
+__global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_kernel(
+    int nxf, int np16, const double *__restrict__ Dp, const double *__restrict__ XF,
+    const int *__restrict__ xnbrf, const double *__restrict__ rhsp, const double *__restrict__ Up,
+    float *__restrict__ R32, double *__restrict__ partials, const float *__restrict__ Dinv32,
+    float *__restrict__ b32, float *__restrict__ c32, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
+    full_resid_pos_body(nxf, np16, Dp, XF, xnbrf, rhsp, Up, R32, partials, Dinv32, b32, c32, status,
+                        blockIdx.x, bar, 0);
+}
+
+int launch_full_resid_pos(cudaStream_t st, const FastLayout &L, const double *Dp, const double *XF,
+                          const double *rhsp, const double *Up, float *R32, double *partials,
+                          const float *Dinv32, float *b32, float *c32, unsigned *status) {
+    if (L.nxf < 0 || L.nxf > 4) return (int)cudaErrorInvalidValue;
+    full_resid_pos_kernel<<<fast_resid_grid(L.np16), RES_THREADS_FAST, fullpos_smem_bytes(L.nxf), st>>>(
+        L.nxf, L.np16, Dp, XF, L.xnbrf, rhsp, Up, R32, partials, Dinv32, b32, c32, status);
+    return (int)cudaGetLastError();
+}
+
 /* ================================================ mixed-precision prime
  * Per tile of RES_TILE positions (160 threads, 144 active): U = 0, the
  * FP32 copy of the residual R = rhs, and the tile's sum rhs^2 in a fixed
  * order (lane order within a warp, then warps in order). */
 __device__ __forceinline__ void mixed_prime_body(const double *__restrict__ rhsp,
                                                  float *__restrict__ R32, double *__restrict__ Up,
-                                                 double *__restrict__ partials, int blk) {
+                                                 double *__restrict__ partials,
+                                                 const float *__restrict__ Dinv32,
+                                                 float *__restrict__ b32, float *__restrict__ c32,
+                                                 int blk) {
     const int tid = threadIdx.x;
     const bool act = tid < RES_TILE * NV;
+    __shared__ float sR[RES_TILE * NV];
     double sq = 0.0;
     if (act) {
         const size_t q = (size_t)blk * RES_TILE * NV + tid;
         const double v = rhsp[q];
         R32[q] = (float)v;
+        sR[tid] = (float)v;
         Up[q] = 0.0;
+        if (c32) c32[q] = 0.0f;
         sq = v * v;
+    }
+    if (Dinv32) {
+        /* the first inner solve's right-hand side b32 = -Dinv32 R32, from
+         * the tile's Dinv32 blocks staged with coalesced loads */
+        __shared__ float sDi[RES_TILE * NB];
+        const float *src = Dinv32 + (size_t)blk * RES_TILE * NB;
+        for (int t = tid; t < RES_TILE * NB; t += blockDim.x) sDi[t] = src[t];
+        __syncthreads();
+        if (act) {
+            const int c = tid % RES_TILE, i = tid / RES_TILE;
+            b32[((size_t)blk * RES_TILE + c) * NV + i] = neg_dinv_row(sDi + c * NB + i, sR + c * NV);
+        }
     }
     __shared__ double red[RES_THREADS_FAST / 32];
     for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
@@ -1527,14 +1734,15 @@ __device__ __forceinline__ void mixed_prime_body(const double *__restrict__ rhsp
 
 __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_kernel(
     const double *__restrict__ rhsp, float *__restrict__ R32, double *__restrict__ Up,
-    double *__restrict__ partials) {
-    mixed_prime_body(rhsp, R32, Up, partials, blockIdx.x);
+    double *__restrict__ partials, const float *__restrict__ Dinv32, float *__restrict__ b32,
+    float *__restrict__ c32) {
+    mixed_prime_body(rhsp, R32, Up, partials, Dinv32, b32, c32, blockIdx.x);
 }
 
 int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
-                       double *Up, double *partials) {
-    mixed_prime_kernel<<<fast_resid_grid(L.np16), RES_THREADS_FAST, 0, st>>>(rhsp, R32, Up,
-                                                                             partials);
+                       double *Up, double *partials, const float *Dinv32, float *b32, float *c32) {
+    mixed_prime_kernel<<<fast_resid_grid(L.np16), RES_THREADS_FAST, 0, st>>>(rhsp, R32, Up, partials,
+                                                                             Dinv32, b32, c32);
     return (int)cudaGetLastError();
 }
 
@@ -1676,7 +1884,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_batch_kernel(
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
         const WorkItem it = group_item(groups, w);
         const VecSys S = sys[it.sys];
-        mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, it.unit);
+        mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, S.Dinv32, S.b32, S.c32, it.unit);
         __syncthreads();
     }
 }
@@ -1708,13 +1916,41 @@ int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, co
     return (int)cudaGetLastError();
 }
 
+__global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_batch_kernel(
+    const FullPosSys *__restrict__ sys, const int *__restrict__ groups,
+    const int *__restrict__ active, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
+    const int nwork = group_items(groups);
+    uint32_t parity = 0;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const WorkItem it = group_item(groups, w);
+        if (active && !active[it.sys]) continue;
+        const FullPosSys S = sys[it.sys];
+        const bool ok = full_resid_pos_body(S.nxf, S.np16, S.Dp, S.XF, S.xnbrf, S.rhsp, S.Up, S.R32,
+                                            S.partials, S.Dinv32, S.b32, S.c32, status, it.unit, bar,
+                                            parity);
+        parity ^= 1u;
+        if (!ok) break;
+        __syncthreads(); /* the next tile's copies overwrite the stages */
+    }
+}
+
+int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
+                                const int *groups, const int *active, unsigned *status) {
+    const size_t smem = fullpos_smem_bytes(max_nxf);
+    const int grid = resid_batch_grid(smem, (const void *)full_resid_pos_batch_kernel);
+    full_resid_pos_batch_kernel<<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, active, status);
+    return (int)cudaGetLastError();
+}
+
 /* One CTA per descriptor (grid = capacity; CTAs beyond *nred only take
  * their ticket).  The last CTA to finish decides whether the graph's loop
  * goes on: some member is active, the sweep limit of the launch is not
  * reached and, when asked, no member stopped during the launch. */
 __global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, const int *__restrict__ nred_p,
                                     int is_start, int *active, BatchCtl *ctl, unsigned *counter,
-                                    cudaGraphConditionalHandle handle, int use_cond) {
+                                    cudaGraphConditionalHandle handle, int use_cond,
+                                    cudaGraphConditionalHandle handle2, int use2) {
     __shared__ double red[32];
     __shared__ unsigned ticket;
     const int s = blockIdx.x;
@@ -1763,17 +1999,20 @@ __global__ void batch_reduce_kernel(const ReduceSys *__restrict__ sys, const int
         }
         if (ctl->stop_on_finish && __ldcg(&ctl->finished)) go = false;
         if (use_cond) cudaGraphSetConditional(handle, go ? 1u : 0u);
+        if (use2) cudaGraphSetConditional(handle2, go ? 1u : 0u);
         *counter = 0u;
     }
 }
 
 int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, const int *nred,
                         int cap, int is_start, int *active, BatchCtl *ctl, unsigned *counter,
-                        unsigned long long cond_handle, int use_cond) {
+                        unsigned long long cond_handle, int use_cond,
+                        unsigned long long cond_handle2, int use2) {
     if (cap <= 0) return 0;
-    if (threads != RES_THREADS_FAST && threads != 256) return (int)cudaErrorInvalidValue;
+    if (threads != RES_THREADS_FAST && threads != REDUCE_THREADS) return (int)cudaErrorInvalidValue;
     batch_reduce_kernel<<<cap, threads, 0, st>>>(sys, nred, is_start, active, ctl, counter,
-                                                 (cudaGraphConditionalHandle)cond_handle, use_cond);
+                                                 (cudaGraphConditionalHandle)cond_handle, use_cond,
+                                                 (cudaGraphConditionalHandle)cond_handle2, use2);
     return (int)cudaGetLastError();
 }
 
@@ -1783,7 +2022,12 @@ int batch_prepare(int max_nx) {
     int rc = set_smem((const void *)fast_resid_batch_kernel<double>, resid_smem_bytes<double>(max_nx));
     if (!rc)
         rc = set_smem((const void *)fast_resid_batch_kernel<float>, resid_smem_bytes<float>(max_nx));
+    if (!rc) rc = set_smem((const void *)full_resid_pos_batch_kernel, fullpos_smem_bytes(4));
     return rc;
+}
+
+int fullpos_prepare(const FastLayout &L) {
+    return set_smem((const void *)full_resid_pos_kernel, fullpos_smem_bytes(L.nxf));
 }
 
 template size_t thomas_batch_smem<double>(int);

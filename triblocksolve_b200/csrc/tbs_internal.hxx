@@ -102,6 +102,10 @@ struct FastLayout {
     int *elem_of_pos;  /* [np16], -1 for pads */
     int *xnbr;         /* [nx*np16] slot-major: neighbour position or -1 */
     int *xsrc;         /* [nx*np16] 2*face + (1 if the block is O2), or -1 */
+    int nxf;           /* all-face slots per position (the full residual) */
+    int *xnbrf;        /* [nxf*np16] slot-major: neighbour position over every interior
+                        * face of the cell in ef order, or -1 */
+    int *xsrcf;        /* [nxf*np16] 2*face + (1 if the block is O2), or -1 */
     int *fsrc;         /* [np16*5] factor sources: elem, face to the chain
                         * predecessor (-1 at a chain start), side (1 if elem is
                         * fc[2f]); the twist position adds the face to its
@@ -133,7 +137,8 @@ int ref_line_res_partials(int nelem);
 int launch_norm_partials(cudaStream_t st, const double *v, long long n, double *partials,
                          int npart);
 int launch_reduce_norm(cudaStream_t st, const double *partials, int n, SolveState *state,
-                       double *hist, int is_start, unsigned long long cond_handle, int use_cond);
+                       double *hist, int is_start, unsigned long long cond_handle, int use_cond,
+                       unsigned long long cond_handle2 = 0, int use2 = 0);
 int launch_zero(cudaStream_t st, double *p, long long n);
 int launch_permute_to_pos(cudaStream_t st, int nv, int nelem, const int *pos_of_elem,
                           const double *src_elem, double *dst_pos);
@@ -184,15 +189,30 @@ int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *
                       const int *pos_of_elem, const double *D, const double *O1, const double *O2,
                       const double *rhs, const double *Up, T *Rp, double *partials);
 
+/* The FP64 residual R = rhs + J U in position order from position-ordered
+ * copies of the original blocks (Dp: diagonal, XF: one slot per interior
+ * face in ef order), streamed per tile with bulk copies like the sweep
+ * residual; R goes out in FP32 (the inner solve's right-hand side) with
+ * per-tile partials of R^2; with Dinv32 also b32 = -Dinv32 R32 and
+ * c32 = 0 for the next inner solve.  Needs L.nxf <= 4. */
+int launch_fullpos_layout(cudaStream_t st, const FastLayout &L, const double *jacD,
+                          const double *O1, const double *O2, double *Dp, double *XF);
+int launch_full_resid_pos(cudaStream_t st, const FastLayout &L, const double *Dp,
+                          const double *XF, const double *rhsp, const double *Up, float *R32,
+                          double *partials, const float *Dinv32, float *b32, float *c32,
+                          unsigned *status);
+int fullpos_prepare(const FastLayout &L);
+
 /* mixed-precision glue (kernels_fast.cu) */
 int launch_cast_f64_f32(cudaStream_t st, const double *src, float *dst, long long n);
 int launch_axpy_f32_f64(cudaStream_t st, const float *d, double *U, long long n);
 int launch_axpy2_f32_f64(cudaStream_t st, const float *c, const float *d, double *U, long long n);
 int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
 /* per tile of RES_TILE positions: Up = 0, R32 = (float)rhsp, partials[tile]
- * = sum rhsp^2 in a fixed order (the start of a TBS_ALGO_MIXED solve) */
+ * = sum rhsp^2 in a fixed order (the start of a TBS_ALGO_MIXED solve); with
+ * Dinv32 also the first inner right-hand side b32 = -Dinv32 R32, c32 = 0 */
 int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
-                       double *Up, double *partials);
+                       double *Up, double *partials, const float *Dinv32, float *b32, float *c32);
 
 /* ------------------------------------------------------------ batches
  * Many independent systems swept together.  Each kernel takes one
@@ -226,11 +246,22 @@ struct FullResSys {
     float *R32;
     double *partials;
 };
+struct FullPosSys {
+    int np16, nxf;
+    const int *xnbrf;
+    const double *Dp, *XF, *rhsp, *Up;
+    float *R32;
+    double *partials;
+    const float *Dinv32;        /* non-null: also b32 = -Dinv32 R32, c32 = 0 */
+    float *b32, *c32;
+};
 struct VecSys {                 /* mixed-precision glue of one system */
     const double *rhsp;
     float *R32, *c32, *d32;
     double *Up;
     double *partials;
+    const float *Dinv32;        /* non-null: the prime also sets b32 (and c32 = 0) */
+    float *b32;
 };
 struct ReduceSys {
     const double *partials;
@@ -284,16 +315,19 @@ int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> 
                        const int *groups, const int *active, unsigned *status);
 int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *groups,
                             const int *active);
+int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
+                                const int *groups, const int *active, unsigned *status);
 int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const int *groups);
 int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, const int *active);
 /* one CTA of `threads` threads per norm descriptor (grid = cap, *nred in
  * use): the fixed-order sum of the member's partials (the order of
- * finalize_norm for threads = 160 and of reduce_norm for threads = 256),
+ * finalize_norm for threads = 160 and of reduce_norm for threads = 1024),
  * its norm history and active flag; the last CTA sets the graph condition
  * by the rule in `ctl` */
 int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, const int *nred,
                         int cap, int is_start, int *active, BatchCtl *ctl, unsigned *counter,
-                        unsigned long long cond_handle, int use_cond);
+                        unsigned long long cond_handle, int use_cond,
+                        unsigned long long cond_handle2 = 0, int use2 = 0);
 int batch_prepare(int max_nx);
 
 }  // namespace tbs

@@ -285,8 +285,18 @@ class Solver:
     def set_inner_sweeps(self, m: int):
         self._chk(N.lib.tbs_set_inner_sweeps(self.ctx, m))
 
+    def set_inner_schedule(self, first: int, rest: int):
+        """TBS_ALGO_MIXED: `first` inner sweeps in a solve's first outer step, `rest` after."""
+        self._chk(N.lib.tbs_set_inner_schedule(self.ctx, first, rest))
+
+    def inner_schedule(self):
+        f, r = C.c_int(), C.c_int()
+        self._chk(N.lib.tbs_get_inner_schedule(self.ctx, C.byref(f), C.byref(r)))
+        return f.value, r.value
+
     def tune_inner(self, rel_tol: float, max_sweeps: int = 100):
-        """Pick the fastest FP32 inner sweep count for TBS_ALGO_MIXED (device timing)."""
+        """Pick the fastest FP32 inner sweep schedule for TBS_ALGO_MIXED (device timing);
+        returns (steady inner sweeps, ms); inner_schedule() gives the first step's too."""
         m = C.c_int()
         ms = C.c_double()
         self._chk(N.lib.tbs_tune_inner(self.ctx, rel_tol, max_sweeps, C.byref(m), C.byref(ms)))
@@ -404,6 +414,9 @@ class Batch:
 
     def set_inner_sweeps(self, m: int):
         self._chk(N.lib.tbs_batch_set_inner_sweeps(self.handle, m))
+
+    def set_inner_schedule(self, first: int, rest: int):
+        self._chk(N.lib.tbs_batch_set_inner_schedule(self.handle, first, rest))
 
     def profile(self, on: bool = True):
         self._chk(N.lib.tbs_batch_profile_enable(self.handle, 1 if on else 0))
