@@ -602,16 +602,16 @@ int fast_resid_grid(int np16) { return np16 / RES_TILE > 0 ? np16 / RES_TILE : 1
 /* Fixed-order sum of the per-CTA partials by the last CTA; updates the
  * solve state like reduce_norm_kernel.  Called by every thread of the
  * block; `block_sum` is valid in thread 0. */
-__device__ void finalize_norm(const NormSink &ns, double block_sum, int blk) {
+/* After a CTA's last tile: a ticket per CTA; the last CTA to finish adds
+ * the n per-tile partials in a fixed order and, when asked, records the
+ * norm like reduce_norm (history, sweep count, graph loop condition).
+ * Called by every thread of the block. */
+__device__ void finalize_total(const NormSink &ns, int n) {
     __shared__ unsigned ticket;
     __shared__ double red[32];
-    if (!ns.partials) return;
-    if (!ns.counter) { /* batched launch: the partial only, reduced per system later */
-        if (threadIdx.x == 0) ns.partials[blk] = block_sum;
-        return;
-    }
+    if (!ns.partials || !ns.counter) return;
+    __syncthreads(); /* this CTA's partials are written */
     if (threadIdx.x == 0) {
-        ns.partials[blockIdx.x] = block_sum;
         __threadfence();
         ticket = atomicAdd(ns.counter, 1u);
     }
@@ -622,7 +622,7 @@ __device__ void finalize_norm(const NormSink &ns, double block_sum, int blk) {
         return;
     }
     __threadfence();
-    double acc = strided_sum(ns.partials, (int)gridDim.x, (int)blockDim.x);
+    double acc = strided_sum(ns.partials, n, (int)blockDim.x);
     for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
     if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
     __syncthreads();
@@ -769,12 +769,34 @@ __device__ __forceinline__ bool fast_resid_body(
         for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
         if ((tid & 31) == 0) red[tid >> 5] = sq;
         __syncthreads();
-        double tot = 0.0;
-        if (tid == 0)
+        if (tid == 0) {
+            double tot = 0.0;
             for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[w];
-        finalize_norm(ns, tot, blk);
+            ns.partials[blk] = tot; /* the tile's sum R^2; totals by finalize_total */
+        }
     }
     return true;
+}
+
+/* The single-system residual launches are persistent: CTA k takes tiles
+ * k, k + grid, ...; each tile completes one phase of the CTA's barrier and
+ * writes its partial; finalize_total then sums the tiles' partials in tile
+ * order (the order of the batched norm kernel with 160 threads). */
+template <typename T>
+__device__ __forceinline__ void resid_tiles(int nx, int np16, int mode, const T *Dinv, const T *X,
+                                            const int *xnbr, const T *dU, const T *Rsrc, T *b,
+                                            T *Uacc, const NormSink &ns, unsigned *status) {
+    uint64_t *bar = resid_bar_init();
+    const int ntiles = np16 / RES_TILE;
+    uint32_t parity = 0;
+    for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        const bool ok = fast_resid_body<T>(nx, np16, mode, Dinv, X, xnbr, dU, Rsrc, b, Uacc, ns,
+                                           status, w, bar, parity);
+        parity ^= 1u;
+        if (!ok) break;
+        __syncthreads(); /* the next tile's copies overwrite the stages */
+    }
+    finalize_total(ns, ntiles);
 }
 
 /* mode 1 (R = sum X dU over the cross-line slots) */
@@ -783,9 +805,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     int nx, int np16, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, T *__restrict__ b,
     T *__restrict__ Uacc, NormSink ns, unsigned *status) {
-    uint64_t *bar = resid_bar_init();
-    fast_resid_body<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status, blockIdx.x,
-                       bar, 0);
+    resid_tiles<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status);
 }
 
 /* mode 3 (b = -sum (Dinv X) dU: premultiplied cross-line blocks, no norm) */
@@ -793,9 +813,7 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_dx_kernel(
     int nx, int np16, const T *__restrict__ DX, const int *__restrict__ xnbr,
     const T *__restrict__ dU, T *__restrict__ b, T *__restrict__ Uacc, unsigned *status) {
-    uint64_t *bar = resid_bar_init();
-    fast_resid_body<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status,
-                       blockIdx.x, bar, 0);
+    resid_tiles<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status);
 }
 
 /* mode 0 (R given in position order) */
@@ -803,9 +821,19 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
     int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
     T *__restrict__ Uzero, NormSink ns, unsigned *status) {
-    uint64_t *bar = resid_bar_init();
-    fast_resid_body<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status,
-                       blockIdx.x, bar, 0);
+    resid_tiles<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status);
+}
+
+/* CTAs of a persistent single-system residual launch: as many as fit */
+static int resid_grid_persistent(const void *fn, size_t smem, int ntiles) {
+    int dev = 0, nsm = 148, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, RES_THREADS_FAST, smem) != cudaSuccess ||
+        per < 1)
+        per = 1;
+    const int g = per * nsm;
+    return ntiles < g ? (ntiles > 0 ? ntiles : 1) : g;
 }
 
 template <typename T>
@@ -831,14 +859,16 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
     if (mode == 0 && !Rsrc) return (int)cudaErrorInvalidValue;
     const size_t smem = resid_smem_bytes<T>(mode >= 1 ? L.nx : 0);
     if (mode == 3)
-        fast_resid_dx_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, X, L.xnbr, dU,
-                                                                      b, Uacc, status);
+        fast_resid_dx_kernel<T><<<resid_grid_persistent((const void *)fast_resid_dx_kernel<T>, smem, grid),
+                                  RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, X, L.xnbr, dU, b, Uacc,
+                                                                status);
     else if (mode == 1)
-        fast_resid_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr,
-                                                                   dU, b, Uacc, ns, status);
+        fast_resid_kernel<T><<<resid_grid_persistent((const void *)fast_resid_kernel<T>, smem, grid),
+                               RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr, dU, b, Uacc,
+                                                             ns, status);
     else
-        fast_resid_rhs_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b,
-                                                                       Uacc, ns, status);
+        fast_resid_rhs_kernel<T><<<resid_grid_persistent((const void *)fast_resid_rhs_kernel<T>, smem, grid),
+                                   RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b, Uacc, ns, status);
     return (int)cudaGetLastError();
 }
 

@@ -321,7 +321,7 @@ int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const int *grou
 int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, const int *active);
 /* one CTA of `threads` threads per norm descriptor (grid = cap, *nred in
  * use): the fixed-order sum of the member's partials (the order of
- * finalize_norm for threads = 160 and of reduce_norm for threads = 1024),
+ * finalize_total for threads = 160 and of reduce_norm for threads = 1024),
  * its norm history and active flag; the last CTA sets the graph condition
  * by the rule in `ctl` */
 int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, const int *nred,
