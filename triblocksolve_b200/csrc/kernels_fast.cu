@@ -1697,22 +1697,34 @@ __device__ __forceinline__ bool full_resid_pos_body(
     return true;
 }
 
+/* persistent: CTA k takes tiles k, k + grid, ... */
 __global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_kernel(
     int nxf, int np16, const double *__restrict__ Dp, const double *__restrict__ XF,
     const int *__restrict__ xnbrf, const double *__restrict__ rhsp, const double *__restrict__ Up,
     float *__restrict__ R32, double *__restrict__ partials, const float *__restrict__ Dinv32,
     float *__restrict__ b32, float *__restrict__ c32, unsigned *status) {
     uint64_t *bar = resid_bar_init();
-    full_resid_pos_body(nxf, np16, Dp, XF, xnbrf, rhsp, Up, R32, partials, Dinv32, b32, c32, status,
-                        blockIdx.x, bar, 0);
+    const int ntiles = np16 / RES_TILE;
+    uint32_t parity = 0;
+    for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        const bool ok = full_resid_pos_body(nxf, np16, Dp, XF, xnbrf, rhsp, Up, R32, partials, Dinv32,
+                                            b32, c32, status, w, bar, parity);
+        parity ^= 1u;
+        if (!ok) break;
+        __syncthreads(); /* the next tile's copies overwrite the stages */
+    }
 }
 
 int launch_full_resid_pos(cudaStream_t st, const FastLayout &L, const double *Dp, const double *XF,
                           const double *rhsp, const double *Up, float *R32, double *partials,
                           const float *Dinv32, float *b32, float *c32, unsigned *status) {
     if (L.nxf < 0 || L.nxf > 4) return (int)cudaErrorInvalidValue;
-    full_resid_pos_kernel<<<fast_resid_grid(L.np16), RES_THREADS_FAST, fullpos_smem_bytes(L.nxf), st>>>(
-        L.nxf, L.np16, Dp, XF, L.xnbrf, rhsp, Up, R32, partials, Dinv32, b32, c32, status);
+    const size_t smem = fullpos_smem_bytes(L.nxf);
+    const int grid = resid_grid_persistent((const void *)full_resid_pos_kernel, smem,
+                                           fast_resid_grid(L.np16));
+    full_resid_pos_kernel<<<grid, RES_THREADS_FAST, smem, st>>>(L.nxf, L.np16, Dp, XF, L.xnbrf, rhsp,
+                                                                Up, R32, partials, Dinv32, b32, c32,
+                                                                status);
     return (int)cudaGetLastError();
 }
 
@@ -1762,6 +1774,7 @@ __device__ __forceinline__ void mixed_prime_body(const double *__restrict__ rhsp
     }
 }
 
+/* one CTA per tile (measured faster than a persistent loop here) */
 __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_kernel(
     const double *__restrict__ rhsp, float *__restrict__ R32, double *__restrict__ Up,
     double *__restrict__ partials, const float *__restrict__ Dinv32, float *__restrict__ b32,
