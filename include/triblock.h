@@ -214,6 +214,27 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out);
 int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps,
               int *sweeps_out, double *hist_out);
 
+/* nrhs right-hand sides with the factors of the last
+ * tbs_factor(TBS_ALGO_FP64), each from U = 0: the multi-RHS form of the
+ * sweep loop of src/main.cxx:180-229 (the reference solves one per run).
+ * rhs and U hold nrhs vectors of 9*nelem doubles, element order, one after
+ * the other.  Groups of up to 8 sweep together in one CUDA graph launch,
+ * the line blocks read once per sweep for the group; each right-hand side
+ * stops at its own tolerance or max_sweeps.  sweeps (may be NULL) gets
+ * nrhs counts; hist (may be NULL) row r, at hist + r * hist_stride, gets
+ * min(sweeps[r] + 1, hist_stride) norms as tbs_solve's hist_out.  Every
+ * right-hand side's U, sweep count and norms are bit-identical to
+ * tbs_set_rhs + tbs_solve of it alone.  The context's own rhs and solution
+ * are left alone.  TBS_ERR_UNSUPPORTED for the other algorithms.
+ * tbs_solve_multi takes host arrays; tbs_solve_multi_device device arrays
+ * (work on the context's stream; returns after it is done). */
+int tbs_solve_multi(tbs_ctx *ctx, int nrhs, const double *rhs, double *U,
+                    double rel_tol, int max_sweeps, int *sweeps, double *hist,
+                    int hist_stride);
+int tbs_solve_multi_device(tbs_ctx *ctx, int nrhs, const double *d_rhs,
+                           double *d_U, double rel_tol, int max_sweeps,
+                           int *sweeps, double *hist, int hist_stride);
+
 /* Jacobian::fromDevice (src/Jacobian.cxx:279-290) for the vectors, in the
  * element order of the input (9*nelem doubles each). */
 int tbs_get_solution(tbs_ctx *ctx, double *U);

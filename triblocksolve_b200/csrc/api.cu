@@ -117,6 +117,7 @@ static void drop_graph(tbs_ctx *ctx) {
 
 /* free everything that depends on the mesh */
 static void drop_mesh(tbs_ctx *ctx) {
+    multi_free(ctx);
     drop_graph(ctx);
     for (auto &a : ctx->allocs) cudaFree(a.first);
     ctx->allocs.clear();
@@ -202,6 +203,21 @@ static int timed(tbs_ctx *ctx, const char *name, F &&launch) {
 }
 
 #define RUN(name, call) CKL(timed(ctx, name, [&]() { return (int)(call); }))
+
+int ctx_prof_begin(tbs_ctx *ctx, const char *name) {
+    if (!ctx->prof || capturing(ctx)) return -1;
+    if (ctx->pending.size() > 4000) prof_resolve(ctx);
+    PendingEvent pe{prof_slot(ctx, name), prof_event(ctx), prof_event(ctx)};
+    cudaEventRecord(pe.a, ctx->stream);
+    ctx->pending.push_back(pe);
+    return (int)ctx->pending.size() - 1;
+}
+
+void ctx_prof_end(tbs_ctx *ctx, int h) {
+    if (h >= 0 && h < (int)ctx->pending.size()) cudaEventRecord(ctx->pending[h].b, ctx->stream);
+}
+
+void ctx_prof_resolve(tbs_ctx *ctx) { prof_resolve(ctx); }
 
 /* ============================================================ layout (host) */
 
@@ -373,6 +389,8 @@ static int status_check(tbs_ctx *ctx) {
     }
     return TBS_OK;
 }
+
+int ctx_status(tbs_ctx *ctx) { return status_check(ctx); }
 
 static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; }
 
@@ -810,6 +828,7 @@ int tbs_set_stream(tbs_ctx *ctx, void *cuda_stream) {
     if (ns != ctx->stream) {
         cudaStreamSynchronize(ctx->stream);
         drop_graph(ctx); /* graphs are launched on, and captured from, the stream */
+        multi_drop_graph(ctx);
         ctx->stream = ns;
     }
     return TBS_OK;
@@ -1141,7 +1160,7 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
 
 int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes) {
     if (!ctx || !bytes) return ctx_fail(nullptr, TBS_ERR_ARG, "null argument");
-    *bytes = ctx->bytes;
+    *bytes = ctx->bytes + multi_bytes(ctx);
     return TBS_OK;
 }
 

@@ -26,6 +26,8 @@ struct PendingEvent {
     cudaEvent_t a, b;
 };
 
+struct MultiBufs; /* several right-hand sides (multi.cu) */
+
 struct tbs_ctx {
     int device = 0;
     cudaStream_t own = nullptr;
@@ -81,6 +83,9 @@ struct tbs_ctx {
     cudaGraph_t graph = nullptr;
     int graph_algo = -1;
 
+    /* ---- several right-hand sides: vectors and graph, made on first use ---- */
+    MultiBufs *multi = nullptr;
+
     /* ---- memory accounting ---- */
     std::vector<std::pair<void *, size_t>> allocs;
     size_t bytes = 0;
@@ -98,5 +103,18 @@ bool fullpos_ok(const tbs_ctx *ctx);
 int ctx_ensure_hist(tbs_ctx *ctx, int need);
 /* tolerance, sweep limit and history capacity of the device SolveState */
 int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps);
+/* reads and clears the device status word; a set bit becomes the error */
+int ctx_status(tbs_ctx *ctx);
+/* profiling brackets (a no-op unless profiling, outside stream capture):
+ * begin records the start event of a launch named `name` and returns its
+ * handle, end records its end event; resolve adds the finished pairs up */
+int ctx_prof_begin(tbs_ctx *ctx, const char *name);
+void ctx_prof_end(tbs_ctx *ctx, int h);
+void ctx_prof_resolve(tbs_ctx *ctx);
+/* multi.cu: free the multi-RHS vectors and graph / drop only the graph /
+ * their device bytes */
+void multi_free(tbs_ctx *ctx);
+void multi_drop_graph(tbs_ctx *ctx);
+size_t multi_bytes(const tbs_ctx *ctx);
 
 #endif /* TBS_CTX_HXX */

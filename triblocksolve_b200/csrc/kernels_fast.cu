@@ -2088,4 +2088,683 @@ template int launch_resid_batch<double>(cudaStream_t, int, int, const ResidSys<d
 template int launch_resid_batch<float>(cudaStream_t, int, int, const ResidSys<float> *,
                                        const int *, const int *, unsigned *);
 
+
+/* ============================================== several right-hand sides
+ * nr <= MULTI_MAX right-hand sides of one factored system swept together
+ * (TBS_ALGO_FP64): the line blocks (G, Gam, Dinv, X) are read once per
+ * sweep for all of them.  Vectors are RHS-major: right-hand side r of a
+ * vector v starts at v + r * vs, vs = np16 * 9.  A right-hand side whose
+ * solve has ended (active[r] == 0) is skipped by every kernel, so its
+ * solution stays the one of its last sweep, and the per-element arithmetic
+ * is the single-system kernels' own: every right-hand side's iterates,
+ * norms and sweep count are bit-identical to a solve of it alone. */
+
+/* Forward / backward chunk steps of thomas_line's chains for MULTI_RPW
+ * right-hand sides at once: the row of G (Gam) is loaded once per step and
+ * feeds one dot product per right-hand side, each with row_dot's own
+ * expression, so every right-hand side's values are those of fwd_chunk /
+ * bwd_chunk.  Right-hand side j reads its b chunk at sB[j], publishes its
+ * vector through bc[j] and writes y (dU) through yg[j] (dUl[j]); only the
+ * first `nown` of them write. */
+constexpr int MULTI_RPW = 2;
+
+template <int P, bool CHECK>
+__device__ __forceinline__ void fwd_chunk_m(const double *sG, const double *const *sB,
+                                            double *const *bc, double *const *yg, int nown,
+                                            int kbase, int len, int cpos, int i, bool writer,
+                                            const LaneOff &o) {
+    RowD cur_row, next_row;
+    load_row(cur_row, sG, o, 0);
+    double cur_b[MULTI_RPW], next_b[MULTI_RPW];
+#pragma unroll
+    for (int j = 0; j < MULTI_RPW; ++j) cur_b[j] = sB[j][i];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        const int odd = q & 1;
+#pragma unroll
+        for (int j = 0; j < MULTI_RPW; ++j) next_b[j] = 0.0;
+        if (q + 1 < P) {
+            load_row(next_row, sG + (q + 1) * NB, o, odd ^ 1);
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) next_b[j] = sB[j][(q + 1) * NV + i];
+        }
+        double yi[MULTI_RPW];
+#pragma unroll
+        for (int j = 0; j < MULTI_RPW; ++j) yi[j] = row_dot(cur_row, bc[j] + odd * 20, o, odd, cur_b[j]);
+        if (writer && (!CHECK || kbase + q < len)) {
+            const int pos = cpos + kbase + q;
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) {
+                if (j < nown) {
+                    double *nxt = bc[j] + (odd ^ 1) * 20;
+                    nxt[i] = yi[j];
+                    nxt[11 + i] = yi[j];
+                    yg[j][(size_t)pos * NV + i] = yi[j];
+                }
+            }
+        }
+        __syncwarp();
+        cur_row = next_row;
+#pragma unroll
+        for (int j = 0; j < MULTI_RPW; ++j) cur_b[j] = next_b[j];
+    }
+}
+
+template <int P, bool CHECK>
+__device__ __forceinline__ void bwd_chunk_m(const double *sG, double *const *bc,
+                                            const double (*yv)[P], double *const *dUl, int nown,
+                                            int kbase, int len, int cpos, int i, bool writer,
+                                            const LaneOff &o) {
+    RowD cur_row, next_row;
+    load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q) {
+        const int odd = q & 1;
+        if (q > 0) load_row(next_row, sG + (q - 1) * NB, o, odd ^ 1);
+        const int f = (P - 1 - q) & 1;
+        const bool valid = !CHECK || (kbase + q >= 0 && kbase + q < len);
+        const int pos = cpos + kbase + q;
+        double d[MULTI_RPW];
+#pragma unroll
+        for (int j = 0; j < MULTI_RPW; ++j)
+            d[j] = row_dot(cur_row, bc[j] + f * 20, o, odd, valid ? yv[j][q] : 0.0);
+        if (writer && valid) {
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) {
+                if (j < nown) {
+                    double *nxt = bc[j] + (f ^ 1) * 20;
+                    nxt[i] = d[j];
+                    nxt[11 + i] = d[j];
+                    dUl[j][(size_t)pos * NV + i] = d[j];
+                }
+            }
+        }
+        __syncwarp();
+        cur_row = next_row;
+    }
+}
+
+/* Thomas: one CTA per line; warp w solves the active right-hand sides
+ * 2w and 2w+1 (in active order) with the chains of thomas_line (y in
+ * global memory).  Thread 0 streams the jobs through an NS-stage ring; a
+ * forward stage holds, for either chain, a chunk of G rows followed by the
+ * chunks of b of the active right-hand sides, a backward stage a chunk of
+ * Gam rows.  All warps have consumed a stage before it is refilled (one
+ * CTA barrier per chunk). */
+template <int P>
+__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kernel(
+    int nline, int NS, int nr, long long vs, const int *__restrict__ line_start,
+    const int *__restrict__ line_len, const int *__restrict__ line_twist,
+    const double *__restrict__ G, const double *__restrict__ Gam, const double *__restrict__ b,
+    double *__restrict__ y, double *__restrict__ dU, const int *__restrict__ active,
+    unsigned *status) {
+    using T = double;
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned amask_s;
+    __shared__ int rid[MULTI_MAX];
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    if (tid == 0) {
+        unsigned am = 0;
+        int k = 0;
+        for (int r = 0; r < nr; ++r)
+            if (active[r]) {
+                am |= 1u << r;
+                rid[k++] = r;
+            }
+        amask_s = am;
+        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const unsigned amask = amask_s;
+    if (amask == 0u) return;
+    const int nact = __popc(amask);
+    const int k0 = w * MULTI_RPW;                  /* this warp's first active slot */
+    const int nown = max(0, min(MULTI_RPW, nact - k0));
+    const bool mine = nown > 0;
+    const uint32_t halfb = P * (NB + nr * NV) * sizeof(T);
+    const uint32_t stage = 2 * halfb;
+    unsigned char *st0 = smem + 128;
+    T *bcw = reinterpret_cast<T *>(st0 + (size_t)NS * stage) + w * MULTI_RPW * 80;
+    const int ps = line_start[l], n = line_len[l], m = line_twist[l];
+    const int h = lane >> 4, li = lane & 15;
+    const int i = li < NV ? li : NV - 1;
+    const bool writer = li < NV;
+    const LaneOff off = lane_offsets(i);
+    const int nb = n - 1 - m;
+    const int len = h ? nb : m;
+    const int cpos = h ? m : 0;
+    const int nchT = (m + P - 1) / P, nchB = (nb + P - 1) / P;
+    const int nch = h ? nchB : nchT;
+    const int nf = nchT > nchB ? nchT : nchB;
+    const int njobs = 2 * nf;
+    /* per owned right-hand side: its broadcast buffers (this half), y, dU
+     * and b (slots beyond nown alias slot 0 and never write) */
+    T *bc[MULTI_RPW], *yl[MULTI_RPW], *dUl[MULTI_RPW];
+    const T *bg[MULTI_RPW];
+    int slot[MULTI_RPW];
+#pragma unroll
+    for (int j = 0; j < MULTI_RPW; ++j) {
+        const int jj = j < nown ? j : 0;
+        slot[j] = mine ? k0 + jj : 0;
+        const size_t ro = (size_t)(mine ? rid[k0 + jj] : 0) * (size_t)vs;
+        bc[j] = bcw + j * 80 + h * 40;
+        yl[j] = y + ro + (size_t)ps * NV;
+        dUl[j] = dU + ro + (size_t)ps * NV;
+        bg[j] = b + ro + (size_t)ps * NV;
+    }
+    const uint64_t pol = tid == 0 ? policy_evict_first() : 0;
+    for (int t = lane; t < MULTI_RPW * 80; t += 32) bcw[t] = T(0);
+    __syncwarp();
+
+    auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
+    auto issue = [&](int job, int s) {
+        unsigned char *base = st0 + (size_t)s * stage;
+        uint32_t bytes = 0;
+        if (job < nf) {
+            if (job < nchT) bytes += cells(m, job) * (NB + nact * NV) * sizeof(T);
+            if (job < nchB) bytes += cells(nb, job) * (NB + nact * NV) * sizeof(T);
+        } else {
+            const int jb = job - nf;
+            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * NB * sizeof(T);
+            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * NB * sizeof(T);
+        }
+        mbar_arrive_expect_tx(&bars[s], bytes);
+        for (int hh = 0; hh < 2; ++hh) {
+            const int ln = hh ? nb : m, nc = hh ? nchB : nchT, cp = hh ? m : 0;
+            unsigned char *hb = base + hh * halfb;
+            if (job < nf) {
+                const int c = job;
+                if (c >= nc) continue;
+                const int cnt = cells(ln, c);
+                const size_t p = (size_t)(ps + cp + c * P);
+                bulk_g2s_hint(hb, G + p * NB, cnt * NB * sizeof(T), &bars[s], pol);
+                for (int k = 0; k < nact; ++k)
+                    bulk_g2s(hb + (size_t)(P * NB + k * P * NV) * sizeof(T),
+                             b + (size_t)rid[k] * (size_t)vs + p * NV, cnt * NV * sizeof(T), &bars[s]);
+            } else {
+                const int c = nc - 1 - (job - nf);
+                if (c < 0) continue;
+                const int cnt = cells(ln, c);
+                bulk_g2s_hint(hb, Gam + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(T),
+                              &bars[s], pol);
+            }
+        }
+    };
+    int issued = 0;
+    if (tid == 0) {
+        for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
+    }
+    int consumed = 0;
+    bool timed_out = false;
+    const int both_full = (m < nb ? m : nb) / P;
+
+    /* ---------------- forward */
+    for (int c = 0; c < nf; ++c) {
+        const int s = c % NS;
+        const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(c / NS) & 1u));
+        if (ok && mine) {
+            const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
+            const T *sB[MULTI_RPW];
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) sB[j] = sG + P * NB + slot[j] * P * NV;
+            if (c < both_full)
+                fwd_chunk_m<P, false>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
+            else
+                fwd_chunk_m<P, true>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
+            __syncwarp();
+        }
+        if (__syncthreads_or(!ok)) {
+            timed_out = true;
+            break;
+        }
+        ++consumed;
+        if (tid == 0 && issued < njobs) {
+            issue(issued, s);
+            ++issued;
+        }
+    }
+
+    if (!timed_out) {
+        /* ---------------- twist: x_m = b_m - G_tw y_top - Gam_tw y_bot */
+        const int ptw = n - 1;
+        T xm[MULTI_RPW];
+#pragma unroll
+        for (int j = 0; j < MULTI_RPW; ++j) xm[j] = T(0);
+        if (mine && lane < NV) {
+            const T *gr = G + (size_t)(ps + ptw) * NB + NV * lane;
+            const T *cr = Gam + (size_t)(ps + ptw) * NB + NV * lane;
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) {
+                const T *base = bcw + j * 80;
+                const T *ytop = base + 0 * 40 + (m & 1) * 20;
+                const T *ybot = base + 1 * 40 + (nb & 1) * 20;
+                T acc = bg[j][(size_t)ptw * NV + lane];
+#pragma unroll
+                for (int jj = 0; jj < NV; ++jj) acc -= gr[jj] * ytop[jj] + cr[jj] * ybot[jj];
+                xm[j] = acc;
+            }
+        }
+        __syncwarp();
+        if (mine && lane < NV) {
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j) {
+                if (j < nown) {
+                    T *base = bcw + j * 80;
+                    for (int t = 0; t < 4; ++t) {
+                        base[t * 20 + lane] = xm[j];
+                        base[t * 20 + 11 + lane] = xm[j];
+                    }
+                    dUl[j][(size_t)ptw * NV + lane] = xm[j];
+                }
+            }
+        }
+        __syncwarp();
+
+        /* ---------------- backward */
+        T yv[MULTI_RPW][P], nyv[MULTI_RPW][P];
+        auto load_chunk = [&](int c, T (*yy)[P]) {
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j)
+#pragma unroll
+                for (int q = 0; q < P; ++q) {
+                    const int k = c * P + q;
+                    yy[j][q] = T(0);
+                    if (j < nown && c >= 0 && k < len && writer)
+                        yy[j][q] = yl[j][(size_t)(cpos + k) * NV + i];
+                }
+        };
+        load_chunk(nch - 1, yv);
+        for (int jb = 0; jb < nf; ++jb) {
+            const int job = nf + jb;
+            const int c = nch - 1 - jb;
+            load_chunk(c - 1, nyv);
+            const int s = job % NS;
+            const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(job / NS) & 1u));
+            if (ok && mine) {
+                const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
+                const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
+                                  nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
+                if (full)
+                    bwd_chunk_m<P, false>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
+                else
+                    bwd_chunk_m<P, true>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
+                __syncwarp();
+            }
+            if (__syncthreads_or(!ok)) {
+                timed_out = true;
+                break;
+            }
+            ++consumed;
+            if (tid == 0 && issued < njobs) {
+                issue(issued, s);
+                ++issued;
+            }
+#pragma unroll
+            for (int j = 0; j < MULTI_RPW; ++j)
+#pragma unroll
+                for (int q = 0; q < P; ++q) yv[j][q] = nyv[j][q];
+        }
+    }
+    if (timed_out && tid == 0) {
+        atomicOr(status, ST_TIMEOUT);
+        for (int job = consumed; job < issued; ++job)
+            mbar_wait(&bars[job % NS], (uint32_t)(job / NS) & 1u, 1LL << 28);
+    }
+}
+
+static int multi_thomas_warps(int nr) { return (nr + MULTI_RPW - 1) / MULTI_RPW; }
+
+static size_t multi_thomas_stage(int nr) {
+    return 2 * (size_t)THOMAS_P * (NB + nr * NV) * sizeof(double);
+}
+
+static size_t multi_thomas_smem(int nr, int NS) {
+    return 128 + (size_t)NS * multi_thomas_stage(nr) +
+           (size_t)multi_thomas_warps(nr) * MULTI_RPW * 80 * sizeof(double);
+}
+
+/* ring depth: the shared memory each of the SM's resident lines may use,
+ * at least 3 and at most 8 stages */
+static int multi_thomas_ns(const FastLayout &L, int nr) {
+    int dev = 0, nsm = 148, smem_sm = 228 * 1024, reserved = 1024;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (nsm < 1) nsm = 148;
+    int per_sm = (L.nline + nsm - 1) / nsm;
+    const int by_threads = 2048 / (32 * multi_thomas_warps(nr));
+    if (per_sm > by_threads) per_sm = by_threads;
+    if (per_sm < 1) per_sm = 1;
+    const long long budget = (long long)smem_sm / per_sm - reserved - (long long)multi_thomas_smem(nr, 0);
+    long long ns = budget / (long long)multi_thomas_stage(nr);
+    if (ns > 8) ns = 8;
+    if (ns < 3) ns = 3;
+    return (int)ns;
+}
+
+int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const double *G,
+                        const double *Gam, const double *b, double *y, double *dU,
+                        const int *active, unsigned *status) {
+    if (L.nv != NV || nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
+    const int NS = multi_thomas_ns(L, nr);
+    const long long vs = (long long)L.np16 * NV;
+    multi_thomas_kernel<THOMAS_P><<<L.nline, 32 * multi_thomas_warps(nr), multi_thomas_smem(nr, NS), st>>>(
+        L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
+        status);
+    return (int)cudaGetLastError();
+}
+
+/* Residual of several right-hand sides per tile: Dinv and the cross-line
+ * blocks are staged once, then for every active right-hand side r
+ *   mode 0 (the start):  R = Rsrc_r (staged), U_r = 0
+ *   mode 1 (a sweep):    R = sum X dU_r (gathers of all r issued together),
+ *                        U_r += dU_r
+ * followed by b_r = -Dinv R and the tile's sum R^2 for r, each with the
+ * expressions (and summation order) of fast_resid_body.  The last CTA to
+ * finish adds every active r's partials in tile order (finalize_total's
+ * order), records the norms, retires the right-hand sides whose solve has
+ * ended and keeps the graph's loop running while any is active. */
+static size_t multi_resid_smem(int nx, int nr) {
+    const int nxa = nx > 0 ? nx : 1;
+    return 128 + (size_t)RES_TILE * NB * sizeof(double) * (1 + nx) +
+           (size_t)nr * nxa * RES_TILE * NV * sizeof(double) +
+           (size_t)nr * RES_TILE * NV * sizeof(double);
+}
+
+template <int MODE>
+__global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
+    MultiSys M, const double *__restrict__ Dinv, const double *__restrict__ X,
+    const int *__restrict__ xnbr, const double *__restrict__ Rsrc, unsigned long long handle,
+    int use_cond, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ unsigned amask_s, ticket;
+    __shared__ double red[MULTI_MAX][RES_THREADS_FAST / 32];
+    const int tid = threadIdx.x;
+    const int nx = MODE == 1 ? M.nx : 0;
+    const int nxa = nx > 0 ? nx : 1;
+    const int nr = M.nr;
+    const long long vs = (long long)M.np16 * NV;
+    const int ntiles = M.np16 / RES_TILE;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    double *sD = reinterpret_cast<double *>(smem + 128);
+    double *sX = sD + RES_TILE * NB;
+    double *sg = sX + nx * RES_TILE * NB; /* [k][s][c][i] gathers; mode 0: [k][c][i] R */
+    double *sr = sg + (size_t)nr * nxa * RES_TILE * NV; /* [k][c][i] R, then b */
+    __shared__ int rid[MULTI_MAX]; /* the k-th active right-hand side */
+    if (tid == 0) {
+        unsigned am = 0;
+        int k = 0;
+        for (int r = 0; r < nr; ++r)
+            if (MODE == 0 || M.active[r]) {
+                am |= 1u << r;
+                rid[k++] = r;
+            }
+        amask_s = am;
+        mbar_init(bar, 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const unsigned amask = amask_s;
+    const int nact = __popc(amask);
+    const int c = tid % RES_TILE, i = tid / RES_TILE;
+    const bool act = tid < RES_TILE * NV;
+    const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
+    uint32_t parity = 0;
+    bool failed = false;
+    for (int blk = blockIdx.x; blk < ntiles && nact > 0; blk += gridDim.x) {
+        const int p0 = blk * RES_TILE;
+        if (tid == 0) {
+            const uint64_t pol = policy_evict_first();
+            mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : nact * szR));
+            bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+            if (MODE == 1) {
+                for (int s = 0; s < nx; ++s)
+                    bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * M.np16 + p0) * NB, szD,
+                                  bar, pol);
+            } else {
+                int k = 0;
+                for (int r = 0; r < nr; ++r) {
+                    if (!((amask >> r) & 1u)) continue;
+                    bulk_g2s(sg + (size_t)k * RES_TILE * NV, Rsrc + (size_t)r * vs + (size_t)p0 * NV,
+                             szR, bar);
+                    ++k;
+                }
+            }
+        }
+        if (act) {
+            const size_t q = (size_t)p0 * NV + tid;
+            if (MODE == 1) {
+                /* every load of the tile (the neighbour dU gathers, U and dU
+                 * of each active r) is issued before the first store, so
+                 * that their latencies overlap */
+                int nbr[MULTI_NX];
+#pragma unroll
+                for (int s = 0; s < MULTI_NX; ++s)
+                    nbr[s] = s < nx ? __ldg(xnbr + (size_t)s * M.np16 + p0 + c) : -1;
+                double gv[MULTI_MAX][MULTI_NX], uv[MULTI_MAX], dv[MULTI_MAX];
+#pragma unroll
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    uv[k] = dv[k] = 0.0;
+#pragma unroll
+                    for (int s = 0; s < MULTI_NX; ++s) gv[k][s] = 0.0;
+                    if (k < nact) {
+                        const size_t ro = (size_t)rid[k] * vs;
+#pragma unroll
+                        for (int s = 0; s < MULTI_NX; ++s)
+                            if (nbr[s] >= 0) gv[k][s] = __ldg(M.dU + ro + (size_t)nbr[s] * NV + i);
+                        uv[k] = M.U[ro + q];
+                        dv[k] = __ldg(M.dU + ro + q);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
+#pragma unroll
+                        for (int s = 0; s < MULTI_NX; ++s)
+                            if (s < nx) sg[((size_t)(k * nx + s) * RES_TILE + c) * NV + i] = gv[k][s];
+                        M.U[(size_t)rid[k] * vs + q] = uv[k] + dv[k];
+                    }
+                }
+            } else {
+                for (int k = 0; k < nact; ++k) M.U[(size_t)rid[k] * vs + q] = 0.0;
+            }
+        }
+        const bool ok = mbar_wait(bar, parity);
+        parity ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(status, ST_TIMEOUT);
+                mbar_wait(bar, parity ^ 1u, 1LL << 28);
+            }
+            failed = true;
+            break;
+        }
+        /* R for every active r: the row of each slot's block is read once
+         * and feeds every r; per r the products are added in
+         * fast_resid_body's order (slots ascending, three accumulators) */
+        double sq[MULTI_MAX];
+#pragma unroll
+        for (int k = 0; k < MULTI_MAX; ++k) sq[k] = 0.0;
+        if (act) {
+            if (MODE == 1) {
+                double a0[MULTI_MAX], a1[MULTI_MAX], a2[MULTI_MAX];
+#pragma unroll
+                for (int k = 0; k < MULTI_MAX; ++k) a0[k] = a1[k] = a2[k] = 0.0;
+                for (int s = 0; s < nx; ++s) {
+                    const double *xr = sX + (s * RES_TILE + c) * NB + i;
+                    double x[NV];
+#pragma unroll
+                    for (int j = 0; j < NV; ++j) x[j] = xr[9 * j];
+#pragma unroll
+                    for (int k = 0; k < MULTI_MAX; ++k) {
+                        if (k < nact) {
+                            const double *g = sg + ((size_t)(k * nx + s) * RES_TILE + c) * NV;
+                            a0[k] += x[0] * g[0];
+                            a1[k] += x[1] * g[1];
+                            a2[k] += x[2] * g[2];
+                            a0[k] += x[3] * g[3];
+                            a1[k] += x[4] * g[4];
+                            a2[k] += x[5] * g[5];
+                            a0[k] += x[6] * g[6];
+                            a1[k] += x[7] * g[7];
+                            a2[k] += x[8] * g[8];
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
+                        const double rr = a0[k] + (a1[k] + a2[k]);
+                        sr[(size_t)k * RES_TILE * NV + c * NV + i] = rr;
+                        sq[k] = rr * rr;
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
+                        const double rr = sg[(size_t)k * RES_TILE * NV + c * NV + i];
+                        sq[k] = rr * rr;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        /* b = -Dinv R for every active r (into sg, free now); the row of
+         * Dinv is read once */
+        const double *rsrc = MODE == 1 ? sr : sg;
+        double *sb = MODE == 1 ? sg : sr;
+        if (act) {
+            const double *drow = sD + c * NB + i;
+            double dr[NV];
+#pragma unroll
+            for (int j = 0; j < NV; ++j) dr[j] = drow[9 * j];
+#pragma unroll
+            for (int k = 0; k < MULTI_MAX; ++k) {
+                if (k < nact) {
+                    const double *rv = rsrc + (size_t)k * RES_TILE * NV + c * NV;
+                    double a0 = dr[0] * rv[0], a1 = dr[1] * rv[1], a2 = dr[2] * rv[2];
+                    a0 += dr[3] * rv[3];
+                    a1 += dr[4] * rv[4];
+                    a2 += dr[5] * rv[5];
+                    a0 += dr[6] * rv[6];
+                    a1 += dr[7] * rv[7];
+                    a2 += dr[8] * rv[8];
+                    sb[(size_t)k * RES_TILE * NV + c * NV + i] = -(a0 + (a1 + a2));
+                }
+            }
+        }
+        __syncthreads();
+        if (act) {
+            int k = 0;
+            for (int r = 0; r < nr; ++r) {
+                if (!((amask >> r) & 1u)) continue;
+                M.b[(size_t)r * vs + (size_t)p0 * NV + tid] = sb[(size_t)k * RES_TILE * NV + tid];
+                ++k;
+            }
+        }
+        /* the tile's sum R^2 per r, in fast_resid_body's order */
+#pragma unroll
+        for (int k = 0; k < MULTI_MAX; ++k) {
+            if (k < nact) {
+                double v = sq[k];
+                for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
+                if ((tid & 31) == 0) red[k][tid >> 5] = v;
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            int k = 0;
+            for (int r = 0; r < nr; ++r) {
+                if (!((amask >> r) & 1u)) continue;
+                double tot = 0.0;
+                for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[k][w];
+                M.partials[(size_t)r * ntiles + blk] = tot;
+                ++k;
+            }
+        }
+        __syncthreads(); /* the next tile's copies overwrite the stages */
+    }
+    (void)failed;
+
+    /* ---------------- the last CTA: norms of every active r */
+    __syncthreads();
+    if (tid == 0) {
+        __threadfence();
+        ticket = atomicAdd(M.counter, 1u);
+    }
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return;
+    __threadfence();
+    __shared__ int any_go;
+    if (tid == 0) any_go = 0;
+    for (int r = 0; r < nr; ++r) {
+        if (!((amask >> r) & 1u)) continue;
+        double acc = strided_sum(M.partials + (size_t)r * ntiles, ntiles, (int)blockDim.x);
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
+        __syncthreads(); /* red[0] of the previous r is read */
+        if ((tid & 31) == 0) red[0][tid >> 5] = acc;
+        __syncthreads();
+        if (tid == 0) {
+            double tot = 0.0;
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[0][w];
+            const double nrm = sqrt(tot);
+            SolveState *S = M.state + r;
+            if (MODE == 0) {
+                S->sweep = 0;
+                S->norm0 = nrm;
+            } else {
+                S->sweep += 1;
+            }
+            const int sw = S->sweep;
+            if (sw < S->hist_cap) M.hist[(size_t)r * M.hist_stride + sw] = nrm;
+            S->last = nrm;
+            const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
+            M.active[r] = go ? 1 : 0;
+            if (go) any_go = 1;
+        }
+    }
+    __syncthreads();
+    if (tid == 0) {
+        if (use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)handle, any_go ? 1u : 0u);
+        *M.counter = 0u;
+    }
+}
+
+int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const MultiSys &M,
+                       const double *Dinv, const double *X, const double *Rsrc,
+                       unsigned long long cond_handle, int use_cond, unsigned *status) {
+    if (L.nv != NV || M.nr < 1 || M.nr > MULTI_MAX || (mode != 0 && mode != 1))
+        return (int)cudaErrorInvalidValue;
+    const int ntiles = L.np16 / RES_TILE;
+    if (mode == 1) {
+        const size_t smem = multi_resid_smem(L.nx, M.nr);
+        multi_resid_kernel<1><<<resid_grid_persistent((const void *)multi_resid_kernel<1>, smem, ntiles),
+                                RES_THREADS_FAST, smem, st>>>(M, Dinv, X, L.xnbr, nullptr,
+                                                              cond_handle, use_cond, status);
+    } else {
+        const size_t smem = multi_resid_smem(0, M.nr);
+        multi_resid_kernel<0><<<resid_grid_persistent((const void *)multi_resid_kernel<0>, smem, ntiles),
+                                RES_THREADS_FAST, smem, st>>>(M, Dinv, nullptr, nullptr, Rsrc,
+                                                              cond_handle, use_cond, status);
+    }
+    return (int)cudaGetLastError();
+}
+
+/* opt the multi-RHS kernels into the shared memory of nr right-hand sides
+ * (outside stream capture) */
+int multi_prepare(const FastLayout &L, int nr) {
+    if (nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
+    int rc = set_smem((const void *)multi_thomas_kernel<THOMAS_P>,
+                      multi_thomas_smem(nr, multi_thomas_ns(L, nr)));
+    if (!rc) rc = set_smem((const void *)multi_resid_kernel<1>, multi_resid_smem(L.nx, nr));
+    if (!rc) rc = set_smem((const void *)multi_resid_kernel<0>, multi_resid_smem(0, nr));
+    return rc;
+}
+
 }  // namespace tbs

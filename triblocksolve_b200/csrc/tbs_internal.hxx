@@ -214,6 +214,33 @@ int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
 int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
                        double *Up, double *partials, const float *Dinv32, float *b32, float *c32);
 
+/* ------------------------------------- several right-hand sides (FP64)
+ * Up to MULTI_MAX right-hand sides of one system swept together, the line
+ * blocks read once per sweep for all of them.  Vectors are RHS-major with
+ * stride np16 * 9; state, active and the history rows are per right-hand
+ * side, partials [nr][np16 / RES_TILE]. */
+constexpr int MULTI_MAX = 8;
+constexpr int MULTI_NX = 4;     /* cross-line slots per position of the fast layout */
+struct MultiSys {
+    int nr, np16, nx, hist_stride;
+    double *U, *b, *partials, *hist;
+    const double *dU;
+    SolveState *state;
+    int *active;
+    unsigned *counter;
+};
+/* dU of every active right-hand side from its b (the line solves) */
+int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const double *G,
+                        const double *Gam, const double *b, double *y, double *dU,
+                        const int *active, unsigned *status);
+/* mode 0: R = Rsrc (position order, RHS-major), U = 0, the solve's start
+ * (every r becomes active); mode 1: R = sum X dU, U += dU.  Then b = -Dinv R,
+ * the norms, and the graph condition (any right-hand side still active). */
+int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const MultiSys &M,
+                       const double *Dinv, const double *X, const double *Rsrc,
+                       unsigned long long cond_handle, int use_cond, unsigned *status);
+int multi_prepare(const FastLayout &L, int nr);
+
 /* ------------------------------------------------------------ batches
  * Many independent systems swept together.  Each kernel takes one
  * descriptor per system and a list of work items (system, unit), so that

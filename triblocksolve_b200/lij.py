@@ -316,6 +316,31 @@ class Solver:
         self._chk(N.lib.tbs_solve(self.ctx, rel_tol, max_sweeps, C.byref(s), N.dptr(h)))
         return s.value, h[: s.value + 1]
 
+    def solve_multi(self, rhs: np.ndarray, rel_tol: float, max_sweeps: int = 1000):
+        """Several right-hand sides (rows of ``rhs``, 9*nelem each) from U = 0
+        with the current factors (ALGO_FP64), groups of up to 8 sweeping
+        together.  Returns (U [nrhs, 9*nelem], sweeps [nrhs], list of norm
+        histories); each row equals ``set_rhs`` + ``solve`` of it alone."""
+        n = self.nvar * self.nelem
+        rhs = np.ascontiguousarray(rhs, np.float64).reshape(-1, n)
+        nrhs = rhs.shape[0]
+        U = np.zeros((nrhs, n))
+        sw = np.zeros(nrhs, np.int32)
+        h = np.zeros((nrhs, max_sweeps + 1))
+        self._chk(N.lib.tbs_solve_multi(self.ctx, nrhs, N.dptr(rhs), N.dptr(U), rel_tol,
+                                        max_sweeps, N.iptr(sw), N.dptr(h), max_sweeps + 1))
+        return U, sw, [h[r, : sw[r] + 1].copy() for r in range(nrhs)]
+
+    def solve_multi_device(self, d_rhs: int, d_U: int, nrhs: int, rel_tol: float,
+                           max_sweeps: int = 1000):
+        """``solve_multi`` on device buffers (addresses of nrhs * 9*nelem
+        doubles, element order).  Returns (sweeps [nrhs], norm histories)."""
+        sw = np.zeros(nrhs, np.int32)
+        h = np.zeros((nrhs, max_sweeps + 1))
+        self._chk(N.lib.tbs_solve_multi_device(self.ctx, nrhs, d_rhs, d_U, rel_tol, max_sweeps,
+                                               N.iptr(sw), N.dptr(h), max_sweeps + 1))
+        return sw, [h[r, : sw[r] + 1].copy() for r in range(nrhs)]
+
     def _vec(self, fn):
         out = np.zeros(self.nvar * self.nelem)
         self._chk(fn(self.ctx, N.dptr(out)))
