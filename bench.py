@@ -656,6 +656,140 @@ def run_batch_reference(args):
     return 0
 
 
+def run_multi(args, L, K, shift, tol):
+    """--nrhs N (N > 1): N right-hand sides of one system solved together per
+    step through tbs_solve_multi_device (FP64; groups of up to 8 read the
+    line blocks once per sweep).  value = right-hand-side sweeps per second;
+    e2e = tbs_solve_multi from pinned host arrays (right-hand sides in,
+    solutions out)."""
+    import torch
+
+    import triblocksolve_b200 as tbs
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    nrhs = args.nrhs
+    mesh, host = build_problem(L, K, shift, pinned=True)
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    solver = tbs.Solver(local)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_mesh(mesh)
+    solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+    solver.factor(tbs.ALGO_FP64)
+    n = 9 * mesh.nelem
+    rows = torch.empty((nrhs, n), dtype=torch.float64, pin_memory=True).numpy()
+    rows[0] = host["rhs"]
+    rng = np.random.default_rng(SEED)
+    for r in range(1, nrhs):
+        rows[r] = rng.uniform(-1, 1, n)
+    d_rhs = torch.from_numpy(rows).to(f"cuda:{local}", non_blocking=False)
+    d_U = torch.zeros_like(d_rhs)
+    Uh = torch.empty((nrhs, n), dtype=torch.float64, pin_memory=True).numpy()
+    max_sweeps = 400
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 0)):
+            solver.solve_multi_device(d_rhs.data_ptr(), d_U.data_ptr(), nrhs, tol, max_sweeps)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        sweeps_total = 0
+        for _ in range(args.steps):
+            sw, _h = solver.solve_multi_device(d_rhs.data_ptr(), d_U.data_ptr(), nrhs, tol,
+                                               max_sweeps)
+            sweeps_total += int(sw.sum())
+        t1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        elapsed_ms = t0.elapsed_time(t1)
+        solver.profile(True)
+        solver.profile_reset()
+        nprof = max(1, min(args.steps, 10))
+        for _ in range(nprof):
+            solver.solve_multi_device(d_rhs.data_ptr(), d_U.data_ptr(), nrhs, tol, max_sweeps)
+        prof = solver.profile_read()
+        solver.profile(False)
+        ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 10))
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_sweeps = 0
+        for _ in range(ne2e):
+            U, sw, _h = solver.solve_multi(rows, tol, max_sweeps)
+            Uh[:] = U
+            e2e_sweeps += int(sw.sum())
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.summary()
+    max_ms = dist.reduce(elapsed_ms, "max")
+    all_sweeps = dist.reduce(sweeps_total, "sum")
+    max_e2e_ms = dist.reduce(e2e_ms, "max")
+    all_e2e = dist.reduce(e2e_sweeps, "sum")
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        g = min(nrhs, 8)
+        kern = {}
+        for name, (launches, ms) in prof.items():
+            b = None
+            if name in ("multi_thomas", "multi_resid"):
+                b = solver.kernel_bytes(f"{name}/{g}")
+            avg_us = 1e3 * ms / launches if launches else 0.0
+            kern[name] = {"launches": launches, "total_ms": round(ms, 4), "avg_us": round(avg_us, 3),
+                          "bytes_per_launch": b,
+                          "gbs": round(b / (avg_us * 1e-6) / 1e9, 1) if b and avg_us > 0 else None}
+        hot = [k for k in kern if kern[k]["bytes_per_launch"]]
+        dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
+        roof = None
+        if dom:
+            ach = kern[dom]["gbs"]
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "traffic": None,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": kern[dom]["bytes_per_launch"],
+                    "avg_launch_us": kern[dom]["avg_us"],
+                    "note": "algorithmic bytes with every right-hand side of the group active"}
+        line = {
+            "metric": "LIJ sweeps/s", "value": round(all_sweeps / (max_ms * 1e-3), 2),
+            "unit": "sweeps/s (one right-hand side each)", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 5),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured mesh and values (shift %g, seed %d); right-hand "
+                    "side 0 is the generated rhs, the others seeded U(-1,1)" % (shift, SEED),
+            "config": {
+                "workload": f"{nrhs} right-hand sides of one LIJ system solved together to {tol:g} "
+                            f"from U=0, {L} lines x {K} cells ({mesh.nelem} cells), FP64, "
+                            f"groups of up to 8",
+                "cells": mesh.nelem, "nrhs": nrhs, "tol": tol,
+                "rhs_sweeps_per_step": all_sweeps / ws / args.steps,
+                "ms_per_rhs_solve": round(max_ms / args.steps / nrhs, 4),
+                "l2": "no flush: every sweep streams the line blocks (> 126 MB L2)",
+                "parallelism": f"{ws} independent systems, one per GPU" if ws > 1 else "1 GPU",
+            },
+            "roofline": roof, "kernels": kern,
+            "e2e": {"value": round(all_e2e / (max_e2e_ms * 1e-3), 2),
+                    "unit": "sweeps/s (one right-hand side each)",
+                    "h2d_bytes_per_step": int(rows.nbytes), "d2h_bytes_per_step": int(Uh.nbytes),
+                    "steps": ne2e,
+                    "what": "per step: tbs_solve_multi from pinned host arrays (right-hand "
+                            "sides in, solutions out), factors resident"},
+            "gpu_launches": int(round(sum(v["launches"] for v in kern.values()) / nprof * args.steps)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    dist.close()
+    return 0
+
+
 def run_reference(args, L, K, shift, tol):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -698,9 +832,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2",
                     choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS))
-    ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed"])
+    ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed", "pij"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nrhs", type=int, default=1,
+                    help="right-hand sides per solve (> 1: tbs_solve_multi, FP64)")
     args = ap.parse_args()
     if args.config in SERVE_CONFIGS:
         if args.impl == "reference":
@@ -713,6 +849,10 @@ def main():
     L, K, shift, tol = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, L, K, shift, tol)
+    if args.nrhs > 1:
+        if args.algo != "fp64":
+            ap.error("--nrhs > 1 needs --algo fp64")
+        return run_multi(args, L, K, shift, tol)
 
     import torch
 
@@ -720,7 +860,8 @@ def main():
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = Dist(ws, rank, local, "nccl")
-    algo = {"fp64": tbs.ALGO_FP64, "ref": tbs.ALGO_REFERENCE, "mixed": tbs.ALGO_MIXED}[args.algo]
+    algo = {"fp64": tbs.ALGO_FP64, "ref": tbs.ALGO_REFERENCE, "mixed": tbs.ALGO_MIXED,
+            "pij": tbs.ALGO_PIJ}[args.algo]
 
     mesh, host = build_problem(L, K, shift, pinned=True)
     # a dedicated stream: CUDA graphs cannot be captured on the legacy default stream
@@ -846,7 +987,7 @@ def main():
             "ms_per_step": round(max_ms / args.steps, 5), "higher_is_better": True,
             "scaling": "weak",
             "vs_baseline": (round(value / ws / PUBLISHED_SWEEPS_PER_S[args.config], 3)
-                            if args.config in PUBLISHED_SWEEPS_PER_S and args.algo != "mixed"
+                            if args.config in PUBLISHED_SWEEPS_PER_S and args.algo in ("fp64", "ref")
                             else None),
             "dtype": "f64" if args.algo != "mixed" else "f32+f64",
             "data": "synthetic: seeded structured mesh and values (shift %g, seed %d); the "
@@ -879,7 +1020,12 @@ def main():
             "clocks": clk,
         }
         if ws == 1 and not args.no_cpu_baseline:
-            line["cpu_baseline"] = cpu_baseline(mesh, host)
+            if args.algo == "pij":
+                import oracle
+                line["cpu_baseline"] = cpu_baseline(oracle.point_lines(mesh), host)
+                line["cpu_baseline"]["sample"] += " (one-cell lines: the point-implicit sweep)"
+            else:
+                line["cpu_baseline"] = cpu_baseline(mesh, host)
         print(json.dumps(line), flush=True)
     solver.close()
     dist.close()

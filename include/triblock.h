@@ -53,10 +53,16 @@ extern "C" {
  * TBS_ALGO_MIXED      FP32 line factors and FP32 inner sweeps on the
  *                     correction equation; residual, solution accumulation
  *                     and convergence test in FP64 (outer refinement).
+ * TBS_ALGO_PIJ        point-implicit Jacobi, the line sweep's sibling with
+ *                     the diagonal block alone as the implicit operator
+ *                     (dU = -D^-1 R, U += dU, R = rhs + J U; every cell its
+ *                     own line), FP64, residual updated from the face
+ *                     couplings like TBS_ALGO_FP64.
  */
 #define TBS_ALGO_REFERENCE 0
 #define TBS_ALGO_FP64      1
 #define TBS_ALGO_MIXED     2
+#define TBS_ALGO_PIJ       3
 
 /* compute modes of the reference CLI (include/Platform.hxx:17-23) */
 #define TBS_SERIAL_MODE 0
@@ -277,7 +283,9 @@ int tbs_profile_read(tbs_ctx *ctx, int *n, const char **names,
                      long long *launches, double *ms);
 
 /* Algorithmic bytes one launch of each kernel moves (reads + writes of
- * every array it must touch once), for the roofline numerator. */
+ * every array it must touch once), for the roofline numerator.  The
+ * multi-RHS kernels take the group size as a suffix: "multi_thomas/8",
+ * "multi_resid/8" (every right-hand side active). */
 int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
 
 /* Linear residual R = rhs + J U (the rule of the reference's lineRes) and

@@ -98,6 +98,33 @@ def lij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1, want_factor
     return out
 
 
+def point_lines(mesh):
+    """The mesh with every cell as its own line, faces unchanged.
+
+    The reference's line sweep (src/main.cxx:180-229) on it solves the
+    diagonal block alone per cell, dU = -D^-1 R (LU of lineLU_v2.okl:17-27,
+    solveLU of :30-52), then U += dU and R = rhs + J U over all faces: the
+    point-implicit Jacobi sweep of the paper (p.10-11, Table 4), which the
+    reference repository has no code for.  lineface is never read for the
+    first cell of a line, so it holds boundary markers."""
+    from types import SimpleNamespace
+    n = int(mesh.nelem)
+    return SimpleNamespace(
+        nvar=int(mesh.nvar), nelem=n, nintface=int(mesh.nintface), eftot=int(mesh.eftot),
+        nline=n, nlineelem=n, max_line_nelem=1 if n else 0,
+        epoint=np.ascontiguousarray(mesh.epoint, np.int32),
+        ef=np.ascontiguousarray(mesh.ef, np.int32), fc=np.ascontiguousarray(mesh.fc, np.int32),
+        linesize=np.ones(n, np.int32), linepoint=np.arange(n + 1, dtype=np.int32),
+        lines=np.arange(n, dtype=np.int32), lineface=np.full(n, -1, np.int32))
+
+
+def pij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1):
+    """Point-implicit Jacobi for `iters` sweeps from U = 0 in the reference's
+    operation order: the line sweep on point_lines(mesh).  Returns
+    dict(U, R, dU, hist) like lij."""
+    return lij(point_lines(mesh), jacD, jacO1, jacO2, rhs, iters, threads)
+
+
 def resize_block_size(nv_old, nv_new, nelem, nintface, D, O1, O2, rhs, U0):
     """Jacobian.cxx:153-238 restated; returns the new (D, O1, O2, rhs, U0)."""
     bn = nv_new * nv_new

@@ -98,3 +98,12 @@ def ragged_mesh(lens, seed=0, nvar=9, permute=True) -> Mesh:
 
 def problem(mesh: Mesh, shift=9.0, seed=1) -> Jacobian:
     return Jacobian.generate(mesh, shift, seed)
+
+
+def point_mesh(mesh: Mesh) -> Mesh:
+    """The same cells and faces with every cell its own line (the line sweep
+    on it is the point-implicit Jacobi sweep)."""
+    n = mesh.nelem
+    return Mesh.from_arrays(mesh.nvar, epoint=mesh.epoint, ef=mesh.ef, fc=mesh.fc,
+                            linesize=np.ones(n, np.int32), linepoint=np.arange(n + 1, dtype=np.int32),
+                            lines=np.arange(n, dtype=np.int32), lineface=np.full(n, -1, np.int32))

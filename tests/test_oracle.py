@@ -134,3 +134,30 @@ def test_assemble_triblocks_matches_oracle():
                                  j.jacO1.ctypes.data_as(dp), j.jacO2.ctypes.data_as(dp),
                                  A.ctypes.data_as(dp))
     np.testing.assert_array_equal(j.A[:A.size], A)
+
+
+@pytest.mark.parametrize("lens,shift,seed", [([6, 6, 6, 6], 9.0, 1), ([5, 1, 7, 3, 3, 8], 4.0, 2),
+                                             ([12], 9.0, 4)])
+def test_oracle_pij_against_dense(lens, shift, seed):
+    """oracle.pij (the line sweep on one-cell lines) is the point-implicit
+    Jacobi iteration dU = -D^-1 R, U += dU, R = rhs + J U, written densely."""
+    m = ragged_mesh(lens, seed=seed)
+    j = Jacobian.generate(m, shift, seed)
+    J, _ = dense_system(m, j)
+    nv = m.nvar
+    D = blocks(j.jacD, nv)
+    U = np.zeros(J.shape[0])
+    R = j.rhs.copy()
+    hist = [np.linalg.norm(R)]
+    for _ in range(8):
+        dU = -np.linalg.solve(D, R.reshape(-1, nv, 1)).reshape(-1)
+        U = U + dU
+        R = j.rhs + J @ U
+        hist.append(np.linalg.norm(R))
+    r = oracle.pij(m, j.jacD, j.jacO1, j.jacO2, j.rhs, 8)
+    assert np.linalg.norm(r["U"] - U) <= 1e-12 * np.linalg.norm(U)
+    np.testing.assert_allclose(r["hist"], hist, rtol=0, atol=1e-12 * hist[0])
+    # it converges more slowly than the line sweep on the same system
+    lij = oracle.lij(m, j.jacD, j.jacO1, j.jacO2, j.rhs, 8)
+    if len(lens) > 1:
+        assert lij["hist"][-1] < r["hist"][-1]

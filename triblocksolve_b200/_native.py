@@ -31,6 +31,7 @@ TBS_ERR_NOMEM = 8
 ALGO_REFERENCE = 0
 ALGO_FP64 = 1
 ALGO_MIXED = 2
+ALGO_PIJ = 3
 
 CUDA_MODE = 2
 

@@ -20,6 +20,7 @@
 #include <cmath>
 #include <cstddef>
 #include <cstring>
+#include <cstdlib>
 #include <new>
 #include <string>
 #include <vector>
@@ -454,8 +455,11 @@ static int prime(tbs_ctx *ctx, CondCtl cc) {
         return reduce(ctx, np, 1, cc);
     }
     const FastLayout &L = ctx->L;
-    if (ctx->algo == TBS_ALGO_FP64) {
+    if (ctx->algo == TBS_ALGO_FP64 || ctx->algo == TBS_ALGO_PIJ) {
+        const bool pij = ctx->algo == TBS_ALGO_PIJ;
         const double *Rsrc = ctx->d_rhsp;
+        /* TBS_ALGO_PIJ: the first update goes to buffer A (d_b), parity 0 */
+        if (pij) CK(cudaMemsetAsync(&ctx->d_state->pad, 0, sizeof(int), st));
         if (ctx->d_Uinit) {
             RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
             RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
@@ -465,7 +469,7 @@ static int prime(tbs_ctx *ctx, CondCtl cc) {
             Rsrc = ctx->d_Rp;
         }
         /* from U = 0 the same launch clears U */
-        RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
+        RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, pij ? nullptr : ctx->d_X, ctx->d_dUp,
                                                         Rsrc, ctx->d_b, sink(ctx, 1, cc),
                                                         ctx->d_status,
                                                         ctx->d_Uinit ? nullptr : ctx->d_Up));
@@ -513,6 +517,11 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
         return reduce(ctx, np, 0, cc);
     }
     const FastLayout &L = ctx->L;
+    if (ctx->algo == TBS_ALGO_PIJ) {
+        RUN("pij_sweep", launch_pij_sweep(st, L, ctx->d_Dinv, ctx->d_XF, ctx->d_b, ctx->d_dUp, ctx->d_Up,
+                                          sink(ctx, 0, cc), ctx->d_status));
+        return TBS_OK;
+    }
     if (ctx->algo == TBS_ALGO_FP64) {
         /* the Thomas kernel writes dU; the residual kernel adds it to U */
         RUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
@@ -696,6 +705,13 @@ static int alloc_algo(tbs_ctx *ctx, int algo) {
     DA(ctx->d_Up, npv);
     DA(ctx->d_rhsp, npv);
     DA(ctx->d_Rp, npv);
+    if (algo == TBS_ALGO_PIJ) {
+        DA(ctx->d_Dinv, npb); /* D^-1 per position, built in place */
+        if (L.nxf > 0) DA(ctx->d_XF, (size_t)L.np16 * L.nxf * bs);
+        DA(ctx->d_dUp, npv);  /* the two update buffers */
+        DA(ctx->d_b, npv);
+        return TBS_OK;
+    }
     if (algo == TBS_ALGO_FP64) {
         DA(ctx->d_Dinv, npb);
         DA(ctx->d_G, npb);
@@ -743,6 +759,13 @@ static int run_factor(tbs_ctx *ctx, int algo) {
     const FastLayout &L = ctx->L;
     CKL(fast_prepare(L));
     RUN("permute", launch_permute_to_pos(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_rhs, ctx->d_rhsp));
+    if (algo == TBS_ALGO_PIJ) {
+        CKL(pij_prepare(L));
+        RUN("fullpos_layout", launch_fullpos_layout(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                    ctx->d_Dinv, ctx->d_XF));
+        RUN("pij_invert", launch_pij_invert(st, L, ctx->d_Dinv, ctx->d_status));
+        return TBS_OK;
+    }
     if (algo == TBS_ALGO_FP64) {
         RUN("fast_factor", launch_fast_factor(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,
                                               ctx->d_G, ctx->d_Gam, nullptr, nullptr, nullptr,
@@ -942,9 +965,13 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
     GUARD_BEGIN
     CK(cudaSetDevice(ctx->device));
     if (!ctx->have_jac) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_jacobian must come first");
-    if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_FP64 && algo != TBS_ALGO_MIXED)
+    if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_FP64 && algo != TBS_ALGO_MIXED &&
+        algo != TBS_ALGO_PIJ)
         return ctx_fail(ctx, TBS_ERR_ARG, "unknown algorithm " + std::to_string(algo));
-    if (algo != TBS_ALGO_REFERENCE && !ctx->layout_ok)
+    if (algo == TBS_ALGO_PIJ && (ctx->nvar != 9 || !fullpos_ok(ctx)))
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
+                        "TBS_ALGO_PIJ needs nvar == 9 and at most 4 interior faces per cell");
+    if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_PIJ && !ctx->layout_ok)
         return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
                         "TBS_ALGO_FP64 / TBS_ALGO_MIXED need nvar == 9 and at most 4 cross-line "
                         "faces per cell; use TBS_ALGO_REFERENCE");
@@ -1087,6 +1114,13 @@ static int get_vec(tbs_ctx *ctx, int which, double *out) {
             RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_Rp, ctx->d_scratch));
         } else if (ctx->algo == TBS_ALGO_FP64) {
             RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_dUp, ctx->d_scratch));
+        } else if (ctx->algo == TBS_ALGO_PIJ) {
+            /* the last sweep added the buffer it read: A (d_b) when the
+             * parity it flipped is now 1 */
+            int rc = read_state(ctx);
+            if (rc) return rc;
+            const double *du = (ctx->h_state->pad & 1) ? ctx->d_b : ctx->d_dUp;
+            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, du, ctx->d_scratch));
         } else {
             RUN("permute", launch_permute_f32_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_c32, ctx->d_scratch));
             /* the outer correction is c + d (see body()); add d */
@@ -1322,6 +1356,17 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     else if (k == "ref_line_res")
         b = N * blk + 2 * F * blk + N * vec + 2 * F * vec + 2 * N * vec +
             4.0 * (N + 1 + ctx->eftot + 2 * F);
+    else if (k.rfind("multi_thomas/", 0) == 0 || k.rfind("multi_resid/", 0) == 0) {
+        const int nr = std::atoi(k.c_str() + k.find('/') + 1);
+        if (nr >= 1 && nr <= MULTI_MAX) {
+            if (k[6] == 't') /* G, Gam once; per r: b in, y out and back in, dU out */
+                b = N * 2 * blk + nr * N * 4 * vec;
+            else /* Dinv, X blocks + xnbr once; per r: neighbour dU, b out, own dU + U in/out */
+                b = N * blk + X * (blk + 4.0) + nr * (N * 4 * vec + X * vec);
+        }
+    }
+    else if (k == "pij_sweep") /* Dinv, face blocks + index + neighbour dU, own dU, U in/out, b out */
+        b = N * (blk + 4 * vec) + (double)ctx->n_fslots_real * (blk + 4.0 + vec);
     else if (k == "fast_factor") /* D, A, C in; Dinv, G, Gam out */
         b = N * blk + 2 * (N - ctx->nline) * blk + 3 * N * blk;
     if (b < 0) return ctx_fail(ctx, TBS_ERR_ARG, "unknown kernel name " + k);

@@ -606,20 +606,20 @@ int fast_resid_grid(int np16) { return np16 / RES_TILE > 0 ? np16 / RES_TILE : 1
  * the n per-tile partials in a fixed order and, when asked, records the
  * norm like reduce_norm (history, sweep count, graph loop condition).
  * Called by every thread of the block. */
-__device__ void finalize_total(const NormSink &ns, int n) {
+__device__ bool finalize_total(const NormSink &ns, int n) {
     __shared__ unsigned ticket;
     __shared__ double red[32];
-    if (!ns.partials || !ns.counter) return;
+    if (!ns.partials || !ns.counter) return false;
     __syncthreads(); /* this CTA's partials are written */
     if (threadIdx.x == 0) {
         __threadfence();
         ticket = atomicAdd(ns.counter, 1u);
     }
     __syncthreads();
-    if (ticket != gridDim.x - 1) return;
+    if (ticket != gridDim.x - 1) return false;
     if (!ns.state) {
         if (threadIdx.x == 0) *ns.counter = 0u;
-        return;
+        return true;
     }
     __threadfence();
     double acc = strided_sum(ns.partials, n, (int)blockDim.x);
@@ -644,6 +644,7 @@ __device__ void finalize_total(const NormSink &ns, int n) {
         if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
         *ns.counter = 0u;
     }
+    return true;
 }
 
 template <typename T>
@@ -783,7 +784,7 @@ __device__ __forceinline__ bool fast_resid_body(
  * writes its partial; finalize_total then sums the tiles' partials in tile
  * order (the order of the batched norm kernel with 160 threads). */
 template <typename T>
-__device__ __forceinline__ void resid_tiles(int nx, int np16, int mode, const T *Dinv, const T *X,
+__device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T *Dinv, const T *X,
                                             const int *xnbr, const T *dU, const T *Rsrc, T *b,
                                             T *Uacc, const NormSink &ns, unsigned *status) {
     uint64_t *bar = resid_bar_init();
@@ -796,7 +797,7 @@ __device__ __forceinline__ void resid_tiles(int nx, int np16, int mode, const T 
         if (!ok) break;
         __syncthreads(); /* the next tile's copies overwrite the stages */
     }
-    finalize_total(ns, ntiles);
+    return finalize_total(ns, ntiles);
 }
 
 /* mode 1 (R = sum X dU over the cross-line slots) */
@@ -2765,6 +2766,73 @@ int multi_prepare(const FastLayout &L, int nr) {
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<1>, multi_resid_smem(L.nx, nr));
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<0>, multi_resid_smem(0, nr));
     return rc;
+}
+
+
+/* ================================================ point-implicit Jacobi
+ * TBS_ALGO_PIJ: the sweep dU = -D^-1 R, U += dU, R = rhs + J U with the
+ * diagonal block alone as the implicit operator (every cell its own
+ * line).  As for the line form, D dU = -R makes the new residual
+ * R + J dU = sum over the interior faces of offJ dU_nbr, so one sweep is
+ * one streaming launch of the residual kernel over the position-ordered
+ * face blocks (slot s = the s-th interior face of the cell in ef order):
+ *     U += dU;  R = sum_s XF_s dU_nbr(s);  b = -Dinv R  (= the next dU)
+ * with dU and b in two buffers that swap every sweep.  The buffer parity
+ * lives in SolveState::pad, flipped by the launch's last CTA, so graph and
+ * eager sweep sequences agree on where the latest update is. */
+
+/* Dinv = D^-1 per position, in place (Gauss-Jordan without pivoting, as
+ * the reference's LU has none); pads stay zero.  One warp per position. */
+__global__ void __launch_bounds__(32) pij_invert_kernel(int np16, const int *__restrict__ elem_of_pos,
+                                                        double *__restrict__ D, unsigned *status) {
+    const int j = threadIdx.x;
+    for (int p = blockIdx.x; p < np16; p += gridDim.x) {
+        if (elem_of_pos[p] < 0) continue;
+        double w[NV];
+        double *blk = D + (size_t)p * NB;
+#pragma unroll
+        for (int i = 0; i < NV; ++i) w[i] = j < NV ? blk[NV * j + i] : (i == j ? 1.0 : 0.0);
+        gj_invert_cols(w, j, status);
+        if (j < NV) {
+#pragma unroll
+            for (int i = 0; i < NV; ++i) blk[NV * j + i] = w[i];
+        }
+        __syncwarp();
+    }
+}
+
+int launch_pij_invert(cudaStream_t st, const FastLayout &L, double *D, unsigned *status) {
+    const int grid = L.np16 < 148 * 32 ? (L.np16 > 0 ? L.np16 : 1) : 148 * 32;
+    pij_invert_kernel<<<grid, 32, 0, st>>>(L.np16, L.elem_of_pos, D, status);
+    return (int)cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(RES_THREADS_FAST) pij_sweep_kernel(
+    int nxf, int np16, const double *__restrict__ Dinv, const double *__restrict__ XF,
+    const int *__restrict__ xnbrf, double *bufA, double *bufB, double *__restrict__ Up,
+    NormSink ns, unsigned *status) {
+    /* read before any CTA can finish: the last CTA flips it after every
+     * CTA has taken its ticket */
+    const int odd = ns.state->pad & 1;
+    const double *dU = odd ? bufB : bufA;
+    double *b = odd ? bufA : bufB;
+    const bool last = resid_tiles<double>(nxf, np16, 1, Dinv, XF, xnbrf, dU, nullptr, b, Up, ns, status);
+    if (last && threadIdx.x == 0) ns.state->pad = odd ^ 1;
+}
+
+int launch_pij_sweep(cudaStream_t st, const FastLayout &L, const double *Dinv, const double *XF,
+                     double *bufA, double *bufB, double *Up, const NormSink &ns, unsigned *status) {
+    /* nxf == 0 (no interior faces): no slot is read and R_new = 0 */
+    if (L.nv != NV || L.nxf > 4 || !ns.state || !ns.partials) return (int)cudaErrorInvalidValue;
+    const size_t smem = resid_smem_bytes<double>(L.nxf);
+    pij_sweep_kernel<<<resid_grid_persistent((const void *)pij_sweep_kernel, smem, L.np16 / RES_TILE),
+                       RES_THREADS_FAST, smem, st>>>(L.nxf, L.np16, Dinv, XF, L.xnbrf, bufA, bufB, Up,
+                                                     ns, status);
+    return (int)cudaGetLastError();
+}
+
+int pij_prepare(const FastLayout &L) {
+    return set_smem((const void *)pij_sweep_kernel, resid_smem_bytes<double>(L.nxf));
 }
 
 }  // namespace tbs

@@ -13,7 +13,7 @@
  *   --iters N          fixed number of sweeps (default 30, src/main.cxx:20)
  *   --tol T            sweep until ||R||/||R0|| <= T instead (device-side test)
  *   --max-sweeps N     sweep limit with --tol (default 1000)
- *   --algo ref|fp64|mixed   TBS_ALGO_* (default fp64)
+ *   --algo ref|fp64|mixed|pij   TBS_ALGO_* (default fp64; pij: point-implicit Jacobi)
  *   --inner M          FP32 inner sweeps per outer step for --algo mixed
  *   --gen L K SHIFT SEED    synthetic structured mesh + seeded Jacobian
  *   --write-files      with --gen: also write the two data files to cwd
@@ -46,7 +46,7 @@ static void usage() {
         "                (this build: 2=CUDA on sm_100a only)\n"
         "  device_id:    Device ID on node\n"
         "  block_size:   Size of the matrix sub-block (i.e., # of variables/eqns; e.g., 9x9 default)\n"
-        "Options: --iters N | --tol T [--max-sweeps N] | --algo ref|fp64|mixed | --inner M\n"
+        "Options: --iters N | --tol T [--max-sweeps N] | --algo ref|fp64|mixed|pij | --inner M\n"
         "         --gen L K SHIFT SEED [--write-files] | --mesh PATH | --jac PATH | --json\n");
 }
 
@@ -87,6 +87,7 @@ int main(int argc, char **argv) {
                 if (v == "ref") algo = TBS_ALGO_REFERENCE;
                 else if (v == "fp64") algo = TBS_ALGO_FP64;
                 else if (v == "mixed") algo = TBS_ALGO_MIXED;
+                else if (v == "pij") algo = TBS_ALGO_PIJ;
                 else { std::fprintf(stderr, RED "ERROR: unknown --algo %s" COLOR_OFF "\n", v.c_str()); return 2; }
             } else if (s == "--gen") {
                 need(4);

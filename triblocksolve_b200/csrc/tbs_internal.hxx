@@ -214,6 +214,15 @@ int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
 int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
                        double *Up, double *partials, const float *Dinv32, float *b32, float *c32);
 
+/* point-implicit Jacobi (TBS_ALGO_PIJ): D^-1 in place of the
+ * position-ordered diagonal blocks; one sweep = U += dU, R = sum over the
+ * interior faces of XF dU_nbr, b = -Dinv R, with dU / b alternating between
+ * bufA and bufB by SolveState::pad (flipped by each sweep) */
+int launch_pij_invert(cudaStream_t st, const FastLayout &L, double *D, unsigned *status);
+int launch_pij_sweep(cudaStream_t st, const FastLayout &L, const double *Dinv, const double *XF,
+                     double *bufA, double *bufB, double *Up, const NormSink &ns, unsigned *status);
+int pij_prepare(const FastLayout &L);
+
 /* ------------------------------------- several right-hand sides (FP64)
  * Up to MULTI_MAX right-hand sides of one system swept together, the line
  * blocks read once per sweep for all of them.  Vectors are RHS-major with
