@@ -241,6 +241,20 @@ int tbs_solve_multi_device(tbs_ctx *ctx, int nrhs, const double *d_rhs,
                            double *d_U, double rel_tol, int max_sweeps,
                            int *sweeps, double *hist, int hist_stride);
 
+/* Restarted GMRES(restart) on J U = -rhs from U = 0, right preconditioned
+ * by precond_sweeps LIJ sweeps from zero with the TBS_ALGO_FP64 factors
+ * (one sweep: the line block-tridiagonal solve) -- the Krylov caller of the
+ * line sweep in the paper (p.14, Table 6), which the reference repository
+ * does not contain.  Stops when the residual norm reaches rel_tol * ||rhs||
+ * or after max_iters Arnoldi steps (each one preconditioner application
+ * and one product with J).  *iters_out = Arnoldi steps; hist_out (may be
+ * NULL, max_iters + 1 entries) gets ||rhs|| and then the GMRES residual
+ * estimate after each step, replaced by the true ||rhs + J U|| at the end
+ * of every restart cycle.  The solution is read with tbs_get_solution;
+ * tbs_solve / tbs_set_rhs start over from U = 0.  restart <= 64. */
+int tbs_gmres(tbs_ctx *ctx, int restart, int precond_sweeps, double rel_tol,
+              int max_iters, int *iters_out, double *hist_out);
+
 /* Jacobian::fromDevice (src/Jacobian.cxx:279-290) for the vectors, in the
  * element order of the input (9*nelem doubles each). */
 int tbs_get_solution(tbs_ctx *ctx, double *U);

@@ -125,6 +125,81 @@ def pij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1):
     return lij(point_lines(mesh), jacD, jacO1, jacO2, rhs, iters, threads)
 
 
+def gmres(mesh, jacD, jacO1, jacO2, rhs, restart: int, precond_sweeps: int, tol: float,
+          max_iters: int, threads: int = 1):
+    """Restarted GMRES(restart) on J U = -rhs from U = 0, right preconditioned
+    by `precond_sweeps` line sweeps from zero (the paper's line-preconditioned
+    GMRES, p.14 Table 6; no code for it in the reference repository).
+
+    The preconditioner is the reference's own sweep loop (lij with rhs = v,
+    U after k sweeps ~ -J^-1 v) and the product with J its residual rule
+    (true_residual with rhs = 0).  Arnoldi with classical Gram-Schmidt done
+    twice, the preconditioned directions kept, Givens rotations for the
+    least-squares problem, the true residual recomputed at every restart.
+    Returns dict(U, iters, hist) with hist as tbs_gmres fills it."""
+    n = rhs.size
+    zero = np.zeros(n)
+
+    def P(v):
+        return lij(mesh, jacD, jacO1, jacO2, v, precond_sweeps, threads)["U"]
+
+    def J(z, b=zero):
+        return true_residual(mesh, jacD, jacO1, jacO2, b, z)
+
+    U = np.zeros(n)
+    R = np.array(rhs, dtype=np.float64)
+    beta0 = float(np.linalg.norm(R))
+    hist = [beta0]
+    beta, iters = beta0, 0
+    m = restart
+    while beta > tol * beta0 and np.isfinite(beta) and iters < max_iters:
+        V = [-R / beta]
+        Z = []
+        H = np.zeros((m + 1, m))
+        cs, sn = np.zeros(m), np.zeros(m)
+        g = np.zeros(m + 1)
+        g[0] = beta
+        j = 0
+        stop = False
+        while j < m and not stop:
+            Z.append(P(V[j]))
+            w = J(Z[j])
+            Vm = np.array(V)
+            h1 = Vm @ w
+            w = w - Vm.T @ h1
+            h2 = Vm @ w
+            ww = float(w @ w)
+            w = w - Vm.T @ h2
+            H[: j + 1, j] = h1 + h2
+            hn = np.sqrt(max(ww - float(h2 @ h2), 0.0))
+            H[j + 1, j] = hn
+            for i in range(j):
+                a, b = H[i, j], H[i + 1, j]
+                H[i, j], H[i + 1, j] = cs[i] * a + sn[i] * b, -sn[i] * a + cs[i] * b
+            a, b = H[j, j], H[j + 1, j]
+            r = np.hypot(a, b)
+            cs[j], sn[j] = (a / r, b / r) if r > 0 else (1.0, 0.0)
+            H[j, j], H[j + 1, j] = r, 0.0
+            g[j + 1] = -sn[j] * g[j]
+            g[j] = cs[j] * g[j]
+            iters += 1
+            res = abs(g[j + 1])
+            hist.append(res)
+            j += 1
+            if res <= tol * beta0 or iters >= max_iters or not hn > 0 or not np.isfinite(res):
+                stop = True
+            elif j < m:
+                V.append(w / hn)
+        y = np.zeros(j)
+        for i in range(j - 1, -1, -1):
+            y[i] = (g[i] - H[i, i + 1:j] @ y[i + 1:j]) / H[i, i] if H[i, i] != 0 else 0.0
+        U = U + np.array(Z[:j]).T @ y
+        R = J(U, rhs)
+        beta = float(np.linalg.norm(R))
+        hist[iters] = beta
+    return dict(U=U, iters=iters, hist=np.array(hist))
+
+
 def resize_block_size(nv_old, nv_new, nelem, nintface, D, O1, O2, rhs, U0):
     """Jacobian.cxx:153-238 restated; returns the new (D, O1, O2, rhs, U0)."""
     bn = nv_new * nv_new

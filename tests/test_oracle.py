@@ -161,3 +161,20 @@ def test_oracle_pij_against_dense(lens, shift, seed):
     lij = oracle.lij(m, j.jacD, j.jacO1, j.jacO2, j.rhs, 8)
     if len(lens) > 1:
         assert lij["hist"][-1] < r["hist"][-1]
+
+
+@pytest.mark.parametrize("restart,psweeps", [(30, 1), (4, 1), (6, 2)])
+def test_oracle_gmres_solves_the_dense_system(restart, psweeps):
+    """oracle.gmres (line-preconditioned GMRES over the oracle's own sweep
+    and residual) reaches the solution of the dense system J U = -rhs."""
+    m = ragged_mesh([5, 1, 7, 3, 3, 8], seed=2)
+    j = Jacobian.generate(m, 2.5, 2)  # weak diagonal: plain line sweeps are slow here
+    J, _ = dense_system(m, j)
+    U_exact = np.linalg.solve(J, -j.rhs)
+    r = oracle.gmres(m, j.jacD, j.jacO1, j.jacO2, j.rhs, restart, psweeps, 1e-11, 200)
+    assert r["hist"][-1] <= 1e-11 * r["hist"][0]
+    assert np.linalg.norm(r["U"] - U_exact) <= 1e-9 * np.linalg.norm(U_exact)
+    # far fewer preconditioner applications than plain line sweeps to 1e-11
+    lij = oracle.lij(m, j.jacD, j.jacO1, j.jacO2, j.rhs, 200)
+    n_lij = int(np.argmax(lij["hist"] <= 1e-11 * lij["hist"][0]))
+    assert 2 * r["iters"] * psweeps < n_lij

@@ -119,6 +119,7 @@ static void drop_graph(tbs_ctx *ctx) {
 /* free everything that depends on the mesh */
 static void drop_mesh(tbs_ctx *ctx) {
     multi_free(ctx);
+    krylov_free(ctx);
     drop_graph(ctx);
     for (auto &a : ctx->allocs) cudaFree(a.first);
     ctx->allocs.clear();
@@ -1194,7 +1195,7 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
 
 int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes) {
     if (!ctx || !bytes) return ctx_fail(nullptr, TBS_ERR_ARG, "null argument");
-    *bytes = ctx->bytes + multi_bytes(ctx);
+    *bytes = ctx->bytes + multi_bytes(ctx) + krylov_bytes(ctx);
     return TBS_OK;
 }
 
@@ -1365,6 +1366,8 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
                 b = N * blk + X * (blk + 4.0) + nr * (N * 4 * vec + X * vec);
         }
     }
+    else if (k == "fast_resid_jv") /* X blocks, xnbr, neighbour dU, own dU, U in/out, v in, w out */
+        b = N * 5 * vec + X * (blk + 4.0 + vec);
     else if (k == "pij_sweep") /* Dinv, face blocks + index + neighbour dU, own dU, U in/out, b out */
         b = N * (blk + 4 * vec) + (double)ctx->n_fslots_real * (blk + 4.0 + vec);
     else if (k == "fast_factor") /* D, A, C in; Dinv, G, Gam out */

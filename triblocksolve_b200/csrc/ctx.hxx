@@ -26,7 +26,8 @@ struct PendingEvent {
     cudaEvent_t a, b;
 };
 
-struct MultiBufs; /* several right-hand sides (multi.cu) */
+struct MultiBufs;  /* several right-hand sides (multi.cu) */
+struct KrylovBufs; /* line-preconditioned GMRES (krylov.cu) */
 
 struct tbs_ctx {
     int device = 0;
@@ -85,6 +86,8 @@ struct tbs_ctx {
 
     /* ---- several right-hand sides: vectors and graph, made on first use ---- */
     MultiBufs *multi = nullptr;
+    /* ---- GMRES: Krylov basis and work vectors, made on first use ---- */
+    KrylovBufs *krylov = nullptr;
 
     /* ---- memory accounting ---- */
     std::vector<std::pair<void *, size_t>> allocs;
@@ -116,5 +119,8 @@ void ctx_prof_resolve(tbs_ctx *ctx);
 void multi_free(tbs_ctx *ctx);
 void multi_drop_graph(tbs_ctx *ctx);
 size_t multi_bytes(const tbs_ctx *ctx);
+/* krylov.cu: free the GMRES vectors / their device bytes */
+void krylov_free(tbs_ctx *ctx);
+size_t krylov_bytes(const tbs_ctx *ctx);
 
 #endif /* TBS_CTX_HXX */

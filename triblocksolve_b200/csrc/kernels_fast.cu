@@ -692,9 +692,10 @@ __device__ __forceinline__ bool fast_resid_body(
 
     if (tid == 0) {
         const uint64_t pol = policy_evict_first();
-        const uint32_t bytes = (mode == 3 ? 0u : szD) + (mode >= 1 ? nx * szD : szR);
+        const bool noD = mode == 3 || mode == 4;
+        const uint32_t bytes = (noD ? 0u : szD) + (mode >= 1 ? nx * szD : szR);
         mbar_arrive_expect_tx(bar, bytes);
-        if (mode != 3) bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+        if (!noD) bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
         if (mode >= 1) {
             for (int s = 0; s < nx; ++s)
                 bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
@@ -751,6 +752,9 @@ __device__ __forceinline__ bool fast_resid_body(
     if (mode == 3) {
         /* X held Dinv X: r is already Dinv R */
         if (act) sb[c * NV + i] = -r;
+    } else if (mode == 4) {
+        /* R = v + J z after the line solves, so J z = R - v */
+        if (act) sb[c * NV + i] = r - Rsrc[(size_t)p0 * NV + c * NV + i];
     } else if (act) {
         const T *dr = sD + c * NB + i;
         const T *rv = sr + c * NV;
@@ -817,6 +821,17 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_dx_kernel(
     resid_tiles<T>(nx, np16, 3, nullptr, DX, xnbr, dU, nullptr, b, Uacc, NormSink{}, status);
 }
 
+/* mode 4 (the product with J of a preconditioned direction: R = sum X dU
+ * is the residual of v + J z after the line solves, so w = R - v; no
+ * Dinv, no norm) */
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_jv_kernel(
+    int nx, int np16, const T *__restrict__ X, const int *__restrict__ xnbr,
+    const T *__restrict__ dU, const T *__restrict__ v, T *__restrict__ w, T *__restrict__ Uacc,
+    unsigned *status) {
+    resid_tiles<T>(nx, np16, 4, nullptr, X, xnbr, dU, v, w, Uacc, NormSink{}, status);
+}
+
 /* mode 0 (R given in position order) */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
@@ -843,6 +858,15 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
                       T *Uacc) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     const int grid = fast_resid_grid(L.np16);
+    if (mode == 4) {
+        /* nx == 0 runs the kernel too: no slot is read, w = -v */
+        if (!Rsrc) return (int)cudaErrorInvalidValue;
+        const size_t smem4 = resid_smem_bytes<T>(L.nx);
+        fast_resid_jv_kernel<T><<<resid_grid_persistent((const void *)fast_resid_jv_kernel<T>, smem4, grid),
+                                  RES_THREADS_FAST, smem4, st>>>(L.nx, L.np16, X, L.xnbr, dU, Rsrc, b,
+                                                                 Uacc, status);
+        return (int)cudaGetLastError();
+    }
     if (mode >= 1 && L.nx == 0) {
         /* a mesh that is one line: the line solve is exact, R_new = 0 */
         if (Uacc) {
@@ -1436,6 +1460,7 @@ static int set_smem(const void *fn, size_t need) {
  * known: opts the streaming kernels into the shared memory they need. */
 int fast_prepare(const FastLayout &L) {
     int rc = set_smem((const void *)fast_resid_kernel<double>, resid_smem_bytes<double>(L.nx));
+    if (!rc) rc = set_smem((const void *)fast_resid_jv_kernel<double>, resid_smem_bytes<double>(L.nx));
     if (!rc) rc = set_smem((const void *)fast_resid_kernel<float>, resid_smem_bytes<float>(L.nx));
     const ThomasCfg c64 = thomas_cfg<double>(L), c32 = thomas_cfg<float>(L);
     if (!rc)
@@ -1499,7 +1524,7 @@ __device__ __forceinline__ void full_resid_body(
                 a2 += o[72] * un[8];
             }
         }
-        const double r = rhs[(size_t)e * NV + i] + (a0 + (a1 + a2));
+        const double r = (rhs ? rhs[(size_t)e * NV + i] : 0.0) + (a0 + (a1 + a2));
         Rp[(size_t)pe * NV + i] = (T)r;
         sq = r * r;
     }

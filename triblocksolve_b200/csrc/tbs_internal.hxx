@@ -172,7 +172,8 @@ struct NormSink {
 };
 
 /* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
- * b = -sum X dU, no norm.  Uacc (may be null): modes 1, 3 add dU to it for
+ * b = -sum X dU, no norm; 4: b = sum X dU - Rsrc (the product with J of
+ * the iterate of line sweeps on Rsrc + J z = 0), no Dinv, no norm.  Uacc (may be null): modes 1, 3 add dU to it for
  * the tile's positions, mode 0 sets it to zero there */
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
@@ -184,6 +185,7 @@ int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T
 int fast_kernels_init();
 int fast_prepare(const FastLayout &L);
 int full_resid_blocks(int nelem);
+/* rhs may be null (zero): Rp = J U, the matrix-vector product */
 template <typename T>
 int launch_full_resid(cudaStream_t st, int nelem, const int *epoint, const int *ef, const int *fc,
                       const int *pos_of_elem, const double *D, const double *O1, const double *O2,

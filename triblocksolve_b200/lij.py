@@ -316,6 +316,16 @@ class Solver:
         self._chk(N.lib.tbs_solve(self.ctx, rel_tol, max_sweeps, C.byref(s), N.dptr(h)))
         return s.value, h[: s.value + 1]
 
+    def gmres(self, rel_tol: float, restart: int = 30, precond_sweeps: int = 1,
+              max_iters: int = 300):
+        """Line-preconditioned restarted GMRES on J U = -rhs (ALGO_FP64 factors).
+        Returns (Arnoldi steps, residual history); the solution is in ``solution()``."""
+        h = np.zeros(max_iters + 1)
+        it = C.c_int()
+        self._chk(N.lib.tbs_gmres(self.ctx, restart, precond_sweeps, rel_tol, max_iters,
+                                  C.byref(it), N.dptr(h)))
+        return it.value, h[: it.value + 1]
+
     def solve_multi(self, rhs: np.ndarray, rel_tol: float, max_sweeps: int = 1000):
         """Several right-hand sides (rows of ``rhs``, 9*nelem each) from U = 0
         with the current factors (ALGO_FP64), groups of up to 8 sweeping
