@@ -790,6 +790,135 @@ def run_multi(args, L, K, shift, tol):
     return 0
 
 
+def run_gmres(args, L, K, shift, tol):
+    """--gmres M: restarted GMRES(M) on the system, right preconditioned by
+    one LIJ sweep (tbs_gmres, FP64 line factors), to the config's tolerance
+    from U = 0; value = solves per second, with the plain LIJ solve of the
+    same system timed beside it.  e2e: tbs_set_rhs from pinned host memory,
+    tbs_gmres, tbs_get_solution per step."""
+    import torch
+
+    import triblocksolve_b200 as tbs
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    mesh, host = build_problem(L, K, shift, pinned=True)
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    solver = tbs.Solver(local)
+    solver.set_stream(stream.cuda_stream)
+    solver.set_mesh(mesh)
+    solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+    solver.factor(tbs.ALGO_FP64)
+    m, max_iters = args.gmres, 400
+    with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 0)):
+            solver.gmres(tol, m, 1, max_iters)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        iters = 0
+        for _ in range(args.steps):
+            it, h = solver.gmres(tol, m, 1, max_iters)
+            iters += it
+        t1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        elapsed_ms = t0.elapsed_time(t1)
+        true_rel = solver.true_residual_norm() / float(h[0])
+        # the plain line sweep on the same system, for comparison
+        solver.solve(tol, max_iters)
+        torch.cuda.synchronize()
+        l0, l1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0.record(stream)
+        nl = max(1, min(args.steps, 20))
+        for _ in range(nl):
+            lij_sweeps, lh = solver.solve(tol, max_iters)
+        l1.record(stream)
+        torch.cuda.synchronize()
+        lij_ms = l0.elapsed_time(l1) / nl
+        solver.profile(True)
+        solver.profile_reset()
+        nprof = max(1, min(args.steps, 10))
+        for _ in range(nprof):
+            solver.gmres(tol, m, 1, max_iters)
+        prof = solver.profile_read()
+        solver.profile(False)
+        ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 10))
+        Uh = torch.empty(9 * mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(ne2e):
+            solver.set_rhs(host["rhs"])
+            solver.gmres(tol, m, 1, max_iters)
+            Uh[:] = solver.solution()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.summary()
+    max_ms = dist.reduce(elapsed_ms, "max")
+    max_e2e = dist.reduce(e2e_ms, "max")
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        kern = {}
+        for name, (launches, ms) in prof.items():
+            try:
+                b = solver.kernel_bytes(name)
+            except Exception:
+                b = None
+            avg_us = 1e3 * ms / launches if launches else 0.0
+            kern[name] = {"launches": launches, "total_ms": round(ms, 4), "avg_us": round(avg_us, 3),
+                          "bytes_per_launch": b,
+                          "gbs": round(b / (avg_us * 1e-6) / 1e9, 1) if b and avg_us > 0 else None}
+        hot = [k for k in kern if kern[k]["bytes_per_launch"] and k != "fast_resid_rhs"]
+        dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
+        roof = None
+        if dom:
+            ach = kern[dom]["gbs"]
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "traffic": None,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": kern[dom]["bytes_per_launch"],
+                    "avg_launch_us": kern[dom]["avg_us"]}
+        line = {
+            "metric": "GMRES solves/s", "value": round(ws * args.steps / (max_ms * 1e-3), 3),
+            "unit": "solves/s", "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(max_ms / args.steps, 5), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured mesh and values (shift %g, seed %d)" % (shift, SEED),
+            "config": {
+                "workload": f"GMRES({m}) right-preconditioned by one LIJ sweep, to {tol:g} from "
+                            f"U=0, {L} lines x {K} cells ({mesh.nelem} cells), FP64",
+                "cells": mesh.nelem, "restart": m, "tol": tol,
+                "arnoldi_steps_per_solve": iters / args.steps,
+                "time_to_tol_ms": round(max_ms / args.steps, 4),
+                "true_rel_residual": true_rel,
+                "lij_sweeps_to_tol": int(lij_sweeps), "lij_time_to_tol_ms": round(lij_ms, 4),
+                "l2": "no flush: every step streams the line blocks and the basis (> 126 MB L2)",
+                "parallelism": f"{ws} independent systems, one per GPU" if ws > 1 else "1 GPU",
+            },
+            "roofline": roof, "kernels": kern,
+            "e2e": {"value": round(ws * ne2e / (max_e2e * 1e-3), 3), "unit": "solves/s",
+                    "h2d_bytes_per_step": int(host["rhs"].nbytes), "d2h_bytes_per_step": int(Uh.nbytes),
+                    "steps": ne2e,
+                    "what": "per step: tbs_set_rhs from pinned host memory, tbs_gmres, tbs_get_solution"},
+            "gpu_launches": int(round(sum(v["launches"] for v in kern.values()) / nprof * args.steps)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    solver.close()
+    dist.close()
+    return 0
+
+
 def run_reference(args, L, K, shift, tol):
     ws, rank, local = dist_env()
     if rank != 0:
@@ -835,6 +964,8 @@ def main():
     ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed", "pij"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gmres", type=int, default=0,
+                    help="restart length: time line-preconditioned GMRES instead of the sweep loop")
     ap.add_argument("--nrhs", type=int, default=1,
                     help="right-hand sides per solve (> 1: tbs_solve_multi, FP64)")
     args = ap.parse_args()
@@ -849,6 +980,8 @@ def main():
     L, K, shift, tol = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, L, K, shift, tol)
+    if args.gmres > 0:
+        return run_gmres(args, L, K, shift, tol)
     if args.nrhs > 1:
         if args.algo != "fp64":
             ap.error("--nrhs > 1 needs --algo fp64")

@@ -55,15 +55,18 @@ def test_bad_device_id():
     assert e.value.code == N.TBS_ERR_ARG
 
 
-def test_fast_algos_need_nvar9():
+def test_block_size_support():
+    """FP64 runs at any nvar in 2..16 (general-size kernels); the mixed form
+    needs nvar 9 and says so; the reference order takes every size."""
     s = Solver(0)
     from meshes import ragged_mesh
     mesh = ragged_mesh([3, 4], seed=1, nvar=5)
     jac = Jacobian.generate(mesh, 5.0, 1)
     s.set_mesh(mesh)
     s.set_jacobian(jac)
+    s.factor(ALGO_FP64)
     with pytest.raises(TbsError) as e:
-        s.factor(ALGO_FP64)
+        s.factor(ALGO_MIXED)
     assert e.value.code == N.TBS_ERR_UNSUPPORTED
     s.factor(ALGO_REFERENCE)
     s.close()

@@ -236,7 +236,7 @@ static int build_layout(tbs_ctx *ctx) {
         twist[l] = line_twist_of(ls[l]);
         np += (ls[l] + 3) & ~3;
     }
-    if (np > 0x7fffffffLL / 81)
+    if (np > 0x7fffffffLL / ((long long)ctx->nvar * ctx->nvar))
         return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "mesh too large for int32 block offsets");
     const int np16 = (int)((np + RES_TILE - 1) / RES_TILE * RES_TILE);
     std::vector<int> pos_of_elem(nelem), elem_of_pos(np16, -1), fsrc((size_t)np16 * 5, -1);
@@ -352,7 +352,7 @@ static int build_layout(tbs_ctx *ctx) {
     DA(L.xnbr, (size_t)np16 * std::max(nx, 1));
     DA(L.xsrcf, (size_t)np16 * nxfa);
     DA(L.xnbrf, (size_t)np16 * nxfa);
-    DA(ctx->d_gamlast, (size_t)nline * 2 * 81);
+    DA(ctx->d_gamlast, (size_t)nline * 2 * ctx->nvar * ctx->nvar);
     cudaStream_t st = ctx->stream;
     CK(cudaMemcpyAsync(L.line_start, start.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
     CK(cudaMemcpyAsync(L.line_len, len.data(), nline * sizeof(int), cudaMemcpyHostToDevice, st));
@@ -368,7 +368,7 @@ static int build_layout(tbs_ctx *ctx) {
     /* the residual kernel stages RES_TILE cells x nx blocks per tile; beyond
      * 4 cross-line couplings per cell it would not fit in shared memory,
      * and such meshes use TBS_ALGO_REFERENCE */
-    ctx->layout_ok = (ctx->nvar == 9) && nx <= 4;
+    ctx->layout_ok = (ctx->nvar == 9 || nv_supported(ctx->nvar)) && nx <= 4;
     return TBS_OK;
 }
 
@@ -399,6 +399,37 @@ static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; 
 /* TBS_ALGO_MIXED's outer residual streams position-ordered copies of the
  * blocks when a cell has at most 4 interior faces (one shared-memory tile) */
 bool fullpos_ok(const tbs_ctx *ctx) { return ctx->L.nxf <= 4; }
+
+/* The TBS_ALGO_FP64 sweep kernels for the context's block size: the tuned
+ * size-9 kernels or their general form (kernels_nv.cu). */
+static int thomas64(tbs_ctx *ctx, const double *b, double *dU, double *U, int accumulate) {
+    if (ctx->nvar == 9)
+        return launch_fast_thomas<double>(ctx->stream, ctx->L, ctx->d_G, ctx->d_Gam, b, ctx->d_y, dU, U,
+                                          ctx->d_status, accumulate);
+    return launch_nv_thomas(ctx->stream, ctx->nvar, ctx->L, ctx->d_G, ctx->d_Gam, b, ctx->d_y, dU, U,
+                            accumulate);
+}
+
+static int resid64(tbs_ctx *ctx, int mode, const double *dU, const double *Rsrc, double *b,
+                   const NormSink &ns, double *Uacc) {
+    if (ctx->nvar == 9)
+        return launch_fast_resid<double>(ctx->stream, ctx->L, mode, ctx->d_Dinv, ctx->d_X, dU, Rsrc, b,
+                                         ns, ctx->d_status, Uacc);
+    return launch_nv_resid(ctx->stream, ctx->nvar, ctx->L, mode, ctx->d_Dinv, ctx->d_X, dU, Rsrc, b, ns,
+                           ctx->d_status, Uacc);
+}
+
+/* R = rhs + J U in element order by the reference-order residual kernel
+ * (any block size); U in element order */
+static int ref_residual(tbs_ctx *ctx, const double *U, double *R) {
+    int np = 0;
+    CK(cudaMemcpyAsync(R, ctx->d_rhs, (size_t)ctx->nvar * ctx->nelem * sizeof(double),
+                       cudaMemcpyDeviceToDevice, ctx->stream));
+    CKL(launch_ref_line_res(ctx->stream, ctx->nvar, ctx->nline, ctx->nelem, ctx->d_epoint, ctx->d_ef,
+                            ctx->d_fc, ctx->d_linesize, ctx->d_linepoint, ctx->d_lines, ctx->d_jacD,
+                            ctx->d_O1, ctx->d_O2, U, R, ctx->d_partials2, &np));
+    return TBS_OK;
+}
 
 /* How a sequence ends: the norm of its residual is recorded as the start
  * of a solve (is_start) or as one more sweep, and, inside the solve graph,
@@ -462,18 +493,22 @@ static int prime(tbs_ctx *ctx, CondCtl cc) {
         /* TBS_ALGO_PIJ: the first update goes to buffer A (d_b), parity 0 */
         if (pij) CK(cudaMemsetAsync(&ctx->d_state->pad, 0, sizeof(int), st));
         if (ctx->d_Uinit) {
-            RUN("permute", launch_permute_to_pos(st, 9, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
-            RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
-                                                        L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
-                                                        ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
-                                                        ctx->d_partials2));
+            RUN("permute", launch_permute_to_pos(st, nv, ne, L.pos_of_elem, ctx->d_Uinit, ctx->d_Up));
+            if (nv == 9) {
+                RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                            L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
+                                                            ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
+                                                            ctx->d_partials2));
+            } else {
+                int rc = ref_residual(ctx, ctx->d_Uinit, ctx->d_R);
+                if (rc) return rc;
+                RUN("permute", launch_permute_to_pos(st, nv, ne, L.pos_of_elem, ctx->d_R, ctx->d_Rp));
+            }
             Rsrc = ctx->d_Rp;
         }
         /* from U = 0 the same launch clears U */
-        RUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, pij ? nullptr : ctx->d_X, ctx->d_dUp,
-                                                        Rsrc, ctx->d_b, sink(ctx, 1, cc),
-                                                        ctx->d_status,
-                                                        ctx->d_Uinit ? nullptr : ctx->d_Up));
+        RUN("fast_resid_rhs", resid64(ctx, 0, ctx->d_dUp, Rsrc, ctx->d_b, sink(ctx, 1, cc),
+                                      ctx->d_Uinit ? nullptr : ctx->d_Up));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: R32, its norm, and the first inner right-hand side
@@ -525,11 +560,8 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
     }
     if (ctx->algo == TBS_ALGO_FP64) {
         /* the Thomas kernel writes dU; the residual kernel adds it to U */
-        RUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
-                                                      ctx->d_dUp, ctx->d_Up, ctx->d_status, 2));
-        RUN("fast_resid", launch_fast_resid<double>(st, L, 1, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
-                                                    nullptr, ctx->d_b, sink(ctx, 0, cc),
-                                                    ctx->d_status, ctx->d_Up));
+        RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, 2));
+        RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, cc), ctx->d_Up));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
@@ -678,7 +710,7 @@ static int build_graph(tbs_ctx *ctx) {
 /* =========================================================== algorithms */
 
 static int alloc_algo(tbs_ctx *ctx, int algo) {
-    const size_t bs = 81, ne = ctx->nelem;
+    const size_t bs = (size_t)ctx->nvar * ctx->nvar, ne = ctx->nelem;
     DA(ctx->d_U, (size_t)nvec(ctx));
     DA(ctx->d_dU, (size_t)nvec(ctx));
     DA(ctx->d_R, (size_t)nvec(ctx));
@@ -701,7 +733,7 @@ static int alloc_algo(tbs_ctx *ctx, int algo) {
         return TBS_OK;
     }
     const FastLayout &L = ctx->L;
-    const size_t npb = (size_t)L.np16 * bs, npv = (size_t)L.np16 * 9;
+    const size_t npb = (size_t)L.np16 * bs, npv = (size_t)L.np16 * ctx->nvar;
     const size_t nxb = (size_t)L.np16 * std::max(L.nx, 1) * bs;
     DA(ctx->d_Up, npv);
     DA(ctx->d_rhsp, npv);
@@ -758,8 +790,16 @@ static int run_factor(tbs_ctx *ctx, int algo) {
         return TBS_OK;
     }
     const FastLayout &L = ctx->L;
+    RUN("permute", launch_permute_to_pos(st, nv, ctx->nelem, L.pos_of_elem, ctx->d_rhs, ctx->d_rhsp));
+    if (nv != 9) {
+        /* TBS_ALGO_FP64, general block size */
+        CKL(nv_prepare(nv, L));
+        RUN("fast_factor", launch_nv_factor(st, nv, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_Dinv,
+                                            ctx->d_G, ctx->d_Gam, ctx->d_gamlast, ctx->d_status));
+        RUN("fast_xlayout", launch_nv_xlayout(st, nv, L, ctx->d_O1, ctx->d_O2, ctx->d_X));
+        return TBS_OK;
+    }
     CKL(fast_prepare(L));
-    RUN("permute", launch_permute_to_pos(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_rhs, ctx->d_rhsp));
     if (algo == TBS_ALGO_PIJ) {
         CKL(pij_prepare(L));
         RUN("fullpos_layout", launch_fullpos_layout(st, L, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
@@ -974,8 +1014,10 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
                         "TBS_ALGO_PIJ needs nvar == 9 and at most 4 interior faces per cell");
     if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_PIJ && !ctx->layout_ok)
         return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
-                        "TBS_ALGO_FP64 / TBS_ALGO_MIXED need nvar == 9 and at most 4 cross-line "
-                        "faces per cell; use TBS_ALGO_REFERENCE");
+                        "TBS_ALGO_FP64 needs nvar 2..16 and at most 4 cross-line faces per cell; "
+                        "use TBS_ALGO_REFERENCE");
+    if (algo == TBS_ALGO_MIXED && ctx->nvar != 9)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "TBS_ALGO_MIXED needs nvar == 9");
     int rc = alloc_algo(ctx, algo);
     if (rc) return rc;
     if (ctx->algo != algo) drop_graph(ctx);
@@ -1001,7 +1043,7 @@ int tbs_set_rhs(tbs_ctx *ctx, const double *rhs) {
     CK(cudaMemcpyAsync(ctx->d_rhs, rhs, (size_t)nvec(ctx) * sizeof(double), cudaMemcpyHostToDevice,
                        ctx->stream));
     if (ctx->algo != TBS_ALGO_REFERENCE) {
-        RUN("permute", launch_permute_to_pos(ctx->stream, 9, ctx->nelem, ctx->L.pos_of_elem, ctx->d_rhs,
+        RUN("permute", launch_permute_to_pos(ctx->stream, ctx->nvar, ctx->nelem, ctx->L.pos_of_elem, ctx->d_rhs,
                                              ctx->d_rhsp));
     }
     return prime(ctx, CondCtl{});
@@ -1106,15 +1148,21 @@ static int get_vec(tbs_ctx *ctx, int which, double *out) {
         src = which == 0 ? ctx->d_U : which == 1 ? ctx->d_R : ctx->d_dU;
     } else {
         const FastLayout &L = ctx->L;
+        const int nv = ctx->nvar;
         if (which == 0) {
-            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_Up, ctx->d_scratch));
+            RUN("permute", launch_permute_to_elem(st, nv, ctx->nelem, L.pos_of_elem, ctx->d_Up, ctx->d_scratch));
+        } else if (which == 1 && nv != 9) {
+            /* general block size: the reference-order residual of U */
+            RUN("permute", launch_permute_to_elem(st, nv, ctx->nelem, L.pos_of_elem, ctx->d_Up, ctx->d_U));
+            int rc = ref_residual(ctx, ctx->d_U, ctx->d_scratch);
+            if (rc) return rc;
         } else if (which == 1) {
             RUN("full_resid", launch_full_resid<double>(st, ctx->nelem, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                         L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                         ctx->d_rhs, ctx->d_Up, ctx->d_Rp, ctx->d_partials2));
             RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_Rp, ctx->d_scratch));
         } else if (ctx->algo == TBS_ALGO_FP64) {
-            RUN("permute", launch_permute_to_elem(st, 9, ctx->nelem, L.pos_of_elem, ctx->d_dUp, ctx->d_scratch));
+            RUN("permute", launch_permute_to_elem(st, nv, ctx->nelem, L.pos_of_elem, ctx->d_dUp, ctx->d_scratch));
         } else if (ctx->algo == TBS_ALGO_PIJ) {
             /* the last sweep added the buffer it read: A (d_b) when the
              * parity it flipped is now 1 */

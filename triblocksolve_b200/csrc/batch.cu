@@ -990,9 +990,9 @@ int tbs_batch_create(tbs_ctx *const *systems, int nsys, tbs_batch **out) {
                     return fail(bfail(b, TBS_ERR_ARG, "system " + std::to_string(s) + " appears twice"));
             if (!c->factored)
                 return fail(bfail(b, TBS_ERR_STATE, "system " + std::to_string(s) + " is not factored"));
-            if (c->algo != TBS_ALGO_FP64 && c->algo != TBS_ALGO_MIXED)
+            if ((c->algo != TBS_ALGO_FP64 && c->algo != TBS_ALGO_MIXED) || c->nvar != 9)
                 return fail(bfail(b, TBS_ERR_UNSUPPORTED,
-                                  "batches take TBS_ALGO_FP64 or TBS_ALGO_MIXED systems"));
+                                  "batches take TBS_ALGO_FP64 or TBS_ALGO_MIXED systems of nvar 9"));
             if (s > 0 && (c->algo != systems[0]->algo || c->device != systems[0]->device))
                 return fail(bfail(b, TBS_ERR_ARG,
                                   "all systems of a batch need the same algorithm and GPU"));

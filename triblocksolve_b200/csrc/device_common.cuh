@@ -1,0 +1,79 @@
+/*
+ * device_common.cuh -- device helpers shared by the kernel translation units
+ * (kernels_fast.cu for block size 9, kernels_nv.cu for the other sizes):
+ * the fixed-order sums behind every residual norm.
+ */
+#ifndef TBS_DEVICE_COMMON_CUH
+#define TBS_DEVICE_COMMON_CUH
+
+#include "tbs_internal.hxx"
+
+#include <cuda_runtime.h>
+
+namespace tbs {
+
+/* sum of p[t], p[t + stride], p[t + 2 stride], ... (t = threadIdx.x), added
+ * in that order; eight loads are issued ahead of their adds so that their
+ * latencies overlap without changing the sum */
+static __device__ __forceinline__ double strided_sum(const double *p, int n, int stride) {
+    double acc = 0.0;
+    int t = threadIdx.x;
+    for (; t + 7 * stride < n; t += 8 * stride) {
+        double v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldcg(p + t + k * stride);
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc += v[k];
+    }
+    for (; t < n; t += stride) acc += __ldcg(p + t);
+    return acc;
+}
+
+/* After a CTA's last tile: a ticket per CTA; the last CTA to finish adds
+ * the n per-tile partials in a fixed order and, when asked, records the
+ * norm like reduce_norm (history, sweep count, graph loop condition).
+ * Called by every thread of the block. */
+static __device__ bool finalize_total(const NormSink &ns, int n) {
+    __shared__ unsigned ticket;
+    __shared__ double red[32];
+    if (!ns.partials || !ns.counter) return false;
+    __syncthreads(); /* this CTA's partials are written */
+    if (threadIdx.x == 0) {
+        __threadfence();
+        ticket = atomicAdd(ns.counter, 1u);
+    }
+    __syncthreads();
+    if (ticket != gridDim.x - 1) return false;
+    if (!ns.state) {
+        if (threadIdx.x == 0) *ns.counter = 0u;
+        return true;
+    }
+    __threadfence();
+    double acc = strided_sum(ns.partials, n, (int)blockDim.x);
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double tot = 0.0;
+        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
+        const double nrm = sqrt(tot);
+        SolveState *S = ns.state;
+        if (ns.is_start) {
+            S->sweep = 0;
+            S->norm0 = nrm;
+        } else {
+            S->sweep += 1;
+        }
+        const int sw = S->sweep;
+        if (sw < S->hist_cap) ns.hist[sw] = nrm;
+        S->last = nrm;
+        const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
+        if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
+        *ns.counter = 0u;
+    }
+    return true;
+}
+
+}  // namespace tbs
+
+#endif /* TBS_DEVICE_COMMON_CUH */

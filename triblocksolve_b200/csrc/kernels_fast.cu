@@ -20,6 +20,7 @@
  * multiple of 4 positions, so that runs of cells are 16-byte aligned for
  * cp.async.bulk in FP64 and FP32 alike.
  */
+#include "device_common.cuh"
 #include "tbs_internal.hxx"
 #include "tma.cuh"
 
@@ -49,23 +50,6 @@ static int grid_for(long long n, int threads, int cap = 148 * 8) {
 int launch_zero(cudaStream_t st, double *p, long long n) {
     zero_kernel<<<grid_for(n, 256), 256, 0, st>>>(p, n);
     return (int)cudaGetLastError();
-}
-
-/* sum of p[t], p[t + stride], p[t + 2 stride], ... (t = threadIdx.x), added
- * in that order; eight loads are issued ahead of their adds so that their
- * latencies overlap without changing the sum */
-__device__ __forceinline__ double strided_sum(const double *p, int n, int stride) {
-    double acc = 0.0;
-    int t = threadIdx.x;
-    for (; t + 7 * stride < n; t += 8 * stride) {
-        double v[8];
-#pragma unroll
-        for (int k = 0; k < 8; ++k) v[k] = __ldcg(p + t + k * stride);
-#pragma unroll
-        for (int k = 0; k < 8; ++k) acc += v[k];
-    }
-    for (; t < n; t += stride) acc += __ldcg(p + t);
-    return acc;
 }
 
 /* block b sums v[b*chunk : (b+1)*chunk)^2 in a fixed order */
@@ -598,54 +582,6 @@ int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, 
 constexpr int RES_THREADS_FAST = 160;
 
 int fast_resid_grid(int np16) { return np16 / RES_TILE > 0 ? np16 / RES_TILE : 1; }
-
-/* Fixed-order sum of the per-CTA partials by the last CTA; updates the
- * solve state like reduce_norm_kernel.  Called by every thread of the
- * block; `block_sum` is valid in thread 0. */
-/* After a CTA's last tile: a ticket per CTA; the last CTA to finish adds
- * the n per-tile partials in a fixed order and, when asked, records the
- * norm like reduce_norm (history, sweep count, graph loop condition).
- * Called by every thread of the block. */
-__device__ bool finalize_total(const NormSink &ns, int n) {
-    __shared__ unsigned ticket;
-    __shared__ double red[32];
-    if (!ns.partials || !ns.counter) return false;
-    __syncthreads(); /* this CTA's partials are written */
-    if (threadIdx.x == 0) {
-        __threadfence();
-        ticket = atomicAdd(ns.counter, 1u);
-    }
-    __syncthreads();
-    if (ticket != gridDim.x - 1) return false;
-    if (!ns.state) {
-        if (threadIdx.x == 0) *ns.counter = 0u;
-        return true;
-    }
-    __threadfence();
-    double acc = strided_sum(ns.partials, n, (int)blockDim.x);
-    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
-    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double tot = 0.0;
-        for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
-        const double nrm = sqrt(tot);
-        SolveState *S = ns.state;
-        if (ns.is_start) {
-            S->sweep = 0;
-            S->norm0 = nrm;
-        } else {
-            S->sweep += 1;
-        }
-        const int sw = S->sweep;
-        if (sw < S->hist_cap) ns.hist[sw] = nrm;
-        S->last = nrm;
-        const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
-        if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
-        *ns.counter = 0u;
-    }
-    return true;
-}
 
 template <typename T>
 __host__ __device__ inline size_t resid_smem_bytes(int nx) {

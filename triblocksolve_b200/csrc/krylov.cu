@@ -412,8 +412,9 @@ extern "C" int tbs_gmres(tbs_ctx *ctx, int restart, int precond_sweeps, double r
         if (cudaSetDevice(ctx->device) != cudaSuccess)
             return kfail(ctx, TBS_ERR_CUDA, "cudaSetDevice failed");
         if (!ctx->factored) return kfail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
-        if (ctx->algo != TBS_ALGO_FP64)
-            return kfail(ctx, TBS_ERR_UNSUPPORTED, "GMRES uses the TBS_ALGO_FP64 line factors");
+        if (ctx->algo != TBS_ALGO_FP64 || ctx->nvar != 9)
+            return kfail(ctx, TBS_ERR_UNSUPPORTED,
+                         "GMRES uses the TBS_ALGO_FP64 line factors of nvar == 9");
         if (restart < 1 || restart > KRYLOV_MAX || precond_sweeps < 1 || max_iters < 0 ||
             !(rel_tol >= 0.0))
             return kfail(ctx, TBS_ERR_ARG, "bad restart (1..64), preconditioner sweeps, "

@@ -335,8 +335,8 @@ static int multi_group(tbs_ctx *ctx, int nr, const double *d_rhs, double *d_U, d
 static int multi_check(tbs_ctx *ctx, int nrhs, const void *rhs, const void *U, double tol,
                        int max_sweeps, const double *hist, int hist_stride) {
     if (!ctx->factored) return mfail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
-    if (ctx->algo != TBS_ALGO_FP64)
-        return mfail(ctx, TBS_ERR_UNSUPPORTED, "several right-hand sides need TBS_ALGO_FP64");
+    if (ctx->algo != TBS_ALGO_FP64 || ctx->nvar != 9)
+        return mfail(ctx, TBS_ERR_UNSUPPORTED, "several right-hand sides need TBS_ALGO_FP64 and nvar == 9");
     if (nrhs < 0 || (nrhs > 0 && (!rhs || !U)))
         return mfail(ctx, TBS_ERR_ARG, "bad right-hand-side count or null arrays");
     if (max_sweeps < 0 || !(tol >= 0.0)) return mfail(ctx, TBS_ERR_ARG, "bad tolerance or sweep limit");

@@ -795,6 +795,7 @@ int tbs_server_add_system(tbs_server *s, int nvar, int nelem, int nintface, int 
                           const int *lineface, const double *jacD, const double *jacO1,
                           const double *jacO2, int *system_id) {
     if (!s || !system_id) return sfail(s, TBS_ERR_ARG, "null argument");
+    if (nvar != 9) return sfail(s, TBS_ERR_UNSUPPORTED, "the server takes systems of nvar 9");
     tbs_ctx *c = nullptr;
     int rc = tbs_create(s->device, &c);
     if (rc) return sfail(s, rc, thread_error());

@@ -216,6 +216,24 @@ int launch_axpy_f64(cudaStream_t st, const double *d, double *U, long long n);
 int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp, float *R32,
                        double *Up, double *partials, const float *Dinv32, float *b32, float *c32);
 
+/* TBS_ALGO_FP64 for the block sizes other than 9 (kernels_nv.cu): the
+ * same launch sequence with kernels templated on nv (2..16).  Thomas has
+ * no staging waits (plain loads one step ahead), so it takes no status. */
+bool nv_supported(int nv);
+int nv_prepare(int nv, const FastLayout &L);
+int launch_nv_factor(cudaStream_t st, int nv, const FastLayout &L, const double *jacD,
+                     const double *O1, const double *O2, double *Dinv, double *G, double *Gam,
+                     double *gamlast, unsigned *status);
+int launch_nv_xlayout(cudaStream_t st, int nv, const FastLayout &L, const double *O1,
+                      const double *O2, double *X);
+int launch_nv_thomas(cudaStream_t st, int nv, const FastLayout &L, const double *G,
+                     const double *Gam, const double *b, double *y, double *dU, double *U,
+                     int accumulate);
+/* modes 0 and 1 of launch_fast_resid */
+int launch_nv_resid(cudaStream_t st, int nv, const FastLayout &L, int mode, const double *Dinv,
+                    const double *X, const double *dU, const double *Rsrc, double *b,
+                    const NormSink &ns, unsigned *status, double *Uacc);
+
 /* point-implicit Jacobi (TBS_ALGO_PIJ): D^-1 in place of the
  * position-ordered diagonal blocks; one sweep = U += dU, R = sum over the
  * interior faces of XF dU_nbr, b = -Dinv R, with dU / b alternating between
