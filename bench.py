@@ -153,20 +153,20 @@ def measured_peak_hbm():
         return 6650.0, "fallback"
 
 
-def build_problem(L, K, shift, pinned):
+def build_problem(L, K, shift, pinned, nvar=9):
     from triblocksolve_b200 import Mesh
     from triblocksolve_b200 import _native as N
-    mesh = Mesh.structured(L, K)
-    nb = 81
+    mesh = Mesh.structured(L, K, nvar=nvar)
+    nb = nvar * nvar
     sizes = {"jacD": nb * mesh.nelem, "jacO1": nb * mesh.nintface, "jacO2": nb * mesh.nintface,
-             "rhs": 9 * mesh.nelem}
+             "rhs": nvar * mesh.nelem}
     if pinned:
         import torch
         host = {k: torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
                 for k, n in sizes.items()}
     else:
         host = {k: np.empty(n) for k, n in sizes.items()}
-    N.check(N.lib.tbs_gen_jacobian(9, mesh.nelem, mesh.nintface, float(shift), SEED,
+    N.check(N.lib.tbs_gen_jacobian(nvar, mesh.nelem, mesh.nintface, float(shift), SEED,
                                    N.dptr(host["jacD"]), N.dptr(host["jacO1"]),
                                    N.dptr(host["jacO2"]), N.dptr(host["rhs"]), None))
     return mesh, host
@@ -964,6 +964,8 @@ def main():
     ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed", "pij"])
     ap.add_argument("--e2e-steps", type=int, default=None)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nvar", type=int, default=9,
+                    help="block size of the generated system (the reference's block-size study)")
     ap.add_argument("--gmres", type=int, default=0,
                     help="restart length: time line-preconditioned GMRES instead of the sweep loop")
     ap.add_argument("--nrhs", type=int, default=1,
@@ -996,7 +998,12 @@ def main():
     algo = {"fp64": tbs.ALGO_FP64, "ref": tbs.ALGO_REFERENCE, "mixed": tbs.ALGO_MIXED,
             "pij": tbs.ALGO_PIJ}[args.algo]
 
-    mesh, host = build_problem(L, K, shift, pinned=True)
+    nvar = args.nvar
+    if nvar != 9:
+        if args.algo not in ("fp64", "ref"):
+            ap.error("--nvar other than 9 needs --algo fp64 or ref")
+        shift = max(shift, float(nvar))  # keeps the generated blocks diagonally dominant
+    mesh, host = build_problem(L, K, shift, pinned=True, nvar=nvar)
     # a dedicated stream: CUDA graphs cannot be captured on the legacy default stream
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
@@ -1048,7 +1055,7 @@ def main():
         solver.profile(False)
         # ---------------- e2e: upload + factor + solve + read back, from pinned host memory
         ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 20))
-        Uh = torch.empty(9 * mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
+        Uh = torch.empty(nvar * mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
         for _ in range(1):
             solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
             solver.factor(algo)
@@ -1097,7 +1104,7 @@ def main():
         dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
         traffic = None
         tpath = os.path.join(ROOT, "profiles", "traffic.json")
-        if dom and os.path.exists(tpath):
+        if dom and os.path.exists(tpath) and nvar == 9:
             t = json.load(open(tpath)).get(args.config, {}).get(dom)
             if t:
                 traffic = t
@@ -1113,7 +1120,8 @@ def main():
         sweeps_per_solve = sweeps_total / args.steps
         h2d = sum(host[k].nbytes for k in ("jacD", "jacO1", "jacO2", "rhs"))
         d2h = Uh.nbytes + 8 * (max_sweeps + 1)
-        ref_bytes = (8.0 * (387 * mesh.nelem + 162 * mesh.nintface)) * sweeps_per_solve
+        nb_ = nvar * nvar
+        ref_bytes = (8.0 * ((4 * nb_ + 7 * nvar) * mesh.nelem + 2 * nb_ * mesh.nintface)) * sweeps_per_solve
         line = {
             "metric": "LIJ sweeps/s", "value": round(value, 2), "unit": "sweeps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -1121,13 +1129,14 @@ def main():
             "scaling": "weak",
             "vs_baseline": (round(value / ws / PUBLISHED_SWEEPS_PER_S[args.config], 3)
                             if args.config in PUBLISHED_SWEEPS_PER_S and args.algo in ("fp64", "ref")
+                            and nvar == 9
                             else None),
             "dtype": "f64" if args.algo != "mixed" else "f32+f64",
             "data": "synthetic: seeded structured mesh and values (shift %g, seed %d); the "
                     "reference's real Jacobians are not available" % (shift, SEED),
             "config": {
                 "workload": f"LIJ solve to {tol:g} relative residual from U=0, {L} lines x {K} "
-                            f"cells ({mesh.nelem} cells, {mesh.nintface} faces), 9x9 blocks, "
+                            f"cells ({mesh.nelem} cells, {mesh.nintface} faces), {nvar}x{nvar} blocks, "
                             f"algo {args.algo}",
                 "cells": mesh.nelem, "lines": L, "cells_per_line": K, "tol": tol,
                 "algo": args.algo, "sweeps_per_solve": sweeps_per_solve,
@@ -1136,7 +1145,7 @@ def main():
                 "factor_ms": round(factor_ms, 3),
                 "true_rel_residual": true_rel,
                 "l2": "no flush: every sweep streams %.0f MB of blocks, > 126 MB L2" %
-                      (8 * 81 * 5 * mesh.nelem / 1e6),
+                      (8 * nvar * nvar * 5 * mesh.nelem / 1e6),
                 "reference_model_gbs": round(ref_bytes * value / ws / 1e9, 1),
                 "published_baseline": "V100 FP64 LIJ, paper Table 5 (5 sweeps); vs_baseline "
                                       "is per GPU",

@@ -407,7 +407,7 @@ static int thomas64(tbs_ctx *ctx, const double *b, double *dU, double *U, int ac
         return launch_fast_thomas<double>(ctx->stream, ctx->L, ctx->d_G, ctx->d_Gam, b, ctx->d_y, dU, U,
                                           ctx->d_status, accumulate);
     return launch_nv_thomas(ctx->stream, ctx->nvar, ctx->L, ctx->d_G, ctx->d_Gam, b, ctx->d_y, dU, U,
-                            accumulate);
+                            accumulate, ctx->d_status);
 }
 
 static int resid64(tbs_ctx *ctx, int mode, const double *dU, const double *Rsrc, double *b,

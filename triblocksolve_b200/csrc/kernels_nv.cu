@@ -10,13 +10,16 @@
  *                      every block, Gauss-Jordan by columns with shuffles
  *   nv_twist_kernel    one CTA per line: the twist cell's pivot
  *   nv_thomas_kernel   one warp per line, the two half-warps on the two
- *                      chains, lane i < NV on row i; each step's row of
- *                      G (Gam) and b (y) is loaded one step ahead and the
- *                      previous vector arrives by shuffles
+ *                      chains, lane i < NV on row i; chunks of G (Gam)
+ *                      and b stream through a ring of bulk copies in
+ *                      shared memory and the previous vector arrives by
+ *                      shuffles
  *   nv_resid_kernel    persistent over 16-position tiles, Dinv and the
- *                      cross-line blocks staged by bulk copies
- * Dinv is column-major, G and Gam row-major, as for size 9.  The size-9
- * kernels stay the tuned path; these are their general form.
+ *                      cross-line blocks staged by bulk copies, thread
+ *                      (cell, row) = (t / NV, t % NV)
+ * All blocks are column-major (entry (i, j) at i + NV j), so that lane i
+ * reading row i of a staged block hits consecutive shared-memory words.
+ * The size-9 kernels stay the tuned path; these are their general form.
  */
 #include "device_common.cuh"
 #include "tbs_internal.hxx"
@@ -132,7 +135,7 @@ __global__ void __launch_bounds__(32) nv_factor_kernel(
 #pragma unroll
         for (int i = 0; i < NV; ++i) {
             Dinv[(size_t)cs * NB + i + NV * j] = w[i];
-            G[(size_t)cs * NB + NV * i + j] = 0.0;
+            G[(size_t)cs * NB + i + NV * j] = 0.0;
             sM[i + NV * j] = w[i];
         }
     }
@@ -159,7 +162,7 @@ __global__ void __launch_bounds__(32) nv_factor_kernel(
         if (act) {
 #pragma unroll
             for (int i = 0; i < NV; ++i) {
-                Gam[(size_t)(p - 1) * NB + NV * i + j] = gm[i];
+                Gam[(size_t)(p - 1) * NB + i + NV * j] = gm[i];
                 sA[i + NV * j] = a[i];
             }
         }
@@ -189,7 +192,7 @@ __global__ void __launch_bounds__(32) nv_factor_kernel(
                 double acc = 0.0;
 #pragma unroll
                 for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * a[q];
-                G[(size_t)p * NB + NV * i + j] = acc;
+                G[(size_t)p * NB + i + NV * j] = acc;
             }
         }
     }
@@ -207,7 +210,7 @@ __global__ void __launch_bounds__(32) nv_factor_kernel(
                 double acc = 0.0;
 #pragma unroll
                 for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * c[q];
-                Gam[(size_t)(cs + len - 1) * NB + NV * i + j] = acc;
+                Gam[(size_t)(cs + len - 1) * NB + i + NV * j] = acc;
                 gamlast[((size_t)l * 2 + g) * NB + i + NV * j] = acc;
             }
         }
@@ -261,8 +264,8 @@ __global__ void __launch_bounds__(nv_block_threads<NV>()) nv_twist_kernel(
             gc += sW[i + NV * q] * sC[q + NV * j];
         }
         Dinv[(size_t)ptw * NB + t] = sW[t];
-        G[(size_t)ptw * NB + NV * i + j] = ga;
-        Gam[(size_t)ptw * NB + NV * i + j] = gc;
+        G[(size_t)ptw * NB + t] = ga;
+        Gam[(size_t)ptw * NB + t] = gc;
     }
 }
 
@@ -284,46 +287,107 @@ __global__ void nv_xlayout_kernel(long long nslots, const int *__restrict__ xsrc
 
 /* init - row . v with the previous vector v held one component per lane of
  * this half-warp (lanes src0 .. src0+NV-1) */
+/* init - row . v, row i of the column-major block at blk (entry (i, j)
+ * at i + NV j), with the previous vector v held one component per lane
+ * of this half-warp (lanes src0 .. src0+NV-1) */
 template <int NV>
-__device__ __forceinline__ double nv_row_step(const double (&row)[NV], double init, double vmine,
+__device__ __forceinline__ double nv_row_step(const double *blk, int i, double init, double vmine,
                                               int src0) {
     double a0 = init, a1 = 0.0, a2 = 0.0;
 #pragma unroll
     for (int j = 0; j < NV; ++j) {
         const double vj = __shfl_sync(NFULL, vmine, src0 + j);
+        const double g = blk[i + NV * j];
         if (j % 3 == 0)
-            a0 -= row[j] * vj;
+            a0 -= g * vj;
         else if (j % 3 == 1)
-            a1 += row[j] * vj;
+            a1 += g * vj;
         else
-            a2 += row[j] * vj;
+            a2 += g * vj;
     }
     return a0 - (a1 + a2);
 }
 
-/* one warp per line: half-warp h runs chain h (top: positions 0..m-1 in
- * order, bottom: m..n-2 in elimination order), lane i < NV row i;
- * forward y_s = b_s - G_s y_{s-1}, twist x = b - G_tw y_top - Gam_tw y_bot,
- * backward x_s = y_s - Gam_s x_{s+1}; accumulate 0: U = dU, 1: U += dU,
- * 2: U untouched */
+constexpr int NVT_P = 8; /* cells per chunk of a chain */
+
+template <int NV>
+__host__ __device__ inline size_t nv_thomas_stage() {
+    return 2 * (size_t)NVT_P * (NV * NV + NV) * sizeof(double);
+}
+
+/* One warp per line: half-warp h runs chain h (top: positions 0..m-1 in
+ * order, bottom: m..n-2 in elimination order), lane i < NV row i.  Lane 0
+ * streams "jobs" through an NS-stage ring of bulk copies, each holding one
+ * chunk of NVT_P cells of both chains: forward jobs the blocks of G and the
+ * b vectors, backward jobs (in reverse) the blocks of Gam; y is read back
+ * with plain loads one chunk ahead.  Forward y_s = b_s - G_s y_{s-1}, twist
+ * x = b - G_tw y_top - Gam_tw y_bot, backward x_s = y_s - Gam_s x_{s+1};
+ * accumulate 0: U = dU, 1: U += dU, 2: U untouched.  A staging wait that
+ * runs out of time sets ST_TIMEOUT and the warp drains its copies. */
 template <int NV>
 __global__ void __launch_bounds__(32) nv_thomas_kernel(
-    int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
+    int nline, int NS, const int *__restrict__ line_start, const int *__restrict__ line_len,
     const int *__restrict__ line_twist, const double *__restrict__ G, const double *__restrict__ Gam,
     const double *__restrict__ b, double *__restrict__ y, double *__restrict__ dU,
-    double *__restrict__ U, int accumulate) {
-    constexpr int NB = NV * NV;
+    double *__restrict__ U, int accumulate, unsigned *status) {
+    constexpr int NB = NV * NV, P = NVT_P;
+    extern __shared__ __align__(128) unsigned char smem[];
     const int l = blockIdx.x;
     if (l >= nline) return;
     const int lane = threadIdx.x, h = lane >> 4, i = lane & 15;
     const bool act = i < NV;
     const int ii = act ? i : 0;
     const int src0 = h << 4;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    const size_t half = (size_t)P * (NB + NV) * sizeof(double);
+    const size_t stage = 2 * half;
+    unsigned char *st0 = smem + 128;
+    if (lane == 0) {
+        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        mbar_fence_init();
+    }
+    __syncwarp();
     const int ps = line_start[l], n = line_len[l], m = line_twist[l];
     const int nb = n - 1 - m;
     const int len = h ? nb : m;
-    const int nmax = m > nb ? m : nb;
     const size_t base = (size_t)ps + (h ? m : 0);
+    const int nchT = (m + P - 1) / P, nchB = (nb + P - 1) / P;
+    const int nch = h ? nchB : nchT;
+    const int nf = nchT > nchB ? nchT : nchB;
+    const int njobs = 2 * nf;
+    const uint64_t pol = lane == 0 ? policy_evict_first() : 0;
+    auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
+    auto issue = [&](int job, int s) {
+        unsigned char *st = st0 + (size_t)s * stage;
+        uint32_t bytes = 0;
+        if (job < nf) {
+            if (job < nchT) bytes += cells(m, job) * (NB + NV) * sizeof(double);
+            if (job < nchB) bytes += cells(nb, job) * (NB + NV) * sizeof(double);
+        } else {
+            const int jb = job - nf;
+            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * NB * sizeof(double);
+            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * NB * sizeof(double);
+        }
+        mbar_arrive_expect_tx(&bars[s], bytes);
+        for (int hh = 0; hh < 2; ++hh) {
+            const int ln = hh ? nb : m, nc = hh ? nchB : nchT, cp = hh ? m : 0;
+            unsigned char *hb = st + hh * half;
+            if (job < nf) {
+                const int c = job;
+                if (c >= nc) continue;
+                const int cnt = cells(ln, c);
+                const size_t p = (size_t)(ps + cp + c * P);
+                bulk_g2s_hint(hb, G + p * NB, cnt * NB * sizeof(double), &bars[s], pol);
+                bulk_g2s(hb + (size_t)P * NB * sizeof(double), b + p * NV, cnt * NV * sizeof(double), &bars[s]);
+            } else {
+                const int c = nc - 1 - (job - nf);
+                if (c < 0) continue;
+                const int cnt = cells(ln, c);
+                bulk_g2s_hint(hb, Gam + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(double),
+                              &bars[s], pol);
+            }
+        }
+    };
     auto put = [&](size_t p, double x) {
         dU[p * NV + i] = x;
         if (accumulate == 0)
@@ -331,129 +395,167 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
         else if (accumulate == 1)
             U[p * NV + i] += x;
     };
-    double row[NV], nrow[NV];
-    double cur = 0.0, nxt = 0.0;
+    int issued = 0;
+    if (lane == 0)
+        for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
+    int consumed = 0;
+    bool timed_out = false;
+
     /* ---------------- forward */
-    auto load_f = [&](int s, double (&r)[NV], double &bb) {
-        if (s < len) {
-            const double *gr = G + (base + s) * NB + NV * ii;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) r[j] = gr[j];
-            bb = b[(base + s) * NV + ii];
-        } else {
-#pragma unroll
-            for (int j = 0; j < NV; ++j) r[j] = 0.0;
-            bb = 0.0;
-        }
-    };
-    load_f(0, row, cur);
     double yp = 0.0;
-    for (int s = 0; s < nmax; ++s) {
-        load_f(s + 1, nrow, nxt);
-        const double yi = nv_row_step<NV>(row, cur, yp, src0);
-        if (s < len) {
-            if (act) y[(base + s) * NV + i] = yi;
-            yp = yi;
+    for (int c = 0; c < nf; ++c) {
+        const int s = c % NS;
+        if (!__all_sync(NFULL, mbar_wait(&bars[s], (uint32_t)(c / NS) & 1u))) {
+            timed_out = true;
+            break;
         }
+        ++consumed;
+        const double *sG = reinterpret_cast<const double *>(st0 + (size_t)s * stage + h * half);
+        const double *sB = sG + P * NB;
 #pragma unroll
-        for (int j = 0; j < NV; ++j) row[j] = nrow[j];
-        cur = nxt;
+        for (int q = 0; q < P; ++q) {
+            const int k = c * P + q;
+            const double yi = nv_row_step<NV>(sG + q * NB, ii, sB[q * NV + ii], yp, src0);
+            if (k < len) {
+                if (act) y[(base + k) * NV + i] = yi;
+                yp = yi;
+            }
+        }
+        __syncwarp();
+        if (lane == 0 && issued < njobs) {
+            issue(issued, s);
+            ++issued;
+        }
     }
-    /* ---------------- twist (both halves compute the same values) */
-    const size_t ptw = (size_t)ps + n - 1;
-    double xm = b[ptw * NV + ii];
-    {
-        const double *gr = G + ptw * NB + NV * ii;
-        const double *cr = Gam + ptw * NB + NV * ii;
+    if (!timed_out) {
+        /* ---------------- twist (both halves compute the same values) */
+        const size_t ptw = (size_t)ps + n - 1;
+        double xm = b[ptw * NV + ii];
+        {
+            const double *gr = G + ptw * NB + ii;
+            const double *cr = Gam + ptw * NB + ii;
 #pragma unroll
-        for (int j = 0; j < NV; ++j) {
-            const double yt = __shfl_sync(NFULL, yp, j);
-            const double yb = __shfl_sync(NFULL, yp, 16 + j);
-            xm -= gr[j] * yt + cr[j] * yb;
+            for (int j = 0; j < NV; ++j) {
+                const double yt = __shfl_sync(NFULL, yp, j);
+                const double yb = __shfl_sync(NFULL, yp, 16 + j);
+                xm -= gr[NV * j] * yt + cr[NV * j] * yb;
+            }
+        }
+        if (h == 0 && act) put(ptw, xm);
+        /* ---------------- backward */
+        double yv[P], nyv[P];
+        auto load_y = [&](int c, double *yy) {
+#pragma unroll
+            for (int q = 0; q < P; ++q) {
+                const int k = c * P + q;
+                yy[q] = (c >= 0 && k < len) ? y[(base + k) * NV + ii] : 0.0;
+            }
+        };
+        __syncwarp();
+        load_y(nch - 1, yv);
+        double xp = xm;
+        for (int jb = 0; jb < nf; ++jb) {
+            const int job = nf + jb;
+            const int c = nch - 1 - jb; /* this half's chunk (may be < 0) */
+            load_y(c - 1, nyv);
+            const int s = job % NS;
+            if (!__all_sync(NFULL, mbar_wait(&bars[s], (uint32_t)(job / NS) & 1u))) {
+                timed_out = true;
+                break;
+            }
+            ++consumed;
+            const double *sG = reinterpret_cast<const double *>(st0 + (size_t)s * stage + h * half);
+#pragma unroll
+            for (int q = P - 1; q >= 0; --q) {
+                const int k = c * P + q;
+                const bool valid = c >= 0 && k < len;
+                const double xi = nv_row_step<NV>(sG + q * NB, ii, valid ? yv[q] : 0.0, xp, src0);
+                if (valid) {
+                    if (act) put(base + k, xi);
+                    xp = xi;
+                }
+            }
+            __syncwarp();
+            if (lane == 0 && issued < njobs) {
+                issue(issued, s);
+                ++issued;
+            }
+#pragma unroll
+            for (int q = 0; q < P; ++q) yv[q] = nyv[q];
         }
     }
-    if (h == 0 && act) put(ptw, xm);
-    /* ---------------- backward */
-    auto load_b = [&](int t, double (&r)[NV], double &yy) {
-        const int s = len - 1 - t;
-        if (s >= 0) {
-            const double *cr = Gam + (base + s) * NB + NV * ii;
-#pragma unroll
-            for (int j = 0; j < NV; ++j) r[j] = cr[j];
-            yy = y[(base + s) * NV + ii];
-        } else {
-#pragma unroll
-            for (int j = 0; j < NV; ++j) r[j] = 0.0;
-            yy = 0.0;
-        }
-    };
-    __syncwarp();
-    load_b(0, row, cur);
-    double xp = xm;
-    for (int t = 0; t < nmax; ++t) {
-        load_b(t + 1, nrow, nxt);
-        const double xi = nv_row_step<NV>(row, cur, xp, src0);
-        const int s = len - 1 - t;
-        if (s >= 0) {
-            if (act) put(base + s, xi);
-            xp = xi;
-        }
-#pragma unroll
-        for (int j = 0; j < NV; ++j) row[j] = nrow[j];
-        cur = nxt;
+    if (timed_out && lane == 0) {
+        atomicOr(status, ST_TIMEOUT);
+        for (int job = consumed; job < issued; ++job)
+            mbar_wait(&bars[job % NS], (uint32_t)(job / NS) & 1u, 1LL << 28);
     }
 }
 
+/* positions per residual tile: 16 (the layout's granule), up to 64 for
+ * small blocks so that a tile still moves several KB per barrier phase */
 template <int NV>
-constexpr int nv_resid_threads() { return ((16 * NV + 31) / 32) * 32; }
+constexpr int nv_tile() {
+    return RES_TILE * (128 / (NV * NV) < 1 ? 1 : (128 / (NV * NV) > 4 ? 4 : 128 / (NV * NV)));
+}
+
+template <int NV>
+constexpr int nv_resid_threads() { return ((nv_tile<NV>() * NV + 31) / 32) * 32; }
 
 template <int NV>
 __host__ __device__ inline size_t nv_resid_smem(int nx) {
     const int nxa = nx > 0 ? nx : 1;
-    return 128 + (size_t)RES_TILE * NV * NV * sizeof(double) * (1 + nx) +
-           (size_t)nxa * RES_TILE * NV * sizeof(double) + (size_t)RES_TILE * NV * sizeof(double) * 2;
+    constexpr size_t T = nv_tile<NV>();
+    return 128 + T * NV * NV * sizeof(double) * (1 + nx) + (size_t)nxa * T * NV * sizeof(double) +
+           T * NV * sizeof(double) * 2;
 }
 
-/* persistent over the tiles of RES_TILE positions; per tile
+template <int NV>
+inline int nv_resid_tiles(int np16) { return (np16 + nv_tile<NV>() - 1) / nv_tile<NV>(); }
+
+/* persistent over the tiles of nv_tile<NV>() positions (the last one may
+ * be shorter, by whole 16-position granules); per tile
  *   MODE 0:  R = Rsrc, Uacc = 0 (the start of a sweep sequence)
  *   MODE 1:  R = sum over slots X dU[nbr], Uacc += dU
  * then b = -Dinv R and the tile's sum R^2; thread t < 16 NV owns cell
- * t % 16, row t / 16 */
+ * t / NV, row t % NV, so that the threads of a warp read consecutive rows
+ * of a block in shared memory (no bank conflicts at any NV) and gather a
+ * neighbour's vector with consecutive loads */
 template <int NV, int MODE>
 __global__ void __launch_bounds__(nv_resid_threads<NV>()) nv_resid_kernel(
     int nx, int np16, const double *__restrict__ Dinv, const double *__restrict__ X,
     const int *__restrict__ xnbr, const double *__restrict__ dU, const double *__restrict__ Rsrc,
     double *__restrict__ b, double *__restrict__ Uacc, NormSink ns, unsigned *status) {
-    constexpr int NB = NV * NV, TH = nv_resid_threads<NV>();
+    constexpr int NB = NV * NV, TH = nv_resid_threads<NV>(), TL = nv_tile<NV>();
     extern __shared__ __align__(128) unsigned char smem[];
     uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
     double *sD = reinterpret_cast<double *>(smem + 128);
-    double *sX = sD + RES_TILE * NB;
+    double *sX = sD + TL * NB;
     const int nxa = nx > 0 ? nx : 1;
-    double *sg = sX + (MODE == 1 ? nx : 0) * RES_TILE * NB;
-    double *sr = sg + nxa * RES_TILE * NV;
-    double *sb = sr + RES_TILE * NV;
+    double *sg = sX + (MODE == 1 ? nx : 0) * TL * NB;
+    double *sr = sg + nxa * TL * NV;
+    double *sb = sr + TL * NV;
     __shared__ double red[TH / 32];
     const int tid = threadIdx.x;
-    const int c = tid % RES_TILE, i = tid / RES_TILE;
-    const bool act = tid < RES_TILE * NV;
-    const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
+    const int c = tid / NV, i = tid % NV;
     if (tid == 0) {
         mbar_init(bar, 1);
         mbar_fence_init();
     }
     __syncthreads();
-    const int ntiles = np16 / RES_TILE;
+    const int ntiles = (np16 + TL - 1) / TL;
     uint32_t parity = 0;
     for (int blk = blockIdx.x; blk < ntiles; blk += gridDim.x) {
-        const int p0 = blk * RES_TILE;
+        const int p0 = blk * TL;
+        const int cnt = np16 - p0 < TL ? np16 - p0 : TL; /* a multiple of 16 */
+        const bool act = tid < cnt * NV;
+        const uint32_t szD = cnt * NB * sizeof(double), szR = cnt * NV * sizeof(double);
         if (tid == 0) {
             const uint64_t pol = policy_evict_first();
             mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : szR));
             bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
             if (MODE == 1) {
                 for (int s = 0; s < nx; ++s)
-                    bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
+                    bulk_g2s_hint(sX + s * TL * NB, X + ((size_t)s * np16 + p0) * NB, szD, bar, pol);
             } else {
                 bulk_g2s(sr, Rsrc + (size_t)p0 * NV, szR, bar);
             }
@@ -465,7 +567,7 @@ __global__ void __launch_bounds__(nv_resid_threads<NV>()) nv_resid_kernel(
         if (MODE == 1 && act) {
             for (int s = 0; s < nx; ++s) {
                 const int nb = xnbr[(size_t)s * np16 + p0 + c];
-                sg[(s * RES_TILE + c) * NV + i] = nb >= 0 ? dU[(size_t)nb * NV + i] : 0.0;
+                sg[(s * TL + c) * NV + i] = nb >= 0 ? dU[(size_t)nb * NV + i] : 0.0;
             }
         }
         const bool ok = mbar_wait(bar, parity);
@@ -482,8 +584,8 @@ __global__ void __launch_bounds__(nv_resid_threads<NV>()) nv_resid_kernel(
             if (act) {
                 double a0 = 0.0, a1 = 0.0, a2 = 0.0;
                 for (int s = 0; s < nx; ++s) {
-                    const double *xr = sX + (s * RES_TILE + c) * NB + i;
-                    const double *g = sg + (s * RES_TILE + c) * NV;
+                    const double *xr = sX + (s * TL + c) * NB + i;
+                    const double *g = sg + (s * TL + c) * NV;
 #pragma unroll
                     for (int j = 0; j < NV; ++j) {
                         if (j % 3 == 0)
@@ -533,6 +635,7 @@ __global__ void __launch_bounds__(nv_resid_threads<NV>()) nv_resid_kernel(
     }
     finalize_total(ns, ntiles);
 }
+
 
 /* ---------------------------------------------------------------- host */
 
@@ -586,17 +689,38 @@ struct NvOps {
         nv_xlayout_kernel<NV><<<grid_cap(nslots * 32, 256), 256, 0, st>>>(nslots, L.xsrc, O1, O2, X);
         return (int)cudaGetLastError();
     }
+    /* ring depth: the SM's shared memory over its resident lines, 2..6 */
+    static int thomas_ns(const FastLayout &L) {
+        int dev = 0, nsm = 148, smem_sm = 228 * 1024, reserved = 1024;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+        cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+        cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+        int per_sm = (L.nline + (nsm > 0 ? nsm : 148) - 1) / (nsm > 0 ? nsm : 148);
+        if (per_sm < 1) per_sm = 1;
+        long long ns = ((long long)smem_sm / per_sm - reserved - 128) / (long long)nv_thomas_stage<NV>();
+        if (ns > 6) ns = 6;
+        if (ns < 2) ns = 2;
+        return (int)ns;
+    }
+    static size_t thomas_smem(int ns) { return 128 + (size_t)ns * nv_thomas_stage<NV>(); }
     static int thomas(cudaStream_t st, const FastLayout &L, const double *G, const double *Gam,
-                      const double *b, double *y, double *dU, double *U, int accumulate) {
-        nv_thomas_kernel<NV><<<L.nline, 32, 0, st>>>(L.nline, L.line_start, L.line_len,
-                                                     L.line_twist, G, Gam, b, y, dU, U, accumulate);
+                      const double *b, double *y, double *dU, double *U, int accumulate,
+                      unsigned *status) {
+        const int ns = thomas_ns(L);
+        const size_t smem = thomas_smem(ns);
+        int rc = nv_set_smem((const void *)nv_thomas_kernel<NV>, smem);
+        if (rc) return rc;
+        nv_thomas_kernel<NV><<<L.nline, 32, smem, st>>>(L.nline, ns, L.line_start, L.line_len,
+                                                        L.line_twist, G, Gam, b, y, dU, U,
+                                                        accumulate, status);
         return (int)cudaGetLastError();
     }
     static int resid(cudaStream_t st, const FastLayout &L, int mode, const double *Dinv,
                      const double *X, const double *dU, const double *Rsrc, double *b,
                      const NormSink &ns, unsigned *status, double *Uacc) {
         constexpr int TH = nv_resid_threads<NV>();
-        const int ntiles = L.np16 / RES_TILE;
+        const int ntiles = nv_resid_tiles<NV>(L.np16);
         if (mode == 1) {
             const size_t smem = nv_resid_smem<NV>(L.nx);
             nv_resid_kernel<NV, 1><<<nv_grid_persistent((const void *)nv_resid_kernel<NV, 1>, TH, smem, ntiles),
@@ -611,7 +735,8 @@ struct NvOps {
         return (int)cudaGetLastError();
     }
     static int prepare(const FastLayout &L) {
-        int rc = nv_set_smem((const void *)nv_resid_kernel<NV, 1>, nv_resid_smem<NV>(L.nx));
+        int rc = nv_set_smem((const void *)nv_thomas_kernel<NV>, thomas_smem(thomas_ns(L)));
+        if (!rc) rc = nv_set_smem((const void *)nv_resid_kernel<NV, 1>, nv_resid_smem<NV>(L.nx));
         if (!rc) rc = nv_set_smem((const void *)nv_resid_kernel<NV, 0>, nv_resid_smem<NV>(0));
         return rc;
     }
@@ -651,9 +776,9 @@ int launch_nv_xlayout(cudaStream_t st, int nv, const FastLayout &L, const double
 
 int launch_nv_thomas(cudaStream_t st, int nv, const FastLayout &L, const double *G,
                      const double *Gam, const double *b, double *y, double *dU, double *U,
-                     int accumulate) {
+                     int accumulate, unsigned *status) {
     return nv_dispatch(nv, [&](auto ops) {
-        return decltype(ops)::thomas(st, L, G, Gam, b, y, dU, U, accumulate);
+        return decltype(ops)::thomas(st, L, G, Gam, b, y, dU, U, accumulate, status);
     });
 }
 

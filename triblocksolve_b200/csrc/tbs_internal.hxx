@@ -217,8 +217,8 @@ int launch_mixed_prime(cudaStream_t st, const FastLayout &L, const double *rhsp,
                        double *Up, double *partials, const float *Dinv32, float *b32, float *c32);
 
 /* TBS_ALGO_FP64 for the block sizes other than 9 (kernels_nv.cu): the
- * same launch sequence with kernels templated on nv (2..16).  Thomas has
- * no staging waits (plain loads one step ahead), so it takes no status. */
+ * same launch sequence with kernels templated on nv (2..16); G and Gam are
+ * column-major here (the size-9 kernels keep them row-major). */
 bool nv_supported(int nv);
 int nv_prepare(int nv, const FastLayout &L);
 int launch_nv_factor(cudaStream_t st, int nv, const FastLayout &L, const double *jacD,
@@ -228,7 +228,7 @@ int launch_nv_xlayout(cudaStream_t st, int nv, const FastLayout &L, const double
                       const double *O2, double *X);
 int launch_nv_thomas(cudaStream_t st, int nv, const FastLayout &L, const double *G,
                      const double *Gam, const double *b, double *y, double *dU, double *U,
-                     int accumulate);
+                     int accumulate, unsigned *status);
 /* modes 0 and 1 of launch_fast_resid */
 int launch_nv_resid(cudaStream_t st, int nv, const FastLayout &L, int mode, const double *Dinv,
                     const double *X, const double *dU, const double *Rsrc, double *b,
