@@ -15,7 +15,13 @@
  *   --max-sweeps N     sweep limit with --tol (default 1000)
  *   --algo ref|fp64|mixed|pij   TBS_ALGO_* (default fp64; pij: point-implicit Jacobi)
  *   --inner M          FP32 inner sweeps per outer step for --algo mixed
- *   --gen L K SHIFT SEED    synthetic structured mesh + seeded Jacobian
+ *   --gen L K SHIFT SEED    synthetic structured mesh + seeded Jacobian, at
+ *                      the block size of the third positional argument
+ *   --nrhs N           solve N right-hand sides together (tbs_solve_multi,
+ *                      --algo fp64, to --tol): the Jacobian's rhs and N-1
+ *                      seeded U(-1,1) vectors
+ *   --gmres M          line-preconditioned GMRES(M) to --tol (tbs_gmres,
+ *                      --algo fp64, one sweep per preconditioner step)
  *   --write-files      with --gen: also write the two data files to cwd
  *   --mesh PATH / --jac PATH   other input files
  *   --json             one JSON summary line at the end
@@ -47,13 +53,14 @@ static void usage() {
         "  device_id:    Device ID on node\n"
         "  block_size:   Size of the matrix sub-block (i.e., # of variables/eqns; e.g., 9x9 default)\n"
         "Options: --iters N | --tol T [--max-sweeps N] | --algo ref|fp64|mixed|pij | --inner M\n"
-        "         --gen L K SHIFT SEED [--write-files] | --mesh PATH | --jac PATH | --json\n");
+        "         --gen L K SHIFT SEED [--write-files] | --mesh PATH | --jac PATH | --json\n"
+        "         --nrhs N (with --tol) | --gmres M (with --tol)\n");
 }
 
 int main(int argc, char **argv) {
     int compute_mode = TBS_CUDA_MODE, device_id = 0, block_size = 9, iters = 30;
     double tol = -1.0;
-    int max_sweeps = 1000, algo = TBS_ALGO_FP64, inner = 4;
+    int max_sweeps = 1000, algo = TBS_ALGO_FP64, inner = 4, nrhs = 1, gmres_m = 0;
     bool gen = false, write_files = false, json = false;
     int gL = 0, gK = 0;
     double gshift = 9.0;
@@ -81,6 +88,8 @@ int main(int argc, char **argv) {
             else if (s == "--tol") { need(1); tol = std::stod(argv[++a]); }
             else if (s == "--max-sweeps") { need(1); max_sweeps = std::stoi(argv[++a]); }
             else if (s == "--inner") { need(1); inner = std::stoi(argv[++a]); }
+            else if (s == "--nrhs") { need(1); nrhs = std::stoi(argv[++a]); }
+            else if (s == "--gmres") { need(1); gmres_m = std::stoi(argv[++a]); }
             else if (s == "--algo") {
                 need(1);
                 std::string v = argv[++a];
@@ -134,7 +143,7 @@ int main(int argc, char **argv) {
         Mesh mesh;
         Jacobian Jac;
         if (gen) {
-            if (!mesh.fromStructured(gL, gK, 9)) throw std::runtime_error(mesh.error);
+            if (!mesh.fromStructured(gL, gK, block_size)) throw std::runtime_error(mesh.error);
         } else {
             std::printf("---------------------------------\n");
             std::printf(GREEN "Reading %s" COLOR_OFF "\n", mesh_path.c_str());
@@ -186,10 +195,42 @@ int main(int argc, char **argv) {
         std::printf("   LU Time: %f\n", LU_time);
         tbs_profile_reset(ctx);
 
+        if ((nrhs > 1 || gmres_m > 0) && tol < 0.0)
+            throw std::runtime_error("--nrhs and --gmres need --tol");
         std::vector<double> hist;
         int sweeps = 0;
         t0 = now_s();
-        if (tol >= 0.0) {
+        if (nrhs > 1) {
+            /* the Jacobian's rhs, then seeded U(-1,1) vectors (splitmix64) */
+            const size_t n = (size_t)mesh.nvar * mesh.nelem;
+            std::vector<double> rhs(n * nrhs), U(n * nrhs);
+            std::copy(Jac.rhs.begin(), Jac.rhs.end(), rhs.begin());
+            unsigned long long z0 = gseed + 0x5EEDull;
+            for (size_t t = n; t < rhs.size(); ++t) {
+                unsigned long long z = (z0 += 0x9E3779B97F4A7C15ull);
+                z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+                z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+                z ^= z >> 31;
+                rhs[t] = (double)(z >> 11) * 0x1.0p-53 * 2.0 - 1.0;
+            }
+            std::vector<int> sw(nrhs);
+            hist.assign((size_t)nrhs * (max_sweeps + 1), 0.0);
+            if (tbs_solve_multi(ctx, nrhs, rhs.data(), U.data(), tol, max_sweeps, sw.data(), hist.data(),
+                                max_sweeps + 1) != TBS_OK)
+                throw std::runtime_error(tbs_last_error(ctx));
+            for (int r = 0; r < nrhs; ++r) {
+                const double *h = hist.data() + (size_t)r * (max_sweeps + 1);
+                std::printf("  rhs %3d: %4d sweeps, ||R||/||R0|| = %.3e\n", r, sw[r],
+                            h[0] > 0 ? h[sw[r]] / h[0] : 0.0);
+            }
+            hist.resize(max_sweeps + 1); /* right-hand side 0 in the report below */
+            sweeps = sw[0];
+        } else if (gmres_m > 0) {
+            hist.assign((size_t)max_sweeps + 1, 0.0);
+            if (tbs_gmres(ctx, gmres_m, 1, tol, max_sweeps, &sweeps, hist.data()) != TBS_OK)
+                throw std::runtime_error(tbs_last_error(ctx));
+            std::printf("  GMRES(%d): %d Arnoldi steps\n", gmres_m, sweeps);
+        } else if (tol >= 0.0) {
             hist.assign((size_t)max_sweeps + 1, 0.0);
             if (tbs_solve(ctx, tol, max_sweeps, &sweeps, hist.data()) != TBS_OK)
                 throw std::runtime_error(tbs_last_error(ctx));
