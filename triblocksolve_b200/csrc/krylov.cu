@@ -39,7 +39,10 @@ constexpr int KRYLOV_MAX = 64;
 constexpr unsigned KFULL = 0xffffffffu;
 
 /* partials[c * KR_BLOCKS + block] = this block's part of V_c . w for
- * c < count, and of w . w for c == count when self != 0 */
+ * c < count, and of w . w for c == count when self != 0.  Each thread
+ * keeps KR_UNROLL grid-stride elements' loads in flight at once. */
+constexpr int KR_UNROLL = 4;
+
 __global__ void __launch_bounds__(KR_THREADS) kr_dots_kernel(long long n, const double *__restrict__ w,
                                                              const double *__restrict__ V, long long ldv,
                                                              int count, int self, double *partials) {
@@ -51,7 +54,28 @@ __global__ void __launch_bounds__(KR_THREADS) kr_dots_kernel(long long n, const 
         double acc[KR_CHUNK];
 #pragma unroll
         for (int k = 0; k < KR_CHUNK; ++k) acc[k] = 0.0;
-        for (long long t = t0; t < n; t += stride) {
+        long long t = t0;
+        for (; t + (KR_UNROLL - 1) * stride < n; t += KR_UNROLL * stride) {
+            double wt[KR_UNROLL];
+#pragma unroll
+            for (int u = 0; u < KR_UNROLL; ++u) wt[u] = w[t + u * stride];
+#pragma unroll
+            for (int k = 0; k < KR_CHUNK; ++k) {
+                const int c = c0 + k;
+                if (c < count) {
+                    const double *vc = V + (size_t)c * ldv + t;
+                    double x[KR_UNROLL];
+#pragma unroll
+                    for (int u = 0; u < KR_UNROLL; ++u) x[u] = vc[u * stride];
+#pragma unroll
+                    for (int u = 0; u < KR_UNROLL; ++u) acc[k] += x[u] * wt[u];
+                } else if (c == count && self) {
+#pragma unroll
+                    for (int u = 0; u < KR_UNROLL; ++u) acc[k] += wt[u] * wt[u];
+                }
+            }
+        }
+        for (; t < n; t += stride) {
             const double wt = w[t];
 #pragma unroll
             for (int k = 0; k < KR_CHUNK; ++k) {
@@ -103,8 +127,22 @@ __global__ void __launch_bounds__(KR_THREADS) kr_combine_kernel(long long n, dou
     __shared__ double cs[KRYLOV_MAX + 1];
     for (int c = threadIdx.x; c < count; c += KR_THREADS) cs[c] = sign * coef[c];
     __syncthreads();
-    for (long long t = blockIdx.x * (long long)KR_THREADS + threadIdx.x; t < n;
-         t += (long long)gridDim.x * KR_THREADS) {
+    const long long stride = (long long)gridDim.x * KR_THREADS;
+    long long t = blockIdx.x * (long long)KR_THREADS + threadIdx.x;
+    for (; t + (KR_UNROLL - 1) * stride < n; t += KR_UNROLL * stride) {
+        double acc[KR_UNROLL];
+#pragma unroll
+        for (int u = 0; u < KR_UNROLL; ++u) acc[u] = x[t + u * stride];
+#pragma unroll 4
+        for (int c = 0; c < count; ++c) {
+            const double *vc = V + (size_t)c * ldv + t;
+#pragma unroll
+            for (int u = 0; u < KR_UNROLL; ++u) acc[u] += cs[c] * vc[u * stride];
+        }
+#pragma unroll
+        for (int u = 0; u < KR_UNROLL; ++u) x[t + u * stride] = acc[u];
+    }
+    for (; t < n; t += stride) {
         double acc = x[t];
         for (int c = 0; c < count; ++c) acc += cs[c] * V[(size_t)c * ldv + t];
         x[t] = acc;
@@ -113,9 +151,16 @@ __global__ void __launch_bounds__(KR_THREADS) kr_combine_kernel(long long n, dou
 
 __global__ void __launch_bounds__(KR_THREADS) kr_scale_kernel(long long n, double *__restrict__ dst,
                                                               const double *__restrict__ src, double a) {
-    for (long long t = blockIdx.x * (long long)KR_THREADS + threadIdx.x; t < n;
-         t += (long long)gridDim.x * KR_THREADS)
-        dst[t] = a * src[t];
+    const long long stride = (long long)gridDim.x * KR_THREADS;
+    long long t = blockIdx.x * (long long)KR_THREADS + threadIdx.x;
+    for (; t + (KR_UNROLL - 1) * stride < n; t += KR_UNROLL * stride) {
+        double v[KR_UNROLL];
+#pragma unroll
+        for (int u = 0; u < KR_UNROLL; ++u) v[u] = src[t + u * stride];
+#pragma unroll
+        for (int u = 0; u < KR_UNROLL; ++u) dst[t + u * stride] = a * v[u];
+    }
+    for (; t < n; t += stride) dst[t] = a * src[t];
 }
 
 }  // namespace
