@@ -247,10 +247,11 @@ def run_batch(args):
     cells = np.array([m.nelem for m in meshes], dtype=np.int64)
     max_sweeps = 400
     inner = None
-    if args.algo == "mixed":
-        inner = 3
-        batch.set_inner_sweeps(inner)
     ctas, stages, order, tune_ms = batch.tune()
+    if args.algo == "mixed":
+        # the FP32 inner sweep schedule (first outer step, the others) timed on the batch
+        f_in, r_in, _ = batch.tune_inner(tol, max_sweeps)
+        inner = [f_in, r_in]
     with ClockSampler(local) as clocks:
         for _ in range(max(args.warmup, 0)):
             batch.solve(tol, max_sweeps)
@@ -310,10 +311,14 @@ def run_batch(args):
         for name, (launches, ms) in prof.items():
             b = None
             if name in names:
-                # every system contributes its bytes once per launch in each sweep it runs
-                per_sweep = {"fast_thomas32": inner, "fast_resid32": (inner or 1) - 1}.get(name, 1)
-                b = nprof * per_sweep * sum(s.kernel_bytes(name) * int(n_sw)
-                                            for s, n_sw in zip(solvers, swp))
+                # every system contributes its bytes once per launch it takes part in
+                def runs(n_sw):
+                    n_sw = int(n_sw)
+                    if not inner or n_sw == 0:
+                        return n_sw
+                    th = inner[0] + (n_sw - 1) * inner[1]
+                    return {"fast_thomas32": th, "fast_resid32": th - n_sw}.get(name, n_sw)
+                b = nprof * sum(s.kernel_bytes(name) * runs(n_sw) for s, n_sw in zip(solvers, swp))
             kern[name] = {"launches": launches, "total_ms": round(ms, 3),
                           "avg_us": round(1e3 * ms / launches, 2) if launches else None,
                           "bytes_total": b,

@@ -371,6 +371,12 @@ int tbs_batch_tune(tbs_batch *batch, int *ctas_per_sm, int *stages, int *order,
 int tbs_batch_set_inner_sweeps(tbs_batch *batch, int m);
 int tbs_batch_set_inner_schedule(tbs_batch *batch, int first, int rest);
 
+/* TBS_ALGO_MIXED: times batched solves to rel_tol under the inner sweep
+ * schedules tbs_tune_inner tries, keeps the fastest one with which every
+ * member reaches the tolerance, and reports it (outputs may be NULL). */
+int tbs_batch_tune_inner(tbs_batch *batch, double rel_tol, int max_sweeps,
+                         int *first, int *rest, double *best_ms);
+
 /* Per-kernel CUDA-event timing of batched solves (eager launches while
  * enabled), as tbs_profile_*. */
 int tbs_batch_profile_enable(tbs_batch *batch, int on);

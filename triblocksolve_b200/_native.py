@@ -108,6 +108,7 @@ _sig("tbs_batch_get_schedule", _i, _vp, _ip, _ip, _ip)
 _sig("tbs_batch_tune", _i, _vp, _ip, _ip, _ip, _dp)
 _sig("tbs_batch_set_inner_sweeps", _i, _vp, _i)
 _sig("tbs_batch_set_inner_schedule", _i, _vp, _i, _i)
+_sig("tbs_batch_tune_inner", _i, _vp, C.c_double, _i, _ip, _ip, _dp)
 _sig("tbs_batch_profile_enable", _i, _vp, _i)
 _sig("tbs_batch_profile_reset", _i, _vp)
 _sig("tbs_batch_profile_read", _i, _vp, _ip, C.POINTER(_cp), C.POINTER(C.c_longlong), _dp)

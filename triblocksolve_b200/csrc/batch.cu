@@ -16,6 +16,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <new>
@@ -291,6 +292,7 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         efree_async(e, &e.d_g_tiles);
         efree_async(e, &e.d_g_prime);
         efree_async(e, &e.d_g_blocks);
+        efree_async(e, &e.d_g_chunks);
         if (e.algo == TBS_ALGO_FP64) {
             if (!rc) rc = ealloc_async(e, &e.d_th64, c);
             if (!rc) rc = ealloc_async(e, &e.d_rs_prime, c);
@@ -310,6 +312,7 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         if (!rc) rc = ealloc_async(e, &e.d_g_tiles, gi);
         if (!rc) rc = ealloc_async(e, &e.d_g_prime, gi);
         if (!rc) rc = ealloc_async(e, &e.d_g_blocks, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_chunks, gi);
         e.cap_mem = rc ? 0 : c;
         engine_drop_graph(e);
     }
@@ -471,18 +474,20 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         engine_drop_graph(e);
     }
     /* group indices of the residual-type launches */
-    auto units = [&](const std::vector<std::vector<int>> &g, bool blocks) {
+    /* units: 0 residual tiles, 1 element blocks, 2 chunks of BATCH_CHUNK tiles */
+    auto units = [&](const std::vector<std::vector<int>> &g, int kind) {
         std::vector<int> u;
         for (const auto &grp : g) {
             const tbs_ctx *c = members[grp[0]].sys;
-            u.push_back(blocks ? full_resid_blocks(c->nelem) : fast_resid_grid(c->L.np16));
+            const int nt = fast_resid_grid(c->L.np16);
+            u.push_back(kind == 1 ? full_resid_blocks(c->nelem) : kind == 2 ? batch_chunks(nt) : nt);
         }
         return u;
     };
     const auto g_all = group_members(members, all);
     const auto g_prime = group_members(members, prime);
-    const std::vector<int> gi_tiles = group_index(g_all, units(g_all, false));
-    const std::vector<int> gi_prime = group_index(g_prime, units(g_prime, false));
+    const std::vector<int> gi_tiles = group_index(g_all, units(g_all, 0));
+    const std::vector<int> gi_prime = group_index(g_prime, units(g_prime, 0));
     e.members = members;
     std::vector<WorkItem> lines = line_items(e, members);
     Stager up(e);
@@ -497,12 +502,13 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         up.put(e.d_fr, fr);
         up.put(e.d_fp, fp);
         up.put(e.d_vec, vec);
-        up.put(e.d_g_blocks, group_index(g_all, units(g_all, true)));
+        up.put(e.d_g_blocks, group_index(g_all, units(g_all, 1)));
     }
     up.put(e.d_red_prime, redp);
     up.put(e.d_red_body, redb);
     up.put(e.d_lines, lines);
     up.put(e.d_g_tiles, gi_tiles);
+    up.put(e.d_g_chunks, group_index(g_all, units(g_all, 2)));
     up.put(e.d_g_prime, gi_prime);
     up.put(e.d_active, e.h_active);
     rc = up.flush();
@@ -571,7 +577,7 @@ static int engine_prime(Engine &e, Cond cc) {
     }
     BatchCtl *C = e.d_ctl;
     if (e.algo == TBS_ALGO_FP64) {
-        ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_g_prime,
+        ERUN("fast_resid_rhs", launch_resid_batch<double>(st, 0, e.max_nx, e.d_rs_prime, e.d_g_prime, 1,
                                                           nullptr, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_prime, &C->nprime_sys, e.cap_mem, 1,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use,
@@ -591,8 +597,8 @@ static int engine_body(Engine &e, Cond cc, int inner) {
     if (e.algo == TBS_ALGO_FP64) {
         ERUN("fast_thomas", launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines, &C->nlines,
                                                         e.d_active, e.d_queue, e.d_status));
-        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_tiles,
-                                                      e.d_active, e.d_status));
+        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_chunks,
+                                                      BATCH_CHUNK, e.d_active, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_body, &C->nsys, e.cap_mem, 0,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use));
         return TBS_OK;
@@ -601,19 +607,19 @@ static int engine_body(Engine &e, Cond cc, int inner) {
      * launch, each inner residual adds its sweep's d to it, and the last d
      * goes to U with c (the order of the single-system sequence) */
     if (!e.fullpos)
-        ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_g_tiles,
+        ERUN("fast_resid32_rhs", launch_resid_batch<float>(st, 0, e.max_nx, e.d_rs32_rhs, e.d_g_tiles, 1,
                                                            e.d_active, e.d_status));
     for (int m = 0; m < inner; ++m) {
         ERUN("fast_thomas32", launch_thomas_batch<float>(st, e.sched, e.d_th32, e.d_lines, &C->nlines,
                                                          e.d_active, e.d_queue, e.d_status));
         if (m + 1 < inner)
-            ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_g_tiles,
+            ERUN("fast_resid32", launch_resid_batch<float>(st, 3, e.max_nx, e.d_rs32_dx, e.d_g_tiles, 1,
                                                            e.d_active, e.d_status));
     }
     ERUN("axpy", launch_axpy2_batch(st, e.d_vec, e.d_g_tiles, e.d_active));
     if (e.fullpos)
-        ERUN("full_resid", launch_full_resid_pos_batch(st, e.max_nxf, e.d_fp, e.d_g_tiles, e.d_active,
-                                                       e.d_status));
+        ERUN("full_resid", launch_full_resid_pos_batch(st, e.max_nxf, e.d_fp, e.d_g_chunks, BATCH_CHUNK,
+                                                       e.d_active, e.d_status));
     else
         ERUN("full_resid", launch_full_resid_batch(st, e.d_fr, e.d_g_blocks, e.d_active));
     ERUN("reduce_norm", launch_reduce_batch(st, 1024, e.d_red_body, &C->nsys, e.cap_mem, 0, e.d_active,
@@ -1111,6 +1117,80 @@ int tbs_batch_tune(tbs_batch *b, int *ctas_per_sm, int *stages, int *order, doub
     if (stages) *stages = s.stages;
     if (order) *order = o;
     if (best_ms) *best_ms = ms;
+    return TBS_OK;
+    BGUARD_END
+}
+
+/* one timed batch solve (best of two after a first one that builds the
+ * graph); +inf unless every member reached the tolerance */
+static int batch_time_schedule(tbs_batch *b, int first, int rest, double rel_tol, int max_sweeps,
+                               cudaEvent_t e0, cudaEvent_t e1, double *ms_out) {
+    int rc = tbs_batch_set_inner_schedule(b, first, rest);
+    if (!rc) rc = tbs_batch_solve(b, rel_tol, max_sweeps, nullptr, nullptr);
+    double t = 1e300;
+    for (int rep = 0; rep < 2 && !rc; ++rep) {
+        cudaEventRecord(e0, b->eng.stream);
+        rc = tbs_batch_solve(b, rel_tol, max_sweeps, nullptr, nullptr);
+        cudaEventRecord(e1, b->eng.stream);
+        cudaEventSynchronize(e1);
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        t = std::min(t, (double)ms);
+    }
+    if (rc) return rc;
+    bool conv = true;
+    for (tbs_ctx *c : b->sys) {
+        const SolveState &S = *c->h_state;
+        conv = conv && std::isfinite(S.last) && S.last <= S.tol * S.norm0;
+    }
+    *ms_out = conv ? t : 1e300;
+    return TBS_OK;
+}
+
+int tbs_batch_tune_inner(tbs_batch *b, double rel_tol, int max_sweeps, int *first_out,
+                         int *rest_out, double *best_ms) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (b->eng.algo != TBS_ALGO_MIXED)
+        return bfail(b, TBS_ERR_STATE, "tbs_batch_tune_inner needs TBS_ALGO_MIXED systems");
+    if (max_sweeps < 1 || !(rel_tol >= 0.0)) return bfail(b, TBS_ERR_ARG, "bad tolerance or sweep limit");
+    BGUARD_BEGIN
+    if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
+    const bool prof = b->eng.prof;
+    b->eng.prof = false;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess)
+        return bfail(b, TBS_ERR_CUDA, "cudaEventCreate failed");
+    int bf = -1, br = -1, rc = TBS_OK;
+    double best_t = 1e300;
+    auto consider = [&](int f, int r) {
+        if (rc || f < 1 || r < 1) return;
+        double t = 1e300;
+        rc = batch_time_schedule(b, f, r, rel_tol, max_sweeps, e0, e1, &t);
+        if (!rc && t < best_t) {
+            best_t = t;
+            bf = f;
+            br = r;
+        }
+    };
+    /* the search of tbs_tune_inner: one count for every outer step, then
+     * the first step's own count around the best */
+    for (int m : {2, 3, 4, 5, 6, 8}) consider(m, m);
+    if (!rc && br > 0) {
+        const int m = br;
+        for (int r : {m - 1, m, m + 1})
+            for (int f : {m - 2, m - 1, m, m + 1, m + 2})
+                if (!(f == r && (r == m - 1 || r == m || r == m + 1))) consider(f, r);
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    b->eng.prof = prof;
+    if (rc) return rc;
+    if (bf < 0) return bfail(b, TBS_ERR_NUMERIC, "no inner sweep schedule reached the tolerance");
+    rc = tbs_batch_set_inner_schedule(b, bf, br);
+    if (rc) return rc;
+    if (first_out) *first_out = bf;
+    if (rest_out) *rest_out = br;
+    if (best_ms) *best_ms = best_t;
     return TBS_OK;
     BGUARD_END
 }

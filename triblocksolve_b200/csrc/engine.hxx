@@ -71,6 +71,7 @@ struct Engine {
     ReduceSys *d_red_prime = nullptr, *d_red_body = nullptr;
     WorkItem *d_lines = nullptr;                       /* Thomas items, explicit */
     int *d_g_tiles = nullptr, *d_g_prime = nullptr, *d_g_blocks = nullptr; /* group indices */
+    int *d_g_chunks = nullptr; /* every member, units of BATCH_CHUNK tiles */
     int *d_active = nullptr;
     unsigned *d_queue = nullptr, *d_counter = nullptr, *d_status = nullptr;
     BatchCtl *d_ctl = nullptr;

@@ -1775,6 +1775,37 @@ __device__ __forceinline__ WorkItem group_item(const int *__restrict__ gi, int w
 
 __device__ __forceinline__ int group_items(const int *__restrict__ gi) { return gi[1 + gi[0]]; }
 
+/* group_item for a CTA that visits items in increasing order: the group of
+ * the last item (its range [lo, hi) and index g) is kept, so the binary
+ * search runs only when the item leaves it */
+struct GroupCursor {
+    int lo = 0, hi = 0, g = -1;
+    int r = 1, mo = 0, m0 = 0; /* the group's member count, list offset, first member */
+};
+
+__device__ __forceinline__ WorkItem group_item_next(const int *__restrict__ gi, int w, GroupCursor &c) {
+    const int ng = gi[0];
+    const int *base = gi + 1;
+    const int *nmem = base + ng + 1, *moff = nmem + ng, *mlist = moff + ng;
+    if (c.g < 0 || w < c.lo || w >= c.hi) {
+        int lo = 0, hi = ng - 1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (base[mid] <= w) lo = mid;
+            else hi = mid - 1;
+        }
+        c.g = lo;
+        c.lo = base[lo];
+        c.hi = base[lo + 1];
+        c.r = nmem[lo];
+        c.mo = moff[lo];
+        c.m0 = mlist[c.mo];
+    }
+    const int off = w - c.lo;
+    if (c.r == 1) return WorkItem{c.m0, off};
+    return WorkItem{mlist[c.mo + off % c.r], off / c.r};
+}
+
 static int sm_count() {
     int dev = 0, n = 0;
     cudaGetDevice(&dev);
@@ -1812,27 +1843,41 @@ int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T
     return (int)cudaGetLastError();
 }
 
-/* persistent residual over (member, tile) items: CTA k takes items k,
- * k + grid, ...; each tile completes one phase of the CTA's barrier */
-template <typename T>
-__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_batch_kernel(
+/* The tiles [unit * chunk, ...) of a member: the units of a group index
+ * are single tiles (chunk 1) or chunks of BATCH_CHUNK tiles, which pay the
+ * item's decode and descriptor load once for several tiles */
+__device__ __forceinline__ int chunk_end(int unit, int chunk, int ntiles) {
+    const int e = (unit + 1) * chunk;
+    return e < ntiles ? e : ntiles;
+}
+
+/* persistent residual over (member, tile or chunk) items: CTA k takes
+ * items k, k + grid, ...; each tile completes one phase of the CTA's
+ * barrier and writes its own partial */
+template <typename T, int CHUNK>
+__global__ void __launch_bounds__(RES_THREADS_FAST, CHUNK == 1 ? 8 : 6) fast_resid_batch_kernel(
     const ResidSys<T> *__restrict__ sys, const int *__restrict__ groups, int mode,
     const int *__restrict__ active, unsigned *status) {
+    constexpr int chunk = CHUNK;
     uint64_t *bar = resid_bar_init();
     const int nwork = group_items(groups);
     uint32_t parity = 0;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = group_item(groups, w);
+    GroupCursor gc;
+    bool ok = true;
+    for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
+        const WorkItem it = group_item_next(groups, w, gc);
         if (active && !active[it.sys]) continue;
         const ResidSys<T> S = sys[it.sys];
         NormSink ns{};
         ns.partials = (mode == 3) ? nullptr : S.partials; /* no counter: partials only */
-        const bool ok = fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr,
-                                           S.dU, S.Rsrc, S.b, S.Uacc, ns, status, it.unit, bar,
-                                           parity);
-        parity ^= 1u;
-        if (!ok) break;
-        __syncthreads(); /* the next tile's copies overwrite the stages */
+        const int t1 = chunk_end(it.unit, chunk, S.np16 / RES_TILE);
+        for (int t = it.unit * chunk; t < t1; ++t) {
+            ok = fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr, S.dU,
+                                    S.Rsrc, S.b, S.Uacc, ns, status, t, bar, parity);
+            parity ^= 1u;
+            if (!ok) break;
+            __syncthreads(); /* the next tile's copies overwrite the stages */
+        }
     }
 }
 
@@ -1846,12 +1891,19 @@ static int resid_batch_grid(size_t smem, const void *fn) {
 
 template <typename T>
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const int *groups, const int *active, unsigned *status) {
+                       const int *groups, int chunk, const int *active, unsigned *status) {
     if (mode != 0 && mode != 1 && mode != 3) return (int)cudaErrorInvalidValue;
+    if (chunk != 1 && chunk != BATCH_CHUNK) return (int)cudaErrorInvalidValue;
     const size_t smem = resid_smem_bytes<T>(mode == 0 ? 0 : max_nx);
-    const int grid = resid_batch_grid(smem, (const void *)fast_resid_batch_kernel<T>);
-    fast_resid_batch_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, mode, active,
-                                                                     status);
+    if (chunk == 1) {
+        const int grid = resid_batch_grid(smem, (const void *)fast_resid_batch_kernel<T, 1>);
+        fast_resid_batch_kernel<T, 1><<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, mode, active,
+                                                                            status);
+    } else {
+        const int grid = resid_batch_grid(smem, (const void *)fast_resid_batch_kernel<T, BATCH_CHUNK>);
+        fast_resid_batch_kernel<T, BATCH_CHUNK><<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, mode,
+                                                                                      active, status);
+    }
     return (int)cudaGetLastError();
 }
 
@@ -1859,8 +1911,9 @@ __global__ void __launch_bounds__(FULLRES_THREADS) full_resid_batch_kernel(
     const FullResSys *__restrict__ sys, const int *__restrict__ groups,
     const int *__restrict__ active) {
     const int nwork = group_items(groups);
+    GroupCursor gc;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = group_item(groups, w);
+        const WorkItem it = group_item_next(groups, w, gc);
         if (active && !active[it.sys]) continue;
         const FullResSys S = sys[it.sys];
         full_resid_body<float>(S.nelem, S.epoint, S.ef, S.fc, S.pos_of_elem, S.D, S.O1, S.O2,
@@ -1886,8 +1939,9 @@ int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *g
 __global__ void __launch_bounds__(RES_THREADS_FAST) mixed_prime_batch_kernel(
     const VecSys *__restrict__ sys, const int *__restrict__ groups) {
     const int nwork = group_items(groups);
+    GroupCursor gc;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = group_item(groups, w);
+        const WorkItem it = group_item_next(groups, w, gc);
         const VecSys S = sys[it.sys];
         mixed_prime_body(S.rhsp, S.R32, S.Up, S.partials, S.Dinv32, S.b32, S.c32, it.unit);
         __syncthreads();
@@ -1905,8 +1959,9 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) axpy2_batch_kernel(
     const VecSys *__restrict__ sys, const int *__restrict__ groups,
     const int *__restrict__ active) {
     const int nwork = group_items(groups);
+    GroupCursor gc;
     for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = group_item(groups, w);
+        const WorkItem it = group_item_next(groups, w, gc);
         if (active && !active[it.sys]) continue;
         if (threadIdx.x >= RES_TILE * NV) continue;
         const VecSys S = sys[it.sys];
@@ -1922,29 +1977,34 @@ int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, co
 }
 
 __global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_batch_kernel(
-    const FullPosSys *__restrict__ sys, const int *__restrict__ groups,
+    const FullPosSys *__restrict__ sys, const int *__restrict__ groups, int chunk,
     const int *__restrict__ active, unsigned *status) {
     uint64_t *bar = resid_bar_init();
     const int nwork = group_items(groups);
     uint32_t parity = 0;
-    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
-        const WorkItem it = group_item(groups, w);
+    GroupCursor gc;
+    bool ok = true;
+    for (int w = blockIdx.x; w < nwork && ok; w += gridDim.x) {
+        const WorkItem it = group_item_next(groups, w, gc);
         if (active && !active[it.sys]) continue;
         const FullPosSys S = sys[it.sys];
-        const bool ok = full_resid_pos_body(S.nxf, S.np16, S.Dp, S.XF, S.xnbrf, S.rhsp, S.Up, S.R32,
-                                            S.partials, S.Dinv32, S.b32, S.c32, status, it.unit, bar,
-                                            parity);
-        parity ^= 1u;
-        if (!ok) break;
-        __syncthreads(); /* the next tile's copies overwrite the stages */
+        const int t1 = chunk_end(it.unit, chunk, S.np16 / RES_TILE);
+        for (int t = it.unit * chunk; t < t1; ++t) {
+            ok = full_resid_pos_body(S.nxf, S.np16, S.Dp, S.XF, S.xnbrf, S.rhsp, S.Up, S.R32,
+                                     S.partials, S.Dinv32, S.b32, S.c32, status, t, bar, parity);
+            parity ^= 1u;
+            if (!ok) break;
+            __syncthreads(); /* the next tile's copies overwrite the stages */
+        }
     }
 }
 
 int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
-                                const int *groups, const int *active, unsigned *status) {
+                                const int *groups, int chunk, const int *active, unsigned *status) {
     const size_t smem = fullpos_smem_bytes(max_nxf);
     const int grid = resid_batch_grid(smem, (const void *)full_resid_pos_batch_kernel);
-    full_resid_pos_batch_kernel<<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, active, status);
+    full_resid_pos_batch_kernel<<<grid, RES_THREADS_FAST, smem, st>>>(sys, groups, chunk, active,
+                                                                      status);
     return (int)cudaGetLastError();
 }
 
@@ -2024,9 +2084,15 @@ int launch_reduce_batch(cudaStream_t st, int threads, const ReduceSys *sys, cons
 /* opt the batched kernels into the shared memory of the widest member
  * (outside stream capture) */
 int batch_prepare(int max_nx) {
-    int rc = set_smem((const void *)fast_resid_batch_kernel<double>, resid_smem_bytes<double>(max_nx));
+    int rc = set_smem((const void *)fast_resid_batch_kernel<double, 1>, resid_smem_bytes<double>(max_nx));
     if (!rc)
-        rc = set_smem((const void *)fast_resid_batch_kernel<float>, resid_smem_bytes<float>(max_nx));
+        rc = set_smem((const void *)fast_resid_batch_kernel<double, BATCH_CHUNK>,
+                      resid_smem_bytes<double>(max_nx));
+    if (!rc)
+        rc = set_smem((const void *)fast_resid_batch_kernel<float, 1>, resid_smem_bytes<float>(max_nx));
+    if (!rc)
+        rc = set_smem((const void *)fast_resid_batch_kernel<float, BATCH_CHUNK>,
+                      resid_smem_bytes<float>(max_nx));
     if (!rc) rc = set_smem((const void *)full_resid_pos_batch_kernel, fullpos_smem_bytes(4));
     return rc;
 }
@@ -2046,9 +2112,9 @@ template int launch_thomas_batch<float>(cudaStream_t, const BatchSched &, const 
                                         const WorkItem *, const int *, const int *, unsigned *,
                                         unsigned *);
 template int launch_resid_batch<double>(cudaStream_t, int, int, const ResidSys<double> *,
-                                        const int *, const int *, unsigned *);
+                                        const int *, int, const int *, unsigned *);
 template int launch_resid_batch<float>(cudaStream_t, int, int, const ResidSys<float> *,
-                                       const int *, const int *, unsigned *);
+                                       const int *, int, const int *, unsigned *);
 
 
 /* ============================================== several right-hand sides

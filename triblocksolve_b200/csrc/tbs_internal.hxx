@@ -363,16 +363,20 @@ int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T
  *   [ng][base[0..ng]][nmem[0..ng)][moff[0..ng)][mlist[...]]
  * item w -> member mlist[moff[g] + (w - base[g]) % nmem[g]],
  *           unit (w - base[g]) / nmem[g]. */
+/* units of the chunked group index: up to BATCH_CHUNK residual tiles */
+constexpr int BATCH_CHUNK = 8;
+inline int batch_chunks(int ntiles) { return (ntiles + BATCH_CHUNK - 1) / BATCH_CHUNK; }
 inline size_t group_index_ints(int max_groups, int max_members) {
     return 1 + (size_t)(max_groups + 1) + 2 * (size_t)max_groups + (size_t)max_members;
 }
 template <typename T>
+/* units of `groups`: single tiles (chunk 1) or chunks of BATCH_CHUNK tiles */
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
-                       const int *groups, const int *active, unsigned *status);
+                       const int *groups, int chunk, const int *active, unsigned *status);
 int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *groups,
                             const int *active);
 int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
-                                const int *groups, const int *active, unsigned *status);
+                                const int *groups, int chunk, const int *active, unsigned *status);
 int launch_mixed_prime_batch(cudaStream_t st, const VecSys *sys, const int *groups);
 int launch_axpy2_batch(cudaStream_t st, const VecSys *sys, const int *groups, const int *active);
 /* one CTA of `threads` threads per norm descriptor (grid = cap, *nred in

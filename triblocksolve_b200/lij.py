@@ -450,6 +450,14 @@ class Batch:
     def set_inner_sweeps(self, m: int):
         self._chk(N.lib.tbs_batch_set_inner_sweeps(self.handle, m))
 
+    def tune_inner(self, rel_tol: float, max_sweeps: int = 200):
+        """ALGO_MIXED: pick the fastest inner sweep schedule with which every
+        member reaches rel_tol (device timing); returns (first, rest, ms)."""
+        f, r, ms = C.c_int(), C.c_int(), C.c_double()
+        self._chk(N.lib.tbs_batch_tune_inner(self.handle, rel_tol, max_sweeps, C.byref(f),
+                                             C.byref(r), C.byref(ms)))
+        return f.value, r.value, ms.value
+
     def set_inner_schedule(self, first: int, rest: int):
         self._chk(N.lib.tbs_batch_set_inner_schedule(self.handle, first, rest))
 
