@@ -15,8 +15,8 @@
  *     sweeps is done, so new arrivals join at the next sweep boundary,
  *   - retires each right-hand side as soon as it stops and completes a
  *     request when all of its right-hand sides have.
- * A second thread re-factors systems (upload of the new values and the
- * factorization on the system's own stream) into a spare copy of the
+ * A factor thread per lane re-factors systems (upload of the new values
+ * and the factorization on the system's own stream) into a spare copy of the
  * system's factors, so that the right-hand sides already admitted keep
  * sweeping on the current copy; the system's later requests wait for the
  * new factors.  When the spare copy does not fit the budget, the system is
@@ -127,6 +127,10 @@ struct SrvLane {
     SolveState *h_up_states = nullptr; /* pinned, max_slots: states of admitted ones */
     std::string err;
     std::thread th;
+    /* re-factorizations of this lane's systems, by the lane's own factor
+     * thread: a small system's new Jacobian never waits behind a large one */
+    std::deque<SrvRequest *> factor_jobs;
+    std::thread factor;
 };
 
 struct tbs_server {
@@ -145,7 +149,6 @@ struct tbs_server {
     size_t slot_bytes_in_flight = 0;
     std::deque<SrvRequest *> queue;
     std::map<long long, std::unique_ptr<SrvRequest>> requests;
-    std::deque<SrvRequest *> factor_jobs;
     long long next_id = 1;
 
     /* one loop thread per lane: systems below lane_split cells sweep in
@@ -156,7 +159,6 @@ struct tbs_server {
     cudaMemPool_t pool = nullptr;
     bool pool_reserved = false;
     int rhs_in_flight = 0;             /* admitted, not yet read back (all lanes) */
-    std::thread factor;
 
     /* statistics */
     long long n_done = 0, n_rhs_done = 0, n_launches = 0, n_refactor = 0;
@@ -242,17 +244,17 @@ static void complete(tbs_server *s, SrvRequest *r, int err, const std::string &m
 
 /* ---------------------------------------------------------------- factor thread */
 
-static void factor_main(tbs_server *s) {
+static void factor_main(tbs_server *s, SrvLane *L) {
     cudaSetDevice(s->device);
     std::unique_lock<std::mutex> lk(s->mu);
     for (;;) {
-        s->cv_factor.wait(lk, [&] { return s->stopping || !s->factor_jobs.empty(); });
-        if (s->factor_jobs.empty()) {
+        s->cv_factor.wait(lk, [&] { return s->stopping || !L->factor_jobs.empty(); });
+        if (L->factor_jobs.empty()) {
             if (s->stopping) break;
             continue;
         }
-        SrvRequest *r = s->factor_jobs.front();
-        s->factor_jobs.pop_front();
+        SrvRequest *r = L->factor_jobs.front();
+        L->factor_jobs.pop_front();
         tbs_ctx *c = s->systems[r->sys].ctx[r->target];
         const tbs_ctx *model = s->systems[r->sys].ctx[s->systems[r->sys].cur];
         const bool fresh = r->new_version;
@@ -338,7 +340,7 @@ static void admit_scan(tbs_server *s, SrvLane *L, std::vector<SrvRequest *> &adm
                 r->new_version = fits && !have;
                 if (r->new_version) s->sys_bytes += sys.bytes;
                 r->state = SrvRequest::FACTORING;
-                s->factor_jobs.push_back(r);
+                L->factor_jobs.push_back(r);
                 s->cv_factor.notify_all();
             }
             blocked[r->sys] = 1;
@@ -623,7 +625,7 @@ static void loop_main(tbs_server *s, SrvLane *L) {
                 mine = true;
                 if (r->state == SrvRequest::QUEUED && !s->systems[r->sys].refactoring) ready = true;
             }
-            if (s->stopping && !mine && s->factor_jobs.empty()) break;
+            if (s->stopping && !mine && L->factor_jobs.empty()) break;
             if (!mine)
                 s->cv_loop.wait(lk);
             else if (!ready) /* queued behind a re-factorization */
@@ -683,7 +685,8 @@ static void server_stop(tbs_server *s) {
         s->cv_factor.notify_all();
         s->cv_done.notify_all();
     }
-    if (s->factor.joinable()) s->factor.join();
+    for (auto &L : s->lanes)
+        if (L->factor.joinable()) L->factor.join();
     {
         std::lock_guard<std::mutex> lk(s->mu);
         for (SrvRequest *r : s->queue) complete(s, r, TBS_ERR_STATE, "server stopped");
@@ -741,8 +744,10 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
     uint64_t keep = ~0ull; /* freed right-hand-side memory stays in the pool */
     cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep);
     try {
-        for (auto &L : s->lanes) L->th = std::thread(loop_main, s, L.get());
-        s->factor = std::thread(factor_main, s);
+        for (auto &L : s->lanes) {
+            L->th = std::thread(loop_main, s, L.get());
+            L->factor = std::thread(factor_main, s, L.get());
+        }
     } catch (...) {
         {
             std::lock_guard<std::mutex> lk(s->mu);
@@ -750,9 +755,10 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
             s->cv_loop.notify_all();
             s->cv_factor.notify_all();
         }
-        for (auto &L : s->lanes)
+        for (auto &L : s->lanes) {
             if (L->th.joinable()) L->th.join();
-        if (s->factor.joinable()) s->factor.join();
+            if (L->factor.joinable()) L->factor.join();
+        }
         return fail(TBS_ERR_STATE, "thread start failed");
     }
     *out = s;
