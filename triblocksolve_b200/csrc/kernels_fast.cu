@@ -567,17 +567,18 @@ int launch_fast_xlayout(cudaStream_t st, const FastLayout &L, const double *O1, 
 }
 
 /* ================================================ residual -> Thomas RHS
- * One CTA per tile of RES_TILE positions (no persistent loop: ~6 CTAs per
- * SM keep ~200 KB of bulk copies in flight).  Per tile:
+ * Tiles of RES_TILE positions, each staged by one phase of the CTA's bulk
+ * copy barrier; the single-system launches are persistent (as many CTAs
+ * as fit, tiles round-robin per CTA).  Per tile:
  *   mode 0:  R = Rsrc (a residual already in position order)
  *   mode 1:  R = sum over slots X_slot dU[xnbr_slot]   (R_new = O dU)
  * then b = -Dinv R.  Thread t < 144 owns (cell c = t % 16, row i = t / 16):
  * with blocks 81 doubles apart, the 16 cells of a half-warp hit 16
  * distinct bank pairs, so the shared-memory reads are conflict-free.
  * X and xnbr are slot-major ([slot][position]) for the same reason.
- * Every CTA writes sum R^2 of its tile; the last CTA to finish (atomic
- * ticket) adds the partials in a fixed order and, when asked, records the
- * norm, the sweep count and the graph's loop condition.
+ * Every tile writes its sum R^2; the last CTA to finish (atomic ticket)
+ * adds the partials in tile order and, when asked, records the norm, the
+ * sweep count and the graph's loop condition.
  */
 constexpr int RES_THREADS_FAST = 160;
 
