@@ -308,17 +308,23 @@ __device__ __forceinline__ double nv_row_step(const double *blk, int i, double i
     return a0 - (a1 + a2);
 }
 
-constexpr int NVT_P = 8; /* cells per chunk of a chain */
+/* cells per chunk of a chain: 8, or 4 for blocks of 10..13 so that a
+ * two-stage ring stays small enough for nine lines per SM (one wave at
+ * 1,200 lines; measured: 10-25 % faster there, slower from 14 on, where
+ * even 4-cell chunks do not reach one wave); a multiple of 4 keeps every
+ * bulk copy 16-byte sized */
+template <int NV>
+constexpr int nv_chunk() { return (NV >= 10 && NV <= 13) ? 4 : 8; }
 
 template <int NV>
 __host__ __device__ inline size_t nv_thomas_stage() {
-    return 2 * (size_t)NVT_P * (NV * NV + NV) * sizeof(double);
+    return 2 * (size_t)nv_chunk<NV>() * (NV * NV + NV) * sizeof(double);
 }
 
 /* One warp per line: half-warp h runs chain h (top: positions 0..m-1 in
  * order, bottom: m..n-2 in elimination order), lane i < NV row i.  Lane 0
  * streams "jobs" through an NS-stage ring of bulk copies, each holding one
- * chunk of NVT_P cells of both chains: forward jobs the blocks of G and the
+ * chunk of nv_chunk<NV>() cells of both chains: forward jobs the blocks of G and the
  * b vectors, backward jobs (in reverse) the blocks of Gam; y is read back
  * with plain loads one chunk ahead.  Forward y_s = b_s - G_s y_{s-1}, twist
  * x = b - G_tw y_top - Gam_tw y_bot, backward x_s = y_s - Gam_s x_{s+1};
@@ -330,7 +336,7 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
     const int *__restrict__ line_twist, const double *__restrict__ G, const double *__restrict__ Gam,
     const double *__restrict__ b, double *__restrict__ y, double *__restrict__ dU,
     double *__restrict__ U, int accumulate, unsigned *status) {
-    constexpr int NB = NV * NV, P = NVT_P;
+    constexpr int NB = NV * NV, P = nv_chunk<NV>();
     extern __shared__ __align__(128) unsigned char smem[];
     const int l = blockIdx.x;
     if (l >= nline) return;
