@@ -296,6 +296,15 @@ int tbs_profile_reset(tbs_ctx *ctx);
 int tbs_profile_read(tbs_ctx *ctx, int *n, const char **names,
                      long long *launches, double *ms);
 
+/* Self-test of the failure path of every staging wait: a kernel waits
+ * budget_cycles (clock64) on a copy barrier that nothing completes, gives
+ * up and records the timeout in the context's device status, which this
+ * call reads like any launch sequence: it returns TBS_ERR_CUDA ("a
+ * device-side wait ran out of its time budget") and leaves the context
+ * usable.  The kernels' own waits use a budget of 2^31 cycles (about one
+ * second).  No copy is issued, so nothing is left in flight. */
+int tbs_selftest_timeout(tbs_ctx *ctx, long long budget_cycles);
+
 /* Algorithmic bytes one launch of each kernel moves (reads + writes of
  * every array it must touch once), for the roofline numerator.  The
  * multi-RHS kernels take the group size as a suffix: "multi_thomas/8",

@@ -70,3 +70,24 @@ def test_block_size_support():
     assert e.value.code == N.TBS_ERR_UNSUPPORTED
     s.factor(ALGO_REFERENCE)
     s.close()
+
+
+def test_staging_wait_timeout_is_reported_and_recoverable():
+    """The bounded wait of every bulk-copy pipeline, made to run out on a
+    barrier that nothing completes (no copy is issued): the status comes
+    back as an error and the context keeps working."""
+    s = Solver(0)
+    try:
+        mesh = Mesh.structured(6, 8)
+        jac = Jacobian.generate(mesh, 9.0, 1)
+        s.set_mesh(mesh)
+        s.set_jacobian(jac)
+        s.factor(ALGO_FP64)
+        with pytest.raises(TbsError) as e:
+            N.check(N.lib.tbs_selftest_timeout(s.ctx, 1 << 20), s.ctx)  # ~0.5 ms budget
+        assert e.value.code == N.TBS_ERR_CUDA
+        assert "time budget" in str(e.value)
+        n, h = s.solve(1e-12, 100)
+        assert h[-1] <= 1e-12 * h[0]
+    finally:
+        s.close()

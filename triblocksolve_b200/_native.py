@@ -80,6 +80,7 @@ _sig("tbs_set_initial", _i, _vp, _dp)
 _sig("tbs_factor", _i, _vp, _i)
 _sig("tbs_sweep", _i, _vp, _i, _dp)
 _sig("tbs_solve", _i, _vp, C.c_double, _i, _ip, _dp)
+_sig("tbs_selftest_timeout", _i, _vp, C.c_longlong)
 _sig("tbs_gmres", _i, _vp, _i, _i, C.c_double, _i, _ip, _dp)
 _sig("tbs_solve_multi", _i, _vp, _i, _dp, _dp, C.c_double, _i, _ip, _dp, _i)
 _sig("tbs_solve_multi_device", _i, _vp, _i, _vp, _vp, C.c_double, _i, _ip, _dp, _i)

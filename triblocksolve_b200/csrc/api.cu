@@ -1241,6 +1241,17 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
     GUARD_END
 }
 
+int tbs_selftest_timeout(tbs_ctx *ctx, long long budget_cycles) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_status) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
+    if (budget_cycles < 0) return ctx_fail(ctx, TBS_ERR_ARG, "negative budget");
+    CKL(launch_selftest_timeout(ctx->stream, budget_cycles, ctx->d_status));
+    return status_check(ctx);
+    GUARD_END
+}
+
 int tbs_memory_allocated(const tbs_ctx *ctx, size_t *bytes) {
     if (!ctx || !bytes) return ctx_fail(nullptr, TBS_ERR_ARG, "null argument");
     *bytes = ctx->bytes + multi_bytes(ctx) + krylov_bytes(ctx);

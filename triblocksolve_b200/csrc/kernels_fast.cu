@@ -2863,4 +2863,25 @@ int pij_prepare(const FastLayout &L) {
     return set_smem((const void *)pij_sweep_kernel, resid_smem_bytes<double>(L.nxf));
 }
 
+
+/* =============================================== bounded-wait self-test
+ * One thread arms an mbarrier for 16 bytes that no copy will deliver (no
+ * copy is issued) and waits on it with the given clock budget, the wait
+ * every staging pipeline uses: it must give up, and the status bit it then
+ * records is the one the kernels record on a stalled copy. */
+__global__ void selftest_timeout_kernel(long long budget, unsigned *status) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    mbar_fence_init();
+    mbar_arrive_expect_tx(&bar, 16);
+    if (!mbar_wait(&bar, 0, budget)) atomicOr(status, ST_TIMEOUT);
+}
+
+int launch_selftest_timeout(cudaStream_t st, long long budget_cycles, unsigned *status) {
+    if (budget_cycles < 0) return (int)cudaErrorInvalidValue;
+    selftest_timeout_kernel<<<1, 32, 0, st>>>(budget_cycles, status);
+    return (int)cudaGetLastError();
+}
+
 }  // namespace tbs

@@ -234,6 +234,9 @@ int launch_nv_resid(cudaStream_t st, int nv, const FastLayout &L, int mode, cons
                     const double *X, const double *dU, const double *Rsrc, double *b,
                     const NormSink &ns, unsigned *status, double *Uacc);
 
+/* a staging wait that is made to run out: ST_TIMEOUT into *status */
+int launch_selftest_timeout(cudaStream_t st, long long budget_cycles, unsigned *status);
+
 /* point-implicit Jacobi (TBS_ALGO_PIJ): D^-1 in place of the
  * position-ordered diagonal blocks; one sweep = U += dU, R = sum over the
  * interior faces of XF dU_nbr, b = -Dinv R, with dU / b alternating between
