@@ -255,6 +255,57 @@ int tbs_solve_multi_device(tbs_ctx *ctx, int nrhs, const double *d_rhs,
 int tbs_gmres(tbs_ctx *ctx, int restart, int precond_sweeps, double rel_tol,
               int max_iters, int *iters_out, double *hist_out);
 
+/* ======================================================= line partitions
+ * One mesh split over several contexts (one per GPU, or several on one
+ * GPU), each owning a contiguous range of lines.  The reference solves a
+ * mesh on one device; this splits its sweep loop (src/main.cxx:207-229) at
+ * the one place where partitions need each other's data: the residual
+ * (triblock_lineRes, src/okl/linesmoothLU_TriBlock_v3.okl:228-336) reads
+ * the update of the neighbouring lines.
+ *
+ * tbs_set_partition_mesh: tbs_set_mesh for one partition.  The mesh holds
+ * the owned lines followed by nhalo_lines halo lines: whole copies of the
+ * lines of other partitions that hold a neighbour of an owned cell (their
+ * faces to cells outside this mesh dropped).  The owned lines' cells must
+ * be elements 0..nelem_own-1.  Halo lines are swept like the others, but
+ * no norm counts them; tbs_solve / tbs_sweep / multi-RHS / GMRES / batches
+ * refuse such a context (TBS_ERR_UNSUPPORTED): it sweeps as below.  Needs
+ * tbs_factor(TBS_ALGO_FP64), nvar 9.
+ *
+ * A solve from U = 0:
+ *   tbs_part_start(ctx, &n0)          ||R_0|| over the owned cells
+ *   repeat:
+ *     tbs_part_solve_du(ctx)          line solves, dU of every line
+ *     for each halo line h: copy dU of h from its owner into this context
+ *       (tbs_part_line_vector: owner to_line=0 into a device buffer, the
+ *        buffer to another GPU by NCCL or a peer copy, then to_line=1 here)
+ *     tbs_part_line_res(ctx, &n)      R from dU, U += dU, ||R|| over owned
+ *   the global norm is sqrt(sum over partitions of n^2).
+ * Owned cells' U and dU are bit-identical to a tbs_sweep of the whole mesh;
+ * a halo line's U is its owner's (it accumulates the copied dU).
+ * tbs_true_residual_norm, on such a context, covers the owned cells.
+ * owned_norm may be NULL in tbs_part_line_res: no host synchronisation,
+ * the norm stays in the context (read by the next call that returns one). */
+int tbs_set_partition_mesh(tbs_ctx *ctx, int nhalo_lines, int nvar, int nelem,
+                           int nintface, int eftot, int nline, int nlineelem,
+                           const int *epoint, const int *ef, const int *fc,
+                           const int *linesize, const int *linepoint,
+                           const int *lines, const int *lineface);
+int tbs_part_start(tbs_ctx *ctx, double *owned_norm);
+int tbs_part_solve_du(tbs_ctx *ctx);
+int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm);
+
+/* Copies line `line`'s part of the solution (TBS_VEC_SOLUTION) or of the
+ * last update (TBS_VEC_UPDATE) to (to_line = 0) or from (to_line = 1) the
+ * device buffer d_buf: linesize[line] * 9 doubles, in the line's internal
+ * cell order, which depends only on the line's length, so a buffer taken
+ * from a line's owner fits the same line's halo copy.  Asynchronous on the
+ * context's stream; d_buf may be any address the device can reach. */
+#define TBS_VEC_SOLUTION 0
+#define TBS_VEC_UPDATE   2
+int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
+                         int to_line);
+
 /* Jacobian::fromDevice (src/Jacobian.cxx:279-290) for the vectors, in the
  * element order of the input (9*nelem doubles each). */
 int tbs_get_solution(tbs_ctx *ctx, double *U);

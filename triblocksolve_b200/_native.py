@@ -35,6 +35,9 @@ ALGO_PIJ = 3
 
 CUDA_MODE = 2
 
+VEC_SOLUTION = 0  # TBS_VEC_SOLUTION
+VEC_UPDATE = 2    # TBS_VEC_UPDATE
+
 if not os.path.exists(LIB_PATH):
     raise ImportError(
         f"{LIB_PATH} is missing: build it with `make -C triblocksolve_b200/csrc` "
@@ -84,6 +87,11 @@ _sig("tbs_selftest_timeout", _i, _vp, C.c_longlong)
 _sig("tbs_gmres", _i, _vp, _i, _i, C.c_double, _i, _ip, _dp)
 _sig("tbs_solve_multi", _i, _vp, _i, _dp, _dp, C.c_double, _i, _ip, _dp, _i)
 _sig("tbs_solve_multi_device", _i, _vp, _i, _vp, _vp, C.c_double, _i, _ip, _dp, _i)
+_sig("tbs_set_partition_mesh", _i, _vp, _i, _i, _i, _i, _i, _i, _i, _ip, _ip, _ip, _ip, _ip, _ip, _ip)
+_sig("tbs_part_start", _i, _vp, _dp)
+_sig("tbs_part_solve_du", _i, _vp)
+_sig("tbs_part_line_res", _i, _vp, _dp)
+_sig("tbs_part_line_vector", _i, _vp, _i, _i, _vp, _i)
 _sig("tbs_get_solution", _i, _vp, _dp)
 _sig("tbs_get_residual", _i, _vp, _dp)
 _sig("tbs_get_update", _i, _vp, _dp)

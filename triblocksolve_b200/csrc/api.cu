@@ -230,7 +230,15 @@ static int build_layout(tbs_ctx *ctx) {
     const int *fc = ctx->h_fc.data(), *ep = ctx->h_epoint.data(), *ef = ctx->h_ef.data();
     std::vector<int> start(nline), len(nline), twist(nline);
     long long np = 0;
+    const int nown = nline - ctx->nhalo;
+    long long np_own = 0;
     for (int l = 0; l < nline; ++l) {
+        if (l == nown) {
+            /* halo lines start on a tile boundary: no residual tile mixes
+             * owned and halo cells, so the norm can stop at the owned tiles */
+            np = (np + RES_TILE - 1) / RES_TILE * RES_TILE;
+            np_own = np;
+        }
         start[l] = (int)np;
         len[l] = ls[l];
         twist[l] = line_twist_of(ls[l]);
@@ -336,6 +344,8 @@ static int build_layout(tbs_ctx *ctx) {
     L.nv = ctx->nvar;
     L.np = (int)np;
     L.np16 = np16;
+    L.ntile_own = (ctx->nhalo > 0 ? (int)np_own : np16) / RES_TILE;
+    ctx->h_line_start = start;
     L.nx = nx;
     L.nxf = nxf;
     L.nline = nline;
@@ -450,6 +460,7 @@ static NormSink sink(tbs_ctx *ctx, int is_start, CondCtl cc) {
     ns.is_start = is_start;
     ns.use_cond = cc.use_cond;
     ns.handle = cc.handle;
+    ns.ntiles = ctx->nhalo > 0 ? ctx->L.ntile_own : 0;
     return ns;
 }
 
@@ -898,19 +909,32 @@ int tbs_set_stream(tbs_ctx *ctx, void *cuda_stream) {
     return TBS_OK;
 }
 
-int tbs_set_mesh(tbs_ctx *ctx, int nvar, int nelem, int nintface, int eftot, int nline,
-                 int nlineelem, const int *epoint, const int *ef, const int *fc,
-                 const int *linesize, const int *linepoint, const int *lines,
-                 const int *lineface) {
-    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
-    GUARD_BEGIN
+/* tbs_set_mesh with the last nhalo lines marked as halo lines (0: none) */
+static int set_mesh(tbs_ctx *ctx, int nhalo, int nvar, int nelem, int nintface, int eftot,
+                    int nline, int nlineelem, const int *epoint, const int *ef, const int *fc,
+                    const int *linesize, const int *linepoint, const int *lines,
+                    const int *lineface) {
     CK(cudaSetDevice(ctx->device));
     int hdr[6] = {nvar, nelem, nintface, eftot, nline, nlineelem};
     int st = validate_mesh(hdr, epoint, ef, fc, linesize, linepoint, lines, lineface);
     if (st) return ctx_fail(ctx, st, thread_error());
     if (nvar > 32) return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "nvar > 32 is not supported");
+    int nelem_own = nelem;
+    if (nhalo > 0) {
+        if (nhalo >= nline)
+            return ctx_fail(ctx, TBS_ERR_ARG, "a line partition needs at least one owned line");
+        /* the owned lines' cells must be exactly elements 0..nelem_own-1 */
+        nelem_own = linepoint[nline - nhalo];
+        for (int k = 0; k < nelem_own; ++k)
+            if (lines[k] >= nelem_own)
+                return ctx_fail(ctx, TBS_ERR_FORMAT,
+                                "line partition: the owned lines' cells must be numbered before "
+                                "the halo lines' cells");
+    }
     CK(cudaStreamSynchronize(ctx->stream));
     drop_mesh(ctx);
+    ctx->nhalo = nhalo;
+    ctx->nelem_own = nelem_own;
     CK(cudaMalloc((void **)&ctx->d_status, sizeof(unsigned)));
     ctx->allocs.push_back({ctx->d_status, sizeof(unsigned)});
     CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
@@ -956,6 +980,28 @@ int tbs_set_mesh(tbs_ctx *ctx, int nvar, int nelem, int nintface, int eftot, int
     if (rc) return rc;
     ctx->have_mesh = true;
     return TBS_OK;
+}
+
+int tbs_set_mesh(tbs_ctx *ctx, int nvar, int nelem, int nintface, int eftot, int nline,
+                 int nlineelem, const int *epoint, const int *ef, const int *fc,
+                 const int *linesize, const int *linepoint, const int *lines,
+                 const int *lineface) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    return set_mesh(ctx, 0, nvar, nelem, nintface, eftot, nline, nlineelem, epoint, ef, fc,
+                    linesize, linepoint, lines, lineface);
+    GUARD_END
+}
+
+int tbs_set_partition_mesh(tbs_ctx *ctx, int nhalo_lines, int nvar, int nelem, int nintface,
+                           int eftot, int nline, int nlineelem, const int *epoint, const int *ef,
+                           const int *fc, const int *linesize, const int *linepoint,
+                           const int *lines, const int *lineface) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    if (nhalo_lines < 0) return ctx_fail(ctx, TBS_ERR_ARG, "negative halo line count");
+    GUARD_BEGIN
+    return set_mesh(ctx, nhalo_lines, nvar, nelem, nintface, eftot, nline, nlineelem, epoint, ef,
+                    fc, linesize, linepoint, lines, lineface);
     GUARD_END
 }
 
@@ -1073,6 +1119,7 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
     CK(cudaSetDevice(ctx->device));
     if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
     if (n < 0) return ctx_fail(ctx, TBS_ERR_ARG, "negative sweep count");
+    if (ctx->nhalo > 0) return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "a line partition sweeps with tbs_part_solve_du / tbs_part_line_res");
     int rc = ctx_ensure_hist(ctx, n + 1);
     if (rc) return rc;
     rc = ctx_set_state(ctx, 0.0, n);
@@ -1099,6 +1146,7 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
     CK(cudaSetDevice(ctx->device));
     if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
     if (max_sweeps < 0 || !(rel_tol >= 0.0)) return ctx_fail(ctx, TBS_ERR_ARG, "bad tolerance or sweep limit");
+    if (ctx->nhalo > 0) return ctx_fail(ctx, TBS_ERR_UNSUPPORTED, "a line partition sweeps with tbs_part_solve_du / tbs_part_line_res");
     int rc = ctx_ensure_hist(ctx, max_sweeps + 1);
     if (rc) return rc;
     rc = ctx_set_state(ctx, rel_tol, max_sweeps);
@@ -1219,14 +1267,16 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
         int rc = get_vec(ctx, 1, R.data());
         if (rc) return rc;
         double s = 0.0;
-        for (double v : R) s += v * v;
+        for (size_t k = 0; k < (size_t)ctx->nelem_own * ctx->nvar; ++k) s += R[k] * R[k];
         *out = std::sqrt(s);
         return TBS_OK;
     }
     cudaStream_t st = ctx->stream;
-    const int nb = full_resid_blocks(ctx->nelem);
+    /* a line partition: the owned cells (elements 0..nelem_own-1); their
+     * neighbours in halo lines are read from the halo copies of U */
+    const int nb = full_resid_blocks(ctx->nelem_own);
     const bool ref = ctx->algo == TBS_ALGO_REFERENCE;
-    RUN("full_resid", launch_full_resid<double>(st, ctx->nelem, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+    RUN("full_resid", launch_full_resid<double>(st, ctx->nelem_own, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                 ref ? ctx->d_identity : ctx->L.pos_of_elem,
                                                 ctx->d_jacD, ctx->d_O1, ctx->d_O2, ctx->d_rhs,
                                                 ref ? ctx->d_U : ctx->d_Up,
@@ -1434,6 +1484,96 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     if (b < 0) return ctx_fail(ctx, TBS_ERR_ARG, "unknown kernel name " + k);
     *bytes = b;
     return TBS_OK;
+}
+
+/* ======================================================= line partitions
+ * One mesh split into contiguous line ranges, one context per range; each
+ * context's mesh ends in halo lines (copies of the neighbouring partitions'
+ * boundary lines).  A sweep is split where the halo update goes:
+ *   tbs_part_solve_du   line solves of every line (halo lines included)
+ *   -- the caller copies each halo line's dU from the line's owner --
+ *   tbs_part_line_res   residual from dU, U += dU, norm over the owned lines
+ * The per-position arithmetic is that of tbs_sweep on the whole mesh. */
+
+static int part_check(tbs_ctx *ctx) {
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (ctx->algo != TBS_ALGO_FP64 || ctx->nvar != 9)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
+                        "line-partition sweeps need TBS_ALGO_FP64 with nvar == 9");
+    return TBS_OK;
+}
+
+/* the norm that the last residual launch recorded (owned lines only) */
+static int part_norm(tbs_ctx *ctx, double *out) {
+    int rc = read_state(ctx);
+    if (rc) return rc;
+    rc = status_check(ctx);
+    if (rc) return rc;
+    if (out) *out = ctx->h_state->last;
+    return TBS_OK;
+}
+
+int tbs_part_start(tbs_ctx *ctx, double *owned_norm) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    rc = ctx_ensure_hist(ctx, 1);
+    if (rc) return rc;
+    rc = ctx_set_state(ctx, 0.0, 0x7fffffff);
+    if (rc) return rc;
+    rc = prime(ctx, CondCtl{});
+    if (rc) return rc;
+    return part_norm(ctx, owned_norm);
+    GUARD_END
+}
+
+int tbs_part_solve_du(tbs_ctx *ctx) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, 2));
+    return TBS_OK;
+    GUARD_END
+}
+
+int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, CondCtl{}),
+                              ctx->d_Up));
+    if (!owned_norm) return TBS_OK;
+    rc = part_norm(ctx, owned_norm);
+    if (ctx->prof) prof_resolve(ctx);
+    return rc;
+    GUARD_END
+}
+
+int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf, int to_line) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    if (which != TBS_VEC_SOLUTION && which != TBS_VEC_UPDATE)
+        return ctx_fail(ctx, TBS_ERR_ARG, "which must be TBS_VEC_SOLUTION or TBS_VEC_UPDATE");
+    if (line < 0 || line >= ctx->nline) return ctx_fail(ctx, TBS_ERR_ARG, "line out of range");
+    if (!d_buf) return ctx_fail(ctx, TBS_ERR_ARG, "null buffer");
+    double *v = (which == TBS_VEC_SOLUTION ? ctx->d_Up : ctx->d_dUp) +
+                (size_t)ctx->h_line_start[line] * 9;
+    const size_t bytes = (size_t)ctx->h_linesize[line] * 9 * sizeof(double);
+    if (to_line)
+        CK(cudaMemcpyAsync(v, d_buf, bytes, cudaMemcpyDefault, ctx->stream));
+    else
+        CK(cudaMemcpyAsync(d_buf, v, bytes, cudaMemcpyDefault, ctx->stream));
+    return TBS_OK;
+    GUARD_END
 }
 
 }  // extern "C"

@@ -913,6 +913,9 @@ static int batch_check_members(tbs_batch *b) {
         tbs_ctx *c = b->sys[s];
         if (!c->factored || !c->layout_ok)
             return bfail(b, TBS_ERR_STATE, "batch member " + std::to_string(s) + " is not factored");
+        if (c->nhalo > 0)
+            return bfail(b, TBS_ERR_UNSUPPORTED,
+                         "batch member " + std::to_string(s) + " is a line partition of a larger mesh");
         if (c->algo != b->eng.algo)
             return bfail(b, TBS_ERR_STATE,
                          "batch member " + std::to_string(s) + " was re-factored with another algorithm");

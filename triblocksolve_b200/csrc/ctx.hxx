@@ -39,6 +39,11 @@ struct tbs_ctx {
     bool have_mesh = false, have_jac = false, factored = false;
     int nvar = 0, nelem = 0, nintface = 0, eftot = 0, nline = 0, nlineelem = 0, max_line = 0;
     std::vector<int> h_epoint, h_ef, h_fc, h_linesize, h_linepoint, h_lines, h_lineface;
+    /* line partition of a larger mesh: the last nhalo lines are copies of
+     * lines another partition owns (swept, never counted in a norm); the
+     * owned lines' cells are elements 0..nelem_own-1 */
+    int nhalo = 0, nelem_own = 0;
+    std::vector<int> h_line_start; /* first position of every line */
     int *d_epoint = nullptr, *d_ef = nullptr, *d_fc = nullptr, *d_linesize = nullptr;
     int *d_linepoint = nullptr, *d_lines = nullptr, *d_lineface = nullptr, *d_identity = nullptr;
 

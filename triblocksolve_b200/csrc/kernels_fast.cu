@@ -738,7 +738,8 @@ __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T 
         if (!ok) break;
         __syncthreads(); /* the next tile's copies overwrite the stages */
     }
-    return finalize_total(ns, ntiles);
+    /* a line partition's norm covers its owned lines, which come first */
+    return finalize_total(ns, (ns.ntiles > 0 && ns.ntiles < ntiles) ? ns.ntiles : ntiles);
 }
 
 /* mode 1 (R = sum X dU over the cross-line slots) */

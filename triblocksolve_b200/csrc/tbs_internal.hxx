@@ -91,6 +91,7 @@ struct FastLayout {
     int nv;        /* block size (9) */
     int np;        /* positions incl. line pads */
     int np16;      /* np rounded up to RES_TILE */
+    int ntile_own; /* tiles of the owned lines (all tiles unless the mesh ends in halo lines) */
     int nx;        /* cross-line coupling slots per position */
     int nline;
     int max_len;   /* longest line */
@@ -169,6 +170,8 @@ struct NormSink {
     int is_start;
     int use_cond;
     unsigned long long handle;   /* cudaGraphConditionalHandle */
+    int ntiles;                  /* > 0: the norm sums the first ntiles tiles only (the
+                                  * owned lines of a line partition); 0: every tile */
 };
 
 /* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
