@@ -795,6 +795,156 @@ def run_multi(args, L, K, shift, tol):
     return 0
 
 
+def run_partition(args, L, K, shift, tol):
+    """--partition: ONE mesh of the config split into N contiguous line
+    ranges, one per rank (strong scaling).  Each sweep: line solves, the
+    halo lines' dU exchanged with the neighbouring ranks (NCCL send/recv of
+    one line of 9 doubles per cell per boundary), residual, all-reduce of
+    the owned norms.  value = sweeps of the whole mesh per second; e2e adds
+    the partition's Jacobian upload, factorization and the owned solution's
+    read-back to every step.  At N = 1 the mesh is one partition without
+    halo lines: the host-driven sweep loop beside the graph-launched solve."""
+    import torch
+
+    import triblocksolve_b200 as tbs
+    from triblocksolve_b200 import _native as N
+    from triblocksolve_b200.partition import (DistExchange, PartitionedSolve, PartitionSolver,
+                                              partition_lines)
+    ws, rank, local = dist_env()
+    torch.cuda.set_device(local)
+    dist = Dist(ws, rank, local, "nccl")
+    mesh, whole = build_problem(L, K, shift, pinned=False)
+    parts = partition_lines(mesh, ws)
+    part = parts[rank]
+    host = {}
+    for k, a in zip(("jacD", "jacO1", "jacO2", "rhs"),
+                    part.sub_arrays(whole["jacD"], whole["jacO1"], whole["jacO2"], whole["rhs"])):
+        host[k] = torch.empty(a.size, dtype=torch.float64, pin_memory=True).numpy()
+        host[k][:] = a
+    del whole
+    stream = torch.cuda.Stream(device=local)
+    torch.cuda.set_stream(stream)
+    solver = PartitionSolver(part, local)
+    solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+    solver.factor(tbs.ALGO_FP64)
+    ex = DistExchange(part, solver, device=f"cuda:{local}", group=None) if ws > 1 else None
+
+    class _Single:  # one partition, nothing to exchange
+        def exchange(self, which):
+            pass
+
+        def allreduce_sum(self, x):
+            return x
+
+    run = PartitionedSolve([solver], ex if ex else _Single())
+    max_sweeps = 400
+    Uh = torch.empty(9 * part.mesh.nelem, dtype=torch.float64, pin_memory=True).numpy()
+    with ClockSampler(local) as clocks:
+        for _ in range(max(args.warmup, 0)):
+            run.solve(tol, max_sweeps)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        sweeps_total = 0
+        hist = None
+        for _ in range(args.steps):
+            n, hist = run.solve(tol, max_sweeps)
+            sweeps_total += n
+        t1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        elapsed_ms = t0.elapsed_time(t1)
+        solver.profile(True)
+        solver.profile_reset()
+        nprof = max(1, min(args.steps, 10))
+        for _ in range(nprof):
+            run.solve(tol, max_sweeps)
+        prof = solver.profile_read()
+        solver.profile(False)
+        ne2e = args.e2e_steps if args.e2e_steps is not None else max(1, min(args.steps, 10))
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        e2e_sweeps = 0
+        for _ in range(ne2e):
+            solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
+            solver.factor(tbs.ALGO_FP64)
+            n, _h = run.solve(tol, max_sweeps)
+            Uh[:] = solver.solution()
+            e2e_sweeps += n
+        e1.record(stream)
+        torch.cuda.synchronize()
+        dist.barrier()
+        torch.cuda.synchronize()
+        e2e_ms = e0.elapsed_time(e1)
+    clk = clocks.summary()
+    tn = solver.true_residual_norm()
+    true_rel = float(np.sqrt(dist.reduce(tn * tn, "sum"))) / float(hist[0])
+    max_ms = dist.reduce(elapsed_ms, "max")
+    max_e2e_ms = dist.reduce(e2e_ms, "max")
+    if rank == 0:
+        peak, peak_kind = measured_peak_hbm()
+        kern = {}
+        for name, (launches, ms) in prof.items():
+            try:
+                b = solver.kernel_bytes(name)
+            except Exception:
+                b = None
+            avg_us = 1e3 * ms / launches if launches else 0.0
+            kern[name] = {"launches": launches, "total_ms": round(ms, 4), "avg_us": round(avg_us, 3),
+                          "bytes_per_launch": b,
+                          "gbs": round(b / (avg_us * 1e-6) / 1e9, 1) if b and avg_us > 0 else None}
+        hot = [k for k in kern if kern[k]["bytes_per_launch"] and k != "fast_resid_rhs"]
+        dom = max(hot, key=lambda k: kern[k]["total_ms"]) if hot else None
+        roof = None
+        if dom:
+            ach = kern[dom]["gbs"]
+            roof = {"bound": "hbm", "kernel": dom, "achieved": ach, "peak": peak, "unit": "GB/s",
+                    "frac": round(ach / peak, 4), "traffic": None,
+                    "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)",
+                    "algorithmic_bytes_per_launch": kern[dom]["bytes_per_launch"],
+                    "avg_launch_us": kern[dom]["avg_us"], "rank": 0}
+        halo_bytes = sum(8 * 9 * int(part.mesh.linesize[k]) for ks in part.recvs.values() for k in ks)
+        line = {
+            "metric": "LIJ sweeps/s", "value": round(sweeps_total / (max_ms * 1e-3), 2),
+            "unit": "sweeps/s (of the whole mesh)", "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": round(max_ms / args.steps, 5),
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured mesh and values (shift %g, seed %d)" % (shift, SEED),
+            "config": {
+                "workload": f"one LIJ system of {L} lines x {K} cells ({mesh.nelem} cells) split "
+                            f"into {ws} line partitions, solved to {tol:g} from U=0, FP64",
+                "cells": mesh.nelem, "tol": tol, "partitions": ws,
+                "owned_lines_rank0": part.nowned, "halo_lines_rank0": part.nhalo,
+                "halo_bytes_per_sweep_rank0": halo_bytes,
+                "sweeps_per_solve": sweeps_total / args.steps, "true_rel_residual": true_rel,
+                "l2": "no flush: every sweep streams the line blocks (> 126 MB L2)",
+                "parallelism": f"line partitions of one mesh over {ws} GPUs, NCCL halo exchange"
+                               if ws > 1 else "1 GPU, one partition (host-driven sweep loop)",
+            },
+            "roofline": roof, "kernels": kern,
+            "e2e": {"value": round(e2e_sweeps / (max_e2e_ms * 1e-3), 2),
+                    "unit": "sweeps/s (of the whole mesh)",
+                    "h2d_bytes_per_step": int(sum(a.nbytes for a in host.values())),
+                    "d2h_bytes_per_step": int(Uh.nbytes), "steps": ne2e,
+                    "what": "per step on every rank: tbs_set_jacobian of the partition from "
+                            "pinned host memory, tbs_factor, the partitioned solve, "
+                            "tbs_get_solution (rank 0's bytes)"},
+            "gpu_launches": int(round(sum(v["launches"] for v in kern.values()) / nprof * args.steps)),
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    del ex
+    solver.close()
+    dist.close()
+    return 0
+
+
 def run_gmres(args, L, K, shift, tol):
     """--gmres M: restarted GMRES(M) on the system, right preconditioned by
     one LIJ sweep (tbs_gmres, FP64 line factors), to the config's tolerance
@@ -975,6 +1125,8 @@ def main():
                     help="restart length: time line-preconditioned GMRES instead of the sweep loop")
     ap.add_argument("--nrhs", type=int, default=1,
                     help="right-hand sides per solve (> 1: tbs_solve_multi, FP64)")
+    ap.add_argument("--partition", action="store_true",
+                    help="one mesh split into line partitions over the ranks (strong scaling)")
     args = ap.parse_args()
     if args.config in SERVE_CONFIGS:
         if args.impl == "reference":
@@ -987,6 +1139,10 @@ def main():
     L, K, shift, tol = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, L, K, shift, tol)
+    if args.partition:
+        if args.algo != "fp64" or args.nvar != 9 or args.nrhs > 1 or args.gmres:
+            ap.error("--partition runs the FP64 sweep at nvar 9")
+        return run_partition(args, L, K, shift, tol)
     if args.gmres > 0:
         return run_gmres(args, L, K, shift, tol)
     if args.nrhs > 1:
