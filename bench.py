@@ -825,6 +825,7 @@ def run_partition(args, L, K, shift, tol):
     stream = torch.cuda.Stream(device=local)
     torch.cuda.set_stream(stream)
     solver = PartitionSolver(part, local)
+    solver.set_stream(stream.cuda_stream)  # the stream the CUDA events below are recorded on
     solver.set_jacobian_arrays(host["jacD"], host["jacO1"], host["jacO2"], host["rhs"])
     solver.factor(tbs.ALGO_FP64)
     ex = DistExchange(part, solver, device=f"cuda:{local}", group=None) if ws > 1 else None
