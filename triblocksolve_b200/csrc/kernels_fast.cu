@@ -1038,15 +1038,26 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
  * `pbase` is the parity with which barrier s completes its next phase.
  * Returns false when a staging wait ran out of time; the status bit is
  * then set and the copies in flight have landed. */
-template <typename T, int P, bool YS>
+/* bytes before the first staging buffer: the barriers (and, in the
+ * warp-specialised form, the producer's counters) */
+template <bool WS>
+__host__ __device__ constexpr int thomas_hdr() { return WS ? 256 : 128; }
+
+template <typename T, int P, bool YS, bool WS = false>
 __device__ __forceinline__ bool thomas_line(
     int NS, int accumulate, int ps, int n, int m, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
     T *__restrict__ U, unsigned *status, unsigned char *smem, uint32_t &pbase, uint64_t pol) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    /* WS (warp-specialised CTA of two warps): bars[0..NS) complete when a
+     * stage's copies have landed, bars[8..8+NS) when warp 0 has consumed
+     * it; warp 1 lane 0 issues the copies, warp 0 runs the chains */
+    uint64_t *empty = bars + 8;
+    volatile int *ws_issued = reinterpret_cast<volatile int *>(smem + 128);
+    volatile int *ws_abort = ws_issued + 1;
     const uint32_t stage = 2 * P * (NB + NV) * sizeof(T);
     const uint32_t half = P * (NB + NV) * sizeof(T);
-    unsigned char *st0 = smem + 128;
+    unsigned char *st0 = smem + thomas_hdr<WS>();
     /* broadcast: 2 halves x 2 alternating buffers x [copy A: 10][copy B: 10] */
     T *bcall = reinterpret_cast<T *>(st0 + (size_t)NS * stage);
     T *ys = bcall + 80;
@@ -1068,8 +1079,10 @@ __device__ __forceinline__ bool thomas_line(
     T *Ul = U ? U + (size_t)ps * NV : nullptr;
     auto parity = [&](int job) { return ((pbase >> (job % NS)) ^ (uint32_t)(job / NS)) & 1u; };
 
+    const bool producer = WS && (threadIdx.x >> 5) == 1;
     __syncwarp(); /* the previous line's readers of the stages are done */
-    for (int t = lane; t < 80; t += 32) bcall[t] = T(0);
+    if (!producer)
+        for (int t = lane; t < 80; t += 32) bcall[t] = T(0);
     __syncwarp();
 
     /* copy size of chunk c of a chain of length ln, rounded up to 4 cells
@@ -1106,8 +1119,26 @@ __device__ __forceinline__ bool thomas_line(
             }
         }
     };
+    if (producer) {
+        /* every job as soon as the consumer has released its stage */
+        if (lane == 0) {
+            for (int job = 0; job < njobs; ++job) {
+                if (*ws_abort) break;
+                const int s = job % NS;
+                if (job >= NS && !mbar_wait(&empty[s], (uint32_t)((job / NS - 1) & 1))) {
+                    atomicOr(status, ST_TIMEOUT);
+                    break;
+                }
+                issue(job, s);
+                *ws_issued = job + 1;
+            }
+        }
+        __syncwarp();
+        __syncthreads(); /* meets the consumer's */
+        return true;
+    }
     int issued = 0;
-    if (lane == 0) {
+    if (!WS && lane == 0) {
         for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
     }
     int consumed = 0;
@@ -1130,7 +1161,9 @@ __device__ __forceinline__ bool thomas_line(
         else
             fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, writer, off);
         __syncwarp();
-        if (lane == 0 && issued < njobs) {
+        if (WS) {
+            if (lane == 0) mbar_arrive(&empty[s]);
+        } else if (lane == 0 && issued < njobs) {
             issue(issued, s);
             ++issued;
         }
@@ -1202,7 +1235,9 @@ __device__ __forceinline__ bool thomas_line(
                 bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
                                           c * P, len, cpos, i, writer, off);
             __syncwarp();
-            if (lane == 0 && issued < njobs) {
+            if (WS) {
+                if (lane == 0) mbar_arrive(&empty[s]);
+            } else if (lane == 0 && issued < njobs) {
                 issue(issued, s);
                 ++issued;
             }
@@ -1239,6 +1274,14 @@ __device__ __forceinline__ bool thomas_line(
         }
     }
     if (timed_out) {
+        if (WS) {
+            /* stop the producer (its own waits are bounded), then wait for
+             * the copies it issued */
+            if (lane == 0) *ws_abort = 1;
+            __syncwarp();
+            __syncthreads();
+            issued = *ws_issued;
+        }
         if (lane == 0) {
             atomicOr(status, ST_TIMEOUT);
             for (int job = consumed; job < issued; ++job)
@@ -1247,6 +1290,7 @@ __device__ __forceinline__ bool thomas_line(
         __syncwarp();
         return false;
     }
+    if (WS) __syncthreads(); /* meets the producer's */
     /* every job was waited for: barrier s completed one phase per job
      * j = s, s+NS, ... below njobs */
     for (int s = 0; s < NS && s < njobs; ++s) {
@@ -1280,6 +1324,37 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     uint32_t pbase = 0;
     thomas_line<T, P, YS>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam, b, y,
                           dU, U, status, smem, pbase, pol);
+}
+
+/* Warp-specialised form, one CTA of two warps per line: warp 1 issues the
+ * staging copies, warp 0 runs the chains with the same arithmetic as
+ * fast_thomas_kernel, so its results are bit-identical; the chain warp no
+ * longer stops every chunk to issue the next copies. */
+template <typename T, int P, bool YS>
+__global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
+    int nline, int NS, int accumulate, const int *__restrict__ line_start,
+    const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
+    const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
+    T *__restrict__ U, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    const int l = blockIdx.x;
+    if (l >= nline) return;
+    if (threadIdx.x == 0) {
+        uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&bars[s], 1);
+            mbar_init(&bars[8 + s], 1);
+        }
+        int *cnt = reinterpret_cast<int *>(smem + 128);
+        cnt[0] = 0;
+        cnt[1] = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const uint64_t pol = threadIdx.x == 32 ? policy_evict_first() : 0;
+    uint32_t pbase = 0;
+    thomas_line<T, P, YS, true>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam,
+                                b, y, dU, U, status, smem, pbase, pol);
 }
 
 /* Persistent form over many systems: each CTA (one warp) takes (system,
@@ -1328,7 +1403,7 @@ struct ThomasCfg {
     size_t smem;
 };
 
-template <typename T>
+template <typename T, bool WS = false>
 static ThomasCfg thomas_cfg(const FastLayout &L) {
     const size_t sb = thomas_stage_bytes<T>();
     /* lines resident per SM in one wave, and the shared memory each may use
@@ -1344,7 +1419,7 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
     const int per_sm = (L.nline + nsm - 1) / nsm;
     const long long budget = (long long)smem_sm / (per_sm > 0 ? per_sm : 1) - reserved;
     const size_t ys_bytes = (size_t)((L.max_len + 3) & ~3) * NV * sizeof(T);
-    const size_t fixed = 128 + 80 * sizeof(T);
+    const size_t fixed = thomas_hdr<WS>() + 80 * sizeof(T);
     ThomasCfg c;
     c.ys = (long long)(fixed + ys_bytes + 3 * sb) <= budget;
     long long left = budget - (long long)fixed - (c.ys ? (long long)ys_bytes : 0);
@@ -1356,17 +1431,50 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
     return c;
 }
 
+/* Which single-system line solve: the warp-specialised kernel (a copy
+ * warp beside each chain warp) where few lines share an SM -- there the
+ * launch is bound by the chain's step latency, and taking the copy issue
+ * off the chain warp shortens every step (360 lines: 64 -> 51 us); the
+ * one-warp kernel where many lines share an SM, whose warps hide each
+ * other's latency and which holds more lines per SM in its registers
+ * (1,200 lines: 409 us one-warp, 526 us warp-specialised).  The
+ * environment variable TBS_THOMAS_WS=0 / 1 forces one or the other. */
+static bool thomas_ws(const FastLayout &L) {
+    static const int forced = [] {
+        const char *e = getenv("TBS_THOMAS_WS");
+        return e && e[0] ? (e[0] == '0' ? 0 : 1) : -1;
+    }();
+    if (forced >= 0) return forced == 1;
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (nsm < 1) nsm = 148;
+    return (L.nline + nsm - 1) / nsm <= 4;
+}
+
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
                        T *y, T *dU, T *U, unsigned *status, int accumulate) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    const ThomasCfg cfg = thomas_cfg<T>(L);
+    if (!thomas_ws(L)) {
+        const ThomasCfg c1 = thomas_cfg<T>(L);
+        if (c1.ys)
+            fast_thomas_kernel<T, THOMAS_P, true><<<L.nline, 32, c1.smem, st>>>(
+                L.nline, c1.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y,
+                dU, U, status);
+        else
+            fast_thomas_kernel<T, THOMAS_P, false><<<L.nline, 32, c1.smem, st>>>(
+                L.nline, c1.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y,
+                dU, U, status);
+        return (int)cudaGetLastError();
+    }
+    const ThomasCfg cfg = thomas_cfg<T, true>(L);
     if (cfg.ys)
-        fast_thomas_kernel<T, THOMAS_P, true><<<L.nline, 32, cfg.smem, st>>>(
+        fast_thomas_ws_kernel<T, THOMAS_P, true><<<L.nline, 64, cfg.smem, st>>>(
             L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
             U, status);
     else
-        fast_thomas_kernel<T, THOMAS_P, false><<<L.nline, 32, cfg.smem, st>>>(
+        fast_thomas_ws_kernel<T, THOMAS_P, false><<<L.nline, 64, cfg.smem, st>>>(
             L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
             U, status);
     return (int)cudaGetLastError();
@@ -1409,6 +1517,15 @@ int fast_prepare(const FastLayout &L) {
         rc = set_smem(c32.ys ? (const void *)fast_thomas_kernel<float, THOMAS_P, true>
                              : (const void *)fast_thomas_kernel<float, THOMAS_P, false>,
                       c32.smem);
+    const ThomasCfg w64 = thomas_cfg<double, true>(L), w32 = thomas_cfg<float, true>(L);
+    if (!rc)
+        rc = set_smem(w64.ys ? (const void *)fast_thomas_ws_kernel<double, THOMAS_P, true>
+                             : (const void *)fast_thomas_ws_kernel<double, THOMAS_P, false>,
+                      w64.smem);
+    if (!rc)
+        rc = set_smem(w32.ys ? (const void *)fast_thomas_ws_kernel<float, THOMAS_P, true>
+                             : (const void *)fast_thomas_ws_kernel<float, THOMAS_P, false>,
+                      w32.smem);
     return rc;
 }
 

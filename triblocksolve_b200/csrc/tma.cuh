@@ -47,6 +47,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
     return ok != 0;
 }
 
+/* plain arrival (count 1) on `bar` */
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 /* Wait for phase `parity` of `bar` to complete; false after ~budget cycles. */
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity,
                                           long long budget = (1LL << 31)) {
