@@ -1439,7 +1439,7 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
  * other's latency and which holds more lines per SM in its registers
  * (1,200 lines: 409 us one-warp, 526 us warp-specialised).  The
  * environment variable TBS_THOMAS_WS=0 / 1 forces one or the other. */
-static bool thomas_ws(const FastLayout &L) {
+static bool thomas_ws(const FastLayout &L, int max_per_sm = 4) {
     static const int forced = [] {
         const char *e = getenv("TBS_THOMAS_WS");
         return e && e[0] ? (e[0] == '0' ? 0 : 1) : -1;
@@ -1449,7 +1449,7 @@ static bool thomas_ws(const FastLayout &L) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm < 1) nsm = 148;
-    return (L.nline + nsm - 1) / nsm <= 4;
+    return (L.nline + nsm - 1) / nsm <= max_per_sm;
 }
 
 template <typename T>
@@ -2337,9 +2337,15 @@ __device__ __forceinline__ void bwd_chunk_m(const double *sG, double *const *bc,
  * forward stage holds, for either chain, a chunk of G rows followed by the
  * chunks of b of the active right-hand sides, a backward stage a chunk of
  * Gam rows.  All warps have consumed a stage before it is refilled (one
- * CTA barrier per chunk). */
-template <int P>
-__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kernel(
+ * CTA barrier per chunk).
+ * WS: one more warp (the last) issues the copies; the chain warps wait only
+ * for their stage's copies and release it on a second mbarrier per stage
+ * (count: the chain warps), with no CTA barrier per chunk.  The chain
+ * arithmetic is the same, so the results are bit-identical.  Three such
+ * CTAs (five warps each) fit an SM's registers: the launch is meant for
+ * meshes with at most 4 lines per SM. */
+template <int P, bool WS>
+__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW + (WS ? 32 : 0), WS ? 3 : 1) multi_thomas_kernel(
     int nline, int NS, int nr, long long vs, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist,
     const double *__restrict__ G, const double *__restrict__ Gam, const double *__restrict__ b,
@@ -2349,10 +2355,14 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned amask_s;
     __shared__ int rid[MULTI_MAX];
+    __shared__ int ws_issued, ws_abort;
     const int l = blockIdx.x;
     if (l >= nline) return;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int nw = (int)(blockDim.x >> 5) - (WS ? 1 : 0); /* chain warps */
+    const bool producer = WS && w == nw;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+    uint64_t *empty = bars + 8;
     if (tid == 0) {
         unsigned am = 0;
         int k = 0;
@@ -2362,7 +2372,12 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
                 rid[k++] = r;
             }
         amask_s = am;
-        for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&bars[s], 1);
+            if (WS) mbar_init(&empty[s], (uint32_t)nw);
+        }
+        ws_issued = 0;
+        ws_abort = 0;
         mbar_fence_init();
     }
     __syncthreads();
@@ -2403,8 +2418,9 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
         dUl[j] = dU + ro + (size_t)ps * NV;
         bg[j] = b + ro + (size_t)ps * NV;
     }
-    const uint64_t pol = tid == 0 ? policy_evict_first() : 0;
-    for (int t = lane; t < MULTI_RPW * 80; t += 32) bcw[t] = T(0);
+    const uint64_t pol = tid == (WS ? 32 * nw : 0) ? policy_evict_first() : 0;
+    if (!producer)
+        for (int t = lane; t < MULTI_RPW * 80; t += 32) bcw[t] = T(0);
     __syncwarp();
 
     auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
@@ -2441,8 +2457,25 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
             }
         }
     };
+    if (producer) {
+        if (lane == 0) {
+            for (int job = 0; job < njobs; ++job) {
+                if (*(volatile int *)&ws_abort) break;
+                const int s = job % NS;
+                if (job >= NS && !mbar_wait(&empty[s], (uint32_t)((job / NS - 1) & 1))) {
+                    atomicOr(status, ST_TIMEOUT);
+                    break;
+                }
+                issue(job, s);
+                *(volatile int *)&ws_issued = job + 1;
+            }
+        }
+        __syncwarp();
+        __syncthreads(); /* meets the chain warps' */
+        return;
+    }
     int issued = 0;
-    if (tid == 0) {
+    if (!WS && tid == 0) {
         for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
     }
     int consumed = 0;
@@ -2453,6 +2486,10 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     for (int c = 0; c < nf; ++c) {
         const int s = c % NS;
         const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(c / NS) & 1u));
+        if (WS && !ok) {
+            timed_out = true;
+            break;
+        }
         if (ok && mine) {
             const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
             const T *sB[MULTI_RPW];
@@ -2463,6 +2500,11 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
             else
                 fwd_chunk_m<P, true>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
             __syncwarp();
+        }
+        if (WS) {
+            ++consumed;
+            if (lane == 0) mbar_arrive(&empty[s]);
+            continue;
         }
         if (__syncthreads_or(!ok)) {
             timed_out = true;
@@ -2531,6 +2573,10 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
             load_chunk(c - 1, nyv);
             const int s = job % NS;
             const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(job / NS) & 1u));
+            if (WS && !ok) {
+                timed_out = true;
+                break;
+            }
             if (ok && mine) {
                 const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
                 const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
@@ -2541,20 +2587,38 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
                     bwd_chunk_m<P, true>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
                 __syncwarp();
             }
-            if (__syncthreads_or(!ok)) {
-                timed_out = true;
-                break;
-            }
-            ++consumed;
-            if (tid == 0 && issued < njobs) {
-                issue(issued, s);
-                ++issued;
+            if (WS) {
+                ++consumed;
+                if (lane == 0) mbar_arrive(&empty[s]);
+            } else {
+                if (__syncthreads_or(!ok)) {
+                    timed_out = true;
+                    break;
+                }
+                ++consumed;
+                if (tid == 0 && issued < njobs) {
+                    issue(issued, s);
+                    ++issued;
+                }
             }
 #pragma unroll
             for (int j = 0; j < MULTI_RPW; ++j)
 #pragma unroll
                 for (int q = 0; q < P; ++q) yv[j][q] = nyv[j][q];
         }
+    }
+    if (WS) {
+        /* a chain warp that ran out of time stops the copy warp (whose own
+         * waits are bounded); then the copies in flight land */
+        if (timed_out && lane == 0) *(volatile int *)&ws_abort = 1;
+        __syncthreads(); /* meets the copy warp's */
+        if (tid == 0 && *(volatile int *)&ws_abort) {
+            atomicOr(status, ST_TIMEOUT);
+            const int last = *(volatile int *)&ws_issued;
+            for (int job = last > NS ? last - NS : 0; job < last; ++job)
+                mbar_wait(&bars[job % NS], (uint32_t)(job / NS) & 1u, 1LL << 28);
+        }
+        return;
     }
     if (timed_out && tid == 0) {
         atomicOr(status, ST_TIMEOUT);
@@ -2576,7 +2640,7 @@ static size_t multi_thomas_smem(int nr, int NS) {
 
 /* ring depth: the shared memory each of the SM's resident lines may use,
  * at least 3 and at most 8 stages */
-static int multi_thomas_ns(const FastLayout &L, int nr) {
+static int multi_thomas_ns(const FastLayout &L, int nr, bool ws) {
     int dev = 0, nsm = 148, smem_sm = 228 * 1024, reserved = 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -2584,7 +2648,7 @@ static int multi_thomas_ns(const FastLayout &L, int nr) {
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     if (nsm < 1) nsm = 148;
     int per_sm = (L.nline + nsm - 1) / nsm;
-    const int by_threads = 2048 / (32 * multi_thomas_warps(nr));
+    const int by_threads = 2048 / (32 * (multi_thomas_warps(nr) + (ws ? 1 : 0)));
     if (per_sm > by_threads) per_sm = by_threads;
     if (per_sm < 1) per_sm = 1;
     const long long budget = (long long)smem_sm / per_sm - reserved - (long long)multi_thomas_smem(nr, 0);
@@ -2598,11 +2662,20 @@ int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const doub
                         const double *Gam, const double *b, double *y, double *dU,
                         const int *active, unsigned *status) {
     if (L.nv != NV || nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
-    const int NS = multi_thomas_ns(L, nr);
+    /* the copy warp pays where few lines share an SM (see thomas_ws); three
+     * five-warp CTAs fill an SM's registers */
+    const bool ws = thomas_ws(L, 3);
+    const int NS = multi_thomas_ns(L, nr, ws);
     const long long vs = (long long)L.np16 * NV;
-    multi_thomas_kernel<THOMAS_P><<<L.nline, 32 * multi_thomas_warps(nr), multi_thomas_smem(nr, NS), st>>>(
-        L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
-        status);
+    const int nw = multi_thomas_warps(nr);
+    if (ws)
+        multi_thomas_kernel<THOMAS_P, true><<<L.nline, 32 * (nw + 1), multi_thomas_smem(nr, NS), st>>>(
+            L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
+            status);
+    else
+        multi_thomas_kernel<THOMAS_P, false><<<L.nline, 32 * nw, multi_thomas_smem(nr, NS), st>>>(
+            L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
+            status);
     return (int)cudaGetLastError();
 }
 
@@ -2907,8 +2980,11 @@ int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const Mul
  * (outside stream capture) */
 int multi_prepare(const FastLayout &L, int nr) {
     if (nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
-    int rc = set_smem((const void *)multi_thomas_kernel<THOMAS_P>,
-                      multi_thomas_smem(nr, multi_thomas_ns(L, nr)));
+    int rc = set_smem((const void *)multi_thomas_kernel<THOMAS_P, false>,
+                      multi_thomas_smem(nr, multi_thomas_ns(L, nr, false)));
+    if (!rc)
+        rc = set_smem((const void *)multi_thomas_kernel<THOMAS_P, true>,
+                      multi_thomas_smem(nr, multi_thomas_ns(L, nr, true)));
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<1>, multi_resid_smem(L.nx, nr));
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<0>, multi_resid_smem(0, nr));
     return rc;
