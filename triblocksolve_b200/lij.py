@@ -326,15 +326,22 @@ class Solver:
                                   C.byref(it), N.dptr(h)))
         return it.value, h[: it.value + 1]
 
-    def solve_multi(self, rhs: np.ndarray, rel_tol: float, max_sweeps: int = 1000):
+    def solve_multi(self, rhs: np.ndarray, rel_tol: float, max_sweeps: int = 1000, out=None):
         """Several right-hand sides (rows of ``rhs``, 9*nelem each) from U = 0
         with the current factors (ALGO_FP64), groups of up to 8 sweeping
         together.  Returns (U [nrhs, 9*nelem], sweeps [nrhs], list of norm
-        histories); each row equals ``set_rhs`` + ``solve`` of it alone."""
+        histories); each row equals ``set_rhs`` + ``solve`` of it alone.
+        ``out``: a C-contiguous float64 [nrhs, 9*nelem] array to receive U
+        (pinned host memory makes the device-to-host copy direct)."""
         n = self.nvar * self.nelem
         rhs = np.ascontiguousarray(rhs, np.float64).reshape(-1, n)
         nrhs = rhs.shape[0]
-        U = np.zeros((nrhs, n))
+        if out is None:
+            U = np.zeros((nrhs, n))
+        elif out.dtype != np.float64 or out.size != nrhs * n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of {nrhs} x {n} values")
+        else:
+            U = out.reshape(nrhs, n)
         sw = np.zeros(nrhs, np.int32)
         h = np.zeros((nrhs, max_sweeps + 1))
         self._chk(N.lib.tbs_solve_multi(self.ctx, nrhs, N.dptr(rhs), N.dptr(U), rel_tol,
@@ -351,19 +358,25 @@ class Solver:
                                                N.iptr(sw), N.dptr(h), max_sweeps + 1))
         return sw, [h[r, : sw[r] + 1].copy() for r in range(nrhs)]
 
-    def _vec(self, fn):
-        out = np.zeros(self.nvar * self.nelem)
+    def _vec(self, fn, out=None):
+        """``out``: a C-contiguous float64 array of nvar*nelem to fill (pinned
+        host memory makes the device-to-host copy direct); default a new one."""
+        n = self.nvar * self.nelem
+        if out is None:
+            out = np.zeros(n)
+        elif out.dtype != np.float64 or out.size != n or not out.flags.c_contiguous:
+            raise ValueError(f"out must be a C-contiguous float64 array of {n} values")
         self._chk(fn(self.ctx, N.dptr(out)))
         return out
 
-    def solution(self) -> np.ndarray:
-        return self._vec(N.lib.tbs_get_solution)
+    def solution(self, out=None) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_solution, out)
 
-    def residual(self) -> np.ndarray:
-        return self._vec(N.lib.tbs_get_residual)
+    def residual(self, out=None) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_residual, out)
 
-    def update(self) -> np.ndarray:
-        return self._vec(N.lib.tbs_get_update)
+    def update(self, out=None) -> np.ndarray:
+        return self._vec(N.lib.tbs_get_update, out)
 
     def true_residual_norm(self) -> float:
         v = C.c_double()
