@@ -170,3 +170,29 @@ def test_multi_errors():
             s.solve_multi(np.zeros((2, 9 * mesh.nelem)), -1.0, 10)
     finally:
         s.close()
+
+
+def test_results_into_caller_arrays():
+    """solution(out=...) and solve_multi(out=...) fill the caller's (pinned)
+    arrays with exactly what the allocating forms return; wrong shapes are
+    refused before any copy."""
+    import torch
+    mesh = Mesh.structured(10, 12)
+    jac = Jacobian.generate(mesh, 9.0, 5)
+    s = Solver(0)
+    s.set_mesh(mesh)
+    s.set_jacobian(jac)
+    s.factor(ALGO_FP64)
+    s.solve(1e-12, 100)
+    n = 9 * mesh.nelem
+    pinned = torch.empty(n, dtype=torch.float64, pin_memory=True).numpy()
+    assert s.solution(out=pinned) is pinned
+    assert np.array_equal(pinned, s.solution())
+    with pytest.raises(ValueError):
+        s.solution(out=np.zeros(n - 1))
+    rows = np.stack([jac.rhs, -jac.rhs])
+    U, sw, _h = s.solve_multi(rows, 1e-12, 100)
+    out = torch.empty((2, n), dtype=torch.float64, pin_memory=True).numpy()
+    U2, sw2, _h2 = s.solve_multi(rows, 1e-12, 100, out=out)
+    assert np.array_equal(out, U) and np.array_equal(sw, sw2)
+    s.close()
