@@ -1,12 +1,12 @@
 """The two launch forms of the line solve give bit-identical results.
 
-The single-system and multi-RHS line solves have a one-warp-per-chain form
-and a warp-specialised form (a copy warp beside the chain warps), picked by
-how many lines share an SM; the test meshes are small, so by default they
-always get the warp-specialised form.  Here the same solves run in two
-processes with each form forced (TBS_THOMAS_WS=0 / 1, read once per
-process) and must agree bit for bit: FP64 and mixed-precision solves,
-several right-hand sides.
+The single-system line solve (FP64, and the FP32 inner sweeps of the mixed
+form) has a one-warp form and a warp-specialised form (a copy warp beside
+the chain warp), picked by how many lines share an SM; the test meshes are
+small, so by default they always get the warp-specialised form.  Here the
+same solves run in two processes with each form forced (TBS_THOMAS_WS=0 /
+1, read once per process) and must agree bit for bit; so must the
+several-right-hand-side solve run beside them.
 """
 import os
 import subprocess

@@ -1439,7 +1439,7 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
  * other's latency and which holds more lines per SM in its registers
  * (1,200 lines: 409 us one-warp, 526 us warp-specialised).  The
  * environment variable TBS_THOMAS_WS=0 / 1 forces one or the other. */
-static bool thomas_ws(const FastLayout &L, int max_per_sm = 4) {
+static bool thomas_ws(const FastLayout &L) {
     static const int forced = [] {
         const char *e = getenv("TBS_THOMAS_WS");
         return e && e[0] ? (e[0] == '0' ? 0 : 1) : -1;
@@ -1449,7 +1449,7 @@ static bool thomas_ws(const FastLayout &L, int max_per_sm = 4) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm < 1) nsm = 148;
-    return (L.nline + nsm - 1) / nsm <= max_per_sm;
+    return (L.nline + nsm - 1) / nsm <= 4;
 }
 
 template <typename T>
@@ -2563,296 +2563,6 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     }
 }
 
-/* The warp-specialised form of multi_thomas_kernel, instantiated with WS =
- * true: one more warp (the last) issues the copies; the chain warps wait
- * only for their stage's copies and release it on a second mbarrier per
- * stage (count: the chain warps), with no CTA barrier per chunk.  The chain
- * arithmetic is the same, so the results are bit-identical.  Three such
- * CTAs (five warps each) fit an SM's registers: the launch is meant for
- * meshes with at most 3 lines per SM. */
-template <int P, bool WS>
-__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW + (WS ? 32 : 0), WS ? 3 : 1) multi_thomas_ws_kernel(
-    int nline, int NS, int nr, long long vs, const int *__restrict__ line_start,
-    const int *__restrict__ line_len, const int *__restrict__ line_twist,
-    const double *__restrict__ G, const double *__restrict__ Gam, const double *__restrict__ b,
-    double *__restrict__ y, double *__restrict__ dU, const int *__restrict__ active,
-    unsigned *status) {
-    using T = double;
-    extern __shared__ __align__(128) unsigned char smem[];
-    __shared__ unsigned amask_s;
-    __shared__ int rid[MULTI_MAX];
-    __shared__ int ws_issued, ws_abort;
-    const int l = blockIdx.x;
-    if (l >= nline) return;
-    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-    const int nw = (int)(blockDim.x >> 5) - (WS ? 1 : 0); /* chain warps */
-    const bool producer = WS && w == nw;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
-    uint64_t *empty = bars + 8;
-    if (tid == 0) {
-        unsigned am = 0;
-        int k = 0;
-        for (int r = 0; r < nr; ++r)
-            if (active[r]) {
-                am |= 1u << r;
-                rid[k++] = r;
-            }
-        amask_s = am;
-        for (int s = 0; s < NS; ++s) {
-            mbar_init(&bars[s], 1);
-            if (WS) mbar_init(&empty[s], (uint32_t)nw);
-        }
-        ws_issued = 0;
-        ws_abort = 0;
-        mbar_fence_init();
-    }
-    __syncthreads();
-    const unsigned amask = amask_s;
-    if (amask == 0u) return;
-    const int nact = __popc(amask);
-    const int k0 = w * MULTI_RPW;                  /* this warp's first active slot */
-    const int nown = max(0, min(MULTI_RPW, nact - k0));
-    const bool mine = nown > 0;
-    const uint32_t halfb = P * (NB + nr * NV) * sizeof(T);
-    const uint32_t stage = 2 * halfb;
-    unsigned char *st0 = smem + 128;
-    T *bcw = reinterpret_cast<T *>(st0 + (size_t)NS * stage) + w * MULTI_RPW * 80;
-    const int ps = line_start[l], n = line_len[l], m = line_twist[l];
-    const int h = lane >> 4, li = lane & 15;
-    const int i = li < NV ? li : NV - 1;
-    const bool writer = li < NV;
-    const LaneOff off = lane_offsets(i);
-    const int nb = n - 1 - m;
-    const int len = h ? nb : m;
-    const int cpos = h ? m : 0;
-    const int nchT = (m + P - 1) / P, nchB = (nb + P - 1) / P;
-    const int nch = h ? nchB : nchT;
-    const int nf = nchT > nchB ? nchT : nchB;
-    const int njobs = 2 * nf;
-    /* per owned right-hand side: its broadcast buffers (this half), y, dU
-     * and b (slots beyond nown alias slot 0 and never write) */
-    T *bc[MULTI_RPW], *yl[MULTI_RPW], *dUl[MULTI_RPW];
-    const T *bg[MULTI_RPW];
-    int slot[MULTI_RPW];
-#pragma unroll
-    for (int j = 0; j < MULTI_RPW; ++j) {
-        const int jj = j < nown ? j : 0;
-        slot[j] = mine ? k0 + jj : 0;
-        const size_t ro = (size_t)(mine ? rid[k0 + jj] : 0) * (size_t)vs;
-        bc[j] = bcw + j * 80 + h * 40;
-        yl[j] = y + ro + (size_t)ps * NV;
-        dUl[j] = dU + ro + (size_t)ps * NV;
-        bg[j] = b + ro + (size_t)ps * NV;
-    }
-    const uint64_t pol = tid == (WS ? 32 * nw : 0) ? policy_evict_first() : 0;
-    if (!producer)
-        for (int t = lane; t < MULTI_RPW * 80; t += 32) bcw[t] = T(0);
-    __syncwarp();
-
-    auto cells = [&](int ln, int c) { return ((min(P, ln - c * P) + 3) & ~3); };
-    auto issue = [&](int job, int s) {
-        unsigned char *base = st0 + (size_t)s * stage;
-        uint32_t bytes = 0;
-        if (job < nf) {
-            if (job < nchT) bytes += cells(m, job) * (NB + nact * NV) * sizeof(T);
-            if (job < nchB) bytes += cells(nb, job) * (NB + nact * NV) * sizeof(T);
-        } else {
-            const int jb = job - nf;
-            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * NB * sizeof(T);
-            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * NB * sizeof(T);
-        }
-        mbar_arrive_expect_tx(&bars[s], bytes);
-        for (int hh = 0; hh < 2; ++hh) {
-            const int ln = hh ? nb : m, nc = hh ? nchB : nchT, cp = hh ? m : 0;
-            unsigned char *hb = base + hh * halfb;
-            if (job < nf) {
-                const int c = job;
-                if (c >= nc) continue;
-                const int cnt = cells(ln, c);
-                const size_t p = (size_t)(ps + cp + c * P);
-                bulk_g2s_hint(hb, G + p * NB, cnt * NB * sizeof(T), &bars[s], pol);
-                for (int k = 0; k < nact; ++k)
-                    bulk_g2s(hb + (size_t)(P * NB + k * P * NV) * sizeof(T),
-                             b + (size_t)rid[k] * (size_t)vs + p * NV, cnt * NV * sizeof(T), &bars[s]);
-            } else {
-                const int c = nc - 1 - (job - nf);
-                if (c < 0) continue;
-                const int cnt = cells(ln, c);
-                bulk_g2s_hint(hb, Gam + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(T),
-                              &bars[s], pol);
-            }
-        }
-    };
-    if (producer) {
-        if (lane == 0) {
-            for (int job = 0; job < njobs; ++job) {
-                if (*(volatile int *)&ws_abort) break;
-                const int s = job % NS;
-                if (job >= NS && !mbar_wait(&empty[s], (uint32_t)((job / NS - 1) & 1))) {
-                    atomicOr(status, ST_TIMEOUT);
-                    break;
-                }
-                issue(job, s);
-                *(volatile int *)&ws_issued = job + 1;
-            }
-        }
-        __syncwarp();
-        __syncthreads(); /* meets the chain warps' */
-        return;
-    }
-    int issued = 0;
-    if (!WS && tid == 0) {
-        for (; issued < NS && issued < njobs; ++issued) issue(issued, issued);
-    }
-    int consumed = 0;
-    bool timed_out = false;
-    const int both_full = (m < nb ? m : nb) / P;
-
-    /* ---------------- forward */
-    for (int c = 0; c < nf; ++c) {
-        const int s = c % NS;
-        const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(c / NS) & 1u));
-        if (WS && !ok) {
-            timed_out = true;
-            break;
-        }
-        if (ok && mine) {
-            const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
-            const T *sB[MULTI_RPW];
-#pragma unroll
-            for (int j = 0; j < MULTI_RPW; ++j) sB[j] = sG + P * NB + slot[j] * P * NV;
-            if (c < both_full)
-                fwd_chunk_m<P, false>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
-            else
-                fwd_chunk_m<P, true>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
-            __syncwarp();
-        }
-        if (WS) {
-            ++consumed;
-            if (lane == 0) mbar_arrive(&empty[s]);
-            continue;
-        }
-        if (__syncthreads_or(!ok)) {
-            timed_out = true;
-            break;
-        }
-        ++consumed;
-        if (tid == 0 && issued < njobs) {
-            issue(issued, s);
-            ++issued;
-        }
-    }
-
-    if (!timed_out) {
-        /* ---------------- twist: x_m = b_m - G_tw y_top - Gam_tw y_bot */
-        const int ptw = n - 1;
-        T xm[MULTI_RPW];
-#pragma unroll
-        for (int j = 0; j < MULTI_RPW; ++j) xm[j] = T(0);
-        if (mine && lane < NV) {
-            const T *gr = G + (size_t)(ps + ptw) * NB + NV * lane;
-            const T *cr = Gam + (size_t)(ps + ptw) * NB + NV * lane;
-#pragma unroll
-            for (int j = 0; j < MULTI_RPW; ++j) {
-                const T *base = bcw + j * 80;
-                const T *ytop = base + 0 * 40 + (m & 1) * 20;
-                const T *ybot = base + 1 * 40 + (nb & 1) * 20;
-                T acc = bg[j][(size_t)ptw * NV + lane];
-#pragma unroll
-                for (int jj = 0; jj < NV; ++jj) acc -= gr[jj] * ytop[jj] + cr[jj] * ybot[jj];
-                xm[j] = acc;
-            }
-        }
-        __syncwarp();
-        if (mine && lane < NV) {
-#pragma unroll
-            for (int j = 0; j < MULTI_RPW; ++j) {
-                if (j < nown) {
-                    T *base = bcw + j * 80;
-                    for (int t = 0; t < 4; ++t) {
-                        base[t * 20 + lane] = xm[j];
-                        base[t * 20 + 11 + lane] = xm[j];
-                    }
-                    dUl[j][(size_t)ptw * NV + lane] = xm[j];
-                }
-            }
-        }
-        __syncwarp();
-
-        /* ---------------- backward */
-        T yv[MULTI_RPW][P], nyv[MULTI_RPW][P];
-        auto load_chunk = [&](int c, T (*yy)[P]) {
-#pragma unroll
-            for (int j = 0; j < MULTI_RPW; ++j)
-#pragma unroll
-                for (int q = 0; q < P; ++q) {
-                    const int k = c * P + q;
-                    yy[j][q] = T(0);
-                    if (j < nown && c >= 0 && k < len && writer)
-                        yy[j][q] = yl[j][(size_t)(cpos + k) * NV + i];
-                }
-        };
-        load_chunk(nch - 1, yv);
-        for (int jb = 0; jb < nf; ++jb) {
-            const int job = nf + jb;
-            const int c = nch - 1 - jb;
-            load_chunk(c - 1, nyv);
-            const int s = job % NS;
-            const bool ok = __all_sync(FULL, mbar_wait(&bars[s], (uint32_t)(job / NS) & 1u));
-            if (WS && !ok) {
-                timed_out = true;
-                break;
-            }
-            if (ok && mine) {
-                const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * halfb);
-                const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
-                                  nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
-                if (full)
-                    bwd_chunk_m<P, false>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
-                else
-                    bwd_chunk_m<P, true>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
-                __syncwarp();
-            }
-            if (WS) {
-                ++consumed;
-                if (lane == 0) mbar_arrive(&empty[s]);
-            } else {
-                if (__syncthreads_or(!ok)) {
-                    timed_out = true;
-                    break;
-                }
-                ++consumed;
-                if (tid == 0 && issued < njobs) {
-                    issue(issued, s);
-                    ++issued;
-                }
-            }
-#pragma unroll
-            for (int j = 0; j < MULTI_RPW; ++j)
-#pragma unroll
-                for (int q = 0; q < P; ++q) yv[j][q] = nyv[j][q];
-        }
-    }
-    if (WS) {
-        /* a chain warp that ran out of time stops the copy warp (whose own
-         * waits are bounded); then the copies in flight land */
-        if (timed_out && lane == 0) *(volatile int *)&ws_abort = 1;
-        __syncthreads(); /* meets the copy warp's */
-        if (tid == 0 && *(volatile int *)&ws_abort) {
-            atomicOr(status, ST_TIMEOUT);
-            const int last = *(volatile int *)&ws_issued;
-            for (int job = last > NS ? last - NS : 0; job < last; ++job)
-                mbar_wait(&bars[job % NS], (uint32_t)(job / NS) & 1u, 1LL << 28);
-        }
-        return;
-    }
-    if (timed_out && tid == 0) {
-        atomicOr(status, ST_TIMEOUT);
-        for (int job = consumed; job < issued; ++job)
-            mbar_wait(&bars[job % NS], (uint32_t)(job / NS) & 1u, 1LL << 28);
-    }
-}
-
 static int multi_thomas_warps(int nr) { return (nr + MULTI_RPW - 1) / MULTI_RPW; }
 
 static size_t multi_thomas_stage(int nr) {
@@ -2866,7 +2576,7 @@ static size_t multi_thomas_smem(int nr, int NS) {
 
 /* ring depth: the shared memory each of the SM's resident lines may use,
  * at least 3 and at most 8 stages */
-static int multi_thomas_ns(const FastLayout &L, int nr, bool ws) {
+static int multi_thomas_ns(const FastLayout &L, int nr) {
     int dev = 0, nsm = 148, smem_sm = 228 * 1024, reserved = 1024;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
@@ -2874,7 +2584,7 @@ static int multi_thomas_ns(const FastLayout &L, int nr, bool ws) {
     cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
     if (nsm < 1) nsm = 148;
     int per_sm = (L.nline + nsm - 1) / nsm;
-    const int by_threads = 2048 / (32 * (multi_thomas_warps(nr) + (ws ? 1 : 0)));
+    const int by_threads = 2048 / (32 * multi_thomas_warps(nr));
     if (per_sm > by_threads) per_sm = by_threads;
     if (per_sm < 1) per_sm = 1;
     const long long budget = (long long)smem_sm / per_sm - reserved - (long long)multi_thomas_smem(nr, 0);
@@ -2888,20 +2598,11 @@ int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const doub
                         const double *Gam, const double *b, double *y, double *dU,
                         const int *active, unsigned *status) {
     if (L.nv != NV || nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
-    /* the copy warp pays where few lines share an SM (see thomas_ws); three
-     * five-warp CTAs fill an SM's registers */
-    const bool ws = thomas_ws(L, 3);
-    const int NS = multi_thomas_ns(L, nr, ws);
+    const int NS = multi_thomas_ns(L, nr);
     const long long vs = (long long)L.np16 * NV;
-    const int nw = multi_thomas_warps(nr);
-    if (ws)
-        multi_thomas_ws_kernel<THOMAS_P, true><<<L.nline, 32 * (nw + 1), multi_thomas_smem(nr, NS), st>>>(
-            L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
-            status);
-    else
-        multi_thomas_kernel<THOMAS_P><<<L.nline, 32 * nw, multi_thomas_smem(nr, NS), st>>>(
-            L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
-            status);
+    multi_thomas_kernel<THOMAS_P><<<L.nline, 32 * multi_thomas_warps(nr), multi_thomas_smem(nr, NS), st>>>(
+        L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
+        status);
     return (int)cudaGetLastError();
 }
 
@@ -3207,10 +2908,7 @@ int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const Mul
 int multi_prepare(const FastLayout &L, int nr) {
     if (nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
     int rc = set_smem((const void *)multi_thomas_kernel<THOMAS_P>,
-                      multi_thomas_smem(nr, multi_thomas_ns(L, nr, false)));
-    if (!rc)
-        rc = set_smem((const void *)multi_thomas_ws_kernel<THOMAS_P, true>,
-                      multi_thomas_smem(nr, multi_thomas_ns(L, nr, true)));
+                      multi_thomas_smem(nr, multi_thomas_ns(L, nr)));
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<1>, multi_resid_smem(L.nx, nr));
     if (!rc) rc = set_smem((const void *)multi_resid_kernel<0>, multi_resid_smem(0, nr));
     return rc;
