@@ -984,7 +984,9 @@ __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys
         const T *cur = bc + odd * 20;
         T *nxt = bc + (odd ^ 1) * 20;
         const T yi = row_dot(cur_row, cur, o, odd, cur_b);
-        if (writer && (!CHECK || kbase + q < len)) {
+        /* lanes 9..15 of a half compute row 8 from the same inputs as lane
+         * 8 and store the same value to the same address: no divergence */
+        if (!CHECK || kbase + q < len) {
             nxt[i] = yi;
             nxt[11 + i] = yi;
             const int pos = cpos + kbase + q;
@@ -1017,7 +1019,7 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
         T yk = T(0);
         if (valid) yk = YS ? ys[pos * NV + i] : yv[q];
         const T d = row_dot(cur_row, cur, o, odd, yk);
-        if (writer && valid) {
+        if (valid) { /* lanes 9..15 repeat lane 8's row, value and address */
             nxt[i] = d;
             nxt[11 + i] = d;
             if (YS) {
@@ -1207,7 +1209,7 @@ __device__ __forceinline__ bool thomas_line(
                 const int k = c * P + q;
                 yy[q] = T(0);
                 uu[q] = T(0);
-                if (!YS && c >= 0 && k < len && writer) {
+                if (!YS && c >= 0 && k < len) { /* lanes 9..15: lane 8's values */
                     yy[q] = yl[(size_t)(cpos + k) * NV + i];
                     if (accumulate == 1) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
                 }
