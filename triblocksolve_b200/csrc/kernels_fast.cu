@@ -2280,7 +2280,8 @@ __device__ __forceinline__ void fwd_chunk_m(const double *sG, const double *cons
         double yi[MULTI_RPW];
 #pragma unroll
         for (int j = 0; j < MULTI_RPW; ++j) yi[j] = row_dot(cur_row, bc[j] + odd * 20, o, odd, cur_b[j]);
-        if (writer && (!CHECK || kbase + q < len)) {
+        /* lanes 9..15 repeat lane 8's row, value and address: no divergence */
+        if (!CHECK || kbase + q < len) {
             const int pos = cpos + kbase + q;
 #pragma unroll
             for (int j = 0; j < MULTI_RPW; ++j) {
@@ -2317,7 +2318,7 @@ __device__ __forceinline__ void bwd_chunk_m(const double *sG, double *const *bc,
 #pragma unroll
         for (int j = 0; j < MULTI_RPW; ++j)
             d[j] = row_dot(cur_row, bc[j] + f * 20, o, odd, valid ? yv[j][q] : 0.0);
-        if (writer && valid) {
+        if (valid) { /* lanes 9..15 repeat lane 8's row, value and address */
 #pragma unroll
             for (int j = 0; j < MULTI_RPW; ++j) {
                 if (j < nown) {
@@ -2522,7 +2523,7 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
                 for (int q = 0; q < P; ++q) {
                     const int k = c * P + q;
                     yy[j][q] = T(0);
-                    if (j < nown && c >= 0 && k < len && writer)
+                    if (j < nown && c >= 0 && k < len) /* lanes 9..15: lane 8's values */
                         yy[j][q] = yl[j][(size_t)(cpos + k) * NV + i];
                 }
         };
