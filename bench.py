@@ -188,11 +188,26 @@ def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
     t0 = time.perf_counter()
     b.sweeps(sweeps)
     dt = time.perf_counter() - t0
+    del b
+    # (i) one thread, what the reference's serial mode runs: a bounded sample
+    t0 = time.perf_counter()
+    b1 = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], 1)
+    t_factor1 = time.perf_counter() - t0
+    n1, t1_total = 0, 0.0
+    while t1_total < budget_s / 4 and n1 < sweeps:
+        t0 = time.perf_counter()
+        b1.sweeps(1)
+        t1_total += time.perf_counter() - t0
+        n1 += 1
+    del b1
+    oracle.set_threads(threads)
     return {"value": sweeps / dt, "unit": "sweeps/s", "cores": threads, "kind": "port",
             "sample": f"{sweeps} FP64 sweeps of the same {mesh.nline}x{mesh.max_line_nelem} system "
                       f"after one factorization ({t_factor:.2f} s), oracle/lij_oracle.c, OpenMP "
                       f"over lines, {threads} threads",
-            "factor_s": t_factor, "seconds": dt}
+            "factor_s": t_factor, "seconds": dt,
+            "single_thread": {"value": n1 / t1_total, "unit": "sweeps/s", "cores": 1,
+                              "factor_s": t_factor1, "sweeps": n1, "seconds": t1_total}}
 
 
 def batch_shapes(cfg):
