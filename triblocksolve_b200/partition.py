@@ -211,13 +211,22 @@ def _line_len(part: Partition, k: int) -> int:
 
 
 class LocalExchange:
-    """Halo exchange between partitions that live in this process (one or
-    several GPUs): each halo line's vector is copied from its owner through
-    a staging buffer on the owner's device, in stream order."""
+    """Halo exchange between partitions that live in this process on one
+    device: each halo line's vector is copied from its owner into the
+    receiver through a staging buffer, in the order of one stream.  (Across
+    devices or processes use ``DistExchange``.)"""
 
     def __init__(self, parts: list[Partition], sweepers: list, device: str = "cuda"):
         import torch
         self.parts, self.sweepers = parts, sweepers
+        dev = torch.device(device)
+        if dev.type == "cuda":
+            want = dev.index if dev.index is not None else torch.cuda.current_device()
+            for s in sweepers:
+                got = getattr(getattr(s, "platform", None), "device_id", want)
+                if got != want:
+                    raise ValueError(f"LocalExchange: a partition is on device {got}, the "
+                                     f"exchange on device {want}; use DistExchange across devices")
         longest = max(int(p.mesh.max_line_nelem) for p in parts) * int(parts[0].mesh.nvar)
         self.buf = torch.empty(longest, dtype=torch.float64, device=device)
         if self.buf.is_cuda:
