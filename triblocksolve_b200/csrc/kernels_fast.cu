@@ -968,8 +968,7 @@ __device__ __forceinline__ float row_dot(const RowF &R, const float *cur, const 
  * warp may lie beyond one chain's end; those compute but write nothing. */
 template <typename T, int P, bool CHECK, bool YS>
 __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys, T *yg, int kbase,
-                                          int len, int cpos, int i, bool writer,
-                                          const LaneOff &o) {
+                                          int len, int cpos, int i, const LaneOff &o) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG, o, 0);
     T cur_b = sB[i];
@@ -1004,7 +1003,7 @@ __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys
 template <typename T, int P, bool CHECK, bool YS>
 __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv, const T *uv,
                                           T *dUl, T *Ul, int kbase, int len, int cpos, int i,
-                                          bool writer, const LaneOff &o) {
+                                          const LaneOff &o) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
 #pragma unroll
@@ -1066,7 +1065,6 @@ __device__ __forceinline__ bool thomas_line(
     const int lane = threadIdx.x & 31;
     const int h = lane >> 4, li = lane & 15;
     const int i = li < NV ? li : NV - 1;
-    const bool writer = li < NV;
     const LaneOff off = lane_offsets(i);
     const int nb = n - 1 - m;
     const int len = h ? nb : m;      /* this half's chain length */
@@ -1159,9 +1157,9 @@ __device__ __forceinline__ bool thomas_line(
         const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
         const T *sB = sG + P * NB;
         if (c < both_full)
-            fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, writer, off);
+            fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
         else
-            fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, writer, off);
+            fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
         __syncwarp();
         if (WS) {
             if (lane == 0) mbar_arrive(&empty[s]);
@@ -1232,10 +1230,10 @@ __device__ __forceinline__ bool thomas_line(
                               nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
             if (full)
                 bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
-                                           c * P, len, cpos, i, writer, off);
+                                           c * P, len, cpos, i, off);
             else
                 bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
-                                          c * P, len, cpos, i, writer, off);
+                                          c * P, len, cpos, i, off);
             __syncwarp();
             if (WS) {
                 if (lane == 0) mbar_arrive(&empty[s]);
@@ -2260,7 +2258,7 @@ constexpr int MULTI_RPW = 2;
 template <int P, bool CHECK>
 __device__ __forceinline__ void fwd_chunk_m(const double *sG, const double *const *sB,
                                             double *const *bc, double *const *yg, int nown,
-                                            int kbase, int len, int cpos, int i, bool writer,
+                                            int kbase, int len, int cpos, int i,
                                             const LaneOff &o) {
     RowD cur_row, next_row;
     load_row(cur_row, sG, o, 0);
@@ -2303,7 +2301,7 @@ __device__ __forceinline__ void fwd_chunk_m(const double *sG, const double *cons
 template <int P, bool CHECK>
 __device__ __forceinline__ void bwd_chunk_m(const double *sG, double *const *bc,
                                             const double (*yv)[P], double *const *dUl, int nown,
-                                            int kbase, int len, int cpos, int i, bool writer,
+                                            int kbase, int len, int cpos, int i,
                                             const LaneOff &o) {
     RowD cur_row, next_row;
     load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
@@ -2382,7 +2380,6 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     const int ps = line_start[l], n = line_len[l], m = line_twist[l];
     const int h = lane >> 4, li = lane & 15;
     const int i = li < NV ? li : NV - 1;
-    const bool writer = li < NV;
     const LaneOff off = lane_offsets(i);
     const int nb = n - 1 - m;
     const int len = h ? nb : m;
@@ -2462,9 +2459,9 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
 #pragma unroll
             for (int j = 0; j < MULTI_RPW; ++j) sB[j] = sG + P * NB + slot[j] * P * NV;
             if (c < both_full)
-                fwd_chunk_m<P, false>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
+                fwd_chunk_m<P, false>(sG, sB, bc, yl, nown, c * P, len, cpos, i, off);
             else
-                fwd_chunk_m<P, true>(sG, sB, bc, yl, nown, c * P, len, cpos, i, writer, off);
+                fwd_chunk_m<P, true>(sG, sB, bc, yl, nown, c * P, len, cpos, i, off);
             __syncwarp();
         }
         if (__syncthreads_or(!ok)) {
@@ -2539,9 +2536,9 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
                 const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
                                   nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
                 if (full)
-                    bwd_chunk_m<P, false>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
+                    bwd_chunk_m<P, false>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, off);
                 else
-                    bwd_chunk_m<P, true>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, writer, off);
+                    bwd_chunk_m<P, true>(sG, bc, yv, dUl, nown, c * P, len, cpos, i, off);
                 __syncwarp();
             }
             if (__syncthreads_or(!ok)) {
