@@ -5,8 +5,8 @@ partition is swept by the oracle (the reference's own line solve and
 residual rule, oracle/lij_oracle.c) instead of the GPU kernels, so that the
 partitioned sweep loop is checked against the oracle's sweep of the whole
 mesh: the owned cells' U bit-identical, the global norms within rounding of
-the summation order.  The exchange over torch.distributed runs as two
-gloo ranks (world size 2).
+the summation order.  The exchange over torch.distributed runs as gloo
+ranks (world sizes 2 and 3: a middle partition has two neighbours).
 """
 import os
 import socket
@@ -159,18 +159,18 @@ def _free_port():
     return port
 
 
-def _rank_main(rank, port, out):
+def _rank_main(rank, port, out, world=2):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     sys.path.insert(0, ROOT)
     sys.path.insert(0, os.path.join(ROOT, "tests"))
     import datetime
 
     import torch.distributed as dist
-    dist.init_process_group("gloo", rank=rank, world_size=2,
+    dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
     try:
         mesh, jac = _problem(LENS, 7)
-        parts = partition_lines(mesh, 2)
+        parts = partition_lines(mesh, world)
         part = parts[rank]
         s = OracleSweeper(part, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs)
         run = PartitionedSolve([s], DistExchange(part, s, device="cpu"))
@@ -182,21 +182,22 @@ def _rank_main(rank, port, out):
         dist.destroy_process_group()
 
 
-def test_gloo_two_ranks_match_whole_mesh_oracle():
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_match_whole_mesh_oracle(world):
     port = _free_port()
     with mp.Manager() as m:
         out = m.dict()
-        mp.spawn(_rank_main, args=(port, out), nprocs=2, join=True)
+        mp.spawn(_rank_main, args=(port, out, world), nprocs=world, join=True)
         res = dict(out)
     mesh, jac = _problem(LENS, 7)
     ref = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, 30)
     want = int(np.argmax(ref["hist"] <= 1e-12 * ref["hist"][0]))
     U = np.zeros(9 * mesh.nelem)
-    for rank in (0, 1):
+    for rank in range(world):
         n, hist, u, elems = res[rank]
         assert n == want
         assert np.all(np.abs(np.array(hist) - ref["hist"][:n + 1]) <= NORM_TOL * ref["hist"][0])
         U.reshape(-1, 9)[elems] = np.array(u).reshape(-1, 9)
-    # both ranks stopped at the same sweep: the whole-mesh U after `want` sweeps
+    # every rank stopped at the same sweep: the whole-mesh U after `want` sweeps
     ref_n = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, want)
     assert np.array_equal(U, ref_n["U"])
