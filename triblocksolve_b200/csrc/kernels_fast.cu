@@ -1437,7 +1437,9 @@ static ThomasCfg thomas_cfg(const FastLayout &L) {
  * off the chain warp shortens every step (360 lines: 64 -> 51 us); the
  * one-warp kernel where many lines share an SM, whose warps hide each
  * other's latency and which holds more lines per SM in its registers
- * (1,200 lines: 409 us one-warp, 526 us warp-specialised).  The
+ * (1,200 lines: 409 us one-warp, 526 us warp-specialised).  At 600 lines
+ * (5 per SM) the copy warp still pays: 117 -> 112 us (FP64), 87 -> 81 us
+ * (FP32).  The
  * environment variable TBS_THOMAS_WS=0 / 1 forces one or the other. */
 static bool thomas_ws(const FastLayout &L) {
     static const int forced = [] {
@@ -1449,7 +1451,7 @@ static bool thomas_ws(const FastLayout &L) {
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     if (nsm < 1) nsm = 148;
-    return (L.nline + nsm - 1) / nsm <= 4;
+    return (L.nline + nsm - 1) / nsm <= 5;
 }
 
 template <typename T>
