@@ -172,6 +172,23 @@ def build_problem(L, K, shift, pinned, nvar=9):
     return mesh, host
 
 
+def reference_model_bytes(mesh) -> float:
+    """Bytes per sweep by the reference's own count (src/main.cxx:146-175):
+    duMem (jacDLU, DinvC, A once, dU twice loaded and twice stored, res, the
+    line index arrays), cpMem (five dU-sized vectors) and lrMem (jacD, jacO1,
+    jacO2, U five times, res loaded and stored, all mesh index arrays).
+    Times sweeps/s it gives the GB/s in which the paper quotes its figures
+    (about 6.45 KB per cell for 9x9 blocks)."""
+    nv = int(mesh.nvar)
+    nb = nv * nv
+    N, F, L, eft = int(mesh.nelem), int(mesh.nintface), int(mesh.nline), int(mesh.eftot)
+    du = 8.0 * (3 * nb * N + 4 * nv * N + nv * N) + 4.0 * (L + (L + 1) + N + N)
+    cp = 8.0 * 5 * nv * N
+    lr = (8.0 * (nb * N + 2 * nb * F + 5 * nv * N + 2 * nv * N)
+          + 4.0 * ((N + 1) + eft + 2 * F + L + (L + 1) + N + N))
+    return du + cp + lr
+
+
 def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
     """The oracle (restated reference path) on all host cores; sweeps/s."""
     import oracle
@@ -1297,7 +1314,7 @@ def main():
         h2d = sum(host[k].nbytes for k in ("jacD", "jacO1", "jacO2", "rhs"))
         d2h = Uh.nbytes + 8 * (max_sweeps + 1)
         nb_ = nvar * nvar
-        ref_bytes = (8.0 * ((4 * nb_ + 7 * nvar) * mesh.nelem + 2 * nb_ * mesh.nintface)) * sweeps_per_solve
+        ref_bytes = reference_model_bytes(mesh)
         line = {
             "metric": "LIJ sweeps/s", "value": round(value, 2), "unit": "sweeps/s",
             "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
@@ -1323,6 +1340,7 @@ def main():
                 "l2": "no flush: every sweep streams %.0f MB of blocks, > 126 MB L2" %
                       (8 * nvar * nvar * 5 * mesh.nelem / 1e6),
                 "reference_model_gbs": round(ref_bytes * value / ws / 1e9, 1),
+                "reference_model_bytes_per_sweep": int(ref_bytes),
                 "published_baseline": "V100 FP64 LIJ, paper Table 5 (5 sweeps); vs_baseline "
                                       "is per GPU",
                 "parallelism": f"{ws} independent systems, one per GPU" if ws > 1 else "1 GPU",

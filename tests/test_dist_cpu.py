@@ -77,3 +77,16 @@ def test_reference_arm_under_torchrun_rank0_only():
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
     assert line["cpu_baseline"]["kind"] == "port"
+
+
+def test_reference_byte_model():
+    """bench.py's reference_model_gbs uses the reference's own byte count
+    (src/main.cxx:146-175): 9.92 GB per sweep, 6.45 KB per cell, at
+    1,200 x 1,280 cells with 9 x 9 blocks."""
+    sys.path.insert(0, ROOT)
+    import bench
+    import triblocksolve_b200 as tbs
+    m = tbs.Mesh.structured(1200, 1280)
+    b = bench.reference_model_bytes(m)
+    assert abs(b / 1e9 - 9.92) < 0.005
+    assert 6440 < b / m.nelem < 6470
