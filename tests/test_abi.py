@@ -38,6 +38,10 @@ def test_null_context_is_an_argument_error():
     assert N.lib.tbs_factor(None, 1) == N.TBS_ERR_ARG
     assert N.lib.tbs_sweep(None, 1, None) == N.TBS_ERR_ARG
     assert N.lib.tbs_destroy(None) == N.TBS_OK
+    assert N.lib.tbs_part_start(None, None) == N.TBS_ERR_ARG
+    assert N.lib.tbs_part_solve_du(None) == N.TBS_ERR_ARG
+    assert N.lib.tbs_part_line_res(None, None) == N.TBS_ERR_ARG
+    assert N.lib.tbs_part_line_vector(None, N.VEC_UPDATE, 0, None, 0) == N.TBS_ERR_ARG
     assert N.lib.tbs_create(0, None) == N.TBS_ERR_ARG
 
 
