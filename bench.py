@@ -102,7 +102,8 @@ class ClockSampler:
     def __init__(self, gpu_index):
         self.gpu = gpu_index
         self.proc = None
-        self.path = os.path.join(ROOT, "gpurun_out", f"clocks_rank{gpu_index}.csv")
+        import tempfile
+        self.path = os.path.join(tempfile.gettempdir(), f"tbs_clocks_{os.getpid()}_{gpu_index}.csv")
 
     def __enter__(self):
         try:

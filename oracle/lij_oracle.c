@@ -3,8 +3,8 @@
  * (LIJ) path, run with "OCCA Serial" semantics (every @inner loop a plain
  * loop, @barrier a no-op).  TEST INFRASTRUCTURE: only the tests, the smoke
  * check and the CPU-baseline / reference arm of bench.py load this file's
- * library, and only as the checker or the timed CPU baseline.  The product
- * (libtriblock.so) never calls it.
+ * library, and only as the results the GPU is compared against or as the
+ * timed CPU baseline.  The product (libtriblock.so) never calls it.
  *
  * Parity status: the arithmetic is unpinned by reference outputs.  The
  * reference's kernels are OKL and need the OCCA translator (an empty,
