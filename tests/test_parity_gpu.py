@@ -205,3 +205,24 @@ def test_mixed_inner_schedule(solver):
     solver.set_inner_schedule(4, 4)
     _, h4 = solver.solve(1e-10, 60)
     assert h4[1] != h[1]
+
+
+def test_contexts_of_different_shapes_in_one_process():
+    """A kernel's shared-memory limit is one value for the whole process: a
+    context with short lines, factored after one with long lines, must not
+    lower it under the first one's launches."""
+    big_mesh, small_mesh = Mesh.structured(8, 200), Mesh.structured(4, 4)
+    big_jac, small_jac = Jacobian.generate(big_mesh, 9.0, 2), Jacobian.generate(small_mesh, 9.0, 3)
+    big, small = Solver(0), Solver(0)
+    big.set_mesh(big_mesh)
+    big.set_jacobian(big_jac)
+    big.factor(ALGO_FP64)
+    small.set_mesh(small_mesh)
+    small.set_jacobian(small_jac)
+    small.factor(ALGO_FP64)
+    n, h = big.solve(1e-12, 100)
+    ref = oracle.lij(big_mesh, big_jac.jacD, big_jac.jacO1, big_jac.jacO2, big_jac.rhs, n)
+    assert np.all(np.abs(h - ref["hist"]) <= 1e-12 * ref["hist"][0])
+    small.solve(1e-12, 100)
+    big.close()
+    small.close()

@@ -47,7 +47,7 @@ def _parts(mesh, jac, nparts):
 
 
 @pytest.mark.parametrize("kind,nparts", [((24, 32), 1), ((24, 32), 3), ("ragged", 4),
-                                         ((60, 64), 7)])
+                                         ((60, 64), 7), ("ragged", 15), ((3, 40), 3)])
 def test_partitions_match_the_whole_mesh(kind, nparts):
     mesh, jac = _problem(kind)
     n = 6

@@ -26,6 +26,8 @@
 
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 namespace tbs {
 
 constexpr int NV = 9;
@@ -1498,10 +1500,19 @@ static int smem_limit(const void *fn) {
     return optin - (int)fa.sharedSizeBytes;
 }
 
+int smem_raise(const void *fn, size_t need) {
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    cudaFuncAttributes fa{};
+    if (cudaFuncGetAttributes(&fa, fn) == cudaSuccess && (size_t)fa.maxDynamicSharedSizeBytes >= need)
+        return 0;
+    return (int)cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+}
+
 static int set_smem(const void *fn, size_t need) {
     if ((long long)need > smem_limit(fn)) return (int)cudaErrorInvalidConfiguration;
     if (need <= 48 * 1024) return 0;
-    return (int)cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+    return smem_raise(fn, need);
 }
 
 /* Called before any launch (and outside stream capture) once the layout is
@@ -1943,8 +1954,7 @@ template <typename T>
 int thomas_batch_fit(int stages) {
     int n = 0;
     const size_t smem = thomas_batch_smem<T>(stages);
-    if (cudaFuncSetAttribute((const void *)fast_thomas_batch_kernel<T, THOMAS_P>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    if (smem_raise((const void *)fast_thomas_batch_kernel<T, THOMAS_P>, smem) != cudaSuccess)
         return 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fast_thomas_batch_kernel<T, THOMAS_P>, 32,
                                                       smem) != cudaSuccess)

@@ -657,7 +657,7 @@ int nv_smem_limit(const void *fn) {
 int nv_set_smem(const void *fn, size_t need) {
     if ((long long)need > nv_smem_limit(fn)) return (int)cudaErrorInvalidConfiguration;
     if (need <= 48 * 1024) return 0;
-    return (int)cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)need);
+    return smem_raise(fn, need);
 }
 
 int nv_grid_persistent(const void *fn, int threads, size_t smem, int ntiles) {

@@ -113,6 +113,13 @@ struct FastLayout {
                         * bottom neighbour and its side (its top face in 1-2) */
 };
 
+/* Raise kernel fn's dynamic shared-memory limit to at least `need` bytes.
+ * The limit is one value per kernel for the whole process, shared by every
+ * context (and thread) that launches the kernel, so it is only ever raised:
+ * a context with a smaller mesh must not lower it under a larger one.
+ * Returns a cudaError_t as an int. */
+int smem_raise(const void *fn, size_t need);
+
 /* ------------------------------------------------------ kernel launchers
  * All launches go on `st`; they return cudaGetLastError() as an int. */
 
