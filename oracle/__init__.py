@@ -98,6 +98,156 @@ def lij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1, want_factor
     return out
 
 
+# ---------------------------------------------------------------------------
+# oracle/_ref: the reference's own kernels (OKL translated by okl2c.py) driven
+# in src/main.cxx order.  Built here by `make -C oracle ref REFERENCE=<checkout>`
+# (needs the reference checkout); the built library travels with the tree.
+REF_LIB_PATH = os.path.join(HERE, "_ref", "libokl_ref.so")
+_ref_lib = None
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_LIB_PATH)
+
+
+def build_ref(reference_dir: str) -> str:
+    """Translates and compiles the reference's kernels into oracle/_ref."""
+    subprocess.run(["make", "-C", HERE, "ref", f"REFERENCE={reference_dir}"], check=True,
+                   capture_output=True)
+    return REF_LIB_PATH
+
+
+def _ref():
+    global _ref_lib
+    if _ref_lib is None:
+        if not ref_available():
+            raise FileNotFoundError(f"{REF_LIB_PATH} is not built (make -C oracle ref "
+                                    "REFERENCE=<reference checkout>)")
+        L = C.CDLL(REF_LIB_PATH)
+        L.okl_ref_set_threads.argtypes = [_i]
+        L.okl_ref_lij.restype = _i
+        L.okl_ref_lij.argtypes = [_i] * 7 + [_ip] * 7 + [_dp] * 4 + [_i] + [_dp] * 10
+        L.okl_ref_true_residual.restype = _i
+        L.okl_ref_true_residual.argtypes = [_i] * 7 + [_ip] * 6 + [_dp] * 6
+        L.okl_ref_factor.restype = C.c_void_p
+        L.okl_ref_factor.argtypes = [_i] * 7 + [_ip] * 7 + [_dp] * 4
+        L.okl_ref_sweeps.argtypes = [C.c_void_p, _dp, _dp, _dp, _i]
+        L.okl_ref_free.argtypes = [C.c_void_p]
+        L.okl_ref_assemble_tri_blocks.argtypes = [_i] * 5 + [_ip] * 5 + [_dp] * 3
+        L.okl_ref_resize_block_size.argtypes = [_i] * 4 + [_dp] * 10
+        _ref_lib = L
+    return _ref_lib
+
+
+def _mesh_sizes(mesh):
+    linesize = np.asarray(mesh.linesize)
+    nlineelem = int(getattr(mesh, "nlineelem", int(linesize.sum())))
+    mx = int(getattr(mesh, "max_line_nelem", int(linesize.max()) if linesize.size else 1))
+    return (int(mesh.nvar), int(mesh.nelem), int(mesh.nintface), int(mesh.eftot),
+            int(mesh.nline), max(nlineelem, int(mesh.nelem)), max(mx, 1))
+
+
+def ref_lij(mesh, jacD, jacO1, jacO2, rhs, iters: int, threads: int = 1, per_sweep=False,
+            want_factors=False):
+    """The reference's own kernels for `iters` sweeps from U = 0.
+    Returns dict(U, R, dU, hist[, U_all, R_all, dU_all][, DLU, DinvC, A])."""
+    L = _ref()
+    L.okl_ref_set_threads(int(threads))
+    sz = _mesh_sizes(mesh)
+    nv, ne = sz[0], sz[1]
+    keep, ptrs = [], []
+    for f in ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface"):
+        a, p = _ip_(getattr(mesh, f))
+        keep.append(a)
+        ptrs.append(p)
+    n = nv * ne
+    U, R, dU, hist = np.zeros(n), np.zeros(n), np.zeros(n), np.zeros(iters + 1)
+    alls = [np.zeros((iters, n)) for _ in range(3)] if per_sweep else [None] * 3
+    fac = [np.zeros(nv * nv * ne), np.zeros(nv * nv * ne), np.zeros(nv * nv * sz[5])] \
+        if want_factors else [None] * 3
+    rc = L.okl_ref_lij(*sz, *ptrs, _dp_(np.ascontiguousarray(jacD)), _dp_(np.ascontiguousarray(jacO1)),
+                       _dp_(np.ascontiguousarray(jacO2)), _dp_(np.ascontiguousarray(rhs)),
+                       int(iters), _dp_(U), _dp_(R), _dp_(dU), _dp_(hist),
+                       *[_dp_(a) if a is not None else None for a in fac],
+                       *[_dp_(a) if a is not None else None for a in alls])
+    if rc != 0:
+        raise RuntimeError(f"okl_ref_lij failed ({rc})")
+    out = dict(U=U, R=R, dU=dU, hist=hist)
+    if per_sweep:
+        out.update(U_all=alls[0], R_all=alls[1], dU_all=alls[2])
+    if want_factors:
+        out.update(DLU=fac[0], DinvC=fac[1], A=fac[2])
+    return out
+
+
+def ref_true_residual(mesh, jacD, jacO1, jacO2, rhs, U):
+    """rhs + J U by the reference's own triblock_lineRes."""
+    L = _ref()
+    sz = _mesh_sizes(mesh)
+    keep, ptrs = [], []
+    for f in ("epoint", "ef", "fc", "linesize", "linepoint", "lines"):
+        a, p = _ip_(getattr(mesh, f))
+        keep.append(a)
+        ptrs.append(p)
+    R = np.zeros(sz[0] * sz[1])
+    rc = L.okl_ref_true_residual(*sz, *ptrs, _dp_(np.ascontiguousarray(jacD)),
+                                 _dp_(np.ascontiguousarray(jacO1)), _dp_(np.ascontiguousarray(jacO2)),
+                                 _dp_(np.ascontiguousarray(rhs, np.float64)),
+                                 _dp_(np.ascontiguousarray(U, np.float64)), _dp_(R))
+    if rc != 0:
+        raise RuntimeError(f"okl_ref_true_residual failed ({rc})")
+    return R
+
+
+def ref_resize_block_size(nv_old, nv_new, nelem, nintface, D, O1, O2, rhs, U0):
+    """The reference's own Jacobian::resizeBlockSize; returns (D, O1, O2, rhs, U0)."""
+    L = _ref()
+    bn = nv_new * nv_new
+    out = [np.zeros(bn * nelem), np.zeros(bn * nintface), np.zeros(bn * nintface),
+           np.zeros(nv_new * nelem), np.zeros(nv_new * nelem)]
+    L.okl_ref_resize_block_size(nv_old, nv_new, nelem, nintface, _dp_(D), _dp_(O1), _dp_(O2),
+                                _dp_(rhs), _dp_(U0), *[_dp_(a) for a in out])
+    return out
+
+
+class RefBaseline:
+    """The reference's own kernels, factored once, swept on demand: the
+    `kind: reference` CPU baseline (OpenMP over lines, OCCA's OpenMP mode)."""
+
+    def __init__(self, mesh, jacD, jacO1, jacO2, rhs, threads: int):
+        self.L = _ref()
+        self.L.okl_ref_set_threads(int(threads))
+        sz = _mesh_sizes(mesh)
+        self.n = sz[0] * sz[1]
+        self._ints = {f: np.ascontiguousarray(getattr(mesh, f), np.int32) for f in
+                      ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface")}
+        self._arrs = [np.ascontiguousarray(a, np.float64) for a in (jacD, jacO1, jacO2, rhs)]
+        ip = [self._ints[f].ctypes.data_as(_ip) for f in
+              ("epoint", "ef", "fc", "linesize", "linepoint", "lines", "lineface")]
+        self.h = self.L.okl_ref_factor(*sz, *ip, *[_dp_(a) for a in self._arrs])
+        if not self.h:
+            raise RuntimeError("okl_ref_factor failed")
+        self.reset()
+
+    def reset(self):
+        self.U, self.dU = np.zeros(self.n), np.zeros(self.n)
+        self.R = self._arrs[3].copy()
+
+    def sweeps(self, n: int) -> None:
+        self.L.okl_ref_sweeps(self.h, _dp_(self.U), _dp_(self.R), _dp_(self.dU), int(n))
+
+    def close(self):
+        if self.h:
+            self.L.okl_ref_free(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def point_lines(mesh):
     """The mesh with every cell as its own line, faces unchanged.
 

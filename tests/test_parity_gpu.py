@@ -56,6 +56,23 @@ def test_reference_algo_bit_exact(solver, case):
         np.testing.assert_array_equal(solver.update(), r["dU"])
 
 
+@pytest.mark.skipif(not oracle.ref_available(), reason="oracle/_ref not built")
+@pytest.mark.parametrize("case", list(CASES) + ["nvar5"])
+def test_reference_algo_equals_reference_kernels(solver, case):
+    """TBS_ALGO_REFERENCE against the reference's own kernels (OKL translated
+    to C, oracle/_ref): U, R and dU bit for bit after every sweep."""
+    mesh = Mesh.structured(12, 16, nvar=5) if case == "nvar5" else CASES[case]()
+    jac = Jacobian.generate(mesh, 9.0, 11)
+    setup(solver, mesh, jac, ALGO_REFERENCE)
+    n = 6
+    r = oracle.ref_lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, n, threads=4, per_sweep=True)
+    for p in range(n):
+        solver.sweep(1)
+        np.testing.assert_array_equal(solver.solution(), r["U_all"][p])
+        np.testing.assert_array_equal(solver.residual(), r["R_all"][p])
+        np.testing.assert_array_equal(solver.update(), r["dU_all"][p])
+
+
 def test_reference_algo_generic_block_size(solver):
     mesh = ragged_mesh([4, 6, 2, 5], seed=2, nvar=5)
     jac = Jacobian.generate(mesh, 5.0, 6)
