@@ -4,18 +4,20 @@
                     [--config c2|c3a|c3b] [--algo fp64|ref|mixed]
 
 A step is one LIJ solve of the configured system from U = 0 to the relative
-residual tolerance (default: 360 lines x 384 cells = 138,240 cells, 9x9
-FP64 blocks, seeded synthetic values with shift 9, tolerance 1e-12).  The
+residual tolerance (default: 1200 lines x 1280 cells = 1,536,000 cells, 9x9
+FP64 blocks, seeded synthetic values with shift 4, tolerance 1e-10; the
+mixed-precision solve of the same system is timed beside it).  The
 metric is LIJ sweeps per second: total sweeps of all steps on all GPUs
 divided by the device time (CUDA events, max over ranks).  The blocks stay
 resident in HBM for `value`; `e2e` repeats the step through the C ABI from
 pinned host buffers (Jacobian upload, factorization, solve, solution
 read-back every step).
 
-With N > 1 (torchrun) every rank solves its own independent system of the
-same size: independent systems shard with no data-path collective (weak
-scaling); NCCL carries only the barrier and the max/sum reductions of the
-timings.  --impl reference times the CPU restatement of the reference path
+With N > 1 (torchrun) the mesh is split into N contiguous line ranges, one
+per rank (strong scaling): each sweep exchanges the halo lines' updates
+with the neighbouring ranks (NCCL send/recv) and all-reduces one double
+for the global norm.  --replicas gives every rank its own independent
+system instead (weak scaling, no data-path collective).  --impl reference times the CPU restatement of the reference path
 (oracle/, OpenMP over lines on all host cores) on the same system: one
 sweep per step, rank 0 only.
 """
@@ -190,12 +192,36 @@ def reference_model_bytes(mesh) -> float:
     return du + cp + lr
 
 
-def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
-    """The oracle (restated reference path) on all host cores; sweeps/s."""
+def cpu_system(L, K, shift, nvar=9):
+    """The same seeded system for the CPU legs, built by the oracle's numpy
+    generator (bit-identical to the library's) so that the CPU legs never
+    load the product library."""
+    from oracle import synthetic
+    mesh = synthetic.structured_mesh(L, K, nvar=nvar)
+    D, O1, O2, rhs = synthetic.jacobian(nvar, mesh.nelem, mesh.nintface, shift, SEED)
+    return mesh, {"jacD": D, "jacO1": O1, "jacO2": O2, "rhs": rhs}
+
+
+def cpu_impl():
+    """The CPU implementation of the reference path: the reference's own
+    kernels (OKL translated to C, oracle/_ref, kind "reference") where they
+    were built, else the oracle's restatement (kind "port")."""
     import oracle
+    if oracle.ref_available():
+        return oracle.RefBaseline, "reference", ("the reference's own OKL kernels (lineLU_v2, "
+                                                 "linesmoothLU_TriBlock_v3, linesmoothLU_v5) "
+                                                 "translated to C with OCCA's OpenMP semantics, "
+                                                 "oracle/_ref")
+    return oracle.Baseline, "port", "oracle/lij_oracle.c, OpenMP over lines"
+
+
+def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
+    """The CPU reference path on all host cores (and a one-thread sample); sweeps/s."""
+    import oracle
+    cls, kind, what = cpu_impl()
     threads = os.cpu_count() or 1
     t0 = time.perf_counter()
-    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    b = cls(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
     t_factor = time.perf_counter() - t0
     if sweeps is None:
         t0 = time.perf_counter()
@@ -209,7 +235,7 @@ def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
     del b
     # (i) one thread, what the reference's serial mode runs: a bounded sample
     t0 = time.perf_counter()
-    b1 = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], 1)
+    b1 = cls(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], 1)
     t_factor1 = time.perf_counter() - t0
     n1, t1_total = 0, 0.0
     while t1_total < budget_s / 4 and n1 < sweeps:
@@ -219,10 +245,9 @@ def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
         n1 += 1
     del b1
     oracle.set_threads(threads)
-    return {"value": sweeps / dt, "unit": "sweeps/s", "cores": threads, "kind": "port",
+    return {"value": sweeps / dt, "unit": "sweeps/s", "cores": threads, "kind": kind,
             "sample": f"{sweeps} FP64 sweeps of the same {mesh.nline}x{mesh.max_line_nelem} system "
-                      f"after one factorization ({t_factor:.2f} s), oracle/lij_oracle.c, OpenMP "
-                      f"over lines, {threads} threads",
+                      f"after one factorization ({t_factor:.2f} s), {what}, {threads} threads",
             "factor_s": t_factor, "seconds": dt,
             "single_thread": {"value": n1 / t1_total, "unit": "sweeps/s", "cores": 1,
                               "factor_s": t_factor1, "sweeps": n1, "seconds": t1_total}}
@@ -411,7 +436,7 @@ def run_batch(args):
             # bounded sample: the oracle on the median-size system of the batch
             k = int(np.argsort(cells)[len(cells) // 2])
             L, K = shapes[k]
-            m2, host = build_problem(L, K, shift, pinned=False)
+            m2, host = cpu_system(L, K, shift)
             cb = cpu_baseline(m2, host, budget_s=10.0)
             cb["value"] = cb["value"] * m2.nelem
             cb["unit"] = "cell-sweeps/s"
@@ -600,7 +625,7 @@ def run_serving(args):
         }
         if ws == 1 and not args.no_cpu_baseline:
             L, K, shift = cfg["systems"][1]
-            m2, host = build_problem(L, K, shift, pinned=False)
+            m2, host = cpu_system(L, K, shift)
             cb = cpu_baseline(m2, host, budget_s=8.0)
             # sweeps per solve of that shape from the saturation run
             sw = [int(r[1].mean()) for p, r in zip(plan, res) if p[0] == 1] or [10]
@@ -624,10 +649,10 @@ def run_serving_reference(args):
         return 0
     cfg = SERVE_CONFIGS[args.config]
     L, K, shift = cfg["systems"][1]
-    mesh, host = build_problem(L, K, shift, pinned=False)
-    import oracle
+    mesh, host = cpu_system(L, K, shift)
+    cls, kind, what = cpu_impl()
     threads = os.cpu_count() or 1
-    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    b = cls(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
     for _ in range(args.warmup):
         b.sweeps(1)
     b.reset()
@@ -646,9 +671,8 @@ def run_serving_reference(args):
                                    f"sweeps/s / {sweeps_per_solve:g} sweeps per solve",
                        "cells": mesh.nelem},
             "cpu_baseline": {"value": round(v, 3), "unit": "rhs-solves/s", "cores": threads,
-                             "kind": "port",
-                             "sample": f"{args.steps} sweeps of the {L}x{K} system; "
-                                       "oracle/lij_oracle.c, OpenMP over lines"},
+                             "kind": kind,
+                             "sample": f"{args.steps} sweeps of the {L}x{K} system; {what}"},
             "e2e": {"value": round(v, 3), "unit": "rhs-solves/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -665,10 +689,10 @@ def run_batch_reference(args):
     shapes = batch_shapes(cfg)
     cells = np.array([L * K for L, K in shapes])
     L, K = shapes[int(np.argsort(cells)[len(cells) // 2])]
-    mesh, host = build_problem(L, K, cfg["shift"], pinned=False)
-    import oracle
+    mesh, host = cpu_system(L, K, cfg["shift"])
+    cls, kind, what = cpu_impl()
     threads = os.cpu_count() or 1
-    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    b = cls(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
     for _ in range(args.warmup):
         b.sweeps(1)
     b.reset()
@@ -685,9 +709,8 @@ def run_batch_reference(args):
             "config": {"workload": f"one FP64 sweep per step of the median system ({L}x{K}) of "
                                    f"the {len(shapes)}-system batch", "cells": mesh.nelem},
             "cpu_baseline": {"value": round(v, 1), "unit": "cell-sweeps/s", "cores": threads,
-                             "kind": "port",
-                             "sample": f"{args.steps} sweeps of the {L}x{K} system; "
-                                       "oracle/lij_oracle.c, OpenMP over lines"},
+                             "kind": kind,
+                             "sample": f"{args.steps} sweeps of the {L}x{K} system; {what}"},
             "e2e": {"value": round(v, 1), "unit": "cell-sweeps/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -1108,13 +1131,18 @@ def run_gmres(args, L, K, shift, tol):
 
 
 def run_reference(args, L, K, shift, tol):
+    """The reference's CPU path on the host cores, one FP64 sweep per step
+    (a bounded sample of a solve), rank 0 only; the factorization is timed
+    apart and reported."""
     ws, rank, local = dist_env()
     if rank != 0:
         return 0
-    mesh, host = build_problem(L, K, shift, pinned=False)
-    import oracle
+    mesh, host = cpu_system(L, K, shift)
+    cls, kind, what = cpu_impl()
     threads = os.cpu_count() or 1
-    b = oracle.Baseline(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    t0 = time.perf_counter()
+    b = cls(mesh, host["jacD"], host["jacO1"], host["jacO2"], host["rhs"], threads)
+    t_factor = time.perf_counter() - t0
     for _ in range(args.warmup):
         b.sweeps(1)
     b.reset()
@@ -1131,11 +1159,11 @@ def run_reference(args, L, K, shift, tol):
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"LIJ FP64 sweeps, {L}x{K} structured mesh ({mesh.nelem} cells), "
                                    f"shift {shift}, seed {SEED}; one sweep per step",
-                       "cells": mesh.nelem},
-            "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": threads, "kind": "port",
-                             "sample": f"{done} sweeps (one per step) after one factorization; "
-                                       "oracle/lij_oracle.c with OpenMP over lines (the "
-                                       "reference's OCCA kernels need OCCA/MPI/gfortran, absent)"},
+                       "cells": mesh.nelem, "factor_s": round(t_factor, 3)},
+            "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": threads, "kind": kind,
+                             "sample": f"{done} sweeps (one per step) after one factorization "
+                                       f"({t_factor:.2f} s); {what} (OCCA, MPI and gfortran, "
+                                       "which the reference builds with, are absent)"},
             "e2e": {"value": v, "unit": "sweeps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -1147,7 +1175,7 @@ def main():
     ap.add_argument("--steps", type=int, default=200)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--config", default="c2",
+    ap.add_argument("--config", default="c3b",
                     choices=sorted(CONFIGS) + sorted(BATCH_CONFIGS) + sorted(SERVE_CONFIGS))
     ap.add_argument("--algo", default="fp64", choices=["fp64", "ref", "mixed", "pij"])
     ap.add_argument("--e2e-steps", type=int, default=None)
@@ -1160,6 +1188,11 @@ def main():
                     help="right-hand sides per solve (> 1: tbs_solve_multi, FP64)")
     ap.add_argument("--partition", action="store_true",
                     help="one mesh split into line partitions over the ranks (strong scaling)")
+    ap.add_argument("--replicas", action="store_true",
+                    help="with N > 1: N independent systems, one per rank (weak scaling), "
+                         "instead of one mesh split into line partitions")
+    ap.add_argument("--no-mixed", action="store_true",
+                    help="skip the mixed-precision solve timed beside the FP64 one")
     args = ap.parse_args()
     if args.config in SERVE_CONFIGS:
         if args.impl == "reference":
@@ -1172,7 +1205,9 @@ def main():
     L, K, shift, tol = CONFIGS[args.config]
     if args.impl == "reference":
         return run_reference(args, L, K, shift, tol)
-    if args.partition:
+    ws_env = dist_env()[0]
+    if args.partition or (ws_env > 1 and not args.replicas and args.algo == "fp64"
+                          and args.nvar == 9 and args.nrhs == 1 and not args.gmres):
         if args.algo != "fp64" or args.nvar != 9 or args.nrhs > 1 or args.gmres:
             ap.error("--partition runs the FP64 sweep at nvar 9")
         return run_partition(args, L, K, shift, tol)
@@ -1271,13 +1306,49 @@ def main():
         dist.barrier()
         torch.cuda.synchronize()
         e2e_ms = e0.elapsed_time(e1)
+        check = solver.solve_check() if args.algo == "fp64" else None
+        true_rel = solver.true_residual_norm() / float(last_hist[0])
+        # ---------------- the mixed form beside it: FP32 line factors and inner sweeps,
+        # FP64 outer residual, same system and tolerance, same number of timed solves
+        mixed = None
+        if (args.algo == "fp64" and nvar == 9 and not args.no_mixed
+                and args.config in ("c3a", "c3b")):
+            U64 = solver.solution()
+            solver.factor(tbs.ALGO_MIXED)
+            solver.tune_inner(tol, max_sweeps)
+            for _ in range(max(args.warmup, 0)):
+                solver.solve(tol, max_sweeps)
+            torch.cuda.synchronize()
+            dist.barrier()
+            torch.cuda.synchronize()
+            m0, m1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            m0.record(stream)
+            msteps = 0
+            for _ in range(args.steps):
+                ms_, mh = solver.solve(tol, max_sweeps)
+                msteps += ms_
+            m1.record(stream)
+            torch.cuda.synchronize()
+            dist.barrier()
+            torch.cuda.synchronize()
+            mixed_ms = dist.reduce(m0.elapsed_time(m1), "max") / args.steps
+            Um = solver.solution()
+            mixed = {
+                "ms_per_solve": round(mixed_ms, 4),
+                "outer_steps_per_solve": msteps / args.steps,
+                "inner_sweeps": list(solver.inner_schedule()),
+                "true_rel_residual": solver.true_residual_norm() / float(mh[0]),
+                "rel_error_vs_fp64_solution": float(np.linalg.norm(Um - U64) / np.linalg.norm(U64)),
+                "what": "TBS_ALGO_MIXED: FP32 line factors and inner sweeps, FP64 outer "
+                        "residual from the original blocks, autotuned inner sweep schedule; "
+                        "CUDA events around the same number of graph-launched solves",
+            }
     clk = clocks.summary()
 
     max_ms = dist.reduce(elapsed_ms, "max")
     all_sweeps = dist.reduce(sweeps_total, "sum")
     max_e2e_ms = dist.reduce(e2e_ms, "max")
     all_e2e_sweeps = dist.reduce(e2e_sweeps, "sum")
-    true_rel = solver.true_residual_norm() / float(last_hist[0])
 
     if rank == 0:
         value = all_sweeps / (max_ms * 1e-3)
@@ -1338,6 +1409,9 @@ def main():
                 "time_to_tol_ms": round(max_ms / args.steps, 4),
                 "factor_ms": round(factor_ms, 3),
                 "true_rel_residual": true_rel,
+                "true_residual_check": (None if check is None else
+                                        {"true_norm": check[0], "checks": check[1],
+                                         "restarts": check[2]}),
                 "l2": "no flush: every sweep streams %.0f MB of blocks, > 126 MB L2" %
                       (8 * nvar * nvar * 5 * mesh.nelem / 1e6),
                 "reference_model_gbs": round(ref_bytes * value / ws / 1e9, 1),
@@ -1356,6 +1430,11 @@ def main():
             "gpu_launches": int(round(launches_per_solve * args.steps)),
             "clocks": clk,
         }
+        if mixed is not None:
+            fp64_ms = max_ms / args.steps
+            mixed["fp64_ms_per_solve"] = round(fp64_ms, 4)
+            mixed["speedup_vs_fp64"] = round(fp64_ms / mixed["ms_per_solve"], 3)
+            line["mixed"] = mixed
         if ws == 1 and not args.no_cpu_baseline:
             if args.algo == "pij":
                 import oracle

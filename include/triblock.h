@@ -216,7 +216,14 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out);
 /* Sweeps until ||R|| <= rel_tol * ||R_0|| or max_sweeps, with the
  * convergence test on the device (one CUDA graph launch, no host round
  * trip per sweep).  *sweeps_out = sweeps done; hist_out (may be NULL)
- * receives sweeps+1 norms, hist[0] = ||R_0||. */
+ * receives sweeps+1 norms, hist[0] = ||R_0||.
+ * TBS_ALGO_FP64 tracks R recursively; when that R meets the tolerance the
+ * solve recomputes the true residual rhs + J U from the original blocks
+ * (the rule of src/okl/linesmoothLU_TriBlock_v3.okl:228-336).  If it also
+ * meets the tolerance the solve ends (history unchanged); if not, its norm
+ * replaces the sweep's history entry and the sweeps go on from it.  So a
+ * reported convergence is never one that tbs_true_residual_norm
+ * contradicts.  tbs_set_check(ctx, 0) turns the check off. */
 int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps,
               int *sweeps_out, double *hist_out);
 
@@ -306,6 +313,13 @@ int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm);
 int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
                          int to_line);
 
+/* The same for several lines in one launch: lines[0..nlines) (host array
+ * of local line indices) packed back to back into d_buf (to_line = 0) or
+ * unpacked from it (to_line = 1), each line's span as tbs_part_line_vector
+ * gives it.  A halo exchange with one neighbour is one call per side. */
+int tbs_part_lines_vector(tbs_ctx *ctx, int which, int nlines, const int *lines,
+                          double *d_buf, int to_line);
+
 /* Jacobian::fromDevice (src/Jacobian.cxx:279-290) for the vectors, in the
  * element order of the input (9*nelem doubles each). */
 int tbs_get_solution(tbs_ctx *ctx, double *U);
@@ -315,6 +329,29 @@ int tbs_get_update(tbs_ctx *ctx, double *dU);
 /* ||rhs + J U|| recomputed from the original FP64 blocks, whatever the
  * algorithm (the check behind every reported convergence). */
 int tbs_true_residual_norm(tbs_ctx *ctx, double *out);
+
+/* The true-residual check of TBS_ALGO_FP64 solves (on by default, no
+ * counterpart in the reference, which prints no residual): 1 on, 0 off. */
+int tbs_set_check(tbs_ctx *ctx, int on);
+
+/* The checks of the last solve: *true_norm = ||rhs + J U|| at the last
+ * check (-1 when none ran), *checks = checks run, *restarts = checks whose
+ * true residual missed the tolerance (the solve went on).  Any output may
+ * be NULL. */
+int tbs_solve_check(tbs_ctx *ctx, double *true_norm, int *checks, int *restarts);
+
+/* New values of the factored Jacobian's blocks (host pointers, the layout
+ * of tbs_set_jacobian) for the residual, keeping the line factorization:
+ * the factors of the old values become the preconditioner of the new
+ * system (a lagged factorization, as between the time steps of the flow
+ * solver the reference serves).  TBS_ALGO_REFERENCE and TBS_ALGO_FP64 (with
+ * the true-residual check on) then converge to the new system's solution,
+ * TBS_ALGO_MIXED's FP64 outer residual uses the new values.  Resets U to
+ * zero (or the starting solution) and R to its residual.  TBS_ALGO_PIJ
+ * refuses (re-factor).  No counterpart in the reference, which re-reads
+ * and re-factors (src/main.cxx:86-93,180-190). */
+int tbs_update_values(tbs_ctx *ctx, const double *jacD, const double *jacO1,
+                      const double *jacO2);
 
 /* Device bytes held by the context (replaces
  * gpu.device.memoryAllocated(), src/main.cxx:97-99). */
@@ -362,8 +399,9 @@ int tbs_selftest_timeout(tbs_ctx *ctx, long long budget_cycles);
  * "multi_resid/8" (every right-hand side active). */
 int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
 
-/* Linear residual R = rhs + J U (the rule of the reference's lineRes) and
- * its 2-norm for nvar = 9, on device buffers owned by the caller, without
+/* Linear residual R = rhs + D U + (sum over each cell's interior faces of
+ * offJ U_nbr) and its 2-norm for nvar = 9, on device buffers owned by the
+ * caller, without
  * allocating device memory -- for callers that cannot call cudaMalloc
  * (a solver whose memory pool owns the GPU, a time loop that must not
  * allocate).  No counterpart in the reference.  Arrays are device pointers
@@ -374,7 +412,9 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
  * cells (TBS_ERR_ARG beyond), kept by every GPU that loads the library
  * until exit, shared by all calls (calls that overlap on the GPU race).
  * The first call on a device looks up that array's address and should come
- * before any stream capture. */
+ * before any stream capture; the address is kept for the life of the
+ * process, so a device or primary-context reset (cudaDeviceReset) after
+ * that first call is not supported. */
 int tbs_residual_noalloc(int device_id, void *cuda_stream, int nelem,
                          const int *d_epoint, const int *d_ef, const int *d_fc,
                          const double *d_jacD, const double *d_jacO1,

@@ -76,7 +76,24 @@ def test_reference_arm_under_torchrun_rank0_only():
     line = lines[0]
     assert line["impl"] == "reference" and line["value"] > 0
     assert line["e2e"]["h2d_bytes_per_step"] == 0
-    assert line["cpu_baseline"]["kind"] == "port"
+    import oracle
+    # the reference's own kernels (oracle/_ref) where they were built, else the restatement
+    assert line["cpu_baseline"]["kind"] == ("reference" if oracle.ref_available() else "port")
+
+
+def test_reference_arm_does_not_load_the_product_library():
+    """The CPU reference arm builds its system with the oracle's numpy
+    generator: libtriblock.so must not be mapped in its process."""
+    code = ("import sys, runpy\n"
+            "sys.argv = ['bench.py', '--impl', 'reference', '--config', 'c1', '--steps', '1', "
+            "'--warmup', '0']\n"
+            "try:\n    runpy.run_path('bench.py', run_name='__main__')\n"
+            "except SystemExit as e:\n    assert not e.code, e.code\n"
+            "print('MAPS', 'libtriblock' in open('/proc/self/maps').read())\n")
+    p = subprocess.run([sys.executable, "-c", code], cwd=ROOT, capture_output=True, text=True,
+                       timeout=120)
+    assert p.returncode == 0, p.stderr[-2000:]
+    assert "MAPS False" in p.stdout, p.stdout[-2000:]
 
 
 def test_reference_byte_model():

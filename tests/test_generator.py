@@ -37,3 +37,22 @@ def test_generator_other_block_size():
     jacD, O1, O2, rhs = numpy_jacobian(5, m.nelem, m.nintface, 5.0, 3)
     np.testing.assert_array_equal(j.jacD, jacD)
     np.testing.assert_array_equal(j.rhs, rhs)
+
+
+def test_oracle_synthetic_inputs_equal_the_library():
+    """oracle/synthetic.py (what bench.py's CPU reference arm builds its
+    system from, without loading the product library) against the library's
+    generators, bit for bit."""
+    from oracle import synthetic
+    for (L, K, nv, shift, seed) in [(1, 1, 9, 9.0, 1), (1, 7, 9, 9.0, 2), (6, 1, 9, 4.0, 3),
+                                    (60, 64, 9, 9.0, 1), (7, 5, 5, 5.0, 4)]:
+        m = Mesh.structured(L, K, nvar=nv)
+        s = synthetic.structured_mesh(L, K, nvar=nv)
+        for f in Mesh.FIELDS:
+            np.testing.assert_array_equal(getattr(m, f), getattr(s, f), err_msg=f)
+        for f in ("nvar", "nelem", "nintface", "eftot", "nline", "nlineelem", "max_line_nelem"):
+            assert getattr(m, f) == getattr(s, f), f
+        j = Jacobian.generate(m, shift, seed)
+        for a, b in zip((j.jacD, j.jacO1, j.jacO2, j.rhs),
+                        synthetic.jacobian(nv, m.nelem, m.nintface, shift, seed)):
+            np.testing.assert_array_equal(a, b)

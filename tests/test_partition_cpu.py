@@ -68,6 +68,13 @@ class OracleSweeper:
                                    oracle._dp_(b.R))
         return self._norm()
 
+    def lines_vector(self, which, ks, buf, to_line):
+        off = 0
+        for k in ks:
+            n = int(self.part.mesh.linesize[k]) * self.nv
+            self.line_vector(which, k, buf[off:off + n], to_line)
+            off += n
+
     def line_vector(self, which, k, buf, to_line):
         m = self.part.mesh
         cells = m.lines[m.linepoint[k]:m.linepoint[k] + m.linesize[k]]
@@ -201,3 +208,32 @@ def test_gloo_ranks_match_whole_mesh_oracle(world):
     # every rank stopped at the same sweep: the whole-mesh U after `want` sweeps
     ref_n = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, want)
     assert np.array_equal(U, ref_n["U"])
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_torchrun_ranks_match_whole_mesh_oracle(world, tmp_path):
+    """The partitioned solve as separate processes launched by torchrun (the
+    launch and environment contract of bench.py --gpus N) on gloo: every
+    rank stops at the whole mesh's sweep count and the owned cells' U is
+    bit-identical to the oracle's whole-mesh sweep."""
+    import subprocess
+    lens, seed, tol = [6, 2, 9, 4, 8, 1, 7, 5], 9, 1e-11
+    cmd = [sys.executable, "-m", "torch.distributed.run", "--nnodes=1",
+           f"--nproc-per-node={world}", "--master-addr=127.0.0.1",
+           f"--master-port={_free_port()}",
+           os.path.join(ROOT, "tests", "partition_rank_worker.py"), str(tmp_path),
+           ",".join(map(str, lens)), str(seed), repr(tol)]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, OMP_NUM_THREADS="1"))
+    assert r.returncode == 0, r.stderr[-3000:]
+    mesh, jac = _problem(lens, seed)
+    ref = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, 40)
+    want = int(np.argmax(ref["hist"] <= tol * ref["hist"][0]))
+    U = np.zeros(9 * mesh.nelem)
+    for rank in range(world):
+        d = np.load(os.path.join(tmp_path, f"rank{rank}.npz"))
+        assert int(d["n"]) == want
+        assert np.all(np.abs(d["hist"] - ref["hist"][:want + 1]) <= NORM_TOL * ref["hist"][0])
+        U.reshape(-1, 9)[d["elems"]] = d["U"].reshape(-1, 9)
+    np.testing.assert_array_equal(U, oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs,
+                                                want)["U"])

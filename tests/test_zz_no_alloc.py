@@ -2,8 +2,10 @@
 allocate device memory (a solver whose pool owns the GPU, a time loop that
 must not allocate).  It keeps its work array in a fixed device array instead
 of cudaMalloc; here it is checked, on two calls in a row, against the
-context API's residual (tbs_get_residual / tbs_true_residual_norm) with the
-parity tolerance of the other GPU tests (1e-12 of the initial residual).
+context API's residual (tbs_get_residual / tbs_true_residual_norm) and the
+oracle's (the reference's residual rule restated on the CPU) with the
+parity tolerance of the other GPU tests (1e-12 of the initial residual),
+on the legacy default stream and on a stream of the caller's.
 This file sorts last so that a run stopping at the first failure has already
 run every other test."""
 import ctypes as C
@@ -11,6 +13,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
+import oracle
 from meshes import ragged_mesh
 from triblocksolve_b200 import ALGO_FP64, ALGO_REFERENCE, Jacobian, Mesh, Solver
 from triblocksolve_b200 import _native as N
@@ -23,12 +26,13 @@ def _dev(a):
     return torch.from_numpy(np.ascontiguousarray(a)).cuda()
 
 
-def _noalloc(mesh, bufs, U, want_R=True):
+def _noalloc(mesh, bufs, U, want_R=True, stream=None):
     import torch
     dU = _dev(U)
     dR = torch.empty_like(dU) if want_R else None
     norm = C.c_double(-1.0)
-    rc = N.lib.tbs_residual_noalloc(0, None, mesh.nelem, bufs["epoint"].data_ptr(),
+    torch.cuda.synchronize()
+    rc = N.lib.tbs_residual_noalloc(0, stream, mesh.nelem, bufs["epoint"].data_ptr(),
                                     bufs["ef"].data_ptr(), bufs["fc"].data_ptr(),
                                     bufs["jacD"].data_ptr(), bufs["jacO1"].data_ptr(),
                                     bufs["jacO2"].data_ptr(), bufs["rhs"].data_ptr(),
@@ -62,6 +66,33 @@ def test_noalloc_residual_matches_context(algo, make):
         assert abs(nrm - np.linalg.norm(R)) <= tol
     _, nrm = _noalloc(mesh, bufs, s.solution(), want_R=False)
     assert abs(nrm - s.true_residual_norm()) <= tol
+    s.close()
+
+
+def test_noalloc_on_a_caller_stream_matches_oracle():
+    """The call on a stream of the caller's (ticket clear, kernel, norm copy
+    and synchronisation all on it), two calls in a row, against the oracle's
+    residual (the reference's lineRes rule restated on the CPU) and the
+    context path."""
+    import torch
+    mesh = ragged_mesh([12, 3, 9, 16, 1, 7], seed=6)
+    jac = Jacobian.generate(mesh, 9.0, 5)
+    bufs = {f: _dev(getattr(mesh, f)) for f in ("epoint", "ef", "fc")}
+    bufs.update({f: _dev(getattr(jac, f)) for f in ("jacD", "jacO1", "jacO2", "rhs")})
+    s = Solver(0)
+    s.set_mesh(mesh)
+    s.set_jacobian(jac)
+    s.factor(ALGO_FP64)
+    st = torch.cuda.Stream()
+    tol = 1e-12 * np.linalg.norm(jac.rhs)
+    for sweeps in (1, 2):
+        s.sweep(sweeps)
+        U = s.solution()
+        R, nrm = _noalloc(mesh, bufs, U, stream=C.c_void_p(st.cuda_stream))
+        R_or = oracle.true_residual(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, U)
+        assert np.max(np.abs(R - R_or)) <= tol
+        assert abs(nrm - np.linalg.norm(R_or)) <= tol
+        assert abs(nrm - s.true_residual_norm()) <= tol
     s.close()
 
 

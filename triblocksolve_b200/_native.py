@@ -92,10 +92,14 @@ _sig("tbs_part_start", _i, _vp, _dp)
 _sig("tbs_part_solve_du", _i, _vp)
 _sig("tbs_part_line_res", _i, _vp, _dp)
 _sig("tbs_part_line_vector", _i, _vp, _i, _i, _vp, _i)
+_sig("tbs_part_lines_vector", _i, _vp, _i, _i, _ip, _vp, _i)
 _sig("tbs_get_solution", _i, _vp, _dp)
 _sig("tbs_get_residual", _i, _vp, _dp)
 _sig("tbs_get_update", _i, _vp, _dp)
 _sig("tbs_true_residual_norm", _i, _vp, _dp)
+_sig("tbs_set_check", _i, _vp, _i)
+_sig("tbs_solve_check", _i, _vp, _dp, _ip, _ip)
+_sig("tbs_update_values", _i, _vp, _dp, _dp, _dp)
 _sig("tbs_memory_allocated", _i, _vp, C.POINTER(C.c_size_t))
 _sig("tbs_set_inner_sweeps", _i, _vp, _i)
 _sig("tbs_tune_inner", _i, _vp, C.c_double, _i, _ip, _dp)

@@ -449,6 +449,9 @@ struct CondCtl {
     int use_cond;
     unsigned long long handle2; /* a second condition set to the same value (0: none) */
     int use2;
+    unsigned long long check;   /* set to 1 when a sweep's recursive residual meets the
+                                 * tolerance (the true-residual check's IF node) */
+    int use_check;
 };
 
 static NormSink sink(tbs_ctx *ctx, int is_start, CondCtl cc) {
@@ -461,6 +464,8 @@ static NormSink sink(tbs_ctx *ctx, int is_start, CondCtl cc) {
     ns.use_cond = cc.use_cond;
     ns.handle = cc.handle;
     ns.ntiles = ctx->nhalo > 0 ? ctx->L.ntile_own : 0;
+    ns.use_check = cc.use_check;
+    ns.check_handle = cc.check;
     return ns;
 }
 
@@ -608,6 +613,41 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
     return reduce(ctx, full_resid_blocks(ne), 0, cc);
 }
 
+/* Whether tbs_solve checks a converged solve against the true residual:
+ * TBS_ALGO_FP64 tracks its residual recursively (R = X dU over the
+ * cross-line blocks), so rounding, or Jacobian values changed after the
+ * factorization (tbs_update_values), can make it differ from rhs + J U.
+ * The other algorithms form the true residual every sweep (REFERENCE, the
+ * MIXED outer step) or are point sweeps (PIJ). */
+static bool checks_solve(const tbs_ctx *ctx) { return ctx->check && ctx->algo == TBS_ALGO_FP64; }
+
+/* The check of a converged TBS_ALGO_FP64 solve: R = rhs + J U from the
+ * original blocks (the rule of linesmoothLU_TriBlock_v3.okl:228-336), its
+ * norm recorded as NORM_CHECK (a pass ends the solve; a failure replaces
+ * the sweep's history entry) and the next sweep's input b = -Dinv R made
+ * from it, so that a failed check continues from the true residual. */
+static int check_true(tbs_ctx *ctx, CondCtl cc) {
+    cudaStream_t st = ctx->stream;
+    const FastLayout &L = ctx->L;
+    const int nv = ctx->nvar, ne = ctx->nelem;
+    if (nv == 9) {
+        RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                    L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
+                                                    ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
+                                                    ctx->d_partials2));
+    } else {
+        RUN("permute", launch_permute_to_elem(st, nv, ne, L.pos_of_elem, ctx->d_Up, ctx->d_U));
+        int rc = ref_residual(ctx, ctx->d_U, ctx->d_R);
+        if (rc) return rc;
+        RUN("permute", launch_permute_to_pos(st, nv, ne, L.pos_of_elem, ctx->d_R, ctx->d_Rp));
+    }
+    CondCtl c2 = cc;
+    c2.use_check = 0;
+    RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b,
+                                    sink(ctx, NORM_CHECK, c2), nullptr));
+    return TBS_OK;
+}
+
 int ctx_ensure_hist(tbs_ctx *ctx, int need) {
     if (need <= ctx->hist_cap) return TBS_OK;
     drop_graph(ctx);
@@ -626,8 +666,9 @@ int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
     h->max_sweeps = max_sweeps;
     h->hist_cap = ctx->hist_cap;
     const size_t off = offsetof(SolveState, tol);
+    const size_t end = offsetof(SolveState, hist_cap) + sizeof(int);
     CK(cudaMemcpyAsync(reinterpret_cast<char *>(ctx->d_state) + off,
-                       reinterpret_cast<char *>(h) + off, sizeof(SolveState) - off,
+                       reinterpret_cast<char *>(h) + off, end - off,
                        cudaMemcpyHostToDevice, ctx->stream));
     return TBS_OK;
 }
@@ -691,8 +732,11 @@ static int build_graph(tbs_ctx *ctx) {
     cudaGraphConditionalHandle hw, hf = 0;
     CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
     if (sched) CK(cudaGraphConditionalHandleCreate(&hf, g, 0, cudaGraphCondAssignDefault));
-    const CondCtl loop{(unsigned long long)hw, 1, 0, 0};
-    const CondCtl both{(unsigned long long)hw, 1, (unsigned long long)hf, sched ? 1 : 0};
+    const bool chk = checks_solve(ctx);
+    cudaGraphConditionalHandle hc = 0;
+    if (chk) CK(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
+    const CondCtl loop{(unsigned long long)hw, 1, 0, 0, (unsigned long long)hc, chk ? 1 : 0};
+    const CondCtl both{(unsigned long long)hw, 1, (unsigned long long)hf, sched ? 1 : 0, 0, 0};
     CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
     int rc = prime(ctx, both);
     cudaGraph_t firstg = nullptr, bodyg = nullptr;
@@ -703,8 +747,21 @@ static int build_graph(tbs_ctx *ctx) {
     if (rc == TBS_OK && ee != cudaSuccess) rc = ctx_fail(ctx, TBS_ERR_CUDA, std::string("end capture: ") + cudaGetErrorString(ee));
     if (rc == TBS_OK && sched)
         rc = capture_into(ctx, firstg, [&]() { return body(ctx, loop, ctx->inner_first); });
+    /* the loop's body; with the check, an IF node after the sweep runs the
+     * true residual when the sweep met the tolerance:
+     * while (go) { sweep; if (met) { check } } */
+    cudaGraph_t checkg = nullptr;
     if (rc == TBS_OK)
-        rc = capture_into(ctx, bodyg, [&]() { return body(ctx, loop, ctx->inner_sweeps); });
+        rc = capture_into(ctx, bodyg, [&]() {
+            int r = body(ctx, loop, ctx->inner_sweeps);
+            if (r == TBS_OK && chk) r = add_conditional(ctx, bodyg, hc, cudaGraphCondTypeIf, &checkg);
+            return r;
+        });
+    if (rc == TBS_OK && chk) {
+        CondCtl ck = loop;
+        ck.use_check = 0;
+        rc = capture_into(ctx, checkg, [&]() { return check_true(ctx, ck); });
+    }
     if (rc != TBS_OK) {
         drop_graph(ctx);
         return rc;
@@ -1156,14 +1213,26 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
         /* eager form with a host-side test, so that every kernel is timed */
         rc = prime(ctx, CondCtl{});
         if (rc) return rc;
+        bool checked = true; /* the primed residual is a true residual */
         for (;;) {
             rc = read_state(ctx);
             if (rc) return rc;
             const SolveState &S = *ctx->h_state;
-            const bool go = std::isfinite(S.last) && S.last > S.tol * S.norm0 && S.sweep < S.max_sweeps;
-            if (!go) break;
+            const bool met = std::isfinite(S.last) && S.last <= S.tol * S.norm0;
+            const bool go = std::isfinite(S.last) && !met && S.sweep < S.max_sweeps;
+            if (!go) {
+                if (met && !checked && checks_solve(ctx)) {
+                    /* as the graph's IF node: the true residual of the converged solve */
+                    rc = check_true(ctx, CondCtl{});
+                    if (rc) return rc;
+                    checked = true;
+                    continue;
+                }
+                break;
+            }
             rc = body(ctx, CondCtl{}, inner_for_next(ctx));
             if (rc) return rc;
+            checked = false;
         }
         prof_resolve(ctx);
     } else {
@@ -1288,6 +1357,64 @@ int tbs_true_residual_norm(tbs_ctx *ctx, double *out) {
     for (double v : part) s += v;
     *out = std::sqrt(s);
     return TBS_OK;
+    GUARD_END
+}
+
+int tbs_set_check(tbs_ctx *ctx, int on) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    if (on != 0 && on != 1) return ctx_fail(ctx, TBS_ERR_ARG, "tbs_set_check takes 0 or 1");
+    if (ctx->check != on) {
+        GUARD_BEGIN
+        CK(cudaSetDevice(ctx->device));
+        CK(cudaStreamSynchronize(ctx->stream));
+        drop_graph(ctx);
+        ctx->check = on;
+        return TBS_OK;
+        GUARD_END
+    }
+    return TBS_OK;
+}
+
+int tbs_solve_check(tbs_ctx *ctx, double *true_norm, int *checks, int *restarts) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    int rc = read_state(ctx);
+    if (rc) return rc;
+    if (true_norm) *true_norm = ctx->h_state->true_norm;
+    if (checks) *checks = ctx->h_state->checks;
+    if (restarts) *restarts = ctx->h_state->restarts;
+    return TBS_OK;
+    GUARD_END
+}
+
+int tbs_update_values(tbs_ctx *ctx, const double *jacD, const double *jacO1, const double *jacO2) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->factored) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_factor must come first");
+    if (!jacD || (ctx->nintface > 0 && (!jacO1 || !jacO2)))
+        return ctx_fail(ctx, TBS_ERR_ARG, "null Jacobian array");
+    if (ctx->algo == TBS_ALGO_PIJ)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
+                        "TBS_ALGO_PIJ tracks its residual with the factorization's face blocks; "
+                        "re-factor instead (tbs_set_jacobian + tbs_factor)");
+    if (ctx->algo == TBS_ALGO_FP64 && !ctx->check)
+        return ctx_fail(ctx, TBS_ERR_STATE,
+                        "TBS_ALGO_FP64 with the true-residual check off would converge to the "
+                        "factored system; enable it (tbs_set_check) or re-factor");
+    const size_t nb = (size_t)ctx->nvar * ctx->nvar;
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemcpyAsync(ctx->d_jacD, jacD, nb * ctx->nelem * sizeof(double), cudaMemcpyHostToDevice, st));
+    if (ctx->nintface) {
+        CK(cudaMemcpyAsync(ctx->d_O1, jacO1, nb * ctx->nintface * sizeof(double), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(ctx->d_O2, jacO2, nb * ctx->nintface * sizeof(double), cudaMemcpyHostToDevice, st));
+    }
+    if (ctx->algo == TBS_ALGO_MIXED && fullpos_ok(ctx))
+        RUN("fullpos_layout", launch_fullpos_layout(st, ctx->L, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                    ctx->d_Dp, ctx->d_XF));
+    return prime(ctx, CondCtl{});
     GUARD_END
 }
 
@@ -1441,7 +1568,7 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     double b = -1.0;
     if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out, own dU + U in/out */
         b = N * (blk + vec + 3 * vec) + X * (blk + 4.0 + vec);
-    else if (k == "fast_resid_rhs") /* Dinv, R in, b out */
+    else if (k == "fast_resid_rhs" || k == "fast_resid_check") /* Dinv, R in, b out */
         b = N * (blk + 2 * vec);
     else if (k == "fast_resid32_rhs")
         b = N * (blk + 2 * vec) / 2;
@@ -1572,6 +1699,36 @@ int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf, int t
         CK(cudaMemcpyAsync(v, d_buf, bytes, cudaMemcpyDefault, ctx->stream));
     else
         CK(cudaMemcpyAsync(d_buf, v, bytes, cudaMemcpyDefault, ctx->stream));
+    return TBS_OK;
+    GUARD_END
+}
+
+int tbs_part_lines_vector(tbs_ctx *ctx, int which, int nlines, const int *lines, double *d_buf,
+                          int to_line) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    if (which != TBS_VEC_SOLUTION && which != TBS_VEC_UPDATE)
+        return ctx_fail(ctx, TBS_ERR_ARG, "which must be TBS_VEC_SOLUTION or TBS_VEC_UPDATE");
+    if (nlines < 0 || (nlines > 0 && (!lines || !d_buf)))
+        return ctx_fail(ctx, TBS_ERR_ARG, "bad line list or null buffer");
+    double *vec = which == TBS_VEC_SOLUTION ? ctx->d_Up : ctx->d_dUp;
+    long long off = 0;
+    for (int k0 = 0; k0 < nlines; k0 += PACK_MAX_LINES) {
+        LinePack lp{};
+        lp.n = std::min(PACK_MAX_LINES, nlines - k0);
+        for (int j = 0; j < lp.n; ++j) {
+            const int l = lines[k0 + j];
+            if (l < 0 || l >= ctx->nline) return ctx_fail(ctx, TBS_ERR_ARG, "line out of range");
+            lp.start[j] = ctx->h_line_start[l];
+            lp.len[j] = ctx->h_linesize[l];
+            lp.off[j] = off;
+            off += (long long)ctx->h_linesize[l] * 9;
+        }
+        RUN("line_pack", launch_line_pack(ctx->stream, lp, vec, d_buf, to_line));
+    }
     return TBS_OK;
     GUARD_END
 }

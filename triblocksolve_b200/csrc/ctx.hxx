@@ -71,6 +71,8 @@ struct tbs_ctx {
     int inner_sweeps = 4;  /* TBS_ALGO_MIXED inner sweeps per outer step */
     int inner_first = 0;   /* > 0: the first outer step's inner sweeps */
     int outer_done = 0;    /* outer steps since the last prime (eager sequences) */
+    int check = 1;         /* tbs_solve checks a converged TBS_ALGO_FP64 solve against
+                            * the true residual (tbs_set_check) */
 
     /* ---- norms / solve state ---- */
     double *d_partials = nullptr, *d_partials2 = nullptr;

@@ -58,17 +58,40 @@ static __device__ bool finalize_total(const NormSink &ns, int n) {
         for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[w];
         const double nrm = sqrt(tot);
         SolveState *S = ns.state;
+        if (ns.is_start == NORM_CHECK) {
+            /* the true residual of a solve whose recursive residual passed */
+            const int sw = S->sweep;
+            const bool pass = isfinite(nrm) && nrm <= S->tol * S->norm0;
+            S->true_norm = nrm;
+            S->checks += 1;
+            if (!pass) {
+                S->restarts += 1;
+                if (sw < S->hist_cap) ns.hist[sw] = nrm;
+                S->last = nrm;
+            }
+            const bool go = !pass && isfinite(nrm) && sw < S->max_sweeps;
+            if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
+            *ns.counter = 0u;
+            return true;
+        }
         if (ns.is_start) {
             S->sweep = 0;
             S->norm0 = nrm;
+            S->true_norm = -1.0;
+            S->checks = 0;
+            S->restarts = 0;
         } else {
             S->sweep += 1;
         }
         const int sw = S->sweep;
         if (sw < S->hist_cap) ns.hist[sw] = nrm;
         S->last = nrm;
-        const bool go = isfinite(nrm) && nrm > S->tol * S->norm0 && sw < S->max_sweeps;
+        const bool met = isfinite(nrm) && nrm <= S->tol * S->norm0;
+        const bool go = isfinite(nrm) && !met && sw < S->max_sweeps;
         if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
+        if (ns.use_check)
+            cudaGraphSetConditional((cudaGraphConditionalHandle)ns.check_handle,
+                                    (!ns.is_start && met) ? 1u : 0u);
         *ns.counter = 0u;
     }
     return true;

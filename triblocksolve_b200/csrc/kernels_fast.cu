@@ -105,6 +105,9 @@ __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, S
         if (is_start) {
             state->sweep = 0;
             state->norm0 = nrm;
+            state->true_norm = -1.0;
+            state->checks = 0;
+            state->restarts = 0;
         } else {
             state->sweep += 1;
         }
@@ -1543,6 +1546,28 @@ int fast_prepare(const FastLayout &L) {
 }
 
 int fast_kernels_init() { return 0; }
+
+/* one CTA per line of the pack; the descriptor travels as a kernel parameter */
+__global__ void __launch_bounds__(256) line_pack_kernel(LinePack lp, double *__restrict__ vec,
+                                                        double *__restrict__ buf, int to_line) {
+    const int k = blockIdx.x;
+    if (k >= lp.n) return;
+    const long long n = (long long)lp.len[k] * NV;
+    double *v = vec + (long long)lp.start[k] * NV;
+    double *b = buf + lp.off[k];
+    for (long long t = threadIdx.x; t < n; t += blockDim.x) {
+        if (to_line)
+            v[t] = b[t];
+        else
+            b[t] = v[t];
+    }
+}
+
+int launch_line_pack(cudaStream_t st, const LinePack &lp, double *vec, double *buf, int to_line) {
+    if (lp.n <= 0) return 0;
+    line_pack_kernel<<<lp.n, 256, 0, st>>>(lp, vec, buf, to_line);
+    return (int)cudaGetLastError();
+}
 
 /* ============================================ true residual, any ordering
  * R(pos(e)) = rhs(e) + D_e U(pos(e)) + sum_{faces} offJ U(pos(nbr)) with the

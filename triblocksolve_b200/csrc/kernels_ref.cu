@@ -152,7 +152,10 @@ int launch_ref_line_lu(cudaStream_t st, int nv, int nline, const int *fc, const 
         ref_line_lu_kernel<9><<<nline, 32, smem, st>>>(nv, nline, fc, linesize, linepoint, lines,
                                                        lineface, DLU, O1, O2, DinvC, status);
     } else {
-        if (smem > 48 * 1024) smem_raise((const void *)ref_line_lu_kernel<0>, smem);
+        if (smem > 48 * 1024) {
+            const int e = smem_raise((const void *)ref_line_lu_kernel<0>, smem);
+            if (e != 0) return e;
+        }
         ref_line_lu_kernel<0><<<nline, 32, smem, st>>>(nv, nline, fc, linesize, linepoint, lines,
                                                        lineface, DLU, O1, O2, DinvC, status);
     }

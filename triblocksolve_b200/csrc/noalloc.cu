@@ -23,7 +23,9 @@
  *     race on it, so callers must serialise them;
  *   - the first call on a device looks up the array's device address
  *     (cudaGetSymbolAddress with that device current); that first call
- *     should come before any stream capture.
+ *     should come before any stream capture.  The address is kept for the
+ *     life of the process: resetting the device or its primary context
+ *     (cudaDeviceReset) after the first call is not supported.
  */
 #include "tbs_internal.hxx"
 

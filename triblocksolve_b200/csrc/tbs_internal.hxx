@@ -64,6 +64,11 @@ struct SolveState {
     double tol;        /* relative tolerance */
     int max_sweeps;
     int hist_cap;      /* entries available in hist */
+    /* checks of a converged solve against the true residual (device-written;
+     * reset by the solve's start) */
+    double true_norm;  /* ||rhs + J U|| at the last check, -1 when none ran */
+    int checks;        /* checks run in the current solve */
+    int restarts;      /* checks that failed: the solve went on from the true residual */
 };
 
 /* ------------------------------------------------- fast (line-ordered) layout
@@ -174,12 +179,20 @@ struct NormSink {
     unsigned *counter;           /* zero between launches */
     SolveState *state;           /* null: partials only */
     double *hist;
-    int is_start;
+    int is_start;                /* 1: the norm opens a solve; 0: one more sweep;
+                                  * NORM_CHECK: the true residual of a converged solve */
     int use_cond;
     unsigned long long handle;   /* cudaGraphConditionalHandle */
     int ntiles;                  /* > 0: the norm sums the first ntiles tiles only (the
                                   * owned lines of a line partition); 0: every tile */
+    int use_check;               /* a sweep's norm also sets check_handle: 1 when the
+                                  * recursive residual has met the tolerance */
+    unsigned long long check_handle;
 };
+/* NormSink::is_start of the check of a converged solve: a norm at or below
+ * the tolerance ends the solve with the history unchanged; a larger one
+ * replaces the sweep's entry and the solve goes on from it */
+constexpr int NORM_CHECK = 2;
 
 /* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
  * b = -sum X dU, no norm; 4: b = sum X dU - Rsrc (the product with J of
@@ -193,6 +206,17 @@ template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
                        const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
 int fast_kernels_init();
+/* Several lines' vectors packed into (or unpacked from) one contiguous
+ * buffer by one launch: line k's span is [start[k]*9, start[k]*9 + len[k]*9)
+ * of `vec` and [off[k], off[k] + len[k]*9) of `buf`. */
+constexpr int PACK_MAX_LINES = 64;
+struct LinePack {
+    int n;
+    int start[PACK_MAX_LINES];
+    int len[PACK_MAX_LINES];
+    long long off[PACK_MAX_LINES];
+};
+int launch_line_pack(cudaStream_t st, const LinePack &lp, double *vec, double *buf, int to_line);
 int fast_prepare(const FastLayout &L);
 int full_resid_blocks(int nelem);
 /* rhs may be null (zero): Rp = J U, the matrix-vector product */

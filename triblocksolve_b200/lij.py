@@ -383,6 +383,22 @@ class Solver:
         self._chk(N.lib.tbs_true_residual_norm(self.ctx, C.byref(v)))
         return v.value
 
+    def set_check(self, on: bool = True):
+        """TBS_ALGO_FP64: check a converged solve against rhs + J U (default on)."""
+        self._chk(N.lib.tbs_set_check(self.ctx, 1 if on else 0))
+
+    def solve_check(self):
+        """(true residual norm at the last check or -1, checks, restarts) of the last solve."""
+        t, c, r = C.c_double(), C.c_int(), C.c_int()
+        self._chk(N.lib.tbs_solve_check(self.ctx, C.byref(t), C.byref(c), C.byref(r)))
+        return t.value, c.value, r.value
+
+    def update_values(self, jacD, jacO1, jacO2):
+        """New block values for the residual, the factorization kept (a lagged
+        factorization): the solve converges to the new system."""
+        a = [np.ascontiguousarray(x, np.float64) for x in (jacD, jacO1, jacO2)]
+        self._chk(N.lib.tbs_update_values(self.ctx, *[N.dptr(x) for x in a]))
+
     def profile(self, on: bool = True):
         self._chk(N.lib.tbs_profile_enable(self.ctx, 1 if on else 0))
 

@@ -198,6 +198,14 @@ class PartitionSolver(Solver):
         self._chk(N.lib.tbs_part_line_res(self.ctx, C.byref(n)))
         return n.value
 
+    def lines_vector(self, which: int, lines, buf, to_line: bool) -> None:
+        """Several lines' vectors packed back to back into ``buf`` (or
+        unpacked from it) by one launch."""
+        ls = np.ascontiguousarray(lines, np.int32)
+        ptr = buf if isinstance(buf, int) else buf.data_ptr()
+        self._chk(N.lib.tbs_part_lines_vector(self.ctx, which, int(ls.size), N.iptr(ls),
+                                              C.c_void_p(ptr), 1 if to_line else 0))
+
     def line_vector(self, which: int, line: int, buf, to_line: bool) -> None:
         """Copy a line's vector to / from ``buf`` (a CUDA tensor of
         linesize * 9 doubles, or its address)."""
@@ -280,9 +288,9 @@ class DistExchange:
             off += n
 
     def exchange(self, which: int) -> None:
+        # one pack launch per neighbour and direction
         for q, ks in sorted(self.part.sends.items()):
-            for k, view in self._lines(self.sendbufs[q], ks):
-                self.sweeper.line_vector(which, k, view, False)
+            self.sweeper.lines_vector(which, ks, self.sendbufs[q], False)
         ops = [self.dist.P2POp(self.dist.isend, self.sendbufs[q], q, self.group)
                for q in sorted(self.sendbufs)]
         ops += [self.dist.P2POp(self.dist.irecv, self.recvbufs[q], q, self.group)
@@ -291,8 +299,7 @@ class DistExchange:
             for w in self.dist.batch_isend_irecv(ops):
                 w.wait()
         for q, ks in sorted(self.part.recvs.items()):
-            for k, view in self._lines(self.recvbufs[q], ks):
-                self.sweeper.line_vector(which, k, view, True)
+            self.sweeper.lines_vector(which, ks, self.recvbufs[q], True)
 
     def allreduce_sum(self, x: float) -> float:
         t = self.torch.tensor([x], dtype=self.torch.float64, device=self.device)
