@@ -1,6 +1,8 @@
 """Regenerate the committed fixtures in tests/golden.
 
-Run from the repository root:  python tests/golden/make_golden.py [REFERENCE_DIR]
+Run from the repository root:  python tests/golden/make_golden.py REFERENCE_DIR
+
+REFERENCE_DIR is a checkout of the reference (read only).
 
 Fixtures
   ex05_mesh.json   facts of the reference's only real data file,
@@ -11,9 +13,11 @@ Fixtures
   ex06_sizes.json  sizes and oids of the ex06 Git-LFS pointer files
                    (the data are not in the reference checkout); the size
                    formulas of both layouts must give these byte counts.
-  lij_60x64.json   oracle output (regression fixture, not a reference pin):
-                   per-sweep residual norms and solution checksums of the
-                   60x64 / shift 9 / seed 1 problem for 20 sweeps.
+  lij_60x64.json   output of the reference's own kernels (OKL translated to
+                   C into oracle/_ref by oracle/okl2c.py, built from
+                   REFERENCE_DIR here): per-sweep residual norms and
+                   solution checksums of the 60x64 / shift 9 / seed 1
+                   problem for 20 sweeps.
 """
 from __future__ import annotations
 
@@ -60,29 +64,36 @@ def ex06(refdir: str) -> dict:
     return out
 
 
-def lij_golden() -> dict:
+def lij_golden(refdir: str) -> dict:
     import oracle
     from triblocksolve_b200 import Jacobian, Mesh
+    if not oracle.ref_available():
+        oracle.build_ref(refdir)
     mesh = Mesh.structured(60, 64)
     jac = Jacobian.generate(mesh, 9.0, 1)
-    r = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, 20, threads=1)
+    r = oracle.ref_lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, 20, threads=1)
     U = r["U"]
     return {"problem": {"L": 60, "K": 64, "shift": 9.0, "seed": 1, "sweeps": 20},
             "hist": [float(v) for v in r["hist"]],
             "U_sum": float(U.sum()), "U_sumsq": float((U * U).sum()),
             "U_first": [float(v) for v in U[:9]], "U_last": [float(v) for v in U[-9:]],
-            "note": "oracle output (lij_oracle.c, single thread); regression fixture"}
+            "note": "the reference's own kernels (lineLU_v2.okl, linesmoothLU_TriBlock_v3.okl, "
+                    "linesmoothLU_v5.okl translated to C by oracle/okl2c.py), one thread"}
 
 
 def main():
-    refdir = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
-    if os.path.isdir(refdir):
-        with open(os.path.join(HERE, "ex05_mesh.json"), "w") as f:
-            json.dump(ex05(refdir), f, indent=1)
-        with open(os.path.join(HERE, "ex06_sizes.json"), "w") as f:
-            json.dump(ex06(refdir), f, indent=1)
+    import argparse
+    ap = argparse.ArgumentParser(description="regenerate tests/golden fixtures")
+    ap.add_argument("reference_dir", help="a checkout of the reference (read only)")
+    refdir = ap.parse_args().reference_dir
+    if not os.path.isdir(os.path.join(refdir, "src", "okl")):
+        ap.error(f"{refdir} is not a checkout of the reference")
+    with open(os.path.join(HERE, "ex05_mesh.json"), "w") as f:
+        json.dump(ex05(refdir), f, indent=1)
+    with open(os.path.join(HERE, "ex06_sizes.json"), "w") as f:
+        json.dump(ex06(refdir), f, indent=1)
     with open(os.path.join(HERE, "lij_60x64.json"), "w") as f:
-        json.dump(lij_golden(), f, indent=1)
+        json.dump(lij_golden(refdir), f, indent=1)
     print("fixtures written to", HERE)
 
 
