@@ -412,6 +412,7 @@ def run_batch(args):
                 "sweeps_min": int(sw.min()), "sweeps_max": int(sw.max()),
                 "inner_sweeps": inner,
                 "schedule": {"ctas_per_sm": ctas, "stages": stages,
+                             "warps_per_line": batch.warps_per_line(),
                              "order": "longest lines first" if order == 0 else "mesh order",
                              "tuned_thomas_ms": round(tune_ms, 4)},
                 "setup_s": round(setup_s, 1),

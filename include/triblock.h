@@ -452,16 +452,24 @@ int tbs_batch_set_stream(tbs_batch *batch, void *cuda_stream);
 int tbs_batch_solve(tbs_batch *batch, double rel_tol, int max_sweeps,
                     int *sweeps_out, double *hist_out);
 
-/* Shape of the persistent Thomas launch: CTAs (one warp each, one line at
- * a time) per SM, bulk-copy ring stages (2..8), line order (0: longest
- * first, 1: mesh order).  TBS_ERR_ARG when the shape does not fit. */
+/* Shape of the persistent Thomas launch: CTAs (each one line at a time)
+ * per SM, bulk-copy ring stages (2..8), line order (0: longest first,
+ * 1: mesh order).  TBS_ERR_ARG when the shape does not fit. */
 int tbs_batch_set_schedule(tbs_batch *batch, int ctas_per_sm, int stages, int order);
 int tbs_batch_get_schedule(const tbs_batch *batch, int *ctas_per_sm, int *stages,
                            int *order);
 
-/* Autotuner: times the persistent Thomas launch over every CTAs-per-SM /
- * stage count / line order that fits, keeps the fastest and reports it and
- * its time per launch in ms (any output may be NULL). */
+/* Warps per line of the persistent Thomas launch: 1 (the warp running the
+ * line's two chains also issues its staging copies) or 2 (a second warp
+ * issues them, so that the chains never stop for it).  Results are
+ * bit-identical either way; CTAs per SM are lowered to what fits. */
+int tbs_batch_set_warps_per_line(tbs_batch *batch, int warps);
+int tbs_batch_get_warps_per_line(const tbs_batch *batch, int *warps);
+
+/* Autotuner: times the persistent Thomas launch over every warps-per-line
+ * / CTAs-per-SM / stage count / line order that fits, keeps the fastest
+ * and reports it and its time per launch in ms (any output may be NULL;
+ * tbs_batch_get_warps_per_line gives the warps). */
 int tbs_batch_tune(tbs_batch *batch, int *ctas_per_sm, int *stages, int *order,
                    double *best_ms);
 

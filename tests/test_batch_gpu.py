@@ -104,17 +104,21 @@ def test_batch_schedules_agree(algo):
         tol = 1e-12 if algo == ALGO_FP64 else 1e-10
         sw0, h0 = b.solve(tol, 80)
         u0 = [s.solution() for s, _, _ in members]
-        for ctas, stages, order in [(1, 2, 0), (3, 3, 1), (2, 4, 0), (8, 2, 1)]:
-            b.set_schedule(ctas, stages, order)
-            assert b.schedule() == (ctas, stages, order)
-            sw, h = b.solve(tol, 80)
-            np.testing.assert_array_equal(sw, sw0)
-            for k, (s, _, _) in enumerate(members):
-                np.testing.assert_array_equal(h[k], h0[k])
-                np.testing.assert_array_equal(s.solution(), u0[k])
+        for warps in (1, 2):
+            b.set_warps_per_line(warps)
+            assert b.warps_per_line() == warps
+            for ctas, stages, order in [(1, 2, 0), (3, 3, 1), (2, 4, 0), (6, 2, 1)]:
+                b.set_schedule(ctas, stages, order)
+                assert b.schedule() == (ctas, stages, order)
+                for _ in range(2):  # two solves in a row
+                    sw, h = b.solve(tol, 80)
+                    np.testing.assert_array_equal(sw, sw0)
+                    for k, (s, _, _) in enumerate(members):
+                        np.testing.assert_array_equal(h[k], h0[k])
+                        np.testing.assert_array_equal(s.solution(), u0[k])
         ctas, stages, order, ms = b.tune()
         assert ctas >= 1 and 2 <= stages <= 4 and order in (0, 1) and ms > 0
-        assert b.schedule() == (ctas, stages, order)
+        assert b.schedule() == (ctas, stages, order) and b.warps_per_line() in (1, 2)
         sw, h = b.solve(tol, 80)
         np.testing.assert_array_equal(sw, sw0)
     finally:

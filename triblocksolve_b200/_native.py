@@ -119,6 +119,8 @@ _sig("tbs_batch_solve", _i, _vp, C.c_double, _i, _ip, _dp)
 _sig("tbs_batch_set_schedule", _i, _vp, _i, _i, _i)
 _sig("tbs_batch_get_schedule", _i, _vp, _ip, _ip, _ip)
 _sig("tbs_batch_tune", _i, _vp, _ip, _ip, _ip, _dp)
+_sig("tbs_batch_set_warps_per_line", _i, _vp, _i)
+_sig("tbs_batch_get_warps_per_line", _i, _vp, _ip)
 _sig("tbs_batch_set_inner_sweeps", _i, _vp, _i)
 _sig("tbs_batch_set_inner_schedule", _i, _vp, _i, _i)
 _sig("tbs_batch_tune_inner", _i, _vp, C.c_double, _i, _ip, _ip, _dp)

@@ -235,9 +235,9 @@ int engine_init(Engine &e, int device, cudaStream_t stream, int algo) {
     ECK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
     ECK(cudaMemsetAsync(e.d_ctl, 0, sizeof(BatchCtl), e.stream));
     /* default schedule: 2 stages, as many CTAs per SM as fit, at most 8 */
-    const int fit = algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(2) : thomas_batch_fit<float>(2);
+    const int fit = algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(2, 1) : thomas_batch_fit<float>(2, 1);
     if (fit < 1) return efail(e, TBS_ERR_CUDA, "the batched Thomas kernel does not fit on an SM");
-    e.sched = BatchSched{std::min(fit, 8), 2};
+    e.sched = BatchSched{std::min(fit, 8), 2, 1};
     ECK(cudaStreamSynchronize(e.stream));
     return TBS_OK;
 }
@@ -791,11 +791,14 @@ static int engine_upload_lines(Engine &e) {
 }
 
 int engine_set_schedule(Engine &e, BatchSched s, int order) {
-    const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(s.stages)
-                                            : thomas_batch_fit<float>(s.stages);
-    if (s.stages < 2 || s.stages > 8 || s.ctas_per_sm < 1 || s.ctas_per_sm > fit)
+    if (s.warps != 1 && s.warps != 2) return efail(e, TBS_ERR_ARG, "warps per line must be 1 or 2");
+    if (s.stages < 2 || s.stages > 8) return efail(e, TBS_ERR_ARG, "stages must be in 2..8");
+    const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(s.stages, s.warps)
+                                            : thomas_batch_fit<float>(s.stages, s.warps);
+    if (s.ctas_per_sm < 1 || s.ctas_per_sm > fit)
         return efail(e, TBS_ERR_ARG, "schedule does not fit: at most " + std::to_string(fit) +
-                                         " CTAs per SM with " + std::to_string(s.stages) + " stages");
+                                         " CTAs per SM with " + std::to_string(s.stages) +
+                                         " stages and " + std::to_string(s.warps) + " warp(s) per line");
     const bool new_order = order != e.order;
     e.sched = s;
     e.order = order;
@@ -824,12 +827,13 @@ int engine_tune(Engine &e, BatchSched *best_s, int *best_o, double *best_ms) {
     for (int o = 0; o < 2 && !rc; ++o) {
         e.order = o;
         rc = engine_upload_lines(e);
+        for (int wpl = 1; wpl <= 2 && !rc; ++wpl)
         for (int ns = 2; ns <= 4 && !rc; ++ns) {
-            const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(ns)
-                                                    : thomas_batch_fit<float>(ns);
+            const int fit = e.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(ns, wpl)
+                                                    : thomas_batch_fit<float>(ns, wpl);
             for (int cps : cand_ctas) {
                 if (cps > fit || rc) continue;
-                e.sched = BatchSched{cps, ns};
+                e.sched = BatchSched{cps, ns, wpl};
                 auto launch = [&]() {
                     return e.algo == TBS_ALGO_FP64
                                ? launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines,
@@ -1059,8 +1063,28 @@ int tbs_batch_set_schedule(tbs_batch *b, int ctas_per_sm, int stages, int order)
     if (order != 0 && order != 1) return bfail(b, TBS_ERR_ARG, "bad line order");
     BGUARD_BEGIN
     if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
-    return engine_set_schedule(b->eng, BatchSched{ctas_per_sm, stages}, order);
+    return engine_set_schedule(b->eng, BatchSched{ctas_per_sm, stages, b->eng.sched.warps}, order);
     BGUARD_END
+}
+
+int tbs_batch_set_warps_per_line(tbs_batch *b, int warps) {
+    if (!b) return bfail(nullptr, TBS_ERR_ARG, "null batch");
+    if (warps != 1 && warps != 2) return bfail(b, TBS_ERR_ARG, "warps per line must be 1 or 2");
+    BGUARD_BEGIN
+    if (cudaSetDevice(b->eng.device) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "cudaSetDevice failed");
+    BatchSched s = b->eng.sched;
+    const int fit = b->eng.algo == TBS_ALGO_FP64 ? thomas_batch_fit<double>(s.stages, warps)
+                                                 : thomas_batch_fit<float>(s.stages, warps);
+    s.warps = warps;
+    s.ctas_per_sm = std::max(1, std::min(s.ctas_per_sm, fit));
+    return engine_set_schedule(b->eng, s, b->eng.order);
+    BGUARD_END
+}
+
+int tbs_batch_get_warps_per_line(const tbs_batch *b, int *warps) {
+    if (!b || !warps) return bfail(const_cast<tbs_batch *>(b), TBS_ERR_ARG, "null argument");
+    *warps = b->eng.sched.warps;
+    return TBS_OK;
 }
 
 int tbs_batch_get_schedule(const tbs_batch *b, int *ctas_per_sm, int *stages, int *order) {

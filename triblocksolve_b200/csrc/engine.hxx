@@ -51,7 +51,7 @@ struct Engine {
     int inner = 4;            /* TBS_ALGO_MIXED inner sweeps per outer step */
     int inner_first = 0;      /* > 0: the first outer step's (all members fresh together) */
     cudaStream_t stream = nullptr;
-    BatchSched sched{8, 2};
+    BatchSched sched{8, 2, 1};
     int order = 0;            /* Thomas items: 0 longest lines first, 1 mesh order */
     int max_nx = 0;           /* widest member (shared-memory size of the residual) */
     std::string err;

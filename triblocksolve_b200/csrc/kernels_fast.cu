@@ -1125,12 +1125,16 @@ __device__ __forceinline__ bool thomas_line(
         }
     };
     if (producer) {
-        /* every job as soon as the consumer has released its stage */
+        /* every job as soon as the consumer has released its stage.  Each
+         * empty barrier completes one phase per job consumed from its stage,
+         * as each full barrier does per job landed, so the parity bits of
+         * `pbase` serve both (a persistent CTA carries them across lines);
+         * job j >= NS waits for the consumption of job j - NS */
         if (lane == 0) {
             for (int job = 0; job < njobs; ++job) {
                 if (*ws_abort) break;
                 const int s = job % NS;
-                if (job >= NS && !mbar_wait(&empty[s], (uint32_t)((job / NS - 1) & 1))) {
+                if (job >= NS && !mbar_wait(&empty[s], parity(job - NS))) {
                     atomicOr(status, ST_TIMEOUT);
                     break;
                 }
@@ -1140,6 +1144,10 @@ __device__ __forceinline__ bool thomas_line(
         }
         __syncwarp();
         __syncthreads(); /* meets the consumer's */
+        for (int s = 0; s < NS && s < njobs; ++s) {
+            const int cnt = (njobs - 1 - s) / NS + 1;
+            pbase ^= (uint32_t)(cnt & 1) << s;
+        }
         return true;
     }
     int issued = 0;
@@ -1393,6 +1401,61 @@ __global__ void __launch_bounds__(32) fast_thomas_batch_kernel(
             break;
     }
     if (lane == 0) {
+        __threadfence();
+        if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
+            queue[0] = 0u;
+            queue[1] = 0u;
+            __threadfence();
+        }
+    }
+}
+
+/* The same persistent loop with two warps per CTA: warp 1 issues every
+ * line's staging copies, warp 0 runs its chains (thomas_line's
+ * warp-specialised form, bit-identical results).  Thread 0 takes the next
+ * item for both warps; the staging barriers' parities carry across lines
+ * in `pbase`, kept the same in both warps. */
+template <typename T, int P>
+__global__ void __launch_bounds__(64) fast_thomas_batch_ws_kernel(
+    const ThomasSys<T> *__restrict__ sys, const WorkItem *__restrict__ work,
+    const int *__restrict__ nwork_p, const int *__restrict__ active, unsigned *queue, int NS,
+    unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ int s_item, s_stop;
+    const int nwork = *nwork_p;
+    if (threadIdx.x == 0) {
+        uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
+        for (int s = 0; s < NS; ++s) {
+            mbar_init(&bars[s], 1);
+            mbar_init(&bars[8 + s], 1);
+        }
+        int *cnt = reinterpret_cast<int *>(smem + 128);
+        cnt[0] = 0;
+        cnt[1] = 0;
+        s_stop = 0;
+        mbar_fence_init();
+    }
+    __syncthreads();
+    const uint64_t pol = threadIdx.x == 32 ? policy_evict_first() : 0;
+    uint32_t pbase = 0;
+    for (;;) {
+        if (threadIdx.x == 0) s_item = (int)atomicAdd(queue, 1u);
+        __syncthreads();
+        const int w = s_item;
+        __syncthreads(); /* s_item is read before thread 0 takes the next item */
+        if (w >= nwork) break;
+        const WorkItem it = work[w];
+        if (active && !active[it.sys]) continue;
+        const ThomasSys<T> S = sys[it.sys];
+        const int l = it.unit;
+        const bool ok = thomas_line<T, P, false, true>(NS, 2, S.line_start[l], S.line_len[l],
+                                                       S.line_twist[l], S.G, S.Gam, S.b, S.y, S.dU,
+                                                       nullptr, status, smem, pbase, pol);
+        if (!ok && (threadIdx.x & 31) == 0) s_stop = 1;
+        __syncthreads();
+        if (s_stop) break;
+    }
+    if (threadIdx.x == 0) {
         __threadfence();
         if (atomicAdd(queue + 1, 1u) == gridDim.x - 1) {
             queue[0] = 0u;
@@ -1971,18 +2034,19 @@ static int sm_count() {
 }
 
 template <typename T>
-size_t thomas_batch_smem(int stages) {
-    return 128 + (size_t)stages * 2 * THOMAS_P * (NB + NV) * sizeof(T) + 80 * sizeof(T);
+size_t thomas_batch_smem(int stages, int warps) {
+    return (warps == 2 ? thomas_hdr<true>() : thomas_hdr<false>()) +
+           (size_t)stages * 2 * THOMAS_P * (NB + NV) * sizeof(T) + 80 * sizeof(T);
 }
 
 template <typename T>
-int thomas_batch_fit(int stages) {
+int thomas_batch_fit(int stages, int warps) {
     int n = 0;
-    const size_t smem = thomas_batch_smem<T>(stages);
-    if (smem_raise((const void *)fast_thomas_batch_kernel<T, THOMAS_P>, smem) != cudaSuccess)
-        return 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fast_thomas_batch_kernel<T, THOMAS_P>, 32,
-                                                      smem) != cudaSuccess)
+    const size_t smem = thomas_batch_smem<T>(stages, warps);
+    const void *fn = warps == 2 ? (const void *)fast_thomas_batch_ws_kernel<T, THOMAS_P>
+                                : (const void *)fast_thomas_batch_kernel<T, THOMAS_P>;
+    if (smem_raise(fn, smem) != cudaSuccess) return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, fn, 32 * warps, smem) != cudaSuccess)
         return 0;
     return n;
 }
@@ -1991,11 +2055,16 @@ template <typename T>
 int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
                         const WorkItem *work, const int *nwork, const int *active, unsigned *queue,
                         unsigned *status) {
-    if (bs.stages < 2 || bs.stages > 8 || bs.ctas_per_sm < 1) return (int)cudaErrorInvalidValue;
-    const size_t smem = thomas_batch_smem<T>(bs.stages);
+    if (bs.stages < 2 || bs.stages > 8 || bs.ctas_per_sm < 1 || (bs.warps != 1 && bs.warps != 2))
+        return (int)cudaErrorInvalidValue;
+    const size_t smem = thomas_batch_smem<T>(bs.stages, bs.warps);
     const int grid = bs.ctas_per_sm * sm_count();
-    fast_thomas_batch_kernel<T, THOMAS_P><<<grid, 32, smem, st>>>(sys, work, nwork, active, queue,
-                                                                   bs.stages, status);
+    if (bs.warps == 2)
+        fast_thomas_batch_ws_kernel<T, THOMAS_P><<<grid, 64, smem, st>>>(sys, work, nwork, active,
+                                                                          queue, bs.stages, status);
+    else
+        fast_thomas_batch_kernel<T, THOMAS_P><<<grid, 32, smem, st>>>(sys, work, nwork, active,
+                                                                       queue, bs.stages, status);
     return (int)cudaGetLastError();
 }
 
@@ -2257,10 +2326,10 @@ int fullpos_prepare(const FastLayout &L) {
     return set_smem((const void *)full_resid_pos_kernel, fullpos_smem_bytes(L.nxf));
 }
 
-template size_t thomas_batch_smem<double>(int);
-template size_t thomas_batch_smem<float>(int);
-template int thomas_batch_fit<double>(int);
-template int thomas_batch_fit<float>(int);
+template size_t thomas_batch_smem<double>(int, int);
+template size_t thomas_batch_smem<float>(int, int);
+template int thomas_batch_fit<double>(int, int);
+template int thomas_batch_fit<float>(int, int);
 template int launch_thomas_batch<double>(cudaStream_t, const BatchSched &, const ThomasSys<double> *,
                                          const WorkItem *, const int *, const int *, unsigned *,
                                          unsigned *);
@@ -2655,11 +2724,18 @@ int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const doub
  * ended and keeps the graph's loop running while any is active. */
 static size_t multi_resid_smem(int nx, int nr) {
     const int nxa = nx > 0 ? nx : 1;
+    const int ng = nr < MULTI_G ? nr : MULTI_G;
     return 128 + (size_t)RES_TILE * NB * sizeof(double) * (1 + nx) +
-           (size_t)nr * nxa * RES_TILE * NV * sizeof(double) +
-           (size_t)nr * RES_TILE * NV * sizeof(double);
+           (size_t)ng * nxa * RES_TILE * NV * sizeof(double) +
+           (size_t)ng * RES_TILE * NV * sizeof(double);
 }
 
+/* A work item is one tile and a group of up to MULTI_G of the active
+ * right-hand sides (the k-th active ones, k in [kb, kb + kn)): the groups
+ * of a tile are consecutive items, so the CTAs that take them run at about
+ * the same time and the second fetch of the tile's blocks is served by L2.
+ * Half the right-hand sides per item halves the registers and staging of a
+ * CTA, so more CTAs share an SM and hide each other's load rounds. */
 template <int MODE>
 __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     MultiSys M, const double *__restrict__ Dinv, const double *__restrict__ X,
@@ -2667,7 +2743,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     int use_cond, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned amask_s, ticket;
-    __shared__ double red[MULTI_MAX][RES_THREADS_FAST / 32];
+    __shared__ double red[MULTI_G][RES_THREADS_FAST / 32];
+    __shared__ double redf[RES_THREADS_FAST / 32];
     const int tid = threadIdx.x;
     const int nx = MODE == 1 ? M.nx : 0;
     const int nxa = nx > 0 ? nx : 1;
@@ -2678,7 +2755,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     double *sD = reinterpret_cast<double *>(smem + 128);
     double *sX = sD + RES_TILE * NB;
     double *sg = sX + nx * RES_TILE * NB; /* [k][s][c][i] gathers; mode 0: [k][c][i] R */
-    double *sr = sg + (size_t)nr * nxa * RES_TILE * NV; /* [k][c][i] R, then b */
+    double *sr = sg + (size_t)MULTI_G * nxa * RES_TILE * NV; /* [k][c][i] R, then b */
+    if (nr < MULTI_G) sr = sg + (size_t)nr * nxa * RES_TILE * NV;
     __shared__ int rid[MULTI_MAX]; /* the k-th active right-hand side */
     if (tid == 0) {
         unsigned am = 0;
@@ -2695,49 +2773,59 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     __syncthreads();
     const unsigned amask = amask_s;
     const int nact = __popc(amask);
+    const int ngroups = (nact + MULTI_G - 1) / MULTI_G;
+    const int nitems = ntiles * ngroups;
     const int c = tid % RES_TILE, i = tid / RES_TILE;
     const bool act = tid < RES_TILE * NV;
     const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
     uint32_t parity = 0;
     bool failed = false;
-    for (int blk = blockIdx.x; blk < ntiles && nact > 0; blk += gridDim.x) {
+    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
+        const int blk = w / ngroups;
+        const int kb = (w - blk * ngroups) * MULTI_G;
+        const int kn = nact - kb < MULTI_G ? nact - kb : MULTI_G;
         const int p0 = blk * RES_TILE;
         if (tid == 0) {
             const uint64_t pol = policy_evict_first();
-            mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : nact * szR));
-            bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+            mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : kn * szR));
+            /* a tile read by one item streams through; one read by several
+             * stays in L2 for the others */
+            if (ngroups == 1)
+                bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
+            else
+                bulk_g2s(sD, Dinv + (size_t)p0 * NB, szD, bar);
             if (MODE == 1) {
-                for (int s = 0; s < nx; ++s)
-                    bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * M.np16 + p0) * NB, szD,
-                                  bar, pol);
-            } else {
-                int k = 0;
-                for (int r = 0; r < nr; ++r) {
-                    if (!((amask >> r) & 1u)) continue;
-                    bulk_g2s(sg + (size_t)k * RES_TILE * NV, Rsrc + (size_t)r * vs + (size_t)p0 * NV,
-                             szR, bar);
-                    ++k;
+                for (int s = 0; s < nx; ++s) {
+                    const double *src = X + ((size_t)s * M.np16 + p0) * NB;
+                    if (ngroups == 1)
+                        bulk_g2s_hint(sX + s * RES_TILE * NB, src, szD, bar, pol);
+                    else
+                        bulk_g2s(sX + s * RES_TILE * NB, src, szD, bar);
                 }
+            } else {
+                for (int k = 0; k < kn; ++k)
+                    bulk_g2s(sg + (size_t)k * RES_TILE * NV,
+                             Rsrc + (size_t)rid[kb + k] * vs + (size_t)p0 * NV, szR, bar);
             }
         }
         if (act) {
             const size_t q = (size_t)p0 * NV + tid;
             if (MODE == 1) {
-                /* every load of the tile (the neighbour dU gathers, U and dU
-                 * of each active r) is issued before the first store, so
-                 * that their latencies overlap */
+                /* every load of the item (the neighbour dU gathers, U and dU
+                 * of each of its right-hand sides) is issued before the first
+                 * store, so that their latencies overlap */
                 int nbr[MULTI_NX];
 #pragma unroll
                 for (int s = 0; s < MULTI_NX; ++s)
                     nbr[s] = s < nx ? __ldg(xnbr + (size_t)s * M.np16 + p0 + c) : -1;
-                double gv[MULTI_MAX][MULTI_NX], uv[MULTI_MAX], dv[MULTI_MAX];
+                double gv[MULTI_G][MULTI_NX], uv[MULTI_G], dv[MULTI_G];
 #pragma unroll
-                for (int k = 0; k < MULTI_MAX; ++k) {
+                for (int k = 0; k < MULTI_G; ++k) {
                     uv[k] = dv[k] = 0.0;
 #pragma unroll
                     for (int s = 0; s < MULTI_NX; ++s) gv[k][s] = 0.0;
-                    if (k < nact) {
-                        const size_t ro = (size_t)rid[k] * vs;
+                    if (k < kn) {
+                        const size_t ro = (size_t)rid[kb + k] * vs;
 #pragma unroll
                         for (int s = 0; s < MULTI_NX; ++s)
                             if (nbr[s] >= 0) gv[k][s] = __ldg(M.dU + ro + (size_t)nbr[s] * NV + i);
@@ -2746,16 +2834,16 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < MULTI_MAX; ++k) {
-                    if (k < nact) {
+                for (int k = 0; k < MULTI_G; ++k) {
+                    if (k < kn) {
 #pragma unroll
                         for (int s = 0; s < MULTI_NX; ++s)
                             if (s < nx) sg[((size_t)(k * nx + s) * RES_TILE + c) * NV + i] = gv[k][s];
-                        M.U[(size_t)rid[k] * vs + q] = uv[k] + dv[k];
+                        M.U[(size_t)rid[kb + k] * vs + q] = uv[k] + dv[k];
                     }
                 }
             } else {
-                for (int k = 0; k < nact; ++k) M.U[(size_t)rid[k] * vs + q] = 0.0;
+                for (int k = 0; k < kn; ++k) M.U[(size_t)rid[kb + k] * vs + q] = 0.0;
             }
         }
         const bool ok = mbar_wait(bar, parity);
@@ -2768,25 +2856,26 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
             failed = true;
             break;
         }
-        /* R for every active r: the row of each slot's block is read once
-         * and feeds every r; per r the products are added in
-         * fast_resid_body's order (slots ascending, three accumulators) */
-        double sq[MULTI_MAX];
+        /* R for each right-hand side of the item: the row of each slot's
+         * block is read once and feeds all of them; per r the products are
+         * added in fast_resid_body's order (slots ascending, three
+         * accumulators) */
+        double sq[MULTI_G];
 #pragma unroll
-        for (int k = 0; k < MULTI_MAX; ++k) sq[k] = 0.0;
+        for (int k = 0; k < MULTI_G; ++k) sq[k] = 0.0;
         if (act) {
             if (MODE == 1) {
-                double a0[MULTI_MAX], a1[MULTI_MAX], a2[MULTI_MAX];
+                double a0[MULTI_G], a1[MULTI_G], a2[MULTI_G];
 #pragma unroll
-                for (int k = 0; k < MULTI_MAX; ++k) a0[k] = a1[k] = a2[k] = 0.0;
+                for (int k = 0; k < MULTI_G; ++k) a0[k] = a1[k] = a2[k] = 0.0;
                 for (int s = 0; s < nx; ++s) {
                     const double *xr = sX + (s * RES_TILE + c) * NB + i;
                     double x[NV];
 #pragma unroll
                     for (int j = 0; j < NV; ++j) x[j] = xr[9 * j];
 #pragma unroll
-                    for (int k = 0; k < MULTI_MAX; ++k) {
-                        if (k < nact) {
+                    for (int k = 0; k < MULTI_G; ++k) {
+                        if (k < kn) {
                             const double *g = sg + ((size_t)(k * nx + s) * RES_TILE + c) * NV;
                             a0[k] += x[0] * g[0];
                             a1[k] += x[1] * g[1];
@@ -2801,8 +2890,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < MULTI_MAX; ++k) {
-                    if (k < nact) {
+                for (int k = 0; k < MULTI_G; ++k) {
+                    if (k < kn) {
                         const double rr = a0[k] + (a1[k] + a2[k]);
                         sr[(size_t)k * RES_TILE * NV + c * NV + i] = rr;
                         sq[k] = rr * rr;
@@ -2810,8 +2899,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < MULTI_MAX; ++k) {
-                    if (k < nact) {
+                for (int k = 0; k < MULTI_G; ++k) {
+                    if (k < kn) {
                         const double rr = sg[(size_t)k * RES_TILE * NV + c * NV + i];
                         sq[k] = rr * rr;
                     }
@@ -2819,8 +2908,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
             }
         }
         __syncthreads();
-        /* b = -Dinv R for every active r (into sg, free now); the row of
-         * Dinv is read once */
+        /* b = -Dinv R for each right-hand side of the item (into sg, free
+         * now); the row of Dinv is read once */
         const double *rsrc = MODE == 1 ? sr : sg;
         double *sb = MODE == 1 ? sg : sr;
         if (act) {
@@ -2829,8 +2918,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
 #pragma unroll
             for (int j = 0; j < NV; ++j) dr[j] = drow[9 * j];
 #pragma unroll
-            for (int k = 0; k < MULTI_MAX; ++k) {
-                if (k < nact) {
+            for (int k = 0; k < MULTI_G; ++k) {
+                if (k < kn) {
                     const double *rv = rsrc + (size_t)k * RES_TILE * NV + c * NV;
                     double a0 = dr[0] * rv[0], a1 = dr[1] * rv[1], a2 = dr[2] * rv[2];
                     a0 += dr[3] * rv[3];
@@ -2845,17 +2934,14 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         }
         __syncthreads();
         if (act) {
-            int k = 0;
-            for (int r = 0; r < nr; ++r) {
-                if (!((amask >> r) & 1u)) continue;
-                M.b[(size_t)r * vs + (size_t)p0 * NV + tid] = sb[(size_t)k * RES_TILE * NV + tid];
-                ++k;
-            }
+            for (int k = 0; k < kn; ++k)
+                M.b[(size_t)rid[kb + k] * vs + (size_t)p0 * NV + tid] =
+                    sb[(size_t)k * RES_TILE * NV + tid];
         }
         /* the tile's sum R^2 per r, in fast_resid_body's order */
 #pragma unroll
-        for (int k = 0; k < MULTI_MAX; ++k) {
-            if (k < nact) {
+        for (int k = 0; k < MULTI_G; ++k) {
+            if (k < kn) {
                 double v = sq[k];
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
                 if ((tid & 31) == 0) red[k][tid >> 5] = v;
@@ -2863,16 +2949,13 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         }
         __syncthreads();
         if (tid == 0) {
-            int k = 0;
-            for (int r = 0; r < nr; ++r) {
-                if (!((amask >> r) & 1u)) continue;
+            for (int k = 0; k < kn; ++k) {
                 double tot = 0.0;
-                for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[k][w];
-                M.partials[(size_t)r * ntiles + blk] = tot;
-                ++k;
+                for (int w2 = 0; w2 < RES_THREADS_FAST / 32; ++w2) tot += red[k][w2];
+                M.partials[(size_t)rid[kb + k] * ntiles + blk] = tot;
             }
         }
-        __syncthreads(); /* the next tile's copies overwrite the stages */
+        __syncthreads(); /* the next item's copies overwrite the stages */
     }
     (void)failed;
 
@@ -2891,12 +2974,12 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         if (!((amask >> r) & 1u)) continue;
         double acc = strided_sum(M.partials + (size_t)r * ntiles, ntiles, (int)blockDim.x);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
-        __syncthreads(); /* red[0] of the previous r is read */
-        if ((tid & 31) == 0) red[0][tid >> 5] = acc;
+        __syncthreads(); /* redf of the previous r is read */
+        if ((tid & 31) == 0) redf[tid >> 5] = acc;
         __syncthreads();
         if (tid == 0) {
             double tot = 0.0;
-            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[0][w];
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += redf[w];
             const double nrm = sqrt(tot);
             SolveState *S = M.state + r;
             if (MODE == 0) {
@@ -2928,12 +3011,14 @@ int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const Mul
     const int ntiles = L.np16 / RES_TILE;
     if (mode == 1) {
         const size_t smem = multi_resid_smem(L.nx, M.nr);
-        multi_resid_kernel<1><<<resid_grid_persistent((const void *)multi_resid_kernel<1>, smem, ntiles),
+        const int nitems = ntiles * ((M.nr + MULTI_G - 1) / MULTI_G);
+        multi_resid_kernel<1><<<resid_grid_persistent((const void *)multi_resid_kernel<1>, smem, nitems),
                                 RES_THREADS_FAST, smem, st>>>(M, Dinv, X, L.xnbr, nullptr,
                                                               cond_handle, use_cond, status);
     } else {
         const size_t smem = multi_resid_smem(0, M.nr);
-        multi_resid_kernel<0><<<resid_grid_persistent((const void *)multi_resid_kernel<0>, smem, ntiles),
+        const int nitems = ntiles * ((M.nr + MULTI_G - 1) / MULTI_G);
+        multi_resid_kernel<0><<<resid_grid_persistent((const void *)multi_resid_kernel<0>, smem, nitems),
                                 RES_THREADS_FAST, smem, st>>>(M, Dinv, nullptr, nullptr, Rsrc,
                                                               cond_handle, use_cond, status);
     }

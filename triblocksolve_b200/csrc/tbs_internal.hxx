@@ -287,6 +287,7 @@ int pij_prepare(const FastLayout &L);
  * side, partials [nr][np16 / RES_TILE]. */
 constexpr int MULTI_MAX = 8;
 constexpr int MULTI_NX = 4;     /* cross-line slots per position of the fast layout */
+constexpr int MULTI_G = 4;      /* right-hand sides per work item of the residual launch */
 struct MultiSys {
     int nr, np16, nx, hist_stride;
     double *U, *b, *partials, *hist;
@@ -379,15 +380,17 @@ struct BatchCtl {
     int finished;               /* set by the norm launch when a member stops */
 };
 struct BatchSched {             /* persistent Thomas launch shape */
-    int ctas_per_sm;            /* one warp per CTA, one line at a time */
+    int ctas_per_sm;            /* CTAs per SM, each solving one line at a time */
     int stages;                 /* bulk-copy ring depth */
+    int warps;                  /* warps per line: 1 (the chain warp issues its own copies)
+                                 * or 2 (a second warp issues them) */
 };
 
 template <typename T>
-size_t thomas_batch_smem(int stages);
+size_t thomas_batch_smem(int stages, int warps);
 /* CTAs of the persistent Thomas kernel that fit on one SM with `stages` */
 template <typename T>
-int thomas_batch_fit(int stages);
+int thomas_batch_fit(int stages, int warps);
 template <typename T>
 int launch_thomas_batch(cudaStream_t st, const BatchSched &bs, const ThomasSys<T> *sys,
                         const WorkItem *work, const int *nwork, const int *active, unsigned *queue,

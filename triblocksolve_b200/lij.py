@@ -469,8 +469,19 @@ class Batch:
         self._chk(N.lib.tbs_batch_get_schedule(self.handle, C.byref(a), C.byref(b), C.byref(c)))
         return a.value, b.value, c.value
 
+    def set_warps_per_line(self, warps: int):
+        """1: the chain warp issues its own staging copies; 2: a copy warp per line."""
+        self._chk(N.lib.tbs_batch_set_warps_per_line(self.handle, warps))
+
+    def warps_per_line(self) -> int:
+        w = C.c_int()
+        self._chk(N.lib.tbs_batch_get_warps_per_line(self.handle, C.byref(w)))
+        return w.value
+
     def tune(self):
-        """Autotune the persistent Thomas launch; returns (ctas_per_sm, stages, order, ms)."""
+        """Autotune the persistent Thomas launch (warps per line, CTAs per SM,
+        stages, line order); returns (ctas_per_sm, stages, order, ms);
+        warps_per_line() gives the tuned warps."""
         a, b, c, ms = C.c_int(), C.c_int(), C.c_int(), C.c_double()
         self._chk(N.lib.tbs_batch_tune(self.handle, C.byref(a), C.byref(b), C.byref(c),
                                        C.byref(ms)))
