@@ -313,6 +313,19 @@ int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm);
 int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
                          int to_line);
 
+/* Waits for the context's stream and reports a device-side failure (a
+ * zero pivot, a staging wait that ran out of time) of the launches since
+ * the last call that returned a status: the end of a sequence of calls
+ * that do not synchronise (tbs_part_line_res with a NULL norm). */
+int tbs_sync(tbs_ctx *ctx);
+
+/* The owned norm of the last tbs_part_start / tbs_part_line_res copied to
+ * d_out (one double, any address the device can reach), in stream order,
+ * without a host synchronisation: the input of a device-side all-reduce.
+ * tbs_part_line_res(ctx, NULL) followed by this keeps the sweep loop free
+ * of host round trips until the global norm is read. */
+int tbs_part_owned_norm(tbs_ctx *ctx, double *d_out);
+
 /* The same for several lines in one launch: lines[0..nlines) (host array
  * of local line indices) packed back to back into d_buf (to_line = 0) or
  * unpacked from it (to_line = 1), each line's span as tbs_part_line_vector

@@ -68,6 +68,15 @@ class OracleSweeper:
                                    oracle._dp_(b.R))
         return self._norm()
 
+    def line_res_async(self):
+        self.line_res()
+
+    def owned_norm_to(self, t):
+        t[0] = self._norm()
+
+    def sync(self):
+        pass
+
     def lines_vector(self, which, ks, buf, to_line):
         off = 0
         for k in ks:
@@ -237,3 +246,19 @@ def test_torchrun_ranks_match_whole_mesh_oracle(world, tmp_path):
         U.reshape(-1, 9)[d["elems"]] = d["U"].reshape(-1, 9)
     np.testing.assert_array_equal(U, oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs,
                                                 want)["U"])
+
+
+@pytest.mark.parametrize("limit", [1, 3])
+def test_partitioned_solve_sweep_limit_discards_the_speculative_sweep(limit):
+    """The loop issues the next sweep's line solves before it reads the
+    global norm; at the sweep limit (and at convergence) that line solve is
+    discarded: U is the whole mesh's after exactly `limit` sweeps."""
+    mesh, jac = _problem(LENS, 11)
+    parts = partition_lines(mesh, 3)
+    sw = [OracleSweeper(p, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs) for p in parts]
+    n, hist = PartitionedSolve(sw, LocalExchange(parts, sw, device="cpu")).solve(1e-30, limit)
+    assert n == limit and hist.size == limit + 1
+    ref = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, limit)
+    np.testing.assert_array_equal(gather_solution(parts, [s.base.U for s in sw], mesh.nelem),
+                                  ref["U"])
+    assert np.all(np.abs(hist - ref["hist"]) <= NORM_TOL * ref["hist"][0])

@@ -1703,6 +1703,29 @@ int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf, int t
     GUARD_END
 }
 
+int tbs_sync(tbs_ctx *ctx) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_status) return TBS_OK;
+    int rc = status_check(ctx);
+    if (rc == TBS_OK && ctx->prof) prof_resolve(ctx);
+    return rc;
+    GUARD_END
+}
+
+int tbs_part_owned_norm(tbs_ctx *ctx, double *d_out) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    if (!d_out) return ctx_fail(ctx, TBS_ERR_ARG, "null output");
+    CK(cudaMemcpyAsync(d_out, &ctx->d_state->last, sizeof(double), cudaMemcpyDefault, ctx->stream));
+    return TBS_OK;
+    GUARD_END
+}
+
 int tbs_part_lines_vector(tbs_ctx *ctx, int which, int nlines, const int *lines, double *d_buf,
                           int to_line) {
     if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");

@@ -198,6 +198,17 @@ class PartitionSolver(Solver):
         self._chk(N.lib.tbs_part_line_res(self.ctx, C.byref(n)))
         return n.value
 
+    def line_res_async(self) -> None:
+        """tbs_part_line_res without reading the norm (no host synchronisation)."""
+        self._chk(N.lib.tbs_part_line_res(self.ctx, None))
+
+    def owned_norm_to(self, t) -> None:
+        """The owned norm into the one-element tensor ``t``, in stream order."""
+        self._chk(N.lib.tbs_part_owned_norm(self.ctx, C.c_void_p(t.data_ptr())))
+
+    def sync(self) -> None:
+        self._chk(N.lib.tbs_sync(self.ctx))
+
     def lines_vector(self, which: int, lines, buf, to_line: bool) -> None:
         """Several lines' vectors packed back to back into ``buf`` (or
         unpacked from it) by one launch."""
@@ -256,6 +267,20 @@ class LocalExchange:
     def allreduce_sum(self, x: float) -> float:
         return x
 
+    def norm_sq_async(self, sweepers):
+        """Sum of the squared owned norms as a one-element tensor, not yet read."""
+        return _norm_sq(sweepers, self.buf.device)
+
+
+def _norm_sq(sweepers, device):
+    import torch
+    t = torch.zeros(1, dtype=torch.float64, device=device)
+    one = torch.empty(1, dtype=torch.float64, device=device)
+    for s in sweepers:
+        s.owned_norm_to(one)
+        t.addcmul_(one, one)
+    return t
+
 
 class DistExchange:
     """Halo exchange of this process's partition with the others over
@@ -306,6 +331,14 @@ class DistExchange:
         self.dist.all_reduce(t, group=self.group)
         return float(t.item())
 
+    def norm_sq_async(self, sweepers):
+        """The global sum of the squared owned norms as a one-element tensor:
+        the owned norms copied on the device, squared and all-reduced in
+        stream order, not yet read by the host."""
+        t = _norm_sq(sweepers, self.torch.device(self.device))
+        self.dist.all_reduce(t, group=self.group)
+        return t
+
 
 class PartitionedSolve:
     """The sweep loop of src/main.cxx:207-229 over line partitions: the
@@ -328,14 +361,45 @@ class PartitionedSolve:
         self.ex.exchange(N.VEC_UPDATE)
         return self._global([s.line_res() for s in self.sweepers])
 
+    def _solve_and_exchange(self) -> None:
+        for s in self.sweepers:
+            s.solve_du()
+        self.ex.exchange(N.VEC_UPDATE)
+
+    def _line_res(self):
+        for s in self.sweepers:
+            s.line_res_async()
+        return self.ex.norm_sq_async(self.sweepers)
+
     def solve(self, rel_tol: float, max_sweeps: int = 1000):
         """Sweeps from U = 0 until ||R|| <= rel_tol ||R_0|| or max_sweeps;
-        returns (sweeps, global norm history)."""
+        returns (sweeps, global norm history).
+
+        One host read per sweep: the owned norms stay on the device, are
+        squared and all-reduced there, and the host reads the global norm
+        only after it has issued the next sweep's line solves and halo
+        exchange, which therefore overlap the read and the convergence
+        test.  When the test ends the solve, that speculative line solve
+        is discarded: U and the norms are those of the last sweep counted;
+        the context's last update (tbs_get_update) is the discarded one.
+        Every rank takes the same decisions from the same global norm, so
+        the collectives stay matched."""
         n0 = self.start()
         hist = [n0]
-        while len(hist) - 1 < max_sweeps:
-            last = hist[-1]
-            if not (math.isfinite(last) and last > rel_tol * n0):
+        go = lambda g: math.isfinite(g) and g > rel_tol * n0
+        if max_sweeps < 1 or not go(n0):
+            return 0, np.array(hist)
+        self._solve_and_exchange()
+        pending = self._line_res()
+        while True:
+            more = len(hist) < max_sweeps  # a sweep after the one being read is allowed
+            if more:
+                self._solve_and_exchange()
+            g = math.sqrt(float(pending.item()))
+            hist.append(g)
+            if not (more and go(g)):
                 break
-            hist.append(self.sweep())
+            pending = self._line_res()
+        for s in self.sweepers:
+            s.sync()
         return len(hist) - 1, np.array(hist)
