@@ -1038,6 +1038,89 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
     }
 }
 
+/* The shuffle form of a chain step: the previous step's vector is taken
+ * from the lanes that computed it (lane base + j holds entry j) with warp
+ * shuffles, in the pairing of this lane's row (pairs from entry par, the
+ * single entry 0 or 8), instead of a round trip through shared memory.
+ * The products and their order are row_dot's, so the values are too. */
+template <typename T>
+__device__ __forceinline__ T row_dot_sh(const typename RowOf<T>::type &R, T prev, int base,
+                                        int par, T init) {
+    T v[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) v[k] = __shfl_sync(FULL, prev, base + par + k);
+    const T w = __shfl_sync(FULL, prev, base + (par ? 0 : 8));
+    T a0 = init - R.s * w;
+    T a1 = R.r0.x * v[0];
+    T a2 = R.r0.y * v[1];
+    a0 -= R.r1.x * v[2];
+    a1 += R.r1.y * v[3];
+    a2 += R.r2.x * v[4];
+    a0 -= R.r2.y * v[5];
+    a1 += R.r3.x * v[6];
+    a2 += R.r3.y * v[7];
+    return a0 - (a1 + a2);
+}
+
+/* fwd_chunk with the vector carried in `prev` (this lane's entry of the
+ * last valid step) */
+template <typename T, int P, bool CHECK, bool YS>
+__device__ __forceinline__ void fwd_chunk_sh(const T *sG, const T *sB, T &prev, T *ys, T *yg,
+                                             int kbase, int len, int cpos, int i, int base,
+                                             const LaneOff &o) {
+    typename RowOf<T>::type cur_row, next_row;
+    load_row(cur_row, sG, o, 0);
+    T cur_b = sB[i];
+#pragma unroll
+    for (int q = 0; q < P; ++q) {
+        const int odd = q & 1;
+        T next_b = T(0);
+        if (q + 1 < P) {
+            load_row(next_row, sG + (q + 1) * NB, o, odd ^ 1);
+            next_b = sB[(q + 1) * NV + i];
+        }
+        const T yi = row_dot_sh<T>(cur_row, prev, base, (i + odd) & 1, cur_b);
+        if (!CHECK || kbase + q < len) {
+            prev = yi;
+            const int pos = cpos + kbase + q;
+            if (YS)
+                ys[pos * NV + i] = yi;
+            else
+                yg[(size_t)pos * NV + i] = yi;
+        }
+        cur_row = next_row;
+        cur_b = next_b;
+    }
+}
+
+template <typename T, int P, bool CHECK, bool YS>
+__device__ __forceinline__ void bwd_chunk_sh(const T *sG, T &prev, T *ys, const T *yv, const T *uv,
+                                             T *dUl, T *Ul, int kbase, int len, int cpos, int i,
+                                             int base, const LaneOff &o) {
+    typename RowOf<T>::type cur_row, next_row;
+    load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
+#pragma unroll
+    for (int q = P - 1; q >= 0; --q) {
+        const int odd = q & 1;
+        if (q > 0) load_row(next_row, sG + (q - 1) * NB, o, odd ^ 1);
+        const bool valid = !CHECK || (kbase + q >= 0 && kbase + q < len);
+        const int pos = cpos + kbase + q;
+        T yk = T(0);
+        if (valid) yk = YS ? ys[pos * NV + i] : yv[q];
+        const T d = row_dot_sh<T>(cur_row, prev, base, (i + odd) & 1, yk);
+        if (valid) {
+            prev = d;
+            if (YS) {
+                ys[pos * NV + i] = d;
+            } else {
+                dUl[(size_t)pos * NV + i] = d;
+                if (Ul) Ul[(size_t)pos * NV + i] = uv[q] + d;
+            }
+        }
+        cur_row = next_row;
+    }
+}
+
 /* Solve one line (start ps, n cells, twist m) with the warp of the calling
  * CTA.  The staging barriers live at the start of `smem` and stay
  * initialised across the lines that a persistent CTA solves: bit s of
@@ -1049,7 +1132,7 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
 template <bool WS>
 __host__ __device__ constexpr int thomas_hdr() { return WS ? 256 : 128; }
 
-template <typename T, int P, bool YS, bool WS = false>
+template <typename T, int P, bool YS, bool WS = false, bool SH = false>
 __device__ __forceinline__ bool thomas_line(
     int NS, int accumulate, int ps, int n, int m, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
@@ -1157,6 +1240,8 @@ __device__ __forceinline__ bool thomas_line(
     int consumed = 0;
     bool timed_out = false;
     const int both_full = (m < nb ? m : nb) / P; /* jobs where both chains run P steps */
+    const int base = lane & 16; /* SH: the half-warp's first lane */
+    T prev = T(0);              /* SH: this lane's entry of the chain's last vector */
 
     /* ---------------- forward */
     for (int c = 0; c < nf; ++c) {
@@ -1169,7 +1254,12 @@ __device__ __forceinline__ bool thomas_line(
         ++consumed;
         const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
         const T *sB = sG + P * NB;
-        if (c < both_full)
+        if (SH) {
+            if (c < both_full)
+                fwd_chunk_sh<T, P, false, YS>(sG, sB, prev, ys, yl, c * P, len, cpos, i, base, off);
+            else
+                fwd_chunk_sh<T, P, true, YS>(sG, sB, prev, ys, yl, c * P, len, cpos, i, base, off);
+        } else if (c < both_full)
             fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
         else
             fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
@@ -1183,6 +1273,11 @@ __device__ __forceinline__ bool thomas_line(
     }
 
     if (!timed_out) {
+        if (SH) {
+            /* publish each chain's last vector where the twist reads it */
+            if (li < NV) bc[(len & 1) * 20 + li] = prev;
+            __syncwarp();
+        }
         /* ---------------- twist: x_m = b_m - G_tw y_top - Gam_tw y_bot */
         const int ptw = n - 1; /* relative to ps */
         const T *ytop = bcall + 0 * 40 + (m & 1) * 20;
@@ -1211,6 +1306,7 @@ __device__ __forceinline__ bool thomas_line(
             }
         }
         __syncwarp();
+        if (SH) prev = __shfl_sync(FULL, xm, i); /* both chains start from the twist's vector */
 
         /* ---------------- backward */
         T yv[P], uv[P], nyv[P], nuv[P];
@@ -1241,7 +1337,16 @@ __device__ __forceinline__ bool thomas_line(
             const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
             const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
                               nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
-            if (full)
+            if (SH) {
+                if (full)
+                    bwd_chunk_sh<T, P, false, YS>(sG, prev, ys, yv, uv, dUl,
+                                                  accumulate < 2 ? Ul : nullptr, c * P, len, cpos,
+                                                  i, base, off);
+                else
+                    bwd_chunk_sh<T, P, true, YS>(sG, prev, ys, yv, uv, dUl,
+                                                 accumulate < 2 ? Ul : nullptr, c * P, len, cpos,
+                                                 i, base, off);
+            } else if (full)
                 bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
                                            c * P, len, cpos, i, off);
             else
@@ -1323,7 +1428,7 @@ __device__ __forceinline__ void thomas_init_bars(unsigned char *smem, int NS) {
 }
 
 /* one CTA (one warp) per line */
-template <typename T, int P, bool YS>
+template <typename T, int P, bool YS, bool SH = false>
 __global__ void __launch_bounds__(32) fast_thomas_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
@@ -1335,15 +1440,15 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     thomas_init_bars(smem, NS);
     const uint64_t pol = threadIdx.x == 0 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam, b, y,
-                          dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS, false, SH>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G,
+                                     Gam, b, y, dU, U, status, smem, pbase, pol);
 }
 
 /* Warp-specialised form, one CTA of two warps per line: warp 1 issues the
  * staging copies, warp 0 runs the chains with the same arithmetic as
  * fast_thomas_kernel, so its results are bit-identical; the chain warp no
  * longer stops every chunk to issue the next copies. */
-template <typename T, int P, bool YS>
+template <typename T, int P, bool YS, bool SH = false>
 __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
@@ -1366,8 +1471,8 @@ __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
     __syncthreads();
     const uint64_t pol = threadIdx.x == 32 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS, true>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam,
-                                b, y, dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS, true, SH>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G,
+                                    Gam, b, y, dU, U, status, smem, pbase, pol);
 }
 
 /* Persistent form over many systems: each CTA (one warp) takes (system,
@@ -1522,32 +1627,40 @@ static bool thomas_ws(const FastLayout &L) {
     return (L.nline + nsm - 1) / nsm <= 5;
 }
 
+/* The chain step's vector through warp shuffles (1) or a shared-memory
+ * round trip (0); TBS_THOMAS_SHFL forces either, for measurements.  Both
+ * give the same values. */
+static bool thomas_shfl() {
+    static const int forced = [] {
+        const char *e = getenv("TBS_THOMAS_SHFL");
+        return e && e[0] ? (e[0] == '0' ? 0 : 1) : -1;
+    }();
+    return forced == 1;
+}
+
+template <typename T, bool WS, bool YS, bool SH>
+static const void *thomas_fn() {
+    return WS ? (const void *)fast_thomas_ws_kernel<T, THOMAS_P, YS, SH>
+              : (const void *)fast_thomas_kernel<T, THOMAS_P, YS, SH>;
+}
+
+template <typename T, bool WS>
+static const void *thomas_fn(bool ys, bool sh) {
+    return ys ? (sh ? thomas_fn<T, WS, true, true>() : thomas_fn<T, WS, true, false>())
+              : (sh ? thomas_fn<T, WS, false, true>() : thomas_fn<T, WS, false, false>());
+}
+
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
                        T *y, T *dU, T *U, unsigned *status, int accumulate) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    if (!thomas_ws(L)) {
-        const ThomasCfg c1 = thomas_cfg<T>(L);
-        if (c1.ys)
-            fast_thomas_kernel<T, THOMAS_P, true><<<L.nline, 32, c1.smem, st>>>(
-                L.nline, c1.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y,
-                dU, U, status);
-        else
-            fast_thomas_kernel<T, THOMAS_P, false><<<L.nline, 32, c1.smem, st>>>(
-                L.nline, c1.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y,
-                dU, U, status);
-        return (int)cudaGetLastError();
-    }
-    const ThomasCfg cfg = thomas_cfg<T, true>(L);
-    if (cfg.ys)
-        fast_thomas_ws_kernel<T, THOMAS_P, true><<<L.nline, 64, cfg.smem, st>>>(
-            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
-            U, status);
-    else
-        fast_thomas_ws_kernel<T, THOMAS_P, false><<<L.nline, 64, cfg.smem, st>>>(
-            L.nline, cfg.NS, accumulate, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU,
-            U, status);
-    return (int)cudaGetLastError();
+    const bool ws = thomas_ws(L), sh = thomas_shfl();
+    const ThomasCfg c = ws ? thomas_cfg<T, true>(L) : thomas_cfg<T>(L);
+    const void *fn = ws ? thomas_fn<T, true>(c.ys, sh) : thomas_fn<T, false>(c.ys, sh);
+    int ns = c.NS, nline = L.nline;
+    const int *ls = L.line_start, *ll = L.line_len, *lt = L.line_twist;
+    void *args[] = {&nline, &ns, &accumulate, &ls, &ll, &lt, &G, &Gam, &b, &y, &dU, &U, &status};
+    return (int)cudaLaunchKernel(fn, dim3(L.nline), dim3(ws ? 64 : 32), args, c.smem, st);
 }
 
 template int launch_fast_thomas<double>(cudaStream_t, const FastLayout &, const double *,
@@ -1588,23 +1701,13 @@ int fast_prepare(const FastLayout &L) {
     if (!rc) rc = set_smem((const void *)fast_resid_jv_kernel<double>, resid_smem_bytes<double>(L.nx));
     if (!rc) rc = set_smem((const void *)fast_resid_kernel<float>, resid_smem_bytes<float>(L.nx));
     const ThomasCfg c64 = thomas_cfg<double>(L), c32 = thomas_cfg<float>(L);
-    if (!rc)
-        rc = set_smem(c64.ys ? (const void *)fast_thomas_kernel<double, THOMAS_P, true>
-                             : (const void *)fast_thomas_kernel<double, THOMAS_P, false>,
-                      c64.smem);
-    if (!rc)
-        rc = set_smem(c32.ys ? (const void *)fast_thomas_kernel<float, THOMAS_P, true>
-                             : (const void *)fast_thomas_kernel<float, THOMAS_P, false>,
-                      c32.smem);
     const ThomasCfg w64 = thomas_cfg<double, true>(L), w32 = thomas_cfg<float, true>(L);
-    if (!rc)
-        rc = set_smem(w64.ys ? (const void *)fast_thomas_ws_kernel<double, THOMAS_P, true>
-                             : (const void *)fast_thomas_ws_kernel<double, THOMAS_P, false>,
-                      w64.smem);
-    if (!rc)
-        rc = set_smem(w32.ys ? (const void *)fast_thomas_ws_kernel<float, THOMAS_P, true>
-                             : (const void *)fast_thomas_ws_kernel<float, THOMAS_P, false>,
-                      w32.smem);
+    for (int sh = 0; sh < 2 && !rc; ++sh) {
+        rc = set_smem(thomas_fn<double, false>(c64.ys, sh), c64.smem);
+        if (!rc) rc = set_smem(thomas_fn<float, false>(c32.ys, sh), c32.smem);
+        if (!rc) rc = set_smem(thomas_fn<double, true>(w64.ys, sh), w64.smem);
+        if (!rc) rc = set_smem(thomas_fn<float, true>(w32.ys, sh), w32.smem);
+    }
     return rc;
 }
 
