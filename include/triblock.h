@@ -361,8 +361,11 @@ int tbs_solve_check(tbs_ctx *ctx, double *true_norm, int *checks, int *restarts)
  * the true-residual check on) then converge to the new system's solution,
  * TBS_ALGO_MIXED's FP64 outer residual uses the new values.  Resets U to
  * zero (or the starting solution) and R to its residual.  TBS_ALGO_PIJ
- * refuses (re-factor).  No counterpart in the reference, which re-reads
- * and re-factors (src/main.cxx:86-93,180-190). */
+ * and line partitions refuse (re-factor); so do, until the next
+ * tbs_factor, the TBS_ALGO_FP64 paths that track the residual with the
+ * factorization's blocks alone: batches, several right-hand sides, GMRES.
+ * No counterpart in the reference, which re-reads and re-factors
+ * (src/main.cxx:86-93,180-190). */
 int tbs_update_values(tbs_ctx *ctx, const double *jacD, const double *jacO1,
                       const double *jacO2);
 

@@ -19,8 +19,8 @@ import pytest
 
 import oracle
 from meshes import ragged_mesh
-from triblocksolve_b200 import (ALGO_FP64, ALGO_MIXED, ALGO_PIJ, ALGO_REFERENCE, Jacobian, Mesh,
-                                Solver, TbsError)
+from triblocksolve_b200 import (ALGO_FP64, ALGO_MIXED, ALGO_PIJ, ALGO_REFERENCE, Batch, Jacobian,
+                                Mesh, Solver, TbsError)
 
 pytestmark = pytest.mark.gpu
 
@@ -189,3 +189,18 @@ def test_update_values_refusals(solver):
     solver.update_values(jac.jacD, jac.jacO1, jac.jacO2)  # same values: an ordinary solve
     n, h = solver.solve(1e-12, 100)
     assert solver.solve_check()[1:] == (1, 0)
+    # the paths that track the residual with the factorization's blocks refuse
+    # a context whose values are newer than its factorization, until it is re-factored
+    with pytest.raises(TbsError):
+        solver.solve_multi(np.stack([jac.rhs, jac.rhs]), 1e-10, 50)
+    with pytest.raises(TbsError):
+        solver.gmres(1e-10, 10, 1, 50)
+    with pytest.raises(TbsError):
+        b = Batch([solver])
+        try:
+            b.solve(1e-10, 50)
+        finally:
+            b.close()
+    solver.factor(ALGO_FP64)
+    solver.solve_multi(np.stack([jac.rhs, jac.rhs]), 1e-10, 50)
+    solver.gmres(1e-10, 10, 1, 50)

@@ -1133,6 +1133,7 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
     rc = status_check(ctx);
     if (rc) return rc;
     ctx->factored = true;
+    ctx->lagged = false;
     return TBS_OK;
     GUARD_END
 }
@@ -1400,6 +1401,10 @@ int tbs_update_values(tbs_ctx *ctx, const double *jacD, const double *jacO1, con
         return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
                         "TBS_ALGO_PIJ tracks its residual with the factorization's face blocks; "
                         "re-factor instead (tbs_set_jacobian + tbs_factor)");
+    if (ctx->nhalo > 0)
+        return ctx_fail(ctx, TBS_ERR_UNSUPPORTED,
+                        "a line partition tracks its residual with the factorization's blocks; "
+                        "re-factor instead");
     if (ctx->algo == TBS_ALGO_FP64 && !ctx->check)
         return ctx_fail(ctx, TBS_ERR_STATE,
                         "TBS_ALGO_FP64 with the true-residual check off would converge to the "
@@ -1414,6 +1419,7 @@ int tbs_update_values(tbs_ctx *ctx, const double *jacD, const double *jacO1, con
     if (ctx->algo == TBS_ALGO_MIXED && fullpos_ok(ctx))
         RUN("fullpos_layout", launch_fullpos_layout(st, ctx->L, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                     ctx->d_Dp, ctx->d_XF));
+    ctx->lagged = true;
     return prime(ctx, CondCtl{});
     GUARD_END
 }

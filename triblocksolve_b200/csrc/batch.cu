@@ -923,6 +923,12 @@ static int batch_check_members(tbs_batch *b) {
         if (c->algo != b->eng.algo)
             return bfail(b, TBS_ERR_STATE,
                          "batch member " + std::to_string(s) + " was re-factored with another algorithm");
+        if (c->lagged && c->algo == TBS_ALGO_FP64)
+            return bfail(b, TBS_ERR_UNSUPPORTED,
+                         "batch member " + std::to_string(s) +
+                             " has block values newer than its FP64 factorization (tbs_update_values); "
+                             "the batch tracks the residual with the factorization's blocks: re-factor "
+                             "it or solve it with tbs_solve");
     }
     return TBS_OK;
 }

@@ -71,6 +71,7 @@ struct tbs_ctx {
     int inner_sweeps = 4;  /* TBS_ALGO_MIXED inner sweeps per outer step */
     int inner_first = 0;   /* > 0: the first outer step's inner sweeps */
     int outer_done = 0;    /* outer steps since the last prime (eager sequences) */
+    bool lagged = false;   /* block values replaced since the factorization (tbs_update_values) */
     int check = 1;         /* tbs_solve checks a converged TBS_ALGO_FP64 solve against
                             * the true residual (tbs_set_check) */
 

@@ -460,6 +460,10 @@ extern "C" int tbs_gmres(tbs_ctx *ctx, int restart, int precond_sweeps, double r
         if (ctx->algo != TBS_ALGO_FP64 || ctx->nvar != 9)
             return kfail(ctx, TBS_ERR_UNSUPPORTED,
                          "GMRES uses the TBS_ALGO_FP64 line factors of nvar == 9");
+        if (ctx->lagged)
+            return kfail(ctx, TBS_ERR_UNSUPPORTED,
+                         "block values are newer than the factorization (tbs_update_values); GMRES "
+                         "forms its products with J from the factorization's blocks: re-factor");
         if (ctx->nhalo > 0) return kfail(ctx, TBS_ERR_UNSUPPORTED, "a line partition sweeps with tbs_part_solve_du / tbs_part_line_res");
         if (restart < 1 || restart > KRYLOV_MAX || precond_sweeps < 1 || max_iters < 0 ||
             !(rel_tol >= 0.0))

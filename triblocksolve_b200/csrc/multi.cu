@@ -338,6 +338,10 @@ static int multi_check(tbs_ctx *ctx, int nrhs, const void *rhs, const void *U, d
     if (ctx->algo != TBS_ALGO_FP64 || ctx->nvar != 9)
         return mfail(ctx, TBS_ERR_UNSUPPORTED, "several right-hand sides need TBS_ALGO_FP64 and nvar == 9");
     if (ctx->nhalo > 0) return mfail(ctx, TBS_ERR_UNSUPPORTED, "a line partition sweeps with tbs_part_solve_du / tbs_part_line_res");
+    if (ctx->lagged)
+        return mfail(ctx, TBS_ERR_UNSUPPORTED,
+                     "block values are newer than the factorization (tbs_update_values); several "
+                     "right-hand sides track the residual with the factorization's blocks: re-factor");
     if (nrhs < 0 || (nrhs > 0 && (!rhs || !U)))
         return mfail(ctx, TBS_ERR_ARG, "bad right-hand-side count or null arrays");
     if (max_sweeps < 0 || !(tol >= 0.0)) return mfail(ctx, TBS_ERR_ARG, "bad tolerance or sweep limit");
