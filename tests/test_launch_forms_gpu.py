@@ -41,9 +41,9 @@ np.savez(sys.argv[2], n=n, h=h, U=U, Um=Um, sw=sw, hm=np.concatenate(hm), n2=n2,
 """
 
 
-def _run(tmp_path, form, shfl=0):
-    out = str(tmp_path / f"form{form}_{shfl}.npz")
-    env = dict(os.environ, TBS_THOMAS_WS=str(form), TBS_THOMAS_SHFL=str(shfl))
+def _run(tmp_path, form):
+    out = str(tmp_path / f"form{form}.npz")
+    env = dict(os.environ, TBS_THOMAS_WS=str(form))
     subprocess.run([sys.executable, "-c", SCRIPT, ROOT, out], env=env, check=True, timeout=300)
     return np.load(out)
 
@@ -54,11 +54,3 @@ def test_one_warp_and_warp_specialised_forms_agree(tmp_path):
         assert np.array_equal(a[k], b[k]), k
     assert int(a["n"]) > 1 and np.all(a["sw"] > 1)
 
-
-@pytest.mark.parametrize("form", [0, 1])
-def test_shuffle_and_shared_memory_steps_agree(tmp_path, form):
-    """The chain step's vector taken by warp shuffles or through shared
-    memory (TBS_THOMAS_SHFL=1 / 0): the same products in the same order."""
-    a, b = _run(tmp_path, form, 0), _run(tmp_path, form, 1)
-    for k in a.files:
-        assert np.array_equal(a[k], b[k]), k

@@ -610,6 +610,21 @@ __device__ __forceinline__ uint64_t *resid_bar_init() {
     return bar;
 }
 
+/* -(row of Dinv) . R for one (cell, row): dr points at entry (row, 0) of
+ * the cell's column-major block, rv at the cell's R; three accumulators,
+ * the order every b = -Dinv R of this file uses */
+template <typename T>
+__device__ __forceinline__ T neg_dinv_row(const T *dr, const T *rv) {
+    T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
+    a0 += dr[27] * rv[3];
+    a1 += dr[36] * rv[4];
+    a2 += dr[45] * rv[5];
+    a0 += dr[54] * rv[6];
+    a1 += dr[63] * rv[7];
+    a2 += dr[72] * rv[8];
+    return -(a0 + (a1 + a2));
+}
+
 /* One tile (positions blk*RES_TILE ..) with the staging barrier's phase of
  * the given parity.  Returns false (status set, copies landed) when the
  * wait for the tile's bulk copies ran out of time. */
@@ -698,16 +713,7 @@ __device__ __forceinline__ bool fast_resid_body(
         /* R = v + J z after the line solves, so J z = R - v */
         if (act) sb[c * NV + i] = r - Rsrc[(size_t)p0 * NV + c * NV + i];
     } else if (act) {
-        const T *dr = sD + c * NB + i;
-        const T *rv = sr + c * NV;
-        T a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
-        a0 += dr[27] * rv[3];
-        a1 += dr[36] * rv[4];
-        a2 += dr[45] * rv[5];
-        a0 += dr[54] * rv[6];
-        a1 += dr[63] * rv[7];
-        a2 += dr[72] * rv[8];
-        sb[c * NV + i] = -(a0 + (a1 + a2));
+        sb[c * NV + i] = neg_dinv_row<T>(sD + c * NB + i, sr + c * NV);
     }
     __syncthreads();
     if (act) b[(size_t)p0 * NV + tid] = sb[tid]; /* contiguous tile store */
@@ -780,7 +786,88 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
     int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
     T *__restrict__ Uzero, NormSink ns, unsigned *status) {
-    resid_tiles<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status);
+    /* mode 0 (b = -Dinv R and the norm of a given R) with two staging
+     * buffers: the next tile's bulk copies are in flight while this one is
+     * computed.  A tile is a third of a mode-1 tile's bytes and the CTAs
+     * per SM are bounded by threads, not shared memory, so the second
+     * buffer costs no residency.  Per element the expressions of
+     * fast_resid_body's mode 0. */
+    extern __shared__ __align__(128) unsigned char smem[];
+    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
+    const uint32_t szD = RES_TILE * NB * sizeof(T), szR = RES_TILE * NV * sizeof(T);
+    const uint32_t stage = szD + szR;
+    unsigned char *st0 = smem + 128;
+    T *sb = reinterpret_cast<T *>(st0 + 2 * stage);
+    const int tid = threadIdx.x;
+    const int c = tid % RES_TILE, i = tid / RES_TILE;
+    const bool act = tid < RES_TILE * NV;
+    const int ntiles = np16 / RES_TILE;
+    if (tid == 0) {
+        mbar_init(&bar[0], 1);
+        mbar_init(&bar[1], 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    auto issue = [&](int w, int s) {
+        const uint64_t pol = policy_evict_first();
+        unsigned char *dst = st0 + (size_t)s * stage;
+        mbar_arrive_expect_tx(&bar[s], stage);
+        bulk_g2s_hint(dst, Dinv + (size_t)w * RES_TILE * NB, szD, &bar[s], pol);
+        bulk_g2s(dst + szD, Rsrc + (size_t)w * RES_TILE * NV, szR, &bar[s]);
+    };
+    const int first = blockIdx.x;
+    if (tid == 0 && first < ntiles) issue(first, 0);
+    int k = 0;
+    bool failed = false;
+    for (int w = first; w < ntiles; w += gridDim.x, ++k) {
+        const int s = k & 1;
+        /* the other stage was released by the previous iteration's barrier */
+        if (tid == 0 && w + (int)gridDim.x < ntiles) issue(w + gridDim.x, s ^ 1);
+        const int p0 = w * RES_TILE;
+        if (act && Uzero) Uzero[(size_t)p0 * NV + tid] = T(0);
+        const bool ok = mbar_wait(&bar[s], (uint32_t)((k >> 1) & 1));
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) {
+                atomicOr(status, ST_TIMEOUT);
+                /* both stages may hold copies in flight: let them land */
+                mbar_wait(&bar[s], (uint32_t)((k >> 1) & 1), 1LL << 28);
+                if (w + (int)gridDim.x < ntiles)
+                    mbar_wait(&bar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), 1LL << 28);
+            }
+            failed = true;
+            break;
+        }
+        const T *sD = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
+        const T *sr = reinterpret_cast<const T *>(st0 + (size_t)s * stage + szD);
+        T r = T(0);
+        if (act) {
+            r = sr[c * NV + i];
+            sb[c * NV + i] = neg_dinv_row<T>(sD + c * NB + i, sr + c * NV);
+        }
+        double sq = act ? (double)r * (double)r : 0.0;
+        __syncthreads();
+        if (act) b[(size_t)p0 * NV + tid] = sb[tid]; /* contiguous tile store */
+        if (ns.partials) {
+            __shared__ double red[RES_THREADS_FAST / 32];
+            for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+            if ((tid & 31) == 0) red[tid >> 5] = sq;
+            __syncthreads();
+            if (tid == 0) {
+                double tot = 0.0;
+                for (int w2 = 0; w2 < RES_THREADS_FAST / 32; ++w2) tot += red[w2];
+                ns.partials[w] = tot;
+            }
+        }
+        __syncthreads(); /* stage s and sb are free for the iteration after next */
+    }
+    (void)failed;
+    finalize_total(ns, (ns.ntiles > 0 && ns.ntiles < ntiles) ? ns.ntiles : ntiles);
+}
+
+/* shared memory of fast_resid_rhs_kernel: barriers, two stages, b staging */
+template <typename T>
+__host__ __device__ inline size_t resid_rhs_smem_bytes() {
+    return 128 + 2 * (size_t)RES_TILE * (NB + NV) * sizeof(T) + (size_t)RES_TILE * NV * sizeof(T);
 }
 
 /* CTAs of a persistent single-system residual launch: as many as fit */
@@ -825,7 +912,7 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
         Uacc = nullptr;
     }
     if (mode == 0 && !Rsrc) return (int)cudaErrorInvalidValue;
-    const size_t smem = resid_smem_bytes<T>(mode >= 1 ? L.nx : 0);
+    const size_t smem = mode == 0 ? resid_rhs_smem_bytes<T>() : resid_smem_bytes<T>(L.nx);
     if (mode == 3)
         fast_resid_dx_kernel<T><<<resid_grid_persistent((const void *)fast_resid_dx_kernel<T>, smem, grid),
                                   RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, X, L.xnbr, dU, b, Uacc,
@@ -1038,89 +1125,6 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
     }
 }
 
-/* The shuffle form of a chain step: the previous step's vector is taken
- * from the lanes that computed it (lane base + j holds entry j) with warp
- * shuffles, in the pairing of this lane's row (pairs from entry par, the
- * single entry 0 or 8), instead of a round trip through shared memory.
- * The products and their order are row_dot's, so the values are too. */
-template <typename T>
-__device__ __forceinline__ T row_dot_sh(const typename RowOf<T>::type &R, T prev, int base,
-                                        int par, T init) {
-    T v[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) v[k] = __shfl_sync(FULL, prev, base + par + k);
-    const T w = __shfl_sync(FULL, prev, base + (par ? 0 : 8));
-    T a0 = init - R.s * w;
-    T a1 = R.r0.x * v[0];
-    T a2 = R.r0.y * v[1];
-    a0 -= R.r1.x * v[2];
-    a1 += R.r1.y * v[3];
-    a2 += R.r2.x * v[4];
-    a0 -= R.r2.y * v[5];
-    a1 += R.r3.x * v[6];
-    a2 += R.r3.y * v[7];
-    return a0 - (a1 + a2);
-}
-
-/* fwd_chunk with the vector carried in `prev` (this lane's entry of the
- * last valid step) */
-template <typename T, int P, bool CHECK, bool YS>
-__device__ __forceinline__ void fwd_chunk_sh(const T *sG, const T *sB, T &prev, T *ys, T *yg,
-                                             int kbase, int len, int cpos, int i, int base,
-                                             const LaneOff &o) {
-    typename RowOf<T>::type cur_row, next_row;
-    load_row(cur_row, sG, o, 0);
-    T cur_b = sB[i];
-#pragma unroll
-    for (int q = 0; q < P; ++q) {
-        const int odd = q & 1;
-        T next_b = T(0);
-        if (q + 1 < P) {
-            load_row(next_row, sG + (q + 1) * NB, o, odd ^ 1);
-            next_b = sB[(q + 1) * NV + i];
-        }
-        const T yi = row_dot_sh<T>(cur_row, prev, base, (i + odd) & 1, cur_b);
-        if (!CHECK || kbase + q < len) {
-            prev = yi;
-            const int pos = cpos + kbase + q;
-            if (YS)
-                ys[pos * NV + i] = yi;
-            else
-                yg[(size_t)pos * NV + i] = yi;
-        }
-        cur_row = next_row;
-        cur_b = next_b;
-    }
-}
-
-template <typename T, int P, bool CHECK, bool YS>
-__device__ __forceinline__ void bwd_chunk_sh(const T *sG, T &prev, T *ys, const T *yv, const T *uv,
-                                             T *dUl, T *Ul, int kbase, int len, int cpos, int i,
-                                             int base, const LaneOff &o) {
-    typename RowOf<T>::type cur_row, next_row;
-    load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
-#pragma unroll
-    for (int q = P - 1; q >= 0; --q) {
-        const int odd = q & 1;
-        if (q > 0) load_row(next_row, sG + (q - 1) * NB, o, odd ^ 1);
-        const bool valid = !CHECK || (kbase + q >= 0 && kbase + q < len);
-        const int pos = cpos + kbase + q;
-        T yk = T(0);
-        if (valid) yk = YS ? ys[pos * NV + i] : yv[q];
-        const T d = row_dot_sh<T>(cur_row, prev, base, (i + odd) & 1, yk);
-        if (valid) {
-            prev = d;
-            if (YS) {
-                ys[pos * NV + i] = d;
-            } else {
-                dUl[(size_t)pos * NV + i] = d;
-                if (Ul) Ul[(size_t)pos * NV + i] = uv[q] + d;
-            }
-        }
-        cur_row = next_row;
-    }
-}
-
 /* Solve one line (start ps, n cells, twist m) with the warp of the calling
  * CTA.  The staging barriers live at the start of `smem` and stay
  * initialised across the lines that a persistent CTA solves: bit s of
@@ -1132,7 +1136,7 @@ __device__ __forceinline__ void bwd_chunk_sh(const T *sG, T &prev, T *ys, const 
 template <bool WS>
 __host__ __device__ constexpr int thomas_hdr() { return WS ? 256 : 128; }
 
-template <typename T, int P, bool YS, bool WS = false, bool SH = false>
+template <typename T, int P, bool YS, bool WS = false>
 __device__ __forceinline__ bool thomas_line(
     int NS, int accumulate, int ps, int n, int m, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
@@ -1240,8 +1244,6 @@ __device__ __forceinline__ bool thomas_line(
     int consumed = 0;
     bool timed_out = false;
     const int both_full = (m < nb ? m : nb) / P; /* jobs where both chains run P steps */
-    const int base = lane & 16; /* SH: the half-warp's first lane */
-    T prev = T(0);              /* SH: this lane's entry of the chain's last vector */
 
     /* ---------------- forward */
     for (int c = 0; c < nf; ++c) {
@@ -1254,12 +1256,7 @@ __device__ __forceinline__ bool thomas_line(
         ++consumed;
         const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
         const T *sB = sG + P * NB;
-        if (SH) {
-            if (c < both_full)
-                fwd_chunk_sh<T, P, false, YS>(sG, sB, prev, ys, yl, c * P, len, cpos, i, base, off);
-            else
-                fwd_chunk_sh<T, P, true, YS>(sG, sB, prev, ys, yl, c * P, len, cpos, i, base, off);
-        } else if (c < both_full)
+        if (c < both_full)
             fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
         else
             fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
@@ -1273,11 +1270,6 @@ __device__ __forceinline__ bool thomas_line(
     }
 
     if (!timed_out) {
-        if (SH) {
-            /* publish each chain's last vector where the twist reads it */
-            if (li < NV) bc[(len & 1) * 20 + li] = prev;
-            __syncwarp();
-        }
         /* ---------------- twist: x_m = b_m - G_tw y_top - Gam_tw y_bot */
         const int ptw = n - 1; /* relative to ps */
         const T *ytop = bcall + 0 * 40 + (m & 1) * 20;
@@ -1306,7 +1298,6 @@ __device__ __forceinline__ bool thomas_line(
             }
         }
         __syncwarp();
-        if (SH) prev = __shfl_sync(FULL, xm, i); /* both chains start from the twist's vector */
 
         /* ---------------- backward */
         T yv[P], uv[P], nyv[P], nuv[P];
@@ -1337,16 +1328,7 @@ __device__ __forceinline__ bool thomas_line(
             const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
             const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
                               nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
-            if (SH) {
-                if (full)
-                    bwd_chunk_sh<T, P, false, YS>(sG, prev, ys, yv, uv, dUl,
-                                                  accumulate < 2 ? Ul : nullptr, c * P, len, cpos,
-                                                  i, base, off);
-                else
-                    bwd_chunk_sh<T, P, true, YS>(sG, prev, ys, yv, uv, dUl,
-                                                 accumulate < 2 ? Ul : nullptr, c * P, len, cpos,
-                                                 i, base, off);
-            } else if (full)
+            if (full)
                 bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
                                            c * P, len, cpos, i, off);
             else
@@ -1428,7 +1410,7 @@ __device__ __forceinline__ void thomas_init_bars(unsigned char *smem, int NS) {
 }
 
 /* one CTA (one warp) per line */
-template <typename T, int P, bool YS, bool SH = false>
+template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(32) fast_thomas_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
@@ -1440,15 +1422,15 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
     thomas_init_bars(smem, NS);
     const uint64_t pol = threadIdx.x == 0 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS, false, SH>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G,
-                                     Gam, b, y, dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam, b, y,
+                          dU, U, status, smem, pbase, pol);
 }
 
 /* Warp-specialised form, one CTA of two warps per line: warp 1 issues the
  * staging copies, warp 0 runs the chains with the same arithmetic as
  * fast_thomas_kernel, so its results are bit-identical; the chain warp no
  * longer stops every chunk to issue the next copies. */
-template <typename T, int P, bool YS, bool SH = false>
+template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
     int nline, int NS, int accumulate, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
@@ -1471,8 +1453,8 @@ __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
     __syncthreads();
     const uint64_t pol = threadIdx.x == 32 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS, true, SH>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G,
-                                    Gam, b, y, dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS, true>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam,
+                                b, y, dU, U, status, smem, pbase, pol);
 }
 
 /* Persistent form over many systems: each CTA (one warp) takes (system,
@@ -1627,36 +1609,24 @@ static bool thomas_ws(const FastLayout &L) {
     return (L.nline + nsm - 1) / nsm <= 5;
 }
 
-/* The chain step's vector through warp shuffles (1) or a shared-memory
- * round trip (0); TBS_THOMAS_SHFL forces either, for measurements.  Both
- * give the same values. */
-static bool thomas_shfl() {
-    static const int forced = [] {
-        const char *e = getenv("TBS_THOMAS_SHFL");
-        return e && e[0] ? (e[0] == '0' ? 0 : 1) : -1;
-    }();
-    return forced == 1;
-}
-
-template <typename T, bool WS, bool YS, bool SH>
+template <typename T, bool WS, bool YS>
 static const void *thomas_fn() {
-    return WS ? (const void *)fast_thomas_ws_kernel<T, THOMAS_P, YS, SH>
-              : (const void *)fast_thomas_kernel<T, THOMAS_P, YS, SH>;
+    return WS ? (const void *)fast_thomas_ws_kernel<T, THOMAS_P, YS>
+              : (const void *)fast_thomas_kernel<T, THOMAS_P, YS>;
 }
 
 template <typename T, bool WS>
-static const void *thomas_fn(bool ys, bool sh) {
-    return ys ? (sh ? thomas_fn<T, WS, true, true>() : thomas_fn<T, WS, true, false>())
-              : (sh ? thomas_fn<T, WS, false, true>() : thomas_fn<T, WS, false, false>());
+static const void *thomas_fn(bool ys) {
+    return ys ? thomas_fn<T, WS, true>() : thomas_fn<T, WS, false>();
 }
 
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
                        T *y, T *dU, T *U, unsigned *status, int accumulate) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
-    const bool ws = thomas_ws(L), sh = thomas_shfl();
+    const bool ws = thomas_ws(L);
     const ThomasCfg c = ws ? thomas_cfg<T, true>(L) : thomas_cfg<T>(L);
-    const void *fn = ws ? thomas_fn<T, true>(c.ys, sh) : thomas_fn<T, false>(c.ys, sh);
+    const void *fn = ws ? thomas_fn<T, true>(c.ys) : thomas_fn<T, false>(c.ys);
     int ns = c.NS, nline = L.nline;
     const int *ls = L.line_start, *ll = L.line_len, *lt = L.line_twist;
     void *args[] = {&nline, &ns, &accumulate, &ls, &ll, &lt, &G, &Gam, &b, &y, &dU, &U, &status};
@@ -1702,12 +1672,10 @@ int fast_prepare(const FastLayout &L) {
     if (!rc) rc = set_smem((const void *)fast_resid_kernel<float>, resid_smem_bytes<float>(L.nx));
     const ThomasCfg c64 = thomas_cfg<double>(L), c32 = thomas_cfg<float>(L);
     const ThomasCfg w64 = thomas_cfg<double, true>(L), w32 = thomas_cfg<float, true>(L);
-    for (int sh = 0; sh < 2 && !rc; ++sh) {
-        rc = set_smem(thomas_fn<double, false>(c64.ys, sh), c64.smem);
-        if (!rc) rc = set_smem(thomas_fn<float, false>(c32.ys, sh), c32.smem);
-        if (!rc) rc = set_smem(thomas_fn<double, true>(w64.ys, sh), w64.smem);
-        if (!rc) rc = set_smem(thomas_fn<float, true>(w32.ys, sh), w32.smem);
-    }
+    if (!rc) rc = set_smem(thomas_fn<double, false>(c64.ys), c64.smem);
+    if (!rc) rc = set_smem(thomas_fn<float, false>(c32.ys), c32.smem);
+    if (!rc) rc = set_smem(thomas_fn<double, true>(w64.ys), w64.smem);
+    if (!rc) rc = set_smem(thomas_fn<float, true>(w32.ys), w32.smem);
     return rc;
 }
 
@@ -1874,16 +1842,6 @@ __host__ __device__ inline size_t fullpos_smem_bytes(int nxf) {
 
 /* b = -Dinv R of one cell row in FP32, the operation order of the FP32
  * mode-0 residual (fast_resid_body): dr = column-major block row i, rv = R */
-__device__ __forceinline__ float neg_dinv_row(const float *dr, const float *rv) {
-    float a0 = dr[0] * rv[0], a1 = dr[9] * rv[1], a2 = dr[18] * rv[2];
-    a0 += dr[27] * rv[3];
-    a1 += dr[36] * rv[4];
-    a2 += dr[45] * rv[5];
-    a0 += dr[54] * rv[6];
-    a1 += dr[63] * rv[7];
-    a2 += dr[72] * rv[8];
-    return -(a0 + (a1 + a2));
-}
 
 /* One tile of 16 positions (160 threads; thread t < 144 owns cell t % 16,
  * row t / 16).  R = rhs + D u + sum over faces (ef order) offJ u_nbr with
@@ -1966,7 +1924,7 @@ __device__ __forceinline__ bool full_resid_pos_body(
     __syncthreads();
     if (act) R32[(size_t)p0 * NV + tid] = so[tid]; /* contiguous tile store */
     if (Dinv32) {
-        if (act) sb[c * NV + i] = neg_dinv_row(sDi + c * NB + i, so + c * NV);
+        if (act) sb[c * NV + i] = neg_dinv_row<float>(sDi + c * NB + i, so + c * NV);
         __syncthreads();
         if (act) b32[(size_t)p0 * NV + tid] = sb[tid];
     }
@@ -2045,7 +2003,7 @@ __device__ __forceinline__ void mixed_prime_body(const double *__restrict__ rhsp
         __syncthreads();
         if (act) {
             const int c = tid % RES_TILE, i = tid / RES_TILE;
-            b32[((size_t)blk * RES_TILE + c) * NV + i] = neg_dinv_row(sDi + c * NB + i, sR + c * NV);
+            b32[((size_t)blk * RES_TILE + c) * NV + i] = neg_dinv_row<float>(sDi + c * NB + i, sR + c * NV);
         }
     }
     __shared__ double red[RES_THREADS_FAST / 32];
