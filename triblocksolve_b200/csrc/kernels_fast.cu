@@ -786,88 +786,7 @@ template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_rhs_kernel(
     int np16, const T *__restrict__ Dinv, const T *__restrict__ Rsrc, T *__restrict__ b,
     T *__restrict__ Uzero, NormSink ns, unsigned *status) {
-    /* mode 0 (b = -Dinv R and the norm of a given R) with two staging
-     * buffers: the next tile's bulk copies are in flight while this one is
-     * computed.  A tile is a third of a mode-1 tile's bytes and the CTAs
-     * per SM are bounded by threads, not shared memory, so the second
-     * buffer costs no residency.  Per element the expressions of
-     * fast_resid_body's mode 0. */
-    extern __shared__ __align__(128) unsigned char smem[];
-    uint64_t *bar = reinterpret_cast<uint64_t *>(smem);
-    const uint32_t szD = RES_TILE * NB * sizeof(T), szR = RES_TILE * NV * sizeof(T);
-    const uint32_t stage = szD + szR;
-    unsigned char *st0 = smem + 128;
-    T *sb = reinterpret_cast<T *>(st0 + 2 * stage);
-    const int tid = threadIdx.x;
-    const int c = tid % RES_TILE, i = tid / RES_TILE;
-    const bool act = tid < RES_TILE * NV;
-    const int ntiles = np16 / RES_TILE;
-    if (tid == 0) {
-        mbar_init(&bar[0], 1);
-        mbar_init(&bar[1], 1);
-        mbar_fence_init();
-    }
-    __syncthreads();
-    auto issue = [&](int w, int s) {
-        const uint64_t pol = policy_evict_first();
-        unsigned char *dst = st0 + (size_t)s * stage;
-        mbar_arrive_expect_tx(&bar[s], stage);
-        bulk_g2s_hint(dst, Dinv + (size_t)w * RES_TILE * NB, szD, &bar[s], pol);
-        bulk_g2s(dst + szD, Rsrc + (size_t)w * RES_TILE * NV, szR, &bar[s]);
-    };
-    const int first = blockIdx.x;
-    if (tid == 0 && first < ntiles) issue(first, 0);
-    int k = 0;
-    bool failed = false;
-    for (int w = first; w < ntiles; w += gridDim.x, ++k) {
-        const int s = k & 1;
-        /* the other stage was released by the previous iteration's barrier */
-        if (tid == 0 && w + (int)gridDim.x < ntiles) issue(w + gridDim.x, s ^ 1);
-        const int p0 = w * RES_TILE;
-        if (act && Uzero) Uzero[(size_t)p0 * NV + tid] = T(0);
-        const bool ok = mbar_wait(&bar[s], (uint32_t)((k >> 1) & 1));
-        if (__syncthreads_or(!ok)) {
-            if (tid == 0) {
-                atomicOr(status, ST_TIMEOUT);
-                /* both stages may hold copies in flight: let them land */
-                mbar_wait(&bar[s], (uint32_t)((k >> 1) & 1), 1LL << 28);
-                if (w + (int)gridDim.x < ntiles)
-                    mbar_wait(&bar[s ^ 1], (uint32_t)(((k + 1) >> 1) & 1), 1LL << 28);
-            }
-            failed = true;
-            break;
-        }
-        const T *sD = reinterpret_cast<const T *>(st0 + (size_t)s * stage);
-        const T *sr = reinterpret_cast<const T *>(st0 + (size_t)s * stage + szD);
-        T r = T(0);
-        if (act) {
-            r = sr[c * NV + i];
-            sb[c * NV + i] = neg_dinv_row<T>(sD + c * NB + i, sr + c * NV);
-        }
-        double sq = act ? (double)r * (double)r : 0.0;
-        __syncthreads();
-        if (act) b[(size_t)p0 * NV + tid] = sb[tid]; /* contiguous tile store */
-        if (ns.partials) {
-            __shared__ double red[RES_THREADS_FAST / 32];
-            for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
-            if ((tid & 31) == 0) red[tid >> 5] = sq;
-            __syncthreads();
-            if (tid == 0) {
-                double tot = 0.0;
-                for (int w2 = 0; w2 < RES_THREADS_FAST / 32; ++w2) tot += red[w2];
-                ns.partials[w] = tot;
-            }
-        }
-        __syncthreads(); /* stage s and sb are free for the iteration after next */
-    }
-    (void)failed;
-    finalize_total(ns, (ns.ntiles > 0 && ns.ntiles < ntiles) ? ns.ntiles : ntiles);
-}
-
-/* shared memory of fast_resid_rhs_kernel: barriers, two stages, b staging */
-template <typename T>
-__host__ __device__ inline size_t resid_rhs_smem_bytes() {
-    return 128 + 2 * (size_t)RES_TILE * (NB + NV) * sizeof(T) + (size_t)RES_TILE * NV * sizeof(T);
+    resid_tiles<T>(0, np16, 0, Dinv, nullptr, nullptr, nullptr, Rsrc, b, Uzero, ns, status);
 }
 
 /* CTAs of a persistent single-system residual launch: as many as fit */
@@ -912,7 +831,7 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
         Uacc = nullptr;
     }
     if (mode == 0 && !Rsrc) return (int)cudaErrorInvalidValue;
-    const size_t smem = mode == 0 ? resid_rhs_smem_bytes<T>() : resid_smem_bytes<T>(L.nx);
+    const size_t smem = resid_smem_bytes<T>(mode >= 1 ? L.nx : 0);
     if (mode == 3)
         fast_resid_dx_kernel<T><<<resid_grid_persistent((const void *)fast_resid_dx_kernel<T>, smem, grid),
                                   RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, X, L.xnbr, dU, b, Uacc,
