@@ -201,6 +201,25 @@ int tbs_set_rhs(tbs_ctx *ctx, const double *rhs);
  * Checkpoint/resume of a solve; the reference always starts from 0. */
 int tbs_set_initial(tbs_ctx *ctx, const double *U);
 
+/* The next system's Jacobian (host or device pointers, the layout of
+ * tbs_set_jacobian) uploaded into a spare set of device buffers on the
+ * context's own copy stream, while the current system is still being
+ * solved: the call returns at once, and the next tbs_factor waits for the
+ * upload and switches to the staged values (its rhs included).  A stream of
+ * systems then keeps the host-to-device link busy during the solves:
+ *   tbs_stage_jacobian(ctx, J0...);  tbs_factor(ctx, algo);
+ *   for each system k:
+ *     tbs_stage_jacobian(ctx, J[k+1]...);   -- overlaps the solve below
+ *     tbs_solve(ctx, ...);  tbs_get_solution(ctx, U_k);
+ *     tbs_factor(ctx, algo);                -- now the system k+1
+ * The copies overlap the solve only from pinned (page-locked) host memory;
+ * the host arrays must stay unchanged until the tbs_factor that takes them
+ * returns.  tbs_set_jacobian discards a staged set.  The spare set costs
+ * the device memory of one more Jacobian.  No counterpart in the reference,
+ * which reads one Jacobian per run (src/main.cxx:86-93). */
+int tbs_stage_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1,
+                       const double *jacO2, const double *rhs);
+
 /* Replaces copyAtoBjac + lineLU (src/main.cxx:180-190,
  * src/okl/lineLU_v2.okl:58-182, src/okl/linesmoothLU_v5.okl:85-93) and the
  * host packing Jacobian::assembleTriBlocks (src/Jacobian.cxx:76-117).

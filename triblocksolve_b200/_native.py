@@ -79,6 +79,7 @@ _sig("tbs_set_mesh", _i, _vp, _i, _i, _i, _i, _i, _i, _ip, _ip, _ip, _ip, _ip, _
 _sig("tbs_set_jacobian", _i, _vp, _dp, _dp, _dp, _dp, _dp)
 _sig("tbs_set_jacobian_device", _i, _vp, _vp, _vp, _vp, _vp)
 _sig("tbs_set_rhs", _i, _vp, _dp)
+_sig("tbs_stage_jacobian", _i, _vp, _dp, _dp, _dp, _dp)
 _sig("tbs_set_initial", _i, _vp, _dp)
 _sig("tbs_factor", _i, _vp, _i)
 _sig("tbs_sweep", _i, _vp, _i, _dp)

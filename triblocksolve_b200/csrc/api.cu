@@ -111,16 +111,21 @@ static void dfree(tbs_ctx *ctx, T **p) {
 static void drop_graph(tbs_ctx *ctx) {
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->graph) cudaGraphDestroy(ctx->graph);
-    ctx->gexec = nullptr;
-    ctx->graph = nullptr;
-    ctx->graph_algo = -1;
+    if (ctx->gexec_alt) cudaGraphExecDestroy(ctx->gexec_alt);
+    if (ctx->graph_alt) cudaGraphDestroy(ctx->graph_alt);
+    ctx->gexec = ctx->gexec_alt = nullptr;
+    ctx->graph = ctx->graph_alt = nullptr;
+    ctx->graph_algo = ctx->graph_algo_alt = -1;
 }
 
 /* free everything that depends on the mesh */
 static void drop_mesh(tbs_ctx *ctx) {
+    if (ctx->copy) cudaStreamSynchronize(ctx->copy); /* a staged upload may be in flight */
     multi_free(ctx);
     krylov_free(ctx);
     drop_graph(ctx);
+    for (auto &p : ctx->d_spare) p = nullptr; /* freed with the other allocations below */
+    ctx->staged = false;
     for (auto &a : ctx->allocs) cudaFree(a.first);
     ctx->allocs.clear();
     ctx->bytes = 0;
@@ -949,6 +954,9 @@ int tbs_destroy(tbs_ctx *ctx) {
     for (auto ev : ctx->pool) cudaEventDestroy(ev);
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
+    if (ctx->spare_free_ev) cudaEventDestroy(ctx->spare_free_ev);
+    if (ctx->copy) cudaStreamDestroy(ctx->copy);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
     return TBS_OK;
@@ -1082,6 +1090,7 @@ static int upload_jacobian(tbs_ctx *ctx, const double *jacD, const double *O1, c
     /* same mesh -> same allocations, so an instantiated solve graph stays valid */
     ctx->have_jac = true;
     ctx->factored = false;
+    ctx->staged = false; /* these values, not a staged set, are the ones to factor */
     return TBS_OK;
 }
 
@@ -1104,10 +1113,66 @@ int tbs_set_jacobian_device(tbs_ctx *ctx, const double *d_jacD, const double *d_
     GUARD_END
 }
 
+int tbs_stage_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1, const double *jacO2,
+                       const double *rhs) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->have_mesh) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
+    if (!jacD || (ctx->nintface > 0 && (!jacO1 || !jacO2)) || !rhs)
+        return ctx_fail(ctx, TBS_ERR_ARG, "null Jacobian array");
+    if (!ctx->copy) {
+        CK(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
+        CK(cudaEventCreateWithFlags(&ctx->staged_ev, cudaEventDisableTiming));
+        CK(cudaEventCreateWithFlags(&ctx->spare_free_ev, cudaEventDisableTiming));
+    }
+    const size_t nb = (size_t)ctx->nvar * ctx->nvar;
+    DA(ctx->d_spare[0], nb * ctx->nelem);
+    DA(ctx->d_spare[1], nb * ctx->nintface);
+    DA(ctx->d_spare[2], nb * ctx->nintface);
+    DA(ctx->d_spare[3], (size_t)nvec(ctx));
+    /* work already on the context's stream may still read the spare set
+     * (the previous system's true-residual check): the copies wait for it */
+    CK(cudaEventRecord(ctx->spare_free_ev, ctx->stream));
+    CK(cudaStreamWaitEvent(ctx->copy, ctx->spare_free_ev, 0));
+    cudaStream_t c = ctx->copy;
+    CK(cudaMemcpyAsync(ctx->d_spare[0], jacD, nb * ctx->nelem * sizeof(double), cudaMemcpyDefault, c));
+    if (ctx->nintface) {
+        CK(cudaMemcpyAsync(ctx->d_spare[1], jacO1, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
+        CK(cudaMemcpyAsync(ctx->d_spare[2], jacO2, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
+    }
+    CK(cudaMemcpyAsync(ctx->d_spare[3], rhs, (size_t)nvec(ctx) * sizeof(double), cudaMemcpyDefault, c));
+    CK(cudaEventRecord(ctx->staged_ev, c));
+    ctx->staged = true;
+    return TBS_OK;
+    GUARD_END
+}
+
+/* make the staged set the active one (tbs_factor): the context's stream
+ * waits for the upload; the sets and their solve graphs trade places */
+static int take_staged(tbs_ctx *ctx) {
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->staged_ev, 0));
+    std::swap(ctx->d_jacD, ctx->d_spare[0]);
+    std::swap(ctx->d_O1, ctx->d_spare[1]);
+    std::swap(ctx->d_O2, ctx->d_spare[2]);
+    std::swap(ctx->d_rhs, ctx->d_spare[3]);
+    std::swap(ctx->gexec, ctx->gexec_alt);
+    std::swap(ctx->graph, ctx->graph_alt);
+    std::swap(ctx->graph_algo, ctx->graph_algo_alt);
+    ctx->staged = false;
+    ctx->have_jac = true;
+    ctx->factored = false;
+    return TBS_OK;
+}
+
 int tbs_factor(tbs_ctx *ctx, int algo) {
     if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
     GUARD_BEGIN
     CK(cudaSetDevice(ctx->device));
+    if (ctx->staged) {
+        int rs = take_staged(ctx);
+        if (rs) return rs;
+    }
     if (!ctx->have_jac) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_jacobian must come first");
     if (algo != TBS_ALGO_REFERENCE && algo != TBS_ALGO_FP64 && algo != TBS_ALGO_MIXED &&
         algo != TBS_ALGO_PIJ)

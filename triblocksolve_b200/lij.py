@@ -272,6 +272,15 @@ class Solver:
         self._chk(N.lib.tbs_set_jacobian(self.ctx, N.dptr(jacD), N.dptr(jacO1), N.dptr(jacO2),
                                          N.dptr(rhs), None))
 
+    def stage_jacobian_arrays(self, jacD, jacO1, jacO2, rhs):
+        """Upload the next system's Jacobian and rhs while the current one is
+        solved; the next ``factor`` switches to it.  Pass pinned host arrays
+        for the copy to overlap, and keep them unchanged until that
+        ``factor`` returns (this object holds references until then)."""
+        arrs = [np.ascontiguousarray(a, np.float64) for a in (jacD, jacO1, jacO2, rhs)]
+        self._chk(N.lib.tbs_stage_jacobian(self.ctx, *[N.dptr(a) for a in arrs]))
+        self._staged = arrs
+
     def set_jacobian_device(self, d_jacD: int, d_jacO1: int, d_jacO2: int, d_rhs: int):
         self._chk(N.lib.tbs_set_jacobian_device(self.ctx, d_jacD, d_jacO1, d_jacO2, d_rhs))
 
@@ -304,6 +313,7 @@ class Solver:
 
     def factor(self, algo: int = N.ALGO_FP64):
         self._chk(N.lib.tbs_factor(self.ctx, algo))
+        self._staged = None
 
     def sweep(self, n: int) -> np.ndarray:
         h = np.zeros(n + 1)
