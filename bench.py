@@ -865,7 +865,7 @@ def run_partition(args, L, K, shift, tol):
     import triblocksolve_b200 as tbs
     from triblocksolve_b200 import _native as N
     from triblocksolve_b200.partition import (DistExchange, PartitionedSolve, PartitionSolver,
-                                              partition_lines)
+                                              owned_norm_sq, partition_lines)
     ws, rank, local = dist_env()
     torch.cuda.set_device(local)
     dist = Dist(ws, rank, local, "nccl")
@@ -892,6 +892,9 @@ def run_partition(args, L, K, shift, tol):
 
         def allreduce_sum(self, x):
             return x
+
+        def norm_sq_async(self, sweepers):
+            return owned_norm_sq(sweepers, torch.device(f"cuda:{local}"))
 
     run = PartitionedSolve([solver], ex if ex else _Single())
     max_sweeps = 400

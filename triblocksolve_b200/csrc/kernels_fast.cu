@@ -2704,18 +2704,11 @@ int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const doub
  * ended and keeps the graph's loop running while any is active. */
 static size_t multi_resid_smem(int nx, int nr) {
     const int nxa = nx > 0 ? nx : 1;
-    const int ng = nr < MULTI_G ? nr : MULTI_G;
     return 128 + (size_t)RES_TILE * NB * sizeof(double) * (1 + nx) +
-           (size_t)ng * nxa * RES_TILE * NV * sizeof(double) +
-           (size_t)ng * RES_TILE * NV * sizeof(double);
+           (size_t)nr * nxa * RES_TILE * NV * sizeof(double) +
+           (size_t)nr * RES_TILE * NV * sizeof(double);
 }
 
-/* A work item is one tile and a group of up to MULTI_G of the active
- * right-hand sides (the k-th active ones, k in [kb, kb + kn)): the groups
- * of a tile are consecutive items, so the CTAs that take them run at about
- * the same time and the second fetch of the tile's blocks is served by L2.
- * Half the right-hand sides per item halves the registers and staging of a
- * CTA, so more CTAs share an SM and hide each other's load rounds. */
 template <int MODE>
 __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     MultiSys M, const double *__restrict__ Dinv, const double *__restrict__ X,
@@ -2723,8 +2716,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     int use_cond, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned amask_s, ticket;
-    __shared__ double red[MULTI_G][RES_THREADS_FAST / 32];
-    __shared__ double redf[RES_THREADS_FAST / 32];
+    __shared__ double red[MULTI_MAX][RES_THREADS_FAST / 32];
     const int tid = threadIdx.x;
     const int nx = MODE == 1 ? M.nx : 0;
     const int nxa = nx > 0 ? nx : 1;
@@ -2735,8 +2727,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     double *sD = reinterpret_cast<double *>(smem + 128);
     double *sX = sD + RES_TILE * NB;
     double *sg = sX + nx * RES_TILE * NB; /* [k][s][c][i] gathers; mode 0: [k][c][i] R */
-    double *sr = sg + (size_t)MULTI_G * nxa * RES_TILE * NV; /* [k][c][i] R, then b */
-    if (nr < MULTI_G) sr = sg + (size_t)nr * nxa * RES_TILE * NV;
+    double *sr = sg + (size_t)nr * nxa * RES_TILE * NV; /* [k][c][i] R, then b */
     __shared__ int rid[MULTI_MAX]; /* the k-th active right-hand side */
     if (tid == 0) {
         unsigned am = 0;
@@ -2753,59 +2744,49 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     __syncthreads();
     const unsigned amask = amask_s;
     const int nact = __popc(amask);
-    const int ngroups = (nact + MULTI_G - 1) / MULTI_G;
-    const int nitems = ntiles * ngroups;
     const int c = tid % RES_TILE, i = tid / RES_TILE;
     const bool act = tid < RES_TILE * NV;
     const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
     uint32_t parity = 0;
     bool failed = false;
-    for (int w = blockIdx.x; w < nitems; w += gridDim.x) {
-        const int blk = w / ngroups;
-        const int kb = (w - blk * ngroups) * MULTI_G;
-        const int kn = nact - kb < MULTI_G ? nact - kb : MULTI_G;
+    for (int blk = blockIdx.x; blk < ntiles && nact > 0; blk += gridDim.x) {
         const int p0 = blk * RES_TILE;
         if (tid == 0) {
             const uint64_t pol = policy_evict_first();
-            mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : kn * szR));
-            /* a tile read by one item streams through; one read by several
-             * stays in L2 for the others */
-            if (ngroups == 1)
-                bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
-            else
-                bulk_g2s(sD, Dinv + (size_t)p0 * NB, szD, bar);
+            mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : nact * szR));
+            bulk_g2s_hint(sD, Dinv + (size_t)p0 * NB, szD, bar, pol);
             if (MODE == 1) {
-                for (int s = 0; s < nx; ++s) {
-                    const double *src = X + ((size_t)s * M.np16 + p0) * NB;
-                    if (ngroups == 1)
-                        bulk_g2s_hint(sX + s * RES_TILE * NB, src, szD, bar, pol);
-                    else
-                        bulk_g2s(sX + s * RES_TILE * NB, src, szD, bar);
-                }
+                for (int s = 0; s < nx; ++s)
+                    bulk_g2s_hint(sX + s * RES_TILE * NB, X + ((size_t)s * M.np16 + p0) * NB, szD,
+                                  bar, pol);
             } else {
-                for (int k = 0; k < kn; ++k)
-                    bulk_g2s(sg + (size_t)k * RES_TILE * NV,
-                             Rsrc + (size_t)rid[kb + k] * vs + (size_t)p0 * NV, szR, bar);
+                int k = 0;
+                for (int r = 0; r < nr; ++r) {
+                    if (!((amask >> r) & 1u)) continue;
+                    bulk_g2s(sg + (size_t)k * RES_TILE * NV, Rsrc + (size_t)r * vs + (size_t)p0 * NV,
+                             szR, bar);
+                    ++k;
+                }
             }
         }
         if (act) {
             const size_t q = (size_t)p0 * NV + tid;
             if (MODE == 1) {
-                /* every load of the item (the neighbour dU gathers, U and dU
-                 * of each of its right-hand sides) is issued before the first
-                 * store, so that their latencies overlap */
+                /* every load of the tile (the neighbour dU gathers, U and dU
+                 * of each active r) is issued before the first store, so
+                 * that their latencies overlap */
                 int nbr[MULTI_NX];
 #pragma unroll
                 for (int s = 0; s < MULTI_NX; ++s)
                     nbr[s] = s < nx ? __ldg(xnbr + (size_t)s * M.np16 + p0 + c) : -1;
-                double gv[MULTI_G][MULTI_NX], uv[MULTI_G], dv[MULTI_G];
+                double gv[MULTI_MAX][MULTI_NX], uv[MULTI_MAX], dv[MULTI_MAX];
 #pragma unroll
-                for (int k = 0; k < MULTI_G; ++k) {
+                for (int k = 0; k < MULTI_MAX; ++k) {
                     uv[k] = dv[k] = 0.0;
 #pragma unroll
                     for (int s = 0; s < MULTI_NX; ++s) gv[k][s] = 0.0;
-                    if (k < kn) {
-                        const size_t ro = (size_t)rid[kb + k] * vs;
+                    if (k < nact) {
+                        const size_t ro = (size_t)rid[k] * vs;
 #pragma unroll
                         for (int s = 0; s < MULTI_NX; ++s)
                             if (nbr[s] >= 0) gv[k][s] = __ldg(M.dU + ro + (size_t)nbr[s] * NV + i);
@@ -2814,16 +2795,16 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < MULTI_G; ++k) {
-                    if (k < kn) {
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
 #pragma unroll
                         for (int s = 0; s < MULTI_NX; ++s)
                             if (s < nx) sg[((size_t)(k * nx + s) * RES_TILE + c) * NV + i] = gv[k][s];
-                        M.U[(size_t)rid[kb + k] * vs + q] = uv[k] + dv[k];
+                        M.U[(size_t)rid[k] * vs + q] = uv[k] + dv[k];
                     }
                 }
             } else {
-                for (int k = 0; k < kn; ++k) M.U[(size_t)rid[kb + k] * vs + q] = 0.0;
+                for (int k = 0; k < nact; ++k) M.U[(size_t)rid[k] * vs + q] = 0.0;
             }
         }
         const bool ok = mbar_wait(bar, parity);
@@ -2836,26 +2817,25 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
             failed = true;
             break;
         }
-        /* R for each right-hand side of the item: the row of each slot's
-         * block is read once and feeds all of them; per r the products are
-         * added in fast_resid_body's order (slots ascending, three
-         * accumulators) */
-        double sq[MULTI_G];
+        /* R for every active r: the row of each slot's block is read once
+         * and feeds every r; per r the products are added in
+         * fast_resid_body's order (slots ascending, three accumulators) */
+        double sq[MULTI_MAX];
 #pragma unroll
-        for (int k = 0; k < MULTI_G; ++k) sq[k] = 0.0;
+        for (int k = 0; k < MULTI_MAX; ++k) sq[k] = 0.0;
         if (act) {
             if (MODE == 1) {
-                double a0[MULTI_G], a1[MULTI_G], a2[MULTI_G];
+                double a0[MULTI_MAX], a1[MULTI_MAX], a2[MULTI_MAX];
 #pragma unroll
-                for (int k = 0; k < MULTI_G; ++k) a0[k] = a1[k] = a2[k] = 0.0;
+                for (int k = 0; k < MULTI_MAX; ++k) a0[k] = a1[k] = a2[k] = 0.0;
                 for (int s = 0; s < nx; ++s) {
                     const double *xr = sX + (s * RES_TILE + c) * NB + i;
                     double x[NV];
 #pragma unroll
                     for (int j = 0; j < NV; ++j) x[j] = xr[9 * j];
 #pragma unroll
-                    for (int k = 0; k < MULTI_G; ++k) {
-                        if (k < kn) {
+                    for (int k = 0; k < MULTI_MAX; ++k) {
+                        if (k < nact) {
                             const double *g = sg + ((size_t)(k * nx + s) * RES_TILE + c) * NV;
                             a0[k] += x[0] * g[0];
                             a1[k] += x[1] * g[1];
@@ -2870,8 +2850,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                     }
                 }
 #pragma unroll
-                for (int k = 0; k < MULTI_G; ++k) {
-                    if (k < kn) {
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
                         const double rr = a0[k] + (a1[k] + a2[k]);
                         sr[(size_t)k * RES_TILE * NV + c * NV + i] = rr;
                         sq[k] = rr * rr;
@@ -2879,8 +2859,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                 }
             } else {
 #pragma unroll
-                for (int k = 0; k < MULTI_G; ++k) {
-                    if (k < kn) {
+                for (int k = 0; k < MULTI_MAX; ++k) {
+                    if (k < nact) {
                         const double rr = sg[(size_t)k * RES_TILE * NV + c * NV + i];
                         sq[k] = rr * rr;
                     }
@@ -2888,8 +2868,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
             }
         }
         __syncthreads();
-        /* b = -Dinv R for each right-hand side of the item (into sg, free
-         * now); the row of Dinv is read once */
+        /* b = -Dinv R for every active r (into sg, free now); the row of
+         * Dinv is read once */
         const double *rsrc = MODE == 1 ? sr : sg;
         double *sb = MODE == 1 ? sg : sr;
         if (act) {
@@ -2898,8 +2878,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
 #pragma unroll
             for (int j = 0; j < NV; ++j) dr[j] = drow[9 * j];
 #pragma unroll
-            for (int k = 0; k < MULTI_G; ++k) {
-                if (k < kn) {
+            for (int k = 0; k < MULTI_MAX; ++k) {
+                if (k < nact) {
                     const double *rv = rsrc + (size_t)k * RES_TILE * NV + c * NV;
                     double a0 = dr[0] * rv[0], a1 = dr[1] * rv[1], a2 = dr[2] * rv[2];
                     a0 += dr[3] * rv[3];
@@ -2914,14 +2894,17 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         }
         __syncthreads();
         if (act) {
-            for (int k = 0; k < kn; ++k)
-                M.b[(size_t)rid[kb + k] * vs + (size_t)p0 * NV + tid] =
-                    sb[(size_t)k * RES_TILE * NV + tid];
+            int k = 0;
+            for (int r = 0; r < nr; ++r) {
+                if (!((amask >> r) & 1u)) continue;
+                M.b[(size_t)r * vs + (size_t)p0 * NV + tid] = sb[(size_t)k * RES_TILE * NV + tid];
+                ++k;
+            }
         }
         /* the tile's sum R^2 per r, in fast_resid_body's order */
 #pragma unroll
-        for (int k = 0; k < MULTI_G; ++k) {
-            if (k < kn) {
+        for (int k = 0; k < MULTI_MAX; ++k) {
+            if (k < nact) {
                 double v = sq[k];
                 for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(FULL, v, o);
                 if ((tid & 31) == 0) red[k][tid >> 5] = v;
@@ -2929,13 +2912,16 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         }
         __syncthreads();
         if (tid == 0) {
-            for (int k = 0; k < kn; ++k) {
+            int k = 0;
+            for (int r = 0; r < nr; ++r) {
+                if (!((amask >> r) & 1u)) continue;
                 double tot = 0.0;
-                for (int w2 = 0; w2 < RES_THREADS_FAST / 32; ++w2) tot += red[k][w2];
-                M.partials[(size_t)rid[kb + k] * ntiles + blk] = tot;
+                for (int w = 0; w < RES_THREADS_FAST / 32; ++w) tot += red[k][w];
+                M.partials[(size_t)r * ntiles + blk] = tot;
+                ++k;
             }
         }
-        __syncthreads(); /* the next item's copies overwrite the stages */
+        __syncthreads(); /* the next tile's copies overwrite the stages */
     }
     (void)failed;
 
@@ -2954,12 +2940,12 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
         if (!((amask >> r) & 1u)) continue;
         double acc = strided_sum(M.partials + (size_t)r * ntiles, ntiles, (int)blockDim.x);
         for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(FULL, acc, o);
-        __syncthreads(); /* redf of the previous r is read */
-        if ((tid & 31) == 0) redf[tid >> 5] = acc;
+        __syncthreads(); /* red[0] of the previous r is read */
+        if ((tid & 31) == 0) red[0][tid >> 5] = acc;
         __syncthreads();
         if (tid == 0) {
             double tot = 0.0;
-            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += redf[w];
+            for (int w = 0; w < (int)((blockDim.x + 31) >> 5); ++w) tot += red[0][w];
             const double nrm = sqrt(tot);
             SolveState *S = M.state + r;
             if (MODE == 0) {
@@ -2991,14 +2977,12 @@ int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const Mul
     const int ntiles = L.np16 / RES_TILE;
     if (mode == 1) {
         const size_t smem = multi_resid_smem(L.nx, M.nr);
-        const int nitems = ntiles * ((M.nr + MULTI_G - 1) / MULTI_G);
-        multi_resid_kernel<1><<<resid_grid_persistent((const void *)multi_resid_kernel<1>, smem, nitems),
+        multi_resid_kernel<1><<<resid_grid_persistent((const void *)multi_resid_kernel<1>, smem, ntiles),
                                 RES_THREADS_FAST, smem, st>>>(M, Dinv, X, L.xnbr, nullptr,
                                                               cond_handle, use_cond, status);
     } else {
         const size_t smem = multi_resid_smem(0, M.nr);
-        const int nitems = ntiles * ((M.nr + MULTI_G - 1) / MULTI_G);
-        multi_resid_kernel<0><<<resid_grid_persistent((const void *)multi_resid_kernel<0>, smem, nitems),
+        multi_resid_kernel<0><<<resid_grid_persistent((const void *)multi_resid_kernel<0>, smem, ntiles),
                                 RES_THREADS_FAST, smem, st>>>(M, Dinv, nullptr, nullptr, Rsrc,
                                                               cond_handle, use_cond, status);
     }

@@ -287,7 +287,6 @@ int pij_prepare(const FastLayout &L);
  * side, partials [nr][np16 / RES_TILE]. */
 constexpr int MULTI_MAX = 8;
 constexpr int MULTI_NX = 4;     /* cross-line slots per position of the fast layout */
-constexpr int MULTI_G = 4;      /* right-hand sides per work item of the residual launch */
 struct MultiSys {
     int nr, np16, nx, hist_stride;
     double *U, *b, *partials, *hist;

@@ -269,10 +269,12 @@ class LocalExchange:
 
     def norm_sq_async(self, sweepers):
         """Sum of the squared owned norms as a one-element tensor, not yet read."""
-        return _norm_sq(sweepers, self.buf.device)
+        return owned_norm_sq(sweepers, self.buf.device)
 
 
-def _norm_sq(sweepers, device):
+def owned_norm_sq(sweepers, device):
+    """Sum of the sweepers' squared owned norms as a one-element tensor on
+    `device`, formed in stream order without a host read."""
     import torch
     t = torch.zeros(1, dtype=torch.float64, device=device)
     one = torch.empty(1, dtype=torch.float64, device=device)
@@ -335,7 +337,7 @@ class DistExchange:
         """The global sum of the squared owned norms as a one-element tensor:
         the owned norms copied on the device, squared and all-reduced in
         stream order, not yet read by the host."""
-        t = _norm_sq(sweepers, self.torch.device(self.device))
+        t = owned_norm_sq(sweepers, self.torch.device(self.device))
         self.dist.all_reduce(t, group=self.group)
         return t
 
