@@ -983,6 +983,7 @@ def run_partition(args, L, K, shift, tol):
                 "owned_lines_rank0": part.nowned, "halo_lines_rank0": part.nhalo,
                 "halo_bytes_per_sweep_rank0": halo_bytes,
                 "sweeps_per_solve": sweeps_total / args.steps, "true_rel_residual": true_rel,
+                "true_residual_check": {"checks": run.checks, "restarts": run.restarts},
                 "l2": "no flush: every sweep streams the line blocks (> 126 MB L2)",
                 "parallelism": f"line partitions of one mesh over {ws} GPUs, NCCL halo exchange"
                                if ws > 1 else "1 GPU, one partition (host-driven sweep loop)",

@@ -332,6 +332,13 @@ int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm);
 int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
                          int to_line);
 
+/* The true-residual check of a partitioned solve: R = rhs + J U of the
+ * owned cells from the original blocks, the next line solves' input formed
+ * from it (so the sweeps go on from the true residual), its owned norm in
+ * *owned_norm (or, with NULL, kept for tbs_part_owned_norm).  The loop runs
+ * it when the global recursive norm meets the tolerance, as tbs_solve does. */
+int tbs_part_check(tbs_ctx *ctx, double *owned_norm);
+
 /* Waits for the context's stream and reports a device-side failure (a
  * zero pivot, a staging wait that ran out of time) of the launches since
  * the last call that returned a status: the end of a sequence of calls

@@ -85,6 +85,10 @@ def test_partitioned_solve_stops_at_the_same_sweep():
     assert n == nw
     assert np.all(np.abs(hist - hw) <= TOL * hw[0])
     assert np.array_equal(gather_solution(parts, [s.solution() for s in sw], mesh.nelem), Uw)
+    # the convergence was checked against the true residual, as the whole mesh's was
+    assert (run.checks, run.restarts) == (1, 0) and whole.solve_check()[1:] == (1, 0)
+    true = np.sqrt(sum(s.true_residual_norm() ** 2 for s in sw))
+    assert true <= 1e-10 * hist[0] * 1.0000001
     # a second solve of the same partitions repeats the first bit for bit
     n2, hist2 = run.solve(1e-10, 200)
     assert n2 == n and np.array_equal(hist2, hist)

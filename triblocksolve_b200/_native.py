@@ -96,6 +96,7 @@ _sig("tbs_part_line_vector", _i, _vp, _i, _i, _vp, _i)
 _sig("tbs_part_lines_vector", _i, _vp, _i, _i, _ip, _vp, _i)
 _sig("tbs_part_owned_norm", _i, _vp, _vp)
 _sig("tbs_sync", _i, _vp)
+_sig("tbs_part_check", _i, _vp, _dp)
 _sig("tbs_get_solution", _i, _vp, _dp)
 _sig("tbs_get_residual", _i, _vp, _dp)
 _sig("tbs_get_update", _i, _vp, _dp)

@@ -211,6 +211,83 @@ static int timed(tbs_ctx *ctx, const char *name, F &&launch) {
 
 #define RUN(name, call) CKL(timed(ctx, name, [&]() { return (int)(call); }))
 
+/* ======================================== host transfers off the copy engine
+ * Every cudaMemcpyAsync between host and device, whatever its stream, waits
+ * in the copy engine's queue behind the copies issued before it: a 5 GB
+ * staged Jacobian (tbs_stage_jacobian) would hold a solve's 32-byte control
+ * block for the whole upload.  So the solve and factorization paths move
+ * their small words with kernels instead: the control block as kernel
+ * parameters, the state, status and history into mapped pinned host
+ * memory, and a result into the caller's buffer when that is pinned host
+ * memory the device can address. */
+__global__ void set_state_kernel(SolveState *s, double tol, int max_sweeps, int hist_cap) {
+    s->tol = tol;
+    s->max_sweeps = max_sweeps;
+    s->hist_cap = hist_cap;
+}
+
+__global__ void copy_words_kernel(const unsigned long long *__restrict__ src,
+                                  unsigned long long *__restrict__ dst, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        dst[t] = src[t];
+}
+
+static int copy_words(cudaStream_t st, const void *src, void *dst, size_t bytes) {
+    const long long n = (long long)(bytes / 8);
+    const int blocks = (int)std::min<long long>(std::max<long long>((n + 255) / 256, 1), 4 * 148);
+    copy_words_kernel<<<blocks, 256, 0, st>>>(static_cast<const unsigned long long *>(src),
+                                              static_cast<unsigned long long *>(dst), n);
+    return (int)cudaGetLastError();
+}
+
+/* the device address of host memory a kernel may write, or null */
+static void *host_device_view(void *host) {
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return (a.type == cudaMemoryTypeHost && a.devicePointer) ? a.devicePointer : nullptr;
+}
+
+/* device -> host of `bytes` (a multiple of 8, both addresses 8-aligned): a
+ * kernel when the destination is device-addressable pinned memory, else a
+ * copy (which may queue behind a staged upload) */
+static int to_host(tbs_ctx *ctx, void *dst, const void *src, size_t bytes) {
+    void *dv = host_device_view(dst);
+    if (dv && bytes % 8 == 0 && (uintptr_t)dv % 8 == 0 && (uintptr_t)src % 8 == 0) {
+        CKL(copy_words(ctx->stream, src, dv, bytes));
+    } else {
+        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    }
+    return TBS_OK;
+}
+
+/* the mapped host copy of the history, at least n doubles */
+static int ensure_h_hist(tbs_ctx *ctx, int n) {
+    if (n <= ctx->h_hist_cap) return TBS_OK;
+    if (ctx->h_hist) cudaFreeHost(ctx->h_hist);
+    ctx->h_hist = nullptr;
+    ctx->h_hist_dev = nullptr;
+    ctx->h_hist_cap = 0;
+    const int cap = std::max(n, 1024);
+    CK(cudaHostAlloc((void **)&ctx->h_hist, (size_t)cap * sizeof(double), cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void **)&ctx->h_hist_dev, ctx->h_hist, 0));
+    ctx->h_hist_cap = cap;
+    return TBS_OK;
+}
+
+/* the first n norms of the device history into `out` (host) */
+static int hist_to_host(tbs_ctx *ctx, double *out, int n) {
+    int rc = ensure_h_hist(ctx, n);
+    if (rc) return rc;
+    CKL(copy_words(ctx->stream, ctx->d_hist, ctx->h_hist_dev, (size_t)n * sizeof(double)));
+    CK(cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, ctx->h_hist, (size_t)n * sizeof(double));
+    return TBS_OK;
+}
+
 int ctx_prof_begin(tbs_ctx *ctx, const char *name) {
     if (!ctx->prof || capturing(ctx)) return -1;
     if (ctx->pending.size() > 4000) prof_resolve(ctx);
@@ -390,8 +467,9 @@ static int build_layout(tbs_ctx *ctx) {
 /* ============================================================ sequences */
 
 static int status_check(tbs_ctx *ctx) {
-    CK(cudaMemcpyAsync(ctx->h_status, ctx->d_status, sizeof(unsigned), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+    /* the status word (4 bytes) travels in an 8-byte copy: h_status and
+     * d_status are 8-byte allocations */
+    CKL(copy_words(ctx->stream, ctx->d_status, ctx->h_status_dev, 8));
     CK(cudaStreamSynchronize(ctx->stream));
     const unsigned s = *ctx->h_status;
     if (s) {
@@ -670,17 +748,15 @@ int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps) {
     h->tol = tol;
     h->max_sweeps = max_sweeps;
     h->hist_cap = ctx->hist_cap;
-    const size_t off = offsetof(SolveState, tol);
-    const size_t end = offsetof(SolveState, hist_cap) + sizeof(int);
-    CK(cudaMemcpyAsync(reinterpret_cast<char *>(ctx->d_state) + off,
-                       reinterpret_cast<char *>(h) + off, end - off,
-                       cudaMemcpyHostToDevice, ctx->stream));
+    set_state_kernel<<<1, 1, 0, ctx->stream>>>(ctx->d_state, tol, max_sweeps, ctx->hist_cap);
+    CK(cudaGetLastError());
     return TBS_OK;
 }
 
+static_assert(sizeof(SolveState) % 8 == 0, "SolveState is copied in 8-byte words");
+
 static int read_state(tbs_ctx *ctx) {
-    CK(cudaMemcpyAsync(ctx->h_state, ctx->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost,
-                       ctx->stream));
+    CKL(copy_words(ctx->stream, ctx->d_state, ctx->h_state_dev, sizeof(SolveState)));
     CK(cudaStreamSynchronize(ctx->stream));
     return TBS_OK;
 }
@@ -928,8 +1004,10 @@ int tbs_create(int device_id, tbs_ctx **out) {
     ctx->device = device_id;
     e = cudaSetDevice(device_id);
     if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&ctx->own, cudaStreamNonBlocking);
-    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_state, sizeof(SolveState));
-    if (e == cudaSuccess) e = cudaMallocHost((void **)&ctx->h_status, sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&ctx->h_state, sizeof(SolveState), cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&ctx->h_state_dev, ctx->h_state, 0);
+    if (e == cudaSuccess) e = cudaHostAlloc((void **)&ctx->h_status, 8, cudaHostAllocMapped);
+    if (e == cudaSuccess) e = cudaHostGetDevicePointer((void **)&ctx->h_status_dev, ctx->h_status, 0);
     if (e == cudaSuccess) e = (cudaError_t)fast_kernels_init();
     if (e != cudaSuccess) {
         std::string msg = std::string("device setup failed: ") + cudaGetErrorString(e);
@@ -954,6 +1032,7 @@ int tbs_destroy(tbs_ctx *ctx) {
     for (auto ev : ctx->pool) cudaEventDestroy(ev);
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
+    if (ctx->h_hist) cudaFreeHost(ctx->h_hist);
     if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
     if (ctx->spare_free_ev) cudaEventDestroy(ctx->spare_free_ev);
     if (ctx->copy) cudaStreamDestroy(ctx->copy);
@@ -1000,9 +1079,10 @@ static int set_mesh(tbs_ctx *ctx, int nhalo, int nvar, int nelem, int nintface, 
     drop_mesh(ctx);
     ctx->nhalo = nhalo;
     ctx->nelem_own = nelem_own;
-    CK(cudaMalloc((void **)&ctx->d_status, sizeof(unsigned)));
-    ctx->allocs.push_back({ctx->d_status, sizeof(unsigned)});
-    CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
+    /* 8 bytes: the status word is read back in one 8-byte copy */
+    CK(cudaMalloc((void **)&ctx->d_status, 8));
+    ctx->allocs.push_back({ctx->d_status, 8});
+    CK(cudaMemsetAsync(ctx->d_status, 0, 8, ctx->stream));
     DA(ctx->d_state, 1);
     ctx->nvar = nvar;
     ctx->nelem = nelem;
@@ -1255,8 +1335,10 @@ int tbs_sweep(tbs_ctx *ctx, int n, double *rnorm_out) {
         rc = body(ctx, CondCtl{}, inner_for_next(ctx));
         if (rc) return rc;
     }
-    if (rnorm_out)
-        CK(cudaMemcpyAsync(rnorm_out, ctx->d_hist, (n + 1) * sizeof(double), cudaMemcpyDeviceToHost, st));
+    if (rnorm_out) {
+        rc = hist_to_host(ctx, rnorm_out, n + 1);
+        if (rc) return rc;
+    }
     CK(cudaStreamSynchronize(st));
     if (ctx->prof) prof_resolve(ctx);
     return status_check(ctx);
@@ -1313,9 +1395,10 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
     }
     const int sw = ctx->h_state->sweep;
     if (sweeps_out) *sweeps_out = sw;
-    if (hist_out)
-        CK(cudaMemcpyAsync(hist_out, ctx->d_hist, (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double),
-                           cudaMemcpyDeviceToHost, st));
+    if (hist_out) {
+        rc = hist_to_host(ctx, hist_out, std::min(sw, max_sweeps) + 1);
+        if (rc) return rc;
+    }
     CK(cudaStreamSynchronize(st));
     return status_check(ctx);
     GUARD_END
@@ -1361,7 +1444,8 @@ static int get_vec(tbs_ctx *ctx, int which, double *out) {
         }
         src = ctx->d_scratch;
     }
-    CK(cudaMemcpyAsync(out, src, vb, cudaMemcpyDeviceToHost, st));
+    int rc = to_host(ctx, out, src, vb);
+    if (rc) return rc;
     CK(cudaStreamSynchronize(st));
     return TBS_OK;
 }
@@ -1771,6 +1855,25 @@ int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf, int t
     else
         CK(cudaMemcpyAsync(d_buf, v, bytes, cudaMemcpyDefault, ctx->stream));
     return TBS_OK;
+    GUARD_END
+}
+
+int tbs_part_check(tbs_ctx *ctx, double *owned_norm) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    int rc = part_check(ctx);
+    if (rc) return rc;
+    /* R = rhs + J U of the owned cells (their halo neighbours' U are the
+     * owners' copies), b = -Dinv R for the next line solves, owned norm */
+    cudaStream_t st = ctx->stream;
+    RUN("full_resid", launch_full_resid<double>(st, ctx->nelem_own, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
+                                                ctx->L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
+                                                ctx->d_rhs, ctx->d_Up, ctx->d_Rp, ctx->d_partials2));
+    RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b,
+                                    sink(ctx, NORM_CHECK, CondCtl{}), nullptr));
+    if (!owned_norm) return TBS_OK;
+    return part_norm(ctx, owned_norm);
     GUARD_END
 }
 

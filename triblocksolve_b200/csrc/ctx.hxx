@@ -79,11 +79,16 @@ struct tbs_ctx {
     double *d_partials = nullptr, *d_partials2 = nullptr;
     int npart_cap = 0;
     tbs::SolveState *d_state = nullptr;
-    tbs::SolveState *h_state = nullptr; /* pinned */
+    tbs::SolveState *h_state = nullptr; /* pinned, mapped: written by a kernel */
+    tbs::SolveState *h_state_dev = nullptr; /* its device address */
     double *d_hist = nullptr;
     int hist_cap = 0;
+    double *h_hist = nullptr;     /* pinned, mapped copy of the history for the host */
+    double *h_hist_dev = nullptr;
+    int h_hist_cap = 0;
     unsigned *d_status = nullptr;
-    unsigned *h_status = nullptr; /* pinned */
+    unsigned *h_status = nullptr; /* pinned, mapped */
+    unsigned *h_status_dev = nullptr;
     unsigned *d_counter = nullptr; /* last-CTA ticket of the fused norm */
     int algo = -1;
 

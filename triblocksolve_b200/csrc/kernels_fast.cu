@@ -317,129 +317,172 @@ __device__ __forceinline__ void gj_invert_cols(double (&w)[NV], int j, unsigned 
     }
 }
 
-/* One warp per chain (grid = 2 x lines), lane j < 9 owning column j of
- * every block; the matrix that all lanes need in a product (Dinv_{s-1},
- * A_s, Dinv_s) is published in shared memory and read by broadcast. */
+/* Gauss-Jordan inverse of a 9x9 block held by 27 lanes: lane j + 9g
+ * (column j, row group g) holds rows 3g..3g+2 of column j in w[0..2].  For
+ * pivot p, the pivot column's entries of this lane's rows come from lane
+ * p + 9g, the pivot row's entry of this column and the pivot from the lanes
+ * of row group p / 3 (their w[p % 3]).  Each entry is updated with the
+ * operations of gj_invert_cols; no pivoting, as the reference's LU has none. */
+__device__ __forceinline__ void gj_invert_27(double (&w)[3], int j, int g, unsigned *status) {
+#pragma unroll
+    for (int p = 0; p < NV; ++p) {
+        const int pg = p / 3, pr = p % 3;
+        double colp[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) colp[k] = __shfl_sync(FULL, w[k], p + 9 * g);
+        const double rowp = __shfl_sync(FULL, w[pr], j + 9 * pg);
+        const double piv = __shfl_sync(FULL, w[pr], p + 9 * pg);
+        if (threadIdx.x == 0 && !(fabs(piv) > 0.0 && isfinite(piv))) atomicOr(status, ST_PIVOT);
+        const double r = __drcp_rn(piv);
+        const bool isp = (j == p);
+        const double t = rowp * r;
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            if (3 * g + k != p)
+                w[k] = isp ? -colp[k] * r : w[k] - colp[k] * t;
+            else
+                w[k] = isp ? r : t;
+        }
+    }
+}
+
+/* One warp per chain (grid = 2 x lines).  Lane j + 9g (27 lanes) owns rows
+ * 3g..3g+2 of column j of every block, so 27 lanes share each product and
+ * each pivot step; lanes 27..31 repeat lanes 18..22 and store nothing.  The
+ * blocks every lane needs whole (Dinv_{s-1}, C, A, Gam_{s-1}, Dinv_s) are
+ * published in shared memory.  Per entry the products add q = 0..8 in
+ * order, as the column-per-lane form did. */
 __global__ void __launch_bounds__(32) fast_factor_kernel(
     int nline, const int *__restrict__ line_start, const int *__restrict__ line_len,
     const int *__restrict__ line_twist, const int *__restrict__ fsrc,
     const double *__restrict__ jacD, const double *__restrict__ O1, const double *__restrict__ O2,
     FactorOut out, double *__restrict__ gamlast, unsigned *status) {
-    const int l = blockIdx.x >> 1, g = blockIdx.x & 1;
+    const int l = blockIdx.x >> 1, chain = blockIdx.x & 1;
     if (l >= nline) return;
     const int lane = threadIdx.x;
-    const int j = lane < NV ? lane : NV - 1;
-    const bool act = lane < NV;
-    __shared__ double sM[NB], sA[NB];
+    const bool act = lane < 27;
+    const int jj = act ? lane % 9 : lane - 27; /* column */
+    const int gg = act ? lane / 9 : 2;         /* row group: rows 3gg .. 3gg+2 */
+    const int r0 = 3 * gg;
+    __shared__ double sM[NB], sA[NB], sC[NB], sG[NB];
     const int ps = line_start[l], n = line_len[l], m = line_twist[l];
-    const int len = g ? n - 1 - m : m;
-    const int cs = ps + (g ? m : 0);
+    const int len = chain ? n - 1 - m : m;
+    const int cs = ps + (chain ? m : 0);
     const int ptw = ps + n - 1;
     if (len == 0) {
-        for (int t = lane; t < NB; t += 32) gamlast[((size_t)l * 2 + g) * NB + t] = 0.0;
+        for (int t = lane; t < NB; t += 32) gamlast[((size_t)l * 2 + chain) * NB + t] = 0.0;
         return;
     }
-    double w[NV], an[NV], cn[NV], dn[NV];
+    double w[3], an[3], cn[3], dn[3];
     {
-        const double *D0 = jacD + (size_t)fsrc[5 * cs] * NB + NV * j;
+        const double *D0 = jacD + (size_t)fsrc[5 * cs] * NB + NV * jj + r0;
 #pragma unroll
-        for (int i = 0; i < NV; ++i) w[i] = D0[i];
+        for (int k = 0; k < 3; ++k) w[k] = D0[k];
     }
     auto fetch = [&](int p) {
         const int e = fsrc[5 * p], f = fsrc[5 * p + 1], side = fsrc[5 * p + 2];
-        const double *Ap = (side ? O2 : O1) + (size_t)f * NB + NV * j;
-        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * j;
-        const double *Dp = jacD + (size_t)e * NB + NV * j;
+        const double *Ap = (side ? O2 : O1) + (size_t)f * NB + NV * jj + r0;
+        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * jj + r0;
+        const double *Dp = jacD + (size_t)e * NB + NV * jj + r0;
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            an[i] = Ap[i];
-            cn[i] = Cp[i];
-            dn[i] = Dp[i];
+        for (int k = 0; k < 3; ++k) {
+            an[k] = Ap[k];
+            cn[k] = Cp[k];
+            dn[k] = Dp[k];
         }
     };
     if (len > 1) fetch(cs + 1);
-    gj_invert_cols(w, j, status);
+    gj_invert_27(w, jj, gg, status);
     if (act) {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            out.put_dinv(cs, i + NV * j, w[i]);
-            out.put_g(cs, i, j, 0.0);
-            sM[i + NV * j] = w[i];
+        for (int k = 0; k < 3; ++k) {
+            out.put_dinv(cs, r0 + k + NV * jj, w[k]);
+            out.put_g(cs, r0 + k, jj, 0.0);
+            sM[r0 + k + NV * jj] = w[k];
         }
     }
     for (int s = 1; s < len; ++s) {
         const int p = cs + s;
-        double a[NV], c[NV], d[NV];
+        double a[3], c[3], d[3];
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            a[i] = an[i];
-            c[i] = cn[i];
-            d[i] = dn[i];
+        for (int k = 0; k < 3; ++k) {
+            a[k] = an[k];
+            c[k] = cn[k];
+            d[k] = dn[k];
         }
         if (s + 1 < len) fetch(p + 1);
+        if (act) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                sC[r0 + k + NV * jj] = c[k];
+                sA[r0 + k + NV * jj] = a[k];
+            }
+        }
         __syncwarp();
         /* Gam_{s-1}(:, j) = Dinv_{s-1} C(:, j) */
-        double gm[NV];
+        double gm[3];
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
+        for (int k = 0; k < 3; ++k) {
             double acc = 0.0;
 #pragma unroll
-            for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * c[q];
-            gm[i] = acc;
+            for (int q = 0; q < NV; ++q) acc += sM[r0 + k + NV * q] * sC[q + NV * jj];
+            gm[k] = acc;
         }
         if (act) {
 #pragma unroll
-            for (int i = 0; i < NV; ++i) {
-                out.put_gam(p - 1, i, j, gm[i]);
-                sA[i + NV * j] = a[i];
+            for (int k = 0; k < 3; ++k) {
+                out.put_gam(p - 1, r0 + k, jj, gm[k]);
+                sG[r0 + k + NV * jj] = gm[k];
             }
         }
         __syncwarp();
         /* W(:, j) = D(:, j) - A Gam_{s-1}(:, j) */
 #pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            double acc = d[i];
+        for (int k = 0; k < 3; ++k) {
+            double acc = d[k];
 #pragma unroll
-            for (int q = 0; q < NV; ++q) acc -= sA[i + NV * q] * gm[q];
-            w[i] = acc;
+            for (int q = 0; q < NV; ++q) acc -= sA[r0 + k + NV * q] * sG[q + NV * jj];
+            w[k] = acc;
         }
-        gj_invert_cols(w, j, status);
-        __syncwarp();
+        gj_invert_27(w, jj, gg, status);
+        __syncwarp(); /* every lane has read Dinv_{s-1} */
         if (act) {
 #pragma unroll
-            for (int i = 0; i < NV; ++i) {
-                out.put_dinv(p, i + NV * j, w[i]);
-                sM[i + NV * j] = w[i];
+            for (int k = 0; k < 3; ++k) {
+                out.put_dinv(p, r0 + k + NV * jj, w[k]);
+                sM[r0 + k + NV * jj] = w[k];
             }
         }
         __syncwarp();
         /* G_s(:, j) = Dinv_s A(:, j) */
         if (act) {
 #pragma unroll
-            for (int i = 0; i < NV; ++i) {
+            for (int k = 0; k < 3; ++k) {
                 double acc = 0.0;
 #pragma unroll
-                for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * a[q];
-                out.put_g(p, i, j, acc);
+                for (int q = 0; q < NV; ++q) acc += sM[r0 + k + NV * q] * sA[q + NV * jj];
+                out.put_g(p, r0 + k, jj, acc);
             }
         }
+        __syncwarp(); /* sA and sC are rewritten by the next cell */
     }
     /* coupling of the chain's last cell to the twist: Gam = Dinv_last block(row last, col m) */
     {
-        const int f = fsrc[5 * ptw + (g ? 3 : 1)], side = fsrc[5 * ptw + (g ? 4 : 2)];
-        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * j;
-        double c[NV];
+        const int f = fsrc[5 * ptw + (chain ? 3 : 1)], side = fsrc[5 * ptw + (chain ? 4 : 2)];
+        const double *Cp = (side ? O1 : O2) + (size_t)f * NB + NV * jj + r0;
+        if (act) {
 #pragma unroll
-        for (int i = 0; i < NV; ++i) c[i] = Cp[i];
+            for (int k = 0; k < 3; ++k) sC[r0 + k + NV * jj] = Cp[k];
+        }
         __syncwarp();
         if (act) {
 #pragma unroll
-            for (int i = 0; i < NV; ++i) {
+            for (int k = 0; k < 3; ++k) {
                 double acc = 0.0;
 #pragma unroll
-                for (int q = 0; q < NV; ++q) acc += sM[i + NV * q] * c[q];
-                out.put_gam(cs + len - 1, i, j, acc);
-                gamlast[((size_t)l * 2 + g) * NB + i + NV * j] = acc; /* column-major, FP64 */
+                for (int q = 0; q < NV; ++q) acc += sM[r0 + k + NV * q] * sC[q + NV * jj];
+                out.put_gam(cs + len - 1, r0 + k, jj, acc);
+                gamlast[((size_t)l * 2 + chain) * NB + r0 + k + NV * jj] = acc; /* column-major, FP64 */
             }
         }
     }

@@ -234,6 +234,11 @@ int main(int argc, char **argv) {
             hist.assign((size_t)max_sweeps + 1, 0.0);
             if (tbs_solve(ctx, tol, max_sweeps, &sweeps, hist.data()) != TBS_OK)
                 throw std::runtime_error(tbs_last_error(ctx));
+            double tn = -1.0;
+            int checks = 0, restarts = 0;
+            if (tbs_solve_check(ctx, &tn, &checks, &restarts) == TBS_OK && checks > 0)
+                std::printf("  true-residual check at convergence: %d check(s), %d restart(s), "
+                            "||rhs + J U|| = %.10e\n", checks, restarts, tn);
         } else {
             hist.assign((size_t)iters + 1, 0.0);
             if (tbs_sweep(ctx, iters, hist.data()) != TBS_OK) throw std::runtime_error(tbs_last_error(ctx));

@@ -202,6 +202,11 @@ class PartitionSolver(Solver):
         """tbs_part_line_res without reading the norm (no host synchronisation)."""
         self._chk(N.lib.tbs_part_line_res(self.ctx, None))
 
+    def check_async(self) -> None:
+        """tbs_part_check without reading the norm: the true residual of the
+        owned cells and the next line solves' input formed from it."""
+        self._chk(N.lib.tbs_part_check(self.ctx, None))
+
     def owned_norm_to(self, t) -> None:
         """The owned norm into the one-element tensor ``t``, in stream order."""
         self._chk(N.lib.tbs_part_owned_norm(self.ctx, C.c_void_p(t.data_ptr())))
@@ -348,8 +353,10 @@ class PartitionedSolve:
     (``LocalExchange`` or ``DistExchange``).  The convergence test is the
     one of ``tbs_solve`` on the global norm."""
 
-    def __init__(self, sweepers: list, exchange):
+    def __init__(self, sweepers: list, exchange, check: bool = True):
         self.sweepers, self.ex = sweepers, exchange
+        self.check = check  # the true-residual check at convergence, as tbs_solve's
+        self.checks = self.restarts = 0
 
     def _global(self, norms) -> float:
         return math.sqrt(self.ex.allreduce_sum(sum(n * n for n in norms)))
@@ -385,9 +392,16 @@ class PartitionedSolve:
         is discarded: U and the norms are those of the last sweep counted;
         the context's last update (tbs_get_update) is the discarded one.
         Every rank takes the same decisions from the same global norm, so
-        the collectives stay matched."""
+        the collectives stay matched.
+
+        When the recursive norm meets the tolerance, the true residual
+        rhs + J U is formed from the original blocks (tbs_part_check) and
+        its global norm decides: at or below the tolerance the solve ends
+        with the history unchanged; above it, that norm replaces the last
+        entry and the sweeps go on from the true residual."""
         n0 = self.start()
         hist = [n0]
+        self.checks = self.restarts = 0
         go = lambda g: math.isfinite(g) and g > rel_tol * n0
         if max_sweeps < 1 or not go(n0):
             return 0, np.array(hist)
@@ -399,8 +413,27 @@ class PartitionedSolve:
                 self._solve_and_exchange()
             g = math.sqrt(float(pending.item()))
             hist.append(g)
-            if not (more and go(g)):
+            if go(g):
+                if not more:
+                    break
+                pending = self._line_res()
+                continue
+            if not (self.check and math.isfinite(g)):
                 break
+            for s in self.sweepers:
+                s.check_async()
+            t = math.sqrt(float(self.ex.norm_sq_async(self.sweepers).item()))
+            self.checks += 1
+            if t <= rel_tol * n0:
+                break
+            if not math.isfinite(t):
+                hist[-1] = t
+                break
+            self.restarts += 1
+            hist[-1] = t
+            if not more:
+                break
+            self._solve_and_exchange()  # from the true residual: the speculative one is stale
             pending = self._line_res()
         for s in self.sweepers:
             s.sync()
