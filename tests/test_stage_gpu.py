@@ -3,10 +3,10 @@ stream while the current one is solved, switched in by tbs_factor.
 
 Every result of a staged pipeline must be bit-identical to the same system
 set with tbs_set_jacobian and solved alone (the same kernels on the same
-values; only the buffers and the solve graph in use differ), for the FP64,
-mixed and reference-order algorithms, with the solve graph of each buffer
-set reused across switches; a batch over a context that switched sets must
-see the new values.
+values), for the FP64, mixed and reference-order algorithms, with one solve
+graph reused across switches (the first stage, with no active set yet,
+adopts the landing buffers; later ones are copied over the active set); a
+batch over a context that switched sets must see the new values.
 """
 import numpy as np
 import pytest

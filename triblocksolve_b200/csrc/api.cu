@@ -111,11 +111,9 @@ static void dfree(tbs_ctx *ctx, T **p) {
 static void drop_graph(tbs_ctx *ctx) {
     if (ctx->gexec) cudaGraphExecDestroy(ctx->gexec);
     if (ctx->graph) cudaGraphDestroy(ctx->graph);
-    if (ctx->gexec_alt) cudaGraphExecDestroy(ctx->gexec_alt);
-    if (ctx->graph_alt) cudaGraphDestroy(ctx->graph_alt);
-    ctx->gexec = ctx->gexec_alt = nullptr;
-    ctx->graph = ctx->graph_alt = nullptr;
-    ctx->graph_algo = ctx->graph_algo_alt = -1;
+    ctx->gexec = nullptr;
+    ctx->graph = nullptr;
+    ctx->graph_algo = -1;
 }
 
 /* free everything that depends on the mesh */
@@ -233,11 +231,24 @@ __global__ void copy_words_kernel(const unsigned long long *__restrict__ src,
         dst[t] = src[t];
 }
 
+__global__ void copy_quads_kernel(const uint4 *__restrict__ src, uint4 *__restrict__ dst, long long n) {
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
+         t += (long long)gridDim.x * blockDim.x)
+        dst[t] = src[t];
+}
+
+/* `bytes` (a multiple of 8) from src to dst, 8-byte aligned, on the SMs;
+ * 16-byte words when both addresses and the size allow */
 static int copy_words(cudaStream_t st, const void *src, void *dst, size_t bytes) {
-    const long long n = (long long)(bytes / 8);
+    const bool quads = bytes % 16 == 0 && (uintptr_t)src % 16 == 0 && (uintptr_t)dst % 16 == 0;
+    const long long n = (long long)(bytes / (quads ? 16 : 8));
     const int blocks = (int)std::min<long long>(std::max<long long>((n + 255) / 256, 1), 4 * 148);
-    copy_words_kernel<<<blocks, 256, 0, st>>>(static_cast<const unsigned long long *>(src),
-                                              static_cast<unsigned long long *>(dst), n);
+    if (quads)
+        copy_quads_kernel<<<blocks, 256, 0, st>>>(static_cast<const uint4 *>(src),
+                                                  static_cast<uint4 *>(dst), n);
+    else
+        copy_words_kernel<<<blocks, 256, 0, st>>>(static_cast<const unsigned long long *>(src),
+                                                  static_cast<unsigned long long *>(dst), n);
     return (int)cudaGetLastError();
 }
 
@@ -1229,16 +1240,35 @@ int tbs_stage_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1, co
 }
 
 /* make the staged set the active one (tbs_factor): the context's stream
- * waits for the upload; the sets and their solve graphs trade places */
+ * waits for the upload, then a kernel copies the landed set over the active
+ * buffers.  The active buffers keep their addresses, so the solve graph
+ * captured on them stays the one launched: a graph launched for the first
+ * time since another was launched on the stream re-uploads itself through
+ * the copy engine, which would hold the solve behind the next system's
+ * staged upload. */
 static int take_staged(tbs_ctx *ctx) {
     CK(cudaStreamWaitEvent(ctx->stream, ctx->staged_ev, 0));
-    std::swap(ctx->d_jacD, ctx->d_spare[0]);
-    std::swap(ctx->d_O1, ctx->d_spare[1]);
-    std::swap(ctx->d_O2, ctx->d_spare[2]);
-    std::swap(ctx->d_rhs, ctx->d_spare[3]);
-    std::swap(ctx->gexec, ctx->gexec_alt);
-    std::swap(ctx->graph, ctx->graph_alt);
-    std::swap(ctx->graph_algo, ctx->graph_algo_alt);
+    if (!ctx->d_jacD) {
+        /* no active set yet (nothing set before the first stage), so no
+         * graph holds its addresses: the landed set becomes the active one
+         * and the next stage allocates a new landing set */
+        for (int k = 0; k < 4; ++k) {
+            double **act[] = {&ctx->d_jacD, &ctx->d_O1, &ctx->d_O2, &ctx->d_rhs};
+            *act[k] = ctx->d_spare[k];
+            ctx->d_spare[k] = nullptr;
+        }
+        ctx->staged = false;
+        ctx->have_jac = true;
+        ctx->factored = false;
+        return TBS_OK;
+    }
+    const size_t nb = (size_t)ctx->nvar * ctx->nvar * sizeof(double);
+    CKL(copy_words(ctx->stream, ctx->d_spare[0], ctx->d_jacD, nb * ctx->nelem));
+    if (ctx->nintface) {
+        CKL(copy_words(ctx->stream, ctx->d_spare[1], ctx->d_O1, nb * ctx->nintface));
+        CKL(copy_words(ctx->stream, ctx->d_spare[2], ctx->d_O2, nb * ctx->nintface));
+    }
+    CKL(copy_words(ctx->stream, ctx->d_spare[3], ctx->d_rhs, (size_t)nvec(ctx) * sizeof(double)));
     ctx->staged = false;
     ctx->have_jac = true;
     ctx->factored = false;

@@ -96,16 +96,11 @@ struct tbs_ctx {
     cudaGraphExec_t gexec = nullptr;
     cudaGraph_t graph = nullptr;
     int graph_algo = -1;
-    /* the solve graph of the other block set (a graph holds the addresses of
-     * the set that was active when it was captured; they trade places when
-     * tbs_factor switches to a staged set) */
-    cudaGraphExec_t gexec_alt = nullptr;
-    cudaGraph_t graph_alt = nullptr;
-    int graph_algo_alt = -1;
 
     /* ---- a staged Jacobian (tbs_stage_jacobian): the next system's jacD,
-     * O1, O2 and rhs, uploaded on the copy stream into a spare set while
-     * the current system is solved; tbs_factor switches the sets ---- */
+     * O1, O2 and rhs, uploaded on the copy stream into a landing set while
+     * the current system is solved; tbs_factor copies it over the active
+     * set on the device ---- */
     double *d_spare[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaStream_t copy = nullptr;
     cudaEvent_t staged_ev = nullptr;     /* the staged upload has landed */
