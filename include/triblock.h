@@ -202,23 +202,27 @@ int tbs_set_rhs(tbs_ctx *ctx, const double *rhs);
 int tbs_set_initial(tbs_ctx *ctx, const double *U);
 
 /* The next system's Jacobian (host or device pointers, the layout of
- * tbs_set_jacobian) uploaded into a spare set of device buffers on the
+ * tbs_set_jacobian) uploaded into a landing set of device buffers on the
  * context's own copy stream, while the current system is still being
- * solved: the call returns at once, and the next tbs_factor waits for the
- * upload and switches to the staged values (its rhs included).  A stream of
- * systems then keeps the host-to-device link busy during the solves:
- *   tbs_stage_jacobian(ctx, J0...);  tbs_factor(ctx, algo);
+ * solved: the call returns at once, and a later tbs_factor waits for the
+ * upload and switches to the staged values (its rhs included).  Up to two
+ * systems may be staged; each tbs_factor takes the older one.  A stream of
+ * systems then keeps the host-to-device link busy, the factorizations
+ * included:
+ *   tbs_stage_jacobian(ctx, J0...);  tbs_stage_jacobian(ctx, J1...);
+ *   tbs_factor(ctx, algo);                  -- system 0
  *   for each system k:
- *     tbs_stage_jacobian(ctx, J[k+1]...);   -- overlaps the solve below
  *     tbs_solve(ctx, ...);  tbs_get_solution(ctx, U_k);
+ *     tbs_stage_jacobian(ctx, J[k+2]...);   -- queued behind J[k+1]
  *     tbs_factor(ctx, algo);                -- now the system k+1
  * The copies overlap the solve only from pinned (page-locked) host memory;
  * the host arrays must stay unchanged until the tbs_factor that takes them
- * returns.  tbs_set_jacobian discards a staged set.  The landing set costs
- * the device memory of one more Jacobian; tbs_factor copies it over the
- * active set on the device (about 1.6 ms for 5 GB), so the solve graph
- * keeps its addresses and no host copy waits behind the upload.  No
- * counterpart in the reference,
+ * returns.  A third stage before a tbs_factor is refused (TBS_ERR_STATE);
+ * tbs_set_jacobian discards the staged systems.  Each landing set costs
+ * the device memory of one more Jacobian; tbs_factor copies the set it
+ * takes over the active one on the device (about 1.6 ms for 5 GB), so the
+ * solve graph keeps its addresses and no host copy of the solve waits
+ * behind an upload.  No counterpart in the reference,
  * which reads one Jacobian per run (src/main.cxx:86-93). */
 int tbs_stage_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1,
                        const double *jacO2, const double *rhs);

@@ -14,6 +14,7 @@ import torch
 
 from meshes import ragged_mesh
 from triblocksolve_b200 import ALGO_FP64, ALGO_MIXED, ALGO_REFERENCE, Batch, Jacobian, Mesh, Solver
+from triblocksolve_b200._native import TbsError
 
 pytestmark = pytest.mark.gpu
 
@@ -63,11 +64,42 @@ def test_staged_pipeline_equals_alone(algo, tol):
         np.testing.assert_array_equal(U, want[k][2])
         if k + 1 < len(syss):
             s.factor(algo)
-    # a second pass repeats it with both buffer sets' graphs already built
+    # a second pass repeats it with the solve graph already built
     s.stage_jacobian_arrays(*syss[1])
     s.factor(algo)
     n, h = s.solve(tol, 200)
     np.testing.assert_array_equal(s.solution(), want[1][2])
+    s.close()
+
+
+@pytest.mark.parametrize("algo,tol", [(ALGO_FP64, 1e-12), (ALGO_MIXED, 1e-10)])
+def test_two_staged_ahead_equals_alone(algo, tol):
+    """Two systems staged before the first factorization, then one staged
+    two ahead of the solve each step (both landing slots in turn), as the
+    bench's stream of systems runs it; a third stage is refused."""
+    mesh = Mesh.structured(24, 36)
+    syss = systems(mesh, 5, shift=7.0)
+    want = [alone(mesh, sk, algo, tol) for sk in syss]
+    s = Solver(0)
+    s.set_mesh(mesh)
+    s.set_jacobian_arrays(*syss[4])          # an active set that the stream replaces
+    s.factor(algo)
+    s.solve(tol, 200)
+    s.stage_jacobian_arrays(*syss[0])
+    s.stage_jacobian_arrays(*syss[1])
+    with pytest.raises(TbsError):
+        s.stage_jacobian_arrays(*syss[2])
+    s.factor(algo)
+    for k in range(len(syss)):
+        n, h = s.solve(tol, 200)
+        U = s.solution()
+        assert n == want[k][0], k
+        np.testing.assert_array_equal(h, want[k][1])
+        np.testing.assert_array_equal(U, want[k][2])
+        if k + 2 < len(syss):
+            s.stage_jacobian_arrays(*syss[k + 2])
+        if k + 1 < len(syss):
+            s.factor(algo)
     s.close()
 
 

@@ -122,8 +122,10 @@ static void drop_mesh(tbs_ctx *ctx) {
     multi_free(ctx);
     krylov_free(ctx);
     drop_graph(ctx);
-    for (auto &p : ctx->d_spare) p = nullptr; /* freed with the other allocations below */
-    ctx->staged = false;
+    for (auto &slot : ctx->d_land)
+        for (auto &p : slot) p = nullptr; /* freed with the other allocations below */
+    ctx->land_count = 0;
+    ctx->land_head = 0;
     for (auto &a : ctx->allocs) cudaFree(a.first);
     ctx->allocs.clear();
     ctx->bytes = 0;
@@ -1044,8 +1046,10 @@ int tbs_destroy(tbs_ctx *ctx) {
     if (ctx->h_state) cudaFreeHost(ctx->h_state);
     if (ctx->h_status) cudaFreeHost(ctx->h_status);
     if (ctx->h_hist) cudaFreeHost(ctx->h_hist);
-    if (ctx->staged_ev) cudaEventDestroy(ctx->staged_ev);
-    if (ctx->spare_free_ev) cudaEventDestroy(ctx->spare_free_ev);
+    for (int k = 0; k < tbs_ctx::kLandSlots; ++k) {
+        if (ctx->land_ready[k]) cudaEventDestroy(ctx->land_ready[k]);
+        if (ctx->land_free[k]) cudaEventDestroy(ctx->land_free[k]);
+    }
     if (ctx->copy) cudaStreamDestroy(ctx->copy);
     if (ctx->own) cudaStreamDestroy(ctx->own);
     delete ctx;
@@ -1181,7 +1185,7 @@ static int upload_jacobian(tbs_ctx *ctx, const double *jacD, const double *O1, c
     /* same mesh -> same allocations, so an instantiated solve graph stays valid */
     ctx->have_jac = true;
     ctx->factored = false;
-    ctx->staged = false; /* these values, not a staged set, are the ones to factor */
+    ctx->land_count = 0; /* these values, not a staged set, are the ones to factor */
     return TBS_OK;
 }
 
@@ -1212,64 +1216,74 @@ int tbs_stage_jacobian(tbs_ctx *ctx, const double *jacD, const double *jacO1, co
     if (!ctx->have_mesh) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
     if (!jacD || (ctx->nintface > 0 && (!jacO1 || !jacO2)) || !rhs)
         return ctx_fail(ctx, TBS_ERR_ARG, "null Jacobian array");
+    if (ctx->land_count == tbs_ctx::kLandSlots)
+        return ctx_fail(ctx, TBS_ERR_STATE,
+                        "two systems are already staged: tbs_factor takes the older one first");
     if (!ctx->copy) {
         CK(cudaStreamCreateWithFlags(&ctx->copy, cudaStreamNonBlocking));
-        CK(cudaEventCreateWithFlags(&ctx->staged_ev, cudaEventDisableTiming));
-        CK(cudaEventCreateWithFlags(&ctx->spare_free_ev, cudaEventDisableTiming));
+        for (int k = 0; k < tbs_ctx::kLandSlots; ++k) {
+            CK(cudaEventCreateWithFlags(&ctx->land_ready[k], cudaEventDisableTiming));
+            CK(cudaEventCreateWithFlags(&ctx->land_free[k], cudaEventDisableTiming));
+        }
     }
+    const int slot = (ctx->land_head + ctx->land_count) % tbs_ctx::kLandSlots;
+    double **d = ctx->d_land[slot];
     const size_t nb = (size_t)ctx->nvar * ctx->nvar;
-    DA(ctx->d_spare[0], nb * ctx->nelem);
-    DA(ctx->d_spare[1], nb * ctx->nintface);
-    DA(ctx->d_spare[2], nb * ctx->nintface);
-    DA(ctx->d_spare[3], (size_t)nvec(ctx));
-    /* work already on the context's stream may still read the spare set
-     * (the previous system's true-residual check): the copies wait for it */
-    CK(cudaEventRecord(ctx->spare_free_ev, ctx->stream));
-    CK(cudaStreamWaitEvent(ctx->copy, ctx->spare_free_ev, 0));
+    const bool fresh = !d[0]; /* the four buffers are made and given up together */
+    DA(d[0], nb * ctx->nelem);
+    DA(d[1], nb * ctx->nintface);
+    DA(d[2], nb * ctx->nintface);
+    DA(d[3], (size_t)nvec(ctx));
+    /* The copies wait for the slot's last reader, the copy that took its
+     * previous system (tbs_factor), or, for new buffers, for their clearing
+     * on the context's stream. */
+    if (fresh) CK(cudaEventRecord(ctx->land_free[slot], ctx->stream));
     cudaStream_t c = ctx->copy;
-    CK(cudaMemcpyAsync(ctx->d_spare[0], jacD, nb * ctx->nelem * sizeof(double), cudaMemcpyDefault, c));
+    CK(cudaStreamWaitEvent(c, ctx->land_free[slot], 0));
+    CK(cudaMemcpyAsync(d[0], jacD, nb * ctx->nelem * sizeof(double), cudaMemcpyDefault, c));
     if (ctx->nintface) {
-        CK(cudaMemcpyAsync(ctx->d_spare[1], jacO1, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
-        CK(cudaMemcpyAsync(ctx->d_spare[2], jacO2, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
+        CK(cudaMemcpyAsync(d[1], jacO1, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
+        CK(cudaMemcpyAsync(d[2], jacO2, nb * ctx->nintface * sizeof(double), cudaMemcpyDefault, c));
     }
-    CK(cudaMemcpyAsync(ctx->d_spare[3], rhs, (size_t)nvec(ctx) * sizeof(double), cudaMemcpyDefault, c));
-    CK(cudaEventRecord(ctx->staged_ev, c));
-    ctx->staged = true;
+    CK(cudaMemcpyAsync(d[3], rhs, (size_t)nvec(ctx) * sizeof(double), cudaMemcpyDefault, c));
+    CK(cudaEventRecord(ctx->land_ready[slot], c));
+    ctx->land_count++;
     return TBS_OK;
     GUARD_END
 }
 
-/* make the staged set the active one (tbs_factor): the context's stream
- * waits for the upload, then a kernel copies the landed set over the active
- * buffers.  The active buffers keep their addresses, so the solve graph
- * captured on them stays the one launched: a graph launched for the first
- * time since another was launched on the stream re-uploads itself through
- * the copy engine, which would hold the solve behind the next system's
- * staged upload. */
+/* make the oldest staged system the active one (tbs_factor): the context's
+ * stream waits for its upload, then a kernel copies the slot over the
+ * active buffers.  The active buffers keep their addresses, so the solve
+ * graph captured on them stays the one launched: a graph launched for the
+ * first time since another was launched on the stream re-uploads itself
+ * through the copy engine, which would hold the solve behind the next
+ * system's staged upload. */
 static int take_staged(tbs_ctx *ctx) {
-    CK(cudaStreamWaitEvent(ctx->stream, ctx->staged_ev, 0));
+    const int slot = ctx->land_head;
+    double **d = ctx->d_land[slot];
+    CK(cudaStreamWaitEvent(ctx->stream, ctx->land_ready[slot], 0));
     if (!ctx->d_jacD) {
         /* no active set yet (nothing set before the first stage), so no
-         * graph holds its addresses: the landed set becomes the active one
-         * and the next stage allocates a new landing set */
+         * graph holds its addresses: the slot's buffers become the active
+         * set and the slot allocates new ones when it is next staged */
+        double **act[] = {&ctx->d_jacD, &ctx->d_O1, &ctx->d_O2, &ctx->d_rhs};
         for (int k = 0; k < 4; ++k) {
-            double **act[] = {&ctx->d_jacD, &ctx->d_O1, &ctx->d_O2, &ctx->d_rhs};
-            *act[k] = ctx->d_spare[k];
-            ctx->d_spare[k] = nullptr;
+            *act[k] = d[k];
+            d[k] = nullptr;
         }
-        ctx->staged = false;
-        ctx->have_jac = true;
-        ctx->factored = false;
-        return TBS_OK;
+    } else {
+        const size_t nb = (size_t)ctx->nvar * ctx->nvar * sizeof(double);
+        CKL(copy_words(ctx->stream, d[0], ctx->d_jacD, nb * ctx->nelem));
+        if (ctx->nintface) {
+            CKL(copy_words(ctx->stream, d[1], ctx->d_O1, nb * ctx->nintface));
+            CKL(copy_words(ctx->stream, d[2], ctx->d_O2, nb * ctx->nintface));
+        }
+        CKL(copy_words(ctx->stream, d[3], ctx->d_rhs, (size_t)nvec(ctx) * sizeof(double)));
+        CK(cudaEventRecord(ctx->land_free[slot], ctx->stream));
     }
-    const size_t nb = (size_t)ctx->nvar * ctx->nvar * sizeof(double);
-    CKL(copy_words(ctx->stream, ctx->d_spare[0], ctx->d_jacD, nb * ctx->nelem));
-    if (ctx->nintface) {
-        CKL(copy_words(ctx->stream, ctx->d_spare[1], ctx->d_O1, nb * ctx->nintface));
-        CKL(copy_words(ctx->stream, ctx->d_spare[2], ctx->d_O2, nb * ctx->nintface));
-    }
-    CKL(copy_words(ctx->stream, ctx->d_spare[3], ctx->d_rhs, (size_t)nvec(ctx) * sizeof(double)));
-    ctx->staged = false;
+    ctx->land_head = (slot + 1) % tbs_ctx::kLandSlots;
+    ctx->land_count--;
     ctx->have_jac = true;
     ctx->factored = false;
     return TBS_OK;
@@ -1279,7 +1293,7 @@ int tbs_factor(tbs_ctx *ctx, int algo) {
     if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
     GUARD_BEGIN
     CK(cudaSetDevice(ctx->device));
-    if (ctx->staged) {
+    if (ctx->land_count > 0) {
         int rs = take_staged(ctx);
         if (rs) return rs;
     }

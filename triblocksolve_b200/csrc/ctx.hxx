@@ -97,15 +97,17 @@ struct tbs_ctx {
     cudaGraph_t graph = nullptr;
     int graph_algo = -1;
 
-    /* ---- a staged Jacobian (tbs_stage_jacobian): the next system's jacD,
-     * O1, O2 and rhs, uploaded on the copy stream into a landing set while
-     * the current system is solved; tbs_factor copies it over the active
-     * set on the device ---- */
-    double *d_spare[4] = {nullptr, nullptr, nullptr, nullptr};
+    /* ---- staged Jacobians (tbs_stage_jacobian): up to two next systems'
+     * jacD, O1, O2 and rhs, uploaded on the copy stream into landing slots
+     * while the current system is solved; tbs_factor copies the oldest over
+     * the active set on the device ---- */
+    static constexpr int kLandSlots = 2;
+    double *d_land[kLandSlots][4] = {};
     cudaStream_t copy = nullptr;
-    cudaEvent_t staged_ev = nullptr;     /* the staged upload has landed */
-    cudaEvent_t spare_free_ev = nullptr; /* earlier work has stopped reading the spare set */
-    bool staged = false;
+    cudaEvent_t land_ready[kLandSlots] = {}; /* the slot's upload has landed */
+    cudaEvent_t land_free[kLandSlots] = {};  /* the copy out of the slot is done */
+    int land_head = 0;                       /* oldest staged slot */
+    int land_count = 0;                      /* staged systems waiting for tbs_factor */
 
     /* ---- several right-hand sides: vectors and graph, made on first use ---- */
     MultiBufs *multi = nullptr;

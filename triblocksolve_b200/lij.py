@@ -252,6 +252,7 @@ class Solver:
         self.platform = platform or Platform(N.CUDA_MODE, device_id)
         self.ctx = self.platform.ctx
         self.nvar = self.nelem = 0
+        self._staged = []  # host arrays of staged systems, oldest first
 
     def _chk(self, rc):
         N.check(rc, self.ctx)
@@ -263,26 +264,31 @@ class Solver:
         mesh.setupDevice(self.platform)
         mesh.toDevice()
         self.nvar, self.nelem = mesh.nvar, mesh.nelem
+        self._staged = []
 
     def set_jacobian(self, jac: Jacobian):
         jac.setupDevice(self.platform)
         jac.toDevice()
+        self._staged = []
 
     def set_jacobian_arrays(self, jacD, jacO1, jacO2, rhs):
         self._chk(N.lib.tbs_set_jacobian(self.ctx, N.dptr(jacD), N.dptr(jacO1), N.dptr(jacO2),
                                          N.dptr(rhs), None))
+        self._staged = []  # discarded by the call
 
     def stage_jacobian_arrays(self, jacD, jacO1, jacO2, rhs):
-        """Upload the next system's Jacobian and rhs while the current one is
-        solved; the next ``factor`` switches to it.  Pass pinned host arrays
-        for the copy to overlap, and keep them unchanged until that
-        ``factor`` returns (this object holds references until then)."""
+        """Upload a coming system's Jacobian and rhs while the current one is
+        solved; up to two may wait, and each ``factor`` switches to the older
+        one.  Pass pinned host arrays for the copy to overlap, and keep them
+        unchanged until that ``factor`` returns (this object holds
+        references until then)."""
         arrs = [np.ascontiguousarray(a, np.float64) for a in (jacD, jacO1, jacO2, rhs)]
         self._chk(N.lib.tbs_stage_jacobian(self.ctx, *[N.dptr(a) for a in arrs]))
-        self._staged = arrs
+        self._staged.append(arrs)
 
     def set_jacobian_device(self, d_jacD: int, d_jacO1: int, d_jacO2: int, d_rhs: int):
         self._chk(N.lib.tbs_set_jacobian_device(self.ctx, d_jacD, d_jacO1, d_jacO2, d_rhs))
+        self._staged = []
 
     def set_rhs(self, rhs: np.ndarray):
         self._chk(N.lib.tbs_set_rhs(self.ctx, N.dptr(np.ascontiguousarray(rhs, np.float64))))
@@ -313,7 +319,8 @@ class Solver:
 
     def factor(self, algo: int = N.ALGO_FP64):
         self._chk(N.lib.tbs_factor(self.ctx, algo))
-        self._staged = None
+        if self._staged:
+            self._staged.pop(0)
 
     def sweep(self, n: int) -> np.ndarray:
         h = np.zeros(n + 1)
