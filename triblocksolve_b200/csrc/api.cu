@@ -212,68 +212,30 @@ static int timed(tbs_ctx *ctx, const char *name, F &&launch) {
 #define RUN(name, call) CKL(timed(ctx, name, [&]() { return (int)(call); }))
 
 /* ======================================== host transfers off the copy engine
- * Every cudaMemcpyAsync between host and device, whatever its stream, waits
- * in the copy engine's queue behind the copies issued before it: a 5 GB
- * staged Jacobian (tbs_stage_jacobian) would hold a solve's 32-byte control
- * block for the whole upload.  So the solve and factorization paths move
- * their small words with kernels instead: the control block as kernel
- * parameters, the state, status and history into mapped pinned host
- * memory, and a result into the caller's buffer when that is pinned host
- * memory the device can address. */
+ * A cudaMemcpyAsync between host and device waits in the copy engine's
+ * queue behind every copy issued before it: a 5 GB staged Jacobian
+ * (tbs_stage_jacobian) would hold a solve's 32-byte control block for the
+ * whole upload.  So the solve and factorization paths move their small
+ * words with kernels (xfer.cu): the control block as kernel parameters,
+ * the state, status and history into mapped pinned host memory, and a
+ * result into the caller's buffer when that is pinned host memory the
+ * device can address. */
 __global__ void set_state_kernel(SolveState *s, double tol, int max_sweeps, int hist_cap) {
     s->tol = tol;
     s->max_sweeps = max_sweeps;
     s->hist_cap = hist_cap;
 }
 
-__global__ void copy_words_kernel(const unsigned long long *__restrict__ src,
-                                  unsigned long long *__restrict__ dst, long long n) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x)
-        dst[t] = src[t];
-}
-
-__global__ void copy_quads_kernel(const uint4 *__restrict__ src, uint4 *__restrict__ dst, long long n) {
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n;
-         t += (long long)gridDim.x * blockDim.x)
-        dst[t] = src[t];
-}
-
-/* `bytes` (a multiple of 8) from src to dst, 8-byte aligned, on the SMs;
- * 16-byte words when both addresses and the size allow */
+/* device -> device (or into mapped host memory) on the SMs */
 static int copy_words(cudaStream_t st, const void *src, void *dst, size_t bytes) {
-    const bool quads = bytes % 16 == 0 && (uintptr_t)src % 16 == 0 && (uintptr_t)dst % 16 == 0;
-    const long long n = (long long)(bytes / (quads ? 16 : 8));
-    const int blocks = (int)std::min<long long>(std::max<long long>((n + 255) / 256, 1), 4 * 148);
-    if (quads)
-        copy_quads_kernel<<<blocks, 256, 0, st>>>(static_cast<const uint4 *>(src),
-                                                  static_cast<uint4 *>(dst), n);
-    else
-        copy_words_kernel<<<blocks, 256, 0, st>>>(static_cast<const unsigned long long *>(src),
-                                                  static_cast<unsigned long long *>(dst), n);
-    return (int)cudaGetLastError();
+    return xfer_copy(st, src, dst, bytes, 0);
 }
 
-/* the device address of host memory a kernel may write, or null */
-static void *host_device_view(void *host) {
-    cudaPointerAttributes a{};
-    if (cudaPointerGetAttributes(&a, host) != cudaSuccess) {
-        cudaGetLastError();
-        return nullptr;
-    }
-    return (a.type == cudaMemoryTypeHost && a.devicePointer) ? a.devicePointer : nullptr;
-}
-
-/* device -> host of `bytes` (a multiple of 8, both addresses 8-aligned): a
- * kernel when the destination is device-addressable pinned memory, else a
- * copy (which may queue behind a staged upload) */
+/* device -> host of `bytes`: a kernel when the destination is
+ * device-addressable pinned memory, else a copy (which may queue behind a
+ * staged upload) */
 static int to_host(tbs_ctx *ctx, void *dst, const void *src, size_t bytes) {
-    void *dv = host_device_view(dst);
-    if (dv && bytes % 8 == 0 && (uintptr_t)dv % 8 == 0 && (uintptr_t)src % 8 == 0) {
-        CKL(copy_words(ctx->stream, src, dv, bytes));
-    } else {
-        CK(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    }
+    CKL(xfer_to_host(ctx->stream, dst, src, bytes, 0));
     return TBS_OK;
 }
 
@@ -1165,8 +1127,11 @@ int tbs_set_partition_mesh(tbs_ctx *ctx, int nhalo_lines, int nvar, int nelem, i
     GUARD_END
 }
 
+/* piece > 0: the copies go in pieces of at most `piece` bytes with at most
+ * two in flight (the call returns when the last is issued), so that copies
+ * from other threads wait behind two pieces, not the whole Jacobian */
 static int upload_jacobian(tbs_ctx *ctx, const double *jacD, const double *O1, const double *O2,
-                           const double *rhs, cudaMemcpyKind kind) {
+                           const double *rhs, cudaMemcpyKind kind, size_t piece = 0) {
     if (!ctx->have_mesh) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
     if (!jacD || (ctx->nintface > 0 && (!O1 || !O2)) || !rhs)
         return ctx_fail(ctx, TBS_ERR_ARG, "null Jacobian array");
@@ -1176,12 +1141,41 @@ static int upload_jacobian(tbs_ctx *ctx, const double *jacD, const double *O1, c
     DA(ctx->d_O2, nb * ctx->nintface);
     DA(ctx->d_rhs, (size_t)nvec(ctx));
     cudaStream_t s = ctx->stream;
-    CK(cudaMemcpyAsync(ctx->d_jacD, jacD, nb * ctx->nelem * sizeof(double), kind, s));
+    struct Part {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    std::vector<Part> parts{{ctx->d_jacD, jacD, nb * ctx->nelem * sizeof(double)}};
     if (ctx->nintface) {
-        CK(cudaMemcpyAsync(ctx->d_O1, O1, nb * ctx->nintface * sizeof(double), kind, s));
-        CK(cudaMemcpyAsync(ctx->d_O2, O2, nb * ctx->nintface * sizeof(double), kind, s));
+        parts.push_back({ctx->d_O1, O1, nb * ctx->nintface * sizeof(double)});
+        parts.push_back({ctx->d_O2, O2, nb * ctx->nintface * sizeof(double)});
     }
-    CK(cudaMemcpyAsync(ctx->d_rhs, rhs, (size_t)nvec(ctx) * sizeof(double), kind, s));
+    parts.push_back({ctx->d_rhs, rhs, (size_t)nvec(ctx) * sizeof(double)});
+    if (piece == 0) {
+        for (const Part &p : parts) CK(cudaMemcpyAsync(p.dst, p.src, p.bytes, kind, s));
+    } else {
+        cudaEvent_t ev[2] = {nullptr, nullptr};
+        int rc = TBS_OK;
+        long long n = 0;
+        for (int k = 0; k < 2 && rc == TBS_OK; ++k)
+            if (cudaEventCreateWithFlags(&ev[k], cudaEventDisableTiming) != cudaSuccess)
+                rc = ctx_fail(ctx, TBS_ERR_CUDA, "cudaEventCreate failed");
+        for (const Part &p : parts) {
+            for (size_t off = 0; off < p.bytes && rc == TBS_OK; off += piece, ++n) {
+                const size_t b = std::min(piece, p.bytes - off);
+                cudaEvent_t e = ev[n & 1];
+                if ((n >= 2 && cudaEventSynchronize(e) != cudaSuccess) ||
+                    cudaMemcpyAsync(static_cast<char *>(p.dst) + off,
+                                    static_cast<const char *>(p.src) + off, b, kind, s) != cudaSuccess ||
+                    cudaEventRecord(e, s) != cudaSuccess)
+                    rc = ctx_fail(ctx, TBS_ERR_CUDA, "paced Jacobian upload failed");
+            }
+        }
+        for (cudaEvent_t e : ev)
+            if (e) cudaEventDestroy(e);
+        if (rc) return rc;
+    }
     /* same mesh -> same allocations, so an instantiated solve graph stays valid */
     ctx->have_jac = true;
     ctx->factored = false;
@@ -1975,4 +1969,15 @@ int tbs_part_lines_vector(tbs_ctx *ctx, int which, int nlines, const int *lines,
 }
 
 }  // extern "C"
+
+/* the server's re-factorizations (csrc/server.cu) */
+int ctx_set_jacobian_paced(tbs_ctx *ctx, const double *jacD, const double *jacO1, const double *jacO2,
+                           const double *rhs, size_t piece) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    return upload_jacobian(ctx, jacD, jacO1, jacO2, rhs, cudaMemcpyHostToDevice, piece);
+    GUARD_END
+}
+
 

@@ -122,22 +122,34 @@ struct Stager {
         host.resize(off + ((b + 255) & ~(size_t)255));
         jobs.push_back({(void *)dst, {off, b}});
     }
+    /* the staged bytes, then the job table, into the pinned buffer; one
+     * launch copies every job from it (the SMs read the host memory) */
     int flush() {
         if (jobs.empty()) return TBS_OK;
         if (e.stage_ev) ECK(cudaEventSynchronize(e.stage_ev));
-        if (host.size() > e.stage_cap) {
+        const size_t table = host.size();
+        const size_t need = table + jobs.size() * sizeof(XferJob);
+        if (need > e.stage_cap) {
             if (e.h_stage) cudaFreeHost(e.h_stage);
             e.h_stage = nullptr;
             e.stage_cap = 0;
-            const size_t cap = host.size() + host.size() / 2;
+            const size_t cap = need + need / 2;
             if (cudaMallocHost(&e.h_stage, cap) != cudaSuccess)
                 return efail(e, TBS_ERR_NOMEM, "pinned staging allocation failed");
             e.stage_cap = cap;
         }
-        std::memcpy(e.h_stage, host.data(), host.size());
-        for (auto &j : jobs)
-            ECK(cudaMemcpyAsync(j.first, e.h_stage + j.second.first, j.second.second,
-                                cudaMemcpyHostToDevice, e.stream));
+        char *dev = static_cast<char *>(xfer_device_view(e.h_stage));
+        if (!dev) return efail(e, TBS_ERR_CUDA, "the staging buffer is not device-addressable");
+        std::memcpy(e.h_stage, host.data(), table);
+        XferJob *tab = reinterpret_cast<XferJob *>(e.h_stage + table);
+        size_t most = 0;
+        for (size_t k = 0; k < jobs.size(); ++k) {
+            tab[k].dst = (unsigned long long)(uintptr_t)jobs[k].first;
+            tab[k].src = (unsigned long long)(uintptr_t)(dev + jobs[k].second.first);
+            tab[k].bytes = jobs[k].second.second;
+            most = std::max(most, jobs[k].second.second);
+        }
+        ECKL(xfer_jobs(e.stream, reinterpret_cast<const XferJob *>(dev + table), (int)jobs.size(), most));
         if (!e.stage_ev) ECK(cudaEventCreateWithFlags(&e.stage_ev, cudaEventDisableTiming));
         ECK(cudaEventRecord(e.stage_ev, e.stream));
         return TBS_OK;
@@ -260,10 +272,13 @@ void engine_free(Engine &e) {
     e.pool.clear();
     if (e.h_ctl) cudaFreeHost(e.h_ctl);
     if (e.h_status) cudaFreeHost(e.h_status);
+    if (e.h_active_pin) cudaFreeHost(e.h_active_pin);
     if (e.h_stage) cudaFreeHost(e.h_stage);
     if (e.stage_ev) cudaEventDestroy(e.stage_ev);
     e.h_ctl = nullptr;
     e.h_status = nullptr;
+    e.h_active_pin = nullptr;
+    e.h_active_cap = 0;
     e.h_stage = nullptr;
     e.stage_cap = 0;
     e.stage_ev = nullptr;
@@ -703,7 +718,7 @@ static int engine_build_graph(Engine &e) {
 }
 
 static int engine_status(Engine &e) {
-    ECK(cudaMemcpyAsync(e.h_status, e.d_status, sizeof(unsigned), cudaMemcpyDeviceToHost, e.stream));
+    ECKL(xfer_to_host(e.stream, e.h_status, e.d_status, sizeof(unsigned), 1));
     ECK(cudaStreamSynchronize(e.stream));
     const unsigned s = *e.h_status;
     if (s) {
@@ -720,10 +735,18 @@ static int engine_status(Engine &e) {
 int engine_read_active(Engine &e) {
     const int n = e.h_ctl->nsys;
     e.h_active.resize(n);
-    if (n > 0)
-        ECK(cudaMemcpyAsync(e.h_active.data(), e.d_active, n * sizeof(int), cudaMemcpyDeviceToHost,
-                            e.stream));
+    if (n > e.h_active_cap) {
+        if (e.h_active_pin) cudaFreeHost(e.h_active_pin);
+        e.h_active_pin = nullptr;
+        e.h_active_cap = 0;
+        const int cap = std::max(n, 256);
+        if (cudaMallocHost(&e.h_active_pin, cap * sizeof(int)) != cudaSuccess)
+            return efail(e, TBS_ERR_NOMEM, "pinned allocation failed");
+        e.h_active_cap = cap;
+    }
+    if (n > 0) ECKL(xfer_to_host(e.stream, e.h_active_pin, e.d_active, n * sizeof(int), 1));
     ECK(cudaStreamSynchronize(e.stream));
+    if (n > 0) std::memcpy(e.h_active.data(), e.h_active_pin, n * sizeof(int));
     return TBS_OK;
 }
 
@@ -733,7 +756,7 @@ int engine_run(Engine &e, int chunk_limit, int stop_on_finish) {
     C.finished = 0;
     C.chunk_limit = chunk_limit;
     C.stop_on_finish = stop_on_finish;
-    ECK(cudaMemcpyAsync(e.d_ctl, e.h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, e.stream));
+    ECKL(xfer_put(e.stream, e.d_ctl, e.h_ctl, sizeof(BatchCtl)));
     if (e.prof) {
         /* eager form with the graph's loop rule tested on the host, so
          * that every kernel is timed */
@@ -771,7 +794,7 @@ int engine_launch(Engine &e, int chunk_limit, int stop_on_finish) {
     C.finished = 0;
     C.chunk_limit = chunk_limit;
     C.stop_on_finish = stop_on_finish;
-    ECK(cudaMemcpyAsync(e.d_ctl, e.h_ctl, sizeof(BatchCtl), cudaMemcpyHostToDevice, e.stream));
+    ECKL(xfer_put(e.stream, e.d_ctl, e.h_ctl, sizeof(BatchCtl)));
     if (!e.graph_ok) {
         int rc = engine_build_graph(e);
         if (rc) return rc;
@@ -1115,8 +1138,7 @@ int tbs_batch_solve(tbs_batch *b, double rel_tol, int max_sweeps, int *sweeps_ou
     const int n = (int)b->sys.size();
     for (int s = 0; s < n; ++s) {
         tbs_ctx *c = b->sys[s];
-        if (cudaMemcpyAsync(c->h_state, c->d_state, sizeof(SolveState), cudaMemcpyDeviceToHost, st) !=
-            cudaSuccess)
+        if (xfer_to_host(st, c->h_state, c->d_state, sizeof(SolveState), 1) != 0)
             return bfail(b, TBS_ERR_CUDA, "state read-back failed");
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "synchronisation failed");
@@ -1125,9 +1147,8 @@ int tbs_batch_solve(tbs_batch *b, double rel_tol, int max_sweeps, int *sweeps_ou
         const int sw = c->h_state->sweep;
         if (sweeps_out) sweeps_out[s] = sw;
         if (hist_out &&
-            cudaMemcpyAsync(hist_out + (size_t)s * (max_sweeps + 1), c->d_hist,
-                            (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double),
-                            cudaMemcpyDeviceToHost, st) != cudaSuccess)
+            xfer_to_host(st, hist_out + (size_t)s * (max_sweeps + 1), c->d_hist,
+                         (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double), 1) != 0)
             return bfail(b, TBS_ERR_CUDA, "history read-back failed");
     }
     if (cudaStreamSynchronize(st) != cudaSuccess) return bfail(b, TBS_ERR_CUDA, "synchronisation failed");

@@ -133,6 +133,10 @@ int ctx_ensure_hist(tbs_ctx *ctx, int need);
 int ctx_set_state(tbs_ctx *ctx, double tol, int max_sweeps);
 /* reads and clears the device status word; a set bit becomes the error */
 int ctx_status(tbs_ctx *ctx);
+/* tbs_set_jacobian from host memory in pieces of at most `piece` bytes, at
+ * most two in flight (returns when the last piece is issued) */
+int ctx_set_jacobian_paced(tbs_ctx *ctx, const double *jacD, const double *jacO1, const double *jacO2,
+                           const double *rhs, size_t piece);
 /* profiling brackets (a no-op unless profiling, outside stream capture):
  * begin records the start event of a launch named `name` and returns its
  * handle, end records its end event; resolve adds the finished pairs up */

@@ -76,10 +76,13 @@ struct Engine {
     unsigned *d_queue = nullptr, *d_counter = nullptr, *d_status = nullptr;
     BatchCtl *d_ctl = nullptr;
     BatchCtl *h_ctl = nullptr;     /* pinned */
-    unsigned *h_status = nullptr;  /* pinned */
+    unsigned *h_status = nullptr;  /* pinned, written by the device */
     std::vector<int> h_active;
-    /* pinned staging of the descriptor and work-list uploads, so that they
-     * never synchronise with the stream; reused once stage_ev has passed */
+    int *h_active_pin = nullptr;   /* pinned, written by the device */
+    int h_active_cap = 0;
+    /* pinned staging of the descriptor and work-list uploads, read by one
+     * copy launch (never by the copy engine, never a synchronisation with
+     * the stream); reused once stage_ev has passed */
     char *h_stage = nullptr;
     size_t stage_cap = 0;
     cudaEvent_t stage_ev = nullptr;

@@ -124,7 +124,6 @@ struct SrvLane {
     std::deque<SrvPending> pending;
     std::vector<cudaEvent_t> ev_pool;
     SolveState *h_states = nullptr;    /* pinned, max_slots: read-back of states */
-    SolveState *h_up_states = nullptr; /* pinned, max_slots: states of admitted ones */
     std::string err;
     std::thread th;
     /* re-factorizations of this lane's systems, by the lane's own factor
@@ -176,6 +175,16 @@ static int sfail(tbs_server *s, int code, const std::string &msg) {
 }
 
 static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
+
+/* CTAs of a right-hand side's or solution's copy through pinned host
+ * memory: enough 16-byte accesses in flight for the host link, while the
+ * sweeps keep the rest of the SMs */
+constexpr int kSysmemCtas = 32;
+
+/* a re-factorization's Jacobian goes up in pieces of this size, at most two
+ * in flight, so that the loop threads' copies never wait behind more than
+ * two pieces (about 2.4 ms of the host link) */
+constexpr size_t kRefactorPiece = 64ull << 20;
 
 /* device bytes of one right-hand side of system c with a history of hist_n */
 static size_t slot_bytes(const tbs_ctx *c, int algo, int hist_n) {
@@ -270,7 +279,7 @@ static void factor_main(tbs_server *s, SrvLane *L) {
                                   model->h_linepoint.data(), model->h_lines.data(),
                                   model->h_lineface.data());
         }
-        if (!rc) rc = tbs_set_jacobian(c, r->jacD, r->jacO1, r->jacO2, r->rhs, nullptr);
+        if (!rc) rc = ctx_set_jacobian_paced(c, r->jacD, r->jacO1, r->jacO2, r->rhs, kRefactorPiece);
         if (!rc) rc = tbs_factor(c, s->algo);
         std::string msg = rc ? std::string(c ? tbs_last_error(c) : thread_error()) : std::string();
         lk.lock();
@@ -399,7 +408,6 @@ static int start_requests(tbs_server *s, SrvLane *L, const std::vector<SrvReques
     if (admitted.empty()) return TBS_OK;
     /* the staging of the previous uploads is free once they have run */
     if (cudaEventSynchronize(L->ev_up) != cudaSuccess) return lfail(L, TBS_ERR_CUDA, "event failed");
-    int nst = 0;
     SrvIncoming batch;
     for (SrvRequest *r : admitted) {
         tbs_ctx *c = r->ctx;
@@ -423,15 +431,16 @@ static int start_requests(tbs_server *s, SrvLane *L, const std::vector<SrvReques
             /* pad positions of the layout are never written by the kernels
              * but enter the first norm (rhs) and the U accumulation: start
              * from zeros, as a context's arrays do */
-            SolveState &st = L->h_up_states[nst++];
-            st = SolveState{};
+            /* the state by kernel parameter and the right-hand side by the
+             * SMs when the caller's memory is pinned: neither waits in the
+             * copy engine behind a re-factorization's Jacobian upload */
+            SolveState st{};
             st.tol = r->tol;
             st.max_sweeps = r->max_sweeps;
             st.hist_cap = r->max_sweeps + 1;
-            ok = cudaMemsetAsync(m.mem, 0, per, L->up) == cudaSuccess &&
-                 cudaMemcpyAsync(m.v.state, &st, sizeof(st), cudaMemcpyHostToDevice, L->up) == cudaSuccess &&
-                 cudaMemcpyAsync(m.rhs_elem, r->rhs + k * nv, nv * sizeof(double),
-                                 cudaMemcpyHostToDevice, L->up) == cudaSuccess &&
+            ok = launch_zero(L->up, static_cast<double *>(m.mem), (long long)(per / sizeof(double))) == 0 &&
+                 xfer_put(L->up, m.v.state, &st, sizeof(st)) == 0 &&
+                 xfer_to_device(L->up, m.rhs_elem, r->rhs + k * nv, nv * sizeof(double), kSysmemCtas) == 0 &&
                  launch_permute_to_pos(L->up, 9, c->nelem, c->L.pos_of_elem, m.rhs_elem, m.v.rhsp) == 0;
         }
         if (!ok) {
@@ -469,8 +478,7 @@ static int retire(SrvLane *L) {
     for (size_t k = 0; k < out.size(); ++k) {
         SrvSlot &sl = out[k];
         tbs_ctx *c = sl.req->ctx;
-        if (cudaMemcpyAsync(&L->h_states[k], sl.v.state, sizeof(SolveState), cudaMemcpyDeviceToHost,
-                            L->stream) != cudaSuccess ||
+        if (xfer_to_host(L->stream, &L->h_states[k], sl.v.state, sizeof(SolveState), 1) != 0 ||
             launch_permute_to_elem(L->stream, 9, c->nelem, c->L.pos_of_elem, sl.v.Up, sl.rhs_elem) != 0)
             return lfail(L, TBS_ERR_CUDA, "solution read-back failed");
     }
@@ -483,8 +491,7 @@ static int retire(SrvLane *L) {
     for (SrvSlot &sl : out) {
         tbs_ctx *c = sl.req->ctx;
         const size_t nv = (size_t)c->nelem * 9;
-        if (cudaMemcpyAsync(sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double),
-                            cudaMemcpyDeviceToHost, L->down) != cudaSuccess)
+        if (xfer_to_host(L->down, sl.req->U + sl.k * nv, sl.rhs_elem, nv * sizeof(double), kSysmemCtas) != 0)
             return lfail(L, TBS_ERR_CUDA, "solution read-back failed");
         cudaFreeAsync(sl.mem, L->down);
     }
@@ -646,11 +653,10 @@ static void lane_free(SrvLane *L) {
     L->ev_pool.clear();
     if (L->ev_up) cudaEventDestroy(L->ev_up);
     if (L->h_states) cudaFreeHost(L->h_states);
-    if (L->h_up_states) cudaFreeHost(L->h_up_states);
     for (cudaStream_t x : {L->stream, L->up, L->down})
         if (x) cudaStreamDestroy(x);
     L->ev_up = nullptr;
-    L->h_states = L->h_up_states = nullptr;
+    L->h_states = nullptr;
     L->stream = L->up = L->down = nullptr;
 }
 
@@ -662,8 +668,7 @@ static int lane_init(tbs_server *s, SrvLane *L, int id) {
         return lfail(L, TBS_ERR_CUDA, "cudaStreamCreate failed");
     if (cudaEventCreateWithFlags(&L->ev_up, cudaEventDisableTiming) != cudaSuccess)
         return lfail(L, TBS_ERR_CUDA, "cudaEventCreate failed");
-    if (cudaMallocHost(&L->h_states, sizeof(SolveState) * (size_t)s->max_slots) != cudaSuccess ||
-        cudaMallocHost(&L->h_up_states, sizeof(SolveState) * (size_t)s->max_slots) != cudaSuccess)
+    if (cudaMallocHost(&L->h_states, sizeof(SolveState) * (size_t)s->max_slots) != cudaSuccess)
         return lfail(L, TBS_ERR_NOMEM, "pinned allocation failed");
     int rc = engine_init(L->eng, s->device, L->stream, s->algo);
     if (rc) return lfail(L, rc, L->eng.err);

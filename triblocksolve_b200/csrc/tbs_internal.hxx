@@ -431,4 +431,27 @@ int batch_prepare(int max_nx);
 
 }  // namespace tbs
 
+/* ------------------------------------------ transfers off the copy engine
+ * (xfer.cu).  Host memory below is pinned memory the device can address;
+ * the functions return a cudaError_t value (0 = success). */
+struct XferJob {               /* one copy of a batched job list */
+    unsigned long long dst, src, bytes; /* device addresses; bytes % 4 == 0 */
+};
+constexpr int kXferPutMax = 256;
+/* bytes (a multiple of 4, both addresses 4-aligned) on the SMs, at most
+ * max_blocks CTAs of 256 threads (< 1: 4 per SM) */
+int xfer_copy(cudaStream_t st, const void *src, void *dst, size_t bytes, int max_blocks);
+/* a small value (at most kXferPutMax bytes) written by a kernel that takes
+ * it as a parameter */
+int xfer_put(cudaStream_t st, void *dst, const void *value, size_t bytes);
+/* njobs copies in one launch; jobs_dev is readable by the device (e.g. the
+ * device view of a pinned staging buffer); max_bytes bounds the largest */
+int xfer_jobs(cudaStream_t st, const XferJob *jobs_dev, int njobs, size_t max_bytes);
+/* the device address of pinned host memory, or null */
+void *xfer_device_view(const void *host);
+/* device -> host / host -> device: by the SMs when the host side is
+ * device-addressable pinned memory, else cudaMemcpyAsync */
+int xfer_to_host(cudaStream_t st, void *dst, const void *src, size_t bytes, int max_blocks);
+int xfer_to_device(cudaStream_t st, void *dst, const void *src, size_t bytes, int max_blocks);
+
 #endif /* TBS_INTERNAL_HXX */
