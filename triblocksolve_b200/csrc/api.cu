@@ -489,13 +489,15 @@ static int resid64(tbs_ctx *ctx, int mode, const double *dU, const double *Rsrc,
 
 /* R = rhs + J U in element order by the reference-order residual kernel
  * (any block size); U in element order */
-static int ref_residual(tbs_ctx *ctx, const double *U, double *R) {
+/* R = rhs + J U in element order, its norm partials in d_partials2 (*np_out
+ * of them, may be null) */
+static int ref_residual(tbs_ctx *ctx, const double *U, double *R, int *np_out = nullptr) {
     int np = 0;
-    CK(cudaMemcpyAsync(R, ctx->d_rhs, (size_t)ctx->nvar * ctx->nelem * sizeof(double),
-                       cudaMemcpyDeviceToDevice, ctx->stream));
+    CKL(copy_words(ctx->stream, ctx->d_rhs, R, (size_t)ctx->nvar * ctx->nelem * sizeof(double)));
     CKL(launch_ref_line_res(ctx->stream, ctx->nvar, ctx->nline, ctx->nelem, ctx->d_epoint, ctx->d_ef,
                             ctx->d_fc, ctx->d_linesize, ctx->d_linepoint, ctx->d_lines, ctx->d_jacD,
                             ctx->d_O1, ctx->d_O2, U, R, ctx->d_partials2, &np));
+    if (np_out) *np_out = np;
     return TBS_OK;
 }
 
@@ -545,9 +547,9 @@ static int prime(tbs_ctx *ctx, CondCtl cc) {
     const size_t vb = (size_t)nvec(ctx) * sizeof(double);
     if (ctx->algo == TBS_ALGO_REFERENCE) {
         int np = 0;
-        CK(cudaMemcpyAsync(ctx->d_R, ctx->d_rhs, vb, cudaMemcpyDeviceToDevice, st));
+        CKL(copy_words(st, ctx->d_rhs, ctx->d_R, vb));
         if (ctx->d_Uinit) {
-            CK(cudaMemcpyAsync(ctx->d_U, ctx->d_Uinit, vb, cudaMemcpyDeviceToDevice, st));
+            CKL(copy_words(st, ctx->d_Uinit, ctx->d_U, vb));
             RUN("ref_line_res", launch_ref_line_res(st, nv, ctx->nline, ne, ctx->d_epoint, ctx->d_ef,
                                                     ctx->d_fc, ctx->d_linesize, ctx->d_linepoint,
                                                     ctx->d_lines, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
@@ -680,29 +682,51 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
 static bool checks_solve(const tbs_ctx *ctx) { return ctx->check && ctx->algo == TBS_ALGO_FP64; }
 
 /* The check of a converged TBS_ALGO_FP64 solve: R = rhs + J U from the
- * original blocks (the rule of linesmoothLU_TriBlock_v3.okl:228-336), its
- * norm recorded as NORM_CHECK (a pass ends the solve; a failure replaces
- * the sweep's history entry) and the next sweep's input b = -Dinv R made
- * from it, so that a failed check continues from the true residual. */
-static int check_true(tbs_ctx *ctx, CondCtl cc) {
+ * original blocks (the rule of linesmoothLU_TriBlock_v3.okl:228-336) and
+ * its norm, recorded as NORM_CHECK: a pass ends the solve; a failure
+ * replaces the sweep's history entry, and the solve continues from the true
+ * residual, for which the next sweep's input b = -Dinv R is made
+ * (check_restart).  In the graph the restart is an IF node whose condition
+ * the norm's reduction sets, so a passing check reads no factor block. */
+static int check_residual(tbs_ctx *ctx, CondCtl cc) {
     cudaStream_t st = ctx->stream;
     const FastLayout &L = ctx->L;
     const int nv = ctx->nvar, ne = ctx->nelem;
+    int np = 0;
     if (nv == 9) {
         RUN("full_resid", launch_full_resid<double>(st, ne, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                     L.pos_of_elem, ctx->d_jacD, ctx->d_O1,
                                                     ctx->d_O2, ctx->d_rhs, ctx->d_Up, ctx->d_Rp,
                                                     ctx->d_partials2));
+        np = full_resid_blocks(ne);
     } else {
         RUN("permute", launch_permute_to_elem(st, nv, ne, L.pos_of_elem, ctx->d_Up, ctx->d_U));
-        int rc = ref_residual(ctx, ctx->d_U, ctx->d_R);
+        int rc = ref_residual(ctx, ctx->d_U, ctx->d_R, &np);
         if (rc) return rc;
         RUN("permute", launch_permute_to_pos(st, nv, ne, L.pos_of_elem, ctx->d_R, ctx->d_Rp));
     }
-    CondCtl c2 = cc;
-    c2.use_check = 0;
-    RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b,
-                                    sink(ctx, NORM_CHECK, c2), nullptr));
+    RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials2, np, ctx->d_state, ctx->d_hist,
+                                          NORM_CHECK, cc.handle, cc.use_cond, cc.handle2, cc.use2));
+    return TBS_OK;
+}
+
+/* b = -Dinv R of the true residual, for the sweeps after a failed check */
+static int check_restart(tbs_ctx *ctx) {
+    RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b, no_sink(), nullptr));
+    return TBS_OK;
+}
+
+/* eager form: the host reads the recorded check and makes b only after a
+ * failure that leaves sweeps to do (the graph's IF node) */
+static int read_state(tbs_ctx *ctx);
+static int check_true_eager(tbs_ctx *ctx) {
+    int rc = check_residual(ctx, CondCtl{});
+    if (rc) return rc;
+    rc = read_state(ctx);
+    if (rc) return rc;
+    const SolveState &S = *ctx->h_state;
+    const bool pass = std::isfinite(S.true_norm) && S.true_norm <= S.tol * S.norm0;
+    if (!pass && std::isfinite(S.true_norm) && S.sweep < S.max_sweeps) return check_restart(ctx);
     return TBS_OK;
 }
 
@@ -789,8 +813,11 @@ static int build_graph(tbs_ctx *ctx) {
     CK(cudaGraphConditionalHandleCreate(&hw, g, 0, cudaGraphCondAssignDefault));
     if (sched) CK(cudaGraphConditionalHandleCreate(&hf, g, 0, cudaGraphCondAssignDefault));
     const bool chk = checks_solve(ctx);
-    cudaGraphConditionalHandle hc = 0;
-    if (chk) CK(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
+    cudaGraphConditionalHandle hc = 0, hr = 0;
+    if (chk) {
+        CK(cudaGraphConditionalHandleCreate(&hc, g, 0, cudaGraphCondAssignDefault));
+        CK(cudaGraphConditionalHandleCreate(&hr, g, 0, cudaGraphCondAssignDefault));
+    }
     const CondCtl loop{(unsigned long long)hw, 1, 0, 0, (unsigned long long)hc, chk ? 1 : 0};
     const CondCtl both{(unsigned long long)hw, 1, (unsigned long long)hf, sched ? 1 : 0, 0, 0};
     CK(cudaStreamBeginCaptureToGraph(st, g, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal));
@@ -804,8 +831,9 @@ static int build_graph(tbs_ctx *ctx) {
     if (rc == TBS_OK && sched)
         rc = capture_into(ctx, firstg, [&]() { return body(ctx, loop, ctx->inner_first); });
     /* the loop's body; with the check, an IF node after the sweep runs the
-     * true residual when the sweep met the tolerance:
-     * while (go) { sweep; if (met) { check } } */
+     * true residual when the sweep met the tolerance, and an IF node inside
+     * it makes the next sweep's input when the check failed:
+     * while (go) { sweep; if (met) { true residual; if (failed) { b } } } */
     cudaGraph_t checkg = nullptr;
     if (rc == TBS_OK)
         rc = capture_into(ctx, bodyg, [&]() {
@@ -814,9 +842,15 @@ static int build_graph(tbs_ctx *ctx) {
             return r;
         });
     if (rc == TBS_OK && chk) {
-        CondCtl ck = loop;
-        ck.use_check = 0;
-        rc = capture_into(ctx, checkg, [&]() { return check_true(ctx, ck); });
+        /* the check's reduction sets the loop's condition and the restart's */
+        const CondCtl ck{(unsigned long long)hw, 1, (unsigned long long)hr, 1, 0, 0};
+        cudaGraph_t restartg = nullptr;
+        rc = capture_into(ctx, checkg, [&]() {
+            int r = check_residual(ctx, ck);
+            if (r == TBS_OK) r = add_conditional(ctx, checkg, hr, cudaGraphCondTypeIf, &restartg);
+            return r;
+        });
+        if (rc == TBS_OK) rc = capture_into(ctx, restartg, [&]() { return check_restart(ctx); });
     }
     if (rc != TBS_OK) {
         drop_graph(ctx);
@@ -901,7 +935,7 @@ static int run_factor(tbs_ctx *ctx, int algo) {
     const int nv = ctx->nvar;
     if (algo == TBS_ALGO_REFERENCE) {
         const size_t nb = (size_t)nv * nv * ctx->nelem;
-        CK(cudaMemcpyAsync(ctx->d_DLU, ctx->d_jacD, nb * sizeof(double), cudaMemcpyDeviceToDevice, st));
+        CKL(copy_words(st, ctx->d_jacD, ctx->d_DLU, nb * sizeof(double)));
         CK(cudaMemsetAsync(ctx->d_DinvC, 0, nb * sizeof(double), st));
         CK(cudaMemsetAsync(ctx->d_A, 0, nb * sizeof(double), st));
         RUN("ref_assemble_A", launch_ref_assemble_A(st, nv, ctx->nline, ctx->d_fc, ctx->d_linesize,
@@ -1409,7 +1443,7 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
             if (!go) {
                 if (met && !checked && checks_solve(ctx)) {
                     /* as the graph's IF node: the true residual of the converged solve */
-                    rc = check_true(ctx, CondCtl{});
+                    rc = check_true_eager(ctx);
                     if (rc) return rc;
                     checked = true;
                     continue;

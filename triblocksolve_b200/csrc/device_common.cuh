@@ -29,6 +29,23 @@ static __device__ __forceinline__ double strided_sum(const double *p, int n, int
     return acc;
 }
 
+/* Record the norm of a converged solve's true residual (NORM_CHECK): a
+ * pass leaves the history alone and ends the solve; a failure counts a
+ * restart, replaces the last history entry and the latest norm, and goes on
+ * while sweeps are left.  Returns whether the solve goes on. */
+static __device__ __forceinline__ bool record_check(SolveState *S, double *hist, double nrm) {
+    const int sw = S->sweep;
+    const bool pass = isfinite(nrm) && nrm <= S->tol * S->norm0;
+    S->true_norm = nrm;
+    S->checks += 1;
+    if (!pass) {
+        S->restarts += 1;
+        if (sw < S->hist_cap) hist[sw] = nrm;
+        S->last = nrm;
+    }
+    return !pass && isfinite(nrm) && sw < S->max_sweeps;
+}
+
 /* After a CTA's last tile: a ticket per CTA; the last CTA to finish adds
  * the n per-tile partials in a fixed order and, when asked, records the
  * norm like reduce_norm (history, sweep count, graph loop condition).
@@ -60,16 +77,7 @@ static __device__ bool finalize_total(const NormSink &ns, int n) {
         SolveState *S = ns.state;
         if (ns.is_start == NORM_CHECK) {
             /* the true residual of a solve whose recursive residual passed */
-            const int sw = S->sweep;
-            const bool pass = isfinite(nrm) && nrm <= S->tol * S->norm0;
-            S->true_norm = nrm;
-            S->checks += 1;
-            if (!pass) {
-                S->restarts += 1;
-                if (sw < S->hist_cap) ns.hist[sw] = nrm;
-                S->last = nrm;
-            }
-            const bool go = !pass && isfinite(nrm) && sw < S->max_sweeps;
+            const bool go = record_check(S, ns.hist, nrm);
             if (ns.use_cond) cudaGraphSetConditional((cudaGraphConditionalHandle)ns.handle, go ? 1u : 0u);
             *ns.counter = 0u;
             return true;

@@ -88,7 +88,8 @@ constexpr int REDUCE_THREADS = 1024;
 /* Sum the partials in a fixed order, record the norm and decide whether the
  * solve goes on.  The decision feeds the CUDA graph's while-node, so the
  * sweep loop never returns to the host.  n == 0 re-records the latest norm
- * (state->last) as the start of a new sweep sequence. */
+ * (state->last) as the start of a new sweep sequence; is_start ==
+ * NORM_CHECK records a converged solve's true residual. */
 __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, SolveState *state,
                                    double *hist, int is_start,
                                    cudaGraphConditionalHandle handle, int use_cond,
@@ -102,6 +103,15 @@ __global__ void reduce_norm_kernel(const double *__restrict__ partials, int n, S
         double tot = 0.0;
         for (int w = 0; w < REDUCE_THREADS / 32; ++w) tot += red[w];
         const double nrm = n > 0 ? sqrt(tot) : state->last;
+        if (is_start == NORM_CHECK) {
+            /* the true residual of a solve whose recursive residual passed:
+             * both conditions (the loop's, and the IF node that makes the
+             * restart's input) say whether the solve goes on */
+            const bool go = record_check(state, hist, nrm);
+            if (use_cond) cudaGraphSetConditional(handle, go ? 1u : 0u);
+            if (use2) cudaGraphSetConditional(handle2, go ? 1u : 0u);
+            return;
+        }
         if (is_start) {
             state->sweep = 0;
             state->norm0 = nrm;

@@ -347,7 +347,7 @@ static int gmres(tbs_ctx *ctx, int m, int psweeps, double tol, int max_iters, in
     int iters = 0;
     /* U = 0; R = rhs (position order) */
     KCK(cudaMemsetAsync(ctx->d_Up, 0, (size_t)n * sizeof(double), st));
-    KCK(cudaMemcpyAsync(k->w, ctx->d_rhsp, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+    KCK((cudaError_t)xfer_copy(st, ctx->d_rhsp, k->w, (size_t)n * sizeof(double), 0));
     rc = dots(ctx, k->w, nullptr, 0, 1, k->h);
     if (rc) return rc;
     rc = read_back(ctx, k->h, 1, hh);
