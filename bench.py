@@ -215,6 +215,18 @@ def cpu_impl():
     return oracle.Baseline, "port", "oracle/lij_oracle.c, OpenMP over lines"
 
 
+def cpu_model() -> str:
+    """The host CPU's model name, as /proc/cpuinfo gives it."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
     """The CPU reference path on all host cores (and a one-thread sample); sweeps/s."""
     import oracle
@@ -246,6 +258,7 @@ def cpu_baseline(mesh, host, budget_s=12.0, sweeps=None):
     del b1
     oracle.set_threads(threads)
     return {"value": sweeps / dt, "unit": "sweeps/s", "cores": threads, "kind": kind,
+            "cpu_model": cpu_model(), "nproc": os.cpu_count(),
             "sample": f"{sweeps} FP64 sweeps of the same {mesh.nline}x{mesh.max_line_nelem} system "
                       f"after one factorization ({t_factor:.2f} s), {what}, {threads} threads",
             "factor_s": t_factor, "seconds": dt,
@@ -1161,11 +1174,17 @@ def run_reference(args, L, K, shift, tol):
     line = {"impl": "reference", "metric": "LIJ sweeps/s", "value": v, "unit": "sweeps/s",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * dt / args.steps, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"LIJ FP64 sweeps, {L}x{K} structured mesh ({mesh.nelem} cells), "
-                                   f"shift {shift}, seed {SEED}; one sweep per step",
-                       "cells": mesh.nelem, "factor_s": round(t_factor, 3)},
+            "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic: seeded structured mesh and values (shift %g, seed %d)" % (shift, SEED),
+            "config": {"workload": f"LIJ solve to {tol:g} relative residual from U=0, {L} lines x {K} "
+                                   f"cells ({mesh.nelem} cells, {mesh.nintface} faces), 9x9 blocks, "
+                                   f"algo fp64",
+                       "cells": mesh.nelem, "lines": L, "cells_per_line": K, "tol": tol,
+                       "algo": "fp64", "factor_s": round(t_factor, 3),
+                       "step": "one FP64 sweep of the solve (a bounded sample; sweeps/s does not "
+                               "depend on how many are timed)"},
             "cpu_baseline": {"value": v, "unit": "sweeps/s", "cores": threads, "kind": kind,
+                             "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                              "sample": f"{done} sweeps (one per step) after one factorization "
                                        f"({t_factor:.2f} s); {what} (OCCA, MPI and gfortran, "
                                        "which the reference builds with, are absent)"},
