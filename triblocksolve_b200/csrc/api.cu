@@ -441,12 +441,8 @@ static int build_layout(tbs_ctx *ctx) {
 
 /* ============================================================ sequences */
 
-static int status_check(tbs_ctx *ctx) {
-    /* the status word (4 bytes) travels in an 8-byte copy: h_status and
-     * d_status are 8-byte allocations */
-    CKL(copy_words(ctx->stream, ctx->d_status, ctx->h_status_dev, 8));
-    CK(cudaStreamSynchronize(ctx->stream));
-    const unsigned s = *ctx->h_status;
+/* the error of a status word read from the device (0: none); clears it */
+static int status_error(tbs_ctx *ctx, unsigned s) {
     if (s) {
         CK(cudaMemsetAsync(ctx->d_status, 0, sizeof(unsigned), ctx->stream));
         if (ctx->d_counter) CK(cudaMemsetAsync(ctx->d_counter, 0, sizeof(unsigned), ctx->stream));
@@ -460,7 +456,29 @@ static int status_check(tbs_ctx *ctx) {
     return TBS_OK;
 }
 
+static int status_check(tbs_ctx *ctx) {
+    /* the status word (4 bytes) travels in an 8-byte copy: h_status and
+     * d_status are 8-byte allocations */
+    CKL(copy_words(ctx->stream, ctx->d_status, ctx->h_status_dev, 8));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return status_error(ctx, *ctx->h_status);
+}
+
 int ctx_status(tbs_ctx *ctx) { return status_check(ctx); }
+
+/* Everything a finished solve reports, in one launch and one
+ * synchronisation: the state, the status word and the first nh norms of the
+ * history, into the context's mapped host memory. */
+__global__ void solve_readback_kernel(const SolveState *__restrict__ st,
+                                      const unsigned long long *__restrict__ status,
+                                      const double *__restrict__ hist, int nh, SolveState *o_state,
+                                      unsigned long long *o_status, double *o_hist) {
+    if (threadIdx.x == 0) {
+        *o_state = *st;
+        *o_status = *status;
+    }
+    for (int t = threadIdx.x; t < nh; t += blockDim.x) o_hist[t] = hist[t];
+}
 
 static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; }
 
@@ -1462,8 +1480,21 @@ int tbs_solve(tbs_ctx *ctx, double rel_tol, int max_sweeps, int *sweeps_out, dou
         }
         CK(cudaGraphLaunch(ctx->gexec, st));
         ctx->outer_done = 1; /* later tbs_sweep calls continue with the steady schedule */
-        rc = read_state(ctx);
+        /* state, status and history in one read-back */
+        const int nh = hist_out ? max_sweeps + 1 : 0;
+        rc = ensure_h_hist(ctx, std::max(nh, 1));
         if (rc) return rc;
+        solve_readback_kernel<<<1, 256, 0, st>>>(
+            ctx->d_state, reinterpret_cast<const unsigned long long *>(ctx->d_status), ctx->d_hist,
+            std::min(nh, ctx->hist_cap), ctx->h_state_dev,
+            reinterpret_cast<unsigned long long *>(ctx->h_status_dev), ctx->h_hist_dev);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        const int sw = ctx->h_state->sweep;
+        if (sweeps_out) *sweeps_out = sw;
+        if (hist_out)
+            std::memcpy(hist_out, ctx->h_hist, (size_t)(std::min(sw, max_sweeps) + 1) * sizeof(double));
+        return status_error(ctx, *ctx->h_status);
     }
     const int sw = ctx->h_state->sweep;
     if (sweeps_out) *sweeps_out = sw;
