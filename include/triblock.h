@@ -573,12 +573,16 @@ const char *tbs_server_last_error(const tbs_server *srv);
 /* sweeps per graph launch at most (default 4): how long a new arrival can
  * wait for the next sweep boundary */
 int tbs_server_set_chunk(tbs_server *srv, int sweeps);
-/* Two lanes, each its own loop thread, engine and streams, sharing the
- * budget and the limit on right-hand sides in flight: systems of fewer
- * than split_cells cells sweep in one lane, the others in the other, so
- * that small systems are not held to the pace of large ones (default
- * 262,144 cells; 0: one lane).  Set before any system is added. */
+/* Lanes, each its own loop thread, factor thread, engine and streams,
+ * sharing the budget and the limit on right-hand sides in flight, so that
+ * small systems are not held to the pace of large ones.  A system sweeps in
+ * lane k = how many of the ascending splits its cell count reaches.
+ * Default: three lanes, splits 262,144 and 1,048,576 cells.
+ * tbs_server_set_lanes: two lanes split at split_cells (0: one lane).
+ * tbs_server_set_lane_splits: up to three splits (four lanes).  Set before
+ * any system is added. */
 int tbs_server_set_lanes(tbs_server *srv, long long split_cells);
+int tbs_server_set_lane_splits(tbs_server *srv, const long long *splits, int n);
 /* uploads and factors a system (blocking); arrays as tbs_set_mesh and
  * tbs_set_jacobian */
 int tbs_server_add_system(tbs_server *srv, int nvar, int nelem, int nintface, int eftot,

@@ -145,6 +145,29 @@ def test_admission_by_footprint():
         srv.close()
 
 
+def test_three_lanes_same_as_alone():
+    """Lane splits [100, 1000]: the 51- and 37-cell systems sweep in lane 0,
+    the 480-cell one in lane 1, the 3,072-cell one in lane 2."""
+    sy = systems()
+    rng = np.random.default_rng(13)
+    srv = Server(0, ALGO_FP64, budget_bytes=8 << 30, max_rhs=32, chunk=2, lane_split=[100, 1000])
+    try:
+        ids = [srv.add_system(m, j) for m, j in sy]
+        reqs = []
+        for k in range(12):
+            s = k % len(sy)
+            rows = rng.uniform(-1, 1, (int(rng.integers(1, 4)), 9 * sy[s][0].nelem))
+            reqs.append((s, rows, srv.submit(ids[s], rows, TOL)))
+        for s, rows, r in reqs:
+            check(r.wait(), alone(*sy[s], rows, ALGO_FP64))
+    finally:
+        srv.close()
+    with pytest.raises(TbsError):
+        Server(0, ALGO_FP64, budget_bytes=1 << 30, lane_split=[1000, 100])   # not ascending
+    with pytest.raises(TbsError):
+        Server(0, ALGO_FP64, budget_bytes=1 << 30, lane_split=[1, 2, 3, 4])  # too many
+
+
 def test_concurrent_clients():
     sy = systems()
     srv = Server(0, ALGO_FP64, budget_bytes=8 << 30, max_rhs=32, chunk=1, lane_split=500)

@@ -136,6 +136,7 @@ _sig("tbs_server_destroy", _i, _vp)
 _sig("tbs_server_last_error", _cp, _vp)
 _sig("tbs_server_set_chunk", _i, _vp, _i)
 _sig("tbs_server_set_lanes", _i, _vp, C.c_longlong)
+_sig("tbs_server_set_lane_splits", _i, _vp, C.POINTER(C.c_longlong), _i)
 _sig("tbs_server_add_system", _i, _vp, _i, _i, _i, _i, _i, _i, _ip, _ip, _ip, _ip, _ip, _ip, _ip,
      _dp, _dp, _dp, _ip)
 _sig("tbs_server_system_bytes", _i, _vp, _i, _i, C.POINTER(C.c_size_t), C.POINTER(C.c_size_t))

@@ -150,10 +150,11 @@ struct tbs_server {
     std::map<long long, std::unique_ptr<SrvRequest>> requests;
     long long next_id = 1;
 
-    /* one loop thread per lane: systems below lane_split cells sweep in
-     * lane 0, the others in lane 1, so that small systems are not held to
-     * the pace of the large ones */
-    long long lane_split = 262144;
+    /* one loop thread per lane: a system sweeps in the lane given by how
+     * many of the ascending lane_splits its cell count reaches, so that
+     * small systems are not held to the pace of large ones (by default
+     * three lanes: below 262,144 cells, below 1,048,576, and larger) */
+    std::vector<long long> lane_splits{262144, 1048576};
     std::vector<std::unique_ptr<struct SrvLane>> lanes;
     cudaMemPool_t pool = nullptr;
     bool pool_reserved = false;
@@ -180,6 +181,10 @@ static size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
  * memory: enough 16-byte accesses in flight for the host link, while the
  * sweeps keep the rest of the SMs */
 constexpr int kSysmemCtas = 32;
+
+/* lanes (loop and factor threads, engines) a server runs; the lane splits
+ * decide how many of them receive systems */
+constexpr int kMaxLanes = 4;
 
 /* a re-factorization's Jacobian goes up in pieces of this size, at most two
  * in flight, so that the loop threads' copies never wait behind more than
@@ -720,7 +725,7 @@ int tbs_server_create(int device_id, int algo, size_t device_budget_bytes, int m
     tbs_server *s = nullptr;
     try {
         s = new tbs_server();
-        for (int k = 0; k < 2; ++k) s->lanes.emplace_back(new SrvLane());
+        for (int k = 0; k < kMaxLanes; ++k) s->lanes.emplace_back(new SrvLane());
     } catch (...) {
         delete s;
         return sfail(nullptr, TBS_ERR_NOMEM, "host allocation failed");
@@ -786,9 +791,19 @@ int tbs_server_destroy(tbs_server *s) {
 int tbs_server_set_lanes(tbs_server *s, long long split_cells) {
     if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
     if (split_cells < 0) return sfail(s, TBS_ERR_ARG, "negative split");
+    return tbs_server_set_lane_splits(s, &split_cells, split_cells > 0 ? 1 : 0);
+}
+
+int tbs_server_set_lane_splits(tbs_server *s, const long long *splits, int n) {
+    if (!s) return sfail(nullptr, TBS_ERR_ARG, "null server");
+    if (n < 0 || n > kMaxLanes - 1 || (n > 0 && !splits))
+        return sfail(s, TBS_ERR_ARG, "at most " + std::to_string(kMaxLanes - 1) + " lane splits");
+    for (int k = 0; k < n; ++k)
+        if (splits[k] <= 0 || (k > 0 && splits[k] <= splits[k - 1]))
+            return sfail(s, TBS_ERR_ARG, "lane splits must be positive and ascending");
     std::lock_guard<std::mutex> lk(s->mu);
     if (!s->systems.empty()) return sfail(s, TBS_ERR_STATE, "lanes are set before systems are added");
-    s->lane_split = split_cells;
+    s->lane_splits.assign(splits, splits + n);
     return TBS_OK;
 }
 
@@ -838,7 +853,9 @@ int tbs_server_add_system(tbs_server *s, int nvar, int nelem, int nintface, int 
     SrvSystem sys;
     sys.ctx[0] = c;
     sys.bytes = bytes;
-    sys.lane = (s->lane_split > 0 && nelem >= s->lane_split) ? 1 : 0;
+    sys.lane = 0;
+    for (long long split : s->lane_splits)
+        if (nelem >= split) sys.lane += 1;
     s->systems.push_back(sys);
     *system_id = (int)s->systems.size() - 1;
     return TBS_OK;

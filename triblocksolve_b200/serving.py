@@ -58,15 +58,25 @@ class Request:
 
 class Server:
     def __init__(self, device_id: int = 0, algo: int = N.ALGO_FP64, budget_bytes: int = 32 << 30,
-                 max_rhs: int = 64, chunk: int | None = None, lane_split: int | None = None):
+                 max_rhs: int = 64, chunk: int | None = None,
+                 lane_split: int | list[int] | None = None):
+        """lane_split: one cell count (two lanes; 0 = one lane) or an ascending
+        list of up to three (default: [262144, 1048576], three lanes)."""
         h = C.c_void_p()
         N.check_server(N.lib.tbs_server_create(device_id, algo, budget_bytes, max_rhs, C.byref(h)))
         self.handle = h
         self.nelem = {}
-        if chunk is not None:
-            self.set_chunk(chunk)
-        if lane_split is not None:
-            self._chk(N.lib.tbs_server_set_lanes(self.handle, lane_split))
+        try:
+            if chunk is not None:
+                self.set_chunk(chunk)
+            if isinstance(lane_split, (list, tuple)):
+                arr = (C.c_longlong * max(len(lane_split), 1))(*lane_split)
+                self._chk(N.lib.tbs_server_set_lane_splits(self.handle, arr, len(lane_split)))
+            elif lane_split is not None:
+                self._chk(N.lib.tbs_server_set_lanes(self.handle, lane_split))
+        except Exception:
+            self.close()
+            raise
 
     def _chk(self, rc):
         N.check_server(rc, self.handle)
