@@ -346,6 +346,15 @@ int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
  * it when the global recursive norm meets the tolerance, as tbs_solve does. */
 int tbs_part_check(tbs_ctx *ctx, double *owned_norm);
 
+/* The device-clock record of the sweeps' cross-line residual launches
+ * (block size 9; every launch, graph-launched ones included): the sum of
+ * their durations in microseconds, each from its earliest CTA start to the
+ * finish of its last CTA on the GPU's global nanosecond clock, and their
+ * number.  reset != 0 starts a new record.  Waits for the context's
+ * stream.  No counterpart in the reference (its timing is host-side,
+ * src/main.cxx:233-252). */
+int tbs_resid_timer(tbs_ctx *ctx, double *total_us, long long *launches, int reset);
+
 /* Waits for the context's stream and reports a device-side failure (a
  * zero pivot, a staging wait that ran out of time) of the launches since
  * the last call that returned a status: the end of a sequence of calls

@@ -95,6 +95,7 @@ _sig("tbs_part_line_res", _i, _vp, _dp)
 _sig("tbs_part_line_vector", _i, _vp, _i, _i, _vp, _i)
 _sig("tbs_part_lines_vector", _i, _vp, _i, _i, _ip, _vp, _i)
 _sig("tbs_part_owned_norm", _i, _vp, _vp)
+_sig("tbs_resid_timer", _i, _vp, C.POINTER(C.c_double), C.POINTER(C.c_longlong), _i)
 _sig("tbs_sync", _i, _vp)
 _sig("tbs_part_check", _i, _vp, _dp)
 _sig("tbs_get_solution", _i, _vp, _dp)

@@ -146,6 +146,7 @@ static void drop_mesh(tbs_ctx *ctx) {
     for (auto p : ips) *p = nullptr;
     ctx->d_state = nullptr;
     ctx->d_status = nullptr;
+    ctx->d_ktimer = nullptr;
     ctx->d_counter = nullptr;
     ctx->npart_cap = 0;
     ctx->hist_cap = 0;
@@ -498,9 +499,14 @@ static int thomas64(tbs_ctx *ctx, const double *b, double *dU, double *U, int ac
 
 static int resid64(tbs_ctx *ctx, int mode, const double *dU, const double *Rsrc, double *b,
                    const NormSink &ns, double *Uacc) {
-    if (ctx->nvar == 9)
+    if (ctx->nvar == 9) {
+        /* the sweeps' residual launches keep a device-clock record of their
+         * durations (tbs_resid_timer), graph-launched ones included */
+        NormSink nt = ns;
+        if (mode == 1) nt.timer = ctx->d_ktimer;
         return launch_fast_resid<double>(ctx->stream, ctx->L, mode, ctx->d_Dinv, ctx->d_X, dU, Rsrc, b,
-                                         ns, ctx->d_status, Uacc);
+                                         nt, ctx->d_status, Uacc);
+    }
     return launch_nv_resid(ctx->stream, ctx->nvar, ctx->L, mode, ctx->d_Dinv, ctx->d_X, dU, Rsrc, b, ns,
                            ctx->d_status, Uacc);
 }
@@ -1113,6 +1119,11 @@ static int set_mesh(tbs_ctx *ctx, int nhalo, int nvar, int nelem, int nintface, 
     ctx->allocs.push_back({ctx->d_status, 8});
     CK(cudaMemsetAsync(ctx->d_status, 0, 8, ctx->stream));
     DA(ctx->d_state, 1);
+    DA(ctx->d_ktimer, 3);
+    {
+        const unsigned long long init[3] = {~0ull, 0ull, 0ull};
+        CKL(xfer_put(ctx->stream, ctx->d_ktimer, init, sizeof(init)));
+    }
     ctx->nvar = nvar;
     ctx->nelem = nelem;
     ctx->nintface = nintface;
@@ -1977,6 +1988,25 @@ int tbs_part_check(tbs_ctx *ctx, double *owned_norm) {
                                     sink(ctx, NORM_CHECK, CondCtl{}), nullptr));
     if (!owned_norm) return TBS_OK;
     return part_norm(ctx, owned_norm);
+    GUARD_END
+}
+
+int tbs_resid_timer(tbs_ctx *ctx, double *total_us, long long *launches, int reset) {
+    if (!ctx) return ctx_fail(nullptr, TBS_ERR_ARG, "null context");
+    GUARD_BEGIN
+    CK(cudaSetDevice(ctx->device));
+    if (!ctx->d_ktimer) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_set_mesh must come first");
+    CK(cudaStreamSynchronize(ctx->stream));
+    unsigned long long t[3] = {0, 0, 0};
+    CK(cudaMemcpy(t, ctx->d_ktimer, sizeof(t), cudaMemcpyDeviceToHost));
+    if (total_us) *total_us = 1e-3 * (double)t[1];
+    if (launches) *launches = (long long)t[2];
+    if (reset) {
+        const unsigned long long init[3] = {~0ull, 0ull, 0ull};
+        CKL(xfer_put(ctx->stream, ctx->d_ktimer, init, sizeof(init)));
+        CK(cudaStreamSynchronize(ctx->stream));
+    }
+    return TBS_OK;
     GUARD_END
 }
 

@@ -87,6 +87,7 @@ struct tbs_ctx {
     double *h_hist_dev = nullptr;
     int h_hist_cap = 0;
     unsigned *d_status = nullptr;
+    unsigned long long *d_ktimer = nullptr; /* device-clock record of the sweeps' residual launches */
     unsigned *h_status = nullptr; /* pinned, mapped */
     unsigned *h_status_dev = nullptr;
     unsigned *d_counter = nullptr; /* last-CTA ticket of the fused norm */

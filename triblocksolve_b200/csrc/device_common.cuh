@@ -29,6 +29,26 @@ static __device__ __forceinline__ double strided_sum(const double *p, int n, int
     return acc;
 }
 
+/* the device's global nanosecond clock */
+static __device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+/* a launch's duration on the device clock, from its earliest CTA start to
+ * the finish of its last CTA (called by that CTA's thread 0) */
+static __device__ __forceinline__ void timer_launch_start(unsigned long long *timer) {
+    if (timer && threadIdx.x == 0) atomicMin(timer, globaltimer_ns());
+}
+static __device__ __forceinline__ void timer_launch_end(unsigned long long *timer) {
+    if (!timer || threadIdx.x != 0) return;
+    const unsigned long long t1 = globaltimer_ns();
+    const unsigned long long t0 = atomicExch(timer, ~0ull);
+    if (t0 != ~0ull && t1 > t0) atomicAdd(timer + 1, t1 - t0);
+    atomicAdd(timer + 2, 1ull);
+}
+
 /* Record the norm of a converged solve's true residual (NORM_CHECK): a
  * pass leaves the history alone and ends the solve; a failure counts a
  * restart, replaces the last history entry and the latest norm, and goes on
@@ -61,6 +81,7 @@ static __device__ bool finalize_total(const NormSink &ns, int n) {
     }
     __syncthreads();
     if (ticket != gridDim.x - 1) return false;
+    timer_launch_end(ns.timer); /* every other CTA has finished its tiles */
     if (!ns.state) {
         if (threadIdx.x == 0) *ns.counter = 0u;
         return true;

@@ -792,6 +792,7 @@ template <typename T>
 __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T *Dinv, const T *X,
                                             const int *xnbr, const T *dU, const T *Rsrc, T *b,
                                             T *Uacc, const NormSink &ns, unsigned *status) {
+    timer_launch_start(ns.timer);
     uint64_t *bar = resid_bar_init();
     const int ntiles = np16 / RES_TILE;
     uint32_t parity = 0;

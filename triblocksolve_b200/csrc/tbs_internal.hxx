@@ -188,6 +188,9 @@ struct NormSink {
     int use_check;               /* a sweep's norm also sets check_handle: 1 when the
                                   * recursive residual has met the tolerance */
     unsigned long long check_handle;
+    unsigned long long *timer;   /* null, or the launch's device-clock record: [0] the
+                                  * earliest CTA start (all ones between launches),
+                                  * [1] += last finish - [0] in ns, [2] += 1 launch */
 };
 /* NormSink::is_start of the check of a converged solve: a norm at or below
  * the tolerance ends the solve with the history unchanged; a larger one

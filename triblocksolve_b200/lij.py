@@ -400,6 +400,13 @@ class Solver:
         self._chk(N.lib.tbs_true_residual_norm(self.ctx, C.byref(v)))
         return v.value
 
+    def resid_timer(self, reset: bool = False):
+        """(total microseconds, launches) of the sweeps' residual launches on
+        the device clock since the last reset; reset=True starts anew."""
+        us, n = C.c_double(), C.c_longlong()
+        self._chk(N.lib.tbs_resid_timer(self.ctx, C.byref(us), C.byref(n), 1 if reset else 0))
+        return us.value, n.value
+
     def set_check(self, on: bool = True):
         """TBS_ALGO_FP64: check a converged solve against rhs + J U (default on)."""
         self._chk(N.lib.tbs_set_check(self.ctx, 1 if on else 0))
