@@ -6,7 +6,7 @@ tests/test_ref_pin.py) on all host cores.
   600 x 640   (384,000 cells), shift 4, tolerance 1e-10
   1200 x 1280 (1,536,000 cells), shift 4, tolerance 1e-10
 
-Tolerances, as the loop of src/main.cxx:207-229 is judged:
+Tolerances, for the loop of src/main.cxx:207-229:
   TBS_ALGO_FP64       every sweep | ||R_k|| - ||R_k||_oracle | <= 1e-12 ||R_0||,
                       the same sweep count at the tolerance, ||U - U_oracle||
                       <= 1e-12 ||U_oracle||.
