@@ -2,8 +2,8 @@
  * tma.cuh -- thin inline-PTX wrappers for the Blackwell (sm_100a) bulk-copy
  * engine and shared-memory mbarriers used by the streaming kernels.
  *
- * Only the untiled bulk form is used (cp.async.bulk global -> shared, no
- * multicast): every copy starts on a 16-byte boundary and moves a multiple
+ * Only the untiled bulk form is used (cp.async.bulk global -> shared, each
+ * copy into the issuing CTA alone): every copy starts on a 16-byte boundary and moves a multiple
  * of 16 bytes, which the callers guarantee through the even-cell layout.
  * Every wait is bounded by a clock64 budget; on expiry the caller gets
  * `false`, records ST_TIMEOUT and leaves instead of spinning forever.
