@@ -1033,7 +1033,8 @@ __device__ __forceinline__ float row_dot(const RowF &R, const float *cur, const 
  * warp may lie beyond one chain's end; those compute but write nothing. */
 template <typename T, int P, bool CHECK, bool YS>
 __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys, T *yg, int kbase,
-                                          int len, int cpos, int i, const LaneOff &o) {
+                                          int len, int cpos, int i, const LaneOff &o,
+                                          uint64_t ypol) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG, o, 0);
     T cur_b = sB[i];
@@ -1056,8 +1057,8 @@ __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys
             const int pos = cpos + kbase + q;
             if (YS)
                 ys[pos * NV + i] = yi;
-            else
-                yg[(size_t)pos * NV + i] = yi;
+            else /* kept in L2 for the backward chain (the blocks stream evict-first) */
+                st_hint(yg + (size_t)pos * NV + i, yi, ypol);
         }
         __syncwarp();
         cur_row = next_row;
@@ -1217,6 +1218,9 @@ __device__ __forceinline__ bool thomas_line(
     int consumed = 0;
     bool timed_out = false;
     const int both_full = (m < nb ? m : nb) / P; /* jobs where both chains run P steps */
+    /* y, written by the forward chains and read once by the backward ones */
+    const uint64_t ypol_last = YS ? 0ull : policy_evict_last();
+    const uint64_t ypol_first = YS ? 0ull : policy_evict_first();
 
     /* ---------------- forward */
     for (int c = 0; c < nf; ++c) {
@@ -1230,9 +1234,9 @@ __device__ __forceinline__ bool thomas_line(
         const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
         const T *sB = sG + P * NB;
         if (c < both_full)
-            fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
+            fwd_chunk<T, P, false, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off, ypol_last);
         else
-            fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off);
+            fwd_chunk<T, P, true, YS>(sG, sB, bc, ys, yl, c * P, len, cpos, i, off, ypol_last);
         __syncwarp();
         if (WS) {
             if (lane == 0) mbar_arrive(&empty[s]);
@@ -1281,7 +1285,7 @@ __device__ __forceinline__ bool thomas_line(
                 yy[q] = T(0);
                 uu[q] = T(0);
                 if (!YS && c >= 0 && k < len) { /* lanes 9..15: lane 8's values */
-                    yy[q] = yl[(size_t)(cpos + k) * NV + i];
+                    yy[q] = ld_hint(yl + (size_t)(cpos + k) * NV + i, ypol_first);
                     if (accumulate == 1) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
                 }
             }
