@@ -686,7 +686,7 @@ __device__ __forceinline__ bool fast_resid_body(
     int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
     T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status, int blk,
-    uint64_t *bar, uint32_t parity) {
+    uint64_t *bar, uint32_t parity, const int *nbr_pre = nullptr) {
     extern __shared__ __align__(128) unsigned char smem[];
     T *sD = reinterpret_cast<T *>(smem + 128);
     T *sX = sD + RES_TILE * NB;
@@ -720,10 +720,21 @@ __device__ __forceinline__ bool fast_resid_body(
         Uacc[q] = (mode >= 1) ? Uacc[q] + dU[q] : T(0);
     }
     if (mode >= 1 && act) {
-        /* neighbour dU gathers overlap the bulk copies */
-        for (int s = 0; s < nx; ++s) {
-            const int nb = xnbr[(size_t)s * np16 + p0 + c];
-            sg[(s * RES_TILE + c) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
+        /* neighbour dU gathers overlap the bulk copies (their indices
+         * loaded during the previous tile when the caller prefetched them) */
+        if (nbr_pre) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if (s < nx) {
+                    const int nb = nbr_pre[s];
+                    sg[(s * RES_TILE + c) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
+                }
+            }
+        } else {
+            for (int s = 0; s < nx; ++s) {
+                const int nb = xnbr[(size_t)s * np16 + p0 + c];
+                sg[(s * RES_TILE + c) * NV + i] = (nb >= 0) ? dU[(size_t)nb * NV + i] : T(0);
+            }
         }
     }
     const bool ok = mbar_wait(bar, parity);
@@ -796,11 +807,27 @@ __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T 
     uint64_t *bar = resid_bar_init();
     const int ntiles = np16 / RES_TILE;
     uint32_t parity = 0;
+    /* the neighbour indices of a CTA's next tile are loaded while it works
+     * on the current one, so that a tile's gathers wait for one memory
+     * round trip, not two */
+    constexpr int PRE = 4;
+    const bool pre = mode >= 1 && nx <= PRE && threadIdx.x < RES_TILE * NV;
+    const int c = threadIdx.x % RES_TILE;
+    int nbr[PRE], nxt[PRE];
+#pragma unroll
+    for (int s = 0; s < PRE; ++s) nbr[s] = (pre && s < nx && blockIdx.x < ntiles)
+                                               ? xnbr[(size_t)s * np16 + blockIdx.x * RES_TILE + c] : -1;
     for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        const int wn = w + gridDim.x;
+#pragma unroll
+        for (int s = 0; s < PRE; ++s)
+            nxt[s] = (pre && s < nx && wn < ntiles) ? xnbr[(size_t)s * np16 + wn * RES_TILE + c] : -1;
         const bool ok = fast_resid_body<T>(nx, np16, mode, Dinv, X, xnbr, dU, Rsrc, b, Uacc, ns,
-                                           status, w, bar, parity);
+                                           status, w, bar, parity, pre ? nbr : nullptr);
         parity ^= 1u;
         if (!ok) break;
+#pragma unroll
+        for (int s = 0; s < PRE; ++s) nbr[s] = nxt[s];
         __syncthreads(); /* the next tile's copies overwrite the stages */
     }
     /* a line partition's norm covers its owned lines, which come first */
