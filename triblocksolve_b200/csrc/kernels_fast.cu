@@ -2161,11 +2161,26 @@ __global__ void __launch_bounds__(RES_THREADS_FAST, CHUNK == 1 ? 8 : 6) fast_res
         NormSink ns{};
         ns.partials = (mode == 3) ? nullptr : S.partials; /* no counter: partials only */
         const int t1 = chunk_end(it.unit, chunk, S.np16 / RES_TILE);
-        for (int t = it.unit * chunk; t < t1; ++t) {
-            ok = fast_resid_body<T>(mode == 0 ? 0 : S.nx, S.np16, mode, S.Dinv, S.X, S.xnbr, S.dU,
-                                    S.Rsrc, S.b, S.Uacc, ns, status, t, bar, parity);
+        /* the next tile's neighbour indices load during the current tile */
+        const int nxm = mode == 0 ? 0 : S.nx;
+        const bool pre = CHUNK > 1 && nxm >= 1 && nxm <= 4 && threadIdx.x < RES_TILE * NV;
+        const int c = threadIdx.x % RES_TILE;
+        int nbr[4], nxt[4];
+        const int tb = it.unit * chunk;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            nbr[s] = (pre && s < nxm && tb < t1) ? S.xnbr[(size_t)s * S.np16 + tb * RES_TILE + c] : -1;
+        for (int t = tb; t < t1; ++t) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                nxt[s] = (pre && s < nxm && t + 1 < t1) ? S.xnbr[(size_t)s * S.np16 + (t + 1) * RES_TILE + c]
+                                                        : -1;
+            ok = fast_resid_body<T>(nxm, S.np16, mode, S.Dinv, S.X, S.xnbr, S.dU, S.Rsrc, S.b, S.Uacc, ns,
+                                    status, t, bar, parity, pre ? nbr : nullptr);
             parity ^= 1u;
             if (!ok) break;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) nbr[s] = nxt[s];
             __syncthreads(); /* the next tile's copies overwrite the stages */
         }
     }
@@ -2834,8 +2849,20 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
     const uint32_t szD = RES_TILE * NB * sizeof(double), szR = RES_TILE * NV * sizeof(double);
     uint32_t parity = 0;
     bool failed = false;
+    /* the neighbour indices of the CTA's next tile load during the current one */
+    int pnbr[MULTI_NX];
+#pragma unroll
+    for (int s = 0; s < MULTI_NX; ++s)
+        pnbr[s] = (MODE == 1 && act && s < nx && (int)blockIdx.x < ntiles)
+                      ? __ldg(xnbr + (size_t)s * M.np16 + blockIdx.x * RES_TILE + c) : -1;
     for (int blk = blockIdx.x; blk < ntiles && nact > 0; blk += gridDim.x) {
         const int p0 = blk * RES_TILE;
+        const int bn = blk + gridDim.x;
+        int pnxt[MULTI_NX];
+#pragma unroll
+        for (int s = 0; s < MULTI_NX; ++s)
+            pnxt[s] = (MODE == 1 && act && s < nx && bn < ntiles)
+                          ? __ldg(xnbr + (size_t)s * M.np16 + bn * RES_TILE + c) : -1;
         if (tid == 0) {
             const uint64_t pol = policy_evict_first();
             mbar_arrive_expect_tx(bar, szD + (MODE == 1 ? nx * szD : nact * szR));
@@ -2862,8 +2889,7 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                  * that their latencies overlap */
                 int nbr[MULTI_NX];
 #pragma unroll
-                for (int s = 0; s < MULTI_NX; ++s)
-                    nbr[s] = s < nx ? __ldg(xnbr + (size_t)s * M.np16 + p0 + c) : -1;
+                for (int s = 0; s < MULTI_NX; ++s) nbr[s] = pnbr[s];
                 double gv[MULTI_MAX][MULTI_NX], uv[MULTI_MAX], dv[MULTI_MAX];
 #pragma unroll
                 for (int k = 0; k < MULTI_MAX; ++k) {
@@ -3006,6 +3032,8 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) multi_resid_kernel(
                 ++k;
             }
         }
+#pragma unroll
+        for (int s = 0; s < MULTI_NX; ++s) pnbr[s] = pnxt[s];
         __syncthreads(); /* the next tile's copies overwrite the stages */
     }
     (void)failed;
