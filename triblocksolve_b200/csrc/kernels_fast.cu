@@ -1857,7 +1857,7 @@ __device__ __forceinline__ bool full_resid_pos_body(
     const int *__restrict__ xnbrf, const double *__restrict__ rhsp, const double *__restrict__ Up,
     float *__restrict__ R32, double *__restrict__ partials, const float *__restrict__ Dinv32,
     float *__restrict__ b32, float *__restrict__ c32, unsigned *status, int blk, uint64_t *bar,
-    uint32_t parity) {
+    uint32_t parity, const int *nbr_pre = nullptr) {
     extern __shared__ __align__(128) unsigned char smem[];
     double *sD = reinterpret_cast<double *>(smem + 128);
     double *sX = sD + RES_TILE * NB;
@@ -1884,9 +1884,19 @@ __device__ __forceinline__ bool full_resid_pos_body(
     if (act && c32) c32[(size_t)p0 * NV + tid] = 0.0f;
     if (act) {
         sg[c * NV + i] = Up[(size_t)(p0 + c) * NV + i];
-        for (int s = 0; s < nxf; ++s) {
-            const int nb = xnbrf[(size_t)s * np16 + p0 + c];
-            sg[((s + 1) * RES_TILE + c) * NV + i] = (nb >= 0) ? Up[(size_t)nb * NV + i] : 0.0;
+        if (nbr_pre) { /* indices loaded during the previous tile */
+#pragma unroll
+            for (int s = 0; s < 4; ++s) {
+                if (s < nxf) {
+                    const int nb = nbr_pre[s];
+                    sg[((s + 1) * RES_TILE + c) * NV + i] = (nb >= 0) ? Up[(size_t)nb * NV + i] : 0.0;
+                }
+            }
+        } else {
+            for (int s = 0; s < nxf; ++s) {
+                const int nb = xnbrf[(size_t)s * np16 + p0 + c];
+                sg[((s + 1) * RES_TILE + c) * NV + i] = (nb >= 0) ? Up[(size_t)nb * NV + i] : 0.0;
+            }
         }
     }
     const bool ok = mbar_wait(bar, parity);
@@ -1953,11 +1963,25 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_kernel(
     uint64_t *bar = resid_bar_init();
     const int ntiles = np16 / RES_TILE;
     uint32_t parity = 0;
+    /* the next tile's neighbour indices load during the current one */
+    const bool pre = nxf >= 1 && nxf <= 4 && threadIdx.x < RES_TILE * NV;
+    const int c = threadIdx.x % RES_TILE;
+    int nbr[4], nxt[4];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+        nbr[s] = (pre && s < nxf && (int)blockIdx.x < ntiles)
+                     ? xnbrf[(size_t)s * np16 + blockIdx.x * RES_TILE + c] : -1;
     for (int w = blockIdx.x; w < ntiles; w += gridDim.x) {
+        const int wn = w + gridDim.x;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            nxt[s] = (pre && s < nxf && wn < ntiles) ? xnbrf[(size_t)s * np16 + wn * RES_TILE + c] : -1;
         const bool ok = full_resid_pos_body(nxf, np16, Dp, XF, xnbrf, rhsp, Up, R32, partials, Dinv32,
-                                            b32, c32, status, w, bar, parity);
+                                            b32, c32, status, w, bar, parity, pre ? nbr : nullptr);
         parity ^= 1u;
         if (!ok) break;
+#pragma unroll
+        for (int s = 0; s < 4; ++s) nbr[s] = nxt[s];
         __syncthreads(); /* the next tile's copies overwrite the stages */
     }
 }
@@ -2294,11 +2318,26 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_batch_kernel(
         if (active && !active[it.sys]) continue;
         const FullPosSys S = sys[it.sys];
         const int t1 = chunk_end(it.unit, chunk, S.np16 / RES_TILE);
-        for (int t = it.unit * chunk; t < t1; ++t) {
+        /* the next tile's neighbour indices load during the current one */
+        const bool pre = chunk > 1 && S.nxf >= 1 && S.nxf <= 4 && threadIdx.x < RES_TILE * NV;
+        const int c = threadIdx.x % RES_TILE;
+        int nbr[4], nxt[4];
+        const int tb = it.unit * chunk;
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            nbr[s] = (pre && s < S.nxf && tb < t1) ? S.xnbrf[(size_t)s * S.np16 + tb * RES_TILE + c] : -1;
+        for (int t = tb; t < t1; ++t) {
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                nxt[s] = (pre && s < S.nxf && t + 1 < t1)
+                             ? S.xnbrf[(size_t)s * S.np16 + (t + 1) * RES_TILE + c] : -1;
             ok = full_resid_pos_body(S.nxf, S.np16, S.Dp, S.XF, S.xnbrf, S.rhsp, S.Up, S.R32,
-                                     S.partials, S.Dinv32, S.b32, S.c32, status, t, bar, parity);
+                                     S.partials, S.Dinv32, S.b32, S.c32, status, t, bar, parity,
+                                     pre ? nbr : nullptr);
             parity ^= 1u;
             if (!ok) break;
+#pragma unroll
+            for (int s = 0; s < 4; ++s) nbr[s] = nxt[s];
             __syncthreads(); /* the next tile's copies overwrite the stages */
         }
     }
