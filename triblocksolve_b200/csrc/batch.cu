@@ -308,6 +308,8 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         efree_async(e, &e.d_g_prime);
         efree_async(e, &e.d_g_blocks);
         efree_async(e, &e.d_g_chunks);
+        efree_async(e, &e.d_g_units);
+        efree_async(e, &e.d_g_solo);
         if (e.algo == TBS_ALGO_FP64) {
             if (!rc) rc = ealloc_async(e, &e.d_th64, c);
             if (!rc) rc = ealloc_async(e, &e.d_rs_prime, c);
@@ -328,6 +330,8 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         if (!rc) rc = ealloc_async(e, &e.d_g_prime, gi);
         if (!rc) rc = ealloc_async(e, &e.d_g_blocks, gi);
         if (!rc) rc = ealloc_async(e, &e.d_g_chunks, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_units, gi);
+        if (!rc) rc = ealloc_async(e, &e.d_g_solo, gi);
         e.cap_mem = rc ? 0 : c;
         engine_drop_graph(e);
     }
@@ -359,16 +363,18 @@ static std::vector<std::vector<int>> group_members(const std::vector<Member> &m,
     return g;
 }
 
-/* host image of a group index (layout in tbs_internal.hxx) */
+/* host image of a group index (layout in tbs_internal.hxx); per_member:
+ * a group's items are its units times its members (an item is one member's
+ * unit), else its units (an item is a unit of every member) */
 static std::vector<int> group_index(const std::vector<std::vector<int>> &g,
-                                    const std::vector<int> &units_per_group) {
+                                    const std::vector<int> &units_per_group, bool per_member = true) {
     const int ng = (int)g.size();
     std::vector<int> v;
     v.push_back(ng);
     long long base = 0;
     for (int j = 0; j < ng; ++j) {
         v.push_back((int)base);
-        base += (long long)units_per_group[j] * (long long)g[j].size();
+        base += (long long)units_per_group[j] * (per_member ? (long long)g[j].size() : 1LL);
     }
     v.push_back((int)base);
     for (int j = 0; j < ng; ++j) v.push_back((int)g[j].size());
@@ -524,6 +530,15 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
     up.put(e.d_lines, lines);
     up.put(e.d_g_tiles, gi_tiles);
     up.put(e.d_g_chunks, group_index(g_all, units(g_all, 2)));
+    {
+        /* the sweep residual: members alone in their system run per member,
+         * several members of one system together over one staging of its
+         * blocks per tile */
+        std::vector<std::vector<int>> g_solo, g_multi;
+        for (const auto &grp : g_all) (grp.size() > 1 ? g_multi : g_solo).push_back(grp);
+        up.put(e.d_g_solo, group_index(g_solo, units(g_solo, 2)));
+        up.put(e.d_g_units, group_index(g_multi, units(g_multi, 2), false));
+    }
     up.put(e.d_g_prime, gi_prime);
     up.put(e.d_active, e.h_active);
     rc = up.flush();
@@ -612,8 +627,10 @@ static int engine_body(Engine &e, Cond cc, int inner) {
     if (e.algo == TBS_ALGO_FP64) {
         ERUN("fast_thomas", launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines, &C->nlines,
                                                         e.d_active, e.d_queue, e.d_status));
-        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_chunks,
+        ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_solo,
                                                       BATCH_CHUNK, e.d_active, e.d_status));
+        ERUN("fast_resid_group", launch_resid_group<double>(st, e.max_nx, e.d_rs_body, e.d_g_units,
+                                                            BATCH_CHUNK, e.d_active, e.d_status));
         ERUN("reduce_norm", launch_reduce_batch(st, 160, e.d_red_body, &C->nsys, e.cap_mem, 0,
                                                 e.d_active, C, e.d_counter, cc.handle, cc.use));
         return TBS_OK;

@@ -72,6 +72,8 @@ struct Engine {
     WorkItem *d_lines = nullptr;                       /* Thomas items, explicit */
     int *d_g_tiles = nullptr, *d_g_prime = nullptr, *d_g_blocks = nullptr; /* group indices */
     int *d_g_chunks = nullptr; /* every member, units of BATCH_CHUNK tiles */
+    int *d_g_solo = nullptr;   /* members alone in their system, units of BATCH_CHUNK tiles */
+    int *d_g_units = nullptr;  /* systems with several members, units of BATCH_CHUNK tiles */
     int *d_active = nullptr;
     unsigned *d_queue = nullptr, *d_counter = nullptr, *d_status = nullptr;
     BatchCtl *d_ctl = nullptr;

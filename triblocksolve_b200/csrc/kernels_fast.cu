@@ -2210,6 +2210,189 @@ __global__ void __launch_bounds__(RES_THREADS_FAST, CHUNK == 1 ? 8 : 6) fast_res
     }
 }
 
+/* Item w of a unit index (the group index layout with base[] the prefix
+ * sums of each group's units, not units x members): (group, unit). */
+__device__ __forceinline__ int2 group_unit(const int *__restrict__ gi, int w) {
+    const int ng = gi[0];
+    const int *base = gi + 1;
+    int lo = 0, hi = ng - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (base[mid] <= w) lo = mid;
+        else hi = mid - 1;
+    }
+    return make_int2(lo, w - base[lo]);
+}
+
+/* The sweep residual (mode 1) of the members of one system together: an
+ * item is (system group, chunk of tiles); per tile the CTA stages the
+ * system's Dinv and cross-line blocks once and then runs every active
+ * member (one right-hand side each) over them, with fast_resid_body's
+ * arithmetic, in its order, for each: U += dU, neighbour gathers, R, b,
+ * the tile's partial.  The members' blocks are read from HBM once per tile
+ * instead of once per member. */
+template <typename T>
+__global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_group_kernel(
+    const ResidSys<T> *__restrict__ sys, const int *__restrict__ gunits, int chunk,
+    const int *__restrict__ active, unsigned *status) {
+    extern __shared__ __align__(128) unsigned char smem[];
+    __shared__ double red[RES_THREADS_FAST / 32];
+    uint64_t *bar = resid_bar_init();
+    const int ng = gunits[0];
+    const int nwork = gunits[1 + ng];
+    const int *nmem = gunits + 2 + ng, *moff = nmem + ng, *mlist = moff + ng;
+    const int tid = threadIdx.x;
+    const int c = tid % RES_TILE, i = tid / RES_TILE;
+    const bool act = tid < RES_TILE * NV;
+    uint32_t parity = 0;
+    for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+        const int2 gu = group_unit(gunits, w);
+        const int *ml = mlist + moff[gu.x];
+        const int r = nmem[gu.x];
+        const ResidSys<T> S0 = sys[ml[0]];
+        const int nx = S0.nx, np16 = S0.np16;
+        const int nxa = nx > 0 ? nx : 1;
+        T *sD = reinterpret_cast<T *>(smem + 128);
+        T *sX = sD + RES_TILE * NB;
+        T *sg = sX + nx * RES_TILE * NB;
+        T *sr = sg + nxa * RES_TILE * NV;
+        T *sb = sr + RES_TILE * NV;
+        const uint32_t szD = RES_TILE * NB * sizeof(T);
+        const int t1 = chunk_end(gu.y, chunk, np16 / RES_TILE);
+        const int tb = gu.y * chunk;
+        /* a tile's neighbour indices serve every member; the next tile's
+         * load while this one is worked on */
+        int nb[4], nbn[4];
+#pragma unroll
+        for (int s = 0; s < 4; ++s)
+            nb[s] = (act && s < nx && tb < t1) ? S0.xnbr[(size_t)s * np16 + tb * RES_TILE + c] : -1;
+        for (int t = tb; t < t1; ++t) {
+            const int p0 = t * RES_TILE;
+            if (tid == 0) {
+                const uint64_t pol = policy_evict_first();
+                mbar_arrive_expect_tx(bar, (1 + nx) * szD);
+                bulk_g2s_hint(sD, S0.Dinv + (size_t)p0 * NB, szD, bar, pol);
+                for (int s = 0; s < nx; ++s)
+                    bulk_g2s_hint(sX + s * RES_TILE * NB, S0.X + ((size_t)s * np16 + p0) * NB, szD, bar,
+                                  pol);
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s)
+                nbn[s] = (act && s < nx && t + 1 < t1) ? S0.xnbr[(size_t)s * np16 + (t + 1) * RES_TILE + c]
+                                                       : -1;
+            /* members in a software pipeline: the next active member's
+             * loads (its U and dU, its neighbour gathers) are issued before
+             * the current one's products, so they overlap them */
+            const size_t q = (size_t)p0 * NV + tid;
+            auto next_active = [&](int k) {
+                while (k < r && active && !active[ml[k]]) ++k;
+                return k;
+            };
+            auto load_member = [&](const ResidSys<T> &S, T &u, T &d, T (&g)[4]) {
+                u = d = T(0);
+#pragma unroll
+                for (int s = 0; s < 4; ++s) g[s] = T(0);
+                if (!act) return;
+                d = S.dU[q];
+                if (S.Uacc) u = S.Uacc[q];
+#pragma unroll
+                for (int s = 0; s < 4; ++s)
+                    if (s < nx && nb[s] >= 0) g[s] = S.dU[(size_t)nb[s] * NV + i];
+            };
+            bool staged = false;
+            int k = next_active(0);
+            ResidSys<T> Sc{};
+            T cu, cd, cg[4];
+            if (k < r) {
+                Sc = sys[ml[k]];
+                load_member(Sc, cu, cd, cg);
+            }
+            while (k < r) {
+                if (act && Sc.Uacc) Sc.Uacc[q] = cu + cd;
+                if (act) {
+#pragma unroll
+                    for (int s = 0; s < 4; ++s)
+                        if (s < nx) sg[(s * RES_TILE + c) * NV + i] = cg[s];
+                }
+                const int kn = next_active(k + 1);
+                ResidSys<T> Sn{};
+                T nu = T(0), nd = T(0), ngv[4] = {T(0), T(0), T(0), T(0)};
+                if (kn < r) {
+                    Sn = sys[ml[kn]];
+                    load_member(Sn, nu, nd, ngv);
+                }
+                if (!staged) {
+                    const bool ok = mbar_wait(bar, parity);
+                    parity ^= 1u;
+                    staged = true;
+                    if (__syncthreads_or(!ok)) {
+                        if (tid == 0) {
+                            atomicOr(status, ST_TIMEOUT);
+                            mbar_wait(bar, parity ^ 1u, 1LL << 28);
+                        }
+                        return;
+                    }
+                } else {
+                    __syncthreads();
+                }
+                T rr = T(0);
+                if (act) {
+                    T a0 = T(0), a1 = T(0), a2 = T(0);
+                    for (int s = 0; s < nx; ++s) {
+                        const T *xr = sX + (s * RES_TILE + c) * NB + i;
+                        const T *g = sg + (s * RES_TILE + c) * NV;
+                        a0 += xr[0] * g[0];
+                        a1 += xr[9] * g[1];
+                        a2 += xr[18] * g[2];
+                        a0 += xr[27] * g[3];
+                        a1 += xr[36] * g[4];
+                        a2 += xr[45] * g[5];
+                        a0 += xr[54] * g[6];
+                        a1 += xr[63] * g[7];
+                        a2 += xr[72] * g[8];
+                    }
+                    rr = a0 + (a1 + a2);
+                    sr[c * NV + i] = rr;
+                }
+                __syncthreads();
+                double sq = act ? (double)rr * (double)rr : 0.0;
+                if (act) sb[c * NV + i] = neg_dinv_row<T>(sD + c * NB + i, sr + c * NV);
+                __syncthreads();
+                if (act) Sc.b[(size_t)p0 * NV + tid] = sb[tid];
+                for (int o = 16; o > 0; o >>= 1) sq += __shfl_down_sync(FULL, sq, o);
+                if ((tid & 31) == 0) red[tid >> 5] = sq;
+                __syncthreads();
+                if (tid == 0) {
+                    double tot = 0.0;
+                    for (int ww = 0; ww < RES_THREADS_FAST / 32; ++ww) tot += red[ww];
+                    Sc.partials[t] = tot;
+                }
+                __syncthreads(); /* the next member overwrites sg, sr, sb and red */
+                Sc = Sn;
+                cu = nu;
+                cd = nd;
+#pragma unroll
+                for (int s = 0; s < 4; ++s) cg[s] = ngv[s];
+                k = kn;
+            }
+            if (!staged) { /* no member active: the tile's copies still land */
+                const bool ok = mbar_wait(bar, parity);
+                parity ^= 1u;
+                if (__syncthreads_or(!ok)) {
+                    if (tid == 0) {
+                        atomicOr(status, ST_TIMEOUT);
+                        mbar_wait(bar, parity ^ 1u, 1LL << 28);
+                    }
+                    return;
+                }
+            }
+#pragma unroll
+            for (int s = 0; s < 4; ++s) nb[s] = nbn[s];
+            __syncthreads(); /* the next tile's copies overwrite the stages */
+        }
+    }
+}
+
 static int resid_batch_grid(size_t smem, const void *fn) {
     int per = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, fn, RES_THREADS_FAST, smem) != cudaSuccess ||
@@ -2343,6 +2526,17 @@ __global__ void __launch_bounds__(RES_THREADS_FAST) full_resid_pos_batch_kernel(
     }
 }
 
+template <typename T>
+int launch_resid_group(cudaStream_t st, int max_nx, const ResidSys<T> *sys, const int *gunits, int chunk,
+                       const int *active, unsigned *status) {
+    const size_t smem = resid_smem_bytes<T>(max_nx);
+    const int grid = resid_batch_grid(smem, (const void *)fast_resid_group_kernel<T>);
+    fast_resid_group_kernel<T><<<grid, RES_THREADS_FAST, smem, st>>>(sys, gunits, chunk, active, status);
+    return (int)cudaGetLastError();
+}
+template int launch_resid_group<double>(cudaStream_t, int, const ResidSys<double> *, const int *, int,
+                                        const int *, unsigned *);
+
 int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
                                 const int *groups, int chunk, const int *active, unsigned *status) {
     const size_t smem = fullpos_smem_bytes(max_nxf);
@@ -2437,6 +2631,8 @@ int batch_prepare(int max_nx) {
     if (!rc)
         rc = set_smem((const void *)fast_resid_batch_kernel<float, BATCH_CHUNK>,
                       resid_smem_bytes<float>(max_nx));
+    if (!rc)
+        rc = set_smem((const void *)fast_resid_group_kernel<double>, resid_smem_bytes<double>(max_nx));
     if (!rc) rc = set_smem((const void *)full_resid_pos_batch_kernel, fullpos_smem_bytes(4));
     return rc;
 }

@@ -415,6 +415,13 @@ template <typename T>
 /* units of `groups`: single tiles (chunk 1) or chunks of BATCH_CHUNK tiles */
 int launch_resid_batch(cudaStream_t st, int mode, int max_nx, const ResidSys<T> *sys,
                        const int *groups, int chunk, const int *active, unsigned *status);
+/* the sweep residual (mode 1) of every member, the members of one system
+ * together over one staging of its blocks per tile; gunits: the group
+ * index of the members with base[] the prefix sums of units (chunks of
+ * `chunk` tiles) per group */
+template <typename T>
+int launch_resid_group(cudaStream_t st, int max_nx, const ResidSys<T> *sys, const int *gunits, int chunk,
+                       const int *active, unsigned *status);
 int launch_full_resid_batch(cudaStream_t st, const FullResSys *sys, const int *groups,
                             const int *active);
 int launch_full_resid_pos_batch(cudaStream_t st, int max_nxf, const FullPosSys *sys,
