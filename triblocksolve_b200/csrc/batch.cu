@@ -242,6 +242,8 @@ int engine_init(Engine &e, int device, cudaStream_t stream, int algo) {
         cudaMallocHost(&e.h_status, sizeof(unsigned)) != cudaSuccess)
         return efail(e, TBS_ERR_NOMEM, "pinned allocation failed");
     std::memset(e.h_ctl, 0, sizeof(BatchCtl));
+    if (algo == TBS_ALGO_FP64 && multi_items_prepare() != 0)
+        return efail(e, TBS_ERR_CUDA, "shared-memory opt-in failed");
     ECK(cudaMemsetAsync(e.d_queue, 0, 2 * sizeof(unsigned), e.stream));
     ECK(cudaMemsetAsync(e.d_counter, 0, sizeof(unsigned), e.stream));
     ECK(cudaMemsetAsync(e.d_status, 0, sizeof(unsigned), e.stream));
@@ -285,7 +287,7 @@ void engine_free(Engine &e) {
 }
 
 /* grow the capacity-sized arrays (never shrinks); growth invalidates the graph */
-static int ensure_capacity(Engine &e, int nmem, int nlines) {
+static int ensure_capacity(Engine &e, int nmem, int nlines, int nmitems = 0) {
     auto grow = [](int need, int have, int least) {
         return need <= have ? have : std::max({need, 2 * have, least});
     };
@@ -310,7 +312,9 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         efree_async(e, &e.d_g_chunks);
         efree_async(e, &e.d_g_units);
         efree_async(e, &e.d_g_solo);
+        efree_async(e, &e.d_ml);
         if (e.algo == TBS_ALGO_FP64) {
+            if (!rc) rc = ealloc_async(e, &e.d_ml, c);
             if (!rc) rc = ealloc_async(e, &e.d_th64, c);
             if (!rc) rc = ealloc_async(e, &e.d_rs_prime, c);
             if (!rc) rc = ealloc_async(e, &e.d_rs_body, c);
@@ -340,6 +344,15 @@ static int ensure_capacity(Engine &e, int nmem, int nlines) {
         efree_async(e, &e.d_lines);
         rc = ealloc_async(e, &e.d_lines, c);
         e.cap_lines = rc ? 0 : c;
+        engine_drop_graph(e);
+    }
+    /* the multi-RHS line solves launch one CTA per item up to capacity (the
+     * graph holds the grid), so the capacity starts small */
+    if (!rc && e.algo == TBS_ALGO_FP64 && (nmitems > e.cap_mitems || !e.d_mitems)) {
+        const int c = grow(std::max(nmitems, 1), e.cap_mitems, 1024);
+        efree_async(e, &e.d_mitems);
+        rc = ealloc_async(e, &e.d_mitems, c);
+        e.cap_mitems = rc ? 0 : c;
         engine_drop_graph(e);
     }
     return rc;
@@ -391,8 +404,21 @@ static std::vector<int> group_index(const std::vector<std::vector<int>> &g,
 /* Thomas items in the engine's order.  Longest lines first; the items of
  * one line of one system (several right-hand sides) are adjacent, so that
  * the warps running them together share the line's blocks in L2. */
-static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Member> &m) {
+/* the members whose lines the batched line solve runs: all of them, but
+ * for FP64 the members of a system with several members, whose line
+ * solves run together (multi_items) */
+static std::vector<char> thomas_take(const Engine &e, const std::vector<Member> &m) {
+    std::vector<char> take(m.size(), 1);
+    if (e.algo != TBS_ALGO_FP64) return take;
     std::vector<char> all(m.size(), 1);
+    for (const auto &grp : group_members(m, all))
+        if (grp.size() > 1)
+            for (int k : grp) take[k] = 0;
+    return take;
+}
+
+static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Member> &m) {
+    const std::vector<char> all = thomas_take(e, m);
     const std::vector<std::vector<int>> g = group_members(m, all);
     struct GL {
         int len, group, line;
@@ -410,9 +436,50 @@ static std::vector<WorkItem> line_items(const Engine &e, const std::vector<Membe
             for (int k : g[x.group]) items.push_back({k, x.line});
     } else {
         for (size_t k = 0; k < m.size(); ++k)
-            for (int l = 0; l < m[k].sys->nline; ++l) items.push_back({(int)k, l});
+            if (all[k])
+                for (int l = 0; l < m[k].sys->nline; ++l) items.push_back({(int)k, l});
     }
     return items;
+}
+
+/* FP64: the line solves of the members of a system with several members,
+ * up to MULTI_MAX of them per CTA (their lines' blocks read once): one
+ * MultiLine per such group of members, and its (group, line) items,
+ * longest lines first */
+static void multi_items(const std::vector<Member> &m, std::vector<MultiLine> &sys,
+                        std::vector<WorkItem> &items) {
+    sys.clear();
+    items.clear();
+    std::vector<char> all(m.size(), 1);
+    struct GL {
+        int len, grp, line;
+    };
+    std::vector<GL> gl;
+    for (const auto &grp : group_members(m, all)) {
+        if (grp.size() < 2) continue;
+        for (size_t k0 = 0; k0 < grp.size(); k0 += MULTI_MAX) {
+            const tbs_ctx *c = m[grp[k0]].sys;
+            MultiLine L{};
+            L.line_start = c->L.line_start;
+            L.line_len = c->L.line_len;
+            L.line_twist = c->L.line_twist;
+            L.G = c->d_G;
+            L.Gam = c->d_Gam;
+            L.nr = (int)std::min<size_t>(MULTI_MAX, grp.size() - k0);
+            for (int r = 0; r < MULTI_MAX; ++r) {
+                const int k = grp[k0 + (r < L.nr ? r : 0)];
+                L.aid[r] = k;
+                L.b[r] = m[k].v.b;
+                L.y[r] = m[k].v.y;
+                L.dU[r] = m[k].v.dUp;
+            }
+            const int gi = (int)sys.size();
+            sys.push_back(L);
+            for (int l = 0; l < c->nline; ++l) gl.push_back({c->h_linesize[l], gi, l});
+        }
+    }
+    std::stable_sort(gl.begin(), gl.end(), [](const GL &a, const GL &b) { return a.len > b.len; });
+    for (const GL &x : gl) items.push_back({x.grp, x.line});
 }
 
 int engine_set_members(Engine &e, const std::vector<Member> &members) {
@@ -433,7 +500,10 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
         e.max_nx = nx;
         engine_drop_graph(e);
     }
-    int rc = ensure_capacity(e, std::max(n, 1), (int)std::max(nlines, 1LL));
+    std::vector<MultiLine> mls;
+    std::vector<WorkItem> mitems;
+    if (!mixed) multi_items(members, mls, mitems);
+    int rc = ensure_capacity(e, std::max(n, 1), (int)std::max(nlines, 1LL), (int)mitems.size());
     if (rc) return rc;
 
     std::vector<ThomasSys<double>> th64;
@@ -514,6 +584,8 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
     Stager up(e);
     if (!mixed) {
         up.put(e.d_th64, th64);
+        up.put(e.d_ml, mls);
+        up.put(e.d_mitems, mitems);
         up.put(e.d_rs_prime, rsp);
         up.put(e.d_rs_body, rsb);
     } else {
@@ -546,6 +618,7 @@ int engine_set_members(Engine &e, const std::vector<Member> &members) {
     BatchCtl &C = *e.h_ctl;
     C.nsys = n;
     C.nlines = (int)lines.size();
+    C.nmitems = (int)mitems.size();
     C.ntiles = gi_tiles[1 + gi_tiles[0]];
     C.nblocks = (int)nblocks;
     C.nprime_sys = (int)redp.size();
@@ -627,6 +700,10 @@ static int engine_body(Engine &e, Cond cc, int inner) {
     if (e.algo == TBS_ALGO_FP64) {
         ERUN("fast_thomas", launch_thomas_batch<double>(st, e.sched, e.d_th64, e.d_lines, &C->nlines,
                                                         e.d_active, e.d_queue, e.d_status));
+        /* the line solves of several members of one system: their blocks
+         * read once per line for up to MULTI_MAX of them */
+        ERUN("multi_thomas", launch_multi_thomas_items(st, e.cap_mitems, e.d_ml, e.d_mitems, &C->nmitems,
+                                                       e.d_active, e.d_status));
         ERUN("fast_resid", launch_resid_batch<double>(st, 1, e.max_nx, e.d_rs_body, e.d_g_solo,
                                                       BATCH_CHUNK, e.d_active, e.d_status));
         ERUN("fast_resid_group", launch_resid_group<double>(st, e.max_nx, e.d_rs_body, e.d_g_units,

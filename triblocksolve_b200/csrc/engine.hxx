@@ -70,6 +70,10 @@ struct Engine {
     VecSys *d_vec = nullptr;
     ReduceSys *d_red_prime = nullptr, *d_red_body = nullptr;
     WorkItem *d_lines = nullptr;                       /* Thomas items, explicit */
+    /* FP64: line solves of groups of one system's members (multi-RHS) */
+    MultiLine *d_ml = nullptr;
+    WorkItem *d_mitems = nullptr;
+    int cap_mitems = 0;
     int *d_g_tiles = nullptr, *d_g_prime = nullptr, *d_g_blocks = nullptr; /* group indices */
     int *d_g_chunks = nullptr; /* every member, units of BATCH_CHUNK tiles */
     int *d_g_solo = nullptr;   /* members alone in their system, units of BATCH_CHUNK tiles */

@@ -2633,6 +2633,7 @@ int batch_prepare(int max_nx) {
                       resid_smem_bytes<float>(max_nx));
     if (!rc)
         rc = set_smem((const void *)fast_resid_group_kernel<double>, resid_smem_bytes<double>(max_nx));
+
     if (!rc) rc = set_smem((const void *)full_resid_pos_batch_kernel, fullpos_smem_bytes(4));
     return rc;
 }
@@ -2761,28 +2762,36 @@ __device__ __forceinline__ void bwd_chunk_m(const double *sG, double *const *bc,
  * Gam rows.  All warps have consumed a stage before it is refilled (one
  * CTA barrier per chunk). */
 template <int P>
-__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kernel(
-    int nline, int NS, int nr, long long vs, const int *__restrict__ line_start,
-    const int *__restrict__ line_len, const int *__restrict__ line_twist,
-    const double *__restrict__ G, const double *__restrict__ Gam, const double *__restrict__ b,
-    double *__restrict__ y, double *__restrict__ dU, const int *__restrict__ active,
-    unsigned *status) {
+__device__ __forceinline__ void multi_thomas_line(const MultiLine &S, int l, int NS,
+                                                  const int *__restrict__ active, unsigned *status) {
     using T = double;
     extern __shared__ __align__(128) unsigned char smem[];
     __shared__ unsigned amask_s;
     __shared__ int rid[MULTI_MAX];
-    const int l = blockIdx.x;
-    if (l >= nline) return;
+    /* the right-hand sides' vectors, indexed by slot */
+    __shared__ const T *sbp[MULTI_MAX];
+    __shared__ T *syp[MULTI_MAX], *sdp[MULTI_MAX];
+    const int nr = S.nr;
+    const int *__restrict__ line_start = S.line_start;
+    const int *__restrict__ line_len = S.line_len;
+    const int *__restrict__ line_twist = S.line_twist;
+    const T *__restrict__ G = S.G;
+    const T *__restrict__ Gam = S.Gam;
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     if (tid == 0) {
         unsigned am = 0;
         int k = 0;
-        for (int r = 0; r < nr; ++r)
-            if (active[r]) {
+#pragma unroll
+        for (int r = 0; r < MULTI_MAX; ++r) {
+            sbp[r] = S.b[r];
+            syp[r] = S.y[r];
+            sdp[r] = S.dU[r];
+            if (r < nr && active[S.aid[r]]) {
                 am |= 1u << r;
                 rid[k++] = r;
             }
+        }
         amask_s = am;
         for (int s = 0; s < NS; ++s) mbar_init(&bars[s], 1);
         mbar_fence_init();
@@ -2818,11 +2827,11 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     for (int j = 0; j < MULTI_RPW; ++j) {
         const int jj = j < nown ? j : 0;
         slot[j] = mine ? k0 + jj : 0;
-        const size_t ro = (size_t)(mine ? rid[k0 + jj] : 0) * (size_t)vs;
+        const int rr = mine ? rid[k0 + jj] : 0;
         bc[j] = bcw + j * 80 + h * 40;
-        yl[j] = y + ro + (size_t)ps * NV;
-        dUl[j] = dU + ro + (size_t)ps * NV;
-        bg[j] = b + ro + (size_t)ps * NV;
+        yl[j] = syp[rr] + (size_t)ps * NV;
+        dUl[j] = sdp[rr] + (size_t)ps * NV;
+        bg[j] = sbp[rr] + (size_t)ps * NV;
     }
     const uint64_t pol = tid == 0 ? policy_evict_first() : 0;
     for (int t = lane; t < MULTI_RPW * 80; t += 32) bcw[t] = T(0);
@@ -2851,8 +2860,8 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
                 const size_t p = (size_t)(ps + cp + c * P);
                 bulk_g2s_hint(hb, G + p * NB, cnt * NB * sizeof(T), &bars[s], pol);
                 for (int k = 0; k < nact; ++k)
-                    bulk_g2s(hb + (size_t)(P * NB + k * P * NV) * sizeof(T),
-                             b + (size_t)rid[k] * (size_t)vs + p * NV, cnt * NV * sizeof(T), &bars[s]);
+                    bulk_g2s(hb + (size_t)(P * NB + k * P * NV) * sizeof(T), sbp[rid[k]] + p * NV,
+                             cnt * NV * sizeof(T), &bars[s]);
             } else {
                 const int c = nc - 1 - (job - nf);
                 if (c < 0) continue;
@@ -2984,6 +2993,24 @@ __global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kerne
     }
 }
 
+/* one line of one system per CTA: the context's solve (tbs_solve_multi) */
+template <int P>
+__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_kernel(
+    int nline, int NS, MultiLine S, const int *__restrict__ active, unsigned *status) {
+    if ((int)blockIdx.x >= nline) return;
+    multi_thomas_line<P>(S, blockIdx.x, NS, active, status);
+}
+
+/* the batch engine: item k = (group of one system's members, line) */
+template <int P>
+__global__ void __launch_bounds__(32 * MULTI_MAX / MULTI_RPW) multi_thomas_items_kernel(
+    const MultiLine *__restrict__ sys, const WorkItem *__restrict__ items, const int *__restrict__ nitems,
+    int NS, const int *__restrict__ active, unsigned *status) {
+    if ((int)blockIdx.x >= *nitems) return;
+    const WorkItem it = items[blockIdx.x];
+    multi_thomas_line<P>(sys[it.sys], it.unit, NS, active, status);
+}
+
 static int multi_thomas_warps(int nr) { return (nr + MULTI_RPW - 1) / MULTI_RPW; }
 
 static size_t multi_thomas_stage(int nr) {
@@ -3021,9 +3048,40 @@ int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const doub
     if (L.nv != NV || nr < 1 || nr > MULTI_MAX) return (int)cudaErrorInvalidValue;
     const int NS = multi_thomas_ns(L, nr);
     const long long vs = (long long)L.np16 * NV;
+    MultiLine S{};
+    S.line_start = L.line_start;
+    S.line_len = L.line_len;
+    S.line_twist = L.line_twist;
+    S.G = G;
+    S.Gam = Gam;
+    S.nr = nr;
+    for (int r = 0; r < MULTI_MAX; ++r) {
+        const int rr = r < nr ? r : 0;
+        S.aid[r] = rr;
+        S.b[r] = b + (size_t)rr * vs;
+        S.y[r] = y + (size_t)rr * vs;
+        S.dU[r] = dU + (size_t)rr * vs;
+    }
     multi_thomas_kernel<THOMAS_P><<<L.nline, 32 * multi_thomas_warps(nr), multi_thomas_smem(nr, NS), st>>>(
-        L.nline, NS, nr, vs, L.line_start, L.line_len, L.line_twist, G, Gam, b, y, dU, active,
-        status);
+        L.nline, NS, S, active, status);
+    return (int)cudaGetLastError();
+}
+
+/* ring depth of the engine's multi-RHS line solves (their shared memory
+ * is sized for MULTI_MAX right-hand sides) */
+constexpr int MULTI_ITEMS_NS = 3;
+
+int multi_items_prepare() {
+    return set_smem((const void *)multi_thomas_items_kernel<THOMAS_P>,
+                    multi_thomas_smem(MULTI_MAX, MULTI_ITEMS_NS));
+}
+
+int launch_multi_thomas_items(cudaStream_t st, int grid, const MultiLine *sys, const WorkItem *items,
+                              const int *nitems, const int *active, unsigned *status) {
+    if (grid < 1) return 0;
+    multi_thomas_items_kernel<THOMAS_P>
+        <<<grid, 32 * multi_thomas_warps(MULTI_MAX), multi_thomas_smem(MULTI_MAX, MULTI_ITEMS_NS), st>>>(
+            sys, items, nitems, MULTI_ITEMS_NS, active, status);
     return (int)cudaGetLastError();
 }
 

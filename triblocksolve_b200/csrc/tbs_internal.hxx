@@ -298,6 +298,17 @@ struct MultiSys {
     int *active;
     unsigned *counter;
 };
+/* The line solves of up to MULTI_MAX right-hand sides of one system: its
+ * line layout and factors, and per slot r < nr its vectors and the index
+ * of its flag in the active array. */
+struct MultiLine {
+    const int *line_start, *line_len, *line_twist;
+    const double *G, *Gam;
+    int nr;
+    int aid[MULTI_MAX];
+    const double *b[MULTI_MAX];
+    double *y[MULTI_MAX], *dU[MULTI_MAX];
+};
 /* dU of every active right-hand side from its b (the line solves) */
 int launch_multi_thomas(cudaStream_t st, const FastLayout &L, int nr, const double *G,
                         const double *Gam, const double *b, double *y, double *dU,
@@ -310,6 +321,7 @@ int launch_multi_resid(cudaStream_t st, const FastLayout &L, int mode, const Mul
                        unsigned long long cond_handle, int use_cond, unsigned *status);
 int multi_prepare(const FastLayout &L, int nr);
 
+
 /* ------------------------------------------------------------ batches
  * Many independent systems swept together.  Each kernel takes one
  * descriptor per system and a list of work items (system, unit), so that
@@ -321,6 +333,11 @@ struct alignas(8) WorkItem {
     int sys;                    /* index into the launch's descriptors */
     int unit;                   /* line, residual tile or element block */
 };
+/* the batch engine's line solves of groups of one system's members: item k
+ * (k < *nitems, grid = capacity) = (index into sys, line) */
+int launch_multi_thomas_items(cudaStream_t st, int grid, const MultiLine *sys, const WorkItem *items,
+                              const int *nitems, const int *active, unsigned *status);
+int multi_items_prepare(); /* shared-memory opt-in of that launch (outside stream capture) */
 template <typename T>
 struct ThomasSys {
     const int *line_start, *line_len, *line_twist;
@@ -380,6 +397,7 @@ struct BatchCtl {
     int chunk_limit;            /* > 0: the loop ends after this many sweeps */
     int stop_on_finish;         /* 1: the loop ends when a member stops */
     int finished;               /* set by the norm launch when a member stops */
+    int nmitems;                /* FP64: (group of one system's members, line) items */
 };
 struct BatchSched {             /* persistent Thomas launch shape */
     int ctas_per_sm;            /* CTAs per SM, each solving one line at a time */
