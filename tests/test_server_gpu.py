@@ -145,6 +145,29 @@ def test_admission_by_footprint():
         srv.close()
 
 
+def test_many_members_of_one_system_same_as_alone():
+    """Twelve right-hand sides of one system in flight at once (the engine
+    runs them as groups of 8 and 4 in the multi-RHS line solve and together
+    in the grouped residual) beside another system's: each equals its solve
+    alone."""
+    sy = systems()
+    rng = np.random.default_rng(21)
+    srv = Server(0, ALGO_FP64, budget_bytes=8 << 30, max_rhs=32, chunk=3, lane_split=0)
+    try:
+        ids = [srv.add_system(m, j) for m, j in sy]
+        big, other = 2, 0
+        reqs = []
+        for k in range(3):
+            rows = rng.uniform(-1, 1, (4, 9 * sy[big][0].nelem))
+            reqs.append((big, rows, srv.submit(ids[big], rows, TOL)))
+            rows2 = rng.uniform(-1, 1, (1, 9 * sy[other][0].nelem))
+            reqs.append((other, rows2, srv.submit(ids[other], rows2, TOL)))
+        for s, rows, r in reqs:
+            check(r.wait(), alone(*sy[s], rows, ALGO_FP64))
+    finally:
+        srv.close()
+
+
 def test_three_lanes_same_as_alone():
     """Lane splits [100, 1000]: the 51- and 37-cell systems sweep in lane 0,
     the 480-cell one in lane 1, the 3,072-cell one in lane 2."""
