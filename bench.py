@@ -1453,7 +1453,9 @@ def main():
                            "%globaltimer (CUDA events cannot sit inside the solve graph's loop); "
                            "achieved/frac above are from CUDA events around eager launches of "
                            "the same solves"}
-        launches_per_solve = sum(v["launches"] for v in kern.values()) / nprof
+        # the profiled kernels of a solve, plus the two each graph-launched
+        # solve adds around its graph (control block in, state read back)
+        launches_per_solve = sum(v["launches"] for v in kern.values()) / nprof + 2
         sweeps_per_solve = sweeps_total / args.steps
         h2d = sum(host[k].nbytes for k in ("jacD", "jacO1", "jacO2", "rhs"))
         d2h = Uh.nbytes + 8 * (max_sweeps + 1)
