@@ -376,8 +376,9 @@ def run_batch(args):
     if rank == 0:
         peak, peak_kind = measured_peak_hbm()
         kern = {}
-        names = {"fast_thomas": "fast_thomas", "fast_resid": "fast_resid",
-                 "fast_thomas32": "fast_thomas32", "fast_resid32": "fast_resid32",
+        # the batch engine's line solves write dU (d) only, its residuals add it to U (c)
+        names = {"fast_thomas": "fast_thomas_dU", "fast_resid": "fast_resid_U",
+                 "fast_thomas32": "fast_thomas32", "fast_resid32": "fast_resid32_U",
                  "full_resid": "full_resid", "fast_resid32_rhs": "fast_resid32_rhs"}
         for name, (launches, ms) in prof.items():
             b = None
@@ -389,7 +390,7 @@ def run_batch(args):
                         return n_sw
                     th = inner[0] + (n_sw - 1) * inner[1]
                     return {"fast_thomas32": th, "fast_resid32": th - n_sw}.get(name, n_sw)
-                b = nprof * sum(s.kernel_bytes(name) * runs(n_sw) for s, n_sw in zip(solvers, swp))
+                b = nprof * sum(s.kernel_bytes(names[name]) * runs(n_sw) for s, n_sw in zip(solvers, swp))
             kern[name] = {"launches": launches, "total_ms": round(ms, 3),
                           "avg_us": round(1e3 * ms / launches, 2) if launches else None,
                           "bytes_total": b,
@@ -965,7 +966,9 @@ def run_partition(args, L, K, shift, tol):
         kern = {}
         for name, (launches, ms) in prof.items():
             try:
-                b = solver.kernel_bytes(name)
+                # a partition's line solve writes dU only; its residual adds dU to U
+                b = solver.kernel_bytes({"fast_thomas": "fast_thomas_dU",
+                                         "fast_resid": "fast_resid_U"}.get(name, name))
             except Exception:
                 b = None
             avg_us = 1e3 * ms / launches if launches else 0.0

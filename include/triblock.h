@@ -454,7 +454,11 @@ int tbs_selftest_timeout(tbs_ctx *ctx, long long budget_cycles);
 /* Algorithmic bytes one launch of each kernel moves (reads + writes of
  * every array it must touch once), for the roofline numerator.  The
  * multi-RHS kernels take the group size as a suffix: "multi_thomas/8",
- * "multi_resid/8" (every right-hand side active). */
+ * "multi_resid/8" (every right-hand side active).  "fast_thomas" and
+ * "fast_resid" are the forms tbs_solve's FP64 sweeps run (at block size 9
+ * the line solve adds dU to U); "fast_thomas_dU", "fast_resid_U" and
+ * "fast_resid32_U" are the forms of line partitions and the batch engine,
+ * whose residual kernels add the update instead. */
 int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
 
 /* Linear residual R = rhs + D U + (sum over each cell's interior faces of

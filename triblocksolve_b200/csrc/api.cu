@@ -487,6 +487,10 @@ static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; 
  * blocks when a cell has at most 4 interior faces (one shared-memory tile) */
 bool fullpos_ok(const tbs_ctx *ctx) { return ctx->L.nxf <= 4; }
 
+/* Whether the FP64 sweep's line solve adds dU to U (the size-9 kernels);
+ * otherwise the residual kernel that follows does */
+static bool thomas_adds_u(const tbs_ctx *ctx) { return ctx->nvar == 9; }
+
 /* The TBS_ALGO_FP64 sweep kernels for the context's block size: the tuned
  * size-9 kernels or their general form (kernels_nv.cu). */
 static int thomas64(tbs_ctx *ctx, const double *b, double *dU, double *U, int accumulate) {
@@ -659,9 +663,13 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
         return TBS_OK;
     }
     if (ctx->algo == TBS_ALGO_FP64) {
-        /* the Thomas kernel writes dU; the residual kernel adds it to U */
-        RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, 2));
-        RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, cc), ctx->d_Up));
+        /* size 9: the Thomas kernel adds dU to U as it writes dU, so the
+         * residual kernel reads neither its own dU nor U (72 bytes a cell
+         * fewer per sweep); other sizes: the residual kernel adds it */
+        const bool t_acc = thomas_adds_u(ctx);
+        RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, t_acc ? 1 : 2));
+        RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, cc),
+                                  t_acc ? nullptr : ctx->d_Up));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
@@ -675,14 +683,17 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
         RUN("fast_resid32_rhs", launch_fast_resid<float>(st, L, 0, ctx->d_Dinv32, ctx->d_X32, ctx->d_d32,
                                                          ctx->d_R32, ctx->d_b32, no_sink(), ctx->d_status,
                                                          ctx->d_c32));
+    /* every inner line solve but the last adds its d to c as it writes d
+     * (the same FP32 sum c + d the residual kernel formed before; the line
+     * solve is bound by its chain, the residual by HBM) */
     for (int m = 0; m < inner; ++m) {
         RUN("fast_thomas32", launch_fast_thomas<float>(st, L, ctx->d_G32, ctx->d_Gam32, ctx->d_b32,
                                                        ctx->d_y32, ctx->d_d32, ctx->d_c32,
-                                                       ctx->d_status, 2));
+                                                       ctx->d_status, m + 1 < inner ? 1 : 2));
         if (m + 1 < inner)
             RUN("fast_resid32", launch_fast_resid<float>(st, L, 3, nullptr, ctx->d_X32, ctx->d_d32,
                                                          nullptr, ctx->d_b32, no_sink(),
-                                                         ctx->d_status, ctx->d_c32));
+                                                         ctx->d_status, nullptr));
     }
     RUN("axpy", launch_axpy2_f32_f64(st, ctx->d_c32, ctx->d_d32, ctx->d_Up, (long long)L.np16 * 9));
     if (pos) {
@@ -1835,17 +1846,26 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     const double X = (double)ctx->n_xslots_real;
     const std::string k(kernel);
     double b = -1.0;
-    if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out, own dU + U in/out */
+    if (k == "fast_resid" && thomas_adds_u(ctx)) /* Dinv, X blocks, xnbr, neighbour dU, b out */
+        b = N * (blk + vec) + X * (blk + 4.0 + vec);
+    else if (k == "fast_resid" || k == "fast_resid_U")
+        /* the form that adds dU to U (line partitions, the batch engine, sizes
+         * other than 9): own dU and U in/out on top */
         b = N * (blk + vec + 3 * vec) + X * (blk + 4.0 + vec);
     else if (k == "fast_resid_rhs" || k == "fast_resid_check") /* Dinv, R in, b out */
         b = N * (blk + 2 * vec);
     else if (k == "fast_resid32_rhs")
         b = N * (blk + 2 * vec) / 2;
-    else if (k == "fast_resid32") /* DX blocks, xnbr, neighbour d, b out, own d + c in/out */
+    else if (k == "fast_resid32") /* DX blocks, xnbr, neighbour d, b out */
+        b = N * vec / 2 + X * (blk / 2 + 4.0 + vec / 2);
+    else if (k == "fast_resid32_U") /* the batch engine's: own d + c in/out on top */
         b = N * (4 * vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
-    else if (k == "fast_thomas") /* G, b | Gam, dU out (y stays on chip when the line fits) */
+    else if (k == "fast_thomas") /* G, b | Gam, dU out (y stays on chip when the line fits),
+                                  * U in/out when the line solve adds dU to U */
+        b = N * (2 * blk + 2 * vec) + (thomas_adds_u(ctx) ? N * 2 * vec : 0.0);
+    else if (k == "fast_thomas_dU") /* dU out only (line partitions, the batch engine) */
         b = N * (2 * blk + 2 * vec);
-    else if (k == "fast_thomas32")
+    else if (k == "fast_thomas32") /* c in/out of all inner solves but the last not counted */
         b = N * (2 * blk + 2 * vec) / 2;
     else if (k == "full_resid" && ctx->algo == TBS_ALGO_MIXED && fullpos_ok(ctx))
         /* position order: D, one block + index + neighbour U per face slot, own U, rhs, R32
@@ -1871,8 +1891,8 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
                 b = N * blk + X * (blk + 4.0) + nr * (N * 4 * vec + X * vec);
         }
     }
-    else if (k == "fast_resid_jv") /* X blocks, xnbr, neighbour dU, own dU, U in/out, v in, w out */
-        b = N * 5 * vec + X * (blk + 4.0 + vec);
+    else if (k == "fast_resid_jv") /* X blocks, xnbr, neighbour dU, v in, w out */
+        b = N * 2 * vec + X * (blk + 4.0 + vec);
     else if (k == "pij_sweep") /* Dinv, face blocks + index + neighbour dU, own dU, U in/out, b out */
         b = N * (blk + 4 * vec) + (double)ctx->n_fslots_real * (blk + 4.0 + vec);
     else if (k == "fast_factor") /* D, A, C in; Dinv, G, Gam out */

@@ -309,15 +309,17 @@ static int precond_product(tbs_ctx *ctx, const double *v, double *z, double *w, 
     /* b = -Dinv v, z = 0 */
     KRUN("fast_resid_rhs", launch_fast_resid<double>(st, L, 0, ctx->d_Dinv, ctx->d_X, ctx->d_dUp, v,
                                                      ctx->d_b, none, ctx->d_status, z));
+    /* each line solve adds its update to z as it writes it */
     for (int s = 0; s < sweeps; ++s) {
         KRUN("fast_thomas", launch_fast_thomas<double>(st, L, ctx->d_G, ctx->d_Gam, ctx->d_b, ctx->d_y,
-                                                       ctx->d_dUp, z, ctx->d_status, 2));
+                                                       ctx->d_dUp, z, ctx->d_status, 1));
         if (s + 1 < sweeps)
             KRUN("fast_resid", launch_fast_resid<double>(st, L, 1, ctx->d_Dinv, ctx->d_X, ctx->d_dUp,
-                                                         nullptr, ctx->d_b, none, ctx->d_status, z));
+                                                         nullptr, ctx->d_b, none, ctx->d_status,
+                                                         nullptr));
         else
             KRUN("fast_resid_jv", launch_fast_resid<double>(st, L, 4, nullptr, ctx->d_X, ctx->d_dUp, v,
-                                                            w, none, ctx->d_status, z));
+                                                            w, none, ctx->d_status, nullptr));
     }
     return TBS_OK;
 }
