@@ -114,6 +114,8 @@ struct Stager {
     explicit Stager(Engine &en) : e(en) {}
     template <typename T>
     void put(T *dst, const std::vector<T> &v) {
+        static_assert(sizeof(T) % 4 == 0 && alignof(T) >= 4,
+                      "xfer_jobs copies whole, aligned 4-byte words");
         if (v.empty()) return;
         const size_t b = v.size() * sizeof(T);
         const size_t off = host.size();
