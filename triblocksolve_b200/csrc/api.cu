@@ -487,9 +487,6 @@ static long long nvec(tbs_ctx *ctx) { return (long long)ctx->nvar * ctx->nelem; 
  * blocks when a cell has at most 4 interior faces (one shared-memory tile) */
 bool fullpos_ok(const tbs_ctx *ctx) { return ctx->L.nxf <= 4; }
 
-/* Whether the FP64 sweep's line solve adds dU to U (the size-9 kernels);
- * otherwise the residual kernel that follows does */
-static bool thomas_adds_u(const tbs_ctx *ctx) { return ctx->nvar == 9; }
 
 /* The TBS_ALGO_FP64 sweep kernels for the context's block size: the tuned
  * size-9 kernels or their general form (kernels_nv.cu). */
@@ -663,13 +660,12 @@ static int body(tbs_ctx *ctx, CondCtl cc, int inner) {
         return TBS_OK;
     }
     if (ctx->algo == TBS_ALGO_FP64) {
-        /* size 9: the Thomas kernel adds dU to U as it writes dU, so the
-         * residual kernel reads neither its own dU nor U (72 bytes a cell
-         * fewer per sweep); other sizes: the residual kernel adds it */
-        const bool t_acc = thomas_adds_u(ctx);
-        RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, t_acc ? 1 : 2));
-        RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, cc),
-                                  t_acc ? nullptr : ctx->d_Up));
+        /* the Thomas kernel adds dU to U as it writes dU (U read one chunk
+         * ahead of the backward chains), so the residual kernel reads
+         * neither its own dU nor U (72 bytes a cell fewer per sweep at
+         * size 9) */
+        RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, 1));
+        RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, cc), nullptr));
         return TBS_OK;
     }
     /* TBS_ALGO_MIXED: inner FP32 LIJ sweeps on J d = -R, then U += d and the
@@ -1846,11 +1842,11 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     const double X = (double)ctx->n_xslots_real;
     const std::string k(kernel);
     double b = -1.0;
-    if (k == "fast_resid" && thomas_adds_u(ctx)) /* Dinv, X blocks, xnbr, neighbour dU, b out */
+    if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out */
         b = N * (blk + vec) + X * (blk + 4.0 + vec);
-    else if (k == "fast_resid" || k == "fast_resid_U")
-        /* the form that adds dU to U (line partitions, the batch engine, sizes
-         * other than 9): own dU and U in/out on top */
+    else if (k == "fast_resid_U")
+        /* the form that adds dU to U (line partitions, the batch engine): own
+         * dU and U in/out on top */
         b = N * (blk + vec + 3 * vec) + X * (blk + 4.0 + vec);
     else if (k == "fast_resid_rhs" || k == "fast_resid_check") /* Dinv, R in, b out */
         b = N * (blk + 2 * vec);
@@ -1860,9 +1856,9 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
         b = N * vec / 2 + X * (blk / 2 + 4.0 + vec / 2);
     else if (k == "fast_resid32_U") /* the batch engine's: own d + c in/out on top */
         b = N * (4 * vec) / 2 + X * (blk / 2 + 4.0 + vec / 2);
-    else if (k == "fast_thomas") /* G, b | Gam, dU out (y stays on chip when the line fits),
-                                  * U in/out when the line solve adds dU to U */
-        b = N * (2 * blk + 2 * vec) + (thomas_adds_u(ctx) ? N * 2 * vec : 0.0);
+    else if (k == "fast_thomas") /* G, b | Gam, dU out, U in/out (y stays on chip when the
+                                  * line fits) */
+        b = N * (2 * blk + 4 * vec);
     else if (k == "fast_thomas_dU") /* dU out only (line partitions, the batch engine) */
         b = N * (2 * blk + 2 * vec);
     else if (k == "fast_thomas32") /* c in/out of all inner solves but the last not counted */

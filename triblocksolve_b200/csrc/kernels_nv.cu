@@ -394,12 +394,13 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
             }
         }
     };
-    auto put = [&](size_t p, double x) {
+    /* u: U at p, read ahead when accumulate == 1 */
+    auto put = [&](size_t p, double x, double u) {
         dU[p * NV + i] = x;
         if (accumulate == 0)
             U[p * NV + i] = x;
         else if (accumulate == 1)
-            U[p * NV + i] += x;
+            U[p * NV + i] = u + x;
     };
     int issued = 0;
     if (lane == 0)
@@ -447,23 +448,26 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
                 xm -= gr[NV * j] * yt + cr[NV * j] * yb;
             }
         }
-        if (h == 0 && act) put(ptw, xm);
+        if (h == 0 && act) put(ptw, xm, accumulate == 1 ? U[ptw * NV + i] : 0.0);
         /* ---------------- backward */
-        double yv[P], nyv[P];
-        auto load_y = [&](int c, double *yy) {
+        /* y, and U when the solve adds dU to it, read one chunk ahead */
+        double yv[P], nyv[P], uv[P], nuv[P];
+        auto load_y = [&](int c, double *yy, double *uu) {
 #pragma unroll
             for (int q = 0; q < P; ++q) {
                 const int k = c * P + q;
-                yy[q] = (c >= 0 && k < len) ? y[(base + k) * NV + ii] : 0.0;
+                const bool ok = c >= 0 && k < len;
+                yy[q] = ok ? y[(base + k) * NV + ii] : 0.0;
+                uu[q] = (ok && accumulate == 1) ? U[(base + k) * NV + ii] : 0.0;
             }
         };
         __syncwarp();
-        load_y(nch - 1, yv);
+        load_y(nch - 1, yv, uv);
         double xp = xm;
         for (int jb = 0; jb < nf; ++jb) {
             const int job = nf + jb;
             const int c = nch - 1 - jb; /* this half's chunk (may be < 0) */
-            load_y(c - 1, nyv);
+            load_y(c - 1, nyv, nuv);
             const int s = job % NS;
             if (!__all_sync(NFULL, mbar_wait(&bars[s], (uint32_t)(job / NS) & 1u))) {
                 timed_out = true;
@@ -477,7 +481,7 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
                 const bool valid = c >= 0 && k < len;
                 const double xi = nv_row_step<NV>(sG + q * NB, ii, valid ? yv[q] : 0.0, xp, src0);
                 if (valid) {
-                    if (act) put(base + k, xi);
+                    if (act) put(base + k, xi, uv[q]);
                     xp = xi;
                 }
             }
@@ -487,7 +491,10 @@ __global__ void __launch_bounds__(32) nv_thomas_kernel(
                 ++issued;
             }
 #pragma unroll
-            for (int q = 0; q < P; ++q) yv[q] = nyv[q];
+            for (int q = 0; q < P; ++q) {
+                yv[q] = nyv[q];
+                uv[q] = nuv[q];
+            }
         }
     }
     if (timed_out && lane == 0) {
