@@ -966,9 +966,9 @@ def run_partition(args, L, K, shift, tol):
         kern = {}
         for name, (launches, ms) in prof.items():
             try:
-                # a partition's line solve writes dU only; its residual adds dU to U
-                b = solver.kernel_bytes({"fast_thomas": "fast_thomas_dU",
-                                         "fast_resid": "fast_resid_U"}.get(name, name))
+                # the owned lines' solves add dU to U; the residual adds it for the
+                # halo lines only (a few lines: counted as the single-system form)
+                b = solver.kernel_bytes(name)
             except Exception:
                 b = None
             avg_us = 1e3 * ms / launches if launches else 0.0

@@ -308,12 +308,18 @@ int tbs_gmres(tbs_ctx *ctx, int restart, int precond_sweeps, double rel_tol,
  * A solve from U = 0:
  *   tbs_part_start(ctx, &n0)          ||R_0|| over the owned cells
  *   repeat:
- *     tbs_part_solve_du(ctx)          line solves, dU of every line
+ *     tbs_part_solve_du(ctx)          line solves, dU of every line (the
+ *                                     owned lines' U + dU into a second U
+ *                                     buffer; the current U is untouched)
  *     for each halo line h: copy dU of h from its owner into this context
  *       (tbs_part_line_vector: owner to_line=0 into a device buffer, the
  *        buffer to another GPU by NCCL or a peer copy, then to_line=1 here)
- *     tbs_part_line_res(ctx, &n)      R from dU, U += dU, ||R|| over owned
- *   the global norm is sqrt(sum over partitions of n^2).
+ *     tbs_part_line_res(ctx, &n)      R from dU, the halo lines' U + dU,
+ *                                     the second buffer becomes the
+ *                                     current U, ||R|| over owned
+ *   the global norm is sqrt(sum over partitions of n^2).  A
+ *   tbs_part_solve_du issued before the norm is read (and dropped when the
+ *   solve ends there) leaves the solution unchanged.
  * Owned cells' U and dU are bit-identical to a tbs_sweep of the whole mesh;
  * a halo line's U is its owner's (it accumulates the copied dU).
  * tbs_true_residual_norm, on such a context, covers the owned cells.
@@ -455,10 +461,10 @@ int tbs_selftest_timeout(tbs_ctx *ctx, long long budget_cycles);
  * every array it must touch once), for the roofline numerator.  The
  * multi-RHS kernels take the group size as a suffix: "multi_thomas/8",
  * "multi_resid/8" (every right-hand side active).  "fast_thomas" and
- * "fast_resid" are the forms tbs_solve's FP64 sweeps run (at block size 9
- * the line solve adds dU to U); "fast_thomas_dU", "fast_resid_U" and
- * "fast_resid32_U" are the forms of line partitions and the batch engine,
- * whose residual kernels add the update instead. */
+ * "fast_resid" are the forms the FP64 sweeps of a context run (the line
+ * solve adds dU to U); "fast_thomas_dU", "fast_resid_U" and
+ * "fast_resid32_U" are the batch engine's forms, whose residual kernels add
+ * the update instead. */
 int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes);
 
 /* Linear residual R = rhs + D U + (sum over each cell's interior faces of

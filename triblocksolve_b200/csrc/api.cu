@@ -17,6 +17,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <utility>
 #include <cmath>
 #include <cstddef>
 #include <cstring>
@@ -132,7 +133,7 @@ static void drop_mesh(tbs_ctx *ctx) {
     double **dps[] = {&ctx->d_jacD, &ctx->d_O1, &ctx->d_O2, &ctx->d_rhs, &ctx->d_U, &ctx->d_dU,
                       &ctx->d_R, &ctx->d_Uinit, &ctx->d_scratch, &ctx->d_DLU, &ctx->d_DinvC,
                       &ctx->d_A, &ctx->d_Dinv, &ctx->d_G, &ctx->d_Gam, &ctx->d_X, &ctx->d_Up,
-                      &ctx->d_dUp, &ctx->d_b, &ctx->d_y, &ctx->d_rhsp, &ctx->d_Rp,
+                      &ctx->d_Up_alt, &ctx->d_dUp, &ctx->d_b, &ctx->d_y, &ctx->d_rhsp, &ctx->d_Rp,
                       &ctx->d_partials, &ctx->d_partials2, &ctx->d_hist, &ctx->d_gamlast,
                       &ctx->d_Dp, &ctx->d_XF};
     for (auto p : dps) *p = nullptr;
@@ -1845,8 +1846,8 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     if (k == "fast_resid") /* Dinv, X blocks, xnbr, neighbour dU, b out */
         b = N * (blk + vec) + X * (blk + 4.0 + vec);
     else if (k == "fast_resid_U")
-        /* the form that adds dU to U (line partitions, the batch engine): own
-         * dU and U in/out on top */
+        /* the form that adds dU to U (the batch engine): own dU and U in/out
+         * on top */
         b = N * (blk + vec + 3 * vec) + X * (blk + 4.0 + vec);
     else if (k == "fast_resid_rhs" || k == "fast_resid_check") /* Dinv, R in, b out */
         b = N * (blk + 2 * vec);
@@ -1859,7 +1860,7 @@ int tbs_kernel_bytes(tbs_ctx *ctx, const char *kernel, double *bytes) {
     else if (k == "fast_thomas") /* G, b | Gam, dU out, U in/out (y stays on chip when the
                                   * line fits) */
         b = N * (2 * blk + 4 * vec);
-    else if (k == "fast_thomas_dU") /* dU out only (line partitions, the batch engine) */
+    else if (k == "fast_thomas_dU") /* dU out only (the batch engine) */
         b = N * (2 * blk + 2 * vec);
     else if (k == "fast_thomas32") /* c in/out of all inner solves but the last not counted */
         b = N * (2 * blk + 2 * vec) / 2;
@@ -1947,7 +1948,15 @@ int tbs_part_solve_du(tbs_ctx *ctx) {
     CK(cudaSetDevice(ctx->device));
     int rc = part_check(ctx);
     if (rc) return rc;
-    RUN("fast_thomas", thomas64(ctx, ctx->d_b, ctx->d_dUp, ctx->d_Up, 2));
+    /* The owned lines' solves write U + dU into the second U buffer as they
+     * write dU; tbs_part_line_res adds the halo lines' (copied) dU there and
+     * makes it the current U.  Until then U stays the last counted sweep's,
+     * so a line solve issued ahead of the convergence test changes nothing
+     * that the solve reports. */
+    DA(ctx->d_Up_alt, (size_t)ctx->L.np16 * ctx->nvar);
+    RUN("fast_thomas", launch_fast_thomas<double>(ctx->stream, ctx->L, ctx->d_G, ctx->d_Gam, ctx->d_b,
+                                                  ctx->d_y, ctx->d_dUp, ctx->d_Up_alt, ctx->d_status, 1,
+                                                  ctx->nline - ctx->nhalo, ctx->d_Up));
     return TBS_OK;
     GUARD_END
 }
@@ -1958,8 +1967,18 @@ int tbs_part_line_res(tbs_ctx *ctx, double *owned_norm) {
     CK(cudaSetDevice(ctx->device));
     int rc = part_check(ctx);
     if (rc) return rc;
-    RUN("fast_resid", resid64(ctx, 1, ctx->d_dUp, nullptr, ctx->d_b, sink(ctx, 0, CondCtl{}),
-                              ctx->d_Up));
+    if (!ctx->d_Up_alt) return ctx_fail(ctx, TBS_ERR_STATE, "tbs_part_solve_du must come first");
+    {
+        /* the halo tiles' U + dU into the second buffer (the owned lines'
+         * were written by their line solves), which becomes the current U */
+        NormSink ns = sink(ctx, 0, CondCtl{});
+        ns.timer = ctx->d_ktimer;
+        RUN("fast_resid", launch_fast_resid<double>(ctx->stream, ctx->L, 1, ctx->d_Dinv, ctx->d_X,
+                                                    ctx->d_dUp, nullptr, ctx->d_b, ns, ctx->d_status,
+                                                    ctx->d_Up_alt, ctx->L.ntile_own, ctx->d_Up));
+        std::swap(ctx->d_Up, ctx->d_Up_alt);
+        drop_graph(ctx); /* a captured solve holds the old address */
+    }
     if (!owned_norm) return TBS_OK;
     rc = part_norm(ctx, owned_norm);
     if (ctx->prof) prof_resolve(ctx);

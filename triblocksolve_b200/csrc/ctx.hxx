@@ -64,6 +64,9 @@ struct tbs_ctx {
     double *d_Dinv = nullptr, *d_G = nullptr, *d_Gam = nullptr, *d_X = nullptr;
     double *d_Dp = nullptr, *d_XF = nullptr; /* MIXED: position-ordered original blocks */
     double *d_Up = nullptr, *d_dUp = nullptr, *d_b = nullptr, *d_y = nullptr;
+    /* a line partition's second U: its line solves write U + dU there and
+     * its residual launch makes it the current U (swapped with d_Up) */
+    double *d_Up_alt = nullptr;
     double *d_rhsp = nullptr, *d_Rp = nullptr;
     float *d_Dinv32 = nullptr, *d_G32 = nullptr, *d_Gam32 = nullptr, *d_X32 = nullptr;
     float *d_b32 = nullptr, *d_y32 = nullptr, *d_d32 = nullptr, *d_c32 = nullptr,

@@ -686,7 +686,7 @@ __device__ __forceinline__ bool fast_resid_body(
     int nx, int np16, int mode, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, const T *__restrict__ Rsrc,
     T *__restrict__ b, T *__restrict__ Uacc, const NormSink &ns, unsigned *status, int blk,
-    uint64_t *bar, uint32_t parity, const int *nbr_pre = nullptr) {
+    uint64_t *bar, uint32_t parity, const int *nbr_pre = nullptr, const T *__restrict__ Uin = nullptr) {
     extern __shared__ __align__(128) unsigned char smem[];
     T *sD = reinterpret_cast<T *>(smem + 128);
     T *sX = sD + RES_TILE * NB;
@@ -715,9 +715,10 @@ __device__ __forceinline__ bool fast_resid_body(
     }
     if (act && Uacc) {
         /* modes 1, 3: U += dU of this tile (the Thomas kernel leaves U to
-         * this kernel); mode 0: U = 0, the start of a sweep sequence */
+         * this kernel), the previous U read from Uin when set; mode 0:
+         * U = 0, the start of a sweep sequence */
         const size_t q = (size_t)p0 * NV + tid;
-        Uacc[q] = (mode >= 1) ? Uacc[q] + dU[q] : T(0);
+        Uacc[q] = (mode >= 1) ? (Uin ? Uin[q] : Uacc[q]) + dU[q] : T(0);
     }
     if (mode >= 1 && act) {
         /* neighbour dU gathers overlap the bulk copies (their indices
@@ -802,7 +803,8 @@ __device__ __forceinline__ bool fast_resid_body(
 template <typename T>
 __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T *Dinv, const T *X,
                                             const int *xnbr, const T *dU, const T *Rsrc, T *b,
-                                            T *Uacc, const NormSink &ns, unsigned *status) {
+                                            T *Uacc, const NormSink &ns, unsigned *status,
+                                            int u_tile0 = 0, const T *Uin = nullptr) {
     timer_launch_start(ns.timer);
     uint64_t *bar = resid_bar_init();
     const int ntiles = np16 / RES_TILE;
@@ -822,8 +824,9 @@ __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T 
 #pragma unroll
         for (int s = 0; s < PRE; ++s)
             nxt[s] = (pre && s < nx && wn < ntiles) ? xnbr[(size_t)s * np16 + wn * RES_TILE + c] : -1;
-        const bool ok = fast_resid_body<T>(nx, np16, mode, Dinv, X, xnbr, dU, Rsrc, b, Uacc, ns,
-                                           status, w, bar, parity, pre ? nbr : nullptr);
+        const bool ok = fast_resid_body<T>(nx, np16, mode, Dinv, X, xnbr, dU, Rsrc, b,
+                                           w >= u_tile0 ? Uacc : nullptr, ns, status, w, bar, parity,
+                                           pre ? nbr : nullptr, Uin);
         parity ^= 1u;
         if (!ok) break;
 #pragma unroll
@@ -834,13 +837,15 @@ __device__ __forceinline__ bool resid_tiles(int nx, int np16, int mode, const T 
     return finalize_total(ns, (ns.ntiles > 0 && ns.ntiles < ntiles) ? ns.ntiles : ntiles);
 }
 
-/* mode 1 (R = sum X dU over the cross-line slots) */
+/* mode 1 (R = sum X dU over the cross-line slots); U += dU (Uacc = Uin +
+ * dU when Uin is set) for the tiles from u_tile0 on: a line partition's
+ * halo tiles, whose line solves leave U alone */
 template <typename T>
 __global__ void __launch_bounds__(RES_THREADS_FAST) fast_resid_kernel(
     int nx, int np16, const T *__restrict__ Dinv, const T *__restrict__ X,
     const int *__restrict__ xnbr, const T *__restrict__ dU, T *__restrict__ b,
-    T *__restrict__ Uacc, NormSink ns, unsigned *status) {
-    resid_tiles<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status);
+    T *__restrict__ Uacc, NormSink ns, unsigned *status, int u_tile0, const T *__restrict__ Uin) {
+    resid_tiles<T>(nx, np16, 1, Dinv, X, xnbr, dU, nullptr, b, Uacc, ns, status, u_tile0, Uin);
 }
 
 /* mode 3 (b = -sum (Dinv X) dU: premultiplied cross-line blocks, no norm) */
@@ -885,7 +890,7 @@ static int resid_grid_persistent(const void *fn, size_t smem, int ntiles) {
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv, const T *X,
                       const T *dU, const T *Rsrc, T *b, const NormSink &ns, unsigned *status,
-                      T *Uacc) {
+                      T *Uacc, int u_tile0, const T *Uin) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     const int grid = fast_resid_grid(L.np16);
     if (mode == 4) {
@@ -920,7 +925,7 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
     else if (mode == 1)
         fast_resid_kernel<T><<<resid_grid_persistent((const void *)fast_resid_kernel<T>, smem, grid),
                                RES_THREADS_FAST, smem, st>>>(L.nx, L.np16, Dinv, X, L.xnbr, dU, b, Uacc,
-                                                             ns, status);
+                                                             ns, status, u_tile0, Uin);
     else
         fast_resid_rhs_kernel<T><<<resid_grid_persistent((const void *)fast_resid_rhs_kernel<T>, smem, grid),
                                    RES_THREADS_FAST, smem, st>>>(L.np16, Dinv, Rsrc, b, Uacc, ns, status);
@@ -929,10 +934,10 @@ int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *D
 
 template int launch_fast_resid<double>(cudaStream_t, const FastLayout &, int, const double *,
                                        const double *, const double *, const double *, double *,
-                                       const NormSink &, unsigned *, double *);
+                                       const NormSink &, unsigned *, double *, int, const double *);
 template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, const float *,
                                       const float *, const float *, const float *, float *,
-                                      const NormSink &, unsigned *, float *);
+                                      const NormSink &, unsigned *, float *, int, const float *);
 
 /* =========================================================== line Thomas
  * One warp per line, twisted: lanes 0..8 run the top chain and lanes
@@ -1137,11 +1142,14 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
 template <bool WS>
 __host__ __device__ constexpr int thomas_hdr() { return WS ? 256 : 128; }
 
+/* accumulate = 1 reads U from Uin when it is set (a second buffer: the
+ * previous U stays intact), else from U itself */
 template <typename T, int P, bool YS, bool WS = false>
 __device__ __forceinline__ bool thomas_line(
     int NS, int accumulate, int ps, int n, int m, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
-    T *__restrict__ U, unsigned *status, unsigned char *smem, uint32_t &pbase, uint64_t pol) {
+    T *__restrict__ U, unsigned *status, unsigned char *smem, uint32_t &pbase, uint64_t pol,
+    const T *__restrict__ Uin = nullptr) {
     uint64_t *bars = reinterpret_cast<uint64_t *>(smem);
     /* WS (warp-specialised CTA of two warps): bars[0..NS) complete when a
      * stage's copies have landed, bars[8..8+NS) when warp 0 has consumed
@@ -1170,6 +1178,7 @@ __device__ __forceinline__ bool thomas_line(
     T *yl = y + (size_t)ps * NV;
     T *dUl = dU + (size_t)ps * NV;
     T *Ul = U ? U + (size_t)ps * NV : nullptr;
+    const T *Uil = Uin ? Uin + (size_t)ps * NV : Ul;
     auto parity = [&](int job) { return ((pbase >> (job % NS)) ^ (uint32_t)(job / NS)) & 1u; };
 
     const bool producer = WS && (threadIdx.x >> 5) == 1;
@@ -1298,7 +1307,7 @@ __device__ __forceinline__ bool thomas_line(
             else {
                 dUl[(size_t)ptw * NV + lane] = xm;
                 if (accumulate < 2)
-                    Ul[(size_t)ptw * NV + lane] = (accumulate ? Ul[(size_t)ptw * NV + lane] : T(0)) + xm;
+                    Ul[(size_t)ptw * NV + lane] = (accumulate ? Uil[(size_t)ptw * NV + lane] : T(0)) + xm;
             }
         }
         __syncwarp();
@@ -1313,7 +1322,7 @@ __device__ __forceinline__ bool thomas_line(
                 uu[q] = T(0);
                 if (!YS && c >= 0 && k < len) { /* lanes 9..15: lane 8's values */
                     yy[q] = ld_hint(yl + (size_t)(cpos + k) * NV + i, ypol_first);
-                    if (accumulate == 1) uu[q] = Ul[(size_t)(cpos + k) * NV + i];
+                    if (accumulate == 1) uu[q] = Uil[(size_t)(cpos + k) * NV + i];
                 }
             }
         };
@@ -1363,7 +1372,7 @@ __device__ __forceinline__ bool thomas_line(
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
                     const int t = t0 + 32 * k;
-                    u[k] = (accumulate == 1 && t < nv) ? Ul[t] : T(0);
+                    u[k] = (accumulate == 1 && t < nv) ? Uil[t] : T(0);
                 }
 #pragma unroll
                 for (int k = 0; k < B; ++k) {
@@ -1414,20 +1423,21 @@ __device__ __forceinline__ void thomas_init_bars(unsigned char *smem, int NS) {
 }
 
 /* one CTA (one warp) per line */
+/* lines from nacc on leave U alone (accumulate 2) */
 template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(32) fast_thomas_kernel(
-    int nline, int NS, int accumulate, const int *__restrict__ line_start,
+    int nline, int NS, int accumulate, int nacc, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
-    T *__restrict__ U, unsigned *status) {
+    T *__restrict__ U, const T *__restrict__ Uin, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int l = blockIdx.x;
     if (l >= nline) return;
     thomas_init_bars(smem, NS);
     const uint64_t pol = threadIdx.x == 0 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam, b, y,
-                          dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS>(NS, l < nacc ? accumulate : 2, line_start[l], line_len[l], line_twist[l], G,
+                          Gam, b, y, dU, U, status, smem, pbase, pol, Uin);
 }
 
 /* Warp-specialised form, one CTA of two warps per line: warp 1 issues the
@@ -1436,10 +1446,10 @@ __global__ void __launch_bounds__(32) fast_thomas_kernel(
  * longer stops every chunk to issue the next copies. */
 template <typename T, int P, bool YS>
 __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
-    int nline, int NS, int accumulate, const int *__restrict__ line_start,
+    int nline, int NS, int accumulate, int nacc, const int *__restrict__ line_start,
     const int *__restrict__ line_len, const int *__restrict__ line_twist, const T *__restrict__ G,
     const T *__restrict__ Gam, const T *__restrict__ b, T *__restrict__ y, T *__restrict__ dU,
-    T *__restrict__ U, unsigned *status) {
+    T *__restrict__ U, const T *__restrict__ Uin, unsigned *status) {
     extern __shared__ __align__(128) unsigned char smem[];
     const int l = blockIdx.x;
     if (l >= nline) return;
@@ -1457,8 +1467,8 @@ __global__ void __launch_bounds__(64) fast_thomas_ws_kernel(
     __syncthreads();
     const uint64_t pol = threadIdx.x == 32 ? policy_evict_first() : 0;
     uint32_t pbase = 0;
-    thomas_line<T, P, YS, true>(NS, accumulate, line_start[l], line_len[l], line_twist[l], G, Gam,
-                                b, y, dU, U, status, smem, pbase, pol);
+    thomas_line<T, P, YS, true>(NS, l < nacc ? accumulate : 2, line_start[l], line_len[l],
+                                line_twist[l], G, Gam, b, y, dU, U, status, smem, pbase, pol, Uin);
 }
 
 /* Persistent form over many systems: each CTA (one warp) takes (system,
@@ -1626,23 +1636,25 @@ static const void *thomas_fn(bool ys) {
 
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam, const T *b,
-                       T *y, T *dU, T *U, unsigned *status, int accumulate) {
+                       T *y, T *dU, T *U, unsigned *status, int accumulate, int nacc, const T *Uin) {
     if (L.nv != NV) return (int)cudaErrorInvalidValue;
     const bool ws = thomas_ws(L);
     const ThomasCfg c = ws ? thomas_cfg<T, true>(L) : thomas_cfg<T>(L);
     const void *fn = ws ? thomas_fn<T, true>(c.ys) : thomas_fn<T, false>(c.ys);
     int ns = c.NS, nline = L.nline;
+    if (nacc < 0 || nacc > nline) nacc = nline;
     const int *ls = L.line_start, *ll = L.line_len, *lt = L.line_twist;
-    void *args[] = {&nline, &ns, &accumulate, &ls, &ll, &lt, &G, &Gam, &b, &y, &dU, &U, &status};
+    void *args[] = {&nline, &ns,  &accumulate, &nacc, &ls, &ll, &lt,
+                    &G,     &Gam, &b,          &y,    &dU, &U,  &Uin, &status};
     return (int)cudaLaunchKernel(fn, dim3(L.nline), dim3(ws ? 64 : 32), args, c.smem, st);
 }
 
 template int launch_fast_thomas<double>(cudaStream_t, const FastLayout &, const double *,
                                         const double *, const double *, double *, double *,
-                                        double *, unsigned *, int);
+                                        double *, unsigned *, int, int, const double *);
 template int launch_fast_thomas<float>(cudaStream_t, const FastLayout &, const float *,
                                        const float *, const float *, float *, float *, float *,
-                                       unsigned *, int);
+                                       unsigned *, int, int, const float *);
 
 static int smem_limit(const void *fn) {
     int dev = 0, optin = 0;

@@ -199,15 +199,21 @@ constexpr int NORM_CHECK = 2;
 
 /* mode 0: R given (Rsrc); 1: R = sum X dU (with norm); 3: X holds Dinv X,
  * b = -sum X dU, no norm; 4: b = sum X dU - Rsrc (the product with J of
- * the iterate of line sweeps on Rsrc + J z = 0), no Dinv, no norm.  Uacc (may be null): modes 1, 3 add dU to it for
- * the tile's positions, mode 0 sets it to zero there */
+ * the iterate of line sweeps on Rsrc + J z = 0), no Dinv, no norm.  Uacc
+ * (may be null): modes 1, 3 add dU to it for the tile's positions, mode 0
+ * sets it to zero there; mode 1 only from tile u_tile0 on, and with Uin
+ * set as Uacc = Uin + dU */
 template <typename T>
 int launch_fast_resid(cudaStream_t st, const FastLayout &L, int mode, const T *Dinv,
                       const T *X, const T *dU, const T *Rsrc, T *b, const NormSink &ns,
-                      unsigned *status, T *Uacc = nullptr);
+                      unsigned *status, T *Uacc = nullptr, int u_tile0 = 0,
+                      const T *Uin = nullptr);
+/* accumulate 0: U = dU, 1: U += dU (U = Uin + dU when Uin is set), 2: U
+ * left alone; lines from nacc on (nacc >= 0) leave U alone */
 template <typename T>
 int launch_fast_thomas(cudaStream_t st, const FastLayout &L, const T *G, const T *Gam,
-                       const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate);
+                       const T *b, T *y, T *dU, T *U, unsigned *status, int accumulate,
+                       int nacc = -1, const T *Uin = nullptr);
 int fast_kernels_init();
 /* Several lines' vectors packed into (or unpacked from) one contiguous
  * buffer by one launch: line k's span is [start[k]*9, start[k]*9 + len[k]*9)
