@@ -346,10 +346,12 @@ int tbs_part_line_vector(tbs_ctx *ctx, int which, int line, double *d_buf,
                          int to_line);
 
 /* The true-residual check of a partitioned solve: R = rhs + J U of the
- * owned cells from the original blocks, the next line solves' input formed
- * from it (so the sweeps go on from the true residual), its owned norm in
- * *owned_norm (or, with NULL, kept for tbs_part_owned_norm).  The loop runs
- * it when the global recursive norm meets the tolerance, as tbs_solve does. */
+ * owned cells from the original blocks and its owned norm in *owned_norm
+ * (or, with NULL, kept for tbs_part_owned_norm).  The next
+ * tbs_part_solve_du forms its line solves' input from that R (so the
+ * sweeps go on from the true residual); a check that ends the solve forms
+ * nothing more.  The loop runs it when the global recursive norm meets the
+ * tolerance, as tbs_solve does. */
 int tbs_part_check(tbs_ctx *ctx, double *owned_norm);
 
 /* The device-clock record of the sweeps' cross-line residual launches

@@ -97,6 +97,41 @@ def test_partitioned_solve_stops_at_the_same_sweep():
         s.close()
 
 
+def test_partitioned_sweeps_restart_from_the_true_residual():
+    """A check after every sweep: each check's true residual is the next
+    line solves' input (tbs_part_solve_du forms it), so every sweep starts
+    from rhs + J U as the reference's own sweep does; the checked norms
+    follow the oracle's history and the solution the whole mesh's."""
+    mesh, jac = _problem("ragged", shift=4.0)
+    n = 5
+    ref = oracle.lij(mesh, jac.jacD, jac.jacO1, jac.jacO2, jac.rhs, n)
+    whole = _whole(mesh, jac)
+    whole.sweep(n)
+    Uw = whole.solution()
+    parts, sw = _parts(mesh, jac, 4)
+    run = PartitionedSolve(sw, LocalExchange(parts, sw))
+    hist = [run.start()]
+    for _ in range(n):
+        run._solve_and_exchange()
+        rec = float(run._line_res().item()) ** 0.5
+        for s in sw:
+            s.check_async()
+        hist.append(float(run.ex.norm_sq_async(sw).item()) ** 0.5)
+        assert abs(hist[-1] - rec) <= TOL * hist[0]
+    hist = np.array(hist)
+    assert np.all(np.abs(hist - ref["hist"]) <= TOL * ref["hist"][0])
+    U = gather_solution(parts, [s.solution() for s in sw], mesh.nelem)
+    assert np.max(np.abs(U - Uw)) <= 1e-12 * np.max(np.abs(Uw))
+    # a check that ends the solve leaves the next start clean: a plain
+    # partitioned sweep sequence afterwards repeats the first one's norms
+    h2 = np.array([run.start()] + [run.sweep() for _ in range(n)])
+    h1 = np.array([run.start()] + [run.sweep() for _ in range(n)])
+    assert np.array_equal(h1, h2)
+    whole.close()
+    for s in sw:
+        s.close()
+
+
 def test_partition_refusals():
     mesh, jac = _problem((12, 16))
     parts, sw = _parts(mesh, jac, 2)

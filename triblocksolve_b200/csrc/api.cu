@@ -1936,6 +1936,7 @@ int tbs_part_start(tbs_ctx *ctx, double *owned_norm) {
     if (rc) return rc;
     rc = ctx_set_state(ctx, 0.0, 0x7fffffff);
     if (rc) return rc;
+    ctx->part_restart = false;
     rc = prime(ctx, CondCtl{});
     if (rc) return rc;
     return part_norm(ctx, owned_norm);
@@ -1954,6 +1955,11 @@ int tbs_part_solve_du(tbs_ctx *ctx) {
      * so a line solve issued ahead of the convergence test changes nothing
      * that the solve reports. */
     DA(ctx->d_Up_alt, (size_t)ctx->L.np16 * ctx->nvar);
+    if (ctx->part_restart) {
+        /* the sweeps go on from the true residual of the last check */
+        RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b, no_sink(), nullptr));
+        ctx->part_restart = false;
+    }
     RUN("fast_thomas", launch_fast_thomas<double>(ctx->stream, ctx->L, ctx->d_G, ctx->d_Gam, ctx->d_b,
                                                   ctx->d_y, ctx->d_dUp, ctx->d_Up_alt, ctx->d_status, 1,
                                                   ctx->nline - ctx->nhalo, ctx->d_Up));
@@ -2014,13 +2020,16 @@ int tbs_part_check(tbs_ctx *ctx, double *owned_norm) {
     int rc = part_check(ctx);
     if (rc) return rc;
     /* R = rhs + J U of the owned cells (their halo neighbours' U are the
-     * owners' copies), b = -Dinv R for the next line solves, owned norm */
+     * owners' copies) and its owned norm; b = -Dinv R for the next line
+     * solves only if sweeps follow (the next tbs_part_solve_du forms it, so
+     * a passing check costs no factor read) */
     cudaStream_t st = ctx->stream;
     RUN("full_resid", launch_full_resid<double>(st, ctx->nelem_own, ctx->d_epoint, ctx->d_ef, ctx->d_fc,
                                                 ctx->L.pos_of_elem, ctx->d_jacD, ctx->d_O1, ctx->d_O2,
                                                 ctx->d_rhs, ctx->d_Up, ctx->d_Rp, ctx->d_partials2));
-    RUN("fast_resid_check", resid64(ctx, 0, ctx->d_dUp, ctx->d_Rp, ctx->d_b,
-                                    sink(ctx, NORM_CHECK, CondCtl{}), nullptr));
+    RUN("reduce_norm", launch_reduce_norm(st, ctx->d_partials2, full_resid_blocks(ctx->nelem_own),
+                                          ctx->d_state, ctx->d_hist, NORM_CHECK, 0, 0, 0, 0));
+    ctx->part_restart = true;
     if (!owned_norm) return TBS_OK;
     return part_norm(ctx, owned_norm);
     GUARD_END

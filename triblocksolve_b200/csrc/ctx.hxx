@@ -43,6 +43,9 @@ struct tbs_ctx {
      * lines another partition owns (swept, never counted in a norm); the
      * owned lines' cells are elements 0..nelem_own-1 */
     int nhalo = 0, nelem_own = 0;
+    /* tbs_part_check left a true residual that the next tbs_part_solve_du
+     * turns into its line solves' input (b = -Dinv R) */
+    bool part_restart = false;
     std::vector<int> h_line_start; /* first position of every line */
     int *d_epoint = nullptr, *d_ef = nullptr, *d_fc = nullptr, *d_linesize = nullptr;
     int *d_linepoint = nullptr, *d_lines = nullptr, *d_lineface = nullptr, *d_identity = nullptr;

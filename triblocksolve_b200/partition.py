@@ -204,7 +204,7 @@ class PartitionSolver(Solver):
 
     def check_async(self) -> None:
         """tbs_part_check without reading the norm: the true residual of the
-        owned cells and the next line solves' input formed from it."""
+        owned cells (the next solve_du forms its input from it)."""
         self._chk(N.lib.tbs_part_check(self.ctx, None))
 
     def owned_norm_to(self, t) -> None:
