@@ -1098,10 +1098,12 @@ __device__ __forceinline__ void fwd_chunk(const T *sG, const T *sB, T *bc, T *ys
     }
 }
 
+/* uv: U of the chunk's cells read ahead in registers, or sU (when set):
+ * the chunk's U staged behind its Gam rows */
 template <typename T, int P, bool CHECK, bool YS>
 __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv, const T *uv,
                                           T *dUl, T *Ul, int kbase, int len, int cpos, int i,
-                                          const LaneOff &o) {
+                                          const LaneOff &o, const T *sU = nullptr) {
     typename RowOf<T>::type cur_row, next_row;
     load_row(cur_row, sG + (P - 1) * NB, o, (P - 1) & 1);
 #pragma unroll
@@ -1123,7 +1125,7 @@ __device__ __forceinline__ void bwd_chunk(const T *sG, T *bc, T *ys, const T *yv
                 ys[pos * NV + i] = d;
             } else {
                 dUl[(size_t)pos * NV + i] = d;
-                if (Ul) Ul[(size_t)pos * NV + i] = uv[q] + d;
+                if (Ul) Ul[(size_t)pos * NV + i] = (sU ? sU[q * NV + i] : uv[q]) + d;
             }
         }
         __syncwarp();
@@ -1182,6 +1184,10 @@ __device__ __forceinline__ bool thomas_line(
     auto parity = [&](int job) { return ((pbase >> (job % NS)) ^ (uint32_t)(job / NS)) & 1u; };
 
     const bool producer = WS && (threadIdx.x >> 5) == 1;
+    /* warp-specialised form: the copy warp also stages U behind the
+     * backward chunks' Gam rows (where the forward stages hold b), so the
+     * chain warp reads it from shared memory */
+    const bool stage_u = WS && !YS && accumulate == 1 && Ul != nullptr;
     __syncwarp(); /* the previous line's readers of the stages are done */
     if (!producer)
         for (int t = lane; t < 80; t += 32) bcall[t] = T(0);
@@ -1198,9 +1204,9 @@ __device__ __forceinline__ bool thomas_line(
             if (c < nchT) bytes += cells(m, c) * (NB + NV) * sizeof(T);
             if (c < nchB) bytes += cells(nb, c) * (NB + NV) * sizeof(T);
         } else {
-            const int jb = job - nf;
-            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * NB * sizeof(T);
-            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * NB * sizeof(T);
+            const int jb = job - nf, bw = NB + (stage_u ? NV : 0);
+            if (nchT - 1 - jb >= 0) bytes += cells(m, nchT - 1 - jb) * bw * sizeof(T);
+            if (nchB - 1 - jb >= 0) bytes += cells(nb, nchB - 1 - jb) * bw * sizeof(T);
         }
         mbar_arrive_expect_tx(&bars[s], bytes);
         for (int hh = 0; hh < 2; ++hh) {
@@ -1218,6 +1224,9 @@ __device__ __forceinline__ bool thomas_line(
                 if (c < 0) continue;
                 const int cnt = cells(ln, c);
                 bulk_g2s_hint(hb, Gam + (size_t)(ps + cp + c * P) * NB, cnt * NB * sizeof(T), &bars[s], pol);
+                if (stage_u)
+                    bulk_g2s(hb + P * NB * sizeof(T), Uil + (size_t)(cp + c * P) * NV, cnt * NV * sizeof(T),
+                             &bars[s]);
             }
         }
     };
@@ -1322,7 +1331,7 @@ __device__ __forceinline__ bool thomas_line(
                 uu[q] = T(0);
                 if (!YS && c >= 0 && k < len) { /* lanes 9..15: lane 8's values */
                     yy[q] = ld_hint(yl + (size_t)(cpos + k) * NV + i, ypol_first);
-                    if (accumulate == 1) uu[q] = Uil[(size_t)(cpos + k) * NV + i];
+                    if (accumulate == 1 && !stage_u) uu[q] = Uil[(size_t)(cpos + k) * NV + i];
                 }
             }
         };
@@ -1341,12 +1350,13 @@ __device__ __forceinline__ bool thomas_line(
             const T *sG = reinterpret_cast<const T *>(st0 + (size_t)s * stage + h * half);
             const bool full = (nchT - 1 - jb) * P + P <= m && (nchB - 1 - jb) * P + P <= nb &&
                               nchT - 1 - jb >= 0 && nchB - 1 - jb >= 0;
+            const T *sU = stage_u ? sG + P * NB : nullptr;
             if (full)
                 bwd_chunk<T, P, false, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
-                                           c * P, len, cpos, i, off);
+                                           c * P, len, cpos, i, off, sU);
             else
                 bwd_chunk<T, P, true, YS>(sG, bc, ys, yv, uv, dUl, accumulate < 2 ? Ul : nullptr,
-                                          c * P, len, cpos, i, off);
+                                          c * P, len, cpos, i, off, sU);
             __syncwarp();
             if (WS) {
                 if (lane == 0) mbar_arrive(&empty[s]);
