@@ -955,11 +955,15 @@ template int launch_fast_resid<float>(cudaStream_t, const FastLayout &, int, con
  * Gam_s x_{s+1} (s+1 toward the twist).
  * YS: the line's y and x live in shared memory, and dU / U are written with
  * coalesced 16-byte accesses after the line is solved; otherwise y goes to
- * global memory (read back one chunk ahead) and dU / U per step.
+ * global memory (read back one chunk ahead) and dU / U per step, U read
+ * one chunk ahead with y (one-warp form) or staged behind the backward
+ * chunk's Gam rows by the copy warp (warp-specialised form).
  *   accumulate = 0:  U = dU
- *   accumulate = 1:  U += dU
+ *   accumulate = 1:  U += dU (the FP64 sweeps of a context; U read from a
+ *                    second buffer Uin when one is given: line partitions)
  *   accumulate = 2:  U untouched (the residual kernel that follows adds
- *                    dU to U for its tile, with coalesced tile accesses)
+ *                    dU to U for its tile, with coalesced tile accesses:
+ *                    the batch engine)
  */
 constexpr int THOMAS_P = 8;
 
