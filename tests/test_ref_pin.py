@@ -6,7 +6,8 @@ src/main.cxx:180-229 order (oracle/ref_driver.c).
 
 Bar: bit-identical factors, packed lower blocks, and U, R, dU after every
 sweep, on the structured meshes of the benchmark configs, ragged meshes with
-permuted numbering, a single line, one-cell lines, and block sizes 9 and 5.
+permuted numbering, a single line, one-cell lines, and block sizes 2, 5, 9,
+12 and 16 (the span of the general-size kernels).
 
 oracle/_ref is built by `make -C oracle ref REFERENCE=<reference checkout>`
 (the package build does it where the checkout exists); without it these
@@ -33,6 +34,9 @@ CASES = {
     "one_cell_lines": (lambda: point_mesh(Mesh.structured(8, 10)), 9.0, 8),
     "nvar5": (lambda: Mesh.structured(12, 16, nvar=5), 9.0, 10),
     "nvar5_ragged": (lambda: ragged_mesh([4, 6, 2, 5], seed=2, nvar=5), 5.0, 8),
+    "nvar2": (lambda: Mesh.structured(10, 12, nvar=2), 4.0, 8),
+    "nvar12_ragged": (lambda: ragged_mesh([3, 7, 1, 5], seed=5, nvar=12), 12.0, 6),
+    "nvar16": (lambda: Mesh.structured(6, 9, nvar=16), 16.0, 6),
 }
 
 
